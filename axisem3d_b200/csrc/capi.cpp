@@ -1,0 +1,426 @@
+// capi.cpp -- the extern "C" boundary (include/axg.h). Copies the caller's
+// arrays into the host model, validates them, and forwards to the engine. No
+// exception crosses this boundary: every failure becomes an AXG_E_* code with a
+// "Class::method || message" text available from axg_last_error().
+#include "engine.hpp"
+
+#include <cstring>
+#include <string>
+
+struct axg_solver {
+    axg_config cfg;
+    axg::HostModel model;
+    std::unique_ptr<axg::EngineBase> eng;
+    std::string err;
+    bool finalized = false;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(axg_solver *h, F &&f) {
+    if (!h) return AXG_E_ARG;
+    try {
+        f();
+        return AXG_OK;
+    } catch (const axg::Error &e) {
+        h->err = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        h->err = e.what();
+        return AXG_E_ARG;
+    }
+}
+
+template <class X>
+std::vector<X> copy(const X *p, size_t n) {
+    return p ? std::vector<X>(p, p + n) : std::vector<X>();
+}
+
+void need_open(const axg_solver *h) {
+    if (h->finalized) throw axg::Error(AXG_E_STATE, "axg_set || model already finalized.");
+}
+
+void points_from(axg::HostPoints &hp, int count, const int32_t *nr, const int32_t *mnr,
+                 const int64_t *moff, const double *mass, const uint8_t *axial,
+                 const uint8_t *surface, int ndim, const char *who) {
+    if (count < 0 || (count && (!nr || !mass)))
+        throw axg::Error(AXG_E_ARG, std::string(who) + " || missing nr or mass.");
+    hp.count = count;
+    hp.ndim = ndim;
+    hp.nr = copy(nr, count);
+    hp.mass_nr = copy(mnr, count);
+    hp.mass_off = copy(moff, count);
+    size_t nmass = 0;
+    for (int p = 0; p < count; p++) {
+        int m = mnr ? mnr[p] : 1;
+        if (nr[p] < 1) throw axg::Error(AXG_E_ARG, std::string(who) + " || nr must be >= 1.");
+        if (m != 1 && m != nr[p]) throw axg::Error(AXG_E_ARG, std::string(who) + " || mass_nr must be 1 or nr.");
+        size_t end = (size_t)(moff ? moff[p] : p) + m;
+        nmass = std::max(nmass, end);
+        if (!moff && m != 1) throw axg::Error(AXG_E_ARG, std::string(who) + " || mass_offset required for 3-D mass.");
+    }
+    hp.mass = copy(mass, nmass);
+    for (double v : hp.mass)
+        if (!(v > 0)) throw axg::Error(AXG_E_ARG, std::string(who) + " || mass must be positive.");
+    hp.axial = copy(axial, count);
+    hp.surface = copy(surface, count);
+}
+
+int nmod(int rheo) { return rheo == AXG_ISO ? 2 : rheo == AXG_TISO ? 5 : 21; }
+
+}  // namespace
+
+extern "C" {
+
+const char *axg_version(void) { return "axg 0.1 (sm_100a, nPol=4)"; }
+
+int axg_create(const axg_config *cfg, axg_solver **out) {
+    if (!cfg || !out) return AXG_E_ARG;
+    *out = nullptr;
+    if (cfg->precision < AXG_FP64 || cfg->precision > AXG_MIXED) return AXG_E_ARG;
+    if (!(cfg->dt > 0) || cfg->nsls < 0 || cfg->nsls > AXG_MAX_SLS) return AXG_E_ARG;
+    axg_solver *h = new axg_solver();
+    h->cfg = *cfg;
+    try {
+        switch (cfg->precision) {
+            case AXG_FP32: h->eng = axg::make_engine_fp32(*cfg); break;
+            case AXG_FP64: h->eng = axg::make_engine_fp64(*cfg); break;
+            default: h->eng = axg::make_engine_mixed(*cfg); break;
+        }
+    } catch (const axg::Error &e) {
+        g_create_error = e.what();
+        delete h;
+        return e.code;
+    }
+    *out = h;
+    return AXG_OK;
+}
+
+int axg_destroy(axg_solver *h) {
+    delete h;
+    return AXG_OK;
+}
+
+const char *axg_last_error(const axg_solver *h) {
+    return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int axg_set_solid_points(axg_solver *h, const axg_solid_points *p) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!p) throw axg::Error(AXG_E_ARG, "SolidPoint || null description.");
+        points_from(h->model.sp, p->count, p->nr, p->mass_nr, p->mass_offset, p->mass, p->axial,
+                    nullptr, 3, "SolidPoint::SolidPoint");
+    });
+}
+
+int axg_set_fluid_points(axg_solver *h, const axg_fluid_points *p) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!p) throw axg::Error(AXG_E_ARG, "FluidPoint || null description.");
+        points_from(h->model.fp, p->count, p->nr, p->mass_nr, p->mass_offset, p->mass, p->axial,
+                    p->surface, 1, "FluidPoint::FluidPoint");
+    });
+}
+
+int axg_set_solid_elements(axg_solver *h, const axg_solid_elements *e) {
+    return guarded(h, [&] {
+        need_open(h);
+        const char *who = "SolidElement::SolidElement";
+        if (!e || e->count < 0) throw axg::Error(AXG_E_ARG, std::string(who) + " || null description.");
+        int n = e->count;
+        if (n && (!e->nr || !e->points || !e->axial || !e->geometry || !e->rheology ||
+                  !e->mat_offset || !e->moduli))
+            throw axg::Error(AXG_E_ARG, std::string(who) + " || missing array.");
+        axg::HostSolidElements &s = h->model.se;
+        s.count = n;
+        s.nr = copy(e->nr, n);
+        s.pts = copy(e->points, (size_t)n * 25);
+        s.axial = copy(e->axial, n);
+        s.geom = copy(e->geometry, (size_t)n * 150);
+        s.rtz = copy(e->rtz, n);
+        s.rheo = copy(e->rheology, n);
+        s.is3d = copy(e->is3d, n);
+        s.att = copy(e->attenuation, n);
+        s.mat_off = copy(e->mat_offset, n);
+        s.att_off = copy(e->att_offset, n);
+        bool any_rtz = false;
+        size_t nm_end = 0, na_end = 0;
+        for (int i = 0; i < n; i++) {
+            if (s.nr[i] < 1) throw axg::Error(AXG_E_ARG, std::string(who) + " || nr must be >= 1.");
+            if (s.rheo[i] < AXG_ISO || s.rheo[i] > AXG_ANISO)
+                throw axg::Error(AXG_E_ARG, std::string(who) + " || unknown rheology.");
+            int ns = (s.is3d.size() && s.is3d[i]) ? s.nr[i] : 1;
+            nm_end = std::max(nm_end, (size_t)s.mat_off[i] + (size_t)nmod(s.rheo[i]) * ns * 25);
+            int att = s.att.size() ? s.att[i] : AXG_ATT_NONE;
+            if (att < AXG_ATT_NONE || att > AXG_ATT_CG4)
+                throw axg::Error(AXG_E_ARG, std::string(who) + " || unknown attenuation.");
+            if (att != AXG_ATT_NONE) {
+                if (!e->att_offset || !e->att_moduli)
+                    throw axg::Error(AXG_E_ARG, std::string(who) + " || attenuation arrays missing.");
+                int npa = att == AXG_ATT_CG4 ? 4 : 25;
+                na_end = std::max(na_end, (size_t)s.att_off[i] + (size_t)2 * ns * npa);
+            }
+            if (s.rtz.size() && s.rtz[i]) any_rtz = true;
+            // the element's nr is the maximum over its points (Element::pointSet)
+        }
+        if (any_rtz && !e->theta) throw axg::Error(AXG_E_ARG, std::string(who) + " || theta required for RTZ.");
+        s.theta = copy(e->theta, any_rtz ? (size_t)n * 25 : 0);
+        s.moduli = copy(e->moduli, nm_end);
+        s.att_moduli = copy(e->att_moduli, na_end);
+    });
+}
+
+int axg_set_fluid_elements(axg_solver *h, const axg_fluid_elements *e) {
+    return guarded(h, [&] {
+        need_open(h);
+        const char *who = "FluidElement::FluidElement";
+        if (!e || e->count < 0) throw axg::Error(AXG_E_ARG, std::string(who) + " || null description.");
+        int n = e->count;
+        if (n && (!e->nr || !e->points || !e->axial || !e->geometry || !e->mat_offset || !e->moduli))
+            throw axg::Error(AXG_E_ARG, std::string(who) + " || missing array.");
+        axg::HostFluidElements &s = h->model.fe;
+        s.count = n;
+        s.nr = copy(e->nr, n);
+        s.pts = copy(e->points, (size_t)n * 25);
+        s.axial = copy(e->axial, n);
+        s.geom = copy(e->geometry, (size_t)n * 150);
+        s.is3d = copy(e->is3d, n);
+        s.mat_off = copy(e->mat_offset, n);
+        size_t end = 0;
+        for (int i = 0; i < n; i++) {
+            if (s.nr[i] < 1) throw axg::Error(AXG_E_ARG, std::string(who) + " || nr must be >= 1.");
+            int ns = (s.is3d.size() && s.is3d[i]) ? s.nr[i] : 1;
+            end = std::max(end, (size_t)s.mat_off[i] + (size_t)ns * 25);
+        }
+        s.moduli = copy(e->moduli, end);
+    });
+}
+
+int axg_set_solid_fluid(axg_solver *h, const axg_solid_fluid *c) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!c || c->count < 0) throw axg::Error(AXG_E_ARG, "SolidFluidCoupling || null description.");
+        axg::HostCoupling &s = h->model.sf;
+        int n = c->count;
+        s.count = n;
+        s.sp = copy(c->solid_point, n); s.fp = copy(c->fluid_point, n);
+        s.nsu = copy(c->ns_unassembled, n); s.nzu = copy(c->nz_unassembled, n);
+        s.nsa = copy(c->ns_assembled, n); s.nza = copy(c->nz_assembled, n);
+        s.mf = copy(c->mass_fluid, n);
+        if (n && (s.sp.empty() || s.fp.empty() || s.nsu.empty() || s.nzu.empty() || s.nsa.empty() ||
+                  s.nza.empty() || s.mf.empty()))
+            throw axg::Error(AXG_E_ARG, "SolidFluidCoupling || missing array.");
+    });
+}
+
+static void sources_from(axg::HostSources &s, int n, const int32_t *el, const int32_t *nu,
+                         const int64_t *po, const double *pat, const axg_stf *stf, int ndim,
+                         const char *who) {
+    if (n < 0 || (n && (!el || !nu || !po || !pat || !stf)))
+        throw axg::Error(AXG_E_ARG, std::string(who) + " || missing array.");
+    s.count = n;
+    s.elem = copy(el, n);
+    s.nu = copy(nu, n);
+    s.pat_off = copy(po, n);
+    s.stf = copy(stf, n);
+    size_t end = 0;
+    for (int i = 0; i < n; i++) {
+        if (nu[i] < 1) throw axg::Error(AXG_E_ARG, std::string(who) + " || pattern needs >= 1 mode.");
+        if (stf[i].derivative_order < -1 || stf[i].derivative_order > 2)
+            throw axg::Error(AXG_E_ARG, "GaussianSTF::getValue || Unsupported derivative order.");
+        end = std::max(end, (size_t)po[i] + (size_t)nu[i] * ndim * 25);
+    }
+    s.pattern = copy(pat, 2 * end);
+}
+
+int axg_set_moment_sources(axg_solver *h, const axg_moment_sources *s) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!s) throw axg::Error(AXG_E_ARG, "SolidMoment || null description.");
+        sources_from(h->model.ms, s->count, s->element, s->nu, s->pattern_offset, s->pattern, s->stf,
+                     6, "SolidMoment::SolidMoment");
+    });
+}
+
+int axg_set_force_sources(axg_solver *h, const axg_force_sources *s) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!s) throw axg::Error(AXG_E_ARG, "SolidForce || null description.");
+        sources_from(h->model.fs, s->count, s->element, s->nu, s->pattern_offset, s->pattern, s->stf,
+                     3, "SolidForce::SolidForce");
+    });
+}
+
+int axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interval) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!s || s->count < 0 || (s->count && (!s->element || !s->weights || !s->phi)))
+            throw axg::Error(AXG_E_ARG, "StationSolid || missing array.");
+        axg::HostStations &st = h->model.st;
+        st.count = s->count;
+        st.interval = record_interval > 0 ? record_interval : 1;
+        st.elem = copy(s->element, s->count);
+        st.w = copy(s->weights, (size_t)s->count * 25);
+        st.phi = copy(s->phi, s->count);
+    });
+}
+
+int axg_finalize(axg_solver *h) {
+    return guarded(h, [&] {
+        need_open(h);
+        axg::HostModel &m = h->model;
+        for (int e = 0; e < m.se.count; e++)
+            for (int q = 0; q < 25; q++) {
+                int p = m.se.pts[(size_t)e * 25 + q];
+                if (p < 0 || p >= m.sp.count)
+                    throw axg::Error(AXG_E_ARG, "SolidElement::SolidElement || point index out of range.");
+                if (m.sp.nr[p] > m.se.nr[e])
+                    throw axg::Error(AXG_E_ARG, "Element::pointSet || element nr below a point's nr.");
+            }
+        for (int e = 0; e < m.fe.count; e++)
+            for (int q = 0; q < 25; q++) {
+                int p = m.fe.pts[(size_t)e * 25 + q];
+                if (p < 0 || p >= m.fp.count)
+                    throw axg::Error(AXG_E_ARG, "FluidElement::FluidElement || point index out of range.");
+                if (m.fp.nr[p] > m.fe.nr[e])
+                    throw axg::Error(AXG_E_ARG, "Element::pointSet || element nr below a point's nr.");
+            }
+        for (int i = 0; i < m.sf.count; i++)
+            if (m.sf.sp[i] < 0 || m.sf.sp[i] >= m.sp.count || m.sf.fp[i] < 0 || m.sf.fp[i] >= m.fp.count)
+                throw axg::Error(AXG_E_ARG, "SolidFluidCoupling || point index out of range.");
+        for (const axg::HostSources *s : {&m.ms, &m.fs})
+            for (int i = 0; i < s->count; i++)
+                if (s->elem[i] < 0 || s->elem[i] >= m.se.count)
+                    throw axg::Error(AXG_E_ARG, "SolidSource || element index out of range.");
+        for (int i = 0; i < m.st.count; i++)
+            if (m.st.elem[i] < 0 || m.st.elem[i] >= m.se.count)
+                throw axg::Error(AXG_E_ARG, "StationSolid || element index out of range.");
+        h->eng->finalize(m);
+        h->finalized = true;
+    });
+}
+
+int axg_apply_sources(axg_solver *h, int32_t tstep) {
+    return guarded(h, [&] { h->eng->apply_sources(tstep); });
+}
+int axg_compute_stiffness(axg_solver *h) {
+    return guarded(h, [&] { h->eng->compute_stiffness(); });
+}
+int axg_apply_bc_before_assembly(axg_solver *h) {
+    return guarded(h, [&] { h->eng->bc_before(); });
+}
+int axg_apply_bc_after_assembly(axg_solver *h) {
+    return guarded(h, [&] { h->eng->point_stage(1); });
+}
+int axg_stiff_to_accel(axg_solver *h) {
+    return guarded(h, [&] { h->eng->point_stage(2); });
+}
+int axg_newmark_update(axg_solver *h) {
+    return guarded(h, [&] { h->eng->point_stage(4); });
+}
+int axg_record_stations(axg_solver *h, int32_t tstep) {
+    return guarded(h, [&] { h->eng->record(tstep); });
+}
+int axg_run(axg_solver *h, int32_t nsteps, int32_t use_graph) {
+    return guarded(h, [&] {
+        if (nsteps < 0) throw axg::Error(AXG_E_ARG, "NewmarkTimeScheme::solve || nsteps < 0.");
+        h->eng->run(nsteps, use_graph != 0);
+    });
+}
+int axg_current_step(const axg_solver *h, int32_t *tstep) {
+    if (!h || !tstep) return AXG_E_ARG;
+    *tstep = h->eng->step();
+    return AXG_OK;
+}
+
+int axg_get_field(axg_solver *h, int32_t solid, int32_t which, double *host_out) {
+    return guarded(h, [&] {
+        if (!host_out || which < 0 || which > 3) throw axg::Error(AXG_E_ARG, "axg_get_field || bad argument.");
+        h->eng->get_field(solid, which, host_out);
+    });
+}
+int axg_set_field(axg_solver *h, int32_t solid, int32_t which, const double *host_in) {
+    return guarded(h, [&] {
+        if (!host_in || which < 0 || which > 3) throw axg::Error(AXG_E_ARG, "axg_set_field || bad argument.");
+        h->eng->set_field(solid, which, host_in);
+    });
+}
+int axg_field_size(const axg_solver *h, int32_t solid, int64_t *n) {
+    if (!h || !n) return AXG_E_ARG;
+    if (!h->finalized) return AXG_E_STATE;
+    *n = h->eng->field_size(solid);
+    return AXG_OK;
+}
+int axg_field_raw_bytes(const axg_solver *h, int32_t solid, int32_t which, int64_t *bytes) {
+    if (!h || !bytes || which < 0 || which > 3) return AXG_E_ARG;
+    if (!h->finalized) return AXG_E_STATE;
+    *bytes = h->eng->field_raw_bytes(solid, which);
+    return AXG_OK;
+}
+int axg_set_field_raw(axg_solver *h, int32_t solid, int32_t which, const void *host, int64_t bytes) {
+    return guarded(h, [&] {
+        if (!host || which < 0 || which > 3) throw axg::Error(AXG_E_ARG, "axg_set_field_raw || bad argument.");
+        h->eng->set_field_raw(solid, which, host, bytes);
+    });
+}
+int axg_get_field_raw(axg_solver *h, int32_t solid, int32_t which, void *host, int64_t bytes) {
+    return guarded(h, [&] {
+        if (!host || which < 0 || which > 3) throw axg::Error(AXG_E_ARG, "axg_get_field_raw || bad argument.");
+        h->eng->get_field_raw(solid, which, host, bytes);
+    });
+}
+int axg_get_seismograms(axg_solver *h, double *host_out, int32_t *nrecords) {
+    return guarded(h, [&] {
+        int n = h->eng->get_seismograms(host_out);
+        if (nrecords) *nrecords = n;
+    });
+}
+int axg_synchronize(axg_solver *h) {
+    return guarded(h, [&] { h->eng->synchronize(); });
+}
+int axg_launch_count(const axg_solver *h, int64_t *n) {
+    if (!h || !n) return AXG_E_ARG;
+    *n = h->eng->launches();
+    return AXG_OK;
+}
+int axg_set_timing(axg_solver *h, int32_t on) {
+    return guarded(h, [&] { h->eng->set_timing(on != 0); });
+}
+int axg_stiffness_time_ms(axg_solver *h, double *ms, int64_t *launches) {
+    return guarded(h, [&] {
+        double t = 0;
+        int64_t n = 0;
+        h->eng->stiffness_time(&t, &n);
+        if (ms) *ms = t;
+        if (launches) *launches = n;
+    });
+}
+int axg_stiffness_cost(const axg_solver *h, double *bytes, double *flops) {
+    if (!h || !bytes || !flops) return AXG_E_ARG;
+    if (!h->finalized) return AXG_E_STATE;
+    h->eng->stiffness_cost(bytes, flops);
+    return AXG_OK;
+}
+int axg_point_cost(const axg_solver *h, double *bytes) {
+    if (!h || !bytes) return AXG_E_ARG;
+    if (!h->finalized) return AXG_E_STATE;
+    *bytes = h->eng->point_cost();
+    return AXG_OK;
+}
+int axg_set_stream(axg_solver *h, void *stream) {
+    return guarded(h, [&] { h->eng->set_stream(stream); });
+}
+int axg_set_team_size(axg_solver *h, int32_t nr_class, int32_t team) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (team != 32 && team != 64 && team != 128 && team != 256)
+            throw axg::Error(AXG_E_ARG, "axg_set_team_size || team must be 32, 64, 128 or 256.");
+        h->eng->set_team_override(nr_class, team);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+// engine.hpp -- host-side engine interface behind the C ABI (include/axg.h).
+#pragma once
+
+#include "../../include/axg.h"
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace axg {
+
+// error carrying one of the AXG_E_* codes; the message follows the reference's
+// "Class::method || message" convention
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+// ------------------------------------------------------------- host model ---
+struct HostPoints {
+    int count = 0, ndim = 3;
+    std::vector<int> nr, mass_nr;
+    std::vector<int64_t> mass_off;
+    std::vector<double> mass;
+    std::vector<uint8_t> axial, surface;
+};
+
+struct HostSolidElements {
+    int count = 0;
+    std::vector<int> nr, pts, rheo, att;
+    std::vector<uint8_t> axial, rtz, is3d;
+    std::vector<double> geom, theta;
+    std::vector<int64_t> mat_off, att_off;
+    std::vector<double> moduli, att_moduli;
+};
+
+struct HostFluidElements {
+    int count = 0;
+    std::vector<int> nr, pts;
+    std::vector<uint8_t> axial, is3d;
+    std::vector<double> geom;
+    std::vector<int64_t> mat_off;
+    std::vector<double> moduli;
+};
+
+struct HostCoupling {
+    int count = 0;
+    std::vector<int> sp, fp;
+    std::vector<double> nsu, nzu, nsa, nza, mf;
+};
+
+struct HostSources {
+    int count = 0;
+    std::vector<int> elem, nu;
+    std::vector<int64_t> pat_off;
+    std::vector<double> pattern;   // (re, im) pairs
+    std::vector<axg_stf> stf;
+};
+
+struct HostStations {
+    int count = 0, interval = 1;
+    std::vector<int> elem;
+    std::vector<double> w, phi;
+};
+
+struct HostModel {
+    HostPoints sp, fp;
+    HostSolidElements se;
+    HostFluidElements fe;
+    HostCoupling sf;
+    HostSources ms, fs;
+    HostStations st;
+};
+
+// ------------------------------------------------------------ engine API ---
+class EngineBase {
+public:
+    virtual ~EngineBase() = default;
+    virtual void finalize(const HostModel &m) = 0;
+    virtual void apply_sources(int tstep) = 0;
+    virtual void compute_stiffness() = 0;
+    virtual void bc_before() = 0;
+    virtual void point_stage(int mask) = 0;   // 1 = BC after assembly, 2 = 1/M, 4 = Newmark
+    virtual void record(int tstep) = 0;
+    virtual void run(int nsteps, bool graph) = 0;
+    virtual int step() const = 0;
+    virtual int64_t field_size(int solid) const = 0;
+    virtual void get_field(int solid, int which, double *out) = 0;
+    virtual void set_field(int solid, int which, const double *in) = 0;
+    virtual int64_t field_raw_bytes(int solid, int which) const = 0;
+    virtual void set_field_raw(int solid, int which, const void *host, int64_t bytes) = 0;
+    virtual void get_field_raw(int solid, int which, void *host, int64_t bytes) = 0;
+    virtual int get_seismograms(double *out) = 0;
+    virtual void synchronize() = 0;
+    virtual int64_t launches() const = 0;
+    virtual void set_timing(bool on) = 0;
+    virtual void stiffness_time(double *ms, int64_t *n) = 0;
+    virtual void stiffness_cost(double *bytes, double *flops) const = 0;
+    virtual double point_cost() const = 0;
+    virtual void set_stream(void *stream) = 0;
+    virtual void set_team_override(int nr_class, int team) = 0;
+    virtual int bucket_count() const = 0;
+};
+
+std::unique_ptr<EngineBase> make_engine_fp32(const axg_config &cfg);
+std::unique_ptr<EngineBase> make_engine_fp64(const axg_config &cfg);
+std::unique_ptr<EngineBase> make_engine_mixed(const axg_config &cfg);
+
+// spectral tables (nPol = 4), derived from their definitions (spectral.cpp)
+struct SpectralTables {
+    double xGLL[5], xGLJ[5], wGLL[5], wGLJ[5];
+    double G_GLL[25], G_GLJ[25];   // G(j, i) = l_j'(x_i), row-major, rounded to 12 decimals
+};
+const SpectralTables &spectral_tables();
+
+}  // namespace axg

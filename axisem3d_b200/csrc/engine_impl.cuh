@@ -1,0 +1,964 @@
+// engine_impl.cuh -- the templated engine: device layout, buckets, step launch
+// sequence and CUDA-graph capture. Instantiated once per precision in
+// engine_fp32.cu, engine_fp64.cu and engine_mixed.cu.
+//
+// Precision parameters:
+//   T   element stiffness, point stiffness/acceleration
+//   AT  attenuation memory variables (state and recursion)
+//   D   Newmark displacement/velocity storage
+#pragma once
+
+#include "engine.hpp"
+#include "fluid_kernel.cuh"
+#include "point_kernels.cuh"
+#include "solid_kernel.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <tuple>
+
+namespace axg {
+
+#define AXG_CUDA(call)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            throw Error(e_ == cudaErrorMemoryAllocation ? AXG_E_NOMEM : AXG_E_CUDA,          \
+                        std::string("Engine::" ) + __func__ + " || " + #call + " || " +      \
+                            cudaGetErrorString(e_));                                         \
+    } while (0)
+
+// owning device buffer
+template <class X>
+struct DBuf {
+    X *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { if (p) cudaFree(p); }
+    void alloc(size_t count) {
+        if (p) { cudaFree(p); p = nullptr; }
+        n = count;
+        if (count) AXG_CUDA(cudaMalloc(&p, count * sizeof(X)));
+    }
+    void zero(cudaStream_t s) { if (n) AXG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(X), s)); }
+    void upload(const std::vector<X> &h) {
+        alloc(h.size());
+        if (n) AXG_CUDA(cudaMemcpy(p, h.data(), n * sizeof(X), cudaMemcpyHostToDevice));
+    }
+};
+
+// team size per nr class and the nr class boundaries
+inline int nr_class(int nr) { return nr <= 3 ? 0 : nr <= 9 ? 1 : nr <= 25 ? 2 : nr <= 64 ? 3 : 4; }
+inline int default_team(int cls) { static const int t[5] = {32, 64, 128, 256, 256}; return t[cls]; }
+
+template <class T>
+std::vector<T> twiddle_pool(const std::vector<int> &nrs, int nr_max, std::vector<int> &off) {
+    // for each nr: cos(2 pi j / nr), j < nr, then sin; exact on the quarter points
+    std::vector<T> pool;
+    off.assign(nr_max + 2, 0);
+    std::vector<char> need(nr_max + 1, 0);
+    for (int n : nrs) need[n] = 1;
+    for (int n = 1; n <= nr_max; n++) {
+        off[n] = (int)pool.size();
+        if (!need[n]) continue;
+        for (int j = 0; j < n; j++) {
+            double a = 2.0 * M_PI * j / n, c = std::cos(a);
+            if (4 * j == n || 4 * j == 3 * n) c = 0; else if (2 * j == n) c = -1;
+            pool.push_back((T)c);
+        }
+        for (int j = 0; j < n; j++) {
+            double a = 2.0 * M_PI * j / n, s = std::sin(a);
+            if (4 * j == n) s = 1; else if (2 * j == n) s = 0; else if (4 * j == 3 * n) s = -1;
+            pool.push_back((T)s);
+        }
+    }
+    off[nr_max + 1] = (int)pool.size();
+    if (pool.empty()) pool.push_back((T)0);
+    return pool;
+}
+
+template <class T, class AT, class D, bool COMP>
+class Engine final : public EngineBase {
+    using C = cx_t<T>;
+    using CD = cx_t<D>;
+
+    struct PointDev {
+        int n = 0, ndim = 3, total = 0, n3d = 0, nr_max = 1;
+        std::vector<int> h_off, h_nu, h_nr;
+        DBuf<int> off, nu, nr, mode_pt, pt3d;
+        DBuf<uint8_t> flags;
+        DBuf<T> inv1, inv3;
+        DBuf<int64_t> im_off;
+        DBuf<C> stiff, accel, displ_elem;
+        DBuf<CD> displ, veloc;
+        DBuf<cx_t<float>> cd, cv;
+    };
+
+    struct SolidBucket {
+        int rheo, att, is3d, rtz, cls, team, tpc, qc, nr_max, n;
+        size_t team_bytes;
+        DBuf<int> nr, pts;
+        DBuf<uint8_t> axial;
+        DBuf<T> geom, trig, mod, attmod;
+        DBuf<int64_t> mod_off, att_off, state_off;
+        double bytes = 0, flops = 0;
+        void (*kernel)(const SolidArgs<T, AT>, int, int, int, size_t) = nullptr;
+    };
+    struct FluidBucket {
+        int is3d, cls, team, tpc, nr_max, n;
+        size_t team_bytes;
+        DBuf<int> nr, pts;
+        DBuf<uint8_t> axial;
+        DBuf<T> geom, K;
+        DBuf<int64_t> K_off;
+        double bytes = 0, flops = 0;
+        void (*kernel)(const FluidArgs<T>, int, int, size_t) = nullptr;
+    };
+
+public:
+    explicit Engine(const axg_config &c) : cfg_(c) {
+        AXG_CUDA(cudaSetDevice(cfg_.device));
+        AXG_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+        stream_ = own_stream_;
+        AXG_CUDA(cudaGetDeviceProperties(&prop_, cfg_.device));
+        for (int i = 0; i < 5; i++) team_override_[i] = 0;
+    }
+    ~Engine() override {
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+        if (own_stream_) cudaStreamDestroy(own_stream_);
+    }
+
+    // ------------------------------------------------------------ finalize ---
+    void finalize(const HostModel &m) override {
+        model_ = m;
+        const SpectralTables &st = spectral_tables();
+        std::vector<T> g(50);
+        for (int i = 0; i < 25; i++) { g[i] = (T)st.G_GLL[i]; g[25 + i] = (T)st.G_GLJ[i]; }
+        gmat_.upload(g);
+        build_points(m.sp, sp_, true);
+        build_points(m.fp, fp_, false);
+        // twiddles for every nr in use (3-D elements and Mass3D points)
+        std::vector<int> nrs;
+        int nrmax = 1;
+        for (int i = 0; i < m.se.count; i++) {
+            nrmax = std::max(nrmax, m.se.nr[i]);
+            if (m.se.is3d.size() && m.se.is3d[i]) nrs.push_back(m.se.nr[i]);
+        }
+        for (int i = 0; i < m.fe.count; i++) {
+            nrmax = std::max(nrmax, m.fe.nr[i]);
+            if (m.fe.is3d.size() && m.fe.is3d[i]) nrs.push_back(m.fe.nr[i]);
+        }
+        for (const HostPoints *hp : {&m.sp, &m.fp})
+            for (int p = 0; p < hp->count; p++) {
+                nrmax = std::max(nrmax, hp->nr[p]);
+                if (hp->mass_nr.size() && hp->mass_nr[p] > 1) nrs.push_back(hp->nr[p]);
+            }
+        std::vector<int> twoff;
+        tw_.upload(twiddle_pool<T>(nrs, nrmax, twoff));
+        tw_off_.upload(twoff);
+        build_solid_buckets(m.se);
+        build_fluid_buckets(m.fe);
+        build_coupling(m.sf);
+        build_sources(m.ms, m.fs);
+        build_stations(m.st);
+        step_dev_.alloc(1);
+        step_dev_.zero(stream_);
+        nonfinite_.alloc(1);
+        nonfinite_.zero(stream_);
+        AXG_CUDA(cudaEventCreate(&ev0_));
+        AXG_CUDA(cudaEventCreate(&ev1_));
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        finalized_ = true;
+    }
+
+    // ------------------------------------------------------------ hooks ---
+    void apply_sources(int tstep) override {
+        need();
+        set_step(tstep);
+        launch_sources();
+    }
+    void compute_stiffness() override { need(); launch_stiffness(); }
+    void bc_before() override { need(); launch_coupling(); }
+    void point_stage(int mask) override { need(); launch_points(mask); }
+    void record(int tstep) override {
+        need();
+        set_step(tstep);
+        ensure_capacity(tstep + 1);
+        launch_stations();
+    }
+
+    void run(int nsteps, bool graph) override {
+        need();
+        if (nsteps <= 0) return;
+        ensure_capacity(step_ + nsteps);
+        set_step(step_);
+        if (timing_) {
+            for (int i = 0; i < nsteps; i++) {
+                launch_step();
+                AXG_CUDA(cudaEventSynchronize(ev1_));
+                float ms = 0;
+                AXG_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+                time_ms_ += ms;
+                time_n_ += 1;
+            }
+        } else if (graph) {
+            if (!graph_exec_) capture();
+            for (int i = 0; i < nsteps; i++) {
+                AXG_CUDA(cudaGraphLaunch(graph_exec_, stream_));
+                launches_ += kernels_per_step_;
+            }
+        } else {
+            for (int i = 0; i < nsteps; i++) launch_step();
+        }
+        step_ += nsteps;
+        if (cfg_.stability_interval > 0) check_finite();
+    }
+    int step() const override { return step_; }
+
+    // ------------------------------------------------------------- fields ---
+    int64_t field_size(int solid) const override {
+        const PointDev &P = solid ? sp_ : fp_;
+        return (int64_t)P.total * P.ndim;
+    }
+    void get_field(int solid, int which, double *out) override {
+        need();
+        PointDev &P = solid ? sp_ : fp_;
+        size_t n = (size_t)P.total * P.ndim;
+        if (!n) return;
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        if (which == AXG_FIELD_DISPL || which == AXG_FIELD_VELOC) {
+            std::vector<CD> h(n);
+            AXG_CUDA(cudaMemcpy(h.data(), which == AXG_FIELD_DISPL ? P.displ.p : P.veloc.p,
+                                n * sizeof(CD), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; i++) { out[2 * i] = (double)h[i].x; out[2 * i + 1] = (double)h[i].y; }
+        } else {
+            std::vector<C> h(n);
+            AXG_CUDA(cudaMemcpy(h.data(), which == AXG_FIELD_STIFF ? P.stiff.p : P.accel.p,
+                                n * sizeof(C), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; i++) { out[2 * i] = (double)h[i].x; out[2 * i + 1] = (double)h[i].y; }
+        }
+    }
+    void set_field(int solid, int which, const double *in) override {
+        need();
+        PointDev &P = solid ? sp_ : fp_;
+        size_t n = (size_t)P.total * P.ndim;
+        if (!n) return;
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        if (which == AXG_FIELD_DISPL || which == AXG_FIELD_VELOC) {
+            std::vector<CD> h(n);
+            for (size_t i = 0; i < n; i++) h[i] = mk<D>((D)in[2 * i], (D)in[2 * i + 1]);
+            AXG_CUDA(cudaMemcpy(which == AXG_FIELD_DISPL ? P.displ.p : P.veloc.p, h.data(),
+                                n * sizeof(CD), cudaMemcpyHostToDevice));
+            if (which == AXG_FIELD_DISPL && P.displ_elem.p) {
+                std::vector<C> hf(n);
+                for (size_t i = 0; i < n; i++) hf[i] = mk<T>((T)h[i].x, (T)h[i].y);
+                AXG_CUDA(cudaMemcpy(P.displ_elem.p, hf.data(), n * sizeof(C), cudaMemcpyHostToDevice));
+            }
+            if (COMP) {
+                if (which == AXG_FIELD_DISPL) P.cd.zero(stream_); else P.cv.zero(stream_);
+            }
+        } else {
+            std::vector<C> h(n);
+            for (size_t i = 0; i < n; i++) h[i] = mk<T>((T)in[2 * i], (T)in[2 * i + 1]);
+            AXG_CUDA(cudaMemcpy(which == AXG_FIELD_STIFF ? P.stiff.p : P.accel.p, h.data(),
+                                n * sizeof(C), cudaMemcpyHostToDevice));
+        }
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+    }
+    int64_t field_raw_bytes(int solid, int which) const override {
+        const PointDev &P = solid ? sp_ : fp_;
+        size_t n = (size_t)P.total * P.ndim;
+        bool dv = which == AXG_FIELD_DISPL || which == AXG_FIELD_VELOC;
+        return (int64_t)(n * (dv ? sizeof(CD) : sizeof(C)));
+    }
+    void *field_ptr(PointDev &P, int which) {
+        switch (which) {
+            case AXG_FIELD_DISPL: return P.displ.p;
+            case AXG_FIELD_VELOC: return P.veloc.p;
+            case AXG_FIELD_STIFF: return P.stiff.p;
+            default: return P.accel.p;
+        }
+    }
+    void set_field_raw(int solid, int which, const void *host, int64_t bytes) override {
+        need();
+        if (bytes != field_raw_bytes(solid, which))
+            throw Error(AXG_E_ARG, "axg_set_field_raw || byte count mismatch.");
+        PointDev &P = solid ? sp_ : fp_;
+        if (!bytes) return;
+        AXG_CUDA(cudaMemcpyAsync(field_ptr(P, which), host, bytes, cudaMemcpyHostToDevice, stream_));
+        if (which == AXG_FIELD_DISPL && P.displ_elem.p) {
+            size_t n = (size_t)P.total * P.ndim;
+            narrow_kernel<T, D><<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(P.displ.p, P.displ_elem.p, n);
+            post_launch();
+        }
+        if (COMP) {
+            if (which == AXG_FIELD_DISPL) P.cd.zero(stream_);
+            if (which == AXG_FIELD_VELOC) P.cv.zero(stream_);
+        }
+    }
+    void get_field_raw(int solid, int which, void *host, int64_t bytes) override {
+        need();
+        if (bytes != field_raw_bytes(solid, which))
+            throw Error(AXG_E_ARG, "axg_get_field_raw || byte count mismatch.");
+        PointDev &P = solid ? sp_ : fp_;
+        if (!bytes) return;
+        AXG_CUDA(cudaMemcpyAsync(host, field_ptr(P, which), bytes, cudaMemcpyDeviceToHost, stream_));
+    }
+    int get_seismograms(double *out) override {
+        need();
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        int nrec = 0;
+        if (st_n_ > 0) nrec = std::min(seis_cap_, (step_ + st_interval_ - 1) / st_interval_);
+        if (out && nrec > 0)
+            AXG_CUDA(cudaMemcpy(out, seis_.p, (size_t)nrec * st_n_ * 3 * sizeof(double),
+                                cudaMemcpyDeviceToHost));
+        return nrec;
+    }
+    void synchronize() override { AXG_CUDA(cudaStreamSynchronize(stream_)); }
+    int64_t launches() const override { return launches_; }
+    void set_timing(bool on) override {
+        timing_ = on;
+        if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+        time_ms_ = 0; time_n_ = 0;
+    }
+    void stiffness_time(double *ms, int64_t *n) override {
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        *ms = time_ms_;
+        *n = time_n_;
+    }
+    void stiffness_cost(double *bytes, double *flops) const override {
+        double b = 0, f = 0;
+        for (auto &bk : sb_) { b += bk->bytes; f += bk->flops; }
+        for (auto &bk : fb_) { b += bk->bytes; f += bk->flops; }
+        // points: read u once, write f once
+        b += (double)sp_.total * 3 * 2 * sizeof(C) + (double)fp_.total * 2 * sizeof(C);
+        *bytes = b;
+        *flops = f;
+    }
+    double point_cost() const override {
+        double b = 0;
+        for (const PointDev *P : {&sp_, &fp_}) {
+            double per = 0;
+            per += 2 * sizeof(C);                          // stiff read + zero write
+            per += 2 * sizeof(C);                          // accel read + write
+            per += 4 * sizeof(CD);                         // d, v read + write
+            if (COMP) per += 4 * sizeof(cx_t<float>);      // compensation terms
+            if (P->displ_elem.p) per += sizeof(C);         // element copy of d
+            b += per * (double)P->total * P->ndim;
+        }
+        return b;
+    }
+    void set_stream(void *s) override {
+        stream_ = s ? (cudaStream_t)s : own_stream_;
+        if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+    }
+    void set_team_override(int cls, int team) override {
+        if (cls < 0 || cls > 4) throw Error(AXG_E_ARG, "Engine::set_team_override || bad class");
+        team_override_[cls] = team;
+    }
+    int bucket_count() const override { return (int)(sb_.size() + fb_.size()); }
+
+private:
+    void need() const {
+        if (!finalized_) throw Error(AXG_E_STATE, "Engine::step || axg_finalize not called.");
+    }
+    void set_step(int tstep) {
+        tstep_host_ = tstep;
+        AXG_CUDA(cudaMemcpyAsync(step_dev_.p, &tstep_host_, sizeof(int), cudaMemcpyHostToDevice, stream_));
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+    }
+    void check_finite() {
+        int flag = 0;
+        AXG_CUDA(cudaMemcpyAsync(&flag, nonfinite_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        if (flag) throw Error(AXG_E_UNSTABLE, "Domain::checkStability || Non-finite displacement.");
+    }
+
+    // -------------------------------------------------------- points ---
+    void build_points(const HostPoints &h, PointDev &P, bool solid) {
+        P.n = h.count;
+        P.ndim = solid ? 3 : 1;
+        P.h_off.resize(P.n); P.h_nu.resize(P.n); P.h_nr.resize(P.n);
+        std::vector<int> mode_pt, pt3d;
+        std::vector<uint8_t> flags(P.n, 0);
+        std::vector<T> inv1(P.n, (T)0), inv3;
+        std::vector<int64_t> im_off(P.n, 0);
+        int o = 0;
+        for (int p = 0; p < P.n; p++) {
+            int nr = h.nr[p];
+            if (nr < 1) throw Error(AXG_E_ARG, "Point::Point || nr must be >= 1.");
+            P.h_nr[p] = nr; P.h_nu[p] = nr / 2 + 1; P.h_off[p] = o;
+            for (int a = 0; a < P.h_nu[p]; a++) mode_pt.push_back(p);
+            o += P.h_nu[p];
+            P.nr_max = std::max(P.nr_max, nr);
+            int mnr = h.mass_nr.size() ? h.mass_nr[p] : 1;
+            int64_t mo = h.mass_off.size() ? h.mass_off[p] : p;
+            if (mnr == 1) {
+                inv1[p] = (T)(1.0 / h.mass[mo]);        // Mass1D: (Real)(1 / mass)
+            } else {
+                if (mnr != nr) throw Error(AXG_E_ARG, "Mass3D::checkCompatibility || Incompatible sizes.");
+                flags[p] |= PT_MASS3D;
+                pt3d.push_back(p);
+                im_off[p] = (int64_t)inv3.size();
+                for (int k = 0; k < mnr; k++) inv3.push_back((T)(1.0 / h.mass[mo + k]));
+            }
+            if (h.axial.size() && h.axial[p]) flags[p] |= PT_AXIAL;
+            if (h.surface.size() && h.surface[p]) flags[p] |= PT_SURFACE;
+        }
+        P.total = o;
+        P.n3d = (int)pt3d.size();
+        P.off.upload(P.h_off); P.nu.upload(P.h_nu); P.nr.upload(P.h_nr);
+        P.mode_pt.upload(mode_pt); P.pt3d.upload(pt3d);
+        P.flags.upload(flags); P.inv1.upload(inv1);
+        if (inv3.empty()) inv3.push_back((T)0);
+        P.inv3.upload(inv3); P.im_off.upload(im_off);
+        size_t nf = (size_t)P.total * P.ndim;
+        P.stiff.alloc(nf); P.stiff.zero(stream_);
+        P.accel.alloc(nf); P.accel.zero(stream_);
+        P.displ.alloc(nf); P.displ.zero(stream_);
+        P.veloc.alloc(nf); P.veloc.zero(stream_);
+        if (sizeof(D) != sizeof(T)) { P.displ_elem.alloc(nf); P.displ_elem.zero(stream_); }
+        if (COMP) { P.cd.alloc(nf); P.cd.zero(stream_); P.cv.alloc(nf); P.cv.zero(stream_); }
+    }
+    // displacement as seen by the elements
+    const C *elem_displ(const PointDev &P) const {
+        if constexpr (sizeof(D) != sizeof(T)) return P.displ_elem.p;
+        else return reinterpret_cast<const C *>(P.displ.p);
+    }
+
+    // ------------------------------------------------------- solid buckets ---
+    using SolidKernel = void (*)(const SolidArgs<T, AT>, int, int, int, size_t);
+    template <int RHEO, int ATT, bool IS3D, bool RTZ>
+    static SolidKernel pick4() { return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ>; }
+    template <int RHEO, int ATT, bool IS3D>
+    static SolidKernel pick3(bool rtz) {
+        if constexpr (RHEO == RHEO_ISO) return pick4<RHEO, ATT, IS3D, false>();
+        else return rtz ? pick4<RHEO, ATT, IS3D, true>() : pick4<RHEO, ATT, IS3D, false>();
+    }
+    template <int RHEO, int ATT>
+    static SolidKernel pick2(bool is3d, bool rtz) {
+        return is3d ? pick3<RHEO, ATT, true>(rtz) : pick3<RHEO, ATT, false>(rtz);
+    }
+    template <int RHEO>
+    static SolidKernel pick1(int att, bool is3d, bool rtz) {
+        switch (att) {
+            case ATT_NONE: return pick2<RHEO, ATT_NONE>(is3d, rtz);
+            case ATT_FULL: return pick2<RHEO, ATT_FULL>(is3d, rtz);
+            default: return pick2<RHEO, ATT_CG4>(is3d, rtz);
+        }
+    }
+    static SolidKernel pick_solid(int rheo, int att, bool is3d, bool rtz) {
+        switch (rheo) {
+            case RHEO_ISO: return pick1<RHEO_ISO>(att, is3d, rtz);
+            case RHEO_TISO: return pick1<RHEO_TISO>(att, is3d, rtz);
+            default: return pick1<RHEO_ANISO>(att, is3d, rtz);
+        }
+    }
+
+    int nmod_of(int rheo) const { return rheo == RHEO_ISO ? 2 : rheo == RHEO_TISO ? 5 : 21; }
+
+    void build_solid_buckets(const HostSolidElements &h) {
+        // group elements by (rheology, attenuation, 1-D/3-D, RTZ, nr class)
+        std::map<std::tuple<int, int, int, int, int>, std::vector<int>> groups;
+        for (int e = 0; e < h.count; e++) {
+            int att = h.att.size() ? h.att[e] : ATT_NONE;
+            int is3d = h.is3d.size() ? h.is3d[e] : 0;
+            int rtz = h.rtz.size() ? h.rtz[e] : 0;
+            if (h.rheo[e] == RHEO_ISO) rtz = 0;   // isotropic rheology is frame invariant
+            if (att != ATT_NONE && cfg_.nsls <= 0)
+                throw Error(AXG_E_ARG, "Attenuation::checkCompatibility || nsls must be > 0.");
+            groups[{h.rheo[e], att, is3d, rtz, nr_class(h.nr[e])}].push_back(e);
+        }
+        int64_t state_total = 0;
+        std::vector<std::vector<int64_t>> state_offs;
+        for (auto &kv : groups) {
+            auto b = std::make_unique<SolidBucket>();
+            std::tie(b->rheo, b->att, b->is3d, b->rtz, b->cls) = kv.first;
+            const std::vector<int> &ids = kv.second;
+            b->n = (int)ids.size();
+            b->nr_max = 1;
+            std::vector<int> nr(b->n), pts((size_t)b->n * 25);
+            std::vector<uint8_t> ax(b->n);
+            std::vector<T> geom((size_t)b->n * 250), trig, mod, attm;
+            std::vector<int64_t> moff(b->n), aoff(b->n, 0), soff(b->n, 0);
+            if (b->rtz) trig.resize((size_t)b->n * 100);
+            int nm = nmod_of(b->rheo);
+            int npa = b->att == ATT_CG4 ? 4 : 25;
+            double bytes = 0, flops = 0;
+            for (int k = 0; k < b->n; k++) {
+                int e = ids[k];
+                int enr = h.nr[e], enu = enr / 2 + 1, ns = b->is3d ? enr : 1;
+                nr[k] = enr;
+                b->nr_max = std::max(b->nr_max, enr);
+                ax[k] = h.axial[e];
+                for (int q = 0; q < 25; q++) {
+                    int p = h.pts[(size_t)e * 25 + q];
+                    if (p < 0 || p >= sp_.n) throw Error(AXG_E_ARG, "SolidElement::SolidElement || point index out of range.");
+                    pts[(size_t)k * 25 + q] = p;
+                }
+                const double *g = &h.geom[(size_t)e * 150];
+                for (int c = 0; c < 5; c++)
+                    for (int q = 0; q < 25; q++) {
+                        // plain operators cast to Real; _IF products formed in double
+                        // (GradientQuadrature.hpp:122-137)
+                        geom[(size_t)k * 250 + c * 25 + q] = (T)g[c * 25 + q];
+                        geom[(size_t)k * 250 + 125 + c * 25 + q] = (T)(g[c * 25 + q] * g[125 + q]);
+                    }
+                if (b->rtz)
+                    for (int q = 0; q < 25; q++) {
+                        double t = h.theta[(size_t)e * 25 + q];
+                        trig[(size_t)k * 100 + q] = (T)std::sin(t);
+                        trig[(size_t)k * 100 + 25 + q] = (T)std::cos(t);
+                        trig[(size_t)k * 100 + 50 + q] = (T)std::sin(2. * t);
+                        trig[(size_t)k * 100 + 75 + q] = (T)std::cos(2. * t);
+                    }
+                moff[k] = (int64_t)mod.size();
+                const double *mm = &h.moduli[h.mat_off[e]];
+                for (size_t i = 0; i < (size_t)nm * ns * 25; i++) mod.push_back((T)mm[i]);
+                if (b->att != ATT_NONE) {
+                    aoff[k] = (int64_t)attm.size();
+                    const double *am = &h.att_moduli[h.att_off[e]];
+                    for (size_t i = 0; i < (size_t)2 * ns * npa; i++) attm.push_back((T)am[i]);
+                    int64_t slots = b->is3d ? (int64_t)enr * npa : (int64_t)enu * npa * 2;
+                    soff[k] = state_total;
+                    state_total += (int64_t)(cfg_.nsls + 1) * 6 * slots;
+                }
+                // algorithmic bytes and flops of this element (stiffness roofline)
+                double s = sizeof(T), sa = sizeof(AT);
+                bytes += 6 * 25 * s + 25 * 4 + 8;                        // geometry, point ids, nr
+                bytes += (double)nm * ns * 25 * s;                        // moduli
+                if (b->att != ATT_NONE) {
+                    bytes += 2.0 * ns * npa * s;                          // dlambda, dmu
+                    double slots = b->is3d ? (double)enr * npa : (double)enu * npa * 2;
+                    bytes += 2.0 * (cfg_.nsls + 1) * 6 * slots * sa;      // state read + write
+                }
+                if (b->rtz) bytes += 25 * s;                              // theta
+                flops += (double)enu * 25 * (2 * 3 * 10 * 4 + 60);        // gradient
+                flops += (double)enu * 25 * (2 * 3 * 10 * 4 + 60);        // quadrature
+                double pw = nm == 2 ? 16 : nm == 5 ? 22 : 72;             // stress per point
+                if (b->is3d) {
+                    flops += 2.0 * 150 * enr * enu * 4;                   // two direct DFTs
+                    flops += (double)enr * 25 * pw;
+                    if (b->att != ATT_NONE) flops += (double)enr * npa * (cfg_.nsls * 6 * 4 + 14);
+                } else {
+                    flops += (double)enu * 25 * pw * 2;
+                    if (b->att != ATT_NONE) flops += (double)enu * npa * 2 * (cfg_.nsls * 6 * 4 + 14);
+                }
+            }
+            b->bytes = bytes;
+            b->flops = flops;
+            b->nr.upload(nr); b->pts.upload(pts); b->axial.upload(ax);
+            b->geom.upload(geom);
+            if (trig.empty()) trig.push_back((T)0);
+            b->trig.upload(trig);
+            if (mod.empty()) mod.push_back((T)0);
+            if (attm.empty()) attm.push_back((T)0);
+            b->mod.upload(mod); b->attmod.upload(attm);
+            b->mod_off.upload(moff); b->att_off.upload(aoff);
+            state_offs.push_back(soff);
+            b->kernel = pick_solid(b->rheo, b->att, b->is3d, b->rtz);
+            configure_bucket(*b);
+            sb_.push_back(std::move(b));
+        }
+        state_.alloc(std::max<int64_t>(state_total, 1));
+        state_.zero(stream_);
+        for (size_t i = 0; i < sb_.size(); i++) sb_[i]->state_off.upload(state_offs[i]);
+    }
+
+    void configure_bucket(SolidBucket &b) {
+        int team = team_override_[b.cls] ? team_override_[b.cls] : default_team(b.cls);
+        // shared memory per team; split the 25 points of the slice phase if needed
+        const size_t budget = 200 * 1024;
+        int qc = 25;
+        TeamLayout L = team_layout<T>(b.nr_max, qc);
+        while (L.total > budget / 1 && qc > 1) { qc = (qc + 1) / 2; L = team_layout<T>(b.nr_max, qc); }
+        if (L.total > budget)
+            throw Error(AXG_E_UNSUPPORTED, "SolidElement::expandWorkspace || nr too large for shared memory.");
+        b.qc = qc;
+        b.team_bytes = L.total;
+        b.team = team;
+        int tpc = std::max(1, 256 / team);
+        while (tpc > 1 && (size_t)tpc * L.total > budget) tpc--;
+        if (team > 32) tpc = std::min(tpc, 15);
+        b.tpc = tpc;
+        AXG_CUDA(cudaFuncSetAttribute(b.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(tpc * L.total)));
+    }
+
+    // ------------------------------------------------------- fluid buckets ---
+    using FluidKernel = void (*)(const FluidArgs<T>, int, int, size_t);
+    void build_fluid_buckets(const HostFluidElements &h) {
+        std::map<std::tuple<int, int>, std::vector<int>> groups;
+        for (int e = 0; e < h.count; e++)
+            groups[{h.is3d.size() ? h.is3d[e] : 0, nr_class(h.nr[e])}].push_back(e);
+        for (auto &kv : groups) {
+            auto b = std::make_unique<FluidBucket>();
+            std::tie(b->is3d, b->cls) = kv.first;
+            const std::vector<int> &ids = kv.second;
+            b->n = (int)ids.size();
+            b->nr_max = 1;
+            std::vector<int> nr(b->n), pts((size_t)b->n * 25);
+            std::vector<uint8_t> ax(b->n);
+            std::vector<T> geom((size_t)b->n * 250), K;
+            std::vector<int64_t> koff(b->n);
+            double bytes = 0, flops = 0;
+            for (int k = 0; k < b->n; k++) {
+                int e = ids[k];
+                int enr = h.nr[e], enu = enr / 2 + 1, ns = b->is3d ? enr : 1;
+                nr[k] = enr;
+                b->nr_max = std::max(b->nr_max, enr);
+                ax[k] = h.axial[e];
+                for (int q = 0; q < 25; q++) {
+                    int p = h.pts[(size_t)e * 25 + q];
+                    if (p < 0 || p >= fp_.n) throw Error(AXG_E_ARG, "FluidElement::FluidElement || point index out of range.");
+                    pts[(size_t)k * 25 + q] = p;
+                }
+                const double *g = &h.geom[(size_t)e * 150];
+                for (int c = 0; c < 5; c++)
+                    for (int q = 0; q < 25; q++) {
+                        geom[(size_t)k * 250 + c * 25 + q] = (T)g[c * 25 + q];
+                        geom[(size_t)k * 250 + 125 + c * 25 + q] = (T)(g[c * 25 + q] * g[125 + q]);
+                    }
+                koff[k] = (int64_t)K.size();
+                const double *mm = &h.moduli[h.mat_off[e]];
+                for (int i = 0; i < ns * 25; i++) K.push_back((T)mm[i]);
+                double s = sizeof(T);
+                bytes += 6 * 25 * s + 25 * 4 + 8 + (double)ns * 25 * s;
+                flops += (double)enu * 25 * 2 * (10 * 4 + 20);
+                if (b->is3d) flops += 2.0 * 75 * enr * enu * 4;
+            }
+            b->bytes = bytes;
+            b->flops = flops;
+            b->nr.upload(nr); b->pts.upload(pts); b->axial.upload(ax);
+            b->geom.upload(geom);
+            if (K.empty()) K.push_back((T)0);
+            b->K.upload(K); b->K_off.upload(koff);
+            b->kernel = b->is3d ? (FluidKernel)fluid_stiffness_kernel<T, true>
+                                : (FluidKernel)fluid_stiffness_kernel<T, false>;
+            int team = team_override_[b->cls] ? team_override_[b->cls] : default_team(b->cls);
+            TeamLayout L = fluid_layout<T>(b->nr_max);
+            if (L.total > 200 * 1024)
+                throw Error(AXG_E_UNSUPPORTED, "FluidElement || nr too large for shared memory.");
+            b->team = team;
+            b->team_bytes = L.total;
+            int tpc = std::max(1, 256 / team);
+            while (tpc > 1 && (size_t)tpc * L.total > 200 * 1024) tpc--;
+            if (team > 32) tpc = std::min(tpc, 15);
+            b->tpc = tpc;
+            AXG_CUDA(cudaFuncSetAttribute(b->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)(tpc * L.total)));
+            fb_.push_back(std::move(b));
+        }
+    }
+
+    // ------------------------------------------------- coupling / sources ---
+    void build_coupling(const HostCoupling &h) {
+        cp_n_ = h.count;
+        if (!cp_n_) return;
+        std::vector<T> nsu(cp_n_), nzu(cp_n_), nsa(cp_n_), nza(cp_n_);
+        for (int i = 0; i < cp_n_; i++) {
+            // SolidFluidCoupling1D: normals cast to Real, assembled normals / fluid mass
+            nsu[i] = (T)h.nsu[i]; nzu[i] = (T)h.nzu[i];
+            nsa[i] = (T)(h.nsa[i] / h.mf[i]); nza[i] = (T)(h.nza[i] / h.mf[i]);
+            if (sp_.h_nu[h.sp[i]] != fp_.h_nu[h.fp[i]])
+                throw Error(AXG_E_ARG, "SolidFluidCoupling::SolidFluidCoupling || coupled points differ in nr.");
+        }
+        cp_sp_.upload(h.sp); cp_fp_.upload(h.fp);
+        cp_nsu_.upload(nsu); cp_nzu_.upload(nzu); cp_nsa_.upload(nsa); cp_nza_.upload(nza);
+    }
+
+    void build_sources(const HostSources &ms, const HostSources &fs) {
+        auto conv = [](const HostSources &h, DBuf<int> &el, DBuf<int> &nu, DBuf<int64_t> &po,
+                       DBuf<C> &pat) {
+            el.upload(h.elem); nu.upload(h.nu);
+            std::vector<int64_t> off(h.count);
+            for (int i = 0; i < h.count; i++) off[i] = h.pat_off[i];
+            po.upload(off);
+            std::vector<C> p(h.pattern.size() / 2);
+            for (size_t i = 0; i < p.size(); i++) p[i] = mk<T>((T)h.pattern[2 * i], (T)h.pattern[2 * i + 1]);
+            if (p.empty()) p.push_back(mk<T>(0, 0));
+            pat.upload(p);
+        };
+        ms_n_ = ms.count;
+        fs_n_ = fs.count;
+        if (ms_n_) conv(ms, ms_el_, ms_nu_, ms_po_, ms_pat_);
+        if (fs_n_) conv(fs, fs_el_, fs_nu_, fs_po_, fs_pat_);
+        for (int i = 0; i < ms.count; i++)
+            if (ms.elem[i] < 0 || ms.elem[i] >= model_.se.count)
+                throw Error(AXG_E_ARG, "SolidMoment::SolidMoment || element index out of range.");
+        // element lookup tables in original order for the source kernels
+        const HostSolidElements &h = model_.se;
+        std::vector<T> g((size_t)h.count * 250);
+        for (int e = 0; e < h.count; e++)
+            for (int c = 0; c < 5; c++)
+                for (int q = 0; q < 25; q++) {
+                    g[(size_t)e * 250 + c * 25 + q] = (T)h.geom[(size_t)e * 150 + c * 25 + q];
+                    g[(size_t)e * 250 + 125 + c * 25 + q] =
+                        (T)(h.geom[(size_t)e * 150 + c * 25 + q] * h.geom[(size_t)e * 150 + 125 + q]);
+                }
+        if (ms_n_ || fs_n_ || model_.st.count) {
+            e_nr_.upload(h.nr); e_pts_.upload(h.pts);
+            std::vector<uint8_t> ax(h.axial.begin(), h.axial.end());
+            e_axial_.upload(ax);
+            if (ms_n_) e_geom_.upload(g);
+        }
+    }
+
+    void build_stations(const HostStations &h) {
+        st_n_ = h.count;
+        st_interval_ = std::max(1, h.interval);
+        if (!st_n_) return;
+        st_el_.upload(h.elem);
+        std::vector<T> w(h.w.size()), phi(h.phi.size());
+        for (size_t i = 0; i < w.size(); i++) w[i] = (T)h.w[i];
+        for (size_t i = 0; i < phi.size(); i++) phi[i] = (T)h.phi[i];
+        st_w_.upload(w); st_phi_.upload(phi);
+    }
+
+    // STF table and seismogram buffer large enough for steps [0, nsteps)
+    void ensure_capacity(int nsteps) {
+        bool changed = false;
+        if ((ms_n_ || fs_n_) && nsteps > stf_cap_) {
+            int cap = std::max(nsteps, 2 * stf_cap_);
+            fill_stf(cap);
+            changed = true;
+        }
+        if (st_n_) {
+            int need_rec = (nsteps + st_interval_ - 1) / st_interval_;
+            if (need_rec > seis_cap_) {
+                int cap = std::max(need_rec, 2 * seis_cap_);
+                DBuf<double> nb;
+                nb.alloc((size_t)cap * st_n_ * 3);
+                nb.zero(stream_);
+                if (seis_cap_)
+                    AXG_CUDA(cudaMemcpyAsync(nb.p, seis_.p, (size_t)seis_cap_ * st_n_ * 3 * sizeof(double),
+                                             cudaMemcpyDeviceToDevice, stream_));
+                AXG_CUDA(cudaStreamSynchronize(stream_));
+                std::swap(seis_.p, nb.p); std::swap(seis_.n, nb.n);
+                seis_cap_ = cap;
+                changed = true;
+            }
+        }
+        if (changed && graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+    }
+    static double stf_value(const axg_stf &s, double time) {
+        // GaussianSTF::getValue (GaussianSTF.hpp:35-58)
+        const double invSqrtPi = 1. / std::sqrt(M_PI);
+        const double f = s.decay_factor / s.half_duration;
+        double t = time - s.time_shift, ft = f * t;
+        switch (s.derivative_order) {
+            case -1: return std::erf(ft) * 0.5 + 0.5;
+            case 0: return invSqrtPi * f * std::exp(-ft * ft);
+            case 1: return invSqrtPi * std::pow(f, 3) * std::exp(-ft * ft) * (-2. * t);
+            case 2: return invSqrtPi * std::pow(f, 3) * std::exp(-ft * ft) * (4. * ft * ft - 2.);
+        }
+        throw Error(AXG_E_ARG, "GaussianSTF::getValue || Unsupported derivative order.");
+    }
+    void fill_stf(int cap) {
+        // t accumulated as NewmarkTimeScheme::solve does (t += mDt)
+        std::vector<T> ms((size_t)cap * std::max(ms_n_, 1)), fs((size_t)cap * std::max(fs_n_, 1));
+        double t = cfg_.t0;
+        for (int k = 0; k < cap; k++) {
+            for (int i = 0; i < ms_n_; i++) ms[(size_t)k * ms_n_ + i] = (T)stf_value(model_.ms.stf[i], t);
+            for (int i = 0; i < fs_n_; i++) fs[(size_t)k * fs_n_ + i] = (T)stf_value(model_.fs.stf[i], t);
+            t += cfg_.dt;
+        }
+        ms_stf_.upload(ms);
+        fs_stf_.upload(fs);
+        stf_cap_ = cap;
+    }
+
+    // ------------------------------------------------------------ launches ---
+    void launch_sources() {
+        if (ms_n_) {
+            MomentArgs<T> a;
+            a.nsrc = ms_n_; a.elem = ms_el_.p; a.nu = ms_nu_.p; a.pat_off = ms_po_.p;
+            a.pattern = ms_pat_.p; a.stf = ms_stf_.p; a.stf_steps = stf_cap_; a.step = step_dev_.p;
+            a.e_nr = e_nr_.p; a.e_pts = e_pts_.p; a.e_axial = e_axial_.p; a.e_geom = e_geom_.p;
+            a.pt_off = sp_.off.p; a.pt_nu = sp_.nu.p; a.stiff = sp_.stiff.p; a.gmat = gmat_.p;
+            moment_source_kernel<T><<<ms_n_, 128, 0, stream_>>>(a);
+            post_launch();
+        }
+        if (fs_n_) {
+            ForceArgs<T> a;
+            a.nsrc = fs_n_; a.elem = fs_el_.p; a.nu = fs_nu_.p; a.pat_off = fs_po_.p;
+            a.pattern = fs_pat_.p; a.stf = fs_stf_.p; a.stf_steps = stf_cap_; a.step = step_dev_.p;
+            a.e_pts = e_pts_.p; a.pt_off = sp_.off.p; a.pt_nu = sp_.nu.p; a.stiff = sp_.stiff.p;
+            force_source_kernel<T><<<fs_n_, 128, 0, stream_>>>(a);
+            post_launch();
+        }
+    }
+
+    void launch_stiffness() {
+        if (timing_) AXG_CUDA(cudaEventRecord(ev0_, stream_));
+        for (auto &bp : sb_) {
+            SolidBucket &b = *bp;
+            SolidArgs<T, AT> a;
+            a.n_elem = b.n; a.nr = b.nr.p; a.pts = b.pts.p; a.axial = b.axial.p;
+            a.geom = b.geom.p; a.trig = b.trig.p; a.mod = b.mod.p; a.mod_off = b.mod_off.p;
+            a.attmod = b.attmod.p; a.att_off = b.att_off.p; a.state = state_.p;
+            a.state_off = b.state_off.p; a.pt_off = sp_.off.p; a.pt_nu = sp_.nu.p;
+            a.displ = elem_displ(sp_); a.stiff = sp_.stiff.p; a.tw = tw_.p; a.tw_off = tw_off_.p;
+            a.nsls = cfg_.nsls;
+            for (int l = 0; l < 8; l++) {
+                a.alpha[l] = (AT)cfg_.att_alpha[l]; a.beta[l] = (AT)cfg_.att_beta[l];
+                a.gamma[l] = (AT)cfg_.att_gamma[l];
+            }
+            a.gmat = gmat_.p;
+            int blocks = (b.n + b.tpc - 1) / b.tpc;
+            b.kernel<<<blocks, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc,
+                                                                              b.tpc, b.team_bytes);
+            post_launch();
+        }
+        if (timing_) AXG_CUDA(cudaEventRecord(ev1_, stream_));
+        for (auto &bp : fb_) {
+            FluidBucket &b = *bp;
+            FluidArgs<T> a;
+            a.n_elem = b.n; a.nr = b.nr.p; a.pts = b.pts.p; a.axial = b.axial.p; a.geom = b.geom.p;
+            a.K = b.K.p; a.K_off = b.K_off.p; a.pt_off = fp_.off.p; a.pt_nu = fp_.nu.p;
+            a.displ = elem_displ(fp_); a.stiff = fp_.stiff.p; a.tw = tw_.p; a.tw_off = tw_off_.p;
+            a.gmat = gmat_.p;
+            int blocks = (b.n + b.tpc - 1) / b.tpc;
+            b.kernel<<<blocks, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.tpc,
+                                                                              b.team_bytes);
+            post_launch();
+        }
+    }
+
+    void launch_coupling() {
+        if (!cp_n_) return;
+        CouplingArgs<T> a;
+        a.n = cp_n_; a.sp = cp_sp_.p; a.fp = cp_fp_.p;
+        a.nsu = cp_nsu_.p; a.nzu = cp_nzu_.p; a.nsa_m = cp_nsa_.p; a.nza_m = cp_nza_.p;
+        a.s_off = sp_.off.p; a.f_off = fp_.off.p; a.f_nu = fp_.nu.p;
+        a.s_displ = elem_displ(sp_); a.s_stiff = sp_.stiff.p; a.f_stiff = fp_.stiff.p;
+        int threads = 256, blocks = (cp_n_ * 32 + threads - 1) / threads;
+        solid_fluid_kernel<T><<<blocks, threads, 0, stream_>>>(a);
+        post_launch();
+    }
+
+    void launch_stations() {
+        if (!st_n_) return;
+        StationArgs<T> a;
+        a.nst = st_n_; a.elem = st_el_.p; a.w = st_w_.p; a.phi = st_phi_.p;
+        a.e_nr = e_nr_.p; a.e_pts = e_pts_.p; a.pt_off = sp_.off.p; a.pt_nu = sp_.nu.p;
+        a.displ = elem_displ(sp_); a.out = seis_.p; a.interval = st_interval_;
+        a.max_rec = seis_cap_; a.step = step_dev_.p;
+        int threads = 128, blocks = (st_n_ * 3 + threads - 1) / threads;
+        station_kernel<T><<<blocks, threads, 0, stream_>>>(a);
+        post_launch();
+    }
+
+    void launch_points(int mask) {
+        for (int solid = 1; solid >= 0; solid--) {
+            PointDev &P = solid ? sp_ : fp_;
+            if (!P.n) continue;
+            if (P.n3d && (mask & 3)) {
+                Mass3DArgs<T> a;
+                a.n = P.n3d; a.pt = P.pt3d.p; a.nr = P.nr.p; a.off = P.off.p; a.flags = P.flags.p;
+                a.inv_mass = P.inv3.p; a.im_off = P.im_off.p; a.tw = tw_.p; a.tw_off = tw_off_.p;
+                a.stiff = P.stiff.p; a.ndim = P.ndim; a.solid = solid; a.nr_max = P.nr_max;
+                int wpb = 4;
+                mass3d_kernel<T><<<(P.n3d + wpb - 1) / wpb, 32 * wpb, wpb * P.nr_max * sizeof(T), stream_>>>(a);
+                post_launch();
+            }
+            PointArgs<T, D> a;
+            a.nmodes = P.total; a.ndim = P.ndim; a.solid = solid; a.mode_pt = P.mode_pt.p;
+            a.off = P.off.p; a.nr = P.nr.p; a.flags = P.flags.p; a.inv_mass1 = P.inv1.p;
+            a.stiff = P.stiff.p; a.accel = P.accel.p; a.displ = P.displ.p; a.veloc = P.veloc.p;
+            a.cd = P.cd.p; a.cv = P.cv.p; a.displ_elem = P.displ_elem.p;
+            if constexpr (sizeof(D) == sizeof(T)) {
+                // NewmarkTimeScheme::update statics, formed in double then cast to Real
+                a.dt = (D)cfg_.dt; a.half_dt = (D)(.5 * cfg_.dt); a.half_dt_dt = (D)(.5 * cfg_.dt * cfg_.dt);
+            } else {
+                a.dt = cfg_.dt; a.half_dt = .5 * cfg_.dt; a.half_dt_dt = .5 * cfg_.dt * cfg_.dt;
+            }
+            a.nonfinite = nonfinite_.p;
+            a.mask = mask;
+            int threads = 256, blocks = (P.total + threads - 1) / threads;
+            point_update_kernel<T, D, COMP><<<blocks, threads, 0, stream_>>>(a);
+            post_launch();
+        }
+    }
+
+    void launch_step() {
+        launch_sources();
+        launch_stiffness();
+        launch_coupling();
+        launch_stations();
+        launch_points(7);
+        advance_step_kernel<T><<<1, 1, 0, stream_>>>(step_dev_.p);
+        post_launch();
+    }
+
+    void post_launch() {
+        launches_++;
+        cudaError_t e = cudaPeekAtLastError();
+        if (e != cudaSuccess)
+            throw Error(AXG_E_CUDA, std::string("Engine::launch || ") + cudaGetErrorString(e));
+    }
+
+    void capture() {
+        cudaGraph_t g;
+        int64_t before = launches_;
+        AXG_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        try {
+            launch_step();
+        } catch (...) {
+            cudaStreamEndCapture(stream_, &g);
+            throw;
+        }
+        AXG_CUDA(cudaStreamEndCapture(stream_, &g));
+        kernels_per_step_ = launches_ - before;
+        launches_ = before;
+        AXG_CUDA(cudaGraphInstantiate(&graph_exec_, g, 0));
+        cudaGraphDestroy(g);
+    }
+
+    // ---------------------------------------------------------------- data ---
+    axg_config cfg_;
+    HostModel model_;
+    cudaDeviceProp prop_;
+    cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
+    bool finalized_ = false;
+    int step_ = 0, tstep_host_ = 0;
+    int64_t launches_ = 0, kernels_per_step_ = 0;
+    bool timing_ = false;
+    double time_ms_ = 0;
+    int64_t time_n_ = 0;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    int team_override_[5];
+
+    DBuf<T> gmat_, tw_;
+    DBuf<int> tw_off_;
+    PointDev sp_, fp_;
+    std::vector<std::unique_ptr<SolidBucket>> sb_;
+    std::vector<std::unique_ptr<FluidBucket>> fb_;
+    DBuf<AT> state_;
+    int cp_n_ = 0;
+    DBuf<int> cp_sp_, cp_fp_;
+    DBuf<T> cp_nsu_, cp_nzu_, cp_nsa_, cp_nza_;
+    int ms_n_ = 0, fs_n_ = 0, stf_cap_ = 0;
+    DBuf<int> ms_el_, ms_nu_, fs_el_, fs_nu_;
+    DBuf<int64_t> ms_po_, fs_po_;
+    DBuf<C> ms_pat_, fs_pat_;
+    DBuf<T> ms_stf_, fs_stf_;
+    DBuf<int> e_nr_, e_pts_;
+    DBuf<uint8_t> e_axial_;
+    DBuf<T> e_geom_;
+    int st_n_ = 0, st_interval_ = 1, seis_cap_ = 0;
+    DBuf<int> st_el_;
+    DBuf<T> st_w_, st_phi_;
+    DBuf<double> seis_;
+    DBuf<int> step_dev_, nonfinite_;
+};
+
+}  // namespace axg

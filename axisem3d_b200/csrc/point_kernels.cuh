@@ -1,0 +1,432 @@
+// point_kernels.cuh -- point-wise kernels of one time step.
+//
+//   solid_fluid_kernel      SolidFluidCoupling::apply (boundary/solid_fluid/SolidFluidCoupling.cpp:30-36,
+//                           SolidFluidCoupling1D.hpp:26-37)
+//   mass3d_kernel           Nyquist + boundary conditions + Mass3D::computeAccel (point/mass/Mass3D.cpp:41-68)
+//   point_update_kernel     AxialBoundary::apply (boundary/axial/AxialBoundary.cpp:21-51),
+//                           FluidSurfaceBoundary::apply (surface/FluidSurfaceBoundary.cpp:20-26),
+//                           Solid/FluidPoint::computeStiffToAccel (SolidPoint.cpp:28-36, FluidPoint.cpp:28-54),
+//                           Mass1D::computeAccel (mass/Mass1D.hpp:25-32),
+//                           NewmarkTimeScheme::update (time/NewmarkTimeScheme.hpp:47-59)
+//   moment_source_kernel    SolidMoment::apply -> SolidElement::addMomentSource
+//                           (source/elem_src/solid/SolidMoment.cpp:29-33, element/SolidElement.cpp:273-356)
+//   force_source_kernel     SolidForce::apply -> SolidPoint::addForceSource (SolidPoint.hpp:112-119)
+//   station_kernel          StationSolid::record, displacement (output/station-wise/station/StationSolid.cpp:58-66,
+//                           Station.hpp:53-72, shared/eigen/eigen_tools.hpp:78-106)
+#pragma once
+
+#include "common.cuh"
+
+namespace axg {
+
+// point flags
+constexpr uint8_t PT_AXIAL = 1, PT_SURFACE = 2, PT_MASS3D = 4;
+
+// ------------------------------------------------------ solid-fluid coupling ---
+template <class T>
+struct CouplingArgs {
+    int n;
+    const int *sp, *fp;            // point indices
+    const T *nsu, *nzu, *nsa_m, *nza_m;
+    const int *s_off, *f_off, *f_nu;
+    const cx_t<T> *s_displ;
+    cx_t<T> *s_stiff, *f_stiff;
+};
+
+template <class T>
+__global__ void solid_fluid_kernel(const CouplingArgs<T> a) {
+    // one warp per pair, lanes over modes
+    const int pair = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x & 31;
+    if (pair >= a.n) return;
+    const int s = a.sp[pair], f = a.fp[pair];
+    const int nu = a.f_nu[f];
+    const T nsu = a.nsu[pair], nzu = a.nzu[pair], nsa = a.nsa_m[pair], nza = a.nza_m[pair];
+    for (int al = lane; al < nu; al += 32) {
+        const cx_t<T> us = a.s_displ[(size_t)(a.s_off[s] + al) * 3 + 0];
+        const cx_t<T> uz = a.s_displ[(size_t)(a.s_off[s] + al) * 3 + 2];
+        cx_t<T> fs = a.f_stiff[a.f_off[f] + al];
+        fs = cadd(fs, cscale(us, nsu));
+        fs = cadd(fs, cscale(uz, nzu));
+        a.f_stiff[a.f_off[f] + al] = fs;
+        cx_t<T> *ss = a.s_stiff + (size_t)(a.s_off[s] + al) * 3;
+        ss[0] = csub(ss[0], cscale(fs, nsa));
+        ss[2] = csub(ss[2], cscale(fs, nza));
+    }
+}
+
+// -------------------------------------------------------- 3-D mass points ---
+template <class T>
+struct Mass3DArgs {
+    int n;                       // number of Mass3D points
+    const int *pt;               // their indices
+    const int *nr, *off;
+    const uint8_t *flags;
+    const T *inv_mass;           // pool
+    const int64_t *im_off;       // [npoints]
+    const T *tw;                 // twiddle pool (cos then sin for each nr)
+    const int *tw_off;
+    cx_t<T> *stiff;
+    int ndim;
+    int solid;
+    int nr_max;                  // scratch reals per warp
+};
+
+// Boundary conditions on one mode of one point, in the reference order:
+// AxialBoundary (after assembly) then the Nyquist rule of computeStiffToAccel.
+template <class T>
+__device__ __forceinline__ void point_bc(cx_t<T> *f, int ndim, int al, int nu, int nr,
+                                         uint8_t flags, bool solid) {
+    const T half = (T)0.5;
+    if (flags & PT_AXIAL) {
+        if (solid) {
+            if (al == 0) {
+                f[0] = mk<T>(0, 0); f[1] = mk<T>(0, 0);
+            } else if (al == 1) {
+                const cx_t<T> a0 = f[0], a1 = f[1];
+                // (stiff(1,0) - i stiff(1,1)) * 0.5, then stiff(1,1) = i stiff(1,0)
+                const cx_t<T> t = mk<T>((a0.x + a1.y) * half, (a0.y - a1.x) * half);
+                f[0] = t;
+                f[1] = mk<T>(-t.y, t.x);
+                f[2] = mk<T>(0, 0);
+            } else {
+                f[0] = mk<T>(0, 0); f[1] = mk<T>(0, 0); f[2] = mk<T>(0, 0);
+            }
+        } else if (al >= 1) {
+            f[0] = mk<T>(0, 0);
+        }
+    }
+    if (!solid && (flags & PT_SURFACE)) f[0] = mk<T>(0, 0);
+    if ((nr & 1) == 0 && al == nu - 1)
+        for (int c = 0; c < ndim; c++) f[c].y = 0;
+}
+
+template <class T>
+__global__ void mass3d_kernel(const Mass3DArgs<T> a) {
+    // one warp per point: boundary conditions, then per dimension
+    // C2R -> x 1/M_k -> R2C with a per-warp scratch of nr reals
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int w = threadIdx.x / 32, lane = threadIdx.x & 31;
+    const int ip = blockIdx.x * (blockDim.x / 32) + w;
+    if (ip >= a.n) return;
+    const int p = a.pt[ip];
+    const int nr = a.nr[p], nu = nr / 2 + 1, off = a.off[p], nd = a.ndim;
+    const uint8_t fl = a.flags[p];
+    T *r = reinterpret_cast<T *>(sm) + (size_t)w * a.nr_max;
+    const T *twc = a.tw + a.tw_off[nr], *tws = twc + nr;
+    for (int al = lane; al < nu; al += 32) {
+        cx_t<T> f[3];
+        for (int d = 0; d < nd; d++) f[d] = a.stiff[(size_t)(off + al) * nd + d];
+        point_bc<T>(f, nd, al, nu, nr, fl, a.solid);
+        for (int d = 0; d < nd; d++) a.stiff[(size_t)(off + al) * nd + d] = f[d];
+    }
+    __syncwarp();
+    const T *im = a.inv_mass + a.im_off[p];
+    const T inv_nr = (T)1 / (T)nr;
+    for (int c = 0; c < nd; c++) {
+        for (int k = lane; k < nr; k += 32) {
+            T acc = a.stiff[(size_t)off * nd + c].x;
+            int j = 0;
+            for (int al = 1; al < nu; al++) {
+                j += k; j = j >= nr ? j - nr : j;
+                const cx_t<T> v = a.stiff[(size_t)(off + al) * nd + c];
+                acc += (T)2 * (v.x * twc[j] - v.y * tws[j]);
+            }
+            r[k] = acc * im[k];
+        }
+        __syncwarp();
+        for (int al = lane; al < nu; al += 32) {
+            T re = 0, imv = 0;
+            int j = 0;
+            const int step = al % nr;
+            for (int k = 0; k < nr; k++) {
+                const T x = r[k] * inv_nr;
+                re += x * twc[j];
+                imv -= x * tws[j];
+                j += step; j = j >= nr ? j - nr : j;
+            }
+            if (al == 0) imv = 0;
+            if ((nr & 1) == 0 && al == nr / 2) { re *= (T)0.5; imv = 0; }
+            a.stiff[(size_t)(off + al) * nd + c] = mk<T>(re, imv);
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------ stiff -> accel + Newmark ---
+// T: stiffness/acceleration type; D: displacement/velocity storage type.
+// MIXED (T = float, D = double): increments formed in double, optionally
+// accumulated with compensated (Kahan) summation; a float copy of d feeds the
+// elements.
+template <class T, class D>
+struct PointArgs {
+    int nmodes;                  // sum nu
+    int ndim;
+    int solid;
+    const int *mode_pt;          // [nmodes] owning point
+    const int *off, *nr;         // per point
+    const uint8_t *flags;
+    const T *inv_mass1;          // per point (1-D mass)
+    cx_t<T> *stiff;
+    cx_t<T> *accel;
+    cx_t<D> *displ, *veloc;
+    cx_t<float> *cd, *cv;        // compensation terms (MIXED + compensated)
+    cx_t<T> *displ_elem;         // float copy of d for elements (MIXED) or null
+    D dt, half_dt, half_dt_dt;
+    int *nonfinite;
+    int mask;                    // 1 = BC after assembly, 2 = 1/M, 4 = Newmark
+};
+
+template <class T, class D, bool COMP>
+__global__ void point_update_kernel(const PointArgs<T, D> a) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= a.nmodes) return;
+    const int p = a.mode_pt[m];
+    const int off = a.off[p], nr = a.nr[p], nu = nr / 2 + 1, al = m - off;
+    const uint8_t fl = a.flags[p];
+    const int nd = a.ndim;
+    cx_t<T> f[3];
+    for (int d = 0; d < nd; d++) f[d] = a.stiff[(size_t)m * nd + d];
+    if (!(fl & PT_MASS3D)) {
+        if (a.mask & 1) point_bc<T>(f, nd, al, nu, nr, fl, a.solid);
+        if (a.mask & 2) {
+            const T im = a.inv_mass1[p];
+            for (int d = 0; d < nd; d++) f[d] = cscale(f[d], im);
+        }
+    }
+    if (!(a.mask & 4)) {
+        // stages without the update: the result stays in the stiffness field, as
+        // computeStiffToAccel works in place on mStiff
+        for (int d = 0; d < nd; d++) a.stiff[(size_t)m * nd + d] = f[d];
+        return;
+    }
+    bool bad = false;
+    for (int d = 0; d < nd; d++) {
+        const size_t q = (size_t)m * nd + d;
+        const cx_t<T> acc = a.accel[q];
+        cx_t<D> v = a.veloc[q], u = a.displ[q];
+        if constexpr (sizeof(D) == sizeof(T)) {
+            // NewmarkTimeScheme::update in the working precision
+            v.x += a.half_dt * (acc.x + f[d].x);
+            v.y += a.half_dt * (acc.y + f[d].y);
+            u.x += a.dt * v.x + a.half_dt_dt * f[d].x;
+            u.y += a.dt * v.y + a.half_dt_dt * f[d].y;
+        } else {
+            const D dvx = a.half_dt * ((D)acc.x + (D)f[d].x);
+            const D dvy = a.half_dt * ((D)acc.y + (D)f[d].y);
+            if constexpr (COMP) {
+                cx_t<float> cv = a.cv[q], cd = a.cd[q];
+                D y = dvx - (D)cv.x, t = v.x + y; cv.x = (float)((t - v.x) - y); v.x = t;
+                y = dvy - (D)cv.y; t = v.y + y; cv.y = (float)((t - v.y) - y); v.y = t;
+                const D dux = a.dt * v.x + a.half_dt_dt * (D)f[d].x;
+                const D duy = a.dt * v.y + a.half_dt_dt * (D)f[d].y;
+                y = dux - (D)cd.x; t = u.x + y; cd.x = (float)((t - u.x) - y); u.x = t;
+                y = duy - (D)cd.y; t = u.y + y; cd.y = (float)((t - u.y) - y); u.y = t;
+                a.cv[q] = cv;
+                a.cd[q] = cd;
+            } else {
+                v.x += dvx; v.y += dvy;
+                u.x += a.dt * v.x + a.half_dt_dt * (D)f[d].x;
+                u.y += a.dt * v.y + a.half_dt_dt * (D)f[d].y;
+            }
+            a.displ_elem[q] = mk<T>((T)u.x, (T)u.y);
+        }
+        bad |= !(isfinite(u.x) && isfinite(u.y));
+        a.veloc[q] = v;
+        a.displ[q] = u;
+        a.accel[q] = f[d];
+        a.stiff[q] = mk<T>(0, 0);
+    }
+    if (bad) atomicOr(a.nonfinite, 1);
+}
+
+// ------------------------------------------------------------------ sources ---
+template <class T>
+struct MomentArgs {
+    int nsrc;
+    const int *elem, *nu;              // per source; nu = pattern rows
+    const int64_t *pat_off;            // complex offset
+    const cx_t<T> *pattern;            // [nu][6][25]
+    const T *stf;                      // [nsteps][nsrc]
+    int stf_steps;
+    const int *step;                   // device step counter
+    const int *e_nr, *e_pts;           // solid elements
+    const uint8_t *e_axial;
+    const T *e_geom;                   // [ne][10][25]
+    const int *pt_off, *pt_nu;
+    cx_t<T> *stiff;
+    const T *gmat;
+};
+
+template <class T>
+__global__ void moment_source_kernel(const MomentArgs<T> a) {
+    using C = cx_t<T>;
+    const int s = blockIdx.x;
+    if (s >= a.nsrc) return;
+    __shared__ T sGll[25], sGlj[25], sGeo[125];
+    __shared__ C sS[3][6][25];     // at most 3 modes on the axis; loop for more
+    __shared__ C sA[3][3][25];
+    __shared__ int sOff[25], sNu[25];
+    const int e = a.elem[s];
+    const int enu = a.e_nr[e] / 2 + 1;
+    const int nuco = min(enu, a.nu[s]);
+    const bool axial = a.e_axial[e] != 0;
+    const int st = min(*a.step, a.stf_steps - 1);
+    const T v = a.stf[(size_t)st * a.nsrc + s];
+    for (int i = threadIdx.x; i < 25; i += blockDim.x) {
+        sGll[i] = a.gmat[i]; sGlj[i] = a.gmat[25 + i];
+        const int p = a.e_pts[(size_t)e * 25 + i];
+        sOff[i] = a.pt_off[p]; sNu[i] = a.pt_nu[p];
+    }
+    for (int i = threadIdx.x; i < 125; i += blockDim.x) sGeo[i] = a.e_geom[(size_t)e * 250 + i];
+    __syncthreads();
+    const T *Gxi = axial ? sGlj : sGll;
+    const T *dsdxii = sGeo, *dsdeta = sGeo + 25, *dzdxii = sGeo + 50, *dzdeta = sGeo + 75,
+            *invs = sGeo + 100;
+    for (int a0 = 0; a0 < nuco; a0 += 3) {
+        const int na = min(3, nuco - a0);
+        // stress = -pattern * stf; X/Y/A terms (computeQuad6_NoIntegration, plain operators)
+        for (int i = threadIdx.x; i < na * 25; i += blockDim.x) {
+            const int aa = i / 25, q = i % 25, al = a0 + aa;
+            C sg[6];
+            for (int d = 0; d < 6; d++) {
+                const C pv = a.pattern[a.pat_off[s] + ((size_t)al * 6 + d) * 25 + q];
+                sg[d] = mk<T>(-(pv.x * v), -(pv.y * v));
+            }
+            const T ze = dzdeta[q], zx = dzdxii[q], se = dsdeta[q], sx = dsdxii[q];
+            sS[aa][0][q] = cadd(cscale(sg[0], ze), cscale(sg[4], se));
+            sS[aa][1][q] = cadd(cscale(sg[0], zx), cscale(sg[4], sx));
+            sS[aa][2][q] = cadd(cscale(sg[5], ze), cscale(sg[3], se));
+            sS[aa][3][q] = cadd(cscale(sg[5], zx), cscale(sg[3], sx));
+            sS[aa][4][q] = cadd(cscale(sg[4], ze), cscale(sg[2], se));
+            sS[aa][5][q] = cadd(cscale(sg[4], zx), cscale(sg[2], sx));
+            const T alf = (T)al;
+            sA[aa][0][q] = csub(cia(alf, sg[5]), sg[1]);
+            sA[aa][1][q] = cadd(cia(alf, sg[1]), sg[5]);
+            sA[aa][2][q] = cia(alf, sg[3]);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < na * 25; i += blockDim.x) {
+            const int aa = i / 25, q = i % 25, al = a0 + aa;
+            const int ii = q / 5, jj = q % 5;
+            for (int c = 0; c < 3; c++) {
+                C g1 = mk<T>(0, 0), g2 = mk<T>(0, 0);
+                for (int k = 0; k < 5; k++) {
+                    const C xv = sS[aa][2 * c][k * 5 + jj], yv = sS[aa][2 * c + 1][ii * 5 + k];
+                    const T gx = Gxi[ii * 5 + k], gt = sGll[jj * 5 + k];
+                    g1.x += gx * xv.x; g1.y += gx * xv.y;
+                    g2.x += yv.x * gt; g2.y += yv.y * gt;
+                }
+                C f = cadd(g1, g2);
+                f = csub(f, cscale(sA[aa][c][q], invs[q]));
+                if (axial) {
+                    f = csub(f, cscale(cscale(sA[aa][c][jj], dzdeta[jj]), Gxi[ii * 5 + 0]));
+                    if (ii == 0) {
+                        C b = mk<T>(0, 0);
+                        for (int k = 0; k < 5; k++) {
+                            const C y0 = cscale(sA[aa][c][k], dzdxii[k]);
+                            const T gt = sGll[jj * 5 + k];
+                            b.x += y0.x * gt; b.y += y0.y * gt;
+                        }
+                        f = csub(f, b);
+                    }
+                }
+                if (al < sNu[q]) atomic_add_cx(a.stiff + (size_t)(sOff[q] + al) * 3 + c, mk<T>(-f.x, -f.y));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <class T>
+struct ForceArgs {
+    int nsrc;
+    const int *elem, *nu;
+    const int64_t *pat_off;
+    const cx_t<T> *pattern;            // [nu][3][25]
+    const T *stf;
+    int stf_steps;
+    const int *step;
+    const int *e_pts;
+    const int *pt_off, *pt_nu;
+    cx_t<T> *stiff;
+};
+
+template <class T>
+__global__ void force_source_kernel(const ForceArgs<T> a) {
+    const int s = blockIdx.x;
+    if (s >= a.nsrc) return;
+    const int e = a.elem[s];
+    const int st = min(*a.step, a.stf_steps - 1);
+    const T v = a.stf[(size_t)st * a.nsrc + s];
+    for (int i = threadIdx.x; i < a.nu[s] * 25; i += blockDim.x) {
+        const int al = i / 25, q = i % 25;
+        const int p = a.e_pts[(size_t)e * 25 + q];
+        if (al >= a.pt_nu[p]) continue;
+        for (int c = 0; c < 3; c++) {
+            const cx_t<T> pv = a.pattern[a.pat_off[s] + ((size_t)al * 3 + c) * 25 + q];
+            atomic_add_cx(a.stiff + (size_t)(a.pt_off[p] + al) * 3 + c, mk<T>(pv.x * v, pv.y * v));
+        }
+    }
+}
+
+// ----------------------------------------------------------------- stations ---
+template <class T>
+struct StationArgs {
+    int nst;
+    const int *elem;
+    const T *w;               // [nst][25]
+    const T *phi;             // [nst]
+    const int *e_nr, *e_pts;
+    const int *pt_off, *pt_nu;
+    const cx_t<T> *displ;
+    double *out;              // [nrec][nst][3]
+    int interval;
+    int max_rec;
+    const int *step;
+};
+
+template <class T>
+__global__ void station_kernel(const StationArgs<T> a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.nst * 3) return;
+    const int step = *a.step;
+    if (step % a.interval != 0) return;
+    const int rec = step / a.interval;
+    if (rec >= a.max_rec) return;
+    const int s = t / 3, c = t % 3;
+    const int e = a.elem[s];
+    const int nu = a.e_nr[e] / 2 + 1;
+    const T phi = a.phi[s];
+    T acc = 0;
+    for (int al = 0; al < nu; al++) {
+        cx_t<T> x = mk<T>(0, 0);
+        for (int q = 0; q < 25; q++) {
+            const T w = a.w[(size_t)s * 25 + q];
+            if (w == (T)0) continue;
+            const int p = a.e_pts[(size_t)e * 25 + q];
+            if (al < a.pt_nu[p]) x = cadd(x, cscale(a.displ[(size_t)(a.pt_off[p] + al) * 3 + c], w));
+        }
+        if (al == 0) {
+            acc += x.x;
+        } else {
+            T sn, cs;
+            if constexpr (sizeof(T) == 4) sincosf((T)al * phi, &sn, &cs);
+            else sincos((T)al * phi, &sn, &cs);
+            acc += (T)2 * (cs * x.x - sn * x.y);
+        }
+    }
+    a.out[((size_t)rec * a.nst + s) * 3 + c] = (double)acc;
+}
+
+// element-facing float copy of a double displacement (mixed precision)
+template <class T, class D>
+__global__ void narrow_kernel(const cx_t<D> *src, cx_t<T> *dst, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = mk<T>((T)src[i].x, (T)src[i].y);
+}
+
+template <class T>
+__global__ void advance_step_kernel(int *step) { *step += 1; }
+
+}  // namespace axg

@@ -1,0 +1,613 @@
+// solid_kernel.cuh -- fused stiffness of solid spectral elements (nPol = 4).
+//
+// One team of threads evaluates one element at a time, entirely on chip:
+//   gather u from the points (zero-padded above each point's nu)
+//     SolidPoint::scatterDisplToElement   (SOLVER/src/core/point/SolidPoint.hpp:82-98)
+//   GLL gradient + analytic d/dphi, axial L'Hopital rows
+//     GradientQuadrature::computeGrad6    (SOLVER/src/core/element/grad/GradientQuadrature.hpp:207-231)
+//   [RTZ] CoordTransformSpherical::transformSPZ_RTZ6 (crd/CoordTransformSpherical.hpp:186-216)
+//   1-D material: strainToStress_FR per Fourier mode
+//   3-D material: Fourier -> phi slices (direct DFT in shared memory, FFTW conventions,
+//     SOLVER/src/core/fft/SolverFFTW.hpp:101-172), strainToStress_CD per slice,
+//     slices -> Fourier
+//   Isotropic / TransverselyIsotropic / Anisotropic::strainToStress
+//     (material/elastic/anisotropy/*.hpp)
+//   AttenuationFull / AttenuationCG4::apply (material/elastic/attenuation/*.hpp)
+//   [RTZ] transformRTZ_SPZ6
+//   GradientQuadrature::computeQuad6 (GradientQuadrature.hpp:294-324)
+//   scatter-add: point.stiff -= f   SolidPoint::gatherStiffFromElement (SolidPoint.hpp:101-109)
+//
+// Shared memory per team (T = float or double, C = complex T):
+//   geometry 10 x 25 T, trig 4 x 25 T, point tables 3 x 25 int, twiddles 2 x nr T,
+//   region A: 6 x nu x 25 C  (strain E, then stress S, then quadrature X/Y)
+//   region B: max(3 x nu x 25 C, nr x 6 x qc T)  (u, then stress slices, then A terms)
+#pragma once
+
+#include "common.cuh"
+
+namespace axg {
+
+constexpr int RHEO_ISO = 0, RHEO_TISO = 1, RHEO_ANISO = 2;
+constexpr int ATT_NONE = 0, ATT_FULL = 1, ATT_CG4 = 2;
+constexpr int KB = 4;   // slices per thread in the Fourier -> slice transform
+constexpr int AB = 4;   // modes per thread in the slice -> Fourier transform
+
+template <class T, class AT>
+struct SolidArgs {
+    int n_elem;
+    const int *nr;             // [n]
+    const int *pts;            // [n*25]
+    const uint8_t *axial;      // [n]
+    const T *geom;             // [n][10][25]
+    const T *trig;             // [n][4][25] sin t, cos t, sin 2t, cos 2t (RTZ only)
+    const T *mod;              // moduli pool
+    const int64_t *mod_off;    // [n]
+    const T *attmod;           // dlambda, dmu pool
+    const int64_t *att_off;    // [n]
+    AT *state;                 // attenuation state pool
+    const int64_t *state_off;  // [n] in AT units
+    const int *pt_off;         // [npoints] first mode of each point
+    const int *pt_nu;          // [npoints]
+    const cx_t<T> *displ;      // [sum nu][3]
+    cx_t<T> *stiff;            // [sum nu][3]
+    const T *tw;               // twiddle pool: for each nr, nr cos then nr sin
+    const int *tw_off;         // [nr_max + 1]
+    int nsls;
+    AT alpha[8], beta[8], gamma[8];
+    const T *gmat;             // [2][25]: G_GLL, G_GLJ (row-major, G(j,i) = l_j'(x_i))
+};
+
+// shared memory layout of one team
+struct TeamLayout {
+    int nr_max, nu_max, qc;
+    size_t geom, trig, ipt, tw, regA, regB, total;
+};
+
+template <class T>
+__host__ __device__ inline TeamLayout team_layout(int nr_max, int qc) {
+    TeamLayout L;
+    L.nr_max = nr_max;
+    L.nu_max = nr_max / 2 + 1;
+    L.qc = qc;
+    size_t o = 0;
+    auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    L.geom = o; o = al(o + 10 * 25 * sizeof(T));
+    L.trig = o; o = al(o + 4 * 25 * sizeof(T));
+    L.ipt = o;  o = al(o + 3 * 25 * sizeof(int));
+    L.tw = o;   o = al(o + 2 * (size_t)nr_max * sizeof(T));
+    L.regA = o; o = al(o + 6 * (size_t)L.nu_max * 25 * 2 * sizeof(T));
+    size_t b1 = 3 * (size_t)L.nu_max * 25 * 2 * sizeof(T);
+    size_t b2 = (size_t)nr_max * 6 * qc * sizeof(T);
+    L.regB = o; o = al(o + (b1 > b2 ? b1 : b2));
+    L.total = o;
+    return L;
+}
+
+// ------------------------------------------------------------ rheology ---
+// Isotropic::strainToStress (Isotropic.hpp:154-170); 2 mu is exact as mu + mu
+template <class V, class R>
+__device__ __forceinline__ void stress_iso(const V e[6], V s[6], R lam, R mu) {
+    R mu2 = mu + mu;
+    V sii = cscale(cadd(cadd(e[0], e[1]), e[2]), lam);
+    s[0] = cadd(sii, cscale(e[0], mu2));
+    s[1] = cadd(sii, cscale(e[1], mu2));
+    s[2] = cadd(sii, cscale(e[2], mu2));
+    s[3] = cscale(e[3], mu);
+    s[4] = cscale(e[4], mu);
+    s[5] = cscale(e[5], mu);
+}
+// TransverselyIsotropic::strainToStress (TransverselyIsotropic.hpp:160-180)
+template <class V, class R>
+__device__ __forceinline__ void stress_tiso(const V e[6], V s[6], R A, R C, R F, R L, R Nn) {
+    R mN2 = -(Nn + Nn);
+    V t3 = cadd(e[0], e[1]);
+    V t4 = cadd(cscale(t3, A), cscale(e[2], F));
+    s[0] = cadd(t4, cscale(e[1], mN2));
+    s[1] = cadd(t4, cscale(e[0], mN2));
+    s[2] = cadd(cscale(t3, F), cscale(e[2], C));
+    s[3] = cscale(e[3], L);
+    s[4] = cscale(e[4], L);
+    s[5] = cscale(e[5], Nn);
+}
+// Anisotropic::strainToStress (Anisotropic.hpp:202-274); c = upper triangle row-major
+template <class V, class R>
+__device__ __forceinline__ void stress_aniso(const V e[6], V s[6], const R c[21]) {
+    const int idx[6][6] = {{0, 1, 2, 3, 4, 5},      {1, 6, 7, 8, 9, 10},
+                           {2, 7, 11, 12, 13, 14},  {3, 8, 12, 15, 16, 17},
+                           {4, 9, 13, 16, 18, 19},  {5, 10, 14, 17, 19, 20}};
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        V acc = cscale(e[0], c[idx[i][0]]);
+#pragma unroll
+        for (int j = 1; j < 6; j++) acc = cadd(acc, cscale(e[j], c[idx[i][j]]));
+        s[i] = acc;
+    }
+}
+
+// scalar "complex" wrapper so that the rheology templates serve real slices too
+template <class T> struct re1 { T x; };
+template <class T> __device__ __forceinline__ re1<T> cadd(re1<T> a, re1<T> b) { return {a.x + b.x}; }
+template <class T> __device__ __forceinline__ re1<T> csub(re1<T> a, re1<T> b) { return {a.x - b.x}; }
+template <class T, class R> __device__ __forceinline__ re1<T> cscale(re1<T> a, R s) { return {a.x * (T)s}; }
+
+template <int RHEO, class T, class V>
+__device__ __forceinline__ void elastic_at(const T *mod, int nslice, int slice, int q,
+                                           const V e[6], V s[6]) {
+    const size_t ns = (size_t)nslice * 25, o = (size_t)slice * 25 + q;
+    if constexpr (RHEO == RHEO_ISO) {
+        stress_iso(e, s, __ldg(mod + o), __ldg(mod + ns + o));
+    } else if constexpr (RHEO == RHEO_TISO) {
+        stress_tiso(e, s, __ldg(mod + o), __ldg(mod + ns + o), __ldg(mod + 2 * ns + o),
+                    __ldg(mod + 3 * ns + o), __ldg(mod + 4 * ns + o));
+    } else {
+        T c[21];
+#pragma unroll
+        for (int k = 0; k < 21; k++) c[k] = __ldg(mod + k * ns + o);
+        stress_aniso(e, s, c);
+    }
+}
+
+// CoordTransformSpherical::transformSPZ_RTZ6 / transformRTZ_SPZ6 (one point of one mode)
+template <class V, class T>
+__device__ __forceinline__ void spz_to_rtz6(V e[6], T s1, T c1, T s2, T c2) {
+    const T half = (T)0.5;
+    V s02 = cadd(e[0], e[2]), d02 = csub(e[0], e[2]);
+    e[0] = cscale(csub(cadd(s02, cscale(d02, c2)), cscale(e[4], s2)), half);
+    e[2] = csub(s02, e[0]);
+    e[4] = cadd(cscale(e[4], c2), cscale(d02, s2));
+    V t3 = e[3];
+    e[3] = cadd(cscale(t3, c1), cscale(e[5], s1));
+    e[5] = csub(cscale(e[5], c1), cscale(t3, s1));
+}
+template <class V, class T>
+__device__ __forceinline__ void rtz_to_spz6(V s[6], T s1, T c1, T s2, T c2) {
+    const T half = (T)0.5;
+    V s02 = cadd(s[0], s[2]), d02 = csub(s[0], s[2]);
+    s[0] = cadd(cscale(cadd(s02, cscale(d02, c2)), half), cscale(s[4], s2));
+    s[2] = csub(s02, s[0]);
+    s[4] = csub(cscale(s[4], c2), cscale(cscale(d02, s2), half));
+    V t3 = s[3];
+    s[3] = csub(cscale(t3, c1), cscale(s[5], s1));
+    s[5] = cadd(cscale(s[5], c1), cscale(t3, s1));
+}
+
+// ----------------------------------------------------------- attenuation ---
+// One point of one mode (complex) or slice (real):
+//   stress -= sum_l mem_l; mem_l = alpha_l mem_l + beta_l dstress;
+//   dstress = iso(dlambda, dmu)(strain); mem_l += gamma_l dstress
+// (AttenuationFull.hpp:189-207, Attenuation.hpp:92-134). The state (dstress,
+// mem) lives in AT (double in the mixed-precision mode) and is streamed from
+// and to HBM once per step.
+template <bool CPLX, class AT, class V>
+__device__ __forceinline__ AT part(const V &v, int w) {
+    if constexpr (CPLX) return (AT)(w ? v.y : v.x);
+    else return (AT)v.x;
+}
+
+template <class T, class AT, bool CPLX, class V>
+__device__ __forceinline__ void attenuate(const SolidArgs<T, AT> &a, AT *state, size_t nslot,
+                                          size_t slot, const V e[6], V s[6], T dl, T dm) {
+    constexpr int W = CPLX ? 2 : 1;
+    AT *dst = state;                             // [6][nslot] (x W)
+    AT *mem = state + 6 * nslot * W;             // [nsls][6][nslot] (x W)
+    const size_t sls = 6 * nslot * W;
+    AT ds[6][W], sv[6][W];
+#pragma unroll
+    for (int d = 0; d < 6; d++)
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            ds[d][w] = dst[(d * nslot + slot) * W + w];
+            sv[d][w] = part<CPLX, AT>(s[d], w);
+        }
+    for (int l = 0; l < a.nsls; l++) {
+        AT *m = mem + l * sls;
+        const AT al = a.alpha[l], be = a.beta[l];
+#pragma unroll
+        for (int d = 0; d < 6; d++)
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                AT mv = m[(d * nslot + slot) * W + w];
+                sv[d][w] -= mv;
+                m[(d * nslot + slot) * W + w] = al * mv + be * ds[d][w];
+            }
+    }
+    // new dstress from the strain (Isotropic::strainToStress with dlambda, dmu)
+    const AT lam = (AT)dl, mu = (AT)dm, mu2 = mu + mu;
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+        const AT e0 = part<CPLX, AT>(e[0], w), e1 = part<CPLX, AT>(e[1], w),
+                 e2 = part<CPLX, AT>(e[2], w);
+        const AT sii = (e0 + e1 + e2) * lam;
+        ds[0][w] = sii + e0 * mu2;
+        ds[1][w] = sii + e1 * mu2;
+        ds[2][w] = sii + e2 * mu2;
+        ds[3][w] = part<CPLX, AT>(e[3], w) * mu;
+        ds[4][w] = part<CPLX, AT>(e[4], w) * mu;
+        ds[5][w] = part<CPLX, AT>(e[5], w) * mu;
+    }
+#pragma unroll
+    for (int d = 0; d < 6; d++)
+#pragma unroll
+        for (int w = 0; w < W; w++) dst[(d * nslot + slot) * W + w] = ds[d][w];
+    for (int l = 0; l < a.nsls; l++) {
+        AT *m = mem + l * sls;
+        const AT ga = a.gamma[l];
+#pragma unroll
+        for (int d = 0; d < 6; d++)
+#pragma unroll
+            for (int w = 0; w < W; w++) m[(d * nslot + slot) * W + w] += ga * ds[d][w];
+    }
+#pragma unroll
+    for (int d = 0; d < 6; d++) {
+        if constexpr (CPLX) { s[d].x = (T)sv[d][0]; s[d].y = (T)sv[d][1]; }
+        else s[d].x = (T)sv[d][0];
+    }
+}
+
+__device__ __forceinline__ int cg4_slot(int q) {
+    // (1,1) (1,3) (3,1) (3,3) -> 0..3, else -1
+    return q == 6 ? 0 : q == 8 ? 1 : q == 16 ? 2 : q == 18 ? 3 : -1;
+}
+
+// ----------------------------------------------------------------- kernel ---
+template <class T, class AT, int RHEO, int ATT, bool IS3D, bool RTZ>
+__global__ void __launch_bounds__(256)
+solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_max,
+                       const int teams_per_cta, const size_t team_bytes) {
+    using C = cx_t<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int TEAM = blockDim.x / teams_per_cta;
+    const int team = threadIdx.x / TEAM;
+    const int lane = threadIdx.x % TEAM;
+    // G tables, once per CTA
+    __shared__ T sGll[25], sGlj[25];
+    for (int i = threadIdx.x; i < 25; i += blockDim.x) {
+        sGll[i] = a.gmat[i];
+        sGlj[i] = a.gmat[25 + i];
+    }
+    __syncthreads();
+    if (team >= teams_per_cta) return;
+
+    const TeamLayout L = team_layout<T>(nr_max, qc_max);
+    unsigned char *base = smem_raw + (size_t)team * team_bytes;
+    T *sGeo = reinterpret_cast<T *>(base + L.geom);
+    T *sTrig = reinterpret_cast<T *>(base + L.trig);
+    int *sPt = reinterpret_cast<int *>(base + L.ipt);
+    int *sOff = sPt + 25;
+    int *sNu = sPt + 50;
+    T *sTw = reinterpret_cast<T *>(base + L.tw);
+    C *rA = reinterpret_cast<C *>(base + L.regA);
+    C *rBc = reinterpret_cast<C *>(base + L.regB);
+    T *rBr = reinterpret_cast<T *>(base + L.regB);
+
+    // geometry aliases
+    const T *dsdxii = sGeo, *dsdeta = sGeo + 25, *dzdxii = sGeo + 50, *dzdeta = sGeo + 75,
+            *invs = sGeo + 100;
+    const T *dsdxii_if = sGeo + 125, *dsdeta_if = sGeo + 150, *dzdxii_if = sGeo + 175,
+            *dzdeta_if = sGeo + 200, *invs_if = sGeo + 225;
+
+    for (int e = blockIdx.x * teams_per_cta + team; e < a.n_elem; e += gridDim.x * teams_per_cta) {
+        const int nr = a.nr[e];
+        const int nu = nr / 2 + 1;
+        const bool axial = a.axial[e] != 0;
+        const T *Gxi = axial ? sGlj : sGll;
+
+        // ---------------- element header -> shared memory ----------------
+        for (int i = lane; i < 250; i += TEAM) sGeo[i] = a.geom[(size_t)e * 250 + i];
+        if constexpr (RTZ)
+            for (int i = lane; i < 100; i += TEAM) sTrig[i] = a.trig[(size_t)e * 100 + i];
+        for (int i = lane; i < 25; i += TEAM) {
+            int p = a.pts[(size_t)e * 25 + i];
+            sPt[i] = p;
+            sOff[i] = a.pt_off[p];
+            sNu[i] = a.pt_nu[p];
+        }
+        if constexpr (IS3D) {
+            const T *tw = a.tw + a.tw_off[nr];
+            for (int i = lane; i < 2 * nr; i += TEAM) sTw[i] = tw[i];
+        }
+        team_sync(team, TEAM);
+
+        // ---------------- gather displacement: U[a][c][q] in region B ----------------
+        for (int i = lane; i < nu * 25; i += TEAM) {
+            const int q = i / nu, al = i - q * nu;
+            C u0 = mk<T>(0, 0), u1 = u0, u2 = u0;
+            if (al < sNu[q]) {
+                const C *src = a.displ + (size_t)(sOff[q] + al) * 3;
+                u0 = src[0]; u1 = src[1]; u2 = src[2];
+            }
+            rBc[(al * 3 + 0) * 25 + q] = u0;
+            rBc[(al * 3 + 1) * 25 + q] = u1;
+            rBc[(al * 3 + 2) * 25 + q] = u2;
+        }
+        team_sync(team, TEAM);
+
+        // ---------------- gradient (computeGrad6) ----------------
+        const int64_t moff = a.mod_off[e];
+        const int nslice = IS3D ? nr : 1;
+        for (int i = lane; i < nu * 25; i += TEAM) {
+            const int al = i / 25, q = i - al * 25;
+            const int ii = q / 5, jj = q - ii * 5;
+            const C *U = rBc + al * 75;
+            C X[3], Y[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                C x = mk<T>(0, 0), y = mk<T>(0, 0);
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    const T gx = Gxi[k * 5 + ii];        // GT_xi(ii, k)
+                    const T gy = sGll[k * 5 + jj];       // G_GLL(k, jj)
+                    const C uc = U[c * 25 + k * 5 + jj];
+                    const C ur = U[c * 25 + ii * 5 + k];
+                    x.x += gx * uc.x; x.y += gx * uc.y;
+                    y.x += ur.x * gy; y.y += ur.y * gy;
+                }
+                X[c] = x; Y[c] = y;
+            }
+            const T ze = dzdeta[q], zx = dzdxii[q], se = dsdeta[q], sx = dsdxii[q];
+            C eps[6];
+            // dS/dZ of u0 -> e0, e4 ; u1 -> e5, e3 ; u2 -> e1, e2
+            eps[0] = cadd(cscale(X[0], ze), cscale(Y[0], zx));
+            eps[4] = cadd(cscale(X[0], se), cscale(Y[0], sx));
+            eps[5] = cadd(cscale(X[1], ze), cscale(Y[1], zx));
+            eps[3] = cadd(cscale(X[1], se), cscale(Y[1], sx));
+            C e1t = cadd(cscale(X[2], ze), cscale(Y[2], zx));
+            eps[2] = cadd(cscale(X[2], se), cscale(Y[2], sx));
+            eps[4] = cadd(eps[4], e1t);
+            // lower-order terms A/s
+            const T alf = (T)al;
+            const C u0 = U[q], u1 = U[25 + q], u2 = U[50 + q];
+            const C A0 = csub(cia(alf, u0), u1);
+            const C A1 = cadd(cia(alf, u1), u0);
+            const C A2 = cia(alf, u2);
+            const T is = invs[q];
+            eps[5] = cadd(eps[5], cscale(A0, is));
+            eps[1] = cscale(A1, is);
+            eps[3] = cadd(eps[3], cscale(A2, is));
+            if (axial && ii == 0) {
+                // L'Hopital on the axis: row 0 of A/s replaced by dA/ds
+                C ax[3], ay[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) { ax[c] = mk<T>(0, 0); ay[c] = mk<T>(0, 0); }
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    const T gx = Gxi[k * 5 + 0];
+                    const T gy = sGll[k * 5 + jj];
+                    const C v0 = U[k * 5 + jj], v1 = U[25 + k * 5 + jj], v2 = U[50 + k * 5 + jj];
+                    const C w0 = U[k], w1 = U[25 + k], w2 = U[50 + k];
+                    C a0 = csub(cia(alf, v0), v1), a1 = cadd(cia(alf, v1), v0), a2 = cia(alf, v2);
+                    C b0 = csub(cia(alf, w0), w1), b1 = cadd(cia(alf, w1), w0), b2 = cia(alf, w2);
+                    ax[0] = cadd(ax[0], cscale(a0, gx)); ax[1] = cadd(ax[1], cscale(a1, gx));
+                    ax[2] = cadd(ax[2], cscale(a2, gx));
+                    ay[0] = cadd(ay[0], cscale(b0, gy)); ay[1] = cadd(ay[1], cscale(b1, gy));
+                    ay[2] = cadd(ay[2], cscale(b2, gy));
+                }
+                eps[5] = cadd(eps[5], cadd(cscale(ax[0], ze), cscale(ay[0], zx)));
+                eps[1] = cadd(cscale(ax[1], ze), cscale(ay[1], zx));
+                eps[3] = cadd(eps[3], cadd(cscale(ax[2], ze), cscale(ay[2], zx)));
+            }
+            if constexpr (RTZ) {
+                spz_to_rtz6(eps, sTrig[q], sTrig[25 + q], sTrig[50 + q], sTrig[75 + q]);
+            }
+            if constexpr (!IS3D) {
+                // strainToStress_FR with 1-D moduli
+                C sig[6];
+                elastic_at<RHEO>(a.mod + moff, 1, 0, q, eps, sig);
+                if constexpr (ATT == ATT_FULL) {
+                    const int64_t ao = a.att_off[e];
+                    AT *st = a.state + a.state_off[e];
+                    attenuate<T, AT, true>(a, st, (size_t)nu * 25, (size_t)al * 25 + q, eps, sig,
+                                           a.attmod[ao + q], a.attmod[ao + 25 + q]);
+                } else if constexpr (ATT == ATT_CG4) {
+                    const int k4 = cg4_slot(q);
+                    if (k4 >= 0) {
+                        const int64_t ao = a.att_off[e];
+                        AT *st = a.state + a.state_off[e];
+                        attenuate<T, AT, true>(a, st, (size_t)nu * 4, (size_t)al * 4 + k4, eps, sig,
+                                               a.attmod[ao + k4], a.attmod[ao + 4 + k4]);
+                    }
+                }
+                if constexpr (RTZ) {
+                    rtz_to_spz6(sig, sTrig[q], sTrig[25 + q], sTrig[50 + q], sTrig[75 + q]);
+                }
+#pragma unroll
+                for (int d = 0; d < 6; d++) rA[(al * 6 + d) * 25 + q] = sig[d];
+            } else {
+#pragma unroll
+                for (int d = 0; d < 6; d++) rA[(al * 6 + d) * 25 + q] = eps[d];
+            }
+        }
+        team_sync(team, TEAM);
+
+        // ---------------- 3-D material: slices ----------------
+        if constexpr (IS3D) {
+            const T *twc = sTw, *tws = sTw + nr;
+            const T inv_nr = (T)1 / (T)nr;
+            const int nkb = (nr + KB - 1) / KB;
+            const int nab = (nu + AB - 1) / AB;
+            for (int q0 = 0; q0 < 25; q0 += qc_max) {
+                const int qcnt = min(qc_max, 25 - q0);
+                // Fourier -> slices (computeC2R), stress, attenuation -> rBr[k][d][qq]
+                for (int i = lane; i < nkb * qcnt; i += TEAM) {
+                    const int kb = i / qcnt, qq = i - kb * qcnt, q = q0 + qq;
+                    const int k0 = kb * KB;
+                    T acc[KB][6];
+                    int j[KB];
+#pragma unroll
+                    for (int d = 0; d < 6; d++) {
+                        const T r0 = rA[d * 25 + q].x;
+#pragma unroll
+                        for (int kk = 0; kk < KB; kk++) acc[kk][d] = r0;
+                    }
+                    int kstep[KB];
+#pragma unroll
+                    for (int kk = 0; kk < KB; kk++) {
+                        j[kk] = 0;
+                        kstep[kk] = (k0 + kk < nr) ? k0 + kk : 0;
+                    }
+                    for (int al = 1; al < nu; al++) {
+                        C ev[6];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) ev[d] = rA[(al * 6 + d) * 25 + q];
+#pragma unroll
+                        for (int kk = 0; kk < KB; kk++) {
+                            j[kk] += kstep[kk];
+                            j[kk] = j[kk] >= nr ? j[kk] - nr : j[kk];
+                            const T c = twc[j[kk]], s = tws[j[kk]];
+#pragma unroll
+                            for (int d = 0; d < 6; d++)
+                                acc[kk][d] += (T)2 * (ev[d].x * c - ev[d].y * s);
+                        }
+                    }
+#pragma unroll
+                    for (int kk = 0; kk < KB; kk++) {
+                        const int k = k0 + kk;
+                        if (k >= nr) break;
+                        re1<T> ev[6], sg[6];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) ev[d].x = acc[kk][d];
+                        elastic_at<RHEO>(a.mod + moff, nslice, k, q, ev, sg);
+                        if constexpr (ATT == ATT_FULL) {
+                            const int64_t ao = a.att_off[e];
+                            AT *st = a.state + a.state_off[e];
+                            const size_t ns = (size_t)nr * 25;
+                            attenuate<T, AT, false>(a, st, ns, (size_t)k * 25 + q, ev, sg,
+                                                    a.attmod[ao + (size_t)k * 25 + q],
+                                                    a.attmod[ao + ns + (size_t)k * 25 + q]);
+                        } else if constexpr (ATT == ATT_CG4) {
+                            const int k4 = cg4_slot(q);
+                            if (k4 >= 0) {
+                                const int64_t ao = a.att_off[e];
+                                AT *st = a.state + a.state_off[e];
+                                const size_t ns = (size_t)nr * 4;
+                                attenuate<T, AT, false>(a, st, ns, (size_t)k * 4 + k4, ev, sg,
+                                                        a.attmod[ao + (size_t)k * 4 + k4],
+                                                        a.attmod[ao + ns + (size_t)k * 4 + k4]);
+                            }
+                        }
+#pragma unroll
+                        for (int d = 0; d < 6; d++) rBr[((size_t)k * 6 + d) * qcnt + qq] = sg[d].x;
+                    }
+                }
+                team_sync(team, TEAM);
+                // slices -> Fourier (computeR2C) into region A for these points
+                for (int i = lane; i < nab * qcnt; i += TEAM) {
+                    const int ab = i / qcnt, qq = i - ab * qcnt, q = q0 + qq;
+                    const int a0 = ab * AB;
+                    T re[AB][6], im[AB][6];
+                    int j[AB], astep[AB];
+#pragma unroll
+                    for (int aa = 0; aa < AB; aa++) {
+                        j[aa] = 0;
+                        astep[aa] = (a0 + aa) % nr;
+#pragma unroll
+                        for (int d = 0; d < 6; d++) { re[aa][d] = 0; im[aa][d] = 0; }
+                    }
+                    for (int k = 0; k < nr; k++) {
+                        T x[6];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) x[d] = rBr[((size_t)k * 6 + d) * qcnt + qq] * inv_nr;
+#pragma unroll
+                        for (int aa = 0; aa < AB; aa++) {
+                            const T c = twc[j[aa]], s = tws[j[aa]];
+#pragma unroll
+                            for (int d = 0; d < 6; d++) {
+                                re[aa][d] += x[d] * c;
+                                im[aa][d] -= x[d] * s;
+                            }
+                            j[aa] += astep[aa];
+                            j[aa] = j[aa] >= nr ? j[aa] - nr : j[aa];
+                        }
+                    }
+#pragma unroll
+                    for (int aa = 0; aa < AB; aa++) {
+                        const int al = a0 + aa;
+                        if (al >= nu) break;
+                        C sg[6];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) {
+                            T r = re[aa][d], m = im[aa][d];
+                            if (al == 0) m = 0;
+                            if ((nr & 1) == 0 && al == nr / 2) { r *= (T)0.5; m = 0; }
+                            sg[d] = mk<T>(r, m);
+                        }
+                        if constexpr (RTZ) {
+                            rtz_to_spz6(sg, sTrig[q], sTrig[25 + q], sTrig[50 + q], sTrig[75 + q]);
+                        }
+#pragma unroll
+                        for (int d = 0; d < 6; d++) rA[(al * 6 + d) * 25 + q] = sg[d];
+                    }
+                }
+                team_sync(team, TEAM);
+            }
+        }
+
+        // ---------------- quadrature (computeQuad6), pass 1: X, Y, A ----------------
+        for (int i = lane; i < nu * 25; i += TEAM) {
+            const int al = i / 25, q = i - al * 25;
+            C s[6];
+#pragma unroll
+            for (int d = 0; d < 6; d++) s[d] = rA[(al * 6 + d) * 25 + q];
+            const T ze = dzdeta_if[q], zx = dzdxii_if[q], se = dsdeta_if[q], sx = dsdxii_if[q];
+            C *xy = rA + al * 150;
+            xy[0 * 25 + q] = cadd(cscale(s[0], ze), cscale(s[4], se));
+            xy[1 * 25 + q] = cadd(cscale(s[0], zx), cscale(s[4], sx));
+            xy[2 * 25 + q] = cadd(cscale(s[5], ze), cscale(s[3], se));
+            xy[3 * 25 + q] = cadd(cscale(s[5], zx), cscale(s[3], sx));
+            xy[4 * 25 + q] = cadd(cscale(s[4], ze), cscale(s[2], se));
+            xy[5 * 25 + q] = cadd(cscale(s[4], zx), cscale(s[2], sx));
+            const T alf = (T)al;
+            rBc[(al * 3 + 0) * 25 + q] = csub(cia(alf, s[5]), s[1]);
+            rBc[(al * 3 + 1) * 25 + q] = cadd(cia(alf, s[1]), s[5]);
+            rBc[(al * 3 + 2) * 25 + q] = cia(alf, s[3]);
+        }
+        team_sync(team, TEAM);
+
+        // ---------------- quadrature pass 2 + scatter-add ----------------
+        for (int i = lane; i < nu * 25; i += TEAM) {
+            const int al = i / 25, q = i - al * 25;
+            const int ii = q / 5, jj = q - ii * 5;
+            const C *xy = rA + al * 150;
+            const C *A = rBc + al * 75;
+            C f[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                C g1 = mk<T>(0, 0), g2 = mk<T>(0, 0);
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    const T gx = Gxi[ii * 5 + k];      // G_xi(ii, k)
+                    const T gt = sGll[jj * 5 + k];     // GT_GLL(k, jj) = G_GLL(jj, k)
+                    const C xv = xy[(2 * c) * 25 + k * 5 + jj];
+                    const C yv = xy[(2 * c + 1) * 25 + ii * 5 + k];
+                    g1.x += gx * xv.x; g1.y += gx * xv.y;
+                    g2.x += yv.x * gt; g2.y += yv.y * gt;
+                }
+                C fc = cadd(g1, g2);
+                fc = csub(fc, cscale(A[c * 25 + q], invs_if[q]));
+                if (axial) {
+                    const T g0 = Gxi[ii * 5 + 0];
+                    fc = csub(fc, cscale(cscale(A[c * 25 + jj], dzdeta_if[jj]), g0));
+                    if (ii == 0) {
+                        C b = mk<T>(0, 0);
+#pragma unroll
+                        for (int k = 0; k < 5; k++) {
+                            const C y0 = cscale(A[c * 25 + k], dzdxii_if[k]);
+                            const T gt = sGll[jj * 5 + k];
+                            b.x += y0.x * gt; b.y += y0.y * gt;
+                        }
+                        fc = csub(fc, b);
+                    }
+                }
+                f[c] = fc;
+            }
+            if (al < sNu[q]) {
+                C *dst = a.stiff + (size_t)(sOff[q] + al) * 3;
+#pragma unroll
+                for (int c = 0; c < 3; c++) atomic_add_cx(dst + c, mk<T>(-f[c].x, -f[c].y));
+            }
+        }
+        team_sync(team, TEAM);
+    }
+}
+
+}  // namespace axg

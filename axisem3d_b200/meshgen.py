@@ -1,0 +1,503 @@
+"""Seeded synthetic meshes and models for the benchmark and parity workloads.
+
+The reference reads Exodus meshes written by its Python mesher and builds
+operands in its preloop; this module plays that role for synthetic inputs. It
+lays out structured quad meshes, calls the engine's host operand builders
+(``axg_quad_geometry_batch``, ``axg_quad_dt``, ``axg_att_*`` -- the
+restatements of Quad::createGradient, Quad::computeDt and AttBuilder) and
+applies the material formulas of Material::createIsotropic / createTISO /
+createAnisotropic (SOLVER/src/preloop/se_model/quad/physical/Material.cpp:385-609).
+All randomness comes from numpy PCG64 generators with the seeds given.
+
+Workloads (sizes in SI units):
+  cartesian_model   plain forward case: 40 x 40 quads on 100 km x 100 km with the
+                    axis at s = 0, nr = 5, homogeneous isotropic medium, moment
+                    tensor on the axis at 10 km depth, Ricker 1 Hz, 20 surface
+                    receivers, dt from Courant 0.6.
+  microbench_model  stiffness microbenchmark: ~200k non-axial solid quads, nr per
+                    element log-uniform on [1, 64], transversely isotropic moduli at
+                    +-10 % around vp = 8, vs = 4.5 km/s, rho = 3.3 g/cc per
+                    (element, slice, point), 3 SLS with Q_mu uniform in [80, 600].
+  spherical_model   spherical-shell analogue: annulus 3480-6371 km with a fluid
+                    layer 3480-3600 km, 1-D layered background, 2 % Gaussian
+                    random-field dlnVs setting per-element nr, Q = 300.
+"""
+import math
+
+import numpy as np
+
+from . import _lib as L
+from .model import Model, STF
+from .solver import att_alpha_beta_gamma, att_moduli, quad_dt
+
+# GLL / GLJ tables (nPol = 4)
+_TAB = None
+
+
+def tables():
+    global _TAB
+    if _TAB is None:
+        from .solver import spectral_tables
+        _TAB = spectral_tables()
+    return _TAB
+
+
+def lagrange(nodes, x):
+    """Lagrange basis values l_j(x) on the given nodes (SE_Model::computeInplaneFactor)."""
+    n = len(nodes)
+    w = np.ones(n)
+    for j in range(n):
+        for k in range(n):
+            if k != j:
+                w[j] *= (x - nodes[k]) / (nodes[j] - nodes[k])
+    return w
+
+
+def inplane_weights(xi, eta, axial):
+    t = tables()
+    wx = lagrange(t["pGLJ"] if axial else t["pGLL"], xi)
+    we = lagrange(t["pGLL"], eta)
+    return np.outer(wx, we).ravel()
+
+
+def round_dt(dt):
+    """SE_Model::computeDt: round to 4 significant figures ("%.3e")."""
+    return float("%.3e" % dt)
+
+
+# ------------------------------------------------------------------ geometry ---
+def geometry_batch(nodal, axial, mapping=L.AXG_MAP_LINEAR):
+    """Quad::createGradient for all quads: (ne, 6, 25) operands and (ne, 2, 25) s, z."""
+    lib = L.lib()
+    ne = len(axial)
+    nodal = np.ascontiguousarray(nodal, dtype=np.float64).reshape(ne, 8)
+    ax = np.ascontiguousarray(axial, dtype=np.uint8)
+    g = np.zeros((ne, 6, 25))
+    sz = np.zeros((ne, 2, 25))
+    rc = lib.axg_quad_geometry_batch(ne, int(mapping), nodal.ctypes.data_as(L.P_f64),
+                                     ax.ctypes.data_as(L.P_u8), g.ctypes.data_as(L.P_f64),
+                                     sz.ctypes.data_as(L.P_f64))
+    if rc != L.AXG_OK:
+        raise RuntimeError("axg_quad_geometry_batch failed (%d)" % rc)
+    return g, sz
+
+
+def structured_points(nx, nz):
+    """Element -> GLL point map of an nx x nz structured quad grid (I = 4i + ipol, J = 4j + jpol)."""
+    nJ = 4 * nz + 1
+    i = np.arange(nx)[:, None, None, None]
+    j = np.arange(nz)[None, :, None, None]
+    ip = np.arange(5)[None, None, :, None]
+    jp = np.arange(5)[None, None, None, :]
+    pts = (4 * i + ip) * nJ + (4 * j + jp)
+    return pts.reshape(nx * nz, 25).astype(np.int32), (4 * nx + 1) * nJ
+
+
+def assemble_mass(pts, ifact, density, npoints):
+    """Material::getMass: mass[ipnt] = density * integral factor, summed over elements."""
+    m = np.zeros(npoints)
+    np.add.at(m, pts.ravel(), (density * ifact).ravel())
+    return m
+
+
+# ------------------------------------------------------------------ materials ---
+def isotropic_moduli(rho, vp, vs):
+    """Material::createIsotropic without attenuation: lambda = rho vp^2 - 2 mu, mu = rho vs^2."""
+    mu = rho * vs ** 2
+    lam = rho * vp ** 2 - 2.0 * mu
+    return lam, mu
+
+
+def tiso_with_attenuation(A, C, F, Lm, N, qkappa, qmu, sls):
+    """Material::createTISO with attenuation (Material.cpp:497-560) -> unrelaxed A, C, F, L, N,
+    dlambda, dmu (AttBuilder::createAttenuation, FULL)."""
+    kp = (A * 4. + C + F * 4. - N * 4.) / 9.
+    mu = (A + C - F * 2. + Lm * 6. + N * 5.) / 15.
+    A = A - (kp + 4. / 3. * mu)
+    C = C - (kp + 4. / 3. * mu)
+    F = F - (kp - 2. / 3. * mu)
+    Lm = Lm - mu
+    N = N - mu
+    kp2, mu2, dkp, dmu = att_moduli(sls["w"], sls["y"], sls["fmin"], sls["fmax"], sls["fref"],
+                                    qkappa, qmu, kp, mu)
+    A = A + (kp2 + 4. / 3. * mu2)
+    C = C + (kp2 + 4. / 3. * mu2)
+    F = F + (kp2 - 2. / 3. * mu2)
+    Lm = Lm + mu2
+    N = N + mu2
+    dlam = dkp - (2. / 3.) * dmu
+    return A, C, F, Lm, N, dlam, dmu
+
+
+def iso_with_attenuation(lam, mu, qkappa, qmu, sls):
+    """Material::createIsotropic with attenuation (Material.cpp:563-609)."""
+    kp = lam + (2. / 3.) * mu
+    kp2, mu2, dkp, dmu = att_moduli(sls["w"], sls["y"], sls["fmin"], sls["fmax"], sls["fref"],
+                                    qkappa, qmu, kp, mu)
+    lam2 = kp2 - (2. / 3.) * mu2
+    return lam2, mu2, dkp - (2. / 3.) * dmu, dmu
+
+
+def att_factors(q, sls):
+    """AttBuilder::createAttenuation factors for one quality factor array
+    (AttBuilder.cpp:106-124): (NA, d, AT) with modulus_unrelaxed = modulus * AT
+    (FULL) and dmodulus = d * modulus."""
+    w, y = np.asarray(sls["w"]), np.asarray(sls["y"])
+    ysum = y.sum()
+    w0 = sls["fref"] * (2 * np.pi)
+    w1 = math.sqrt(sls["fmin"] * sls["fmax"]) * (2. * np.pi)
+    w10f = 2. * math.log(w1 / w0) / np.pi
+    fact = float(np.sum(y * w ** 2 / (w ** 2 + w1 * w1)) / ysum)
+    q = np.asarray(q, dtype=np.float64)
+    na = 1. + w10f / q
+    d = na / (q / ysum + (1. - fact))
+    return na, d, na + d * fact
+
+
+CG4_POINTS = np.array([6, 8, 16, 18])
+
+
+def weights_cg4(ifact):
+    """Quad::computeWeightsCG4 (Quad.cpp:487-511) from the (.., 25) integral factor."""
+    f = np.asarray(ifact).reshape(-1, 5, 5)
+    w = np.zeros((f.shape[0], 4))
+    w[:, 0] = (f[:, 0, 0] + f[:, 0, 1] + f[:, 1, 0] + f[:, 1, 1] +
+               0.50 * (f[:, 0, 2] + f[:, 1, 2] + f[:, 2, 0] + f[:, 2, 1]) + 0.25 * f[:, 2, 2]) / f[:, 1, 1]
+    w[:, 1] = (f[:, 0, 3] + f[:, 0, 4] + f[:, 1, 3] + f[:, 1, 4] +
+               0.50 * (f[:, 0, 2] + f[:, 1, 2] + f[:, 2, 3] + f[:, 2, 4]) + 0.25 * f[:, 2, 2]) / f[:, 1, 3]
+    w[:, 2] = (f[:, 3, 0] + f[:, 3, 1] + f[:, 4, 0] + f[:, 4, 1] +
+               0.50 * (f[:, 2, 0] + f[:, 2, 1] + f[:, 3, 2] + f[:, 4, 2]) + 0.25 * f[:, 2, 2]) / f[:, 3, 1]
+    w[:, 3] = (f[:, 3, 3] + f[:, 3, 4] + f[:, 4, 3] + f[:, 4, 4] +
+               0.50 * (f[:, 2, 3] + f[:, 2, 4] + f[:, 3, 2] + f[:, 4, 2]) + 0.25 * f[:, 2, 2]) / f[:, 3, 3]
+    return w
+
+
+def cg4_correct(kp, mu, qkappa, qmu, wcg4, sls):
+    """AttBuilder::createAttenuation, CG4 branch (AttBuilder.cpp:140-166), on arrays of
+    shape (ne, nslice, 25): returns unrelaxed kp, mu and (ne, nslice, 4) dkappa4, dmu4
+    already weighted by the CG4 weights."""
+    kna, kd, kat = att_factors(np.broadcast_to(qkappa, kp.shape), sls)
+    mna, md, mat = att_factors(np.broadcast_to(qmu, mu.shape), sls)
+    dkp, dmu = kd * kp, md * mu
+    dlm = dkp - (2. / 3.) * dmu
+    w = wcg4[:, None, :]
+    dlm4 = w * dlm[:, :, CG4_POINTS]
+    dmu4 = w * dmu[:, :, CG4_POINTS]
+    kp2, mu2 = kp * kna, mu * mna
+    kp2[:, :, CG4_POINTS] *= 1. + w * (kat[:, :, CG4_POINTS] / kna[:, :, CG4_POINTS] - 1.)
+    mu2[:, :, CG4_POINTS] *= 1. + w * (mat[:, :, CG4_POINTS] / mna[:, :, CG4_POINTS] - 1.)
+    return kp2, mu2, dlm4, dmu4
+
+
+def default_sls(nsls=3, fmin=0.05, fmax=1.0):
+    """SLS relaxation frequencies and weights as the mesher's attenuation_w_i / y_i."""
+    w = 2 * np.pi * np.logspace(np.log10(fmin), np.log10(fmax), nsls)
+    y = np.array([1.69, 1.12, 1.43, 1.2, 1.3, 1.1, 1.0, 1.0][:nsls])
+    return {"w": w, "y": y, "fmin": fmin, "fmax": fmax, "fref": fmax}
+
+
+# ------------------------------------------------------------------- sources ---
+def moment_pattern_axial(mt, weights, nu_elem, axial_quad=True):
+    """Mechanism::release, moment tensor on the axis (Mechanism.cpp:131-222).
+
+    mt = (Mrr, Mtt, Mpp, Mrt, Mrp, Mtp) in the source frame; for an axial source
+    Qzsp is the identity (Source::computeQzsp). Returns (nu, 6, 25) complex."""
+    m = np.zeros((3, 3))
+    m[0, 0], m[1, 1], m[2, 2] = mt[0], mt[1], mt[2]
+    m[0, 1] = m[1, 0] = mt[3]
+    m[0, 2] = m[2, 0] = mt[4]
+    m[1, 2] = m[2, 1] = mt[5]
+    mss, mpp, mzz = m[1, 1] * weights, m[2, 2] * weights, m[0, 0] * weights
+    mpz, msz, msp = m[0, 2] * weights, m[0, 1] * weights, m[1, 2] * weights
+    nu = min(nu_elem, 3)
+    pat = np.zeros((nu, 6, 25), dtype=np.complex128)
+    if axial_quad:
+        ax = slice(0, 5)
+        pat[0, 0, ax] = pat[0, 1, ax] = (mss[ax] + mpp[ax]) / 2.
+        pat[0, 2, ax] = mzz[ax]
+        if nu >= 2:
+            pat[1, 4, ax] = (msz[ax] - 1j * mpz[ax]) / 2.
+            pat[1, 3, ax] = 1j * pat[1, 4, ax]
+        if nu >= 3:
+            pat[2, 0, ax] = (mss[ax] - mpp[ax] - 2. * 1j * msp[ax]) / 4.
+            pat[2, 1, ax] = -pat[2, 0, ax]
+            pat[2, 5, ax] = 1j * pat[2, 0, ax]
+        pat /= (2. * np.pi)
+    return pat
+
+
+def moment_pattern_offaxis(mt, weights, nu_elem, phi=0.0):
+    """Mechanism::release, moment tensor off the axis in a non-axial quad (Qzsp = I)."""
+    m = np.zeros((3, 3))
+    m[0, 0], m[1, 1], m[2, 2] = mt[0], mt[1], mt[2]
+    m[0, 1] = m[1, 0] = mt[3]
+    m[0, 2] = m[2, 0] = mt[4]
+    m[1, 2] = m[2, 1] = mt[5]
+    comps = [m[1, 1], m[2, 2], m[0, 0], m[0, 2], m[0, 1], m[1, 2]]
+    pat = np.zeros((nu_elem, 6, 25), dtype=np.complex128)
+    for a in range(nu_elem):
+        e = np.exp(1. * a * (-1j * phi))
+        for d in range(6):
+            pat[a, d] = e * comps[d] * weights
+    return pat
+
+
+# ------------------------------------------------------------- plain forward ---
+def cartesian_model(nx=40, nz=40, width=100e3, height=100e3, nr=5, rho=2700.0, vp=5800.0,
+                    vs=3460.0, source_depth=10e3, f0=1.0, nstations=20, courant=0.6, seed=0,
+                    moment_scale=1e18, attenuation=None, record_interval=1):
+    """Plain forward case (the reference's CPU-runnable configuration)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    h_s, h_z = width / nx, height / nz
+    ne = nx * nz
+    i = np.repeat(np.arange(nx), nz)
+    j = np.tile(np.arange(nz), nx)
+    s0, s1 = i * h_s, (i + 1) * h_s
+    z0, z1 = -height + j * h_z, -height + (j + 1) * h_z
+    nodal = np.stack([s0, z0, s1, z0, s1, z1, s0, z1], axis=1)
+    axial = (i == 0).astype(np.uint8)
+    geom, sz = geometry_batch(nodal, axial)
+    pts, npts = structured_points(nx, nz)
+    lam, mu = isotropic_moduli(rho, vp, vs)
+    se_moduli = np.zeros((ne, 2, 25))
+    se_moduli[:, 0, :] = lam
+    se_moduli[:, 1, :] = mu
+    mass = assemble_mass(pts, geom[:, 5, :], rho, npts)
+    coords = np.zeros((npts, 2))
+    coords[pts.ravel(), 0] = sz[:, 0, :].ravel()
+    coords[pts.ravel(), 1] = sz[:, 1, :].ravel()
+    sp_axial = (np.abs(coords[:, 0]) < 1e-9 * width).astype(np.uint8)
+    dt_e = min(quad_dt(sz[e], vp) for e in range(ne))
+    dt = round_dt(dt_e * courant)
+    m = Model(dt=dt)
+    m.sp_nr = np.full(npts, nr, np.int32)
+    m.sp_mass = mass
+    m.sp_axial = sp_axial
+    m.sp_coords = coords
+    m.se_nr = np.full(ne, nr, np.int32)
+    m.se_pts = pts
+    m.se_axial = axial
+    m.se_geom = geom
+    m.se_rheo = np.full(ne, L.AXG_ISO, np.int32)
+    m.se_is3d = np.zeros(ne, np.uint8)
+    m.se_mat_off = np.arange(ne, dtype=np.int64) * 50
+    m.se_moduli = se_moduli.ravel()
+    if attenuation:
+        sls = attenuation
+        lam2, mu2, dl, dm = iso_with_attenuation(np.full((ne, 25), lam), np.full((ne, 25), mu),
+                                                 sls["qkappa"], sls["qmu"], sls)
+        se_moduli[:, 0, :], se_moduli[:, 1, :] = lam2, mu2
+        m.se_moduli = se_moduli.ravel()
+        m.se_att = np.full(ne, L.AXG_ATT_FULL, np.int32)
+        am = np.stack([dl, dm], axis=1)
+        m.se_att_off = np.arange(ne, dtype=np.int64) * 50
+        m.se_att_moduli = am.ravel()
+        a, b, g = att_alpha_beta_gamma(sls["w"], sls["y"], dt)
+        m.nsls, m.att_alpha, m.att_beta, m.att_gamma = len(a), a, b, g
+    # moment tensor on the axis at the given depth (Source::release)
+    mt = rng.normal(0.0, moment_scale, 6)
+    zsrc = -source_depth
+    jsrc = int(min(nz - 1, max(0, math.floor((zsrc + height) / h_z - 1e-9))))
+    esrc = 0 * nz + jsrc
+    eta = 2.0 * (zsrc - z0[esrc]) / h_z - 1.0
+    w = inplane_weights(-1.0, eta, True)
+    pat = moment_pattern_axial(mt, w, nr // 2 + 1, True)
+    hd = 1.0
+    m.ms_elem = np.array([esrc], np.int32)
+    m.ms_nu = np.array([pat.shape[0]], np.int32)
+    m.ms_pat_off = np.array([0], np.int64)
+    m.ms_pattern = pat.ravel()
+    m.ms_stf = [STF(half_duration=hd, decay_factor=math.pi * f0 * hd, time_shift=0.0, derivative_order=2)]
+    m.t0 = -2.5 * hd
+    # receivers on the surface (z = 0), one azimuth
+    st_e, st_w = [], []
+    for k in range(1, nstations + 1):
+        s = width * k / nstations
+        ic = min(nx - 1, int(math.floor(s / h_s - 1e-9)))
+        e = ic * nz + (nz - 1)
+        xi = 2.0 * (s - s0[e]) / h_s - 1.0
+        st_e.append(e)
+        st_w.append(inplane_weights(xi, 1.0, bool(axial[e])))
+    m.st_elem = np.array(st_e, np.int32)
+    m.st_w = np.array(st_w)
+    m.st_phi = np.zeros(nstations)
+    m.st_interval = record_interval
+    m.meta = {"workload": "cartesian %dx%d nr=%d" % (nx, nz, nr), "moment": mt.tolist(), "seed": seed}
+    return m
+
+
+# ---------------------------------------------------------- microbenchmark ---
+def microbench_model(n_elem=200000, nr_max=64, seed=1, rheology="tiso", attenuation="full",
+                     is3d=True, nsls=3, aspect=1.25, s_offset=1.0e6, h=2.0e3, axial_column=False,
+                     nr_min=1):
+    """Stiffness microbenchmark: non-axial structured quads with perturbed nodes,
+    per-element nr log-uniform on [1, nr_max] (points take the minimum over their
+    elements, so each element's nr is the maximum over its points)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nz = max(1, int(round(math.sqrt(n_elem / aspect))))
+    nx = max(1, int(math.ceil(n_elem / nz)))
+    ne = nx * nz
+    # perturbed node grid
+    gs = np.arange(nx + 1) * h + s_offset
+    gz = np.arange(nz + 1) * h - nz * h
+    S, Z = np.meshgrid(gs, gz, indexing="ij")
+    if axial_column:
+        gs = gs - s_offset
+        S, Z = np.meshgrid(gs, gz, indexing="ij")
+    dS = rng.uniform(-0.1, 0.1, S.shape) * h
+    if axial_column:
+        dS[0, :] = 0.0
+    S = S + dS
+    Z = Z + rng.uniform(-0.1, 0.1, Z.shape) * h
+    i = np.repeat(np.arange(nx), nz)
+    j = np.tile(np.arange(nz), nx)
+    nodal = np.stack([S[i, j], Z[i, j], S[i + 1, j], Z[i + 1, j], S[i + 1, j + 1], Z[i + 1, j + 1],
+                      S[i, j + 1], Z[i, j + 1]], axis=1)
+    axial = ((i == 0) & axial_column).astype(np.uint8)
+    geom, sz = geometry_batch(nodal, axial)
+    pts, npts = structured_points(nx, nz)
+    # nr: log-uniform per element; points take the minimum over their elements
+    enr = np.clip(np.rint(np.exp(rng.uniform(math.log(nr_min), math.log(nr_max), ne))),
+                  nr_min, nr_max).astype(np.int32)
+    pnr = np.full(npts, nr_max + 1, np.int32)
+    np.minimum.at(pnr, pts.ravel(), np.repeat(enr, 25))
+    enr = np.max(pnr[pts], axis=1).astype(np.int32)
+    rho, vp, vs = 3300.0, 8000.0, 4500.0
+    nsl = enr if is3d else np.ones(ne, np.int32)
+    m = Model(dt=1.0)
+    sls = default_sls(nsls)
+    if rheology == "tiso":
+        nmod = 5
+    elif rheology == "iso":
+        nmod = 2
+    else:
+        nmod = 21
+    mat_off = np.zeros(ne, np.int64)
+    att_off = np.zeros(ne, np.int64)
+    sizes = nmod * nsl * 25
+    mat_off[1:] = np.cumsum(sizes)[:-1]
+    moduli = np.empty(int(np.sum(sizes)))
+    npa = 4 if attenuation == "cg4" else 25
+    att_mod = np.empty(int(np.sum(2 * nsl * npa))) if attenuation else None
+    if attenuation:
+        att_off[1:] = np.cumsum(2 * nsl * npa)[:-1]
+    qmu = rng.uniform(80.0, 600.0, ne)
+    A0, C0, L0 = rho * vp ** 2, rho * vp ** 2, rho * vs ** 2
+    F0, N0 = A0 - 2 * L0, L0
+    lam0, mu0 = isotropic_moduli(rho, vp, vs)
+    tot = int(np.sum(nsl)) * 25
+    # per (element, slice, point) perturbations, drawn in one batch
+    elem_of = np.repeat(np.arange(ne), nsl * 25)
+    if attenuation == "cg4":
+        if not np.all(nsl == nsl[0]):
+            raise ValueError("the CG4 workload uses one nr for all elements")
+        wcg4 = weights_cg4(geom[:, 5, :])
+    if rheology == "tiso":
+        pert = 1.0 + rng.uniform(-0.1, 0.1, (5, tot))
+        A, C, F, Lm, N = A0 * pert[0], C0 * pert[1], F0 * pert[2], L0 * pert[3], N0 * pert[4]
+        if attenuation == "full":
+            A, C, F, Lm, N, dl, dm = tiso_with_attenuation(A, C, F, Lm, N, 57823.0, qmu[elem_of], sls)
+        elif attenuation == "cg4":
+            shp = (ne, nsl[0], 25)
+            A, C, F, Lm, N = [x.reshape(shp) for x in (A, C, F, Lm, N)]
+            kp = (A * 4. + C + F * 4. - N * 4.) / 9.
+            mu = (A + C - F * 2. + Lm * 6. + N * 5.) / 15.
+            kp2, mu2, dl4, dm4 = cg4_correct(kp, mu, 57823.0, qmu[:, None, None], wcg4, sls)
+            A = A - (kp + 4. / 3. * mu) + (kp2 + 4. / 3. * mu2)
+            C = C - (kp + 4. / 3. * mu) + (kp2 + 4. / 3. * mu2)
+            F = F - (kp - 2. / 3. * mu) + (kp2 - 2. / 3. * mu2)
+            Lm = Lm - mu + mu2
+            N = N - mu + mu2
+            A, C, F, Lm, N = [x.ravel() for x in (A, C, F, Lm, N)]
+        mods = [A, C, F, Lm, N]
+    elif rheology == "iso":
+        pert = 1.0 + rng.uniform(-0.1, 0.1, (2, tot))
+        lam, mu = lam0 * pert[0], mu0 * pert[1]
+        if attenuation == "full":
+            lam, mu, dl, dm = iso_with_attenuation(lam, mu, 57823.0, qmu[elem_of], sls)
+        elif attenuation == "cg4":
+            shp = (ne, nsl[0], 25)
+            lam, mu = lam.reshape(shp), mu.reshape(shp)
+            kp = lam + (2. / 3.) * mu
+            kp2, mu2, dl4, dm4 = cg4_correct(kp, mu, 57823.0, qmu[:, None, None], wcg4, sls)
+            lam, mu = (kp2 - (2. / 3.) * mu2).ravel(), mu2.ravel()
+        mods = [lam, mu]
+    else:
+        mods = aniso_moduli(rho, vp, vs, tot, rng)
+        if attenuation:
+            raise ValueError("anisotropic microbenchmark is built without attenuation")
+    # scatter [element][slice][point] samples into [element][mod][slice][point]
+    start = np.zeros(ne, np.int64)
+    start[1:] = np.cumsum(nsl * 25)[:-1]
+    local = np.arange(tot) - np.repeat(start, nsl * 25)
+    for k, v in enumerate(mods):
+        moduli[mat_off[elem_of] + k * (nsl[elem_of] * 25) + local] = v
+    if attenuation == "full":
+        att_mod[att_off[elem_of] + local] = dl
+        att_mod[att_off[elem_of] + nsl[elem_of] * 25 + local] = dm
+    elif attenuation == "cg4":
+        half = nsl[0] * 4
+        for e0 in range(ne):
+            att_mod[att_off[e0]:att_off[e0] + half] = dl4[e0].ravel()
+            att_mod[att_off[e0] + half:att_off[e0] + 2 * half] = dm4[e0].ravel()
+    mass = assemble_mass(pts, geom[:, 5, :], rho, npts)
+    vmax = vp * 1.1
+    dt = round_dt(min(quad_dt(sz[e], vmax) for e in range(0, ne, max(1, ne // 2000))) * 0.6)
+    m.dt = dt
+    m.sp_nr = pnr
+    m.sp_mass = mass
+    coords = np.zeros((npts, 2))
+    coords[pts.ravel(), 0] = sz[:, 0, :].ravel()
+    coords[pts.ravel(), 1] = sz[:, 1, :].ravel()
+    m.sp_coords = coords
+    m.sp_axial = (np.abs(coords[:, 0]) < 1e-9 * h).astype(np.uint8) if axial_column else np.zeros(npts, np.uint8)
+    m.se_nr = enr
+    m.se_pts = pts
+    m.se_axial = axial
+    m.se_geom = geom
+    m.se_rheo = np.full(ne, {"iso": L.AXG_ISO, "tiso": L.AXG_TISO, "aniso": L.AXG_ANISO}[rheology], np.int32)
+    m.se_is3d = np.full(ne, 1 if is3d else 0, np.uint8)
+    m.se_mat_off = mat_off
+    m.se_moduli = moduli
+    if attenuation:
+        m.se_att = np.full(ne, L.AXG_ATT_FULL if attenuation == "full" else L.AXG_ATT_CG4, np.int32)
+        m.se_att_off = att_off
+        m.se_att_moduli = att_mod
+        a, b, g = att_alpha_beta_gamma(sls["w"], sls["y"], dt)
+        m.nsls, m.att_alpha, m.att_beta, m.att_gamma = len(a), a, b, g
+    m.meta = {"workload": "microbench %d elements nr<=%d %s %s %s" %
+              (ne, nr_max, rheology, "3D" if is3d else "1D", attenuation or "elastic"), "seed": seed}
+    return m
+
+
+def aniso_moduli(rho, vp, vs, n, rng, pert=0.05):
+    """21 Cij: isotropic background plus a symmetric perturbation of relative size `pert`,
+    kept positive definite; returns the 21 upper-triangle arrays (row-major)."""
+    lam, mu = isotropic_moduli(rho, vp, vs)
+    Ciso = np.zeros((6, 6))
+    Ciso[:3, :3] = lam
+    for k in range(3):
+        Ciso[k, k] = lam + 2 * mu
+        Ciso[3 + k, 3 + k] = mu
+    R = rng.normal(0.0, 1.0, (n, 6, 6))
+    R = 0.5 * (R + np.transpose(R, (0, 2, 1)))
+    C = Ciso[None] + pert * (lam + 2 * mu) * R / 3.0
+    iu = np.triu_indices(6)
+    return [C[:, a, b] for a, b in zip(*iu)]
+
+
+def random_displacement(model, seed=2, solid=True):
+    """Complex N(0,1)/(1+m) in mode m; mode 0 and Nyquist imaginary parts zero."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nr = np.asarray(model.sp_nr if solid else model.fp_nr)
+    nu = nr // 2 + 1
+    nd = 3 if solid else 1
+    tot = int(np.sum(nu))
+    mode = np.concatenate([np.arange(k) for k in nu]) if tot else np.zeros(0, int)
+    u = (rng.normal(size=(tot, nd)) + 1j * rng.normal(size=(tot, nd))) / (1.0 + mode)[:, None]
+    first = np.concatenate([[0], np.cumsum(nu)[:-1]]).astype(int)
+    u[first, :] = u[first, :].real
+    even = np.nonzero(nr % 2 == 0)[0]
+    last = first[even] + nu[even] - 1
+    u[last, :] = u[last, :].real
+    return u.ravel()

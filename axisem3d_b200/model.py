@@ -1,0 +1,245 @@
+"""Host-side description of one sub-mesh, in the struct-of-arrays form of the C ABI.
+
+A ``Model`` holds numpy arrays for points, elements, boundary couplings,
+sources and stations, plus the time-step constants. ``Model.c_structs()``
+builds the ctypes structs of include/axg.h that point into those arrays (the
+arrays stay owned by the Model), so the same Model feeds the engine and the
+CPU oracle.
+"""
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import ctypes as C
+import numpy as np
+
+from . import _lib as L
+
+
+def _i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _i64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int64)
+
+
+def _u8(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.uint8)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+@dataclass
+class STF:
+    """GaussianSTF parameters (GaussianSTF.hpp:35-58)."""
+    half_duration: float
+    decay_factor: float
+    time_shift: float
+    derivative_order: int = 2
+
+
+@dataclass
+class Model:
+    dt: float
+    t0: float = 0.0
+    nsls: int = 0
+    att_alpha: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    att_beta: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    att_gamma: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    # solid points
+    sp_nr: np.ndarray = None
+    sp_mass: np.ndarray = None
+    sp_mass_nr: Optional[np.ndarray] = None
+    sp_mass_off: Optional[np.ndarray] = None
+    sp_axial: Optional[np.ndarray] = None
+    sp_coords: Optional[np.ndarray] = None        # (n, 2) s, z (not used by the engine)
+    # fluid points
+    fp_nr: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    fp_mass: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    fp_mass_nr: Optional[np.ndarray] = None
+    fp_mass_off: Optional[np.ndarray] = None
+    fp_axial: Optional[np.ndarray] = None
+    fp_surface: Optional[np.ndarray] = None
+    # solid elements
+    se_nr: np.ndarray = None
+    se_pts: np.ndarray = None                     # (ne, 25)
+    se_axial: np.ndarray = None
+    se_geom: np.ndarray = None                    # (ne, 6, 25)
+    se_rheo: np.ndarray = None
+    se_is3d: Optional[np.ndarray] = None
+    se_mat_off: np.ndarray = None
+    se_moduli: np.ndarray = None
+    se_att: Optional[np.ndarray] = None
+    se_att_off: Optional[np.ndarray] = None
+    se_att_moduli: Optional[np.ndarray] = None
+    se_rtz: Optional[np.ndarray] = None
+    se_theta: Optional[np.ndarray] = None         # (ne, 25)
+    # fluid elements
+    fe_nr: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    fe_pts: np.ndarray = field(default_factory=lambda: np.zeros((0, 25), np.int32))
+    fe_axial: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint8))
+    fe_geom: np.ndarray = field(default_factory=lambda: np.zeros((0, 6, 25)))
+    fe_is3d: Optional[np.ndarray] = None
+    fe_mat_off: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    fe_moduli: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    # solid-fluid coupling
+    sf_solid: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    sf_fluid: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    sf_nsu: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    sf_nzu: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    sf_nsa: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    sf_nza: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    sf_mass_fluid: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    # moment sources
+    ms_elem: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    ms_nu: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    ms_pat_off: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    ms_pattern: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex128))
+    ms_stf: List[STF] = field(default_factory=list)
+    # force sources
+    fs_elem: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    fs_nu: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    fs_pat_off: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    fs_pattern: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex128))
+    fs_stf: List[STF] = field(default_factory=list)
+    # stations
+    st_elem: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    st_w: np.ndarray = field(default_factory=lambda: np.zeros((0, 25)))
+    st_phi: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    st_interval: int = 1
+    meta: dict = field(default_factory=dict)
+
+    # ------------------------------------------------------------ sizes ---
+    @property
+    def n_solid_elements(self):
+        return 0 if self.se_nr is None else len(self.se_nr)
+
+    @property
+    def n_fluid_elements(self):
+        return len(self.fe_nr)
+
+    def solid_field_size(self):
+        return int(np.sum(np.asarray(self.sp_nr) // 2 + 1)) * 3
+
+    def fluid_field_size(self):
+        return int(np.sum(np.asarray(self.fp_nr) // 2 + 1)) if len(self.fp_nr) else 0
+
+    def updates_per_step(self):
+        """GLL-point x mode updates of one stiffness evaluation: sum_e 25 nu_e."""
+        u = 25 * int(np.sum(np.asarray(self.se_nr) // 2 + 1))
+        if len(self.fe_nr):
+            u += 25 * int(np.sum(np.asarray(self.fe_nr) // 2 + 1))
+        return u
+
+    # ---------------------------------------------------------- C structs ---
+    def config(self, precision, device=0, stability_interval=0, compensated=1):
+        cfg = L.axg_config()
+        cfg.precision = L.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        cfg.device = device
+        cfg.dt = float(self.dt)
+        cfg.t0 = float(self.t0)
+        cfg.nsls = int(self.nsls)
+        for i in range(self.nsls):
+            cfg.att_alpha[i] = float(self.att_alpha[i])
+            cfg.att_beta[i] = float(self.att_beta[i])
+            cfg.att_gamma[i] = float(self.att_gamma[i])
+        cfg.stability_interval = stability_interval
+        cfg.deterministic = 0
+        cfg.compensated = compensated
+        return cfg
+
+    def c_structs(self):
+        """ctypes structs of the model; the returned dict keeps every array alive."""
+        keep = {}
+
+        def k(name, a, conv, ctype):
+            a = conv(a)
+            keep[name] = a
+            return L.ptr(a, ctype)
+
+        sp = L.axg_solid_points()
+        sp.count = len(self.sp_nr)
+        sp.nr = k("sp_nr", self.sp_nr, _i32, C.c_int32)
+        sp.mass_nr = k("sp_mass_nr", self.sp_mass_nr, _i32, C.c_int32)
+        sp.mass_offset = k("sp_mass_off", self.sp_mass_off, _i64, C.c_int64)
+        sp.mass = k("sp_mass", self.sp_mass, _f64, C.c_double)
+        sp.axial = k("sp_axial", self.sp_axial, _u8, C.c_uint8)
+
+        fp = L.axg_fluid_points()
+        fp.count = len(self.fp_nr)
+        fp.nr = k("fp_nr", self.fp_nr, _i32, C.c_int32)
+        fp.mass_nr = k("fp_mass_nr", self.fp_mass_nr, _i32, C.c_int32)
+        fp.mass_offset = k("fp_mass_off", self.fp_mass_off, _i64, C.c_int64)
+        fp.mass = k("fp_mass", self.fp_mass, _f64, C.c_double)
+        fp.axial = k("fp_axial", self.fp_axial, _u8, C.c_uint8)
+        fp.surface = k("fp_surface", self.fp_surface, _u8, C.c_uint8)
+
+        se = L.axg_solid_elements()
+        se.count = self.n_solid_elements
+        se.nr = k("se_nr", self.se_nr, _i32, C.c_int32)
+        se.points = k("se_pts", self.se_pts, _i32, C.c_int32)
+        se.axial = k("se_axial", self.se_axial, _u8, C.c_uint8)
+        se.geometry = k("se_geom", self.se_geom, _f64, C.c_double)
+        se.rtz = k("se_rtz", self.se_rtz, _u8, C.c_uint8)
+        se.theta = k("se_theta", self.se_theta, _f64, C.c_double)
+        se.rheology = k("se_rheo", self.se_rheo, _i32, C.c_int32)
+        se.is3d = k("se_is3d", self.se_is3d, _u8, C.c_uint8)
+        se.mat_offset = k("se_mat_off", self.se_mat_off, _i64, C.c_int64)
+        se.moduli = k("se_moduli", self.se_moduli, _f64, C.c_double)
+        se.attenuation = k("se_att", self.se_att, _i32, C.c_int32)
+        se.att_offset = k("se_att_off", self.se_att_off, _i64, C.c_int64)
+        se.att_moduli = k("se_att_moduli", self.se_att_moduli, _f64, C.c_double)
+
+        fe = L.axg_fluid_elements()
+        fe.count = self.n_fluid_elements
+        fe.nr = k("fe_nr", self.fe_nr, _i32, C.c_int32)
+        fe.points = k("fe_pts", self.fe_pts, _i32, C.c_int32)
+        fe.axial = k("fe_axial", self.fe_axial, _u8, C.c_uint8)
+        fe.geometry = k("fe_geom", self.fe_geom, _f64, C.c_double)
+        fe.is3d = k("fe_is3d", self.fe_is3d, _u8, C.c_uint8)
+        fe.mat_offset = k("fe_mat_off", self.fe_mat_off, _i64, C.c_int64)
+        fe.moduli = k("fe_moduli", self.fe_moduli, _f64, C.c_double)
+
+        sf = L.axg_solid_fluid()
+        sf.count = len(self.sf_solid)
+        sf.solid_point = k("sf_solid", self.sf_solid, _i32, C.c_int32)
+        sf.fluid_point = k("sf_fluid", self.sf_fluid, _i32, C.c_int32)
+        sf.ns_unassembled = k("sf_nsu", self.sf_nsu, _f64, C.c_double)
+        sf.nz_unassembled = k("sf_nzu", self.sf_nzu, _f64, C.c_double)
+        sf.ns_assembled = k("sf_nsa", self.sf_nsa, _f64, C.c_double)
+        sf.nz_assembled = k("sf_nza", self.sf_nza, _f64, C.c_double)
+        sf.mass_fluid = k("sf_mf", self.sf_mass_fluid, _f64, C.c_double)
+
+        def sources(kind, cls, ndim):
+            s = cls()
+            n = len(getattr(self, kind + "_elem"))
+            s.count = n
+            s.element = k(kind + "_elem", getattr(self, kind + "_elem"), _i32, C.c_int32)
+            s.nu = k(kind + "_nu", getattr(self, kind + "_nu"), _i32, C.c_int32)
+            s.pattern_offset = k(kind + "_po", getattr(self, kind + "_pat_off"), _i64, C.c_int64)
+            pat = np.ascontiguousarray(getattr(self, kind + "_pattern"), dtype=np.complex128)
+            keep[kind + "_pat"] = pat
+            s.pattern = pat.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))
+            stfs = (L.axg_stf * max(n, 1))()
+            for i, st in enumerate(getattr(self, kind + "_stf")):
+                stfs[i].half_duration = st.half_duration
+                stfs[i].decay_factor = st.decay_factor
+                stfs[i].time_shift = st.time_shift
+                stfs[i].derivative_order = st.derivative_order
+            keep[kind + "_stf"] = stfs
+            s.stf = C.cast(stfs, C.POINTER(L.axg_stf))
+            return s
+
+        ms = sources("ms", L.axg_moment_sources, 6)
+        fs = sources("fs", L.axg_force_sources, 3)
+
+        st = L.axg_stations()
+        st.count = len(self.st_elem)
+        st.element = k("st_elem", self.st_elem, _i32, C.c_int32)
+        st.weights = k("st_w", self.st_w, _f64, C.c_double)
+        st.phi = k("st_phi", self.st_phi, _f64, C.c_double)
+
+        return {"sp": sp, "fp": fp, "se": se, "fe": fe, "sf": sf, "ms": ms, "fs": fs, "st": st,
+                "keep": keep}

@@ -1,0 +1,260 @@
+"""Python mirror of the engine's C ABI, shaped like the reference's time loop.
+
+``Solver`` wraps one ``axg_solver`` handle. Its methods are the per-step hooks
+of AxiSEM3D's Domain / NewmarkTimeScheme, in the order of
+NewmarkTimeScheme::solve (SOLVER/src/core/time/NewmarkTimeScheme.cpp:41-108):
+
+    apply_sources(tstep)       Domain::applySources
+    compute_stiffness()        Domain::computeStiffness
+    apply_bc_before_assembly() Domain::applyBC_BeforeAssemblingStiff
+    record_stations(tstep)     Domain::recordOutput (station displacement)
+    apply_bc_after_assembly()  Domain::applyBC_AfterAssemblingStiff
+    stiff_to_accel()           Domain::computeStiffToAccel
+    newmark_update()           NewmarkTimeScheme::update on all points
+    run(nsteps)                the whole loop body, one CUDA graph per step
+
+Errors raise ``RuntimeError`` with the engine's "Class::method || message"
+text, as the reference throws std::runtime_error.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class Solver:
+    def __init__(self, model, precision="fp32", device=0, stability_interval=0, compensated=True,
+                 team_sizes=None):
+        self.lib = L.lib()
+        self.model = model
+        self.precision = precision
+        cfg = model.config(precision, device=device, stability_interval=stability_interval,
+                           compensated=int(bool(compensated)))
+        h = C.c_void_p()
+        rc = self.lib.axg_create(C.byref(cfg), C.byref(h))
+        if rc != L.AXG_OK:
+            raise EngineError(rc, "axg_create failed (%d): %s" % (rc, self.lib.axg_last_error(None).decode()))
+        self.h = h
+        s = model.c_structs()
+        self._keep = s
+        self._check(self.lib.axg_set_solid_points(h, C.byref(s["sp"])))
+        if s["fp"].count:
+            self._check(self.lib.axg_set_fluid_points(h, C.byref(s["fp"])))
+        self._check(self.lib.axg_set_solid_elements(h, C.byref(s["se"])))
+        if s["fe"].count:
+            self._check(self.lib.axg_set_fluid_elements(h, C.byref(s["fe"])))
+        if s["sf"].count:
+            self._check(self.lib.axg_set_solid_fluid(h, C.byref(s["sf"])))
+        if s["ms"].count:
+            self._check(self.lib.axg_set_moment_sources(h, C.byref(s["ms"])))
+        if s["fs"].count:
+            self._check(self.lib.axg_set_force_sources(h, C.byref(s["fs"])))
+        if s["st"].count:
+            self._check(self.lib.axg_set_stations(h, C.byref(s["st"]), int(model.st_interval)))
+        for cls, team in (team_sizes or {}).items():
+            self._check(self.lib.axg_set_team_size(h, int(cls), int(team)))
+        self._check(self.lib.axg_finalize(h))
+
+    # ------------------------------------------------------------------ util ---
+    def _check(self, rc):
+        if rc != L.AXG_OK:
+            msg = self.lib.axg_last_error(self.h).decode()
+            raise EngineError(rc, msg or ("axg error %d" % rc))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.axg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------------ hooks ---
+    def apply_sources(self, tstep):
+        self._check(self.lib.axg_apply_sources(self.h, int(tstep)))
+
+    def compute_stiffness(self):
+        self._check(self.lib.axg_compute_stiffness(self.h))
+
+    def apply_bc_before_assembly(self):
+        self._check(self.lib.axg_apply_bc_before_assembly(self.h))
+
+    def apply_bc_after_assembly(self):
+        self._check(self.lib.axg_apply_bc_after_assembly(self.h))
+
+    def stiff_to_accel(self):
+        self._check(self.lib.axg_stiff_to_accel(self.h))
+
+    def newmark_update(self):
+        self._check(self.lib.axg_newmark_update(self.h))
+
+    def record_stations(self, tstep):
+        self._check(self.lib.axg_record_stations(self.h, int(tstep)))
+
+    def run(self, nsteps, graph=True):
+        self._check(self.lib.axg_run(self.h, int(nsteps), int(bool(graph))))
+
+    def synchronize(self):
+        self._check(self.lib.axg_synchronize(self.h))
+
+    @property
+    def step(self):
+        t = C.c_int32()
+        self._check(self.lib.axg_current_step(self.h, C.byref(t)))
+        return t.value
+
+    # ----------------------------------------------------------------- fields ---
+    def field_size(self, solid=True):
+        n = C.c_int64()
+        self._check(self.lib.axg_field_size(self.h, int(bool(solid)), C.byref(n)))
+        return n.value
+
+    def get_field(self, which="displ", solid=True):
+        w = {"stiff": 0, "displ": 1, "veloc": 2, "accel": 3}[which]
+        n = self.field_size(solid)
+        out = np.zeros(n, dtype=np.complex128)
+        if n:
+            self._check(self.lib.axg_get_field(self.h, int(bool(solid)), w,
+                                               out.view(np.float64).ctypes.data_as(L.P_f64)))
+        return out
+
+    def set_field(self, values, which="displ", solid=True):
+        w = {"stiff": 0, "displ": 1, "veloc": 2, "accel": 3}[which]
+        v = np.ascontiguousarray(values, dtype=np.complex128)
+        if v.size != self.field_size(solid):
+            raise EngineError(L.AXG_E_ARG, "axg_set_field || size mismatch")
+        self._check(self.lib.axg_set_field(self.h, int(bool(solid)), w,
+                                           v.view(np.float64).ctypes.data_as(L.P_f64)))
+
+    def field_raw_bytes(self, which="displ", solid=True):
+        w = {"stiff": 0, "displ": 1, "veloc": 2, "accel": 3}[which]
+        n = C.c_int64()
+        self._check(self.lib.axg_field_raw_bytes(self.h, int(bool(solid)), w, C.byref(n)))
+        return n.value
+
+    def set_field_raw(self, host_ptr, nbytes, which="displ", solid=True):
+        """Asynchronous native-precision copy from a (pinned) host address."""
+        w = {"stiff": 0, "displ": 1, "veloc": 2, "accel": 3}[which]
+        self._check(self.lib.axg_set_field_raw(self.h, int(bool(solid)), w, C.c_void_p(host_ptr), int(nbytes)))
+
+    def get_field_raw(self, host_ptr, nbytes, which="displ", solid=True):
+        w = {"stiff": 0, "displ": 1, "veloc": 2, "accel": 3}[which]
+        self._check(self.lib.axg_get_field_raw(self.h, int(bool(solid)), w, C.c_void_p(host_ptr), int(nbytes)))
+
+    def seismograms(self):
+        """(nrecords, nstations, 3) displacement in s, phi, z."""
+        n = C.c_int32()
+        self._check(self.lib.axg_get_seismograms(self.h, None, C.byref(n)))
+        ns = len(self.model.st_elem)
+        out = np.zeros((n.value, ns, 3))
+        if n.value and ns:
+            self._check(self.lib.axg_get_seismograms(self.h, out.ctypes.data_as(L.P_f64), C.byref(n)))
+        return out
+
+    # ------------------------------------------------------------ diagnostics ---
+    def launch_count(self):
+        n = C.c_int64()
+        self._check(self.lib.axg_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def set_timing(self, on=True):
+        self._check(self.lib.axg_set_timing(self.h, int(bool(on))))
+
+    def stiffness_time(self):
+        ms, n = C.c_double(), C.c_int64()
+        self._check(self.lib.axg_stiffness_time_ms(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def stiffness_cost(self):
+        b, f = C.c_double(), C.c_double()
+        self._check(self.lib.axg_stiffness_cost(self.h, C.byref(b), C.byref(f)))
+        return b.value, f.value
+
+    def point_cost(self):
+        b = C.c_double()
+        self._check(self.lib.axg_point_cost(self.h, C.byref(b)))
+        return b.value
+
+    def set_stream(self, stream_ptr):
+        self._check(self.lib.axg_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+
+# --------------------------------------------------------- operand builders ---
+def spectral_tables():
+    lib = L.lib()
+    bufs = [np.zeros(5) for _ in range(4)] + [np.zeros(25), np.zeros(25)]
+    lib.axg_spectral_tables(*[b.ctypes.data_as(L.P_f64) for b in bufs])
+    return dict(zip(["pGLL", "pGLJ", "wGLL", "wGLJ", "gGLL", "gGLJ"], bufs))
+
+
+def quad_geometry(nodal_sz, axial, mapping=L.AXG_MAP_LINEAR):
+    """Quad::createGradient operands: (6, 25) geometry and (2, 25) point coordinates."""
+    lib = L.lib()
+    n = np.ascontiguousarray(nodal_sz, dtype=np.float64).reshape(8)
+    g = np.zeros(150)
+    sz = np.zeros(50)
+    rc = lib.axg_quad_geometry(int(mapping), n.ctypes.data_as(L.P_f64), int(bool(axial)),
+                               g.ctypes.data_as(L.P_f64), sz.ctypes.data_as(L.P_f64))
+    if rc != L.AXG_OK:
+        raise EngineError(rc, "axg_quad_geometry failed (%d)" % rc)
+    return g.reshape(6, 25), sz.reshape(2, 25)
+
+
+def quad_dt(sz, vmax):
+    lib = L.lib()
+    s = np.ascontiguousarray(sz, dtype=np.float64).reshape(50)
+    dt = C.c_double()
+    rc = lib.axg_quad_dt(s.ctypes.data_as(L.P_f64), float(vmax), C.byref(dt))
+    if rc != L.AXG_OK:
+        raise EngineError(rc, "axg_quad_dt failed")
+    return dt.value
+
+
+def att_alpha_beta_gamma(w, y, dt):
+    lib = L.lib()
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    a, b, g = np.zeros(len(w)), np.zeros(len(w)), np.zeros(len(w))
+    rc = lib.axg_att_alpha_beta_gamma(len(w), w.ctypes.data_as(L.P_f64), y.ctypes.data_as(L.P_f64),
+                                      float(dt), a.ctypes.data_as(L.P_f64), b.ctypes.data_as(L.P_f64),
+                                      g.ctypes.data_as(L.P_f64))
+    if rc != L.AXG_OK:
+        raise EngineError(rc, "axg_att_alpha_beta_gamma failed")
+    return a, b, g
+
+
+def att_moduli(w, y, fmin, fmax, fref, qkappa, qmu, kp, mu):
+    """AttBuilder::createAttenuation (FULL): returns (kp_unrelaxed, mu_unrelaxed, dkp, dmu)."""
+    lib = L.lib()
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    qk = np.ascontiguousarray(np.broadcast_to(qkappa, np.shape(kp)), dtype=np.float64).ravel()
+    qm = np.ascontiguousarray(np.broadcast_to(qmu, np.shape(kp)), dtype=np.float64).ravel()
+    kp2 = np.array(kp, dtype=np.float64).ravel().copy()
+    mu2 = np.array(mu, dtype=np.float64).ravel().copy()
+    dk, dm = np.zeros_like(kp2), np.zeros_like(kp2)
+    rc = lib.axg_att_moduli(len(w), w.ctypes.data_as(L.P_f64), y.ctypes.data_as(L.P_f64),
+                            float(fmin), float(fmax), float(fref), len(kp2),
+                            qk.ctypes.data_as(L.P_f64), qm.ctypes.data_as(L.P_f64),
+                            kp2.ctypes.data_as(L.P_f64), mu2.ctypes.data_as(L.P_f64),
+                            dk.ctypes.data_as(L.P_f64), dm.ctypes.data_as(L.P_f64))
+    if rc != L.AXG_OK:
+        raise EngineError(rc, "axg_att_moduli failed")
+    shp = np.shape(kp)
+    return kp2.reshape(shp), mu2.reshape(shp), dk.reshape(shp), dm.reshape(shp)

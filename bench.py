@@ -1,0 +1,355 @@
+"""Benchmark: GLL-point x mode updates per second of the full time step.
+
+Workload (stiffness microbenchmark, uneven batching): ~200k non-axial solid
+quads with nPol = 4, per-element nr log-uniform on [1, 64], transversely
+isotropic moduli at +-10 % around vp = 8, vs = 4.5 km/s, rho = 3.3 g/cc per
+(element, slice, point) -- the 3-D (slice) path -- with 3 SLS attenuation
+memory variables (Q_mu uniform in [80, 600]). Seeded synthetic data.
+
+One step = the whole Newmark step on every element and point: fused solid
+stiffness (gather, gradient, phi transform, TI stress, SLS attenuation,
+inverse transform, quadrature, scatter-add), then boundary conditions, 1/M and
+the Newmark update. Updates per step = sum_e 25 nu_e (nu = nr/2 + 1).
+
+  value  device-timed with CUDA events on the engine's stream, state resident in
+         HBM, one CUDA graph per step; inputs larger than L2 (the step streams
+         ~20 GB)
+  e2e    the same steps through the C ABI with the displacement field copied
+         host -> device from pinned memory before every step and the updated
+         displacement copied back after it (axg_set_field_raw / axg_run /
+         axg_get_field_raw)
+  roofline  the solid stiffness kernels: algorithmic bytes per evaluation /
+         measured duration, against the measured HBM copy bandwidth
+  cpu_baseline  the C++ CPU restatement (oracle, FP32 like the reference's
+         default build) on all host cores, on a bounded sample of the workload
+
+Run with N GPUs (torchrun): every rank advances its own replica of the
+workload (weak scaling, no exchange); value = all ranks' updates / max time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GLL-pt*mode updates/s"
+UNIT = "updates/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64"])
+    p.add_argument("--elements", type=int, default=200000)
+    p.add_argument("--nr-max", type=int, default=64)
+    p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------- helpers ---
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), float(f[3]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        load = [r for r in rows if r[2] > 250.0] or rows
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in load:
+            for n, v in zip(names, r[3]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(r[0] for r in load), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(load)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per stiffness evaluation from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "stiffness_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def build_model(args, seed=1):
+    from axisem3d_b200 import meshgen
+    return meshgen.microbench_model(n_elem=args.elements, nr_max=args.nr_max, seed=seed)
+
+
+def workload_config(args, m):
+    return {"workload": "stiffness microbenchmark, uneven nr: %d solid quads nPol=4, nr log-uniform "
+                        "[1,%d], TI 3-D slices, 3 SLS FULL, full Newmark step" % (m.n_solid_elements, args.nr_max),
+            "elements": int(m.n_solid_elements), "updates_per_step": int(m.updates_per_step()),
+            "precision": args.precision, "l2": "inputs larger than L2 (the step streams >10 GB)",
+            "graph": "one CUDA graph per step"}
+
+
+# --------------------------------------------------------------- CPU baseline ---
+def cpu_baseline(args, seconds):
+    """Oracle (FP32, the reference's default precision) on all host cores, bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    n = max(200, min(4000, args.elements // 100))
+    m = meshgen.microbench_model(n_elem=n, nr_max=args.nr_max, seed=7)
+    cores = os.cpu_count() or 1
+    o = O.Oracle(m, "fp32", threads=cores)
+    o.set_field(meshgen.random_displacement(m, seed=3) * 1e-6, "displ")
+    o.run(1)
+    steps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        o.run(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    upd = m.updates_per_step() * steps / dt
+    return {"value": upd, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d-element sample of the same distribution, %d full steps in %.1f s, FP32" %
+                      (m.n_solid_elements, steps, dt)}
+
+
+# --------------------------------------------------------------------- arms ---
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    per = max(2.0, min(20.0, 120.0 / (steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_baseline(args, min(per, 2.0))
+    vals = [cpu_baseline(args, per) for _ in range(steps)]
+    v = float(np.median([x["value"] for x in vals]))
+    cb = dict(vals[0])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "stiffness microbenchmark, uneven nr (bounded CPU sample)",
+                       "elements_sample": cb["sample"]},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def time_steps(solver, steps, stream):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    solver.run(steps, graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    m = build_model(args, seed=1 + rank)
+    U = m.updates_per_step()
+    s = Solver(m, args.precision, device=local)
+    s.set_stream(stream.cuda_stream)
+    u0 = meshgen.random_displacement(m, seed=2 + rank) * 1e-6
+    s.set_field(u0, "displ")
+    clocks = ClockSampler(local)
+    with clocks:
+        s.run(max(3, args.warmup), graph=True)
+        barrier(world)
+        torch.cuda.synchronize()
+        n0 = s.launch_count()
+        t = time_steps(s, args.steps, stream)
+        launches = s.launch_count() - n0
+        t = dist_max(t, world)
+        # stiffness kernels alone: per-step events around the solid stiffness launches
+        s.set_timing(True)
+        s.run(5, graph=False)
+        kms, kn = s.stiffness_time()
+        s.set_timing(False)
+        # end to end through the C ABI with host buffers
+        nb = s.field_raw_bytes("displ")
+        host = torch.empty(nb, dtype=torch.uint8, pin_memory=True)
+        s.get_field_raw(host.data_ptr(), nb, "displ")
+        torch.cuda.synchronize()
+        ke = max(3, min(args.steps, 10))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier(world)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(ke):
+            s.set_field_raw(host.data_ptr(), nb, "displ")
+            s.run(1, graph=True)
+            s.get_field_raw(host.data_ptr(), nb, "displ")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        te = max(e0.elapsed_time(e1) / 1e3, time.perf_counter() - w0)
+        te = dist_max(te, world)
+    bytes_, flops = s.stiffness_cost()
+    pbytes = s.point_cost()
+    s.close()
+    value = U * args.steps * world / t
+    out = {"value": value, "t": t, "launches": launches, "kms": kms / max(kn, 1), "bytes": bytes_,
+           "flops": flops, "pbytes": pbytes, "U": U, "e2e": U * ke * world / te, "e2e_bytes": nb,
+           "clocks": clocks.summary(), "model": m}
+    # FP64 run of the same workload (the metric compares FP32 and FP64 paths)
+    if not args.no_fp64 and args.precision != "fp64":
+        s64 = Solver(m, "fp64", device=local)
+        s64.set_stream(stream.cuda_stream)
+        s64.set_field(u0, "displ")
+        s64.run(2, graph=True)
+        k64 = max(3, args.steps // 5)
+        t64 = dist_max(time_steps(s64, k64, stream), world)
+        out["value_fp64"] = U * k64 * world / t64
+        s64.close()
+    return out
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    r = run_ours(args, world, rank, local)
+    if rank == 0:
+        m = r["model"]
+        peak, peak_kind = measured_peaks()
+        achieved = r["bytes"] / (r["kms"] / 1e3) / 1e9
+        trafficd = profiled_traffic()
+        traffic = None
+        if trafficd and trafficd.get("elements") == m.n_solid_elements:
+            traffic = trafficd.get("dram_bytes_per_launch_group")
+        cb = cpu_baseline(args, args.cpu_seconds)
+        line = {
+            "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["t"] / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"mixed": "f32 (f64 Newmark d/v and SLS state)", "fp32": "f32", "fp64": "f64"}[args.precision],
+            "data": "synthetic", "config": workload_config(args, m),
+            "gpu_launches": int(r["launches"]),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "solid stiffness (fused), %.3f ms per evaluation, %.2f GB algorithmic"
+                                   % (r["kms"], r["bytes"] / 1e9),
+                         "peak_kind": peak_kind + " HBM copy bandwidth"},
+            "cpu_baseline": cb,
+            "e2e": {"value": r["e2e"], "unit": UNIT, "h2d_bytes_per_step": int(r["e2e_bytes"]),
+                    "d2h_bytes_per_step": int(r["e2e_bytes"])},
+            "clocks": r["clocks"],
+            "stiffness_flops_per_step": r["flops"],
+            "point_update_bytes_per_step": r["pbytes"],
+        }
+        if "value_fp64" in r:
+            line["value_fp64"] = r["value_fp64"]
+            line["fp32_over_fp64"] = r["value"] / r["value_fp64"]
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

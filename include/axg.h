@@ -1,0 +1,317 @@
+/*
+ * axg.h -- C ABI of the B200 time-step engine for AxiSEM3D (nPol = 4).
+ *
+ * The engine replaces, for one MPI rank's sub-mesh, the per-time-step work that
+ * AxiSEM3D's Domain performs on the CPU:
+ *
+ *   SolidElement::computeStiff / FluidElement::computeStiff
+ *       (SOLVER/src/core/element/SolidElement.cpp:213-222,
+ *        SOLVER/src/core/element/FluidElement.cpp:163-172)
+ *       called in a loop by Domain::computeStiffness
+ *       (SOLVER/src/core/domain/Domain.cpp:298-308)
+ *   Domain::applyBC_BeforeAssemblingStiff / applyBC_AfterAssemblingStiff
+ *       (Domain.cpp:313-326; SolidFluidCoupling, AxialBoundary, FluidSurfaceBoundary)
+ *   Domain::computeStiffToAccel -> SolidPoint/FluidPoint::computeStiffToAccel
+ *       (Domain.cpp:335-345, SOLVER/src/core/point/SolidPoint.cpp:28-36,
+ *        FluidPoint.cpp:28-54, mass/Mass1D.hpp:25-32, mass/Mass3D.cpp:41-68)
+ *   NewmarkTimeScheme::update<Point>
+ *       (SOLVER/src/core/time/NewmarkTimeScheme.hpp:47-71)
+ *   Domain::applySources -> SolidMoment::apply / SolidForce::apply
+ *       (Domain.cpp:285-295, SOLVER/src/core/source/elem_src/solid/SolidMoment.cpp:29-33)
+ *   StationSolid::record (displacement channel)
+ *       (SOLVER/src/core/output/station-wise/station/StationSolid.cpp:58-91)
+ *   the driver loop NewmarkTimeScheme::solve (NewmarkTimeScheme.cpp:41-108)
+ *
+ * Conventions shared with the reference:
+ *   - point index inside an element: ipnt = ipol * 5 + jpol, ipol <-> xi (GLJ on
+ *     axial elements, axis at ipol = 0), jpol <-> eta (spectrals.hpp:321-339);
+ *   - a point of Fourier order nr stores nu = nr / 2 + 1 complex modes;
+ *     an element's nr is the maximum over its 25 points (Element.cpp:28-43);
+ *   - Voigt order 0=ss 1=pp 2=zz 3=pz 4=sz 5=sp, engineering shear strain;
+ *   - 3-D (azimuthally varying) properties are sampled on slices
+ *     phi_k = 2 pi k / nr, k = 0..nr-1.
+ *
+ * Host-side field layout (axg_get_field / axg_set_field): for each point in
+ * point order, nu_p x ndim complex doubles, row-major in (mode, dim), i.e. the
+ * transpose of the reference's column-major eigen::CMatX3 (SolidPoint.hpp:126-131).
+ *
+ * Every function returns AXG_OK (0) or a negative AXG_E_* code; the message is
+ * available from axg_last_error(h) in the reference's "Class::method || message"
+ * format. No C++ exception crosses this boundary.
+ *
+ * A handle is not thread-safe: one handle per host thread / CUDA stream, as the
+ * reference's element code is non-reentrant (static workspaces,
+ * SolidElement.hpp:203-218).
+ */
+#ifndef AXG_H
+#define AXG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AXG_NPED 5
+#define AXG_NPEM 25
+
+/* status codes */
+#define AXG_OK            0
+#define AXG_E_ARG        -1   /* invalid argument or inconsistent sizes   */
+#define AXG_E_STATE      -2   /* call out of order (e.g. step before finalize) */
+#define AXG_E_CUDA       -3   /* CUDA runtime error                         */
+#define AXG_E_UNSTABLE   -4   /* non-finite displacement (Domain::checkStability) */
+#define AXG_E_NOMEM      -5   /* device allocation failed                   */
+#define AXG_E_UNSUPPORTED -6  /* feature combination not built              */
+
+/* precision of the time loop */
+#define AXG_FP64   0  /* everything in double (reference built with -Ddouble=true) */
+#define AXG_FP32   1  /* everything in float (reference default build)            */
+#define AXG_MIXED  2  /* float stiffness; double Newmark d/v with compensated
+                         summation; double attenuation memory variables          */
+
+/* rheology */
+#define AXG_ISO    0  /* lambda, mu                                  (Isotropic.hpp)             */
+#define AXG_TISO   1  /* A, C, F, L, N                               (TransverselyIsotropic.hpp) */
+#define AXG_ANISO  2  /* C11 C12 C13 C14 C15 C16 C22 C23 C24 C25 C26
+                         C33 C34 C35 C36 C44 C45 C46 C55 C56 C66   (Anisotropic.hpp)           */
+
+/* attenuation (SLS memory variables) */
+#define AXG_ATT_NONE 0
+#define AXG_ATT_FULL 1  /* all 25 points          (AttenuationFull.hpp) */
+#define AXG_ATT_CG4  2  /* points (1,1) (1,3) (3,1) (3,3)  (AttenuationCG4.hpp) */
+
+/* fields */
+#define AXG_FIELD_STIFF 0
+#define AXG_FIELD_DISPL 1
+#define AXG_FIELD_VELOC 2
+#define AXG_FIELD_ACCEL 3
+
+/* mapping of a quad (SOLVER/src/preloop/se_model/quad/mapping) */
+#define AXG_MAP_LINEAR    0   /* MappingLinear.hpp    */
+#define AXG_MAP_SPHERICAL 1   /* MappingSpherical.hpp */
+
+#define AXG_MAX_SLS 8
+
+typedef struct axg_config {
+    int32_t precision;          /* AXG_FP64 / AXG_FP32 / AXG_MIXED                        */
+    int32_t device;             /* CUDA device ordinal                                     */
+    double  dt;                 /* time step (NewmarkTimeScheme mDt)                       */
+    double  t0;                 /* time of step 0 (TimeScheme mT0)                         */
+    int32_t nsls;               /* number of standard linear solids (0 if no attenuation) */
+    double  att_alpha[AXG_MAX_SLS]; /* Attenuation::setAlphaBetaGamma statics              */
+    double  att_beta[AXG_MAX_SLS];
+    double  att_gamma[AXG_MAX_SLS];
+    int32_t stability_interval; /* steps between non-finite checks (0 = never)            */
+    int32_t deterministic;      /* reserved: 0 = atomic scatter-add                        */
+    int32_t compensated;        /* MIXED only: 1 = compensated (Kahan) d/v summation      */
+} axg_config;
+
+/* solid GLL points (SolidPoint + Mass1D/Mass3D + AxialBoundary membership) */
+typedef struct axg_solid_points {
+    int32_t        count;
+    const int32_t *nr;          /* [count] Fourier order of each point                      */
+    const int32_t *mass_nr;     /* [count] 1 (Mass1D) or nr (Mass3D); NULL = all 1        */
+    const int64_t *mass_offset; /* [count] offset into mass; NULL = point index            */
+    const double  *mass;        /* integrated mass (not inverted) per point / per slice    */
+    const uint8_t *axial;       /* [count] 1 = point on the axis (AxialBoundary); may be NULL */
+} axg_solid_points;
+
+/* fluid GLL points (FluidPoint) */
+typedef struct axg_fluid_points {
+    int32_t        count;
+    const int32_t *nr;
+    const int32_t *mass_nr;
+    const int64_t *mass_offset;
+    const double  *mass;        /* integrated 1/kappa (Material::getMass, fluid branch) */
+    const uint8_t *axial;       /* AxialBoundary (fluid part) */
+    const uint8_t *surface;     /* FluidSurfaceBoundary: stiffness zeroed */
+} axg_fluid_points;
+
+/* solid elements: the operands SolidElement holds after Quad::release */
+typedef struct axg_solid_elements {
+    int32_t        count;
+    const int32_t *nr;          /* [count] element nr (max over its points)             */
+    const int32_t *points;      /* [count*25] solid point indices                       */
+    const uint8_t *axial;       /* [count] GradientQuadrature mAxial                    */
+    const double  *geometry;    /* [count*6*25] dsdxii, dsdeta, dzdxii, dzdeta, 1/s,
+                                   integral factor (Quad::createGradient, Quad.hpp:155-184) */
+    const uint8_t *rtz;         /* [count] rheology in RTZ (spherical meshes); NULL = none */
+    const double  *theta;       /* [count*25] polar angle for CoordTransformSpherical    */
+    const int32_t *rheology;    /* [count] AXG_ISO / AXG_TISO / AXG_ANISO              */
+    const uint8_t *is3d;        /* [count] 1 = properties per slice (nr x 25)           */
+    const int64_t *mat_offset;  /* [count] offset (doubles) into moduli                 */
+    const double  *moduli;      /* per element [nmod][nslice][25], nslice = nr or 1     */
+    const int32_t *attenuation; /* [count] AXG_ATT_*; NULL = none                        */
+    const int64_t *att_offset;  /* [count] offset (doubles) into att_moduli              */
+    const double  *att_moduli;  /* per element [2][nslice][25 or 4]: dlambda, dmu        */
+} axg_solid_elements;
+
+/* fluid elements: FluidElement + Acoustic (K = 1/rho) */
+typedef struct axg_fluid_elements {
+    int32_t        count;
+    const int32_t *nr;
+    const int32_t *points;      /* [count*25] fluid point indices */
+    const uint8_t *axial;
+    const double  *geometry;    /* [count*6*25] as for solids */
+    const uint8_t *is3d;
+    const int64_t *mat_offset;
+    const double  *moduli;      /* per element [nslice][25]: K */
+} axg_fluid_elements;
+
+/* solid-fluid coupling pairs (SolidFluidCoupling1D.hpp:26-37) */
+typedef struct axg_solid_fluid {
+    int32_t        count;
+    const int32_t *solid_point;
+    const int32_t *fluid_point;
+    const double  *ns_unassembled;
+    const double  *nz_unassembled;
+    const double  *ns_assembled;
+    const double  *nz_assembled;
+    const double  *mass_fluid;
+} axg_solid_fluid;
+
+/* Gaussian-family source-time function (GaussianSTF.hpp:35-58) */
+typedef struct axg_stf {
+    double  half_duration;
+    double  decay_factor;
+    double  time_shift;
+    int32_t derivative_order;   /* -1 erf, 0 Gaussian, 1, 2 (Ricker) */
+} axg_stf;
+
+/* moment-tensor sources (SolidMoment + Mechanism pattern) */
+typedef struct axg_moment_sources {
+    int32_t        count;
+    const int32_t *element;       /* solid element index                        */
+    const int32_t *nu;            /* pattern modes (rows of CMatXN6)             */
+    const int64_t *pattern_offset;/* offset in complex numbers into pattern      */
+    const double  *pattern;       /* per source [nu][6][25] complex (re, im)     */
+    const axg_stf *stf;           /* [count] */
+} axg_moment_sources;
+
+/* point-force sources (SolidForce + Mechanism pattern) */
+typedef struct axg_force_sources {
+    int32_t        count;
+    const int32_t *element;
+    const int32_t *nu;
+    const int64_t *pattern_offset;
+    const double  *pattern;       /* per source [nu][3][25] complex */
+    const axg_stf *stf;
+} axg_force_sources;
+
+/* stations: in-plane Lagrange weights and azimuth (Station.hpp:53-72) */
+typedef struct axg_stations {
+    int32_t        count;
+    const int32_t *element;       /* solid element index  */
+    const double  *weights;       /* [count*25]           */
+    const double  *phi;           /* [count]              */
+} axg_stations;
+
+typedef struct axg_solver axg_solver;
+
+/* ---- lifetime ---- */
+int  axg_create(const axg_config *cfg, axg_solver **out);
+int  axg_destroy(axg_solver *h);
+const char *axg_last_error(const axg_solver *h);
+const char *axg_version(void);
+
+/* ---- model upload (host copies, nothing borrowed after return) ---- */
+int  axg_set_solid_points(axg_solver *h, const axg_solid_points *p);
+int  axg_set_fluid_points(axg_solver *h, const axg_fluid_points *p);
+int  axg_set_solid_elements(axg_solver *h, const axg_solid_elements *e);
+int  axg_set_fluid_elements(axg_solver *h, const axg_fluid_elements *e);
+int  axg_set_solid_fluid(axg_solver *h, const axg_solid_fluid *c);
+int  axg_set_moment_sources(axg_solver *h, const axg_moment_sources *s);
+int  axg_set_force_sources(axg_solver *h, const axg_force_sources *s);
+int  axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interval);
+/* builds buckets, uploads to HBM; must precede any time-loop call */
+int  axg_finalize(axg_solver *h);
+
+/* ---- the per-step hooks, one Domain method each ---- */
+/* Domain::applySources for step tstep (time t0 + tstep*dt accumulated as in solve()) */
+int  axg_apply_sources(axg_solver *h, int32_t tstep);
+/* Domain::computeStiffness: point stiff -= K u for every element */
+int  axg_compute_stiffness(axg_solver *h);
+/* Domain::applyBC_BeforeAssemblingStiff (solid-fluid coupling) */
+int  axg_apply_bc_before_assembly(axg_solver *h);
+/* Domain::applyBC_AfterAssemblingStiff (axial, fluid surface) */
+int  axg_apply_bc_after_assembly(axg_solver *h);
+/* Domain::computeStiffToAccel (Nyquist, 1/M) */
+int  axg_stiff_to_accel(axg_solver *h);
+/* NewmarkTimeScheme::update on all points */
+int  axg_newmark_update(axg_solver *h);
+/* station recording of the displacement at step tstep */
+int  axg_record_stations(axg_solver *h, int32_t tstep);
+/* nsteps full Newmark steps starting at the handle's step counter
+   (NewmarkTimeScheme::solve loop body); use_graph = 1 replays one CUDA graph per step */
+int  axg_run(axg_solver *h, int32_t nsteps, int32_t use_graph);
+/* step counter of the next step */
+int  axg_current_step(const axg_solver *h, int32_t *tstep);
+
+/* ---- fields ---- */
+/* solid = 1 for solid points, 0 for fluid; host buffer of sum(nu_p)*ndim complex doubles */
+int  axg_get_field(axg_solver *h, int32_t solid, int32_t which, double *host_out);
+int  axg_set_field(axg_solver *h, int32_t solid, int32_t which, const double *host_in);
+/* number of complex values of a field (sum(nu_p) * ndim) */
+int  axg_field_size(const axg_solver *h, int32_t solid, int64_t *n);
+/* native-precision copies between a (pinned) host buffer and a device field,
+   asynchronous on the handle's stream: complex float for FP32 fields, complex
+   double for FP64 ones (MIXED: displacement and velocity are double, stiffness
+   and acceleration float). bytes must equal axg_field_raw_bytes(). Setting the
+   displacement also refreshes the element copy and clears the compensation. */
+int  axg_field_raw_bytes(const axg_solver *h, int32_t solid, int32_t which, int64_t *bytes);
+int  axg_set_field_raw(axg_solver *h, int32_t solid, int32_t which, const void *host, int64_t bytes);
+int  axg_get_field_raw(axg_solver *h, int32_t solid, int32_t which, void *host, int64_t bytes);
+/* seismograms recorded so far: [nrecords][nstations][3] doubles, SPZ components */
+int  axg_get_seismograms(axg_solver *h, double *host_out, int32_t *nrecords);
+int  axg_synchronize(axg_solver *h);
+
+/* ---- diagnostics ---- */
+/* number of kernels launched by this handle since creation */
+int  axg_launch_count(const axg_solver *h, int64_t *n);
+/* cumulative device time (ms) of the solid stiffness kernels, when timing is on */
+int  axg_set_timing(axg_solver *h, int32_t on);
+int  axg_stiffness_time_ms(axg_solver *h, double *ms, int64_t *launches);
+/* algorithmic HBM bytes and FP32/FP64 flops of one stiffness evaluation
+   (solid + fluid elements), from the mesh, by the formulas in DESIGN.md */
+int  axg_stiffness_cost(const axg_solver *h, double *bytes, double *flops);
+/* algorithmic bytes of one point update (stiff->accel + Newmark) */
+int  axg_point_cost(const axg_solver *h, double *bytes);
+/* run on the caller's CUDA stream (a cudaStream_t passed as void*; NULL = the
+   handle's own stream). Invalidates a captured step graph. */
+int  axg_set_stream(axg_solver *h, void *stream);
+/* threads per element team for the nr class (0: nr<=3, 1: <=9, 2: <=25, 3: <=64,
+   4: larger); 32, 64, 128 or 256; before axg_finalize (the autotuner's knob) */
+int  axg_set_team_size(axg_solver *h, int32_t nr_class, int32_t team);
+
+/* ---- operand construction (host, double), the preloop numbers ---- */
+/* GLL/GLJ positions, weights and G matrices for nPol = 4, derived from their
+   definitions and rounded to 12 decimals (spectrals.hpp:73-102) */
+int  axg_spectral_tables(double *xgll, double *xglj, double *wgll, double *wglj,
+                         double *ggll, double *gglj);
+/* Quad::createGradient + Quad::computeIntegralFactor (Quad.hpp:155-184,
+   Quad.cpp:403-435) for a quad with the given 4 nodes (s0 z0 s1 z1 s2 z2 s3 z3,
+   counter-clockwise from (xi,eta)=(-1,-1)); out_geometry[6*25], out_sz[2*25] */
+int  axg_quad_geometry(int32_t mapping, const double *nodal_sz, int32_t axial,
+                       double *out_geometry, double *out_sz);
+/* axg_quad_geometry over n quads: nodal_sz [n*8], axial [n], out [n*150], [n*50] */
+int  axg_quad_geometry_batch(int32_t n, int32_t mapping, const double *nodal_sz,
+                             const uint8_t *axial, double *out_geometry, double *out_sz);
+/* Quad::computeDt (Quad.cpp:271-349) for one quad: min neighbour distance / vmax */
+int  axg_quad_dt(const double *sz, double vmax, double *dt);
+/* AttBuilder::setAlphaBetaGamma (AttBuilder.cpp:183-198) */
+int  axg_att_alpha_beta_gamma(int32_t nsls, const double *w, const double *y, double dt,
+                              double *alpha, double *beta, double *gamma);
+/* AttBuilder::createAttenuation (AttBuilder.cpp:102-178), FULL or CG4, for n samples:
+   kp, mu are modified in place (relaxed -> unrelaxed moduli); dkp/dmu outputs are
+   per sample (CG4 weighting is applied by the caller through weights_cg4 when cg4=1,
+   on arrays of 25 points per sample) */
+int  axg_att_moduli(int32_t nsls, const double *w, const double *y,
+                    double fmin, double fmax, double fref,
+                    int32_t n, const double *qkappa, const double *qmu,
+                    double *kp, double *mu, double *dkp, double *dmu);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AXG_H */

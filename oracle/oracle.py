@@ -1,0 +1,167 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so) -- test infrastructure only.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker of the CUDA engine; the product path never imports it.
+The oracle consumes the same ``axisem3d_b200.model.Model`` as the engine.
+"""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+sys.path.insert(0, HERE)
+import spectral  # noqa: E402
+
+
+def build():
+    src = os.path.join(HERE, "axg_oracle.cpp")
+    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        from axisem3d_b200 import _lib as L
+        O = C.CDLL(LIB_PATH)
+        V = C.c_void_p
+        sig = {
+            "axo_set_spectral": (C.c_int, [L.P_f64, L.P_f64]),
+            "axo_create": (V, [C.POINTER(L.axg_config)]),
+            "axo_destroy": (None, [V]),
+            "axo_last_error": (C.c_char_p, [V]),
+            "axo_set_solid_points": (C.c_int, [V, C.POINTER(L.axg_solid_points)]),
+            "axo_set_fluid_points": (C.c_int, [V, C.POINTER(L.axg_fluid_points)]),
+            "axo_set_solid_elements": (C.c_int, [V, C.POINTER(L.axg_solid_elements)]),
+            "axo_set_fluid_elements": (C.c_int, [V, C.POINTER(L.axg_fluid_elements)]),
+            "axo_set_solid_fluid": (C.c_int, [V, C.POINTER(L.axg_solid_fluid)]),
+            "axo_set_moment_sources": (C.c_int, [V, C.POINTER(L.axg_moment_sources)]),
+            "axo_set_force_sources": (C.c_int, [V, C.POINTER(L.axg_force_sources)]),
+            "axo_set_stations": (C.c_int, [V, C.POINTER(L.axg_stations), C.c_int]),
+            "axo_apply_sources": (C.c_int, [V, C.c_int]),
+            "axo_compute_stiffness": (C.c_int, [V, C.c_int]),
+            "axo_bc_before": (C.c_int, [V]),
+            "axo_bc_after": (C.c_int, [V]),
+            "axo_stiff_to_accel": (C.c_int, [V]),
+            "axo_newmark": (C.c_int, [V]),
+            "axo_record": (C.c_int, [V, C.c_int]),
+            "axo_run": (C.c_int, [V, C.c_int, C.c_int]),
+            "axo_get_field": (C.c_int, [V, C.c_int, C.c_int, L.P_f64]),
+            "axo_set_field": (C.c_int, [V, C.c_int, C.c_int, L.P_f64]),
+            "axo_field_size": (C.c_int64, [V, C.c_int]),
+            "axo_get_seismograms": (C.c_int, [V, L.P_f64]),
+            "axo_reset_attenuation": (C.c_int, [V]),
+            "axo_current_step": (C.c_int, [V]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(O, name)
+            f.restype = res
+            f.argtypes = args
+        t = spectral.tables()
+        gll = np.ascontiguousarray(t["gGLL"])
+        glj = np.ascontiguousarray(t["gGLJ"])
+        O.axo_set_spectral(gll.ctypes.data_as(L.P_f64), glj.ctypes.data_as(L.P_f64))
+        _lib = O
+    return _lib
+
+
+class Oracle:
+    """CPU restatement of the time loop; precision 'fp64' (default) or 'fp32'."""
+
+    def __init__(self, model, precision="fp64", threads=1):
+        from axisem3d_b200 import _lib as L
+        self.O = lib()
+        self.L = L
+        self.model = model
+        self.threads = threads
+        cfg = model.config("fp32" if precision == "fp32" else "fp64")
+        self.h = self.O.axo_create(C.byref(cfg))
+        if not self.h:
+            raise RuntimeError("oracle: spectral tables not set")
+        s = model.c_structs()
+        self._keep = s
+        self._chk(self.O.axo_set_solid_points(self.h, C.byref(s["sp"])))
+        self._chk(self.O.axo_set_fluid_points(self.h, C.byref(s["fp"])))
+        self._chk(self.O.axo_set_solid_elements(self.h, C.byref(s["se"])))
+        self._chk(self.O.axo_set_fluid_elements(self.h, C.byref(s["fe"])))
+        self._chk(self.O.axo_set_solid_fluid(self.h, C.byref(s["sf"])))
+        self._chk(self.O.axo_set_moment_sources(self.h, C.byref(s["ms"])))
+        self._chk(self.O.axo_set_force_sources(self.h, C.byref(s["fs"])))
+        self._chk(self.O.axo_set_stations(self.h, C.byref(s["st"]), int(model.st_interval)))
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.O.axo_last_error(self.h).decode())
+
+    def close(self):
+        if self.h:
+            self.O.axo_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def apply_sources(self, tstep):
+        self._chk(self.O.axo_apply_sources(self.h, int(tstep)))
+
+    def compute_stiffness(self):
+        self._chk(self.O.axo_compute_stiffness(self.h, int(self.threads)))
+
+    def apply_bc_before_assembly(self):
+        self._chk(self.O.axo_bc_before(self.h))
+
+    def apply_bc_after_assembly(self):
+        self._chk(self.O.axo_bc_after(self.h))
+
+    def stiff_to_accel(self):
+        self._chk(self.O.axo_stiff_to_accel(self.h))
+
+    def newmark_update(self):
+        self._chk(self.O.axo_newmark(self.h))
+
+    def record_stations(self, tstep):
+        self._chk(self.O.axo_record(self.h, int(tstep)))
+
+    def run(self, nsteps):
+        self._chk(self.O.axo_run(self.h, int(nsteps), int(self.threads)))
+
+    def reset_attenuation(self):
+        self._chk(self.O.axo_reset_attenuation(self.h))
+
+    def field_size(self, solid=True):
+        return int(self.O.axo_field_size(self.h, int(bool(solid))))
+
+    def get_field(self, which="displ", solid=True):
+        w = {"stiff": 0, "displ": 1, "veloc": 2, "accel": 3}[which]
+        out = np.zeros(self.field_size(solid), dtype=np.complex128)
+        if out.size:
+            self._chk(self.O.axo_get_field(self.h, int(bool(solid)), w,
+                                           out.view(np.float64).ctypes.data_as(self.L.P_f64)))
+        return out
+
+    def set_field(self, values, which="displ", solid=True):
+        w = {"stiff": 0, "displ": 1, "veloc": 2, "accel": 3}[which]
+        v = np.ascontiguousarray(values, dtype=np.complex128)
+        assert v.size == self.field_size(solid)
+        self._chk(self.O.axo_set_field(self.h, int(bool(solid)), w,
+                                       v.view(np.float64).ctypes.data_as(self.L.P_f64)))
+
+    def seismograms(self):
+        n = self.O.axo_get_seismograms(self.h, None)
+        ns = len(self.model.st_elem)
+        out = np.zeros((n, ns, 3))
+        if n and ns:
+            self.O.axo_get_seismograms(self.h, out.ctypes.data_as(self.L.P_f64))
+        return out

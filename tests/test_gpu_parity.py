@@ -1,0 +1,220 @@
+"""GPU parity: the CUDA engine, called through the C ABI, against the FP64 oracle.
+
+Tolerances (relative L2 over all point modes, stated per test):
+  per-step stiffness    FP64 engine <= 1e-12, FP32 / mixed engine <= 1e-6
+  full steps            FP64 <= 1e-11; FP32 / mixed <= 1e-5 after 5 steps
+  seismograms           every precision <= 1e-4 after the full plain-forward run
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_STIFF = {"fp64": 1e-12, "fp32": 1e-6, "mixed": 1e-6}
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _case(name):
+    from axisem3d_b200 import meshgen
+    mb = meshgen.microbench_model
+    return {
+        "cart_iso_1d_axial": lambda: meshgen.cartesian_model(nx=6, nz=6, nr=5),
+        "cart_iso_1d_full": lambda: meshgen.cartesian_model(
+            nx=5, nz=4, nr=8, attenuation=dict(meshgen.default_sls(3), qkappa=57823.0, qmu=120.0)),
+        "tiso_3d_full": lambda: mb(n_elem=150, nr_max=64, seed=21),
+        "tiso_3d_full_axial": lambda: mb(n_elem=60, nr_max=32, seed=22, axial_column=True),
+        "tiso_1d_full": lambda: mb(n_elem=120, nr_max=64, seed=23, is3d=False),
+        "iso_3d_elastic": lambda: mb(n_elem=100, nr_max=48, seed=24, rheology="iso", attenuation=None),
+        "iso_1d_full_axial": lambda: mb(n_elem=60, nr_max=20, seed=25, rheology="iso", is3d=False,
+                                        axial_column=True),
+        "tiso_3d_cg4": lambda: mb(n_elem=60, nr_min=8, nr_max=8, seed=26, attenuation="cg4"),
+        "tiso_1d_cg4": lambda: mb(n_elem=60, nr_min=6, nr_max=6, seed=27, attenuation="cg4", is3d=False),
+        "aniso_3d": lambda: mb(n_elem=80, nr_max=40, seed=28, rheology="aniso", attenuation=None),
+        "aniso_1d_axial": lambda: mb(n_elem=60, nr_max=16, seed=29, rheology="aniso", attenuation=None,
+                                     is3d=False, axial_column=True),
+        "nr1_only": lambda: mb(n_elem=40, nr_min=1, nr_max=1, seed=30),
+    }[name]()
+
+
+CASES = ["cart_iso_1d_axial", "cart_iso_1d_full", "tiso_3d_full", "tiso_3d_full_axial", "tiso_1d_full",
+         "iso_3d_elastic", "iso_1d_full_axial", "tiso_3d_cg4", "tiso_1d_cg4", "aniso_3d",
+         "aniso_1d_axial", "nr1_only"]
+
+
+def _oracle_stiff(m, u, steps=1):
+    import oracle as O
+    o = O.Oracle(m, "fp64")
+    o.set_field(u, "displ")
+    for _ in range(steps):
+        o.set_field(np.zeros_like(u), "stiff")
+        o.compute_stiffness()
+    return o.get_field("stiff")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
+@pytest.mark.parametrize("case", CASES)
+def test_stiffness_parity(built, case, precision):
+    """Domain::computeStiffness through axg_compute_stiffness vs the FP64 oracle,
+    two evaluations in a row (the second exercises the attenuation memory)."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = _case(case)
+    u = meshgen.random_displacement(m, seed=5)
+    ref1 = _oracle_stiff(m, u, 1)
+    ref2 = _oracle_stiff(m, u, 2)
+    with Solver(m, precision) as s:
+        s.set_field(u, "displ")
+        s.compute_stiffness()
+        f1 = s.get_field("stiff")
+        s.set_field(np.zeros_like(u), "stiff")
+        s.compute_stiffness()
+        f2 = s.get_field("stiff")
+    assert rel(f1, ref1) <= TOL_STIFF[precision], rel(f1, ref1)
+    assert rel(f2, ref2) <= TOL_STIFF[precision], rel(f2, ref2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
+def test_large_nr_chunked_slices(built, precision):
+    """nr up to 128 (the spherical-shell workload): the slice phase is split over
+    points when shared memory is short."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver, EngineError
+    m = meshgen.microbench_model(n_elem=16, nr_min=90, nr_max=128, seed=31)
+    u = meshgen.random_displacement(m, seed=6)
+    ref = _oracle_stiff(m, u)
+    try:
+        s = Solver(m, precision)
+    except EngineError as e:
+        # FP64 with nr > ~100 does not fit one element's workspace in shared memory
+        assert precision == "fp64" and "shared memory" in str(e)
+        return
+    with s:
+        s.set_field(u, "displ")
+        s.compute_stiffness()
+        f = s.get_field("stiff")
+    assert rel(f, ref) <= TOL_STIFF[precision]
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("fp32", 1e-5), ("mixed", 1e-5)])
+def test_full_steps_parity(built, precision, tol):
+    """Five full Newmark steps (sources, stiffness, BCs, mass, update) with
+    attenuation, on the axis, vs the oracle's NewmarkTimeScheme loop."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.cartesian_model(nx=6, nz=6, nr=5,
+                                attenuation=dict(meshgen.default_sls(3), qkappa=57823.0, qmu=100.0))
+    u0 = meshgen.random_displacement(m, seed=8) * 1e-3
+    o = O.Oracle(m, "fp64")
+    o.set_field(u0, "displ")
+    o.run(5)
+    with Solver(m, precision) as s:
+        s.set_field(u0, "displ")
+        s.run(5, graph=True)
+        for f in ("displ", "veloc", "accel"):
+            assert rel(s.get_field(f), o.get_field(f)) <= tol, (f, rel(s.get_field(f), o.get_field(f)))
+        assert s.step == 5
+
+
+def test_graph_equals_eager_and_hooks(built):
+    """One CUDA graph per step == eager launches == the individual Domain hooks (FP64)."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.cartesian_model(nx=5, nz=5, nr=5)
+    u0 = meshgen.random_displacement(m, seed=9) * 1e-3
+    out = []
+    for mode in ("graph", "eager", "hooks"):
+        with Solver(m, "fp64") as s:
+            s.set_field(u0, "displ")
+            if mode == "hooks":
+                for t in range(4):
+                    s.apply_sources(t)
+                    s.compute_stiffness()
+                    s.apply_bc_before_assembly()
+                    s.record_stations(t)
+                    s.apply_bc_after_assembly()
+                    s.stiff_to_accel()
+                    s.newmark_update()
+            else:
+                s.run(4, graph=(mode == "graph"))
+            out.append((s.get_field("displ"), s.get_field("veloc")))
+    for d, v in out[1:]:
+        assert rel(d, out[0][0]) <= 1e-13 and rel(v, out[0][1]) <= 1e-13
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
+def test_seismograms_plain_forward(built, precision):
+    """Plain forward case (40 x 40 quads, nr = 5, axial moment tensor, 20 surface
+    receivers, 2000 steps): seismogram rel-L2 vs the FP64 oracle <= 1e-4."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.cartesian_model()
+    nsteps = 2000
+    ref = _reference_seismograms(m, nsteps)
+    with Solver(m, precision) as s:
+        s.run(nsteps, graph=True)
+        seis = s.seismograms()
+    assert seis.shape == ref.shape
+    err = rel(seis, ref)
+    assert err <= 1e-4, err
+
+
+_REF_CACHE = {}
+
+
+def _reference_seismograms(m, nsteps):
+    import oracle as O
+    key = (m.meta["workload"], nsteps)
+    if key not in _REF_CACHE:
+        o = O.Oracle(m, "fp64", threads=8)
+        o.run(nsteps)
+        _REF_CACHE[key] = o.seismograms()
+    return _REF_CACHE[key]
+
+
+def test_error_paths(built):
+    """Host-side validation: bad indices and out-of-order calls come back as
+    AXG_E_* codes with the reference-style message; nothing faults."""
+    import ctypes as C
+    from axisem3d_b200 import _lib as L, meshgen
+    from axisem3d_b200.solver import Solver, EngineError
+    m = meshgen.cartesian_model(nx=3, nz=3, nr=5)
+    bad = meshgen.cartesian_model(nx=3, nz=3, nr=5)
+    bad.se_pts = bad.se_pts.copy()
+    bad.se_pts[0, 0] = 10 ** 7
+    with pytest.raises(EngineError) as ei:
+        Solver(bad, "fp32")
+    assert ei.value.code == L.AXG_E_ARG and "||" in str(ei.value)
+    lib = L.lib()
+    h = C.c_void_p()
+    cfg = m.config("fp32")
+    assert lib.axg_create(C.byref(cfg), C.byref(h)) == 0
+    assert lib.axg_run(h, 1, 1) == L.AXG_E_STATE
+    assert b"finalize" in lib.axg_last_error(h)
+    lib.axg_destroy(h)
+    s = Solver(m, "fp32", stability_interval=1)
+    u = np.zeros(s.field_size())
+    u[0] = np.nan
+    s.set_field(u.astype(complex), "displ")
+    with pytest.raises(EngineError) as ei:
+        s.run(2)
+    assert ei.value.code == L.AXG_E_UNSTABLE
+    s.close()
+
+
+def test_launch_count_and_native_library(built):
+    """The run launches the engine's own kernels, from the in-tree library."""
+    from axisem3d_b200 import meshgen, _lib
+    from axisem3d_b200.solver import Solver
+    m = meshgen.cartesian_model(nx=4, nz=4, nr=5)
+    with Solver(m, "fp32") as s:
+        n0 = s.launch_count()
+        s.run(3, graph=True)
+        assert s.launch_count() - n0 >= 3 * 4
+    import os
+    maps = open("/proc/self/maps").read()
+    assert os.path.realpath(_lib.LIB_PATH) in maps

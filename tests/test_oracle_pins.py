@@ -1,0 +1,230 @@
+"""CPU tests: the oracle pinned against the reference's tables and analytic
+invariants, and the C-ABI library's exports (no GPU needed)."""
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden", "spectral_npol4.json")
+
+
+def _golden():
+    with open(GOLDEN) as f:
+        return json.load(f)["tables"]
+
+
+def test_spectral_tables_python_match_reference():
+    import spectral
+    g = _golden()
+    t = spectral.tables()
+    for k, v in g.items():
+        assert np.array_equal(np.asarray(v), t[k]), k
+
+
+def test_spectral_tables_engine_match_reference(built):
+    from axisem3d_b200.solver import spectral_tables
+    g = _golden()
+    t = spectral_tables()
+    for k, v in g.items():
+        assert np.array_equal(np.asarray(v), t[k]), k
+
+
+def test_capi_exports_every_declared_symbol(built):
+    import ctypes
+    hdr = open(os.path.join(ROOT, "include", "axg.h")).read()
+    names = sorted(set(re.findall(r"\b(axg_[a-z0-9_]+)\s*\(", hdr)))
+    assert len(names) > 30
+    lib = ctypes.CDLL(os.path.join(ROOT, "axisem3d_b200", "libaxg.so"))
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    from axisem3d_b200 import _lib
+    assert set(_lib.SIGNATURES) == set(names)
+
+
+def test_capi_rejects_bad_config(built):
+    import ctypes as C
+    from axisem3d_b200 import _lib as L
+    lib = L.lib()
+    h = C.c_void_p()
+    cfg = L.axg_config()
+    cfg.precision = 7
+    cfg.dt = 1.0
+    assert lib.axg_create(C.byref(cfg), C.byref(h)) == L.AXG_E_ARG
+    cfg.precision = L.AXG_FP32
+    cfg.dt = -1.0
+    assert lib.axg_create(C.byref(cfg), C.byref(h)) == L.AXG_E_ARG
+
+
+def test_quad_geometry_linear_square(built):
+    """dsdxii etc. of an axis-aligned 2 x 2 square and the integral factor w_i w_j detJ s."""
+    from axisem3d_b200.solver import quad_geometry, spectral_tables
+    g, sz = quad_geometry([10., 0., 12., 0., 12., 2., 10., 2.], axial=False)
+    t = spectral_tables()
+    assert np.allclose(g[0], 1.0) and np.allclose(g[3], 1.0)     # dsdxii = dzdeta = 1 (J = I)
+    assert np.allclose(g[1], 0.0) and np.allclose(g[2], 0.0)
+    w = np.outer(t["wGLL"], t["wGLL"]).ravel()
+    assert np.allclose(g[5], w * sz[0])
+    assert np.allclose(g[4], 1.0 / sz[0])
+
+
+def test_att_moduli_matches_numpy_restatement(built):
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import att_moduli
+    sls = meshgen.default_sls(3)
+    kp = np.linspace(1e11, 2e11, 7)
+    mu = np.linspace(5e10, 7e10, 7)
+    qk = np.full(7, 57823.0)
+    qm = np.linspace(80, 600, 7)
+    k2, m2, dk, dm = att_moduli(sls["w"], sls["y"], sls["fmin"], sls["fmax"], sls["fref"], qk, qm, kp, mu)
+    kna, kd, kat = meshgen.att_factors(qk, sls)
+    mna, md, mat = meshgen.att_factors(qm, sls)
+    assert np.allclose(k2, kp * kat, rtol=1e-14) and np.allclose(m2, mu * mat, rtol=1e-14)
+    assert np.allclose(dk, kp * kd, rtol=1e-14) and np.allclose(dm, mu * md, rtol=1e-14)
+
+
+# ------------------------------------------------------------ oracle invariants ---
+def _models():
+    from axisem3d_b200 import meshgen
+    return {
+        "cartesian_iso_1d": meshgen.cartesian_model(nx=4, nz=4, nr=5),
+        "tiso_3d_full": meshgen.microbench_model(n_elem=24, nr_max=24, seed=3),
+        "iso_3d_axial": meshgen.microbench_model(n_elem=24, nr_max=16, seed=4, rheology="iso",
+                                                 axial_column=True),
+        "aniso_3d": meshgen.microbench_model(n_elem=24, nr_max=16, seed=5, rheology="aniso",
+                                             attenuation=None),
+    }
+
+
+def _stiff(o, u, fresh=True):
+    """One stiffness evaluation; fresh=True clears the attenuation memory first."""
+    if fresh:
+        o.reset_attenuation()
+    o.set_field(u, "displ")
+    o.set_field(np.zeros_like(u), "stiff")
+    o.compute_stiffness()
+    return o.get_field("stiff")
+
+
+@pytest.mark.parametrize("name", ["cartesian_iso_1d", "tiso_3d_full", "iso_3d_axial", "aniso_3d"])
+def test_oracle_rigid_body_motion_has_no_stiffness(built, name):
+    """Rigid translation along z and rotation about z (mode 0) produce zero strain,
+    hence zero stiffness force, in every rheology and on the axis."""
+    import oracle as O
+    m = _models()[name]
+    o = O.Oracle(m, "fp64")
+    nu = np.asarray(m.sp_nr) // 2 + 1
+    first = np.concatenate([[0], np.cumsum(nu)[:-1]])
+    ref = np.linalg.norm(_stiff(o, __import__("axisem3d_b200").meshgen.random_displacement(m)))
+    u = np.zeros((int(nu.sum()), 3), complex)
+    u[first, 2] = 1.0                        # translation along z
+    f = _stiff(o, u.ravel())
+    assert np.linalg.norm(f) < 1e-11 * ref
+    u = np.zeros((int(nu.sum()), 3), complex)
+    u[first, 1] = m.sp_coords[:, 0] / np.max(m.sp_coords[:, 0])   # rotation about z: u_phi = omega s
+    f = _stiff(o, u.ravel())
+    assert np.linalg.norm(f) < 1e-11 * ref
+
+
+SYM_CASES = {
+    # name: (builder kwargs, Nyquist weight of the element transform)
+    "cartesian_iso_1d": (None, 2.0),
+    "tiso_1d_varying_nr": (dict(n_elem=30, nr_max=24, seed=3, is3d=False, attenuation=None), 2.0),
+    "tiso_3d_even_nr": (dict(n_elem=30, nr_min=8, nr_max=8, seed=3, attenuation=None), 4.0),
+    "aniso_3d_odd_nr": (dict(n_elem=30, nr_min=9, nr_max=9, seed=5, rheology="aniso",
+                             attenuation=None), 2.0),
+    "iso_3d_axial_even_nr": (dict(n_elem=30, nr_min=6, nr_max=6, seed=4, rheology="iso",
+                                  axial_column=True, attenuation=None), 4.0),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SYM_CASES))
+def test_oracle_stiffness_is_self_adjoint(built, name):
+    """<v, K u>_w == <u, K v>_w with the azimuthal weights w_0 = 1, w_a = 2, and
+    w_Nyquist = 4 where a 3-D element's transform halves/doubles its Nyquist mode
+    (SolverFFTW.hpp:101-172). With even-nr 3-D elements of different nr sharing a
+    point the reference's operator is not self-adjoint in any one such inner
+    product, so those cases use a uniform nr."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    kw, wn = SYM_CASES[name]
+    m = meshgen.cartesian_model(nx=4, nz=4, nr=5) if kw is None else meshgen.microbench_model(**kw)
+    o = O.Oracle(m, "fp64")
+    u = meshgen.random_displacement(m, seed=11)
+    v = meshgen.random_displacement(m, seed=12)
+    nr = np.asarray(m.sp_nr)
+    nu = nr // 2 + 1
+    w = np.concatenate([np.where(np.arange(k) == 0, 1.0,
+                                 np.where((np.arange(k) == k - 1) & (r % 2 == 0) & (k > 1), wn, 2.0))
+                        for k, r in zip(nu, nr)])
+    w = np.repeat(w, 3)
+    ku, kv = _stiff(o, u), _stiff(o, v)
+    a = np.sum(w * np.real(np.conj(v) * ku))
+    b = np.sum(w * np.real(np.conj(u) * kv))
+    assert abs(a - b) <= 1e-12 * np.linalg.norm(ku) * np.linalg.norm(v) * 4
+
+
+def test_oracle_3d_constant_slices_equal_1d(built):
+    """A 3-D element whose slices all carry the same moduli gives the 1-D result
+    (the Fourier <-> slice transforms are an exact round trip). Odd nr: for even
+    nr the slice transform drops the imaginary part of the Nyquist mode, which
+    the in-Fourier path keeps."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    m1 = meshgen.microbench_model(n_elem=20, nr_min=11, nr_max=11, seed=7, is3d=False, attenuation=None)
+    m3 = meshgen.microbench_model(n_elem=20, nr_min=11, nr_max=11, seed=7, is3d=False, attenuation=None)
+    ne = m1.n_solid_elements
+    mods = m1.se_moduli.reshape(ne, 5, 25)
+    chunks, off = [], []
+    o_ = 0
+    for e in range(ne):
+        nrs = int(m1.se_nr[e])
+        chunks.append(np.repeat(mods[e][:, None, :], nrs, axis=1).ravel())
+        off.append(o_)
+        o_ += chunks[-1].size
+    m3.se_moduli = np.concatenate(chunks)
+    m3.se_mat_off = np.array(off, np.int64)
+    m3.se_is3d = np.ones(ne, np.uint8)
+    u = meshgen.random_displacement(m1, seed=5)
+    f1 = _stiff(O.Oracle(m1, "fp64"), u)
+    f3 = _stiff(O.Oracle(m3, "fp64"), u)
+    assert np.linalg.norm(f3 - f1) <= 1e-13 * np.linalg.norm(f1)
+
+
+def test_oracle_sls_relaxes_to_relaxed_moduli(built):
+    """Held strain: the SLS memory variables converge to sum_l m_l = dsigma, so the
+    stress relaxes to the one of (lambda - dlambda, mu - dmu) without attenuation
+    (steady state of Attenuation::updateMem*, AttBuilder::setAlphaBetaGamma)."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    m = meshgen.microbench_model(n_elem=12, nr_max=9, seed=9, rheology="iso", is3d=False)
+    # fast relaxation so that steady state is reached in a few hundred evaluations
+    sls = meshgen.default_sls(3, fmin=5.0, fmax=50.0)
+    from axisem3d_b200.solver import att_alpha_beta_gamma
+    m.att_alpha, m.att_beta, m.att_gamma = att_alpha_beta_gamma(sls["w"], sls["y"], 0.01)
+    u = meshgen.random_displacement(m, seed=3)
+    o = O.Oracle(m, "fp64")
+    for _ in range(600):
+        f = _stiff(o, u, fresh=False)
+    ne = m.n_solid_elements
+    relaxed = meshgen.microbench_model(n_elem=12, nr_max=9, seed=9, rheology="iso", is3d=False)
+    mods = relaxed.se_moduli.reshape(ne, 2, 25).copy()
+    am = m.se_att_moduli.reshape(ne, 2, 25)
+    mods -= am
+    relaxed.se_moduli = mods.ravel()
+    relaxed.se_att = None
+    relaxed.nsls = 0
+    fr = _stiff(O.Oracle(relaxed, "fp64"), u)
+    assert np.linalg.norm(f - fr) <= 1e-9 * np.linalg.norm(fr)
+
+
+def test_oracle_fp32_close_to_fp64(built):
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    m = meshgen.microbench_model(n_elem=40, nr_max=32, seed=2)
+    u = meshgen.random_displacement(m, seed=1)
+    f64 = _stiff(O.Oracle(m, "fp64"), u)
+    f32 = _stiff(O.Oracle(m, "fp32"), u)
+    assert np.linalg.norm(f32 - f64) <= 1e-5 * np.linalg.norm(f64)
