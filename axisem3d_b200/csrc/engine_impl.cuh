@@ -100,7 +100,7 @@ class Engine final : public EngineBase {
     };
 
     struct SolidBucket {
-        int rheo, att, is3d, rtz, cls, team, tpc, qc, nr_max, n;
+        int rheo, att, is3d, rtz, cls, team, tpc, qc, nr_max, n, grid = 1;
         size_t team_bytes;
         DBuf<int> nr, pts;
         DBuf<uint8_t> axial;
@@ -181,6 +181,8 @@ public:
     // ------------------------------------------------------------ hooks ---
     void apply_sources(int tstep) override {
         need();
+        if (tstep < 0) throw Error(AXG_E_ARG, "Domain::applySources || negative time step.");
+        ensure_capacity(tstep + 1);   // the STF table must cover this step
         set_step(tstep);
         launch_sources();
     }
@@ -189,8 +191,9 @@ public:
     void point_stage(int mask) override { need(); launch_points(mask); }
     void record(int tstep) override {
         need();
-        set_step(tstep);
+        if (tstep < 0) throw Error(AXG_E_ARG, "Domain::recordOutput || negative time step.");
         ensure_capacity(tstep + 1);
+        set_step(tstep);
         launch_stations();
     }
 
@@ -588,8 +591,22 @@ private:
         while (tpc > 1 && (size_t)tpc * L.total > budget) tpc--;
         if (team > 32) tpc = std::min(tpc, 15);
         b.tpc = tpc;
-        AXG_CUDA(cudaFuncSetAttribute(b.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(tpc * L.total)));
+        raise_smem_limit((const void *)b.kernel, tpc * L.total);
+        // persistent grid: every SM holds as many CTAs as fit; the teams then walk the
+        // bucket, prefetching their next element into L2 while computing the current one
+        int per_sm = 0;
+        AXG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b.kernel, team * tpc,
+                                                               tpc * L.total));
+        b.grid = std::max(1, std::min((b.n + tpc - 1) / tpc, std::max(1, per_sm) * prop_.multiProcessorCount));
+    }
+
+    // several buckets can share one kernel instantiation: its dynamic shared
+    // memory limit must cover the largest of them
+    void raise_smem_limit(const void *kernel, size_t bytes) {
+        size_t &cur = smem_limit_[kernel];
+        if (bytes <= cur) return;
+        cur = bytes;
+        AXG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     }
 
     // ------------------------------------------------------- fluid buckets ---
@@ -652,8 +669,7 @@ private:
             while (tpc > 1 && (size_t)tpc * L.total > 200 * 1024) tpc--;
             if (team > 32) tpc = std::min(tpc, 15);
             b->tpc = tpc;
-            AXG_CUDA(cudaFuncSetAttribute(b->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)(tpc * L.total)));
+            raise_smem_limit((const void *)b->kernel, tpc * L.total);
             fb_.push_back(std::move(b));
         }
     }
@@ -777,6 +793,8 @@ private:
 
     // ------------------------------------------------------------ launches ---
     void launch_sources() {
+        if ((ms_n_ || fs_n_) && stf_cap_ <= 0)
+            throw Error(AXG_E_STATE, "Domain::applySources || source-time table not allocated.");
         if (ms_n_) {
             MomentArgs<T> a;
             a.nsrc = ms_n_; a.elem = ms_el_.p; a.nu = ms_nu_.p; a.pat_off = ms_po_.p;
@@ -812,8 +830,7 @@ private:
                 a.gamma[l] = (AT)cfg_.att_gamma[l];
             }
             a.gmat = gmat_.p;
-            int blocks = (b.n + b.tpc - 1) / b.tpc;
-            b.kernel<<<blocks, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc,
+            b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc,
                                                                               b.tpc, b.team_bytes);
             post_launch();
         }
@@ -936,6 +953,7 @@ private:
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
     int team_override_[5];
+    std::map<const void *, size_t> smem_limit_;
 
     DBuf<T> gmat_, tw_;
     DBuf<int> tw_off_;

@@ -156,24 +156,67 @@ void map_linear(const double *n, double xi, double eta, double &s, double &z, Ja
     }
 }
 
-// MappingSpherical (mapping/MappingSpherical.hpp) for quads whose curved outer
-// edge is edge 2 (nodes 2-3 on the outer circle, nodes 0-1 on the inner one)
-void map_spherical(const double *n, double xi, double eta, double &s, double &z, Jac &J) {
-    double r0 = std::hypot(n[0], n[1]), r2 = std::hypot(n[4], n[5]);
-    double t0 = std::atan2(n[0], n[1]), t1 = std::atan2(n[2], n[3]);
-    double t2 = std::atan2(n[4], n[5]), t3 = std::atan2(n[6], n[7]);
+// MappingSpherical (mapping/MappingSpherical.hpp): the curved outer edge is
+// found from the nodal radii, the quad is rotated by Q2 so that edge lies on
+// edge 2 (Mapping::rotateQ2), mapped there, and rotated back.
+const double kQ2[4][4] = {{-1., 0., 0., -1.}, {0., -1., 1., 0.}, {1., 0., 0., 1.}, {0., 1., -1., 0.}};
+
+inline int cycle4(int p) { return p > 3 ? p - 4 : (p < 0 ? p + 4 : p); }
+
+inline void angles_close(double &a, double &b) {
+    if (a - b > M_PI) b += 2. * M_PI;
+    if (b - a > M_PI) a += 2. * M_PI;
+}
+
+int curved_outer(const double *n) {
+    double r[4], e[4];
+    for (int k = 0; k < 4; k++) r[k] = std::hypot(n[2 * k], n[2 * k + 1]);
+    for (int k = 0; k < 4; k++) {
+        int k1 = (k + 1) % 4;
+        e[k] = std::hypot(n[2 * k] - n[2 * k1], n[2 * k + 1] - n[2 * k1 + 1]);
+    }
+    double tol = std::min(std::min(e[0], e[1]), std::min(e[2], e[3])) * 1e-3;
+    if (std::fabs(r[0] - r[1]) < tol && std::fabs(r[2] - r[3]) < tol) return r[2] > r[0] ? 2 : 0;
+    if (std::fabs(r[1] - r[2]) < tol && std::fabs(r[3] - r[0]) < tol) return r[3] > r[1] ? 3 : 1;
+    return -1;
+}
+
+void map_spherical(const double *n, int co, double xi0, double eta0, double &s, double &z, Jac &J) {
+    const double *Q = kQ2[co];
+    double rt[2][4];
+    for (int k = 0; k < 4; k++) {
+        double sq = Q[0] * n[2 * k] + Q[1] * n[2 * k + 1];
+        double zq = Q[2] * n[2 * k] + Q[3] * n[2 * k + 1];
+        rt[0][k] = std::hypot(sq, zq);
+        rt[1][k] = M_PI * .5 - std::atan2(zq, sq);   // angle from the z axis
+    }
+    double xi = Q[0] * xi0 + Q[1] * eta0, eta = Q[2] * xi0 + Q[3] * eta0;
+    double r0 = rt[0][cycle4(co - 2)], r2 = rt[0][cycle4(co)];
+    double t0 = rt[1][cycle4(co - 2)], t1 = rt[1][cycle4(co - 1)];
+    double t2 = rt[1][cycle4(co)], t3 = rt[1][cycle4(co + 1)];
+    angles_close(t3, t2);
+    angles_close(t0, t1);
     double t01 = ((1. - xi) * t0 + (1. + xi) * t1) * .5;
     double t32 = ((1. - xi) * t3 + (1. + xi) * t2) * .5;
     double r0m = (1. - eta) * r0 * .5;
     double r2p = (1. + eta) * r2 * .5;
     double t01_xi = (t1 - t0) * .5, t32_xi = (t2 - t3) * .5;
     double r0m_eta = -r0 * .5, r2p_eta = r2 * .5;
-    s = r0m * std::sin(t01) + r2p * std::sin(t32);
-    z = r0m * std::cos(t01) + r2p * std::cos(t32);
-    J.J00 = r0m * std::cos(t01) * t01_xi + r2p * std::cos(t32) * t32_xi;
-    J.J10 = (r0m * std::sin(t01) * t01_xi + r2p * std::sin(t32) * t32_xi) * (-1.);
-    J.J01 = r0m_eta * std::sin(t01) + r2p_eta * std::sin(t32);
-    J.J11 = r0m_eta * std::cos(t01) + r2p_eta * std::cos(t32);
+    double sq = r0m * std::sin(t01) + r2p * std::sin(t32);
+    double zq = r0m * std::cos(t01) + r2p * std::cos(t32);
+    double j00 = r0m * std::cos(t01) * t01_xi + r2p * std::cos(t32) * t32_xi;
+    double j10 = (r0m * std::sin(t01) * t01_xi + r2p * std::sin(t32) * t32_xi) * (-1.);
+    double j01 = r0m_eta * std::sin(t01) + r2p_eta * std::sin(t32);
+    double j11 = r0m_eta * std::cos(t01) + r2p_eta * std::cos(t32);
+    // back: sz = Q^T sz', J = Q^T J' Q
+    s = Q[0] * sq + Q[2] * zq;
+    z = Q[1] * sq + Q[3] * zq;
+    double a00 = Q[0] * j00 + Q[2] * j10, a01 = Q[0] * j01 + Q[2] * j11;
+    double a10 = Q[1] * j00 + Q[3] * j10, a11 = Q[1] * j01 + Q[3] * j11;
+    J.J00 = a00 * Q[0] + a01 * Q[2];
+    J.J01 = a00 * Q[1] + a01 * Q[3];
+    J.J10 = a10 * Q[0] + a11 * Q[2];
+    J.J11 = a10 * Q[1] + a11 * Q[3];
 }
 
 }  // namespace
@@ -197,12 +240,10 @@ int axg_spectral_tables(double *xgll, double *xglj, double *wgll, double *wglj, 
 int axg_quad_geometry(int32_t mapping, const double *nodal_sz, int32_t axial,
                       double *out_geometry, double *out_sz) {
     if (!nodal_sz || !out_geometry) return AXG_E_ARG;
+    int co = -1;
     if (mapping == AXG_MAP_SPHERICAL) {
-        double rin0 = std::hypot(nodal_sz[0], nodal_sz[1]), rin1 = std::hypot(nodal_sz[2], nodal_sz[3]);
-        double rout2 = std::hypot(nodal_sz[4], nodal_sz[5]), rout3 = std::hypot(nodal_sz[6], nodal_sz[7]);
-        double tol = 1e-9 * std::max(rout2, 1.0);
-        if (std::fabs(rin0 - rin1) > tol || std::fabs(rout2 - rout3) > tol || !(rout2 > rin0))
-            return AXG_E_UNSUPPORTED;
+        co = curved_outer(nodal_sz);
+        if (co < 0) return AXG_E_ARG;   // "Error identifying curved outer edge."
     } else if (mapping != AXG_MAP_LINEAR) {
         return AXG_E_ARG;
     }
@@ -218,7 +259,7 @@ int axg_quad_geometry(int32_t mapping, const double *nodal_sz, int32_t axial,
             double s, z;
             Jac J;
             if (mapping == AXG_MAP_LINEAR) map_linear(nodal_sz, xi, eta, s, z, J);
-            else map_spherical(nodal_sz, xi, eta, s, z, J);
+            else map_spherical(nodal_sz, co, xi, eta, s, z, J);
             double det = J.J00 * J.J11 - J.J01 * J.J10;
             double f = w_xi[ipol] * t.wGLL[jpol] * det;
             if (axial) f *= (ipol == 0) ? J.J00 : s / (1. + xi);

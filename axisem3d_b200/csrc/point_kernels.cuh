@@ -267,11 +267,12 @@ __global__ void moment_source_kernel(const MomentArgs<T> a) {
     __shared__ C sS[3][6][25];     // at most 3 modes on the axis; loop for more
     __shared__ C sA[3][3][25];
     __shared__ int sOff[25], sNu[25];
+    if (a.stf_steps <= 0 || a.stf == nullptr) return;
     const int e = a.elem[s];
     const int enu = a.e_nr[e] / 2 + 1;
     const int nuco = min(enu, a.nu[s]);
     const bool axial = a.e_axial[e] != 0;
-    const int st = min(*a.step, a.stf_steps - 1);
+    const int st = max(0, min(*a.step, a.stf_steps - 1));
     const T v = a.stf[(size_t)st * a.nsrc + s];
     for (int i = threadIdx.x; i < 25; i += blockDim.x) {
         sGll[i] = a.gmat[i]; sGlj[i] = a.gmat[25 + i];
@@ -355,9 +356,9 @@ struct ForceArgs {
 template <class T>
 __global__ void force_source_kernel(const ForceArgs<T> a) {
     const int s = blockIdx.x;
-    if (s >= a.nsrc) return;
+    if (s >= a.nsrc || a.stf_steps <= 0 || a.stf == nullptr) return;
     const int e = a.elem[s];
-    const int st = min(*a.step, a.stf_steps - 1);
+    const int st = max(0, min(*a.step, a.stf_steps - 1));
     const T v = a.stf[(size_t)st * a.nsrc + s];
     for (int i = threadIdx.x; i < a.nu[s] * 25; i += blockDim.x) {
         const int al = i / 25, q = i % 25;
@@ -391,7 +392,7 @@ __global__ void station_kernel(const StationArgs<T> a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.nst * 3) return;
     const int step = *a.step;
-    if (step % a.interval != 0) return;
+    if (step < 0 || a.out == nullptr || step % a.interval != 0) return;
     const int rec = step / a.interval;
     if (rec >= a.max_rec) return;
     const int s = t / 3, c = t % 3;

@@ -244,6 +244,30 @@ __device__ __forceinline__ void attenuate(const SolidArgs<T, AT> &a, AT *state, 
     }
 }
 
+// L2 prefetch of [p, p + bytes), 128-byte lines spread over the team; every
+// address issued lies inside the region (lines are aligned down only at the start,
+// and pools are 256-byte aligned allocations)
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes, int lane, int team) {
+    const uintptr_t a1 = (uintptr_t)p + bytes;
+    uintptr_t a = ((uintptr_t)p & ~(uintptr_t)127) + (uintptr_t)lane * 128;
+    for (; a < a1; a += (uintptr_t)team * 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+}
+
+// bytes of the per-element streams (geometry, moduli, attenuation moduli, state)
+template <class T, class AT, int RHEO, int ATT, bool IS3D>
+__device__ __forceinline__ void prefetch_element(const SolidArgs<T, AT> &a, int e, int lane, int team) {
+    const int nr = a.nr[e], nu = nr / 2 + 1, ns = IS3D ? nr : 1;
+    constexpr int nmod = RHEO == RHEO_ISO ? 2 : RHEO == RHEO_TISO ? 5 : 21;
+    prefetch_l2(a.geom + (size_t)e * 250, 250 * sizeof(T), lane, team);
+    prefetch_l2(a.mod + a.mod_off[e], (size_t)nmod * ns * 25 * sizeof(T), lane, team);
+    if constexpr (ATT != ATT_NONE) {
+        constexpr int npa = ATT == ATT_CG4 ? 4 : 25;
+        prefetch_l2(a.attmod + a.att_off[e], (size_t)2 * ns * npa * sizeof(T), lane, team);
+        const size_t slots = IS3D ? (size_t)nr * npa : (size_t)nu * npa * 2;
+        prefetch_l2(a.state + a.state_off[e], (size_t)(a.nsls + 1) * 6 * slots * sizeof(AT), lane, team);
+    }
+}
+
 __device__ __forceinline__ int cg4_slot(int q) {
     // (1,1) (1,3) (3,1) (3,3) -> 0..3, else -1
     return q == 6 ? 0 : q == 8 ? 1 : q == 16 ? 2 : q == 18 ? 3 : -1;
@@ -286,11 +310,16 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
     const T *dsdxii_if = sGeo + 125, *dsdeta_if = sGeo + 150, *dzdxii_if = sGeo + 175,
             *dzdeta_if = sGeo + 200, *invs_if = sGeo + 225;
 
-    for (int e = blockIdx.x * teams_per_cta + team; e < a.n_elem; e += gridDim.x * teams_per_cta) {
+    const int stride = gridDim.x * teams_per_cta;
+    if (blockIdx.x * teams_per_cta + team < a.n_elem)
+        prefetch_element<T, AT, RHEO, ATT, IS3D>(a, blockIdx.x * teams_per_cta + team, lane, TEAM);
+    for (int e = blockIdx.x * teams_per_cta + team; e < a.n_elem; e += stride) {
         const int nr = a.nr[e];
         const int nu = nr / 2 + 1;
         const bool axial = a.axial[e] != 0;
         const T *Gxi = axial ? sGlj : sGll;
+        // the next element of this team streams into L2 while this one computes
+        if (e + stride < a.n_elem) prefetch_element<T, AT, RHEO, ATT, IS3D>(a, e + stride, lane, TEAM);
 
         // ---------------- element header -> shared memory ----------------
         for (int i = lane; i < 250; i += TEAM) sGeo[i] = a.geom[(size_t)e * 250 + i];

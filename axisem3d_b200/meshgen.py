@@ -501,3 +501,366 @@ def random_displacement(model, seed=2, solid=True):
     last = first[even] + nu[even] - 1
     u[last, :] = u[last, :].real
     return u.ravel()
+
+
+# ------------------------------------------------------- spherical shell ---
+def layered_background(seed=11, r_cmb=3480e3, r_fluid_top=3600e3, r_surface=6371e3, nlayers=6):
+    """Seeded piecewise-linear 1-D table (radius -> rho, vp, vs): a fluid layer above
+    the inner boundary, then `nlayers` solid layers whose end values are perturbed
+    by 2 % around a smooth mantle-like trend."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rs = np.linspace(r_fluid_top, r_surface, nlayers + 1)
+    x = (rs - r_fluid_top) / (r_surface - r_fluid_top)
+    rho = (5.5e3 - 2.2e3 * x) * (1 + 0.02 * rng.uniform(-1, 1, x.size))
+    vp = (13.7e3 - 5.7e3 * x) * (1 + 0.02 * rng.uniform(-1, 1, x.size))
+    vs = (7.2e3 - 2.7e3 * x) * (1 + 0.02 * rng.uniform(-1, 1, x.size))
+    fluid = {"r": np.array([r_cmb, r_fluid_top]), "rho": np.array([9.9e3, 9.9e3]),
+             "vp": np.array([8.06e3, 8.0e3])}
+    return {"solid": {"r": rs, "rho": rho, "vp": vp, "vs": vs}, "fluid": fluid}
+
+
+def _interp(table, key, r):
+    return np.interp(r, table["r"], table[key])
+
+
+class GaussianField:
+    """Isotropic Gaussian random field with Gaussian correlation of length L,
+    by random Fourier features: f(x) = sigma sqrt(2/M) sum_m cos(k_m . x + p_m)."""
+
+    def __init__(self, sigma, length, seed, nfeatures=24):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        self.k = rng.normal(0.0, 1.0 / length, (nfeatures, 3))
+        self.p = rng.uniform(0, 2 * np.pi, nfeatures)
+        self.a = sigma * math.sqrt(2.0 / nfeatures)
+
+    def __call__(self, x, y, z):
+        out = np.zeros(np.broadcast(x, y, z).shape)
+        for k, p in zip(self.k, self.p):
+            out += np.cos(k[0] * x + k[1] * y + k[2] * z + p)
+        return self.a * out
+
+
+def spherical_model(n_theta=96, n_solid_layers=24, n_fluid_layers=2, r_cmb=3480e3, r_fluid_top=3600e3,
+                    r_surface=6371e3, nr_min=3, nr_max=128, dlnvs=0.02, corr_length=200e3, three_d=True,
+                    q_mu=300.0, q_kappa=57823.0, attenuation="cg4", rheology="iso", period=20.0,
+                    source_depth=100e3, nstations=20, courant=0.6, seed=12, nr_scale=1.0,
+                    aniso_pert=0.05, record_interval=1):
+    """Half-annulus r in [r_cmb, r_surface], theta in [0, pi] (axis at both ends), with
+    a fluid layer r in [r_cmb, r_fluid_top] (FluidElement, scalar potential) coupled to
+    the solid above, spherical mapping, a seeded 1-D layered background and (three_d)
+    a Gaussian random-field dlnVs sampled on each element's phi slices. Element nr
+    grows with the distance from the axis, nr = clip(round(nr_scale * pi s / L), nr_min,
+    nr_max) at the element centre, and points take the minimum over their elements.
+    rheology 'aniso' carries 21 Cij: the isotropic background plus a seeded
+    positive-definite perturbation of relative size aniso_pert."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    bg = layered_background(seed, r_cmb, r_fluid_top, r_surface)
+    r_edges = np.concatenate([np.linspace(r_cmb, r_fluid_top, n_fluid_layers + 1)[:-1],
+                              np.linspace(r_fluid_top, r_surface, n_solid_layers + 1)])
+    nl = n_fluid_layers + n_solid_layers
+    t_edges = np.linspace(0.0, np.pi, n_theta + 1)
+    nJ = 4 * nl + 1
+    ne = n_theta * nl
+    # element nodes; the south-axis column is rotated so that its axis edge is xi = -1
+    nodal = np.zeros((ne, 8))
+    axial = np.zeros(ne, np.uint8)
+    pts = np.zeros((ne, 25), np.int64)
+    ei = np.zeros(ne, np.int64)
+    ej = np.zeros(ne, np.int64)
+    ip = np.arange(5)
+    for i in range(n_theta):
+        for j in range(nl):
+            e = i * nl + j
+            ei[e], ej[e] = i, j
+            t0_, t1_ = t_edges[i], t_edges[i + 1]
+            r0_, r1_ = r_edges[j], r_edges[j + 1]
+            sz = lambda t, r: (r * math.sin(t), r * math.cos(t))  # noqa: E731
+            if i == n_theta - 1 and n_theta > 1:
+                # nodes: (pi, r1) (t0, r1) (t0, r0) (pi, r0): curved outer = edge 0
+                nodes = [sz(t1_, r1_), sz(t0_, r1_), sz(t0_, r0_), sz(t1_, r0_)]
+                I = 4 * i + 4 - ip[:, None]
+                J = 4 * j + 4 - ip[None, :]
+                axial[e] = 1
+            else:
+                nodes = [sz(t0_, r0_), sz(t1_, r0_), sz(t1_, r1_), sz(t0_, r1_)]
+                I = 4 * i + ip[:, None]
+                J = 4 * j + ip[None, :]
+                axial[e] = 1 if i == 0 else 0
+            nodal[e] = np.array(nodes).ravel()
+            pts[e] = (I * nJ + J).ravel()
+    nodal[:, 0::2] = np.where(np.abs(nodal[:, 0::2]) < 1e-6, 0.0, nodal[:, 0::2])
+    geom, szp = geometry_batch(nodal, axial, L.AXG_MAP_SPHERICAL)
+    fluid_e = ej < n_fluid_layers
+    # split global GLL points into solid and fluid sets
+    gmax = (4 * n_theta + 1) * nJ
+    sid = -np.ones(gmax, np.int64)
+    fid = -np.ones(gmax, np.int64)
+    sp_used = np.unique(pts[~fluid_e].ravel())
+    fp_used = np.unique(pts[fluid_e].ravel())
+    sid[sp_used] = np.arange(len(sp_used))
+    fid[fp_used] = np.arange(len(fp_used))
+    coords = np.zeros((gmax, 2))
+    coords[pts.ravel(), 0] = szp[:, 0, :].ravel()
+    coords[pts.ravel(), 1] = szp[:, 1, :].ravel()
+    coords[:, 0] = np.where(np.abs(coords[:, 0]) < 1e-6, 0.0, coords[:, 0])
+    # element nr from the distance to the axis
+    sc = np.mean(szp[:, 0, :], axis=1)
+    enr = np.clip(np.rint(nr_scale * np.pi * sc / corr_length), nr_min, nr_max).astype(np.int32)
+    pnr = np.full(gmax, nr_max + 1, np.int64)
+    np.minimum.at(pnr, pts.ravel(), np.repeat(enr, 25))
+    enr = np.max(pnr[pts], axis=1).astype(np.int32)
+    sel_s, sel_f = np.nonzero(~fluid_e)[0], np.nonzero(fluid_e)[0]
+    field = GaussianField(dlnvs, corr_length, seed + 1)
+    sls = default_sls(3, fmin=1.0 / (4 * period), fmax=4.0 / period)
+    m = Model(dt=1.0)
+    # ---- solid elements: moduli per point (1-D) or per (slice, point) (3-D)
+    nss = enr[sel_s] if three_d else np.ones(len(sel_s), np.int32)
+    nmod = {"iso": 2, "aniso": 21}[rheology]
+    mat_off = np.zeros(len(sel_s), np.int64)
+    mat_off[1:] = np.cumsum(nmod * nss * 25)[:-1]
+    moduli = np.zeros(int(np.sum(nmod * nss * 25)))
+    npa = 4 if attenuation == "cg4" else 25
+    att_off = np.zeros(len(sel_s), np.int64)
+    att_off[1:] = np.cumsum(2 * nss * npa)[:-1]
+    att_mod = np.zeros(int(np.sum(2 * nss * npa))) if attenuation else None
+    wcg4 = weights_cg4(geom[sel_s, 5, :]) if attenuation == "cg4" else None
+    rho_pt = np.zeros((len(sel_s), 25))
+    vmax = 0.0
+    for k, e in enumerate(sel_s):
+        s_ = szp[e, 0, :]
+        z_ = szp[e, 1, :]
+        r_ = np.hypot(s_, z_)
+        rho0 = _interp(bg["solid"], "rho", r_)
+        vp0 = _interp(bg["solid"], "vp", r_)
+        vs0 = _interp(bg["solid"], "vs", r_)
+        rho_pt[k] = rho0
+        ns = int(nss[k])
+        if three_d:
+            phi = 2 * np.pi * np.arange(ns) / ns
+            x = s_[None, :] * np.cos(phi)[:, None]
+            y = s_[None, :] * np.sin(phi)[:, None]
+            vs = vs0[None, :] * (1.0 + field(x, y, z_[None, :]))
+        else:
+            vs = vs0[None, :] * np.ones((1, 25))
+        vp = np.broadcast_to(vp0[None, :], vs.shape)
+        rho = np.broadcast_to(rho0[None, :], vs.shape)
+        vmax = max(vmax, float(np.max(vp)))
+        lam, mu = isotropic_moduli(rho, vp, vs)
+        if rheology == "aniso":
+            C = aniso_moduli_from(lam, mu, rng, aniso_pert)
+            for c in range(21):
+                moduli[mat_off[k] + c * ns * 25: mat_off[k] + (c + 1) * ns * 25] = C[c].ravel()
+            continue
+        if attenuation == "full":
+            lam, mu, dl, dm = iso_with_attenuation(lam, mu, q_kappa, q_mu, sls)
+            att_mod[att_off[k]:att_off[k] + ns * 25] = dl.ravel()
+            att_mod[att_off[k] + ns * 25:att_off[k] + 2 * ns * 25] = dm.ravel()
+        elif attenuation == "cg4":
+            kp = lam + (2. / 3.) * mu
+            kp2, mu2, dl4, dm4 = cg4_correct(kp[None], np.array(mu)[None], q_kappa, q_mu, wcg4[k:k + 1], sls)
+            lam, mu = (kp2 - (2. / 3.) * mu2)[0], mu2[0]
+            att_mod[att_off[k]:att_off[k] + ns * 4] = dl4.ravel()
+            att_mod[att_off[k] + ns * 4:att_off[k] + 2 * ns * 4] = dm4.ravel()
+        moduli[mat_off[k]:mat_off[k] + ns * 25] = np.asarray(lam).ravel()
+        moduli[mat_off[k] + ns * 25:mat_off[k] + 2 * ns * 25] = np.asarray(mu).ravel()
+    # ---- fluid elements: K = 1 / rho (Material::createAcoustic), 1-D
+    K = np.zeros((len(sel_f), 25))
+    fmass_pt = np.zeros((len(sel_f), 25))
+    for k, e in enumerate(sel_f):
+        r_ = np.hypot(szp[e, 0, :], szp[e, 1, :])
+        rho = _interp(bg["fluid"], "rho", r_)
+        vp = _interp(bg["fluid"], "vp", r_)
+        vmax = max(vmax, float(np.max(vp)))
+        K[k] = 1.0 / rho
+        fmass_pt[k] = 1.0 / (rho * vp ** 2)          # Material::getMass, fluid branch
+    # ---- masses
+    nsp, nfp = len(sp_used), len(fp_used)
+    smass = np.zeros(nsp)
+    np.add.at(smass, sid[pts[sel_s]].ravel(), (rho_pt * geom[sel_s, 5, :]).ravel())
+    fmass = np.zeros(nfp)
+    np.add.at(fmass, fid[pts[sel_f]].ravel(), (fmass_pt * geom[sel_f, 5, :]).ravel())
+    # ---- solid-fluid coupling on r = r_fluid_top (Quad::setupGLL, computeNormal)
+    normal = np.zeros((gmax, 2))
+    wt = tables()
+    for e in np.concatenate([sel_s, sel_f]):
+        fl = fluid_e[e]
+        j = ej[e]
+        on = (fl and j == n_fluid_layers - 1) or ((not fl) and j == n_fluid_layers)
+        if not on:
+            continue
+        rotated = (ei[e] == n_theta - 1 and n_theta > 1)
+        # local edge on the interface: fluid top (r1), solid bottom (r0)
+        outer = fl
+        if not rotated:
+            edge = 2 if outer else 0
+        else:
+            edge = 0 if outer else 2
+        ed_pts = {0: [0, 5, 10, 15, 20], 2: [24, 19, 14, 9, 4]}[edge]
+        J = _jacobians(nodal[e], bool(axial[e]))
+        for q in ed_pts:
+            ipol, jpol = q // 5, q % 5
+            Jq = J[q]
+            if edge == 0:
+                n = np.array([Jq[1, 0], -Jq[0, 0]])
+            else:
+                n = np.array([-Jq[1, 0], Jq[0, 0]])
+            n = n * (wt["wGLJ"][ipol] if axial[e] else wt["wGLL"][ipol])
+            s_ = szp[e, 0, q]
+            if axial[e]:
+                xi = wt["pGLJ"][ipol]
+                n = n * (Jq[0, 0] if ipol == 0 else s_ / (1. + xi))
+            else:
+                n = n * s_
+            normal[pts[e, q]] += (n / 2.) if fl else (-n / 2.)
+    iface = np.intersect1d(sp_used, fp_used)
+    # ---- time step (Quad::computeDt with the solid-fluid factor 0.9, rounded)
+    dts = [quad_dt(szp[e], vmax) for e in range(ne)]
+    dt = round_dt(min(dts) * 0.9 * courant)
+    m.dt = dt
+    m.sp_nr = pnr[sp_used].astype(np.int32)
+    m.sp_mass = smass
+    m.sp_axial = (coords[sp_used, 0] == 0.0).astype(np.uint8)
+    m.sp_coords = coords[sp_used]
+    m.fp_nr = pnr[fp_used].astype(np.int32)
+    m.fp_mass = fmass
+    m.fp_axial = (coords[fp_used, 0] == 0.0).astype(np.uint8)
+    m.fp_surface = np.zeros(nfp, np.uint8)
+    m.se_nr = enr[sel_s]
+    m.se_pts = sid[pts[sel_s]].astype(np.int32)
+    m.se_axial = axial[sel_s]
+    m.se_geom = geom[sel_s]
+    m.se_rheo = np.full(len(sel_s), L.AXG_ANISO if rheology == "aniso" else L.AXG_ISO, np.int32)
+    m.se_rtz = np.full(len(sel_s), 1 if rheology == "aniso" else 0, np.uint8)
+    th = np.arctan2(szp[sel_s, 0, :], szp[sel_s, 1, :])
+    m.se_theta = th
+    m.se_is3d = np.full(len(sel_s), 1 if three_d else 0, np.uint8)
+    m.se_mat_off = mat_off
+    m.se_moduli = moduli
+    if attenuation and rheology != "aniso":
+        m.se_att = np.full(len(sel_s), L.AXG_ATT_CG4 if attenuation == "cg4" else L.AXG_ATT_FULL, np.int32)
+        m.se_att_off = att_off
+        m.se_att_moduli = att_mod
+        a, b, g = att_alpha_beta_gamma(sls["w"], sls["y"], dt)
+        m.nsls, m.att_alpha, m.att_beta, m.att_gamma = len(a), a, b, g
+    m.fe_nr = enr[sel_f]
+    m.fe_pts = fid[pts[sel_f]].astype(np.int32)
+    m.fe_axial = axial[sel_f]
+    m.fe_geom = geom[sel_f]
+    m.fe_is3d = np.zeros(len(sel_f), np.uint8)
+    m.fe_mat_off = np.arange(len(sel_f), dtype=np.int64) * 25
+    m.fe_moduli = K.ravel()
+    m.sf_solid = sid[iface].astype(np.int32)
+    m.sf_fluid = fid[iface].astype(np.int32)
+    m.sf_nsu = normal[iface, 0]
+    m.sf_nzu = normal[iface, 1]
+    m.sf_nsa = normal[iface, 0]
+    m.sf_nza = normal[iface, 1]
+    m.sf_mass_fluid = fmass[fid[iface]]
+    # ---- moment tensor on the north axis at the given depth, Ricker of the given period
+    mt = rng.normal(0.0, 1e20, 6)
+    r_src = r_surface - source_depth
+    jsrc = int(np.searchsorted(r_edges, r_src) - 1)
+    esrc = 0 * nl + jsrc
+    eta = 2.0 * (r_src - r_edges[jsrc]) / (r_edges[jsrc + 1] - r_edges[jsrc]) - 1.0
+    k_src = int(np.nonzero(sel_s == esrc)[0][0])
+    w = inplane_weights(-1.0, eta, True)
+    pat = moment_pattern_axial(mt, w, int(enr[esrc]) // 2 + 1, True)
+    hd = period / 2.0
+    m.ms_elem = np.array([k_src], np.int32)
+    m.ms_nu = np.array([pat.shape[0]], np.int32)
+    m.ms_pat_off = np.array([0], np.int64)
+    m.ms_pattern = pat.ravel()
+    m.ms_stf = [STF(half_duration=hd, decay_factor=math.pi * hd / period, time_shift=0.0,
+                    derivative_order=2)]
+    m.t0 = -2.5 * hd
+    # ---- stations on the surface at theta in (0, pi)
+    st_e, st_w = [], []
+    for kk in range(1, nstations + 1):
+        t = np.pi * kk / (nstations + 1)
+        i = min(n_theta - 2, int(t / (np.pi / n_theta))) if n_theta > 1 else 0
+        e = i * nl + (nl - 1)
+        xi = 2.0 * (t - t_edges[i]) / (t_edges[i + 1] - t_edges[i]) - 1.0
+        st_e.append(int(np.nonzero(sel_s == e)[0][0]))
+        st_w.append(inplane_weights(xi, 1.0, bool(axial[e])))
+    m.st_elem = np.array(st_e, np.int32)
+    m.st_w = np.array(st_w)
+    m.st_phi = np.zeros(nstations)
+    m.st_interval = record_interval
+    m.meta = {"workload": "spherical shell %dx%d (%d fluid layers) nr %d..%d %s %s" %
+              (n_theta, nl, n_fluid_layers, int(enr.min()), int(enr.max()), rheology,
+               "3D" if three_d else "1D"), "seed": seed}
+    return m
+
+
+def _jacobians(nodal, axial):
+    """Jacobian d(s,z)/d(xi,eta) at the 25 points by central differences of the
+    spherical map (used for the solid-fluid normals)."""
+    t = tables()
+    xn = t["pGLJ"] if axial else t["pGLL"]
+    out = np.zeros((25, 2, 2))
+    eps = 1e-6
+    for ip in range(5):
+        for jp in range(5):
+            xi, eta = xn[ip], t["pGLL"][jp]
+            cols = []
+            for dx, de in ((eps, 0.0), (0.0, eps)):
+                a = _sph_map(nodal, xi + dx, eta + de)
+                b = _sph_map(nodal, xi - dx, eta - de)
+                cols.append((a - b) / (2 * eps))
+            out[ip * 5 + jp] = np.array(cols).T
+    return out
+
+
+def _sph_map(nodal, xi, eta):
+    """Point of the spherical map (MappingSpherical::mapping) at (xi, eta)."""
+    n = np.asarray(nodal).reshape(4, 2)
+    r = np.hypot(n[:, 0], n[:, 1])
+    if abs(r[0] - r[1]) < 1e-6 * r.max() and abs(r[2] - r[3]) < 1e-6 * r.max():
+        co = 2 if r[2] > r[0] else 0
+    else:
+        co = 3 if r[3] > r[1] else 1
+    Q = {0: np.array([[-1., 0.], [0., -1.]]), 1: np.array([[0., -1.], [1., 0.]]),
+         2: np.eye(2), 3: np.array([[0., 1.], [-1., 0.]])}[co]
+    nq = n @ Q.T
+    rr = np.hypot(nq[:, 0], nq[:, 1])
+    th = np.pi / 2 - np.arctan2(nq[:, 1], nq[:, 0])
+    xq, eq = Q @ np.array([xi, eta])
+    c = lambda p: p % 4  # noqa: E731
+    r0, r2 = rr[c(co - 2)], rr[c(co)]
+    t0, t1, t2, t3 = th[c(co - 2)], th[c(co - 1)], th[c(co)], th[c(co + 1)]
+    if t3 - t2 > np.pi:
+        t2 += 2 * np.pi
+    if t2 - t3 > np.pi:
+        t3 += 2 * np.pi
+    if t0 - t1 > np.pi:
+        t1 += 2 * np.pi
+    if t1 - t0 > np.pi:
+        t0 += 2 * np.pi
+    t01 = ((1 - xq) * t0 + (1 + xq) * t1) * .5
+    t32 = ((1 - xq) * t3 + (1 + xq) * t2) * .5
+    r0m, r2p = (1 - eq) * r0 * .5, (1 + eq) * r2 * .5
+    sz = np.array([r0m * np.sin(t01) + r2p * np.sin(t32), r0m * np.cos(t01) + r2p * np.cos(t32)])
+    return Q.T @ sz
+
+
+def aniso_moduli_from(lam, mu, rng, pert):
+    """21 Cij per (slice, point): the isotropic tensor of (lam, mu) plus a seeded
+    symmetric perturbation of relative size `pert`, checked positive definite."""
+    lam = np.asarray(lam)
+    mu = np.asarray(mu)
+    shp = lam.shape
+    n = lam.size
+    C = np.zeros((n, 6, 6))
+    lf, mf = lam.ravel(), mu.ravel()
+    C[:, :3, :3] = lf[:, None, None]
+    for k in range(3):
+        C[:, k, k] = lf + 2 * mf
+        C[:, 3 + k, 3 + k] = mf
+    R = rng.normal(0.0, 1.0, (n, 6, 6))
+    R = 0.5 * (R + np.transpose(R, (0, 2, 1)))
+    C = C + pert * mf[:, None, None] * R / 3.0
+    ev = np.linalg.eigvalsh(C)
+    if np.min(ev) <= 0:
+        raise ValueError("perturbed Cij not positive definite")
+    iu = np.triu_indices(6)
+    return [C[:, a, b].reshape(shp) for a, b in zip(*iu)]

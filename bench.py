@@ -237,32 +237,49 @@ def time_steps(solver, steps, stream):
     return e0.elapsed_time(e1) / 1e3
 
 
+def log(msg):
+    sys.stderr.write("[bench %.1fs] %s\n" % (time.time() - T_START, msg))
+    sys.stderr.flush()
+
+
+T_START = time.time()
+
+
 def run_ours(args, world, rank, local):
     import torch
     from axisem3d_b200 import meshgen
     from axisem3d_b200.solver import Solver
     torch.cuda.set_device(local)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    log("building model")
     m = build_model(args, seed=1 + rank)
     U = m.updates_per_step()
+    log("model: %d elements, %d updates/step" % (m.n_solid_elements, U))
     s = Solver(m, args.precision, device=local)
+    log("solver finalized")
     s.set_stream(stream.cuda_stream)
     u0 = meshgen.random_displacement(m, seed=2 + rank) * 1e-6
     s.set_field(u0, "displ")
     clocks = ClockSampler(local)
     with clocks:
+        log("warmup")
         s.run(max(3, args.warmup), graph=True)
+        s.synchronize()
+        log("timed run")
         barrier(world)
         torch.cuda.synchronize()
         n0 = s.launch_count()
         t = time_steps(s, args.steps, stream)
         launches = s.launch_count() - n0
         t = dist_max(t, world)
+        log("stiffness timing")
         # stiffness kernels alone: per-step events around the solid stiffness launches
         s.set_timing(True)
         s.run(5, graph=False)
         kms, kn = s.stiffness_time()
         s.set_timing(False)
+        log("e2e")
         # end to end through the C ABI with host buffers
         nb = s.field_raw_bytes("displ")
         host = torch.empty(nb, dtype=torch.uint8, pin_memory=True)
@@ -292,6 +309,7 @@ def run_ours(args, world, rank, local):
            "clocks": clocks.summary(), "model": m}
     # FP64 run of the same workload (the metric compares FP32 and FP64 paths)
     if not args.no_fp64 and args.precision != "fp64":
+        log("fp64 run")
         s64 = Solver(m, "fp64", device=local)
         s64.set_stream(stream.cuda_stream)
         s64.set_field(u0, "displ")
@@ -304,6 +322,8 @@ def run_ours(args, world, rank, local):
 
 
 def main():
+    import faulthandler
+    faulthandler.enable()
     args = parse()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
@@ -321,6 +341,7 @@ def main():
         traffic = None
         if trafficd and trafficd.get("elements") == m.n_solid_elements:
             traffic = trafficd.get("dram_bytes_per_launch_group")
+        log("cpu baseline")
         cb = cpu_baseline(args, args.cpu_seconds)
         line = {
             "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,

@@ -427,10 +427,16 @@ struct Oracle : OracleBase {
         }
     }
 
-    const Twiddle<R> &twiddle(int nr) {
+    // twiddle tables are built up front (prepare_twiddles) so that the worker
+    // threads of compute_stiffness only read them
+    const Twiddle<R> &twiddle(int nr) const {
+        if ((int)tw.size() <= nr || tw[nr].nr != nr)
+            throw std::runtime_error("Oracle::twiddle || table for nr not prepared.");
+        return tw[nr];
+    }
+    void prepare_twiddle(int nr) {
         if ((int)tw.size() <= nr) tw.resize(nr + 1);
         if (tw[nr].nr != nr) tw[nr].set(nr);
-        return tw[nr];
     }
 
     static void make_ops(const double *g, bool axial, Ops<R> &o) {
@@ -457,9 +463,13 @@ struct Oracle : OracleBase {
 
     void set_solid_points(const axg_solid_points *p) override {
         sp.build(p->count, p->nr, p->mass_nr, p->mass_offset, p->mass, p->axial, nullptr, 3);
+        for (int q = 0; q < sp.n; q++)
+            if (sp.mass_nr[q] > 1) prepare_twiddle(sp.nr[q]);
     }
     void set_fluid_points(const axg_fluid_points *p) override {
         fp.build(p->count, p->nr, p->mass_nr, p->mass_offset, p->mass, p->axial, p->surface, 1);
+        for (int q = 0; q < fp.n; q++)
+            if (fp.mass_nr[q] > 1) prepare_twiddle(fp.nr[q]);
     }
 
     void set_solid_elements(const axg_solid_elements *e) override {
@@ -474,6 +484,7 @@ struct Oracle : OracleBase {
             el.att = e->attenuation ? e->attenuation[i] : AXG_ATT_NONE;
             el.rtz = e->rtz ? e->rtz[i] : 0;
             el.nslice = el.is3d ? el.nr : 1;
+            if (el.is3d) prepare_twiddle(el.nr);
             int nm = nmod_of(el.rheo);
             size_t cnt = (size_t)nm * el.nslice * N;
             el.mod.resize(cnt);
@@ -538,6 +549,7 @@ struct Oracle : OracleBase {
             make_ops(e->geometry + (size_t)i * 150, e->axial[i] != 0, el.ops);
             el.is3d = e->is3d ? e->is3d[i] : 0;
             el.nslice = el.is3d ? el.nr : 1;
+            if (el.is3d) prepare_twiddle(el.nr);
             el.K.resize((size_t)el.nslice * N);
             const double *m = e->moduli + e->mat_offset[i];
             for (size_t q = 0; q < el.K.size(); q++) el.K[q] = (R)m[q];
