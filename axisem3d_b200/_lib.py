@@ -32,7 +32,8 @@ class axg_config(C.Structure):
                 ("t0", C.c_double), ("nsls", C.c_int32),
                 ("att_alpha", C.c_double * AXG_MAX_SLS), ("att_beta", C.c_double * AXG_MAX_SLS),
                 ("att_gamma", C.c_double * AXG_MAX_SLS), ("stability_interval", C.c_int32),
-                ("deterministic", C.c_int32), ("compensated", C.c_int32)]
+                ("deterministic", C.c_int32), ("compensated", C.c_int32), ("plain", C.c_int32),
+                ("autotune", C.c_int32)]
 
 
 class axg_solid_points(C.Structure):
@@ -111,6 +112,8 @@ SIGNATURES = {
     "axg_set_field": (C.c_int, [H, C.c_int32, C.c_int32, P_f64]),
     "axg_field_size": (C.c_int, [H, C.c_int32, P_i64]),
     "axg_get_seismograms": (C.c_int, [H, P_f64, P_i32]),
+    "axg_forward_checkpointed": (C.c_int, [H, C.c_int32, C.c_int32]),
+    "axg_adjoint_run": (C.c_int, [H, P_f64, P_f64, P_f64, P_f64, P_f64]),
     "axg_field_raw_bytes": (C.c_int, [H, C.c_int32, C.c_int32, P_i64]),
     "axg_set_field_raw": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_int64]),
     "axg_get_field_raw": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_int64]),

@@ -1,0 +1,316 @@
+// adjoint_kernel.cuh -- the time-reversed adjoint of the elastic time step.
+//
+// The reference has no adjoint (no sensitivity kernels, no checkpointing); this is
+// the discrete adjoint of the forward loop the engine runs (NewmarkTimeScheme::solve,
+// SOLVER/src/core/time/NewmarkTimeScheme.cpp:41-108), for isotropic elements whose
+// moduli are constant in phi (the in-Fourier path), without attenuation.
+//
+// Forward step n:   a_n = M^-1 P (F_n - K u_n)
+//                   v_{n+1} = v_n + h/2 (a_{n-1} + a_n)
+//                   u_{n+1} = u_n + h v_{n+1} + h^2/2 a_n
+//                   seismograms d_n = R u_n
+// with P the (symmetric) axial / Nyquist projection. With phi-constant moduli
+// the modes decouple and the quadrature is the Hermitian transpose of the
+// gradient with the integral factor (GradientQuadrature.hpp:294-324 vs
+// 207-231), so each mode's stiffness block is Hermitian: as a real-linear map
+// K^T = K, and the transpose is applied with the forward kernel itself.
+// Reverse step n (cotangents of u_{n+1}, v_{n+1}, a_n), real inner products:
+//   abar_n  = abar_out + h/2 vbar + h^2/2 ubar
+//   g       = P (M^-1 abar_n)                        (cotangent of the stiffness)
+//   ubar_n  = ubar + (-K g) + R^T r_n
+//   vbar_n  = vbar + h ubar,  abar_out' = h/2 vbar
+//   dJ/dM_p     += -<abar_n, a_n>_p / M_p
+//   dJ/dlambda  += -sum_a ifact_q Re(conj(tr e(g)) tr e(u_n))
+//   dJ/dmu      += -sum_a ifact_q Re(conj(e(g)) . D_mu e(u_n)),  D_mu = diag(2,2,2,1,1,1)
+#pragma once
+
+#include "common.cuh"
+#include "point_kernels.cuh"
+#include "solid_kernel.cuh"
+
+namespace axg {
+
+template <class T>
+struct AdjointArgs {
+    int n_elem;
+    const int *nr, *pts;
+    const uint8_t *axial;
+    const T *geom;              // [n][10][25]
+    const T *mod;               // lambda, mu pool [2][25] per element
+    const int64_t *mod_off;
+    const int *pt_off, *pt_nu;
+    const cx_t<T> *u;           // forward displacement at step n
+    const cx_t<T> *g;           // W^-1 P M^-1 abar_n
+    cx_t<T> *out;               // receives -K g (scatter-add)
+    const T *ifact;             // [n][25] integral factor
+    T *grad;                    // [n][2][25]: dJ/dlambda, dJ/dmu per element point
+    const T *gmat;
+};
+
+// strains of one element field at (mode al, point q) from U[a][c][25] in shared memory
+template <class T>
+__device__ __forceinline__ void strain_at(const cx_t<T> *U, int al, int q, bool axial, const T *Gxi,
+                                          const T *sGll, const T *geo, cx_t<T> eps[6]) {
+    using C = cx_t<T>;
+    const int ii = q / 5, jj = q - ii * 5;
+    const T *dsdxii = geo, *dsdeta = geo + 25, *dzdxii = geo + 50, *dzdeta = geo + 75, *invs = geo + 100;
+    C X[3], Y[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        C x = mk<T>(0, 0), y = mk<T>(0, 0);
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            const T gx = Gxi[k * 5 + ii], gy = sGll[k * 5 + jj];
+            const C uc = U[c * 25 + k * 5 + jj], ur = U[c * 25 + ii * 5 + k];
+            x.x += gx * uc.x; x.y += gx * uc.y;
+            y.x += ur.x * gy; y.y += ur.y * gy;
+        }
+        X[c] = x; Y[c] = y;
+    }
+    const T ze = dzdeta[q], zx = dzdxii[q], se = dsdeta[q], sx = dsdxii[q];
+    eps[0] = cadd(cscale(X[0], ze), cscale(Y[0], zx));
+    eps[4] = cadd(cscale(X[0], se), cscale(Y[0], sx));
+    eps[5] = cadd(cscale(X[1], ze), cscale(Y[1], zx));
+    eps[3] = cadd(cscale(X[1], se), cscale(Y[1], sx));
+    const C e1t = cadd(cscale(X[2], ze), cscale(Y[2], zx));
+    eps[2] = cadd(cscale(X[2], se), cscale(Y[2], sx));
+    eps[4] = cadd(eps[4], e1t);
+    const T alf = (T)al;
+    const C A0 = csub(cia(alf, U[q]), U[25 + q]);
+    const C A1 = cadd(cia(alf, U[25 + q]), U[q]);
+    const C A2 = cia(alf, U[50 + q]);
+    const T is = invs[q];
+    eps[5] = cadd(eps[5], cscale(A0, is));
+    eps[1] = cscale(A1, is);
+    eps[3] = cadd(eps[3], cscale(A2, is));
+    if (axial && ii == 0) {
+        C ax[3], ay[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) { ax[c] = mk<T>(0, 0); ay[c] = mk<T>(0, 0); }
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            const T gx = Gxi[k * 5 + 0], gy = sGll[k * 5 + jj];
+            const C v0 = U[k * 5 + jj], v1 = U[25 + k * 5 + jj], v2 = U[50 + k * 5 + jj];
+            const C w0 = U[k], w1 = U[25 + k], w2 = U[50 + k];
+            C a0 = csub(cia(alf, v0), v1), a1 = cadd(cia(alf, v1), v0), a2 = cia(alf, v2);
+            C b0 = csub(cia(alf, w0), w1), b1 = cadd(cia(alf, w1), w0), b2 = cia(alf, w2);
+            ax[0] = cadd(ax[0], cscale(a0, gx)); ax[1] = cadd(ax[1], cscale(a1, gx));
+            ax[2] = cadd(ax[2], cscale(a2, gx));
+            ay[0] = cadd(ay[0], cscale(b0, gy)); ay[1] = cadd(ay[1], cscale(b1, gy));
+            ay[2] = cadd(ay[2], cscale(b2, gy));
+        }
+        eps[5] = cadd(eps[5], cadd(cscale(ax[0], ze), cscale(ay[0], zx)));
+        eps[1] = cadd(cscale(ax[1], ze), cscale(ay[1], zx));
+        eps[3] = cadd(eps[3], cadd(cscale(ax[2], ze), cscale(ay[2], zx)));
+    }
+}
+
+// one CTA (team of blockDim.x threads) per element: -K g scattered to `out`, and the
+// lambda / mu sensitivities of this step accumulated into grad
+template <class T>
+__global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArgs<T> a, const int nu_max) {
+    using C = cx_t<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T sGll[25], sGlj[25], sGeo[250];
+    __shared__ int sOff[25], sNu[25];
+    __shared__ T sGl[25], sGm[25];
+    C *Ug = reinterpret_cast<C *>(smem_raw);            // [nu][3][25] g, then A terms
+    C *Uu = Ug + (size_t)nu_max * 75;                    // [nu][3][25] u
+    C *S = Uu + (size_t)nu_max * 75;                     // [nu][6][25] stress of g, then X/Y
+    for (int i = threadIdx.x; i < 25; i += blockDim.x) {
+        sGll[i] = a.gmat[i];
+        sGlj[i] = a.gmat[25 + i];
+    }
+    for (int e = blockIdx.x; e < a.n_elem; e += gridDim.x) {
+        const int nr = a.nr[e], nu = nr / 2 + 1;
+        const bool axial = a.axial[e] != 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < 250; i += blockDim.x) sGeo[i] = a.geom[(size_t)e * 250 + i];
+        for (int i = threadIdx.x; i < 25; i += blockDim.x) {
+            const int p = a.pts[(size_t)e * 25 + i];
+            sOff[i] = a.pt_off[p];
+            sNu[i] = a.pt_nu[p];
+            sGl[i] = 0;
+            sGm[i] = 0;
+        }
+        __syncthreads();
+        const T *Gxi = axial ? sGlj : sGll;
+        for (int i = threadIdx.x; i < nu * 25; i += blockDim.x) {
+            const int q = i / nu, al = i - q * nu;
+            C g0 = mk<T>(0, 0), g1 = g0, g2 = g0, u0 = g0, u1 = g0, u2 = g0;
+            if (al < sNu[q]) {
+                const size_t o = (size_t)(sOff[q] + al) * 3;
+                g0 = a.g[o]; g1 = a.g[o + 1]; g2 = a.g[o + 2];
+                u0 = a.u[o]; u1 = a.u[o + 1]; u2 = a.u[o + 2];
+            }
+            Ug[(al * 3 + 0) * 25 + q] = g0; Ug[(al * 3 + 1) * 25 + q] = g1; Ug[(al * 3 + 2) * 25 + q] = g2;
+            Uu[(al * 3 + 0) * 25 + q] = u0; Uu[(al * 3 + 1) * 25 + q] = u1; Uu[(al * 3 + 2) * 25 + q] = u2;
+        }
+        __syncthreads();
+        const T *mod = a.mod + a.mod_off[e];
+        for (int i = threadIdx.x; i < nu * 25; i += blockDim.x) {
+            const int al = i / 25, q = i - al * 25;
+            C eg[6], eu[6], sg[6];
+            strain_at<T>(Ug + al * 75, al, q, axial, Gxi, sGll, sGeo, eg);
+            strain_at<T>(Uu + al * 75, al, q, axial, Gxi, sGll, sGeo, eu);
+            const T lam = mod[q], mu = mod[25 + q];
+            stress_iso(eg, sg, lam, mu);
+#pragma unroll
+            for (int d = 0; d < 6; d++) S[(al * 6 + d) * 25 + q] = sg[d];
+            // sensitivities Re(conj(e(g)) . de/dm e(u)), times ifact below
+            const C tg = cadd(cadd(eg[0], eg[1]), eg[2]), tu = cadd(cadd(eu[0], eu[1]), eu[2]);
+            const T pl = tg.x * tu.x + tg.y * tu.y;
+            T pm = 0;
+#pragma unroll
+            for (int d = 0; d < 6; d++) pm += (d < 3 ? (T)2 : (T)1) * (eg[d].x * eu[d].x + eg[d].y * eu[d].y);
+            atomicAdd(&sGl[q], pl);
+            atomicAdd(&sGm[q], pm);
+        }
+        __syncthreads();
+        // quadrature of the stress of g (computeQuad6): pass 1, X/Y in place, A terms in Ug
+        const T *dsdxii_if = sGeo + 125, *dsdeta_if = sGeo + 150, *dzdxii_if = sGeo + 175,
+                *dzdeta_if = sGeo + 200, *invs_if = sGeo + 225;
+        for (int i = threadIdx.x; i < nu * 25; i += blockDim.x) {
+            const int al = i / 25, q = i - al * 25;
+            C s[6];
+#pragma unroll
+            for (int d = 0; d < 6; d++) s[d] = S[(al * 6 + d) * 25 + q];
+            const T ze = dzdeta_if[q], zx = dzdxii_if[q], se = dsdeta_if[q], sx = dsdxii_if[q];
+            C *xy = S + al * 150;
+            xy[0 * 25 + q] = cadd(cscale(s[0], ze), cscale(s[4], se));
+            xy[1 * 25 + q] = cadd(cscale(s[0], zx), cscale(s[4], sx));
+            xy[2 * 25 + q] = cadd(cscale(s[5], ze), cscale(s[3], se));
+            xy[3 * 25 + q] = cadd(cscale(s[5], zx), cscale(s[3], sx));
+            xy[4 * 25 + q] = cadd(cscale(s[4], ze), cscale(s[2], se));
+            xy[5 * 25 + q] = cadd(cscale(s[4], zx), cscale(s[2], sx));
+            const T alf = (T)al;
+            Ug[(al * 3 + 0) * 25 + q] = csub(cia(alf, s[5]), s[1]);
+            Ug[(al * 3 + 1) * 25 + q] = cadd(cia(alf, s[1]), s[5]);
+            Ug[(al * 3 + 2) * 25 + q] = cia(alf, s[3]);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nu * 25; i += blockDim.x) {
+            const int al = i / 25, q = i - al * 25;
+            const int ii = q / 5, jj = q - ii * 5;
+            const C *xy = S + al * 150;
+            const C *A = Ug + al * 75;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                C g1 = mk<T>(0, 0), g2 = mk<T>(0, 0);
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    const T gx = Gxi[ii * 5 + k], gt = sGll[jj * 5 + k];
+                    const C xv = xy[(2 * c) * 25 + k * 5 + jj], yv = xy[(2 * c + 1) * 25 + ii * 5 + k];
+                    g1.x += gx * xv.x; g1.y += gx * xv.y;
+                    g2.x += yv.x * gt; g2.y += yv.y * gt;
+                }
+                C fc = cadd(g1, g2);
+                fc = csub(fc, cscale(A[c * 25 + q], invs_if[q]));
+                if (axial) {
+                    fc = csub(fc, cscale(cscale(A[c * 25 + jj], dzdeta_if[jj]), Gxi[ii * 5 + 0]));
+                    if (ii == 0) {
+                        C b = mk<T>(0, 0);
+#pragma unroll
+                        for (int k = 0; k < 5; k++) {
+                            const C y0 = cscale(A[c * 25 + k], dzdxii_if[k]);
+                            const T gt = sGll[jj * 5 + k];
+                            b.x += y0.x * gt; b.y += y0.y * gt;
+                        }
+                        fc = csub(fc, b);
+                    }
+                }
+                if (al < sNu[q]) atomic_add_cx(a.out + (size_t)(sOff[q] + al) * 3 + c, mk<T>(-fc.x, -fc.y));
+            }
+        }
+        __syncthreads();
+        // grad (each element belongs to one CTA per launch, so no race): -ifact * products
+        for (int q = threadIdx.x; q < 25; q += blockDim.x) {
+            const T f = a.ifact[(size_t)e * 25 + q];
+            T *gr = a.grad + (size_t)e * 50;
+            gr[q] -= f * sGl[q];
+            gr[25 + q] -= f * sGm[q];
+        }
+    }
+}
+
+// per point mode: abar_n, dJ/dM, g = W^-1 P M^-1 abar_n, vbar_n, abar_out'
+template <class T>
+struct AdjPointArgs {
+    int nmodes;
+    const int *mode_pt, *off, *nr;
+    const uint8_t *flags;
+    const T *inv_mass1;
+    cx_t<T> *ubar, *vbar, *abar_out;   // in: step n+1 cotangents; out: updated
+    const cx_t<T> *a_n;                // forward acceleration of step n
+    cx_t<T> *g;                        // out
+    T *grad_mass;                      // [npoints] dJ/dM
+    T h;
+};
+
+template <class T>
+__global__ void adjoint_point_kernel(const AdjPointArgs<T> a) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= a.nmodes) return;
+    const int p = a.mode_pt[m];
+    const int off = a.off[p], nr = a.nr[p], nu = nr / 2 + 1, al = m - off;
+    const T im = a.inv_mass1[p];
+    const T h = a.h;
+    cx_t<T> ab[3], gv[3];
+    T dm = 0;
+    for (int c = 0; c < 3; c++) {
+        const size_t q = (size_t)m * 3 + c;
+        const cx_t<T> ub = a.ubar[q], vb = a.vbar[q], ao = a.abar_out[q];
+        cx_t<T> abn = mk<T>(ao.x + h / 2 * vb.x + h * h / 2 * ub.x, ao.y + h / 2 * vb.y + h * h / 2 * ub.y);
+        const cx_t<T> an = a.a_n[q];
+        dm -= (abn.x * an.x + abn.y * an.y) * im;
+        ab[c] = cscale(abn, im);
+        a.vbar[q] = mk<T>(vb.x + h * ub.x, vb.y + h * ub.y);
+        a.abar_out[q] = mk<T>(h / 2 * vb.x, h / 2 * vb.y);
+    }
+    // P is symmetric (axial projection and Nyquist rule), so P^T = P
+    point_bc<T>(ab, 3, al, nu, nr, a.flags[p], true);
+    for (int c = 0; c < 3; c++) gv[c] = ab[c];
+    for (int c = 0; c < 3; c++) a.g[(size_t)m * 3 + c] = gv[c];
+    atomicAdd(&a.grad_mass[p], dm);
+}
+
+// ubar_n = ubar_{n+1} + (-K g), -K g being in `kg` (which is then cleared)
+template <class T>
+__global__ void adjoint_combine_kernel(int nvals, cx_t<T> *ubar, cx_t<T> *kg) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nvals) return;
+    const cx_t<T> k = kg[q];
+    ubar[q] = mk<T>(ubar[q].x + k.x, ubar[q].y + k.y);
+    kg[q] = mk<T>(0, 0);
+}
+
+// R^T r_n: the seismogram cotangent of step n injected into ubar
+template <class T>
+__global__ void adjoint_station_kernel(int nst, const int *elem, const T *w, const T *phi, const int *e_nr,
+                                       const int *e_pts, const int *pt_off, const int *pt_nu,
+                                       const double *r, cx_t<T> *ubar) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nst * 3) return;
+    const int s = t / 3, c = t % 3;
+    const int e = elem[s], nu = e_nr[e] / 2 + 1;
+    const T rv = (T)r[(size_t)s * 3 + c];
+    for (int al = 0; al < nu; al++) {
+        // seismogram = sum_a Re(z_a x_a), z_0 = 1, z_a = 2 e^{i a phi}: cotangent conj(z_a) rv
+        T zr = 1, zi = 0;
+        if (al > 0) {
+            T sn, cs;
+            if constexpr (sizeof(T) == 4) sincosf((T)al * phi[s], &sn, &cs);
+            else sincos((T)al * phi[s], &sn, &cs);
+            zr = 2 * cs; zi = 2 * sn;
+        }
+        for (int q = 0; q < 25; q++) {
+            const T wq = w[(size_t)s * 25 + q];
+            if (wq == (T)0) continue;
+            const int p = e_pts[(size_t)e * 25 + q];
+            if (al >= pt_nu[p]) continue;
+            atomic_add_cx(ubar + (size_t)(pt_off[p] + al) * 3 + c, mk<T>(rv * wq * zr, -rv * wq * zi));
+        }
+    }
+}
+
+}  // namespace axg

@@ -355,6 +355,13 @@ int axg_field_size(const axg_solver *h, int32_t solid, int64_t *n) {
     *n = h->eng->field_size(solid);
     return AXG_OK;
 }
+int axg_forward_checkpointed(axg_solver *h, int32_t nsteps, int32_t checkpoint_interval) {
+    return guarded(h, [&] { h->eng->forward_checkpointed(nsteps, checkpoint_interval); });
+}
+int axg_adjoint_run(axg_solver *h, const double *seis_adjoint, double *grad_moduli, double *grad_mass,
+                    double *grad_displ0, double *grad_veloc0) {
+    return guarded(h, [&] { h->eng->adjoint_run(seis_adjoint, grad_moduli, grad_mass, grad_displ0, grad_veloc0); });
+}
 int axg_field_raw_bytes(const axg_solver *h, int32_t solid, int32_t which, int64_t *bytes) {
     if (!h || !bytes || which < 0 || which > 3) return AXG_E_ARG;
     if (!h->finalized) return AXG_E_STATE;

@@ -102,6 +102,9 @@ public:
     virtual void set_stream(void *stream) = 0;
     virtual void set_team_override(int nr_class, int team) = 0;
     virtual int bucket_count() const = 0;
+    virtual void forward_checkpointed(int nsteps, int interval) = 0;
+    virtual void adjoint_run(const double *seis_adj, double *grad_mod, double *grad_mass,
+                             double *grad_u0, double *grad_v0) = 0;
 };
 
 std::unique_ptr<EngineBase> make_engine_fp32(const axg_config &cfg);

@@ -9,6 +9,7 @@
 #pragma once
 
 #include "engine.hpp"
+#include "adjoint_kernel.cuh"
 #include "fluid_kernel.cuh"
 #include "point_kernels.cuh"
 #include "solid_kernel.cuh"
@@ -165,6 +166,7 @@ public:
         tw_off_.upload(twoff);
         build_solid_buckets(m.se);
         build_fluid_buckets(m.fe);
+        if (cfg_.autotune && !cfg_.plain) autotune();
         build_coupling(m.sf);
         build_sources(m.ms, m.fs);
         build_stations(m.st);
@@ -211,7 +213,7 @@ public:
                 time_ms_ += ms;
                 time_n_ += 1;
             }
-        } else if (graph) {
+        } else if (graph && !cfg_.plain) {
             if (!graph_exec_) capture();
             for (int i = 0; i < nsteps; i++) {
                 AXG_CUDA(cudaGraphLaunch(graph_exec_, stream_));
@@ -368,7 +370,186 @@ public:
     }
     int bucket_count() const override { return (int)(sb_.size() + fb_.size()); }
 
+    // ------------------------------------------------------------ adjoint ---
+    void forward_checkpointed(int nsteps, int interval) override {
+        need();
+        if (!std::is_same<T, double>::value || !std::is_same<D, double>::value)
+            throw Error(AXG_E_UNSUPPORTED, "axg_forward_checkpointed || needs an FP64 handle.");
+        check_adjoint_model();
+        if (nsteps <= 0 || interval <= 0) throw Error(AXG_E_ARG, "axg_forward_checkpointed || bad sizes.");
+        ensure_capacity(step_ + nsteps);
+        const size_t nf = (size_t)sp_.total * 3;
+        const int nck = (nsteps + interval - 1) / interval;
+        ck_displ_.alloc(nf * nck); ck_veloc_.alloc(nf * nck); ck_accel_.alloc(nf * nck);
+        ck_n_ = nsteps; ck_interval_ = interval; ck_step0_ = step_;
+        for (int c = 0; c < nck; c++) {
+            copy_fields_out(c);
+            run(std::min(interval, nsteps - c * interval), true);
+        }
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+    }
+
+    void adjoint_run(const double *seis_adj, double *grad_mod, double *grad_mass, double *grad_u0,
+                     double *grad_v0) override {
+        need();
+        if (ck_n_ <= 0) throw Error(AXG_E_STATE, "axg_adjoint_run || no checkpointed forward run.");
+        if (st_n_ > 0 && !seis_adj) throw Error(AXG_E_ARG, "axg_adjoint_run || seismogram cotangents missing.");
+        build_adjoint_arrays();
+        const size_t nf = (size_t)sp_.total * 3;
+        const int nck = (ck_n_ + ck_interval_ - 1) / ck_interval_;
+        const int end_step = ck_step0_ + ck_n_;
+        // state after the forward run, restored at the end
+        DBuf<C> fin_d, fin_v, fin_a;
+        fin_d.alloc(nf); fin_v.alloc(nf); fin_a.alloc(nf);
+        AXG_CUDA(cudaMemcpyAsync(fin_d.p, sp_.displ.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        AXG_CUDA(cudaMemcpyAsync(fin_v.p, sp_.veloc.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        AXG_CUDA(cudaMemcpyAsync(fin_a.p, sp_.accel.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        DBuf<C> ub, vb, ab, g, kg, seg_u, seg_a;
+        ub.alloc(nf); vb.alloc(nf); ab.alloc(nf); g.alloc(nf); kg.alloc(nf);
+        ub.zero(stream_); vb.zero(stream_); ab.zero(stream_); kg.zero(stream_);
+        seg_u.alloc(nf * ck_interval_); seg_a.alloc(nf * ck_interval_);
+        adj_grad_.zero(stream_);
+        adj_gmass_.zero(stream_);
+        DBuf<double> r;
+        if (st_n_) r.alloc((size_t)st_n_ * 3);
+        const int threads = 256;
+        const int mblocks = (sp_.total + threads - 1) / threads;
+        const int vblocks = (int)((nf + threads - 1) / threads);
+        for (int c = nck - 1; c >= 0; c--) {
+            const int len = std::min(ck_interval_, ck_n_ - c * ck_interval_);
+            copy_fields_in(c);
+            step_ = ck_step0_ + c * ck_interval_;
+            set_step(step_);
+            // recompute the segment, keeping u_n and a_n
+            for (int i = 0; i < len; i++) {
+                AXG_CUDA(cudaMemcpyAsync(seg_u.p + nf * i, sp_.displ.p, nf * sizeof(C),
+                                         cudaMemcpyDeviceToDevice, stream_));
+                launch_step();
+                AXG_CUDA(cudaMemcpyAsync(seg_a.p + nf * i, sp_.accel.p, nf * sizeof(C),
+                                         cudaMemcpyDeviceToDevice, stream_));
+            }
+            for (int i = len - 1; i >= 0; i--) {
+                const int n = step_ + i;
+                AdjPointArgs<T> pa;
+                pa.nmodes = sp_.total; pa.mode_pt = sp_.mode_pt.p; pa.off = sp_.off.p; pa.nr = sp_.nr.p;
+                pa.flags = sp_.flags.p; pa.inv_mass1 = sp_.inv1.p; pa.ubar = ub.p; pa.vbar = vb.p;
+                pa.abar_out = ab.p; pa.a_n = seg_a.p + nf * i; pa.g = g.p; pa.grad_mass = adj_gmass_.p;
+                pa.h = (T)cfg_.dt;
+                adjoint_point_kernel<T><<<mblocks, threads, 0, stream_>>>(pa);
+                post_launch();
+                AdjointArgs<T> aa;
+                aa.n_elem = model_.se.count; aa.nr = e_nr_.p; aa.pts = e_pts_.p; aa.axial = e_axial_.p;
+                aa.geom = adj_geom_.p; aa.mod = adj_mod_.p; aa.mod_off = adj_mod_off_.p;
+                aa.pt_off = sp_.off.p; aa.pt_nu = sp_.nu.p; aa.u = seg_u.p + nf * i; aa.g = g.p;
+                aa.out = kg.p; aa.ifact = adj_ifact_.p; aa.grad = adj_grad_.p; aa.gmat = gmat_.p;
+                const int nu_max = adj_nr_max_ / 2 + 1;
+                const size_t smem = (size_t)nu_max * (75 + 75 + 150) * sizeof(C);
+                const int grid = std::min(model_.se.count, prop_.multiProcessorCount * 8);
+                adjoint_stiffness_kernel<T><<<grid, 128, smem, stream_>>>(aa, nu_max);
+                post_launch();
+                adjoint_combine_kernel<T><<<vblocks, threads, 0, stream_>>>((int)nf, ub.p, kg.p);
+                post_launch();
+                if (st_n_ && n % st_interval_ == 0) {
+                    const int rec = n / st_interval_;
+                    AXG_CUDA(cudaMemcpyAsync(r.p, seis_adj + (size_t)rec * st_n_ * 3,
+                                             (size_t)st_n_ * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                             stream_));
+                    adjoint_station_kernel<T><<<(st_n_ * 3 + 127) / 128, 128, 0, stream_>>>(
+                        st_n_, st_el_.p, st_w_.p, st_phi_.p, e_nr_.p, e_pts_.p, sp_.off.p, sp_.nu.p, r.p, ub.p);
+                    post_launch();
+                    AXG_CUDA(cudaStreamSynchronize(stream_));   // r is reused next step
+                }
+            }
+        }
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        auto d2h_cx = [&](const C *src, double *dst) {
+            std::vector<C> hbuf(nf);
+            AXG_CUDA(cudaMemcpy(hbuf.data(), src, nf * sizeof(C), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < nf; i++) { dst[2 * i] = (double)hbuf[i].x; dst[2 * i + 1] = (double)hbuf[i].y; }
+        };
+        if (grad_u0) d2h_cx(ub.p, grad_u0);
+        if (grad_v0) d2h_cx(vb.p, grad_v0);
+        if (grad_mod) {
+            std::vector<T> hg((size_t)model_.se.count * 50);
+            AXG_CUDA(cudaMemcpy(hg.data(), adj_grad_.p, hg.size() * sizeof(T), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < hg.size(); i++) grad_mod[i] = (double)hg[i];
+        }
+        if (grad_mass) {
+            std::vector<T> hm(sp_.n);
+            AXG_CUDA(cudaMemcpy(hm.data(), adj_gmass_.p, hm.size() * sizeof(T), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < sp_.n; i++) grad_mass[i] = (double)hm[i];
+        }
+        // back to the state after the forward run
+        AXG_CUDA(cudaMemcpyAsync(sp_.displ.p, fin_d.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        AXG_CUDA(cudaMemcpyAsync(sp_.veloc.p, fin_v.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        AXG_CUDA(cudaMemcpyAsync(sp_.accel.p, fin_a.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        sp_.stiff.zero(stream_);
+        step_ = end_step;
+        set_step(step_);
+    }
+
 private:
+    void check_adjoint_model() const {
+        const HostSolidElements &h = model_.se;
+        if (fp_.n > 0) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || fluid elements are not differentiated.");
+        for (int e = 0; e < h.count; e++) {
+            bool ok = h.rheo[e] == AXG_ISO && !(h.is3d.size() && h.is3d[e]) &&
+                      !(h.att.size() && h.att[e] != AXG_ATT_NONE);
+            if (!ok)
+                throw Error(AXG_E_UNSUPPORTED,
+                            "axg_adjoint || needs isotropic, phi-constant, non-attenuating solid elements.");
+        }
+        for (int p = 0; p < sp_.n; p++)
+            if (model_.sp.mass_nr.size() && model_.sp.mass_nr[p] > 1)
+                throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || 3-D masses are not differentiated.");
+    }
+    void copy_fields_out(int c) {
+        const size_t nf = (size_t)sp_.total * 3;
+        AXG_CUDA(cudaMemcpyAsync(ck_displ_.p + nf * c, sp_.displ.p, nf * sizeof(CD), cudaMemcpyDeviceToDevice, stream_));
+        AXG_CUDA(cudaMemcpyAsync(ck_veloc_.p + nf * c, sp_.veloc.p, nf * sizeof(CD), cudaMemcpyDeviceToDevice, stream_));
+        AXG_CUDA(cudaMemcpyAsync(ck_accel_.p + nf * c, sp_.accel.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+    }
+    void copy_fields_in(int c) {
+        const size_t nf = (size_t)sp_.total * 3;
+        AXG_CUDA(cudaMemcpyAsync(sp_.displ.p, ck_displ_.p + nf * c, nf * sizeof(CD), cudaMemcpyDeviceToDevice, stream_));
+        AXG_CUDA(cudaMemcpyAsync(sp_.veloc.p, ck_veloc_.p + nf * c, nf * sizeof(CD), cudaMemcpyDeviceToDevice, stream_));
+        AXG_CUDA(cudaMemcpyAsync(sp_.accel.p, ck_accel_.p + nf * c, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        sp_.stiff.zero(stream_);
+    }
+    void build_adjoint_arrays() {
+        if (adj_built_) return;
+        const HostSolidElements &h = model_.se;
+        std::vector<T> geom((size_t)h.count * 250), ifact((size_t)h.count * 25), mod((size_t)h.count * 50);
+        std::vector<int64_t> moff(h.count);
+        adj_nr_max_ = 1;
+        for (int e = 0; e < h.count; e++) {
+            adj_nr_max_ = std::max(adj_nr_max_, h.nr[e]);
+            for (int c = 0; c < 5; c++)
+                for (int q = 0; q < 25; q++) {
+                    geom[(size_t)e * 250 + c * 25 + q] = (T)h.geom[(size_t)e * 150 + c * 25 + q];
+                    geom[(size_t)e * 250 + 125 + c * 25 + q] =
+                        (T)(h.geom[(size_t)e * 150 + c * 25 + q] * h.geom[(size_t)e * 150 + 125 + q]);
+                }
+            for (int q = 0; q < 25; q++) ifact[(size_t)e * 25 + q] = (T)h.geom[(size_t)e * 150 + 125 + q];
+            for (int i = 0; i < 50; i++) mod[(size_t)e * 50 + i] = (T)h.moduli[h.mat_off[e] + i];
+            moff[e] = (int64_t)e * 50;
+        }
+        adj_geom_.upload(geom); adj_ifact_.upload(ifact); adj_mod_.upload(mod); adj_mod_off_.upload(moff);
+        adj_grad_.alloc((size_t)h.count * 50);
+        adj_gmass_.alloc(sp_.n);
+        if (!e_nr_.p) {
+            e_nr_.upload(h.nr); e_pts_.upload(h.pts);
+            std::vector<uint8_t> ax(h.axial.begin(), h.axial.end());
+            e_axial_.upload(ax);
+        }
+        int nu_max = adj_nr_max_ / 2 + 1;
+        size_t smem = (size_t)nu_max * 300 * sizeof(C);
+        if (smem > 200 * 1024) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || nr too large.");
+        AXG_CUDA(cudaFuncSetAttribute((const void *)adjoint_stiffness_kernel<T>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        adj_built_ = true;
+    }
+
     void need() const {
         if (!finalized_) throw Error(AXG_E_STATE, "Engine::step || axg_finalize not called.");
     }
@@ -477,7 +658,7 @@ private:
             if (h.rheo[e] == RHEO_ISO) rtz = 0;   // isotropic rheology is frame invariant
             if (att != ATT_NONE && cfg_.nsls <= 0)
                 throw Error(AXG_E_ARG, "Attenuation::checkCompatibility || nsls must be > 0.");
-            groups[{h.rheo[e], att, is3d, rtz, nr_class(h.nr[e])}].push_back(e);
+            groups[{h.rheo[e], att, is3d, rtz, cfg_.plain ? 0 : nr_class(h.nr[e])}].push_back(e);
         }
         int64_t state_total = 0;
         std::vector<std::vector<int64_t>> state_offs;
@@ -575,8 +756,9 @@ private:
         for (size_t i = 0; i < sb_.size(); i++) sb_[i]->state_off.upload(state_offs[i]);
     }
 
-    void configure_bucket(SolidBucket &b) {
-        int team = team_override_[b.cls] ? team_override_[b.cls] : default_team(b.cls);
+    void configure_bucket(SolidBucket &b, int team_req = 0) {
+        int team = team_req ? team_req
+                            : (cfg_.plain ? 256 : (team_override_[b.cls] ? team_override_[b.cls] : default_team(b.cls)));
         // shared memory per team; split the 25 points of the slice phase if needed
         const size_t budget = 200 * 1024;
         int qc = 25;
@@ -598,6 +780,44 @@ private:
         AXG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b.kernel, team * tpc,
                                                                tpc * L.total));
         b.grid = std::max(1, std::min((b.n + tpc - 1) / tpc, std::max(1, per_sm) * prop_.multiProcessorCount));
+        if (cfg_.plain) b.grid = (b.n + tpc - 1) / tpc;   // one team per element, no persistence
+    }
+
+    // The project's autotuner: for every solid bucket, time each feasible team size
+    // (threads per element) on the bucket's own elements and keep the fastest. The
+    // fields are zero at this point, so the trial launches change no result; the
+    // attenuation state and the stiffness are cleared afterwards all the same.
+    void autotune() {
+        cudaEvent_t t0, t1;
+        AXG_CUDA(cudaEventCreate(&t0));
+        AXG_CUDA(cudaEventCreate(&t1));
+        for (auto &bp : sb_) {
+            SolidBucket &b = *bp;
+            float best = 1e30f;
+            int best_team = b.team;
+            for (int team : {32, 64, 128, 256}) {
+                b.team = team;
+                configure_bucket(b, team);
+                float ms = 0;
+                for (int rep = 0; rep < 3; rep++) {
+                    AXG_CUDA(cudaEventRecord(t0, stream_));
+                    launch_solid_bucket(b);
+                    AXG_CUDA(cudaEventRecord(t1, stream_));
+                    AXG_CUDA(cudaEventSynchronize(t1));
+                    float x = 0;
+                    AXG_CUDA(cudaEventElapsedTime(&x, t0, t1));
+                    if (rep > 0) ms += x;   // the first launch warms caches
+                }
+                if (ms < best) { best = ms; best_team = team; }
+            }
+            configure_bucket(b, best_team);
+            tuned_.push_back({b.cls, best_team, best / 2});
+        }
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        state_.zero(stream_);
+        sp_.stiff.zero(stream_);
+        AXG_CUDA(cudaStreamSynchronize(stream_));
     }
 
     // several buckets can share one kernel instantiation: its dynamic shared
@@ -614,7 +834,7 @@ private:
     void build_fluid_buckets(const HostFluidElements &h) {
         std::map<std::tuple<int, int>, std::vector<int>> groups;
         for (int e = 0; e < h.count; e++)
-            groups[{h.is3d.size() ? h.is3d[e] : 0, nr_class(h.nr[e])}].push_back(e);
+            groups[{h.is3d.size() ? h.is3d[e] : 0, cfg_.plain ? 0 : nr_class(h.nr[e])}].push_back(e);
         for (auto &kv : groups) {
             auto b = std::make_unique<FluidBucket>();
             std::tie(b->is3d, b->cls) = kv.first;
@@ -659,7 +879,7 @@ private:
             b->K.upload(K); b->K_off.upload(koff);
             b->kernel = b->is3d ? (FluidKernel)fluid_stiffness_kernel<T, true>
                                 : (FluidKernel)fluid_stiffness_kernel<T, false>;
-            int team = team_override_[b->cls] ? team_override_[b->cls] : default_team(b->cls);
+            int team = cfg_.plain ? 256 : (team_override_[b->cls] ? team_override_[b->cls] : default_team(b->cls));
             TeamLayout L = fluid_layout<T>(b->nr_max);
             if (L.total > 200 * 1024)
                 throw Error(AXG_E_UNSUPPORTED, "FluidElement || nr too large for shared memory.");
@@ -816,8 +1036,13 @@ private:
 
     void launch_stiffness() {
         if (timing_) AXG_CUDA(cudaEventRecord(ev0_, stream_));
-        for (auto &bp : sb_) {
-            SolidBucket &b = *bp;
+        for (auto &bp : sb_) launch_solid_bucket(*bp);
+        if (timing_) AXG_CUDA(cudaEventRecord(ev1_, stream_));
+        launch_fluid();
+    }
+
+    void launch_solid_bucket(SolidBucket &b) {
+        {
             SolidArgs<T, AT> a;
             a.n_elem = b.n; a.nr = b.nr.p; a.pts = b.pts.p; a.axial = b.axial.p;
             a.geom = b.geom.p; a.trig = b.trig.p; a.mod = b.mod.p; a.mod_off = b.mod_off.p;
@@ -834,7 +1059,9 @@ private:
                                                                               b.tpc, b.team_bytes);
             post_launch();
         }
-        if (timing_) AXG_CUDA(cudaEventRecord(ev1_, stream_));
+    }
+
+    void launch_fluid() {
         for (auto &bp : fb_) {
             FluidBucket &b = *bp;
             FluidArgs<T> a;
@@ -954,6 +1181,16 @@ private:
     cudaGraphExec_t graph_exec_ = nullptr;
     int team_override_[5];
     std::map<const void *, size_t> smem_limit_;
+    struct Tuned { int cls, team; float ms; };
+    std::vector<Tuned> tuned_;
+    // differentiation
+    DBuf<CD> ck_displ_, ck_veloc_;
+    DBuf<C> ck_accel_;
+    int ck_n_ = 0, ck_interval_ = 0, ck_step0_ = 0;
+    bool adj_built_ = false;
+    int adj_nr_max_ = 1;
+    DBuf<T> adj_geom_, adj_ifact_, adj_mod_, adj_grad_, adj_gmass_;
+    DBuf<int64_t> adj_mod_off_;
 
     DBuf<T> gmat_, tw_;
     DBuf<int> tw_off_;

@@ -282,6 +282,7 @@ def cartesian_model(nx=40, nz=40, width=100e3, height=100e3, nr=5, rho=2700.0, v
     m.se_is3d = np.zeros(ne, np.uint8)
     m.se_mat_off = np.arange(ne, dtype=np.int64) * 50
     m.se_moduli = se_moduli.ravel()
+    m.meta_rho = np.full((ne, 25), rho)
     if attenuation:
         sls = attenuation
         lam2, mu2, dl, dm = iso_with_attenuation(np.full((ne, 25), lam), np.full((ne, 25), mu),
@@ -484,6 +485,34 @@ def aniso_moduli(rho, vp, vs, n, rng, pert=0.05):
     C = Ciso[None] + pert * (lam + 2 * mu) * R / 3.0
     iu = np.triu_indices(6)
     return [C[:, a, b] for a, b in zip(*iu)]
+
+
+def blob_model(base, amp=0.05, fields=("mu", "rho"), center=None, radius=None, seed=0):
+    """A copy of an isotropic 1-D Cartesian model with a seeded Gaussian blob of
+    relative amplitude `amp` in mu and / or rho (the adjoint workload)."""
+    import copy
+    rng = np.random.Generator(np.random.PCG64(seed))
+    m = copy.copy(base)
+    ne = base.n_solid_elements
+    coords = base.sp_coords[base.se_pts]                       # (ne, 25, 2)
+    smax, zmin = coords[..., 0].max(), coords[..., 1].min()
+    if center is None:
+        center = (rng.uniform(0.3, 0.7) * smax, zmin * rng.uniform(0.3, 0.7))
+    if radius is None:
+        radius = 0.15 * smax
+    d2 = (coords[..., 0] - center[0]) ** 2 + (coords[..., 1] - center[1]) ** 2
+    blob = amp * np.exp(-d2 / (2 * radius ** 2))
+    mods = base.se_moduli.reshape(ne, 2, 25).copy()
+    lam, mu = mods[:, 0], mods[:, 1]
+    rho = base.meta_rho.copy()
+    if "mu" in fields:
+        mu = mu * (1 + blob)
+    if "rho" in fields:
+        rho = rho * (1 + blob)
+    m.se_moduli = np.stack([lam, mu], axis=1).ravel()
+    m.meta_rho = rho
+    m.sp_mass = assemble_mass(base.se_pts, base.se_geom[:, 5, :], rho, len(base.sp_nr))
+    return m
 
 
 def random_displacement(model, seed=2, solid=True):

@@ -110,6 +110,7 @@ class Model:
     st_phi: np.ndarray = field(default_factory=lambda: np.zeros(0))
     st_interval: int = 1
     meta: dict = field(default_factory=dict)
+    meta_rho: Optional[np.ndarray] = None          # (ne, 25) density at element points (generators)
 
     # ------------------------------------------------------------ sizes ---
     @property
@@ -134,7 +135,7 @@ class Model:
         return u
 
     # ---------------------------------------------------------- C structs ---
-    def config(self, precision, device=0, stability_interval=0, compensated=1):
+    def config(self, precision, device=0, stability_interval=0, compensated=1, plain=0, autotune=0):
         cfg = L.axg_config()
         cfg.precision = L.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         cfg.device = device
@@ -148,6 +149,8 @@ class Model:
         cfg.stability_interval = stability_interval
         cfg.deterministic = 0
         cfg.compensated = compensated
+        cfg.plain = int(bool(plain))
+        cfg.autotune = int(bool(autotune))
         return cfg
 
     def c_structs(self):

@@ -31,12 +31,12 @@ class EngineError(RuntimeError):
 
 class Solver:
     def __init__(self, model, precision="fp32", device=0, stability_interval=0, compensated=True,
-                 team_sizes=None):
+                 team_sizes=None, plain=False, autotune=False):
         self.lib = L.lib()
         self.model = model
         self.precision = precision
         cfg = model.config(precision, device=device, stability_interval=stability_interval,
-                           compensated=int(bool(compensated)))
+                           compensated=int(bool(compensated)), plain=plain, autotune=autotune)
         h = C.c_void_p()
         rc = self.lib.axg_create(C.byref(cfg), C.byref(h))
         if rc != L.AXG_OK:
@@ -166,6 +166,29 @@ class Solver:
         if n.value and ns:
             self._check(self.lib.axg_get_seismograms(self.h, out.ctypes.data_as(L.P_f64), C.byref(n)))
         return out
+
+    # -------------------------------------------------------- differentiation ---
+    def forward_checkpointed(self, nsteps, interval=100):
+        """nsteps forward steps keeping a device checkpoint every `interval` steps."""
+        self._check(self.lib.axg_forward_checkpointed(self.h, int(nsteps), int(interval)))
+
+    def adjoint(self, seis_adjoint):
+        """Discrete adjoint of the last checkpointed run for dJ/d(seismograms).
+
+        Returns dJ/d(lambda, mu) per element point (ne, 2, 25), dJ/d(point mass),
+        and dJ/d(initial displacement / velocity) in the field layout."""
+        ne = self.model.n_solid_elements
+        r = np.ascontiguousarray(seis_adjoint, dtype=np.float64)
+        gm = np.zeros((ne, 2, 25))
+        gmass = np.zeros(len(self.model.sp_nr))
+        nf = self.field_size(True)
+        gu = np.zeros(nf, dtype=np.complex128)
+        gv = np.zeros(nf, dtype=np.complex128)
+        self._check(self.lib.axg_adjoint_run(self.h, r.ctypes.data_as(L.P_f64), gm.ctypes.data_as(L.P_f64),
+                                             gmass.ctypes.data_as(L.P_f64),
+                                             gu.view(np.float64).ctypes.data_as(L.P_f64),
+                                             gv.view(np.float64).ctypes.data_as(L.P_f64)))
+        return {"moduli": gm, "mass": gmass, "displ0": gu, "veloc0": gv}
 
     # ------------------------------------------------------------ diagnostics ---
     def launch_count(self):

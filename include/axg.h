@@ -105,6 +105,13 @@ typedef struct axg_config {
     int32_t stability_interval; /* steps between non-finite checks (0 = never)            */
     int32_t deterministic;      /* reserved: 0 = atomic scatter-add                        */
     int32_t compensated;        /* MIXED only: 1 = compensated (Kahan) d/v summation      */
+    int32_t plain;              /* 1 = the plain method: one element bucket per material
+                                   kind with a fixed 256-thread team (no nr bucketing, no
+                                   persistent grid), eager launches instead of CUDA graphs,
+                                   no autotuning -- the baseline the batched path is
+                                   measured against                                       */
+    int32_t autotune;           /* 1 = time the candidate team sizes of every nr bucket at
+                                   axg_finalize and keep the fastest                      */
 } axg_config;
 
 /* solid GLL points (SolidPoint + Mass1D/Mass3D + AxialBoundary membership) */
@@ -247,6 +254,21 @@ int  axg_record_stations(axg_solver *h, int32_t tstep);
 int  axg_run(axg_solver *h, int32_t nsteps, int32_t use_graph);
 /* step counter of the next step */
 int  axg_current_step(const axg_solver *h, int32_t *tstep);
+
+/* ---- differentiation (FP64 handles; isotropic phi-constant solid elements,
+        no attenuation, no fluid; no counterpart in the reference, which has no
+        adjoint) ---- */
+/* nsteps forward steps from the current state, storing the state every
+   checkpoint_interval steps on the device for axg_adjoint_run */
+int  axg_forward_checkpointed(axg_solver *h, int32_t nsteps, int32_t checkpoint_interval);
+/* time-reversed discrete adjoint of the last axg_forward_checkpointed run, each
+   segment recomputed from its checkpoint. seis_adjoint = dJ/d(seismograms),
+   [nrecords][nstations][3]. Outputs (host, each may be NULL):
+   grad_moduli [n_solid_elements][2][25] dJ/d(lambda, mu), grad_mass [n_solid_points]
+   dJ/d(point mass), grad_displ0 / grad_veloc0 (sum(nu)*3 complex) dJ/d(initial
+   displacement / velocity). The fields end in the state after the forward run. */
+int  axg_adjoint_run(axg_solver *h, const double *seis_adjoint, double *grad_moduli,
+                     double *grad_mass, double *grad_displ0, double *grad_veloc0);
 
 /* ---- fields ---- */
 /* solid = 1 for solid points, 0 for fluid; host buffer of sum(nu_p)*ndim complex doubles */

@@ -19,7 +19,9 @@ import spectral  # noqa: E402
 
 def build():
     src = os.path.join(HERE, "axg_oracle.cpp")
-    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    hdr = os.path.join(HERE, "..", "include", "axg.h")
+    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(os.path.getmtime(src),
+                                                                         os.path.getmtime(hdr)):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 

@@ -218,3 +218,64 @@ def test_launch_count_and_native_library(built):
     import os
     maps = open("/proc/self/maps").read()
     assert os.path.realpath(_lib.LIB_PATH) in maps
+
+
+SPH = {
+    "sph_iso_3d_cg4_fluid": dict(n_theta=24, n_solid_layers=6, n_fluid_layers=2, nr_max=40),
+    "sph_aniso_rtz_3d_fluid": dict(n_theta=16, n_solid_layers=4, n_fluid_layers=2, nr_max=24,
+                                   rheology="aniso", attenuation=None),
+    "sph_iso_1d_full_fluid": dict(n_theta=16, n_solid_layers=4, n_fluid_layers=2, nr_max=24,
+                                  three_d=False, attenuation="full"),
+}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
+@pytest.mark.parametrize("case", sorted(SPH))
+def test_spherical_shell_parity(built, case, precision):
+    """Spherical mapping, both axes, fluid layer with solid-fluid coupling, RTZ
+    rheology: solid and fluid stiffness of one evaluation, then five full steps."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.spherical_model(**SPH[case])
+    us = meshgen.random_displacement(m, seed=3)
+    uf = meshgen.random_displacement(m, seed=4, solid=False)
+    o = O.Oracle(m, "fp64")
+    o.set_field(us, "displ")
+    o.set_field(uf, "displ", solid=False)
+    o.compute_stiffness()
+    ref_s, ref_f = o.get_field("stiff"), o.get_field("stiff", solid=False)
+    tol = TOL_STIFF[precision]
+    with Solver(m, precision) as s:
+        s.set_field(us, "displ")
+        s.set_field(uf, "displ", solid=False)
+        s.compute_stiffness()
+        assert rel(s.get_field("stiff"), ref_s) <= tol
+        assert rel(s.get_field("stiff", solid=False), ref_f) <= tol
+    o2 = O.Oracle(m, "fp64")
+    o2.set_field(us * 1e-9, "displ")
+    o2.set_field(uf * 1e-9, "displ", solid=False)
+    o2.run(5)
+    with Solver(m, precision) as s:
+        s.set_field(us * 1e-9, "displ")
+        s.set_field(uf * 1e-9, "displ", solid=False)
+        s.run(5)
+        tol5 = 1e-11 if precision == "fp64" else 1e-5
+        assert rel(s.get_field("displ"), o2.get_field("displ")) <= tol5
+        assert rel(s.get_field("displ", solid=False), o2.get_field("displ", solid=False)) <= tol5
+
+
+def test_plain_and_autotuned_match(built):
+    """The plain method (one bucket, eager launches) and the autotuned batched path
+    compute the same steps."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.microbench_model(n_elem=300, nr_max=64, seed=41)
+    u = meshgen.random_displacement(m, seed=2) * 1e-6
+    out = []
+    for kw in (dict(plain=True), dict(autotune=True), dict()):
+        with Solver(m, "fp64", **kw) as s:
+            s.set_field(u, "displ")
+            s.run(3)
+            out.append(s.get_field("displ"))
+    assert rel(out[0], out[2]) <= 1e-13 and rel(out[1], out[2]) <= 1e-13

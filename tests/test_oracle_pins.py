@@ -228,3 +228,23 @@ def test_oracle_fp32_close_to_fp64(built):
     f64 = _stiff(O.Oracle(m, "fp64"), u)
     f32 = _stiff(O.Oracle(m, "fp32"), u)
     assert np.linalg.norm(f32 - f64) <= 1e-5 * np.linalg.norm(f64)
+
+
+def test_spherical_mapping_geometry(built):
+    """MappingSpherical: GLL points of a shell quad lie on their circles, the four
+    orientations of the same quad give the same points and the same integral factor."""
+    from axisem3d_b200 import _lib as L
+    from axisem3d_b200.solver import quad_geometry
+    r0, r1, t0, t1 = 4.0e6, 4.2e6, 0.3, 0.35
+    P = lambda t, r: (r * np.sin(t), r * np.cos(t))  # noqa: E731
+    n = [P(t0, r0), P(t1, r0), P(t1, r1), P(t0, r1)]
+    g, sz = quad_geometry(np.array(n).ravel(), False, L.AXG_MAP_SPHERICAL)
+    r = np.hypot(sz[0], sz[1]).reshape(5, 5)
+    assert np.allclose(r[:, 0], r0, rtol=1e-13) and np.allclose(r[:, 4], r1, rtol=1e-13)
+    ref = {tuple(np.round(p, 3)) for p in sz.T}
+    for rot in range(1, 4):
+        nn = n[rot:] + n[:rot]
+        g2, sz2 = quad_geometry(np.array(nn).ravel(), False, L.AXG_MAP_SPHERICAL)
+        assert {tuple(np.round(p, 3)) for p in sz2.T} == ref
+        assert np.isclose(np.sum(g2[5]), np.sum(g[5]), rtol=1e-12)
+    assert np.all(g[5] > 0)
