@@ -33,7 +33,7 @@ class axg_config(C.Structure):
                 ("att_alpha", C.c_double * AXG_MAX_SLS), ("att_beta", C.c_double * AXG_MAX_SLS),
                 ("att_gamma", C.c_double * AXG_MAX_SLS), ("stability_interval", C.c_int32),
                 ("deterministic", C.c_int32), ("compensated", C.c_int32), ("plain", C.c_int32),
-                ("autotune", C.c_int32)]
+                ("autotune", C.c_int32), ("nwave", C.c_int32)]
 
 
 class axg_solid_points(C.Structure):
@@ -71,16 +71,21 @@ class axg_stf(C.Structure):
 
 class axg_moment_sources(C.Structure):
     _fields_ = [("count", C.c_int32), ("element", P_i32), ("nu", P_i32), ("pattern_offset", P_i64),
-                ("pattern", P_f64), ("stf", C.POINTER(axg_stf))]
+                ("pattern", P_f64), ("stf", C.POINTER(axg_stf)), ("wavefield", P_i32)]
 
 
 class axg_force_sources(C.Structure):
     _fields_ = [("count", C.c_int32), ("element", P_i32), ("nu", P_i32), ("pattern_offset", P_i64),
-                ("pattern", P_f64), ("stf", C.POINTER(axg_stf))]
+                ("pattern", P_f64), ("stf", C.POINTER(axg_stf)), ("wavefield", P_i32)]
 
 
 class axg_stations(C.Structure):
     _fields_ = [("count", C.c_int32), ("element", P_i32), ("weights", P_f64), ("phi", P_f64)]
+
+
+class axg_clayton(C.Structure):
+    _fields_ = [("count", C.c_int32), ("point", P_i32), ("rho_vp", P_f64), ("rho_vs", P_f64),
+                ("area", P_f64), ("theta", P_f64)]
 
 
 # name -> (restype, argtypes) of every entry point declared in include/axg.h
@@ -98,6 +103,8 @@ SIGNATURES = {
     "axg_set_moment_sources": (C.c_int, [H, C.POINTER(axg_moment_sources)]),
     "axg_set_force_sources": (C.c_int, [H, C.POINTER(axg_force_sources)]),
     "axg_set_stations": (C.c_int, [H, C.POINTER(axg_stations), C.c_int32]),
+    "axg_set_clayton": (C.c_int, [H, C.c_int32, C.POINTER(axg_clayton)]),
+    "axg_set_sponge": (C.c_int, [H, C.c_int32, C.c_int32, P_i32, P_f64]),
     "axg_finalize": (C.c_int, [H]),
     "axg_apply_sources": (C.c_int, [H, C.c_int32]),
     "axg_compute_stiffness": (C.c_int, [H]),

@@ -81,7 +81,7 @@ int axg_create(const axg_config *cfg, axg_solver **out) {
     if (!cfg || !out) return AXG_E_ARG;
     *out = nullptr;
     if (cfg->precision < AXG_FP64 || cfg->precision > AXG_MIXED) return AXG_E_ARG;
-    if (!(cfg->dt > 0) || cfg->nsls < 0 || cfg->nsls > AXG_MAX_SLS) return AXG_E_ARG;
+    if (!(cfg->dt > 0) || cfg->nsls < 0 || cfg->nsls > AXG_MAX_SLS || cfg->nwave < 0) return AXG_E_ARG;
     axg_solver *h = new axg_solver();
     h->cfg = *cfg;
     try {
@@ -218,8 +218,8 @@ int axg_set_solid_fluid(axg_solver *h, const axg_solid_fluid *c) {
 }
 
 static void sources_from(axg::HostSources &s, int n, const int32_t *el, const int32_t *nu,
-                         const int64_t *po, const double *pat, const axg_stf *stf, int ndim,
-                         const char *who) {
+                         const int64_t *po, const double *pat, const axg_stf *stf, const int32_t *wave,
+                         int nwave, int ndim, const char *who) {
     if (n < 0 || (n && (!el || !nu || !po || !pat || !stf)))
         throw axg::Error(AXG_E_ARG, std::string(who) + " || missing array.");
     s.count = n;
@@ -227,6 +227,10 @@ static void sources_from(axg::HostSources &s, int n, const int32_t *el, const in
     s.nu = copy(nu, n);
     s.pat_off = copy(po, n);
     s.stf = copy(stf, n);
+    s.wave = wave ? copy(wave, n) : std::vector<int>(n, 0);
+    for (int i = 0; i < n; i++)
+        if (s.wave[i] < 0 || s.wave[i] >= nwave)
+            throw axg::Error(AXG_E_ARG, std::string(who) + " || wavefield index out of range.");
     size_t end = 0;
     for (int i = 0; i < n; i++) {
         if (nu[i] < 1) throw axg::Error(AXG_E_ARG, std::string(who) + " || pattern needs >= 1 mode.");
@@ -242,7 +246,7 @@ int axg_set_moment_sources(axg_solver *h, const axg_moment_sources *s) {
         need_open(h);
         if (!s) throw axg::Error(AXG_E_ARG, "SolidMoment || null description.");
         sources_from(h->model.ms, s->count, s->element, s->nu, s->pattern_offset, s->pattern, s->stf,
-                     6, "SolidMoment::SolidMoment");
+                     s->wavefield, std::max(1, h->cfg.nwave), 6, "SolidMoment::SolidMoment");
     });
 }
 
@@ -251,7 +255,7 @@ int axg_set_force_sources(axg_solver *h, const axg_force_sources *s) {
         need_open(h);
         if (!s) throw axg::Error(AXG_E_ARG, "SolidForce || null description.");
         sources_from(h->model.fs, s->count, s->element, s->nu, s->pattern_offset, s->pattern, s->stf,
-                     3, "SolidForce::SolidForce");
+                     s->wavefield, std::max(1, h->cfg.nwave), 3, "SolidForce::SolidForce");
     });
 }
 
@@ -266,6 +270,35 @@ int axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interv
         st.elem = copy(s->element, s->count);
         st.w = copy(s->weights, (size_t)s->count * 25);
         st.phi = copy(s->phi, s->count);
+    });
+}
+
+int axg_set_clayton(axg_solver *h, int32_t solid, const axg_clayton *c) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!c || c->count < 0 || (c->count && (!c->point || !c->rho_vp || !c->area ||
+                                                 (solid && (!c->rho_vs || !c->theta)))))
+            throw axg::Error(AXG_E_ARG, "ClaytonSolid1D || missing array.");
+        axg::HostClayton &x = solid ? h->model.cl_s : h->model.cl_f;
+        x.count = c->count;
+        x.pt = copy(c->point, c->count);
+        x.rvp = copy(c->rho_vp, c->count);
+        x.rvs = solid ? copy(c->rho_vs, c->count) : std::vector<double>(c->count, 0.);
+        x.area = copy(c->area, c->count);
+        x.theta = solid ? copy(c->theta, c->count) : std::vector<double>(c->count, 0.);
+        for (int i = 0; i < c->count; i++)
+            if (!solid && !(x.rvp[i] > 0)) throw axg::Error(AXG_E_ARG, "ClaytonFluid1D || rho vp must be positive.");
+    });
+}
+
+int axg_set_sponge(axg_solver *h, int32_t solid, int32_t count, const int32_t *point, const double *gamma) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (count < 0 || (count && (!point || !gamma))) throw axg::Error(AXG_E_ARG, "Sponge || missing array.");
+        axg::HostSponge &x = solid ? h->model.sg_s : h->model.sg_f;
+        x.count = count;
+        x.pt = copy(point, count);
+        x.gamma = copy(gamma, count);
     });
 }
 
@@ -299,6 +332,22 @@ int axg_finalize(axg_solver *h) {
         for (int i = 0; i < m.st.count; i++)
             if (m.st.elem[i] < 0 || m.st.elem[i] >= m.se.count)
                 throw axg::Error(AXG_E_ARG, "StationSolid || element index out of range.");
+        for (int i = 0; i < m.cl_s.count; i++)
+            if (m.cl_s.pt[i] < 0 || m.cl_s.pt[i] >= m.sp.count)
+                throw axg::Error(AXG_E_ARG, "ClaytonSolid1D || point index out of range.");
+        for (int i = 0; i < m.cl_f.count; i++)
+            if (m.cl_f.pt[i] < 0 || m.cl_f.pt[i] >= m.fp.count)
+                throw axg::Error(AXG_E_ARG, "ClaytonFluid1D || point index out of range.");
+        // one Sponge per point (GLLPoint::release averages the boundaries' gammas first)
+        for (const auto &sg : {std::make_pair(&m.sg_s, m.sp.count), std::make_pair(&m.sg_f, m.fp.count)}) {
+            std::vector<char> seen(sg.second, 0);
+            for (int i = 0; i < sg.first->count; i++) {
+                const int p = sg.first->pt[i];
+                if (p < 0 || p >= sg.second) throw axg::Error(AXG_E_ARG, "Sponge || point index out of range.");
+                if (seen[p]) throw axg::Error(AXG_E_ARG, "Sponge || point listed twice.");
+                seen[p] = 1;
+            }
+        }
         h->eng->finalize(m);
         h->finalized = true;
     });

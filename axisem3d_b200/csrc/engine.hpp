@@ -53,7 +53,7 @@ struct HostCoupling {
 
 struct HostSources {
     int count = 0;
-    std::vector<int> elem, nu;
+    std::vector<int> elem, nu, wave;
     std::vector<int64_t> pat_off;
     std::vector<double> pattern;   // (re, im) pairs
     std::vector<axg_stf> stf;
@@ -65,7 +65,21 @@ struct HostStations {
     std::vector<double> w, phi;
 };
 
+struct HostClayton {
+    int count = 0;
+    std::vector<int> pt;
+    std::vector<double> rvp, rvs, area, theta;
+};
+
+struct HostSponge {
+    int count = 0;
+    std::vector<int> pt;
+    std::vector<double> gamma;
+};
+
 struct HostModel {
+    HostClayton cl_s, cl_f;
+    HostSponge sg_s, sg_f;
     HostPoints sp, fp;
     HostSolidElements se;
     HostFluidElements fe;

@@ -123,6 +123,7 @@ class Engine final : public EngineBase {
 
 public:
     explicit Engine(const axg_config &c) : cfg_(c) {
+        nwave_ = std::max(1, cfg_.nwave);
         AXG_CUDA(cudaSetDevice(cfg_.device));
         AXG_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
         stream_ = own_stream_;
@@ -168,6 +169,7 @@ public:
         build_fluid_buckets(m.fe);
         if (cfg_.autotune && !cfg_.plain) autotune();
         build_coupling(m.sf);
+        build_abc(m);
         build_sources(m.ms, m.fs);
         build_stations(m.st);
         step_dev_.alloc(1);
@@ -189,7 +191,7 @@ public:
         launch_sources();
     }
     void compute_stiffness() override { need(); launch_stiffness(); }
-    void bc_before() override { need(); launch_coupling(); }
+    void bc_before() override { need(); launch_clayton(); launch_coupling(); }
     void point_stage(int mask) override { need(); launch_points(mask); }
     void record(int tstep) override {
         need();
@@ -230,12 +232,12 @@ public:
     // ------------------------------------------------------------- fields ---
     int64_t field_size(int solid) const override {
         const PointDev &P = solid ? sp_ : fp_;
-        return (int64_t)P.total * P.ndim;
+        return (int64_t)P.total * P.ndim * nwave_;
     }
     void get_field(int solid, int which, double *out) override {
         need();
         PointDev &P = solid ? sp_ : fp_;
-        size_t n = (size_t)P.total * P.ndim;
+        size_t n = (size_t)P.total * P.ndim * nwave_;
         if (!n) return;
         AXG_CUDA(cudaStreamSynchronize(stream_));
         if (which == AXG_FIELD_DISPL || which == AXG_FIELD_VELOC) {
@@ -253,7 +255,7 @@ public:
     void set_field(int solid, int which, const double *in) override {
         need();
         PointDev &P = solid ? sp_ : fp_;
-        size_t n = (size_t)P.total * P.ndim;
+        size_t n = (size_t)P.total * P.ndim * nwave_;
         if (!n) return;
         AXG_CUDA(cudaStreamSynchronize(stream_));
         if (which == AXG_FIELD_DISPL || which == AXG_FIELD_VELOC) {
@@ -279,7 +281,7 @@ public:
     }
     int64_t field_raw_bytes(int solid, int which) const override {
         const PointDev &P = solid ? sp_ : fp_;
-        size_t n = (size_t)P.total * P.ndim;
+        size_t n = (size_t)P.total * P.ndim * nwave_;
         bool dv = which == AXG_FIELD_DISPL || which == AXG_FIELD_VELOC;
         return (int64_t)(n * (dv ? sizeof(CD) : sizeof(C)));
     }
@@ -299,7 +301,7 @@ public:
         if (!bytes) return;
         AXG_CUDA(cudaMemcpyAsync(field_ptr(P, which), host, bytes, cudaMemcpyHostToDevice, stream_));
         if (which == AXG_FIELD_DISPL && P.displ_elem.p) {
-            size_t n = (size_t)P.total * P.ndim;
+            size_t n = (size_t)P.total * P.ndim * nwave_;
             narrow_kernel<T, D><<<(unsigned)((n + 255) / 256), 256, 0, stream_>>>(P.displ.p, P.displ_elem.p, n);
             post_launch();
         }
@@ -322,7 +324,7 @@ public:
         int nrec = 0;
         if (st_n_ > 0) nrec = std::min(seis_cap_, (step_ + st_interval_ - 1) / st_interval_);
         if (out && nrec > 0)
-            AXG_CUDA(cudaMemcpy(out, seis_.p, (size_t)nrec * st_n_ * 3 * sizeof(double),
+            AXG_CUDA(cudaMemcpy(out, seis_.p, (size_t)nrec * nwave_ * st_n_ * 3 * sizeof(double),
                                 cudaMemcpyDeviceToHost));
         return nrec;
     }
@@ -342,8 +344,8 @@ public:
         double b = 0, f = 0;
         for (auto &bk : sb_) { b += bk->bytes; f += bk->flops; }
         for (auto &bk : fb_) { b += bk->bytes; f += bk->flops; }
-        // points: read u once, write f once
-        b += (double)sp_.total * 3 * 2 * sizeof(C) + (double)fp_.total * 2 * sizeof(C);
+        // points: read u once, write f once, per wavefield
+        b += nwave_ * ((double)sp_.total * 3 * 2 * sizeof(C) + (double)fp_.total * 2 * sizeof(C));
         *bytes = b;
         *flops = f;
     }
@@ -356,7 +358,7 @@ public:
             per += 4 * sizeof(CD);                         // d, v read + write
             if (COMP) per += 4 * sizeof(cx_t<float>);      // compensation terms
             if (P->displ_elem.p) per += sizeof(C);         // element copy of d
-            b += per * (double)P->total * P->ndim;
+            b += per * (double)P->total * P->ndim * nwave_;
         }
         return b;
     }
@@ -492,6 +494,7 @@ private:
     void check_adjoint_model() const {
         const HostSolidElements &h = model_.se;
         if (fp_.n > 0) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || fluid elements are not differentiated.");
+        if (nwave_ != 1) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || one wavefield per handle.");
         for (int e = 0; e < h.count; e++) {
             bool ok = h.rheo[e] == AXG_ISO && !(h.is3d.size() && h.is3d[e]) &&
                       !(h.att.size() && h.att[e] != AXG_ATT_NONE);
@@ -603,7 +606,7 @@ private:
         P.flags.upload(flags); P.inv1.upload(inv1);
         if (inv3.empty()) inv3.push_back((T)0);
         P.inv3.upload(inv3); P.im_off.upload(im_off);
-        size_t nf = (size_t)P.total * P.ndim;
+        size_t nf = (size_t)P.total * P.ndim * nwave_;
         P.stiff.alloc(nf); P.stiff.zero(stream_);
         P.accel.alloc(nf); P.accel.zero(stream_);
         P.displ.alloc(nf); P.displ.zero(stream_);
@@ -619,30 +622,40 @@ private:
 
     // ------------------------------------------------------- solid buckets ---
     using SolidKernel = void (*)(const SolidArgs<T, AT>, int, int, int, size_t);
+    // NS: the register-resident slice path is built for 3 and 5 SLS (3-D elements);
+    // other counts and 1-D elements take the generic path
     template <int RHEO, int ATT, bool IS3D, bool RTZ>
-    static SolidKernel pick4() { return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ>; }
+    static SolidKernel pick4(int nsls) {
+#ifndef AXG_GENERIC_SLS_ONLY
+        if constexpr (IS3D && ATT != ATT_NONE) {
+            if (nsls == 3) return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 3>;
+            if (nsls == 5) return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 5>;
+        }
+#endif
+        return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 0>;
+    }
     template <int RHEO, int ATT, bool IS3D>
-    static SolidKernel pick3(bool rtz) {
-        if constexpr (RHEO == RHEO_ISO) return pick4<RHEO, ATT, IS3D, false>();
-        else return rtz ? pick4<RHEO, ATT, IS3D, true>() : pick4<RHEO, ATT, IS3D, false>();
+    static SolidKernel pick3(bool rtz, int nsls) {
+        if constexpr (RHEO == RHEO_ISO) return pick4<RHEO, ATT, IS3D, false>(nsls);
+        else return rtz ? pick4<RHEO, ATT, IS3D, true>(nsls) : pick4<RHEO, ATT, IS3D, false>(nsls);
     }
     template <int RHEO, int ATT>
-    static SolidKernel pick2(bool is3d, bool rtz) {
-        return is3d ? pick3<RHEO, ATT, true>(rtz) : pick3<RHEO, ATT, false>(rtz);
+    static SolidKernel pick2(bool is3d, bool rtz, int nsls) {
+        return is3d ? pick3<RHEO, ATT, true>(rtz, nsls) : pick3<RHEO, ATT, false>(rtz, nsls);
     }
     template <int RHEO>
-    static SolidKernel pick1(int att, bool is3d, bool rtz) {
+    static SolidKernel pick1(int att, bool is3d, bool rtz, int nsls) {
         switch (att) {
-            case ATT_NONE: return pick2<RHEO, ATT_NONE>(is3d, rtz);
-            case ATT_FULL: return pick2<RHEO, ATT_FULL>(is3d, rtz);
-            default: return pick2<RHEO, ATT_CG4>(is3d, rtz);
+            case ATT_NONE: return pick2<RHEO, ATT_NONE>(is3d, rtz, nsls);
+            case ATT_FULL: return pick2<RHEO, ATT_FULL>(is3d, rtz, nsls);
+            default: return pick2<RHEO, ATT_CG4>(is3d, rtz, nsls);
         }
     }
-    static SolidKernel pick_solid(int rheo, int att, bool is3d, bool rtz) {
+    static SolidKernel pick_solid(int rheo, int att, bool is3d, bool rtz, int nsls) {
         switch (rheo) {
-            case RHEO_ISO: return pick1<RHEO_ISO>(att, is3d, rtz);
-            case RHEO_TISO: return pick1<RHEO_TISO>(att, is3d, rtz);
-            default: return pick1<RHEO_ANISO>(att, is3d, rtz);
+            case RHEO_ISO: return pick1<RHEO_ISO>(att, is3d, rtz, nsls);
+            case RHEO_TISO: return pick1<RHEO_TISO>(att, is3d, rtz, nsls);
+            default: return pick1<RHEO_ANISO>(att, is3d, rtz, nsls);
         }
     }
 
@@ -721,19 +734,19 @@ private:
                 if (b->att != ATT_NONE) {
                     bytes += 2.0 * ns * npa * s;                          // dlambda, dmu
                     double slots = b->is3d ? (double)enr * npa : (double)enu * npa * 2;
-                    bytes += 2.0 * (cfg_.nsls + 1) * 6 * slots * sa;      // state read + write
+                    bytes += 2.0 * (cfg_.nsls + 1) * 6 * slots * sa * nwave_;   // state read + write
                 }
                 if (b->rtz) bytes += 25 * s;                              // theta
-                flops += (double)enu * 25 * (2 * 3 * 10 * 4 + 60);        // gradient
-                flops += (double)enu * 25 * (2 * 3 * 10 * 4 + 60);        // quadrature
+                flops += nwave_ * (double)enu * 25 * (2 * 3 * 10 * 4 + 60);   // gradient
+                flops += nwave_ * (double)enu * 25 * (2 * 3 * 10 * 4 + 60);   // quadrature
                 double pw = nm == 2 ? 16 : nm == 5 ? 22 : 72;             // stress per point
                 if (b->is3d) {
-                    flops += 2.0 * 150 * enr * enu * 4;                   // two direct DFTs
-                    flops += (double)enr * 25 * pw;
-                    if (b->att != ATT_NONE) flops += (double)enr * npa * (cfg_.nsls * 6 * 4 + 14);
+                    flops += nwave_ * 2.0 * 150 * enr * enu * 4;          // two direct DFTs
+                    flops += nwave_ * (double)enr * 25 * pw;
+                    if (b->att != ATT_NONE) flops += nwave_ * (double)enr * npa * (cfg_.nsls * 6 * 4 + 14);
                 } else {
-                    flops += (double)enu * 25 * pw * 2;
-                    if (b->att != ATT_NONE) flops += (double)enu * npa * 2 * (cfg_.nsls * 6 * 4 + 14);
+                    flops += nwave_ * (double)enu * 25 * pw * 2;
+                    if (b->att != ATT_NONE) flops += nwave_ * (double)enu * npa * 2 * (cfg_.nsls * 6 * 4 + 14);
                 }
             }
             b->bytes = bytes;
@@ -747,11 +760,12 @@ private:
             b->mod.upload(mod); b->attmod.upload(attm);
             b->mod_off.upload(moff); b->att_off.upload(aoff);
             state_offs.push_back(soff);
-            b->kernel = pick_solid(b->rheo, b->att, b->is3d, b->rtz);
+            b->kernel = pick_solid(b->rheo, b->att, b->is3d, b->rtz, cfg_.nsls);
             configure_bucket(*b);
             sb_.push_back(std::move(b));
         }
-        state_.alloc(std::max<int64_t>(state_total, 1));
+        state_wave_ = state_total;
+        state_.alloc(std::max<int64_t>(state_total * nwave_, 1));
         state_.zero(stream_);
         for (size_t i = 0; i < sb_.size(); i++) sb_[i]->state_off.upload(state_offs[i]);
     }
@@ -780,6 +794,9 @@ private:
         AXG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b.kernel, team * tpc,
                                                                tpc * L.total));
         b.grid = std::max(1, std::min((b.n + tpc - 1) / tpc, std::max(1, per_sm) * prop_.multiProcessorCount));
+#ifdef AXG_NO_PERSISTENT_GRID
+        b.grid = (b.n + tpc - 1) / tpc;
+#endif
         if (cfg_.plain) b.grid = (b.n + tpc - 1) / tpc;   // one team per element, no persistence
     }
 
@@ -910,6 +927,68 @@ private:
         cp_nsu_.upload(nsu); cp_nzu_.upload(nzu); cp_nsa_.upload(nsa); cp_nza_.upload(nza);
     }
 
+    void build_abc(const HostModel &m) {
+        // ClaytonSolid1D / ClaytonFluid1D constructors: coefficients in double, cast to Real
+        auto solid = [&](const HostClayton &h) {
+            std::vector<T> c((size_t)4 * h.count);
+            for (int i = 0; i < h.count; i++) {
+                const double ct = std::cos(h.theta[i]), st = std::sin(h.theta[i]);
+                const double rsa = h.rvs[i] * h.area[i], rpa = h.rvp[i] * h.area[i];
+                c[4 * i] = (T)(rsa * ct * ct + rpa * st * st);
+                c[4 * i + 1] = (T)(rsa * st * st + rpa * ct * ct);
+                c[4 * i + 2] = (T)((rpa - rsa) * ct * st);
+                c[4 * i + 3] = (T)rsa;
+            }
+            return c;
+        };
+        // group conditions per point, keeping the given order within a point
+        auto group = [](const std::vector<int> &pt, int ncoef, const std::vector<T> &c, DBuf<int> &upt,
+                        DBuf<int> &first, DBuf<T> &cdev) {
+            std::vector<int> idx(pt.size());
+            for (size_t i = 0; i < idx.size(); i++) idx[i] = (int)i;
+            std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return pt[x] < pt[y]; });
+            std::vector<int> u, f;
+            std::vector<T> cs;
+            for (size_t k = 0; k < idx.size(); k++) {
+                if (k == 0 || pt[idx[k]] != pt[idx[k - 1]]) { u.push_back(pt[idx[k]]); f.push_back((int)k); }
+                for (int j = 0; j < ncoef; j++) cs.push_back(c[(size_t)idx[k] * ncoef + j]);
+            }
+            f.push_back((int)idx.size());
+            upt.upload(u); first.upload(f); cdev.upload(cs);
+            return (int)u.size();
+        };
+        cls_n_ = m.cl_s.count ? group(m.cl_s.pt, 4, solid(m.cl_s), cls_pt_, cls_first_, cls_c_) : 0;
+        clf_n_ = 0;
+        if (m.cl_f.count) {
+            std::vector<T> c(m.cl_f.count);
+            for (int i = 0; i < m.cl_f.count; i++) c[i] = (T)(m.cl_f.area[i] / m.cl_f.rvp[i]);
+            clf_n_ = group(m.cl_f.pt, 1, c, clf_pt_, clf_first_, clf_c_);
+        }
+        auto sponge = [&](const HostSponge &h, int np, DBuf<T> &out) {
+            if (!h.count) return;
+            std::vector<T> g(np, (T)0);
+            for (int i = 0; i < h.count; i++) g[h.pt[i]] = (T)h.gamma[i];
+            out.upload(g);
+        };
+        sponge(m.sg_s, sp_.n, sg_s_);
+        sponge(m.sg_f, fp_.n, sg_f_);
+    }
+
+    void launch_clayton() {
+        for (int solid = 1; solid >= 0; solid--) {
+            const int n = solid ? cls_n_ : clf_n_;
+            if (!n) continue;
+            PointDev &P = solid ? sp_ : fp_;
+            ClaytonArgs<T, D> a;
+            a.n = n; a.ndim = P.ndim; a.pt = solid ? cls_pt_.p : clf_pt_.p; a.off = P.off.p; a.nu = P.nu.p;
+            a.first = solid ? cls_first_.p : clf_first_.p;
+            a.c = solid ? cls_c_.p : clf_c_.p; a.veloc = P.veloc.p; a.stiff = P.stiff.p;
+            a.nwave = nwave_; a.fstride = (size_t)P.total * P.ndim;
+            clayton_kernel<T, D><<<(n * 32 + 255) / 256, 256, 0, stream_>>>(a);
+            post_launch();
+        }
+    }
+
     void build_sources(const HostSources &ms, const HostSources &fs) {
         auto conv = [](const HostSources &h, DBuf<int> &el, DBuf<int> &nu, DBuf<int64_t> &po,
                        DBuf<C> &pat) {
@@ -924,8 +1003,8 @@ private:
         };
         ms_n_ = ms.count;
         fs_n_ = fs.count;
-        if (ms_n_) conv(ms, ms_el_, ms_nu_, ms_po_, ms_pat_);
-        if (fs_n_) conv(fs, fs_el_, fs_nu_, fs_po_, fs_pat_);
+        if (ms_n_) { conv(ms, ms_el_, ms_nu_, ms_po_, ms_pat_); ms_wave_.upload(ms.wave); }
+        if (fs_n_) { conv(fs, fs_el_, fs_nu_, fs_po_, fs_pat_); fs_wave_.upload(fs.wave); }
         for (int i = 0; i < ms.count; i++)
             if (ms.elem[i] < 0 || ms.elem[i] >= model_.se.count)
                 throw Error(AXG_E_ARG, "SolidMoment::SolidMoment || element index out of range.");
@@ -971,10 +1050,10 @@ private:
             if (need_rec > seis_cap_) {
                 int cap = std::max(need_rec, 2 * seis_cap_);
                 DBuf<double> nb;
-                nb.alloc((size_t)cap * st_n_ * 3);
+                nb.alloc((size_t)cap * nwave_ * st_n_ * 3);
                 nb.zero(stream_);
                 if (seis_cap_)
-                    AXG_CUDA(cudaMemcpyAsync(nb.p, seis_.p, (size_t)seis_cap_ * st_n_ * 3 * sizeof(double),
+                    AXG_CUDA(cudaMemcpyAsync(nb.p, seis_.p, (size_t)seis_cap_ * nwave_ * st_n_ * 3 * sizeof(double),
                                              cudaMemcpyDeviceToDevice, stream_));
                 AXG_CUDA(cudaStreamSynchronize(stream_));
                 std::swap(seis_.p, nb.p); std::swap(seis_.n, nb.n);
@@ -1021,6 +1100,7 @@ private:
             a.pattern = ms_pat_.p; a.stf = ms_stf_.p; a.stf_steps = stf_cap_; a.step = step_dev_.p;
             a.e_nr = e_nr_.p; a.e_pts = e_pts_.p; a.e_axial = e_axial_.p; a.e_geom = e_geom_.p;
             a.pt_off = sp_.off.p; a.pt_nu = sp_.nu.p; a.stiff = sp_.stiff.p; a.gmat = gmat_.p;
+            a.wave = ms_wave_.p; a.fstride = (size_t)sp_.total * 3;
             moment_source_kernel<T><<<ms_n_, 128, 0, stream_>>>(a);
             post_launch();
         }
@@ -1029,6 +1109,7 @@ private:
             a.nsrc = fs_n_; a.elem = fs_el_.p; a.nu = fs_nu_.p; a.pat_off = fs_po_.p;
             a.pattern = fs_pat_.p; a.stf = fs_stf_.p; a.stf_steps = stf_cap_; a.step = step_dev_.p;
             a.e_pts = e_pts_.p; a.pt_off = sp_.off.p; a.pt_nu = sp_.nu.p; a.stiff = sp_.stiff.p;
+            a.wave = fs_wave_.p; a.fstride = (size_t)sp_.total * 3;
             force_source_kernel<T><<<fs_n_, 128, 0, stream_>>>(a);
             post_launch();
         }
@@ -1055,6 +1136,9 @@ private:
                 a.gamma[l] = (AT)cfg_.att_gamma[l];
             }
             a.gmat = gmat_.p;
+            a.nwave = nwave_;
+            a.fstride = (size_t)sp_.total * 3;
+            a.sstride = (size_t)state_wave_;
             b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc,
                                                                               b.tpc, b.team_bytes);
             post_launch();
@@ -1069,6 +1153,8 @@ private:
             a.K = b.K.p; a.K_off = b.K_off.p; a.pt_off = fp_.off.p; a.pt_nu = fp_.nu.p;
             a.displ = elem_displ(fp_); a.stiff = fp_.stiff.p; a.tw = tw_.p; a.tw_off = tw_off_.p;
             a.gmat = gmat_.p;
+            a.nwave = nwave_;
+            a.fstride = (size_t)fp_.total;
             int blocks = (b.n + b.tpc - 1) / b.tpc;
             b.kernel<<<blocks, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.tpc,
                                                                               b.team_bytes);
@@ -1083,6 +1169,7 @@ private:
         a.nsu = cp_nsu_.p; a.nzu = cp_nzu_.p; a.nsa_m = cp_nsa_.p; a.nza_m = cp_nza_.p;
         a.s_off = sp_.off.p; a.f_off = fp_.off.p; a.f_nu = fp_.nu.p;
         a.s_displ = elem_displ(sp_); a.s_stiff = sp_.stiff.p; a.f_stiff = fp_.stiff.p;
+        a.nwave = nwave_; a.s_stride = (size_t)sp_.total * 3; a.f_stride = (size_t)fp_.total;
         int threads = 256, blocks = (cp_n_ * 32 + threads - 1) / threads;
         solid_fluid_kernel<T><<<blocks, threads, 0, stream_>>>(a);
         post_launch();
@@ -1095,7 +1182,8 @@ private:
         a.e_nr = e_nr_.p; a.e_pts = e_pts_.p; a.pt_off = sp_.off.p; a.pt_nu = sp_.nu.p;
         a.displ = elem_displ(sp_); a.out = seis_.p; a.interval = st_interval_;
         a.max_rec = seis_cap_; a.step = step_dev_.p;
-        int threads = 128, blocks = (st_n_ * 3 + threads - 1) / threads;
+        a.nwave = nwave_; a.fstride = (size_t)sp_.total * 3;
+        int threads = 128, blocks = (st_n_ * 3 * nwave_ + threads - 1) / threads;
         station_kernel<T><<<blocks, threads, 0, stream_>>>(a);
         post_launch();
     }
@@ -1109,8 +1197,9 @@ private:
                 a.n = P.n3d; a.pt = P.pt3d.p; a.nr = P.nr.p; a.off = P.off.p; a.flags = P.flags.p;
                 a.inv_mass = P.inv3.p; a.im_off = P.im_off.p; a.tw = tw_.p; a.tw_off = tw_off_.p;
                 a.stiff = P.stiff.p; a.ndim = P.ndim; a.solid = solid; a.nr_max = P.nr_max;
+                a.nwave = nwave_; a.fstride = (size_t)P.total * P.ndim;
                 int wpb = 4;
-                mass3d_kernel<T><<<(P.n3d + wpb - 1) / wpb, 32 * wpb, wpb * P.nr_max * sizeof(T), stream_>>>(a);
+                mass3d_kernel<T><<<(P.n3d * nwave_ + wpb - 1) / wpb, 32 * wpb, wpb * P.nr_max * sizeof(T), stream_>>>(a);
                 post_launch();
             }
             PointArgs<T, D> a;
@@ -1126,7 +1215,9 @@ private:
             }
             a.nonfinite = nonfinite_.p;
             a.mask = mask;
-            int threads = 256, blocks = (P.total + threads - 1) / threads;
+            a.nwave = nwave_;
+            a.sponge = solid ? sg_s_.p : sg_f_.p;
+            int threads = 256, blocks = (int)(((int64_t)P.total * nwave_ + threads - 1) / threads);
             point_update_kernel<T, D, COMP><<<blocks, threads, 0, stream_>>>(a);
             post_launch();
         }
@@ -1135,6 +1226,7 @@ private:
     void launch_step() {
         launch_sources();
         launch_stiffness();
+        launch_clayton();
         launch_coupling();
         launch_stations();
         launch_points(7);
@@ -1202,7 +1294,12 @@ private:
     DBuf<int> cp_sp_, cp_fp_;
     DBuf<T> cp_nsu_, cp_nzu_, cp_nsa_, cp_nza_;
     int ms_n_ = 0, fs_n_ = 0, stf_cap_ = 0;
-    DBuf<int> ms_el_, ms_nu_, fs_el_, fs_nu_;
+    DBuf<int> ms_el_, ms_nu_, fs_el_, fs_nu_, ms_wave_, fs_wave_;
+    int nwave_ = 1;
+    int64_t state_wave_ = 0;
+    int cls_n_ = 0, clf_n_ = 0;
+    DBuf<int> cls_pt_, clf_pt_, cls_first_, clf_first_;
+    DBuf<T> cls_c_, clf_c_, sg_s_, sg_f_;
     DBuf<int64_t> ms_po_, fs_po_;
     DBuf<C> ms_pat_, fs_pat_;
     DBuf<T> ms_stf_, fs_stf_;

@@ -29,6 +29,8 @@ struct FluidArgs {
     const T *tw;
     const int *tw_off;
     const T *gmat;
+    int nwave;
+    size_t fstride;
 };
 
 template <class T>
@@ -100,9 +102,12 @@ fluid_stiffness_kernel(const FluidArgs<T> a, const int nr_max, const int teams_p
             for (int i = lane; i < 2 * nr; i += TEAM) sTw[i] = tw[i];
         }
         team_sync(team, TEAM);
+        for (int w = 0; w < a.nwave; w++) {
+        const C *displw = a.displ + (size_t)w * a.fstride;
+        C *stiffw = a.stiff + (size_t)w * a.fstride;
         for (int i = lane; i < nu * 25; i += TEAM) {
             const int q = i / nu, al = i - q * nu;
-            rBc[al * 25 + q] = al < sNu[q] ? a.displ[sOff[q] + al] : mk<T>(0, 0);
+            rBc[al * 25 + q] = al < sNu[q] ? displw[sOff[q] + al] : mk<T>(0, 0);
         }
         team_sync(team, TEAM);
         const int64_t koff = a.K_off[e];
@@ -228,9 +233,10 @@ fluid_stiffness_kernel(const FluidArgs<T> a, const int nr_max, const int teams_p
                     f = csub(f, b);
                 }
             }
-            if (al < sNu[q]) atomic_add_cx(a.stiff + sOff[q] + al, mk<T>(-f.x, -f.y));
+            if (al < sNu[q]) atomic_add_cx(stiffw + sOff[q] + al, mk<T>(-f.x, -f.y));
         }
         team_sync(team, TEAM);
+        }   // wavefields
     }
 }
 

@@ -31,6 +31,8 @@ struct CouplingArgs {
     const int *s_off, *f_off, *f_nu;
     const cx_t<T> *s_displ;
     cx_t<T> *s_stiff, *f_stiff;
+    int nwave;
+    size_t s_stride, f_stride;     // complex values between wavefields
 };
 
 template <class T>
@@ -42,16 +44,72 @@ __global__ void solid_fluid_kernel(const CouplingArgs<T> a) {
     const int s = a.sp[pair], f = a.fp[pair];
     const int nu = a.f_nu[f];
     const T nsu = a.nsu[pair], nzu = a.nzu[pair], nsa = a.nsa_m[pair], nza = a.nza_m[pair];
-    for (int al = lane; al < nu; al += 32) {
-        const cx_t<T> us = a.s_displ[(size_t)(a.s_off[s] + al) * 3 + 0];
-        const cx_t<T> uz = a.s_displ[(size_t)(a.s_off[s] + al) * 3 + 2];
-        cx_t<T> fs = a.f_stiff[a.f_off[f] + al];
-        fs = cadd(fs, cscale(us, nsu));
-        fs = cadd(fs, cscale(uz, nzu));
-        a.f_stiff[a.f_off[f] + al] = fs;
-        cx_t<T> *ss = a.s_stiff + (size_t)(a.s_off[s] + al) * 3;
-        ss[0] = csub(ss[0], cscale(fs, nsa));
-        ss[2] = csub(ss[2], cscale(fs, nza));
+    for (int w = 0; w < a.nwave; w++) {
+        const cx_t<T> *sd = a.s_displ + (size_t)w * a.s_stride;
+        cx_t<T> *sst = a.s_stiff + (size_t)w * a.s_stride;
+        cx_t<T> *fst = a.f_stiff + (size_t)w * a.f_stride;
+        for (int al = lane; al < nu; al += 32) {
+            const cx_t<T> us = sd[(size_t)(a.s_off[s] + al) * 3 + 0];
+            const cx_t<T> uz = sd[(size_t)(a.s_off[s] + al) * 3 + 2];
+            cx_t<T> fs = fst[a.f_off[f] + al];
+            fs = cadd(fs, cscale(us, nsu));
+            fs = cadd(fs, cscale(uz, nzu));
+            fst[a.f_off[f] + al] = fs;
+            cx_t<T> *ss = sst + (size_t)(a.s_off[s] + al) * 3;
+            ss[0] = csub(ss[0], cscale(fs, nsa));
+            ss[2] = csub(ss[2], cscale(fs, nza));
+        }
+    }
+}
+
+// ----------------------------------------------------- Clayton-Engquist ABC ---
+// ClaytonSolid1D::apply (ABC/ClaytonSolid1D.cpp:16-29) and ClaytonFluid1D::apply
+// (ABC/ClaytonFluid1D.cpp:16-24): stiff -= C veloc, one warp per point, lanes over modes.
+// A point on several boundaries (a corner) carries one condition per boundary, applied in
+// the order given; conditions are grouped per point (first[i] .. first[i+1]) so that one
+// warp owns the point and no two warps update the same stiffness entries.
+template <class T, class D>
+struct ClaytonArgs {
+    int n, ndim;                 // n distinct points
+    const int *pt, *first;       // point index; conditions of point i: first[i] .. first[i+1]-1
+    const int *off, *nu;
+    const T *c;                  // per condition; solid: [4] (ss, zz, sz, pp); fluid: area / (rho vp)
+    const cx_t<D> *veloc;
+    cx_t<T> *stiff;
+    int nwave;
+    size_t fstride;
+};
+
+template <class T, class D>
+__global__ void clayton_kernel(const ClaytonArgs<T, D> a) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x & 31;
+    if (i >= a.n) return;
+    const int p = a.pt[i];
+    const int c0 = a.first[i], c1 = a.first[i + 1];
+    for (int w = 0; w < a.nwave; w++) {
+        const cx_t<D> *v = a.veloc + (size_t)w * a.fstride;
+        cx_t<T> *f = a.stiff + (size_t)w * a.fstride;
+        for (int al = lane; al < a.nu[p]; al += 32) {
+            const size_t q = (size_t)(a.off[p] + al) * a.ndim;
+            if (a.ndim == 3) {
+                const cx_t<T> v0 = mk<T>((T)v[q].x, (T)v[q].y), v1 = mk<T>((T)v[q + 1].x, (T)v[q + 1].y),
+                              v2 = mk<T>((T)v[q + 2].x, (T)v[q + 2].y);
+                cx_t<T> f0 = f[q], f1 = f[q + 1], f2 = f[q + 2];
+                for (int k = c0; k < c1; k++) {
+                    const T css = a.c[4 * k], czz = a.c[4 * k + 1], csz = a.c[4 * k + 2], cpp = a.c[4 * k + 3];
+                    f0 = csub(f0, cadd(cscale(v0, css), cscale(v2, csz)));
+                    f2 = csub(f2, cadd(cscale(v0, csz), cscale(v2, czz)));
+                    f1 = csub(f1, cscale(v1, cpp));
+                }
+                f[q] = f0; f[q + 1] = f1; f[q + 2] = f2;
+            } else {
+                const cx_t<T> v0 = mk<T>((T)v[q].x, (T)v[q].y);
+                cx_t<T> f0 = f[q];
+                for (int k = c0; k < c1; k++) f0 = csub(f0, cscale(v0, a.c[k]));
+                f[q] = f0;
+            }
+        }
     }
 }
 
@@ -70,6 +128,8 @@ struct Mass3DArgs {
     int ndim;
     int solid;
     int nr_max;                  // scratch reals per warp
+    int nwave;
+    size_t fstride;
 };
 
 // Boundary conditions on one mode of one point, in the reference order:
@@ -107,8 +167,10 @@ __global__ void mass3d_kernel(const Mass3DArgs<T> a) {
     // C2R -> x 1/M_k -> R2C with a per-warp scratch of nr reals
     extern __shared__ __align__(16) unsigned char sm[];
     const int w = threadIdx.x / 32, lane = threadIdx.x & 31;
-    const int ip = blockIdx.x * (blockDim.x / 32) + w;
-    if (ip >= a.n) return;
+    const int item = blockIdx.x * (blockDim.x / 32) + w;
+    if (item >= a.n * a.nwave) return;
+    const int ip = item % a.n, wf = item / a.n;
+    cx_t<T> *stiff = a.stiff + (size_t)wf * a.fstride;
     const int p = a.pt[ip];
     const int nr = a.nr[p], nu = nr / 2 + 1, off = a.off[p], nd = a.ndim;
     const uint8_t fl = a.flags[p];
@@ -116,20 +178,20 @@ __global__ void mass3d_kernel(const Mass3DArgs<T> a) {
     const T *twc = a.tw + a.tw_off[nr], *tws = twc + nr;
     for (int al = lane; al < nu; al += 32) {
         cx_t<T> f[3];
-        for (int d = 0; d < nd; d++) f[d] = a.stiff[(size_t)(off + al) * nd + d];
+        for (int d = 0; d < nd; d++) f[d] = stiff[(size_t)(off + al) * nd + d];
         point_bc<T>(f, nd, al, nu, nr, fl, a.solid);
-        for (int d = 0; d < nd; d++) a.stiff[(size_t)(off + al) * nd + d] = f[d];
+        for (int d = 0; d < nd; d++) stiff[(size_t)(off + al) * nd + d] = f[d];
     }
     __syncwarp();
     const T *im = a.inv_mass + a.im_off[p];
     const T inv_nr = (T)1 / (T)nr;
     for (int c = 0; c < nd; c++) {
         for (int k = lane; k < nr; k += 32) {
-            T acc = a.stiff[(size_t)off * nd + c].x;
+            T acc = stiff[(size_t)off * nd + c].x;
             int j = 0;
             for (int al = 1; al < nu; al++) {
                 j += k; j = j >= nr ? j - nr : j;
-                const cx_t<T> v = a.stiff[(size_t)(off + al) * nd + c];
+                const cx_t<T> v = stiff[(size_t)(off + al) * nd + c];
                 acc += (T)2 * (v.x * twc[j] - v.y * tws[j]);
             }
             r[k] = acc * im[k];
@@ -147,7 +209,7 @@ __global__ void mass3d_kernel(const Mass3DArgs<T> a) {
             }
             if (al == 0) imv = 0;
             if ((nr & 1) == 0 && al == nr / 2) { re *= (T)0.5; imv = 0; }
-            a.stiff[(size_t)(off + al) * nd + c] = mk<T>(re, imv);
+            stiff[(size_t)(off + al) * nd + c] = mk<T>(re, imv);
         }
         __syncwarp();
     }
@@ -175,14 +237,18 @@ struct PointArgs {
     D dt, half_dt, half_dt_dt;
     int *nonfinite;
     int mask;                    // 1 = BC after assembly, 2 = 1/M, 4 = Newmark
+    int nwave;                   // wavefields; fields are [nwave][nmodes][ndim]
+    const T *sponge;             // [npoints] Kosloff gamma (0 = none) or null
 };
 
 template <class T, class D, bool COMP>
 __global__ void point_update_kernel(const PointArgs<T, D> a) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= a.nmodes) return;
-    const int p = a.mode_pt[m];
-    const int off = a.off[p], nr = a.nr[p], nu = nr / 2 + 1, al = m - off;
+    const int64_t mw = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (mw >= (int64_t)a.nmodes * a.nwave) return;
+    const int mm = (int)(mw % a.nmodes);
+    const size_t m = (size_t)mw;              // index into the batched fields
+    const int p = a.mode_pt[mm];
+    const int off = a.off[p], nr = a.nr[p], nu = nr / 2 + 1, al = mm - off;
     const uint8_t fl = a.flags[p];
     const int nd = a.ndim;
     cx_t<T> f[3];
@@ -192,6 +258,19 @@ __global__ void point_update_kernel(const PointArgs<T, D> a) {
         if (a.mask & 2) {
             const T im = a.inv_mass1[p];
             for (int d = 0; d < nd; d++) f[d] = cscale(f[d], im);
+        }
+    }
+    if ((a.mask & 2) && a.sponge) {
+        // Sponge::apply (ABC/Sponge.hpp:74-98), 1-D gamma, on the acceleration
+        const T g = a.sponge[p];
+        if (g != (T)0) {
+            const T two = 2;
+            for (int d = 0; d < nd; d++) {
+                const size_t q = m * nd + d;
+                const cx_t<T> v = mk<T>((T)a.veloc[q].x, (T)a.veloc[q].y);
+                const cx_t<T> u = mk<T>((T)a.displ[q].x, (T)a.displ[q].y);
+                f[d] = csub(f[d], cadd(cscale(v, two * g), cscale(u, g * g)));
+            }
         }
     }
     if (!(a.mask & 4)) {
@@ -256,6 +335,8 @@ struct MomentArgs {
     const int *pt_off, *pt_nu;
     cx_t<T> *stiff;
     const T *gmat;
+    const int *wave;                   // wavefield of each source
+    size_t fstride;
 };
 
 template <class T>
@@ -332,7 +413,9 @@ __global__ void moment_source_kernel(const MomentArgs<T> a) {
                         f = csub(f, b);
                     }
                 }
-                if (al < sNu[q]) atomic_add_cx(a.stiff + (size_t)(sOff[q] + al) * 3 + c, mk<T>(-f.x, -f.y));
+                if (al < sNu[q])
+                    atomic_add_cx(a.stiff + (size_t)a.wave[s] * a.fstride + (size_t)(sOff[q] + al) * 3 + c,
+                                  mk<T>(-f.x, -f.y));
             }
         }
         __syncthreads();
@@ -351,6 +434,8 @@ struct ForceArgs {
     const int *e_pts;
     const int *pt_off, *pt_nu;
     cx_t<T> *stiff;
+    const int *wave;
+    size_t fstride;
 };
 
 template <class T>
@@ -366,7 +451,8 @@ __global__ void force_source_kernel(const ForceArgs<T> a) {
         if (al >= a.pt_nu[p]) continue;
         for (int c = 0; c < 3; c++) {
             const cx_t<T> pv = a.pattern[a.pat_off[s] + ((size_t)al * 3 + c) * 25 + q];
-            atomic_add_cx(a.stiff + (size_t)(a.pt_off[p] + al) * 3 + c, mk<T>(pv.x * v, pv.y * v));
+            atomic_add_cx(a.stiff + (size_t)a.wave[s] * a.fstride + (size_t)(a.pt_off[p] + al) * 3 + c,
+                          mk<T>(pv.x * v, pv.y * v));
         }
     }
 }
@@ -385,17 +471,21 @@ struct StationArgs {
     int interval;
     int max_rec;
     const int *step;
+    int nwave;
+    size_t fstride;
 };
 
 template <class T>
 __global__ void station_kernel(const StationArgs<T> a) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.nst * 3) return;
+    const int tt = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tt >= a.nst * 3 * a.nwave) return;
     const int step = *a.step;
     if (step < 0 || a.out == nullptr || step % a.interval != 0) return;
     const int rec = step / a.interval;
     if (rec >= a.max_rec) return;
+    const int wf = tt / (a.nst * 3), t = tt % (a.nst * 3);
     const int s = t / 3, c = t % 3;
+    const cx_t<T> *displ = a.displ + (size_t)wf * a.fstride;
     const int e = a.elem[s];
     const int nu = a.e_nr[e] / 2 + 1;
     const T phi = a.phi[s];
@@ -406,7 +496,7 @@ __global__ void station_kernel(const StationArgs<T> a) {
             const T w = a.w[(size_t)s * 25 + q];
             if (w == (T)0) continue;
             const int p = a.e_pts[(size_t)e * 25 + q];
-            if (al < a.pt_nu[p]) x = cadd(x, cscale(a.displ[(size_t)(a.pt_off[p] + al) * 3 + c], w));
+            if (al < a.pt_nu[p]) x = cadd(x, cscale(displ[(size_t)(a.pt_off[p] + al) * 3 + c], w));
         }
         if (al == 0) {
             acc += x.x;
@@ -417,7 +507,7 @@ __global__ void station_kernel(const StationArgs<T> a) {
             acc += (T)2 * (cs * x.x - sn * x.y);
         }
     }
-    a.out[((size_t)rec * a.nst + s) * 3 + c] = (double)acc;
+    a.out[(((size_t)rec * a.nwave + wf) * a.nst + s) * 3 + c] = (double)acc;
 }
 
 // element-facing float copy of a double displacement (mixed precision)

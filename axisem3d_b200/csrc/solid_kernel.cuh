@@ -29,8 +29,22 @@ namespace axg {
 
 constexpr int RHEO_ISO = 0, RHEO_TISO = 1, RHEO_ANISO = 2;
 constexpr int ATT_NONE = 0, ATT_FULL = 1, ATT_CG4 = 2;
-constexpr int KB = 4;   // slices per thread in the Fourier -> slice transform
-constexpr int AB = 4;   // modes per thread in the slice -> Fourier transform
+// register blocking of the two phi transforms and the occupancy target of the
+// solid kernel (build-time tuning knobs)
+#ifndef AXG_KB
+#define AXG_KB 2
+#endif
+#ifndef AXG_AB
+#define AXG_AB 2
+#endif
+#ifndef AXG_SOLID_MIN_BLOCKS
+#define AXG_SOLID_MIN_BLOCKS 2
+#endif
+#ifndef AXG_PREFETCH_NEXT
+#define AXG_PREFETCH_NEXT 0
+#endif
+constexpr int KB = AXG_KB;   // slices per thread in the Fourier -> slice transform
+constexpr int AB = AXG_AB;   // modes per thread in the slice -> Fourier transform
 
 template <class T, class AT>
 struct SolidArgs {
@@ -55,6 +69,9 @@ struct SolidArgs {
     int nsls;
     AT alpha[8], beta[8], gamma[8];
     const T *gmat;             // [2][25]: G_GLL, G_GLJ (row-major, G(j,i) = l_j'(x_i))
+    int nwave;                 // wavefields sharing the mesh (independent sources)
+    size_t fstride;            // complex values between wavefields in displ / stiff
+    size_t sstride;            // AT values between wavefields in the state pool
 };
 
 // shared memory layout of one team
@@ -268,14 +285,48 @@ __device__ __forceinline__ void prefetch_element(const SolidArgs<T, AT> &a, int 
     }
 }
 
+// SLS recursion on one real slice point with the state already in registers
+// (same steps and order as attenuate<>; NS = number of SLS, a compile-time size)
+template <int NS, class T, class AT>
+__device__ __forceinline__ void attenuate_regs(const AT *alpha, const AT *beta, const AT *gamma, AT ds[6],
+                                               AT mem[NS][6], const T e[6], T s[6], T dl, T dm) {
+    AT sv[6];
+#pragma unroll
+    for (int d = 0; d < 6; d++) sv[d] = (AT)s[d];
+#pragma unroll
+    for (int l = 0; l < NS; l++)
+#pragma unroll
+        for (int d = 0; d < 6; d++) {
+            sv[d] -= mem[l][d];
+            mem[l][d] = alpha[l] * mem[l][d] + beta[l] * ds[d];
+        }
+    const AT lam = (AT)dl, mu = (AT)dm, mu2 = mu + mu;
+    const AT e0 = (AT)e[0], e1 = (AT)e[1], e2 = (AT)e[2];
+    const AT sii = (e0 + e1 + e2) * lam;
+    ds[0] = sii + e0 * mu2;
+    ds[1] = sii + e1 * mu2;
+    ds[2] = sii + e2 * mu2;
+    ds[3] = (AT)e[3] * mu;
+    ds[4] = (AT)e[4] * mu;
+    ds[5] = (AT)e[5] * mu;
+#pragma unroll
+    for (int l = 0; l < NS; l++)
+#pragma unroll
+        for (int d = 0; d < 6; d++) mem[l][d] += gamma[l] * ds[d];
+#pragma unroll
+    for (int d = 0; d < 6; d++) s[d] = (T)sv[d];
+}
+
 __device__ __forceinline__ int cg4_slot(int q) {
     // (1,1) (1,3) (3,1) (3,3) -> 0..3, else -1
     return q == 6 ? 0 : q == 8 ? 1 : q == 16 ? 2 : q == 18 ? 3 : -1;
 }
 
 // ----------------------------------------------------------------- kernel ---
-template <class T, class AT, int RHEO, int ATT, bool IS3D, bool RTZ>
-__global__ void __launch_bounds__(256)
+// NS: compile-time number of SLS for the register-resident slice path (3-D
+// elements); 0 = the generic path with the count read at run time
+template <class T, class AT, int RHEO, int ATT, bool IS3D, bool RTZ, int NS>
+__global__ void __launch_bounds__(256, AXG_SOLID_MIN_BLOCKS)
 solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_max,
                        const int teams_per_cta, const size_t team_bytes) {
     using C = cx_t<T>;
@@ -311,7 +362,7 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             *dzdeta_if = sGeo + 200, *invs_if = sGeo + 225;
 
     const int stride = gridDim.x * teams_per_cta;
-    if (blockIdx.x * teams_per_cta + team < a.n_elem)
+    if (AXG_PREFETCH_NEXT && blockIdx.x * teams_per_cta + team < a.n_elem)
         prefetch_element<T, AT, RHEO, ATT, IS3D>(a, blockIdx.x * teams_per_cta + team, lane, TEAM);
     for (int e = blockIdx.x * teams_per_cta + team; e < a.n_elem; e += stride) {
         const int nr = a.nr[e];
@@ -319,7 +370,8 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
         const bool axial = a.axial[e] != 0;
         const T *Gxi = axial ? sGlj : sGll;
         // the next element of this team streams into L2 while this one computes
-        if (e + stride < a.n_elem) prefetch_element<T, AT, RHEO, ATT, IS3D>(a, e + stride, lane, TEAM);
+        if (AXG_PREFETCH_NEXT && e + stride < a.n_elem)
+            prefetch_element<T, AT, RHEO, ATT, IS3D>(a, e + stride, lane, TEAM);
 
         // ---------------- element header -> shared memory ----------------
         for (int i = lane; i < 250; i += TEAM) sGeo[i] = a.geom[(size_t)e * 250 + i];
@@ -337,12 +389,17 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
         }
         team_sync(team, TEAM);
 
+        // every wavefield of the batch reuses the element header loaded above
+        for (int w = 0; w < a.nwave; w++) {
+        const C *displw = a.displ + (size_t)w * a.fstride;
+        C *stiffw = a.stiff + (size_t)w * a.fstride;
+        AT *statew = a.state + (size_t)w * a.sstride;
         // ---------------- gather displacement: U[a][c][q] in region B ----------------
         for (int i = lane; i < nu * 25; i += TEAM) {
             const int q = i / nu, al = i - q * nu;
             C u0 = mk<T>(0, 0), u1 = u0, u2 = u0;
             if (al < sNu[q]) {
-                const C *src = a.displ + (size_t)(sOff[q] + al) * 3;
+                const C *src = displw + (size_t)(sOff[q] + al) * 3;
                 u0 = src[0]; u1 = src[1]; u2 = src[2];
             }
             rBc[(al * 3 + 0) * 25 + q] = u0;
@@ -424,14 +481,14 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 elastic_at<RHEO>(a.mod + moff, 1, 0, q, eps, sig);
                 if constexpr (ATT == ATT_FULL) {
                     const int64_t ao = a.att_off[e];
-                    AT *st = a.state + a.state_off[e];
+                    AT *st = statew + a.state_off[e];
                     attenuate<T, AT, true>(a, st, (size_t)nu * 25, (size_t)al * 25 + q, eps, sig,
                                            a.attmod[ao + q], a.attmod[ao + 25 + q]);
                 } else if constexpr (ATT == ATT_CG4) {
                     const int k4 = cg4_slot(q);
                     if (k4 >= 0) {
                         const int64_t ao = a.att_off[e];
-                        AT *st = a.state + a.state_off[e];
+                        AT *st = statew + a.state_off[e];
                         attenuate<T, AT, true>(a, st, (size_t)nu * 4, (size_t)al * 4 + k4, eps, sig,
                                                a.attmod[ao + k4], a.attmod[ao + 4 + k4]);
                     }
@@ -456,6 +513,90 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             const int nab = (nu + AB - 1) / AB;
             for (int q0 = 0; q0 < 25; q0 += qc_max) {
                 const int qcnt = min(qc_max, 25 - q0);
+                if constexpr (NS > 0 || ATT == ATT_NONE) {
+                // One thread per (slice, point): the global operands of the point-slice
+                // (moduli, attenuation moduli, SLS state) are loaded into registers
+                // first, so that their latency overlaps the Fourier -> slice sum
+                // (computeC2R) that follows, then stress and attenuation are applied
+                // and the state is stored back.
+                constexpr int NM = RHEO == RHEO_ISO ? 2 : RHEO == RHEO_TISO ? 5 : 21;
+                constexpr int NSR = NS > 0 ? NS : 1;
+                constexpr int NPA = ATT == ATT_CG4 ? 4 : 25;
+                const T *modp = a.mod + moff;
+                const size_t nsl = (size_t)nslice * 25;
+                for (int i = lane; i < nr * qcnt; i += TEAM) {
+                    const int k = i / qcnt, qq = i - k * qcnt, q = q0 + qq;
+                    T md[NM];
+#pragma unroll
+                    for (int mm = 0; mm < NM; mm++) md[mm] = __ldg(modp + mm * nsl + (size_t)k * 25 + q);
+                    AT ds[6], mem[NSR][6];
+                    T dl = 0, dmu = 0;
+                    AT *st = nullptr;
+                    size_t slot = 0, nslot = 0;
+                    bool att_here = false;
+                    if constexpr (ATT != ATT_NONE) {
+                        const int k4 = ATT == ATT_CG4 ? cg4_slot(q) : q;
+                        att_here = k4 >= 0;
+                        if (att_here) {
+                            nslot = (size_t)nr * NPA;
+                            slot = (size_t)k * NPA + k4;
+                            st = statew + a.state_off[e];
+                            const T *am = a.attmod + a.att_off[e];
+                            dl = __ldg(am + slot);
+                            dmu = __ldg(am + nslot + slot);
+#pragma unroll
+                            for (int d = 0; d < 6; d++) ds[d] = st[d * nslot + slot];
+#pragma unroll
+                            for (int l = 0; l < NSR; l++)
+#pragma unroll
+                                for (int d = 0; d < 6; d++) mem[l][d] = st[(6 + l * 6 + d) * nslot + slot];
+                        }
+                    }
+                    // computeC2R at slice k: r = Re c0 + 2 sum Re(c_a e^{i a phi_k})
+                    T acc[6];
+#pragma unroll
+                    for (int d = 0; d < 6; d++) acc[d] = rA[d * 25 + q].x;
+                    int j = 0;
+                    for (int al = 1; al < nu; al++) {
+                        j += k;
+                        j = j >= nr ? j - nr : j;
+                        const T c = twc[j], sn = tws[j];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) {
+                            const C ev = rA[(al * 6 + d) * 25 + q];
+                            acc[d] += (T)2 * (ev.x * c - ev.y * sn);
+                        }
+                    }
+                    re1<T> ev[6], sg[6];
+#pragma unroll
+                    for (int d = 0; d < 6; d++) ev[d].x = acc[d];
+                    if constexpr (RHEO == RHEO_ISO) {
+                        stress_iso(ev, sg, md[0], md[1]);
+                    } else if constexpr (RHEO == RHEO_TISO) {
+                        stress_tiso(ev, sg, md[0], md[1], md[2], md[3], md[4]);
+                    } else {
+                        stress_aniso(ev, sg, md);
+                    }
+                    if constexpr (ATT != ATT_NONE) {
+                        if (att_here) {
+                            T e6[6], s6[6];
+#pragma unroll
+                            for (int d = 0; d < 6; d++) { e6[d] = ev[d].x; s6[d] = sg[d].x; }
+                            attenuate_regs<NSR, T, AT>(a.alpha, a.beta, a.gamma, ds, mem, e6, s6, dl, dmu);
+#pragma unroll
+                            for (int d = 0; d < 6; d++) sg[d].x = s6[d];
+#pragma unroll
+                            for (int d = 0; d < 6; d++) st[d * nslot + slot] = ds[d];
+#pragma unroll
+                            for (int l = 0; l < NSR; l++)
+#pragma unroll
+                                for (int d = 0; d < 6; d++) st[(6 + l * 6 + d) * nslot + slot] = mem[l][d];
+                        }
+                    }
+#pragma unroll
+                    for (int d = 0; d < 6; d++) rBr[((size_t)k * 6 + d) * qcnt + qq] = sg[d].x;
+                }
+                } else
                 // Fourier -> slices (computeC2R), stress, attenuation -> rBr[k][d][qq]
                 for (int i = lane; i < nkb * qcnt; i += TEAM) {
                     const int kb = i / qcnt, qq = i - kb * qcnt, q = q0 + qq;
@@ -498,7 +639,7 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                         elastic_at<RHEO>(a.mod + moff, nslice, k, q, ev, sg);
                         if constexpr (ATT == ATT_FULL) {
                             const int64_t ao = a.att_off[e];
-                            AT *st = a.state + a.state_off[e];
+                            AT *st = statew + a.state_off[e];
                             const size_t ns = (size_t)nr * 25;
                             attenuate<T, AT, false>(a, st, ns, (size_t)k * 25 + q, ev, sg,
                                                     a.attmod[ao + (size_t)k * 25 + q],
@@ -507,7 +648,7 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                             const int k4 = cg4_slot(q);
                             if (k4 >= 0) {
                                 const int64_t ao = a.att_off[e];
-                                AT *st = a.state + a.state_off[e];
+                                AT *st = statew + a.state_off[e];
                                 const size_t ns = (size_t)nr * 4;
                                 attenuate<T, AT, false>(a, st, ns, (size_t)k * 4 + k4, ev, sg,
                                                         a.attmod[ao + (size_t)k * 4 + k4],
@@ -630,12 +771,13 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 f[c] = fc;
             }
             if (al < sNu[q]) {
-                C *dst = a.stiff + (size_t)(sOff[q] + al) * 3;
+                C *dst = stiffw + (size_t)(sOff[q] + al) * 3;
 #pragma unroll
                 for (int c = 0; c < 3; c++) atomic_add_cx(dst + c, mk<T>(-f[c].x, -f[c].y));
             }
         }
         team_sync(team, TEAM);
+        }   // wavefields
     }
 }
 

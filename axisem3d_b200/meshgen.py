@@ -243,10 +243,24 @@ def moment_pattern_offaxis(mt, weights, nu_elem, phi=0.0):
 
 
 # ------------------------------------------------------------- plain forward ---
+def azimuthal_dt(sz, nr, vmax):
+    """Stability bound of the azimuthal terms: the order-alpha stiffness grows like
+    alpha v / s next to the axis, which Quad::computeDt (Quad.cpp:271-349) does not
+    bound; min over off-axis points of s / ((nr // 2) v)."""
+    s = np.asarray(sz)[..., 0, :]
+    amax = max(1, int(nr) // 2)
+    sp = s[s > 0]
+    return float(np.min(sp) / (amax * vmax)) if sp.size else np.inf
+
+
 def cartesian_model(nx=40, nz=40, width=100e3, height=100e3, nr=5, rho=2700.0, vp=5800.0,
                     vs=3460.0, source_depth=10e3, f0=1.0, nstations=20, courant=0.6, seed=0,
-                    moment_scale=1e18, attenuation=None, record_interval=1):
-    """Plain forward case (the reference's CPU-runnable configuration)."""
+                    moment_scale=1e18, attenuation=None, record_interval=1, nr_aware_dt=False,
+                    absorbing=False):
+    """Plain forward case (the reference's CPU-runnable configuration).
+
+    nr_aware_dt: also bound dt by the azimuthal terms next to the axis (azimuthal_dt);
+    a uniform high nr on a fine axial mesh is unstable at the reference's dt."""
     rng = np.random.Generator(np.random.PCG64(seed))
     h_s, h_z = width / nx, height / nz
     ne = nx * nz
@@ -267,7 +281,11 @@ def cartesian_model(nx=40, nz=40, width=100e3, height=100e3, nr=5, rho=2700.0, v
     coords[pts.ravel(), 0] = sz[:, 0, :].ravel()
     coords[pts.ravel(), 1] = sz[:, 1, :].ravel()
     sp_axial = (np.abs(coords[:, 0]) < 1e-9 * width).astype(np.uint8)
-    dt_e = min(quad_dt(sz[e], vp) for e in range(ne))
+    # Quad::computeDt (Quad.cpp:329-345): quads on a Clayton boundary take half the step
+    on_abc = (i == nx - 1) | (j == 0) if absorbing else np.zeros(ne, bool)
+    dt_e = min(quad_dt(sz[e], vp) * (0.5 if on_abc[e] else 1.0) for e in range(ne))
+    if nr_aware_dt:
+        dt_e = min(dt_e, azimuthal_dt(sz, nr, vp))
     dt = round_dt(dt_e * courant)
     m = Model(dt=dt)
     m.sp_nr = np.full(npts, nr, np.int32)
@@ -324,6 +342,50 @@ def cartesian_model(nx=40, nz=40, width=100e3, height=100e3, nr=5, rho=2700.0, v
     m.st_phi = np.zeros(nstations)
     m.st_interval = record_interval
     m.meta = {"workload": "cartesian %dx%d nr=%d" % (nx, nz, nr), "moment": mt.tolist(), "seed": seed}
+    if absorbing:
+        add_absorbing(m, nx, nz, width, height, rho, vp, vs)
+    return m
+
+
+def add_absorbing(m, nx, nz, width, height, rho=2700.0, vp=5800.0, vs=3460.0, sponge_frac=0.15,
+                  sponge_gamma=None):
+    """Clayton-Engquist 1-D coefficients on the outer (s = width) and bottom (z = -height)
+    edges of a cartesian_model grid, and a Kosloff sponge whose gamma rises as cos^2 over the
+    last sponge_frac of the domain (AbsorbingBoundary / ClaytonSolid1D / Sponge).
+
+    area = GLL weight * half edge length * s (the axisymmetric line integral of the normal);
+    theta = polar angle of the outward normal (pi/2 on the outer edge, pi at the bottom)."""
+    wgll = np.array([0.1, 49.0 / 90.0, 32.0 / 45.0, 49.0 / 90.0, 0.1])
+    h_s, h_z = width / nx, height / nz
+    pts, _ = structured_points(nx, nz)
+    # one dict per boundary key: normals of neighbouring elements add up per point
+    right, bottom = {}, {}
+    for e in range(nx * nz):
+        i, j = divmod(e, nz)
+        if i == nx - 1:
+            for jp in range(5):
+                p = int(pts[e, 4 * 5 + jp])
+                right[p] = right.get(p, 0.0) + wgll[jp] * 0.5 * h_z * width
+        if j == 0:
+            for ip in range(5):
+                p = int(pts[e, ip * 5 + 0])
+                bottom[p] = bottom.get(p, 0.0) + wgll[ip] * 0.5 * h_s * max(m.sp_coords[p, 0], 0.0)
+    cp = list(bottom) + list(right)
+    area = list(bottom.values()) + list(right.values())
+    theta = [math.pi] * len(bottom) + [math.pi / 2] * len(right)
+    keep = [k for k in range(len(cp)) if area[k] > 0.0]
+    n = len(keep)
+    m.cl_solid = {"point": np.array([cp[k] for k in keep], np.int32), "rho_vp": np.full(n, rho * vp),
+                  "rho_vs": np.full(n, rho * vs), "area": np.array([area[k] for k in keep]),
+                  "theta": np.array([theta[k] for k in keep])}
+    # sponge: distance into the layer along s and depth, normalised to [0, 1]
+    span = sponge_frac * min(width, height)
+    g0 = sponge_gamma if sponge_gamma is not None else 0.5 * vp / span
+    ds = np.clip((m.sp_coords[:, 0] - (width - span)) / span, 0.0, 1.0)
+    dz = np.clip(((-height + span) - m.sp_coords[:, 1]) / span, 0.0, 1.0)
+    x = np.maximum(ds, dz)
+    sel = np.nonzero(x > 0.0)[0].astype(np.int32)
+    m.sponge_solid = (sel, g0 * np.sin(0.5 * math.pi * x[sel]) ** 2)
     return m
 
 
@@ -893,3 +955,61 @@ def aniso_moduli_from(lam, mu, rng, pert):
         raise ValueError("perturbed Cij not positive definite")
     iu = np.triu_indices(6)
     return [C[:, a, b].reshape(shp) for a, b in zip(*iu)]
+
+
+def ensemble_model(base, nsrc=64, seed=21, periods=(10.0, 40.0), moment_scale=1e20):
+    """Batched ensemble: `nsrc` independent moment-tensor sources on the mesh of
+    `base`, one wavefield each, all advanced in the same launches. Sources sit at
+    seeded random (element, xi, eta) in non-axial solid elements with seeded
+    tensors (drawn directly in the element's s, phi, z frame, i.e. after the
+    Qzsp rotation of Mechanism::release) and Ricker wavelets with periods uniform
+    in `periods`."""
+    import copy
+    rng = np.random.Generator(np.random.PCG64(seed))
+    m = copy.copy(base)
+    t = tables()
+    cand = np.nonzero(base.se_axial == 0)[0]
+    elems = rng.choice(cand, size=nsrc, replace=len(cand) < nsrc)
+    pats, offs, nus, stfs = [], [], [], []
+    o = 0
+    t0 = 0.0
+    for i, e in enumerate(elems):
+        xi, eta = rng.uniform(-1, 1, 2)
+        w = np.outer(lagrange(t["pGLL"], xi), lagrange(t["pGLL"], eta)).ravel()
+        nu = int(base.se_nr[e]) // 2 + 1
+        pat = moment_pattern_offaxis(rng.normal(0.0, moment_scale, 6), w, nu, phi=rng.uniform(0, 2 * np.pi))
+        pats.append(pat.ravel())
+        offs.append(o)
+        nus.append(nu)
+        o += pat.size
+        period = rng.uniform(*periods)
+        hd = period / 2.0
+        stfs.append(STF(half_duration=hd, decay_factor=math.pi * hd / period, time_shift=0.0,
+                        derivative_order=2))
+        t0 = min(t0, -2.5 * hd)
+    m.ms_elem = elems.astype(np.int32)
+    m.ms_nu = np.array(nus, np.int32)
+    m.ms_pat_off = np.array(offs, np.int64)
+    m.ms_pattern = np.concatenate(pats)
+    m.ms_stf = stfs
+    m.ms_wave = np.arange(nsrc, dtype=np.int32)
+    m.nwave = nsrc
+    m.t0 = t0
+    m.meta = dict(base.meta, workload=base.meta.get("workload", "") + " x %d sources" % nsrc)
+    return m
+
+
+def single_source(ens, i):
+    """The i-th source of an ensemble model as its own one-wavefield model."""
+    import copy
+    m = copy.copy(ens)
+    nu = int(ens.ms_nu[i])
+    o = int(ens.ms_pat_off[i])
+    m.ms_elem = ens.ms_elem[i:i + 1].copy()
+    m.ms_nu = ens.ms_nu[i:i + 1].copy()
+    m.ms_pat_off = np.zeros(1, np.int64)
+    m.ms_pattern = ens.ms_pattern[o:o + nu * 150].copy()
+    m.ms_stf = [ens.ms_stf[i]]
+    m.ms_wave = None
+    m.nwave = 1
+    return m

@@ -98,17 +98,25 @@ class Model:
     ms_pat_off: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     ms_pattern: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex128))
     ms_stf: List[STF] = field(default_factory=list)
+    ms_wave: Optional[np.ndarray] = None          # wavefield of each source (batched sources)
     # force sources
     fs_elem: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     fs_nu: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     fs_pat_off: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     fs_pattern: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex128))
     fs_stf: List[STF] = field(default_factory=list)
+    fs_wave: Optional[np.ndarray] = None
+    nwave: int = 1                                # independent wavefields on this mesh
     # stations
     st_elem: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     st_w: np.ndarray = field(default_factory=lambda: np.zeros((0, 25)))
     st_phi: np.ndarray = field(default_factory=lambda: np.zeros(0))
     st_interval: int = 1
+    # absorbing boundaries (Clayton 1-D coefficients; sponge gamma per point)
+    cl_solid: Optional[dict] = None               # point, rho_vp, rho_vs, area, theta
+    cl_fluid: Optional[dict] = None               # point, rho_vp, area
+    sponge_solid: Optional[tuple] = None          # (points, gamma)
+    sponge_fluid: Optional[tuple] = None
     meta: dict = field(default_factory=dict)
     meta_rho: Optional[np.ndarray] = None          # (ne, 25) density at element points (generators)
 
@@ -122,7 +130,7 @@ class Model:
         return len(self.fe_nr)
 
     def solid_field_size(self):
-        return int(np.sum(np.asarray(self.sp_nr) // 2 + 1)) * 3
+        return int(np.sum(np.asarray(self.sp_nr) // 2 + 1)) * 3 * max(1, self.nwave)
 
     def fluid_field_size(self):
         return int(np.sum(np.asarray(self.fp_nr) // 2 + 1)) if len(self.fp_nr) else 0
@@ -151,6 +159,7 @@ class Model:
         cfg.compensated = compensated
         cfg.plain = int(bool(plain))
         cfg.autotune = int(bool(autotune))
+        cfg.nwave = int(self.nwave)
         return cfg
 
     def c_structs(self):
@@ -233,6 +242,7 @@ class Model:
                 stfs[i].derivative_order = st.derivative_order
             keep[kind + "_stf"] = stfs
             s.stf = C.cast(stfs, C.POINTER(L.axg_stf))
+            s.wavefield = k(kind + "_wave", getattr(self, kind + "_wave"), _i32, C.c_int32)
             return s
 
         ms = sources("ms", L.axg_moment_sources, 6)
@@ -244,5 +254,28 @@ class Model:
         st.weights = k("st_w", self.st_w, _f64, C.c_double)
         st.phi = k("st_phi", self.st_phi, _f64, C.c_double)
 
+        def clay(name, d, solid):
+            c = L.axg_clayton()
+            if not d:
+                c.count = 0
+                return c
+            c.count = len(d["point"])
+            c.point = k(name + "_pt", d["point"], _i32, C.c_int32)
+            c.rho_vp = k(name + "_rvp", d["rho_vp"], _f64, C.c_double)
+            c.area = k(name + "_area", d["area"], _f64, C.c_double)
+            if solid:
+                c.rho_vs = k(name + "_rvs", d["rho_vs"], _f64, C.c_double)
+                c.theta = k(name + "_th", d["theta"], _f64, C.c_double)
+            return c
+
+        def sponge(name, t):
+            if not t:
+                return (None, None)
+            pt, g = _i32(t[0]), _f64(t[1])
+            keep[name + "_pt"], keep[name + "_g"] = pt, g
+            return (pt, g)
+
         return {"sp": sp, "fp": fp, "se": se, "fe": fe, "sf": sf, "ms": ms, "fs": fs, "st": st,
+                "cl_s": clay("cls", self.cl_solid, True), "cl_f": clay("clf", self.cl_fluid, False),
+                "sg_s": sponge("sgs", self.sponge_solid), "sg_f": sponge("sgf", self.sponge_fluid),
                 "keep": keep}

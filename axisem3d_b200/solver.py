@@ -58,6 +58,13 @@ class Solver:
             self._check(self.lib.axg_set_force_sources(h, C.byref(s["fs"])))
         if s["st"].count:
             self._check(self.lib.axg_set_stations(h, C.byref(s["st"]), int(model.st_interval)))
+        for solid, key in ((1, "cl_s"), (0, "cl_f")):
+            if s[key].count:
+                self._check(self.lib.axg_set_clayton(h, solid, C.byref(s[key])))
+        for solid, (pt, g) in ((1, s["sg_s"]), (0, s["sg_f"])):
+            if pt is not None and len(pt):
+                self._check(self.lib.axg_set_sponge(h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
+                                                    g.ctypes.data_as(L.P_f64)))
         for cls, team in (team_sizes or {}).items():
             self._check(self.lib.axg_set_team_size(h, int(cls), int(team)))
         self._check(self.lib.axg_finalize(h))
@@ -158,14 +165,16 @@ class Solver:
         self._check(self.lib.axg_get_field_raw(self.h, int(bool(solid)), w, C.c_void_p(host_ptr), int(nbytes)))
 
     def seismograms(self):
-        """(nrecords, nstations, 3) displacement in s, phi, z."""
+        """(nrecords, nstations, 3) displacement in s, phi, z; with batched
+        wavefields (nrecords, nwave, nstations, 3)."""
         n = C.c_int32()
         self._check(self.lib.axg_get_seismograms(self.h, None, C.byref(n)))
         ns = len(self.model.st_elem)
-        out = np.zeros((n.value, ns, 3))
+        nw = max(1, int(self.model.nwave))
+        out = np.zeros((n.value, nw, ns, 3))
         if n.value and ns:
             self._check(self.lib.axg_get_seismograms(self.h, out.ctypes.data_as(L.P_f64), C.byref(n)))
-        return out
+        return out[:, 0] if nw == 1 else out
 
     # -------------------------------------------------------- differentiation ---
     def forward_checkpointed(self, nsteps, interval=100):

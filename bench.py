@@ -54,7 +54,9 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64"])
     p.add_argument("--elements", type=int, default=200000)
     p.add_argument("--nr-max", type=int, default=64)
-    p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison runs")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
+    p.add_argument("--adjoint-steps", type=int, default=4000)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     return p.parse_args()
 
@@ -225,13 +227,13 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def time_steps(solver, steps, stream):
+def time_steps(solver, steps, stream, graph=True):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
-    solver.run(steps, graph=True)
+    solver.run(steps, graph=graph)
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / 1e3
@@ -307,18 +309,79 @@ def run_ours(args, world, rank, local):
     out = {"value": value, "t": t, "launches": launches, "kms": kms / max(kn, 1), "bytes": bytes_,
            "flops": flops, "pbytes": pbytes, "U": U, "e2e": U * ke * world / te, "e2e_bytes": nb,
            "clocks": clocks.summary(), "model": m}
-    # FP64 run of the same workload (the metric compares FP32 and FP64 paths)
+    # FP64 runs of the same workload: the plain method (one team per element, one
+    # launch per kernel, no graph) and the fused batched path in FP64
     if not args.no_fp64 and args.precision != "fp64":
-        log("fp64 run")
-        s64 = Solver(m, "fp64", device=local)
-        s64.set_stream(stream.cuda_stream)
-        s64.set_field(u0, "displ")
-        s64.run(2, graph=True)
-        k64 = max(3, args.steps // 5)
-        t64 = dist_max(time_steps(s64, k64, stream), world)
-        out["value_fp64"] = U * k64 * world / t64
-        s64.close()
+        for key, kw in (("value_fp64_plain", dict(plain=True)), ("value_fp64", {})):
+            log("fp64 run " + key)
+            s64 = Solver(m, "fp64", device=local, **kw)
+            s64.set_stream(stream.cuda_stream)
+            s64.set_field(u0, "displ")
+            s64.run(2, graph=not kw)
+            k64 = max(3, args.steps // 5)
+            t64 = dist_max(time_steps(s64, k64, stream, graph=not kw), world)
+            out[key] = U * k64 * world / t64
+            s64.close()
+        log("trace error")
+        out["trace"] = trace_error(args, local)
+    if not args.no_adjoint:
+        log("adjoint")
+        out["adjoint"] = adjoint_timing(args, local, stream, world)
     return out
+
+
+def trace_error(args, local):
+    """Seismograms of the plain forward case (40 x 40 quads, nr = 5, 2000 steps) in the
+    bench precision against the FP64 engine: relative L2 over all traces."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.cartesian_model(nx=40, nz=40, nr=5)
+    seis = {}
+    for prec in (args.precision, "fp64"):
+        with Solver(m, prec, device=local) as s:
+            s.run(2000)
+            seis[prec] = s.seismograms()
+    ref = seis["fp64"]
+    return {"workload": "cartesian 40x40 quads, nr=5, 20 stations, 2000 steps",
+            "rel_l2": float(np.linalg.norm(seis[args.precision] - ref) / np.linalg.norm(ref))}
+
+
+def adjoint_timing(args, local, stream, world):
+    """Adjoint sensitivity workload: 200 x 200 quads, uniform nr = 9, 5 % Gaussian blob in
+    mu and rho, 50 surface receivers, checkpoint every 100 steps. Ratio = time of the
+    adjoint sweep (recompute from checkpoints + time-reversed adjoint steps) over the time
+    of a plain forward solve of the same steps, both in FP64 (the adjoint's precision)."""
+    import torch
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    base = meshgen.cartesian_model(nx=200, nz=200, nr=9, nstations=50, nr_aware_dt=True)
+    m = meshgen.blob_model(base, amp=0.05, seed=3)
+    n = args.adjoint_steps
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, max(e0.elapsed_time(e1) / 1e3, time.perf_counter() - w0)
+
+    # the adjoint is an FP64 path: forward and adjoint are both timed in FP64
+    with Solver(m, "fp64", device=local) as f:
+        f.set_stream(stream.cuda_stream)
+        _, t_fwd = timed(lambda: (f.run(n), f.synchronize()))
+    with Solver(m, "fp64", device=local) as s:
+        s.set_stream(stream.cuda_stream)
+        _, t_ck = timed(lambda: (s.forward_checkpointed(n, 100), s.synchronize()))
+        seis = s.seismograms()
+        _, t_adj = timed(lambda: s.adjoint(seis))
+    t_fwd, t_ck, t_adj = (dist_max(x, world) for x in (t_fwd, t_ck, t_adj))
+    return {"workload": "cartesian 200x200 quads, nr=9, mu/rho blob, 50 receivers, %d steps, "
+                        "checkpoint every 100" % n,
+            "forward_s": t_fwd, "forward_checkpointed_s": t_ck, "adjoint_s": t_adj,
+            "adjoint_over_forward": t_adj / t_fwd}
 
 
 def main():
@@ -363,8 +426,13 @@ def main():
             "point_update_bytes_per_step": r["pbytes"],
         }
         if "value_fp64" in r:
+            line["value_fp64_plain"] = r["value_fp64_plain"]
             line["value_fp64"] = r["value_fp64"]
+            line["fp32_over_fp64_plain"] = r["value"] / r["value_fp64_plain"]
             line["fp32_over_fp64"] = r["value"] / r["value_fp64"]
+            line["trace"] = r["trace"]
+        if "adjoint" in r:
+            line["adjoint"] = r["adjoint"]
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -31,9 +31,10 @@
  *   - 3-D (azimuthally varying) properties are sampled on slices
  *     phi_k = 2 pi k / nr, k = 0..nr-1.
  *
- * Host-side field layout (axg_get_field / axg_set_field): for each point in
- * point order, nu_p x ndim complex doubles, row-major in (mode, dim), i.e. the
- * transpose of the reference's column-major eigen::CMatX3 (SolidPoint.hpp:126-131).
+ * Host-side field layout (axg_get_field / axg_set_field): for each wavefield, for
+ * each point in point order, nu_p x ndim complex doubles, row-major in (mode, dim),
+ * i.e. the transpose of the reference's column-major eigen::CMatX3
+ * (SolidPoint.hpp:126-131).
  *
  * Every function returns AXG_OK (0) or a negative AXG_E_* code; the message is
  * available from axg_last_error(h) in the reference's "Class::method || message"
@@ -112,6 +113,9 @@ typedef struct axg_config {
                                    measured against                                       */
     int32_t autotune;           /* 1 = time the candidate team sizes of every nr bucket at
                                    axg_finalize and keep the fastest                      */
+    int32_t nwave;              /* independent wavefields (sources) advanced together on
+                                   the same mesh; fields, state and seismograms gain a
+                                   leading wavefield dimension (0 or 1 = one)             */
 } axg_config;
 
 /* solid GLL points (SolidPoint + Mass1D/Mass3D + AxialBoundary membership) */
@@ -194,6 +198,7 @@ typedef struct axg_moment_sources {
     const int64_t *pattern_offset;/* offset in complex numbers into pattern      */
     const double  *pattern;       /* per source [nu][6][25] complex (re, im)     */
     const axg_stf *stf;           /* [count] */
+    const int32_t *wavefield;     /* [count] wavefield each source drives; NULL = 0 */
 } axg_moment_sources;
 
 /* point-force sources (SolidForce + Mechanism pattern) */
@@ -204,6 +209,7 @@ typedef struct axg_force_sources {
     const int64_t *pattern_offset;
     const double  *pattern;       /* per source [nu][3][25] complex */
     const axg_stf *stf;
+    const int32_t *wavefield;     /* [count]; NULL = 0 */
 } axg_force_sources;
 
 /* stations: in-plane Lagrange weights and azimuth (Station.hpp:53-72) */
@@ -213,6 +219,17 @@ typedef struct axg_stations {
     const double  *weights;       /* [count*25]           */
     const double  *phi;           /* [count]              */
 } axg_stations;
+
+/* Clayton-Engquist absorbing points with 1-D coefficients (ClaytonSolid1D.hpp,
+   ClaytonFluid1D.hpp), applied in Domain::applyBC_BeforeAssemblingStiff */
+typedef struct axg_clayton {
+    int32_t        count;
+    const int32_t *point;         /* solid or fluid point index                       */
+    const double  *rho_vp;
+    const double  *rho_vs;        /* solid only                                       */
+    const double  *area;          /* length of the boundary normal (integration weight) */
+    const double  *theta;         /* polar angle of the normal (solid only)            */
+} axg_clayton;
 
 typedef struct axg_solver axg_solver;
 
@@ -231,6 +248,14 @@ int  axg_set_solid_fluid(axg_solver *h, const axg_solid_fluid *c);
 int  axg_set_moment_sources(axg_solver *h, const axg_moment_sources *s);
 int  axg_set_force_sources(axg_solver *h, const axg_force_sources *s);
 int  axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interval);
+/* Clayton-Engquist conditions (GLLPoint.cpp:148-190 builds one ClaytonSolid1D /
+   ClaytonFluid1D per point and boundary key); a point on two boundaries is listed once per
+   boundary, and its conditions are applied in the order listed */
+int  axg_set_clayton(axg_solver *h, int32_t solid, const axg_clayton *c);
+/* Kosloff sponge (Sponge.hpp, 1-D gamma per point, each point at most once), applied to the acceleration in
+   Domain::applyBC_AfterComputingAccel: accel -= 2 gamma veloc + gamma^2 displ */
+int  axg_set_sponge(axg_solver *h, int32_t solid, int32_t count, const int32_t *point,
+                    const double *gamma);
 /* builds buckets, uploads to HBM; must precede any time-loop call */
 int  axg_finalize(axg_solver *h);
 
@@ -284,7 +309,7 @@ int  axg_field_size(const axg_solver *h, int32_t solid, int64_t *n);
 int  axg_field_raw_bytes(const axg_solver *h, int32_t solid, int32_t which, int64_t *bytes);
 int  axg_set_field_raw(axg_solver *h, int32_t solid, int32_t which, const void *host, int64_t bytes);
 int  axg_get_field_raw(axg_solver *h, int32_t solid, int32_t which, void *host, int64_t bytes);
-/* seismograms recorded so far: [nrecords][nstations][3] doubles, SPZ components */
+/* seismograms recorded so far: [nrecords][nwave][nstations][3] doubles, SPZ components */
 int  axg_get_seismograms(axg_solver *h, double *host_out, int32_t *nrecords);
 int  axg_synchronize(axg_solver *h);
 

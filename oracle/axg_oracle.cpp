@@ -377,6 +377,8 @@ struct OracleBase {
     virtual void set_moment_sources(const axg_moment_sources *) = 0;
     virtual void set_force_sources(const axg_force_sources *) = 0;
     virtual void set_stations(const axg_stations *, int) = 0;
+    virtual void set_clayton(int solid, const axg_clayton *) = 0;
+    virtual void set_sponge(int solid, int n, const int32_t *pt, const double *g) = 0;
     virtual void apply_sources(int tstep) = 0;
     virtual void compute_stiffness(int nthreads) = 0;
     virtual void bc_before() = 0;
@@ -411,6 +413,12 @@ struct Oracle : OracleBase {
     std::vector<double> seis;   // [nrec][nst][3]
     int nrec = 0;
     std::vector<Twiddle<R>> tw;  // by nr
+    // absorbing boundaries
+    struct ClaytonS { int p; R ss, zz, sz, pp; };
+    struct ClaytonF { int p; R c; };
+    std::vector<ClaytonS> cls;
+    std::vector<ClaytonF> clf;
+    std::vector<std::pair<int, R>> sgs, sgf;
 
     explicit Oracle(const axg_config *c) : cfg(*c) {
         for (int i = 0; i < P; i++)
@@ -599,6 +607,23 @@ struct Oracle : OracleBase {
             st[i].phi = s->phi[i];
         }
         rec_interval = interval > 0 ? interval : 1;
+    }
+
+    // ClaytonSolid1D / ClaytonFluid1D constructors (coefficients in double, cast)
+    void set_clayton(int solid, const axg_clayton *c) override {
+        for (int i = 0; i < c->count; i++) {
+            if (solid) {
+                double ct = std::cos(c->theta[i]), st = std::sin(c->theta[i]);
+                double rsa = c->rho_vs[i] * c->area[i], rpa = c->rho_vp[i] * c->area[i];
+                cls.push_back({c->point[i], (R)(rsa * ct * ct + rpa * st * st), (R)(rsa * st * st + rpa * ct * ct),
+                               (R)((rpa - rsa) * ct * st), (R)rsa});
+            } else {
+                clf.push_back({c->point[i], (R)(c->area[i] / c->rho_vp[i])});
+            }
+        }
+    }
+    void set_sponge(int solid, int n, const int32_t *pt, const double *g) override {
+        for (int i = 0; i < n; i++) (solid ? sgs : sgf).push_back({pt[i], (R)g[i]});
     }
 
     // ------------------------------ sources ------------------------------
@@ -938,8 +963,21 @@ struct Oracle : OracleBase {
         }
     }
 
-    // SolidFluidCoupling::apply (SolidFluidCoupling.cpp:30-36)
+    // AbsorbingBoundary::applyClayton, then SolidFluidCoupling::apply
+    // (Domain::applyBC_BeforeAssemblingStiff, Domain.cpp:313-317)
     void bc_before() override {
+        for (auto &c : cls) {
+            Cx<R> *f = &sp.stiff[(size_t)sp.off[c.p] * 3];
+            const Cx<R> *v = &sp.veloc[(size_t)sp.off[c.p] * 3];
+            for (int a = 0; a < sp.nu[c.p]; a++) {
+                f[a * 3 + 0] -= (c.ss * v[a * 3 + 0] + c.sz * v[a * 3 + 2]);
+                f[a * 3 + 2] -= (c.sz * v[a * 3 + 0] + c.zz * v[a * 3 + 2]);
+                f[a * 3 + 1] -= c.pp * v[a * 3 + 1];
+            }
+        }
+        for (auto &c : clf)
+            for (int a = 0; a < fp.nu[c.p]; a++)
+                fp.stiff[(size_t)fp.off[c.p] + a] -= fp.veloc[(size_t)fp.off[c.p] + a] * c.c;
         for (auto &c : sf) {
             int nus = sp.nu[c.s], nuf = fp.nu[c.f];
             int nu = std::min(nus, nuf);
@@ -1008,9 +1046,22 @@ struct Oracle : OracleBase {
             }
         }
     }
+    // computeStiffToAccel on all points, then the sponge
+    // (Domain::applyBC_AfterComputingAccel, Sponge::apply, ABC/Sponge.hpp:74-98)
     void stiff_to_accel() override {
         points_to_accel(sp);
         points_to_accel(fp);
+        const R two = 2;
+        for (auto &g : sgs) {
+            size_t o = (size_t)sp.off[g.first] * 3;
+            for (int q = 0; q < sp.nu[g.first] * 3; q++)
+                sp.stiff[o + q] -= (two * g.second) * sp.veloc[o + q] + (g.second * g.second) * sp.displ[o + q];
+        }
+        for (auto &g : sgf) {
+            size_t o = (size_t)fp.off[g.first];
+            for (int q = 0; q < fp.nu[g.first]; q++)
+                fp.stiff[o + q] -= (two * g.second) * fp.veloc[o + q] + (g.second * g.second) * fp.displ[o + q];
+        }
     }
 
     // NewmarkTimeScheme::update (NewmarkTimeScheme.hpp:47-71)
@@ -1156,6 +1207,8 @@ int axo_set_solid_fluid(void *h, const axg_solid_fluid *c) { AXO_TRY(static_cast
 int axo_set_moment_sources(void *h, const axg_moment_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_moment_sources(s)) }
 int axo_set_force_sources(void *h, const axg_force_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_force_sources(s)) }
 int axo_set_stations(void *h, const axg_stations *s, int interval) { AXO_TRY(static_cast<OracleBase *>(h)->set_stations(s, interval)) }
+int axo_set_clayton(void *h, int solid, const axg_clayton *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton(solid, c)) }
+int axo_set_sponge(void *h, int solid, int n, const int32_t *pt, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge(solid, n, pt, g)) }
 int axo_apply_sources(void *h, int tstep) { AXO_TRY(static_cast<OracleBase *>(h)->apply_sources(tstep)) }
 int axo_compute_stiffness(void *h, int nthreads) { AXO_TRY(static_cast<OracleBase *>(h)->compute_stiffness(nthreads)) }
 int axo_bc_before(void *h) { AXO_TRY(static_cast<OracleBase *>(h)->bc_before()) }

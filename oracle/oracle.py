@@ -50,6 +50,8 @@ def lib():
             "axo_set_force_sources": (C.c_int, [V, C.POINTER(L.axg_force_sources)]),
             "axo_set_stations": (C.c_int, [V, C.POINTER(L.axg_stations), C.c_int]),
             "axo_apply_sources": (C.c_int, [V, C.c_int]),
+            "axo_set_clayton": (C.c_int, [V, C.c_int, C.POINTER(L.axg_clayton)]),
+            "axo_set_sponge": (C.c_int, [V, C.c_int, C.c_int, L.P_i32, L.P_f64]),
             "axo_compute_stiffness": (C.c_int, [V, C.c_int]),
             "axo_bc_before": (C.c_int, [V]),
             "axo_bc_after": (C.c_int, [V]),
@@ -99,6 +101,13 @@ class Oracle:
         self._chk(self.O.axo_set_moment_sources(self.h, C.byref(s["ms"])))
         self._chk(self.O.axo_set_force_sources(self.h, C.byref(s["fs"])))
         self._chk(self.O.axo_set_stations(self.h, C.byref(s["st"]), int(model.st_interval)))
+        for solid, key in ((1, "cl_s"), (0, "cl_f")):
+            if s[key].count:
+                self._chk(self.O.axo_set_clayton(self.h, solid, C.byref(s[key])))
+        for solid, (pt, g) in ((1, s["sg_s"]), (0, s["sg_f"])):
+            if pt is not None and len(pt):
+                self._chk(self.O.axo_set_sponge(self.h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
+                                                g.ctypes.data_as(L.P_f64)))
 
     def _chk(self, rc):
         if rc != 0:

@@ -9,7 +9,7 @@ pytestmark = pytest.mark.gpu
 
 def _model(nx=8, nz=8, nr=9, sources=True, nst=12):
     from axisem3d_b200 import meshgen
-    m = meshgen.cartesian_model(nx=nx, nz=nz, nr=nr, nstations=nst)
+    m = meshgen.cartesian_model(nx=nx, nz=nz, nr=nr, nstations=nst, nr_aware_dt=True)
     if not sources:
         m.ms_elem = np.zeros(0, np.int32)
         m.ms_nu = np.zeros(0, np.int32)

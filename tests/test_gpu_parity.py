@@ -196,6 +196,11 @@ def test_error_paths(built):
     assert lib.axg_run(h, 1, 1) == L.AXG_E_STATE
     assert b"finalize" in lib.axg_last_error(h)
     lib.axg_destroy(h)
+    dup = meshgen.cartesian_model(nx=3, nz=3, nr=5)
+    dup.sponge_solid = (np.array([1, 1], np.int32), np.array([0.1, 0.2]))
+    with pytest.raises(EngineError) as ei:
+        Solver(dup, "fp32")
+    assert ei.value.code == L.AXG_E_ARG and "twice" in str(ei.value)
     s = Solver(m, "fp32", stability_interval=1)
     u = np.zeros(s.field_size())
     u[0] = np.nan
@@ -279,3 +284,81 @@ def test_plain_and_autotuned_match(built):
             s.run(3)
             out.append(s.get_field("displ"))
     assert rel(out[0], out[2]) <= 1e-13 and rel(out[1], out[2]) <= 1e-13
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_sources_equal_separate_runs(built, precision):
+    """Several sources advanced as batched wavefields in the same launches give
+    each source's own run (spherical shell with fluid, 21-Cij, RTZ)."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    base = meshgen.spherical_model(n_theta=16, n_solid_layers=4, n_fluid_layers=2, nr_max=24,
+                                   rheology="aniso", attenuation=None)
+    ens = meshgen.ensemble_model(base, nsrc=3, seed=5)
+    with Solver(ens, precision) as s:
+        s.run(40)
+        d = s.get_field("displ").reshape(3, -1)
+        seis = s.seismograms()
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    for i in range(3):
+        with Solver(meshgen.single_source(ens, i), precision) as s1:
+            s1.run(40)
+            assert rel(d[i], s1.get_field("displ")) <= tol
+            assert rel(seis[:, i], s1.seismograms()) <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 1e-4), ("mixed", 1e-4)])
+def test_absorbing_boundaries_parity(built, precision, tol):
+    """Clayton conditions on the outer and bottom edges (a corner point carries one per
+    boundary) and a Kosloff sponge: 800 steps of the plain forward, long enough for the
+    waves to reach the boundaries, vs the oracle (displacement and seismograms)."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.cartesian_model(nx=8, nz=8, nr=5, nstations=6, absorbing=True,
+                                attenuation=dict(meshgen.default_sls(3), qkappa=57823.0, qmu=200.0))
+    assert len(np.unique(m.cl_solid["point"])) < len(m.cl_solid["point"])   # corner listed twice
+    o = O.Oracle(m, "fp64", threads=4)
+    o.run(800)
+    with Solver(m, precision) as s:
+        s.run(800)
+        assert rel(s.get_field("displ"), o.get_field("displ")) <= 5 * tol
+        assert rel(s.seismograms(), o.seismograms()) <= tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fluid_clayton_and_sponges_parity(built, precision):
+    """ClaytonFluid1D on fluid points, sponges on both solid and fluid points of the
+    spherical shell, five full steps vs the oracle."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.spherical_model(**SPH["sph_iso_1d_full_fluid"])
+    rng = np.random.default_rng(7)
+    nf = len(m.fp_nr)
+    fpt = np.sort(rng.choice(nf, size=max(4, nf // 5), replace=False)).astype(np.int32)
+    rvp = np.full(len(fpt), 1.0e7)
+    m.cl_fluid = {"point": np.concatenate([fpt, fpt[:3]]),
+                  "rho_vp": np.concatenate([rvp, rvp[:3]]),
+                  "area": 0.05 * np.concatenate([m.fp_mass[fpt], m.fp_mass[fpt[:3]]]) * 1.0e7 / m.dt}
+    spt = np.sort(rng.choice(len(m.sp_nr), size=len(m.sp_nr) // 4, replace=False)).astype(np.int32)
+    m.sponge_solid = (spt, rng.uniform(0.0, 0.3 / m.dt, len(spt)))
+    m.sponge_fluid = (fpt, rng.uniform(0.0, 0.3 / m.dt, len(fpt)))
+    us = meshgen.random_displacement(m, seed=3) * 1e-9
+    uf = meshgen.random_displacement(m, seed=4, solid=False) * 1e-9
+    o = O.Oracle(m, "fp64")
+    o.set_field(us, "displ")
+    o.set_field(uf, "displ", solid=False)
+    o.set_field(us, "veloc")
+    o.set_field(uf, "veloc", solid=False)
+    o.run(5)
+    tol = 1e-11 if precision == "fp64" else 1e-5
+    with Solver(m, precision) as s:
+        s.set_field(us, "displ")
+        s.set_field(uf, "displ", solid=False)
+        s.set_field(us, "veloc")
+        s.set_field(uf, "veloc", solid=False)
+        s.run(5)
+        for solid in (True, False):
+            assert rel(s.get_field("displ", solid=solid), o.get_field("displ", solid=solid)) <= tol
+            assert rel(s.get_field("veloc", solid=solid), o.get_field("veloc", solid=solid)) <= tol
