@@ -14,11 +14,14 @@
 // gradient with the integral factor (GradientQuadrature.hpp:294-324 vs
 // 207-231), so each mode's stiffness block is Hermitian: as a real-linear map
 // K^T = K, and the transpose is applied with the forward kernel itself.
-// Reverse step n (cotangents of u_{n+1}, v_{n+1}, a_n), real inner products:
-//   abar_n  = abar_out + h/2 vbar + h^2/2 ubar
+// Since u_{n+1} = u_n + h v_n + h^2/2 a_{n-1} + h^2 a_n, a_n enters v_{n+1} with h/2,
+// u_{n+1} with h^2, and step n+1 (as its a_{n-1}) with the cotangent abar_out.
+// Reverse step n (cotangents ubar, vbar of u_{n+1}, v_{n+1}), real inner products:
+//   abar_n  = abar_out + h/2 vbar + h^2 ubar           (total cotangent of a_n)
 //   g       = P (M^-1 abar_n)                        (cotangent of the stiffness)
 //   ubar_n  = ubar + (-K g) + R^T r_n
-//   vbar_n  = vbar + h ubar,  abar_out' = h/2 vbar
+//   vbar_n  = vbar + h ubar
+//   abar_out' = h/2 vbar + h^2/2 ubar = h/2 vbar_n     (cotangent of a_{n-1})
 //   dJ/dM_p     += -<abar_n, a_n>_p / M_p
 //   dJ/dlambda  += -sum_a ifact_q Re(conj(tr e(g)) tr e(u_n))
 //   dJ/dmu      += -sum_a ifact_q Re(conj(e(g)) . D_mu e(u_n)),  D_mu = diag(2,2,2,1,1,1)
@@ -40,7 +43,7 @@ struct AdjointArgs {
     const int64_t *mod_off;
     const int *pt_off, *pt_nu;
     const cx_t<T> *u;           // forward displacement at step n
-    const cx_t<T> *g;           // W^-1 P M^-1 abar_n
+    const cx_t<T> *g;           // P M^-1 abar_n
     cx_t<T> *out;               // receives -K g (scatter-add)
     const T *ifact;             // [n][25] integral factor
     T *grad;                    // [n][2][25]: dJ/dlambda, dJ/dmu per element point
@@ -233,7 +236,7 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
     }
 }
 
-// per point mode: abar_n, dJ/dM, g = W^-1 P M^-1 abar_n, vbar_n, abar_out'
+// per point mode: abar_n, dJ/dM, g = P M^-1 abar_n, vbar_n, abar_out'
 template <class T>
 struct AdjPointArgs {
     int nmodes;
@@ -260,12 +263,13 @@ __global__ void adjoint_point_kernel(const AdjPointArgs<T> a) {
     for (int c = 0; c < 3; c++) {
         const size_t q = (size_t)m * 3 + c;
         const cx_t<T> ub = a.ubar[q], vb = a.vbar[q], ao = a.abar_out[q];
-        cx_t<T> abn = mk<T>(ao.x + h / 2 * vb.x + h * h / 2 * ub.x, ao.y + h / 2 * vb.y + h * h / 2 * ub.y);
+        const cx_t<T> abn = mk<T>(ao.x + h / 2 * vb.x + h * h * ub.x, ao.y + h / 2 * vb.y + h * h * ub.y);
         const cx_t<T> an = a.a_n[q];
         dm -= (abn.x * an.x + abn.y * an.y) * im;
         ab[c] = cscale(abn, im);
-        a.vbar[q] = mk<T>(vb.x + h * ub.x, vb.y + h * ub.y);
-        a.abar_out[q] = mk<T>(h / 2 * vb.x, h / 2 * vb.y);
+        const cx_t<T> vn = mk<T>(vb.x + h * ub.x, vb.y + h * ub.y);
+        a.vbar[q] = vn;
+        a.abar_out[q] = mk<T>(h / 2 * vn.x, h / 2 * vn.y);
     }
     // P is symmetric (axial projection and Nyquist rule), so P^T = P
     point_bc<T>(ab, 3, al, nu, nr, a.flags[p], true);

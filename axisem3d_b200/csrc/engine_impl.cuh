@@ -788,16 +788,18 @@ private:
         if (team > 32) tpc = std::min(tpc, 15);
         b.tpc = tpc;
         raise_smem_limit((const void *)b.kernel, tpc * L.total);
-        // persistent grid: every SM holds as many CTAs as fit; the teams then walk the
-        // bucket, prefetching their next element into L2 while computing the current one
+        // one CTA per group of tpc elements: measured faster on B200 than a persistent grid
+        // (the hardware scheduler refills an SM as soon as any CTA ends, which hides the
+        // tail of uneven nr better than a fixed walk). AXG_PERSISTENT_GRID restores the
+        // persistent walk with next-element L2 prefetch.
+        b.grid = (b.n + tpc - 1) / tpc;
+#ifdef AXG_PERSISTENT_GRID
         int per_sm = 0;
         AXG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b.kernel, team * tpc,
                                                                tpc * L.total));
-        b.grid = std::max(1, std::min((b.n + tpc - 1) / tpc, std::max(1, per_sm) * prop_.multiProcessorCount));
-#ifdef AXG_NO_PERSISTENT_GRID
-        b.grid = (b.n + tpc - 1) / tpc;
+        if (!cfg_.plain)
+            b.grid = std::max(1, std::min(b.grid, std::max(1, per_sm) * prop_.multiProcessorCount));
 #endif
-        if (cfg_.plain) b.grid = (b.n + tpc - 1) / tpc;   // one team per element, no persistence
     }
 
     // The project's autotuner: for every solid bucket, time each feasible team size
