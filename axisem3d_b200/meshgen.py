@@ -949,9 +949,12 @@ def aniso_moduli_from(lam, mu, rng, pert):
         C[:, 3 + k, 3 + k] = mf
     R = rng.normal(0.0, 1.0, (n, 6, 6))
     R = 0.5 * (R + np.transpose(R, (0, 2, 1)))
-    C = C + pert * mf[:, None, None] * R / 3.0
-    ev = np.linalg.eigvalsh(C)
-    if np.min(ev) <= 0:
+    P = pert * mf[:, None, None] * R / 3.0
+    C = C + P
+    # the isotropic part's smallest eigenvalue is mu (shear, Voigt), so |P|_F < mu
+    # proves C positive definite; only the rest need an eigenvalue check
+    unsure = np.sqrt(np.sum(P * P, axis=(1, 2))) >= mf * (1.0 - 1e-12)
+    if np.any(unsure) and np.min(np.linalg.eigvalsh(C[unsure])) <= 0:
         raise ValueError("perturbed Cij not positive definite")
     iu = np.triu_indices(6)
     return [C[:, a, b].reshape(shp) for a, b in zip(*iu)]
