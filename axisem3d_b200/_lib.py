@@ -108,6 +108,7 @@ SIGNATURES = {
     "axg_finalize": (C.c_int, [H]),
     "axg_apply_sources": (C.c_int, [H, C.c_int32]),
     "axg_compute_stiffness": (C.c_int, [H]),
+    "axg_compute_stiffness_noalloc": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "axg_apply_bc_before_assembly": (C.c_int, [H]),
     "axg_apply_bc_after_assembly": (C.c_int, [H]),
     "axg_stiff_to_accel": (C.c_int, [H]),

@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                    "-diag-suppress", "607"]
-CU_SOURCES = ["engine_fp32.cu", "engine_fp64.cu", "engine_mixed.cu"]
+CU_SOURCES = ["engine_fp32.cu", "engine_fp64.cu", "engine_mixed.cu", "noalloc.cu"]
 CPP_SOURCES = ["capi.cpp", "operands.cpp"]
 
 

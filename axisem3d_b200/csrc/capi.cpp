@@ -359,6 +359,16 @@ int axg_apply_sources(axg_solver *h, int32_t tstep) {
 int axg_compute_stiffness(axg_solver *h) {
     return guarded(h, [&] { h->eng->compute_stiffness(); });
 }
+// no device allocation: the SLS memory of the evaluation lives in the library's fixed
+// device array (noalloc.cu), looked up on this handle's device at the first call there
+int axg_compute_stiffness_noalloc(axg_solver *h, const void *solid_x, void *solid_f, const void *fluid_x,
+                                  void *fluid_f) {
+    return guarded(h, [&] {
+        if (!h->finalized) throw axg::Error(AXG_E_STATE, "axg_compute_stiffness_noalloc || axg_finalize not called.");
+        void *scratch = axg::noalloc_scratch(h->eng->device());
+        h->eng->stiffness_noalloc(solid_x, solid_f, fluid_x, fluid_f, scratch, AXG_NOALLOC_SCRATCH_BYTES);
+    });
+}
 int axg_apply_bc_before_assembly(axg_solver *h) {
     return guarded(h, [&] { h->eng->bc_before(); });
 }

@@ -119,7 +119,16 @@ public:
     virtual void forward_checkpointed(int nsteps, int interval) = 0;
     virtual void adjoint_run(const double *seis_adj, double *grad_mod, double *grad_mass,
                              double *grad_u0, double *grad_v0) = 0;
+    // -K x added to f (device pointers, one wavefield), SLS memory in `scratch` (cap bytes,
+    // cleared here); queues work on the handle's stream and allocates nothing
+    virtual void stiffness_noalloc(const void *sx, void *sf, const void *fx, void *ff, void *scratch,
+                                   size_t cap) = 0;
+    virtual int device() const = 0;
 };
+
+// device address of the library's fixed no-allocation scratch on `device` (looked up
+// once per device; noalloc.cu)
+void *noalloc_scratch(int device);
 
 std::unique_ptr<EngineBase> make_engine_fp32(const axg_config &cfg);
 std::unique_ptr<EngineBase> make_engine_fp64(const axg_config &cfg);

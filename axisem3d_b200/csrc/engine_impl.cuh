@@ -490,6 +490,65 @@ public:
         set_step(step_);
     }
 
+    // The stiffness evaluation of launch_stiffness for one caller-owned wavefield (solid x / f,
+    // fluid x / f on the device, in C), with the SLS memory variables in `scratch` cleared
+    // first: the result is that of a handle at rest. Nothing is allocated.
+    void stiffness_noalloc(const void *sx, void *sf, const void *fx, void *ff, void *scratch,
+                           size_t cap) override {
+        need();
+        const char *who = "axg_compute_stiffness_noalloc || ";
+        auto aligned = [](const void *p) { return ((uintptr_t)p % alignof(C)) == 0; };
+        if (!sb_.empty() && (!sx || !sf))
+            throw Error(AXG_E_ARG, std::string(who) + "solid field pointers missing.");
+        if (!fb_.empty() && (!fx || !ff))
+            throw Error(AXG_E_ARG, std::string(who) + "fluid field pointers missing.");
+        if ((sx && !aligned(sx)) || (sf && !aligned(sf)) || (fx && !aligned(fx)) || (ff && !aligned(ff)))
+            throw Error(AXG_E_ARG, std::string(who) + "field pointers must be aligned to a complex value.");
+        const size_t need_bytes = (size_t)state_wave_ * sizeof(AT);
+        if (need_bytes > cap)
+            throw Error(AXG_E_ARG, std::string(who) + "the model's SLS state (" + std::to_string(need_bytes) +
+                                       " bytes) exceeds the fixed scratch of " + std::to_string(cap) + " bytes.");
+        if (need_bytes) AXG_CUDA(cudaMemsetAsync(scratch, 0, need_bytes, stream_));
+        for (auto &bp : sb_) {
+            SolidBucket &b = *bp;
+            SolidArgs<T, AT> a;
+            a.n_elem = b.n; a.nr = b.nr.p; a.pts = b.pts.p; a.axial = b.axial.p;
+            a.geom = b.geom.p; a.trig = b.trig.p; a.mod = b.mod.p; a.mod_off = b.mod_off.p;
+            a.attmod = b.attmod.p; a.att_off = b.att_off.p; a.state = reinterpret_cast<AT *>(scratch);
+            a.state_off = b.state_off.p; a.pt_off = sp_.off.p; a.pt_nu = sp_.nu.p;
+            a.displ = reinterpret_cast<const C *>(sx); a.stiff = reinterpret_cast<C *>(sf);
+            a.tw = tw_.p; a.tw_off = tw_off_.p;
+            a.nsls = cfg_.nsls;
+            for (int l = 0; l < 8; l++) {
+                a.alpha[l] = (AT)cfg_.att_alpha[l]; a.beta[l] = (AT)cfg_.att_beta[l];
+                a.gamma[l] = (AT)cfg_.att_gamma[l];
+            }
+            a.gmat = gmat_.p;
+            a.nwave = 1;
+            a.fstride = 0;
+            a.sstride = 0;
+            b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc,
+                                                                              b.tpc, b.team_bytes);
+            post_launch();
+        }
+        for (auto &bp : fb_) {
+            FluidBucket &b = *bp;
+            FluidArgs<T> a;
+            a.n_elem = b.n; a.nr = b.nr.p; a.pts = b.pts.p; a.axial = b.axial.p; a.geom = b.geom.p;
+            a.K = b.K.p; a.K_off = b.K_off.p; a.pt_off = fp_.off.p; a.pt_nu = fp_.nu.p;
+            a.displ = reinterpret_cast<const C *>(fx); a.stiff = reinterpret_cast<C *>(ff);
+            a.tw = tw_.p; a.tw_off = tw_off_.p;
+            a.gmat = gmat_.p;
+            a.nwave = 1;
+            a.fstride = 0;
+            int blocks = (b.n + b.tpc - 1) / b.tpc;
+            b.kernel<<<blocks, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.tpc,
+                                                                              b.team_bytes);
+            post_launch();
+        }
+    }
+    int device() const override { return cfg_.device; }
+
 private:
     void check_adjoint_model() const {
         const HostSolidElements &h = model_.se;

@@ -99,6 +99,13 @@ class Solver:
     def compute_stiffness(self):
         self._check(self.lib.axg_compute_stiffness(self.h))
 
+    def compute_stiffness_noalloc(self, solid_x, solid_f, fluid_x=None, fluid_f=None):
+        """f -= K x for caller-owned device buffers (integer device addresses, complex in the
+        handle's stiffness precision), with no device allocation by the library: the
+        evaluation's SLS memory lives in the library's fixed device array (see
+        axg_compute_stiffness_noalloc in include/axg.h for its limit and sharing rules)."""
+        self._check(self.lib.axg_compute_stiffness_noalloc(self.h, solid_x, solid_f, fluid_x, fluid_f))
+
     def apply_bc_before_assembly(self):
         self._check(self.lib.axg_apply_bc_before_assembly(self.h))
 

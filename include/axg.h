@@ -331,6 +331,29 @@ int  axg_set_stream(axg_solver *h, void *stream);
    4: larger); 32, 64, 128 or 256; before axg_finalize (the autotuner's knob) */
 int  axg_set_team_size(axg_solver *h, int32_t nr_class, int32_t team);
 
+/* ---- stiffness of a caller's field with no device allocation ----
+   No counterpart in the reference. Adds -K x to f for every element of a finalized handle,
+   as axg_compute_stiffness does for the handle's own displacement on a freshly created
+   handle (SLS memory at rest). x and f are DEVICE pointers in the handle's field layout
+   ([sum nu][3] complex for solid points, [sum nu] complex for fluid points, the sizes of
+   axg_field_size) and in its stiffness precision: complex float for AXG_FP32 and AXG_MIXED,
+   complex double for AXG_FP64; the fluid pair may be NULL when there are no fluid elements.
+   The handle's own fields and attenuation state are not touched.
+   For callers that must not allocate device memory: a process whose device memory is
+   owned by another runtime (JAX/XLA reserves most of the GPU up front, serving frameworks
+   run their own pools), where cudaMalloc fails or escapes the owner's accounting, and code
+   called back from such a runtime. Working memory (the SLS memory variables of this one
+   evaluation) lives in a fixed device array inside the library, AXG_NOALLOC_SCRATCH_BYTES
+   large, which every GPU that loads the library keeps until the process exits; a model whose
+   SLS state is larger gets AXG_E_ARG. The array is cleared at the start of each call. All
+   calls on a device share it, so calls whose GPU work overlaps (other streams, other handles)
+   race: order them on one stream or synchronize between them. The work is queued on the
+   handle's stream (axg_set_stream). The first call on a device looks the array up
+   (cudaGetSymbolAddress); make that first call before any stream capture. */
+#define AXG_NOALLOC_SCRATCH_BYTES (16u << 20)
+int  axg_compute_stiffness_noalloc(axg_solver *h, const void *solid_x, void *solid_f,
+                                   const void *fluid_x, void *fluid_f);
+
 /* ---- operand construction (host, double), the preloop numbers ---- */
 /* GLL/GLJ positions, weights and G matrices for nPol = 4, derived from their
    definitions and rounded to 12 decimals (spectrals.hpp:73-102) */
