@@ -43,6 +43,28 @@ constexpr int ATT_NONE = 0, ATT_FULL = 1, ATT_CG4 = 2;
 #ifndef AXG_PREFETCH_NEXT
 #define AXG_PREFETCH_NEXT 0
 #endif
+// 1 = the register-resident slice path sums slices k and nr - k together (a pass of its
+// own); 0 = one Fourier -> slice sum per (slice, point) inside the stress pass
+#ifndef AXG_SLICE_PAIRS
+#define AXG_SLICE_PAIRS 1
+#endif
+#ifndef AXG_KP
+#define AXG_KP 2
+#endif
+// the same two blockings for elements without attenuation, whose slice pass holds no SLS
+// state in registers and can afford wider blocks
+#ifndef AXG_KP_ELASTIC
+#define AXG_KP_ELASTIC 4
+#endif
+#ifndef AXG_AB_ELASTIC
+#define AXG_AB_ELASTIC 4
+#endif
+// 1 = L2 prefetch of an element's slice operands (moduli, attenuation moduli, SLS state)
+// at the start of its slice phase
+#ifndef AXG_PREFETCH_SLICES
+#define AXG_PREFETCH_SLICES 1
+#endif
+constexpr int KP = AXG_KP;   // slice pairs per thread in the paired Fourier -> slice pass
 constexpr int KB = AXG_KB;   // slices per thread in the Fourier -> slice transform
 constexpr int AB = AXG_AB;   // modes per thread in the slice -> Fourier transform
 
@@ -331,6 +353,9 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                        const int teams_per_cta, const size_t team_bytes) {
     using C = cx_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    // register blocking of the paired Fourier -> slice pass and of the slice -> Fourier pass
+    constexpr int KPc = ATT == ATT_NONE ? AXG_KP_ELASTIC : KP;
+    constexpr int ABc = ATT == ATT_NONE ? AXG_AB_ELASTIC : AB;
     const int TEAM = blockDim.x / teams_per_cta;
     const int team = threadIdx.x / TEAM;
     const int lane = threadIdx.x % TEAM;
@@ -385,7 +410,8 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
         }
         if constexpr (IS3D) {
             const T *tw = a.tw + a.tw_off[nr];
-            for (int i = lane; i < 2 * nr; i += TEAM) sTw[i] = tw[i];
+            // interleaved (cos, sin) pairs: one 2-word shared load per twiddle
+            for (int i = lane; i < 2 * nr; i += TEAM) sTw[i] = (i & 1) ? tw[nr + (i >> 1)] : tw[i >> 1];
         }
         team_sync(team, TEAM);
 
@@ -507,23 +533,91 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
 
         // ---------------- 3-D material: slices ----------------
         if constexpr (IS3D) {
-            const T *twc = sTw, *tws = sTw + nr;
+            using T2 = cx_t<T>;
+            const T2 *tw2 = reinterpret_cast<const T2 *>(sTw);
             const T inv_nr = (T)1 / (T)nr;
             const int nkb = (nr + KB - 1) / KB;
-            const int nab = (nu + AB - 1) / AB;
+            const int nab = (nu + ABc - 1) / ABc;
+#if AXG_PREFETCH_SLICES
+            if constexpr (NS > 0 || ATT == ATT_NONE) {
+                // the slice operands of this element start moving into L2 now, so that the
+                // stress pass finds them there after the Fourier -> slice pass
+                constexpr int NM_ = RHEO == RHEO_ISO ? 2 : RHEO == RHEO_TISO ? 5 : 21;
+                prefetch_l2(a.mod + moff, (size_t)NM_ * nr * 25 * sizeof(T), lane, TEAM);
+                if constexpr (ATT != ATT_NONE) {
+                    constexpr int NPA_ = ATT == ATT_CG4 ? 4 : 25;
+                    const size_t slots = (size_t)nr * NPA_;
+                    prefetch_l2(a.attmod + a.att_off[e], 2 * slots * sizeof(T), lane, TEAM);
+                    prefetch_l2(statew + a.state_off[e], (size_t)(6 + 6 * NS) * slots * sizeof(AT), lane, TEAM);
+                }
+            }
+#endif
             for (int q0 = 0; q0 < 25; q0 += qc_max) {
                 const int qcnt = min(qc_max, 25 - q0);
                 if constexpr (NS > 0 || ATT == ATT_NONE) {
-                // One thread per (slice, point): the global operands of the point-slice
-                // (moduli, attenuation moduli, SLS state) are loaded into registers
-                // first, so that their latency overlaps the Fourier -> slice sum
-                // (computeC2R) that follows, then stress and attenuation are applied
-                // and the state is stored back.
+                // Register-resident slice path. Two passes:
+                //  1. computeC2R, one thread per (slice pair, point): slices k and nr - k
+                //     share their twiddles (cos equal, sin opposite), so one pass over the
+                //     modes gives both, x_k = c0 + 2 (A - B) and x_{nr-k} = c0 + 2 (A + B)
+                //     with A = sum Re(c) cos, B = sum Im(c) sin; the slice strains go to the
+                //     slots of region B that the slice stresses later overwrite;
+                //  2. one thread per (slice, point): the global operands of the point-slice
+                //     (moduli, attenuation moduli, SLS state) are loaded into registers,
+                //     stress and attenuation applied, the state stored back.
                 constexpr int NM = RHEO == RHEO_ISO ? 2 : RHEO == RHEO_TISO ? 5 : 21;
                 constexpr int NSR = NS > 0 ? NS : 1;
                 constexpr int NPA = ATT == ATT_CG4 ? 4 : 25;
                 const T *modp = a.mod + moff;
                 const size_t nsl = (size_t)nslice * 25;
+#if AXG_SLICE_PAIRS
+                // KPc slice pairs per thread: each mode value read from shared memory feeds
+                // 2 KPc products
+                const int npair = nr / 2 + 1;
+                const int npb = (npair + KPc - 1) / KPc;
+                for (int i = lane; i < npb * qcnt; i += TEAM) {
+                    const int pb = i / qcnt, qq = i - pb * qcnt, q = q0 + qq;
+                    const int k0 = pb * KPc;
+                    T A[KPc][6], B[KPc][6];
+                    int j[KPc], kst[KPc];
+#pragma unroll
+                    for (int kk = 0; kk < KPc; kk++) {
+                        j[kk] = 0;
+                        kst[kk] = k0 + kk < npair ? k0 + kk : 0;
+#pragma unroll
+                        for (int d = 0; d < 6; d++) { A[kk][d] = 0; B[kk][d] = 0; }
+                    }
+                    for (int al = 1; al < nu; al++) {
+                        C ev[6];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) ev[d] = rA[(al * 6 + d) * 25 + q];
+#pragma unroll
+                        for (int kk = 0; kk < KPc; kk++) {
+                            j[kk] += kst[kk];
+                            j[kk] = j[kk] >= nr ? j[kk] - nr : j[kk];
+                            const T2 w2 = tw2[j[kk]];
+                            const T c = w2.x, sn = w2.y;
+#pragma unroll
+                            for (int d = 0; d < 6; d++) {
+                                A[kk][d] += ev[d].x * c;
+                                B[kk][d] += ev[d].y * sn;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int kk = 0; kk < KPc; kk++) {
+                        const int k = k0 + kk;
+                        if (k >= npair) break;
+                        const bool two = k != 0 && 2 * k != nr;
+#pragma unroll
+                        for (int d = 0; d < 6; d++) {
+                            const T c0 = rA[d * 25 + q].x;
+                            rBr[((size_t)k * 6 + d) * qcnt + qq] = c0 + (T)2 * (A[kk][d] - B[kk][d]);
+                            if (two) rBr[((size_t)(nr - k) * 6 + d) * qcnt + qq] = c0 + (T)2 * (A[kk][d] + B[kk][d]);
+                        }
+                    }
+                }
+                team_sync(team, TEAM);
+#endif
                 for (int i = lane; i < nr * qcnt; i += TEAM) {
                     const int k = i / qcnt, qq = i - k * qcnt, q = q0 + qq;
                     T md[NM];
@@ -552,21 +646,27 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                                 for (int d = 0; d < 6; d++) mem[l][d] = st[(6 + l * 6 + d) * nslot + slot];
                         }
                     }
-                    // computeC2R at slice k: r = Re c0 + 2 sum Re(c_a e^{i a phi_k})
                     T acc[6];
+#if AXG_SLICE_PAIRS
+#pragma unroll
+                    for (int d = 0; d < 6; d++) acc[d] = rBr[((size_t)k * 6 + d) * qcnt + qq];
+#else
+                    // computeC2R at slice k: r = Re c0 + 2 sum Re(c_a e^{i a phi_k})
 #pragma unroll
                     for (int d = 0; d < 6; d++) acc[d] = rA[d * 25 + q].x;
                     int j = 0;
                     for (int al = 1; al < nu; al++) {
                         j += k;
                         j = j >= nr ? j - nr : j;
-                        const T c = twc[j], sn = tws[j];
+                        const T2 w2 = tw2[j];
+                        const T c = w2.x, sn = w2.y;
 #pragma unroll
                         for (int d = 0; d < 6; d++) {
                             const C ev = rA[(al * 6 + d) * 25 + q];
                             acc[d] += (T)2 * (ev.x * c - ev.y * sn);
                         }
                     }
+#endif
                     re1<T> ev[6], sg[6];
 #pragma unroll
                     for (int d = 0; d < 6; d++) ev[d].x = acc[d];
@@ -623,7 +723,8 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                         for (int kk = 0; kk < KB; kk++) {
                             j[kk] += kstep[kk];
                             j[kk] = j[kk] >= nr ? j[kk] - nr : j[kk];
-                            const T c = twc[j[kk]], s = tws[j[kk]];
+                            const T2 w2 = tw2[j[kk]];
+                            const T c = w2.x, s = w2.y;
 #pragma unroll
                             for (int d = 0; d < 6; d++)
                                 acc[kk][d] += (T)2 * (ev[d].x * c - ev[d].y * s);
@@ -663,34 +764,43 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 // slices -> Fourier (computeR2C) into region A for these points
                 for (int i = lane; i < nab * qcnt; i += TEAM) {
                     const int ab = i / qcnt, qq = i - ab * qcnt, q = q0 + qq;
-                    const int a0 = ab * AB;
-                    T re[AB][6], im[AB][6];
-                    int j[AB], astep[AB];
+                    const int a0 = ab * ABc;
+                    T re[ABc][6], im[ABc][6];
+                    int j[ABc], astep[ABc];
 #pragma unroll
-                    for (int aa = 0; aa < AB; aa++) {
+                    for (int aa = 0; aa < ABc; aa++) {
                         j[aa] = 0;
                         astep[aa] = (a0 + aa) % nr;
 #pragma unroll
                         for (int d = 0; d < 6; d++) { re[aa][d] = 0; im[aa][d] = 0; }
                     }
-                    for (int k = 0; k < nr; k++) {
-                        T x[6];
+                    // slices k and nr - k in one pass: cos(a phi) is even and sin(a phi) odd
+                    // in k, so they enter as x_k + x_{nr-k} and x_k - x_{nr-k}
+                    for (int k = 0; k <= nr / 2; k++) {
+                        const bool two = k != 0 && 2 * k != nr;
+                        T xs[6], xd[6];
 #pragma unroll
-                        for (int d = 0; d < 6; d++) x[d] = rBr[((size_t)k * 6 + d) * qcnt + qq] * inv_nr;
+                        for (int d = 0; d < 6; d++) {
+                            const T x1 = rBr[((size_t)k * 6 + d) * qcnt + qq];
+                            const T x2 = two ? rBr[((size_t)(nr - k) * 6 + d) * qcnt + qq] : (T)0;
+                            xs[d] = (x1 + x2) * inv_nr;
+                            xd[d] = (x1 - x2) * inv_nr;
+                        }
 #pragma unroll
-                        for (int aa = 0; aa < AB; aa++) {
-                            const T c = twc[j[aa]], s = tws[j[aa]];
+                        for (int aa = 0; aa < ABc; aa++) {
+                            const T2 w2 = tw2[j[aa]];
+                            const T c = w2.x, s = w2.y;
 #pragma unroll
                             for (int d = 0; d < 6; d++) {
-                                re[aa][d] += x[d] * c;
-                                im[aa][d] -= x[d] * s;
+                                re[aa][d] += xs[d] * c;
+                                im[aa][d] -= xd[d] * s;
                             }
                             j[aa] += astep[aa];
                             j[aa] = j[aa] >= nr ? j[aa] - nr : j[aa];
                         }
                     }
 #pragma unroll
-                    for (int aa = 0; aa < AB; aa++) {
+                    for (int aa = 0; aa < ABc; aa++) {
                         const int al = a0 + aa;
                         if (al >= nu) break;
                         C sg[6];
