@@ -105,6 +105,7 @@ SIGNATURES = {
     "axg_set_stations": (C.c_int, [H, C.POINTER(axg_stations), C.c_int32]),
     "axg_set_clayton": (C.c_int, [H, C.c_int32, C.POINTER(axg_clayton)]),
     "axg_set_sponge": (C.c_int, [H, C.c_int32, C.c_int32, P_i32, P_f64]),
+    "axg_set_ocean_load": (C.c_int, [H, C.c_int32, P_i32, P_f64, P_f64]),
     "axg_finalize": (C.c_int, [H]),
     "axg_apply_sources": (C.c_int, [H, C.c_int32]),
     "axg_compute_stiffness": (C.c_int, [H]),

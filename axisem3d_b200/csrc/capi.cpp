@@ -302,6 +302,20 @@ int axg_set_sponge(axg_solver *h, int32_t solid, int32_t count, const int32_t *p
     });
 }
 
+int axg_set_ocean_load(axg_solver *h, int32_t count, const int32_t *point, const double *mass_ocean,
+                       const double *theta) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (count < 0 || (count && (!point || !mass_ocean || !theta)))
+            throw axg::Error(AXG_E_ARG, "MassOceanLoad1D || missing array.");
+        axg::HostOcean &x = h->model.ocean;
+        x.count = count;
+        x.pt = copy(point, count);
+        x.mass_ocean = copy(mass_ocean, count);
+        x.theta = copy(theta, count);
+    });
+}
+
 int axg_finalize(axg_solver *h) {
     return guarded(h, [&] {
         need_open(h);
@@ -338,6 +352,21 @@ int axg_finalize(axg_solver *h) {
         for (int i = 0; i < m.cl_f.count; i++)
             if (m.cl_f.pt[i] < 0 || m.cl_f.pt[i] >= m.fp.count)
                 throw axg::Error(AXG_E_ARG, "ClaytonFluid1D || point index out of range.");
+        {
+            // MassOceanLoad1D replaces a solid point's Mass1D: once per point, 1-D masses only
+            std::vector<char> seen(m.sp.count, 0);
+            for (int i = 0; i < m.ocean.count; i++) {
+                const int p = m.ocean.pt[i];
+                if (p < 0 || p >= m.sp.count)
+                    throw axg::Error(AXG_E_ARG, "MassOceanLoad1D || point index out of range.");
+                if (seen[p]) throw axg::Error(AXG_E_ARG, "MassOceanLoad1D || point listed twice.");
+                seen[p] = 1;
+                if (m.sp.mass_nr.size() && m.sp.mass_nr[p] > 1)
+                    throw axg::Error(AXG_E_UNSUPPORTED, "MassOceanLoad3D || 3-D ocean load is not supported.");
+                if (!(m.ocean.mass_ocean[i] >= 0))
+                    throw axg::Error(AXG_E_ARG, "MassOceanLoad1D || negative ocean mass.");
+            }
+        }
         // one Sponge per point (GLLPoint::release averages the boundaries' gammas first)
         for (const auto &sg : {std::make_pair(&m.sg_s, m.sp.count), std::make_pair(&m.sg_f, m.fp.count)}) {
             std::vector<char> seen(sg.second, 0);

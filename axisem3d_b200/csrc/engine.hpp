@@ -71,6 +71,12 @@ struct HostClayton {
     std::vector<double> rvp, rvs, area, theta;
 };
 
+struct HostOcean {
+    int count = 0;
+    std::vector<int> pt;
+    std::vector<double> mass_ocean, theta;
+};
+
 struct HostSponge {
     int count = 0;
     std::vector<int> pt;
@@ -79,6 +85,7 @@ struct HostSponge {
 
 struct HostModel {
     HostClayton cl_s, cl_f;
+    HostOcean ocean;
     HostSponge sg_s, sg_f;
     HostPoints sp, fp;
     HostSolidElements se;

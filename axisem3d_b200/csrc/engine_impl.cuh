@@ -91,6 +91,7 @@ class Engine final : public EngineBase {
     struct PointDev {
         int n = 0, ndim = 3, total = 0, n3d = 0, nr_max = 1;
         std::vector<int> h_off, h_nu, h_nr;
+        std::vector<uint8_t> h_flags;
         DBuf<int> off, nu, nr, mode_pt, pt3d;
         DBuf<uint8_t> flags;
         DBuf<T> inv1, inv3;
@@ -146,6 +147,7 @@ public:
         gmat_.upload(g);
         build_points(m.sp, sp_, true);
         build_points(m.fp, fp_, false);
+        build_ocean(m);
         // twiddles for every nr in use (3-D elements and Mass3D points)
         std::vector<int> nrs;
         int nrmax = 1;
@@ -628,6 +630,27 @@ private:
     }
 
     // -------------------------------------------------------- points ---
+    // MassOceanLoad1D constructor (MassOceanLoad1D.hpp): coefficients in double, cast
+    void build_ocean(const HostModel &m) {
+        ocean_n_ = m.ocean.count;
+        if (!ocean_n_) return;
+        std::vector<T> c((size_t)4 * ocean_n_);
+        for (int i = 0; i < ocean_n_; i++) {
+            const int p = m.ocean.pt[i];
+            const int64_t mo = m.sp.mass_off.size() ? m.sp.mass_off[p] : p;
+            const double mass = m.sp.mass[mo], mv = mass + m.ocean.mass_ocean[i];
+            const double ct = std::cos(m.ocean.theta[i]), st = std::sin(m.ocean.theta[i]);
+            c[4 * i] = (T)(1. / mass * ct * ct + 1. / mv * st * st);
+            c[4 * i + 1] = (T)(1. / mass * st * st + 1. / mv * ct * ct);
+            c[4 * i + 2] = (T)((1. / mv - 1. / mass) * ct * st);
+            c[4 * i + 3] = (T)(1 / mass);
+            sp_.h_flags[p] |= PT_OCEAN;
+        }
+        ocean_pt_.upload(m.ocean.pt);
+        ocean_c_.upload(c);
+        sp_.flags.upload(sp_.h_flags);
+    }
+
     void build_points(const HostPoints &h, PointDev &P, bool solid) {
         P.n = h.count;
         P.ndim = solid ? 3 : 1;
@@ -663,6 +686,7 @@ private:
         P.off.upload(P.h_off); P.nu.upload(P.h_nu); P.nr.upload(P.h_nr);
         P.mode_pt.upload(mode_pt); P.pt3d.upload(pt3d);
         P.flags.upload(flags); P.inv1.upload(inv1);
+        P.h_flags = flags;
         if (inv3.empty()) inv3.push_back((T)0);
         P.inv3.upload(inv3); P.im_off.upload(im_off);
         size_t nf = (size_t)P.total * P.ndim * nwave_;
@@ -829,6 +853,9 @@ private:
         for (size_t i = 0; i < sb_.size(); i++) sb_[i]->state_off.upload(state_offs[i]);
     }
 
+#ifndef AXG_QC_FOR_TWO_CTAS
+#define AXG_QC_FOR_TWO_CTAS 1
+#endif
     void configure_bucket(SolidBucket &b, int team_req = 0) {
         int team = team_req ? team_req
                             : (cfg_.plain ? 256 : (team_override_[b.cls] ? team_override_[b.cls] : default_team(b.cls)));
@@ -839,6 +866,23 @@ private:
         while (L.total > budget / 1 && qc > 1) { qc = (qc + 1) / 2; L = team_layout<T>(b.nr_max, qc); }
         if (L.total > budget)
             throw Error(AXG_E_UNSUPPORTED, "SolidElement::expandWorkspace || nr too large for shared memory.");
+#if AXG_QC_FOR_TWO_CTAS
+        // a one-element CTA too large for two per SM: smaller point chunks of the slice phase
+        // often let a second CTA in
+        // (kept only when it does: smaller chunks alone idle threads in the slice passes)
+        if (team >= 128 && b.is3d) {
+            const size_t two_per_sm = 110 * 1024;
+            int qn = qc;
+            TeamLayout Ln = L;
+            while (qn > 5 && Ln.total > two_per_sm) {
+                const TeamLayout Lh = team_layout<T>(b.nr_max, (qn + 1) / 2);
+                if (Lh.total >= Ln.total) break;
+                qn = (qn + 1) / 2;
+                Ln = Lh;
+            }
+            if (Ln.total <= two_per_sm) { qc = qn; L = Ln; }
+        }
+#endif
         b.qc = qc;
         b.team_bytes = L.total;
         b.team = team;
@@ -1259,8 +1303,17 @@ private:
                 a.inv_mass = P.inv3.p; a.im_off = P.im_off.p; a.tw = tw_.p; a.tw_off = tw_off_.p;
                 a.stiff = P.stiff.p; a.ndim = P.ndim; a.solid = solid; a.nr_max = P.nr_max;
                 a.nwave = nwave_; a.fstride = (size_t)P.total * P.ndim;
+                a.mask = mask;
                 int wpb = 4;
                 mass3d_kernel<T><<<(P.n3d * nwave_ + wpb - 1) / wpb, 32 * wpb, wpb * P.nr_max * sizeof(T), stream_>>>(a);
+                post_launch();
+            }
+            if (solid && ocean_n_ && (mask & 3)) {
+                OceanArgs<T> o;
+                o.n = ocean_n_; o.pt = ocean_pt_.p; o.c = ocean_c_.p; o.nr = P.nr.p; o.off = P.off.p;
+                o.flags = P.flags.p; o.stiff = P.stiff.p; o.nwave = nwave_;
+                o.fstride = (size_t)P.total * P.ndim; o.mask = mask;
+                ocean_mass_kernel<T><<<(ocean_n_ * nwave_ * 32 + 255) / 256, 256, 0, stream_>>>(o);
                 post_launch();
             }
             PointArgs<T, D> a;
@@ -1359,6 +1412,9 @@ private:
     int nwave_ = 1;
     int64_t state_wave_ = 0;
     int cls_n_ = 0, clf_n_ = 0;
+    int ocean_n_ = 0;
+    DBuf<int> ocean_pt_;
+    DBuf<T> ocean_c_;
     DBuf<int> cls_pt_, clf_pt_, cls_first_, clf_first_;
     DBuf<T> cls_c_, clf_c_, sg_s_, sg_f_;
     DBuf<int64_t> ms_po_, fs_po_;

@@ -20,7 +20,7 @@
 namespace axg {
 
 // point flags
-constexpr uint8_t PT_AXIAL = 1, PT_SURFACE = 2, PT_MASS3D = 4;
+constexpr uint8_t PT_AXIAL = 1, PT_SURFACE = 2, PT_MASS3D = 4, PT_OCEAN = 8;
 
 // ------------------------------------------------------ solid-fluid coupling ---
 template <class T>
@@ -130,6 +130,7 @@ struct Mass3DArgs {
     int nr_max;                  // scratch reals per warp
     int nwave;
     size_t fstride;
+    int mask;                    // 1 = boundary conditions, 2 = 1/M
 };
 
 // Boundary conditions on one mode of one point, in the reference order:
@@ -176,13 +177,16 @@ __global__ void mass3d_kernel(const Mass3DArgs<T> a) {
     const uint8_t fl = a.flags[p];
     T *r = reinterpret_cast<T *>(sm) + (size_t)w * a.nr_max;
     const T *twc = a.tw + a.tw_off[nr], *tws = twc + nr;
-    for (int al = lane; al < nu; al += 32) {
-        cx_t<T> f[3];
-        for (int d = 0; d < nd; d++) f[d] = stiff[(size_t)(off + al) * nd + d];
-        point_bc<T>(f, nd, al, nu, nr, fl, a.solid);
-        for (int d = 0; d < nd; d++) stiff[(size_t)(off + al) * nd + d] = f[d];
+    if (a.mask & 1) {
+        for (int al = lane; al < nu; al += 32) {
+            cx_t<T> f[3];
+            for (int d = 0; d < nd; d++) f[d] = stiff[(size_t)(off + al) * nd + d];
+            point_bc<T>(f, nd, al, nu, nr, fl, a.solid);
+            for (int d = 0; d < nd; d++) stiff[(size_t)(off + al) * nd + d] = f[d];
+        }
+        __syncwarp();
     }
-    __syncwarp();
+    if (!(a.mask & 2)) return;
     const T *im = a.inv_mass + a.im_off[p];
     const T inv_nr = (T)1 / (T)nr;
     for (int c = 0; c < nd; c++) {
@@ -220,6 +224,48 @@ __global__ void mass3d_kernel(const Mass3DArgs<T> a) {
 // MIXED (T = float, D = double): increments formed in double, optionally
 // accumulated with compensated (Kahan) summation; a float copy of d feeds the
 // elements.
+// ------------------------------------------------------------- ocean load ---
+// MassOceanLoad1D::computeAccel (point/mass/MassOceanLoad1D.hpp): the point's own mass acts
+// along the surface, mass + ocean mass across it; one warp per point, lanes over modes,
+// after the boundary conditions of the point (as for Mass3D points)
+template <class T>
+struct OceanArgs {
+    int n;
+    const int *pt;               // ocean points
+    const T *c;                  // [n][4]: (ss, zz, sz, pp) inverse-mass coefficients
+    const int *nr, *off;
+    const uint8_t *flags;
+    cx_t<T> *stiff;
+    int nwave;
+    size_t fstride;
+    int mask;                    // 1 = boundary conditions, 2 = ocean-loaded 1/M
+};
+
+template <class T>
+__global__ void ocean_mass_kernel(const OceanArgs<T> a) {
+    const int item = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x & 31;
+    if (item >= a.n * a.nwave) return;
+    const int i = item % a.n, wf = item / a.n;
+    const int p = a.pt[i];
+    const int nr = a.nr[p], nu = nr / 2 + 1, off = a.off[p];
+    const uint8_t fl = a.flags[p];
+    const T css = a.c[4 * i], czz = a.c[4 * i + 1], csz = a.c[4 * i + 2], cpp = a.c[4 * i + 3];
+    cx_t<T> *stiff = a.stiff + (size_t)wf * a.fstride;
+    for (int al = lane; al < nu; al += 32) {
+        cx_t<T> *f = stiff + (size_t)(off + al) * 3;
+        cx_t<T> v[3] = {f[0], f[1], f[2]};
+        if (a.mask & 1) point_bc<T>(v, 3, al, nu, nr, fl, true);
+        if (a.mask & 2) {
+            const cx_t<T> s0 = v[0];
+            v[0] = cadd(cscale(s0, css), cscale(v[2], csz));
+            v[2] = cadd(cscale(s0, csz), cscale(v[2], czz));
+            v[1] = cscale(v[1], cpp);
+        }
+        f[0] = v[0]; f[1] = v[1]; f[2] = v[2];
+    }
+}
+
 template <class T, class D>
 struct PointArgs {
     int nmodes;                  // sum nu
@@ -253,7 +299,7 @@ __global__ void point_update_kernel(const PointArgs<T, D> a) {
     const int nd = a.ndim;
     cx_t<T> f[3];
     for (int d = 0; d < nd; d++) f[d] = a.stiff[(size_t)m * nd + d];
-    if (!(fl & PT_MASS3D)) {
+    if (!(fl & (PT_MASS3D | PT_OCEAN))) {
         if (a.mask & 1) point_bc<T>(f, nd, al, nu, nr, fl, a.solid);
         if (a.mask & 2) {
             const T im = a.inv_mass1[p];

@@ -389,6 +389,57 @@ def add_absorbing(m, nx, nz, width, height, rho=2700.0, vp=5800.0, vs=3460.0, sp
     return m
 
 
+def add_ocean_load(m, nx, nz, width, rho_water=1020.0, depth_water=3000.0, tilt=0.0, seed=0):
+    """MassOceanLoad1D on the surface points (z = 0) of a cartesian_model grid: ocean mass =
+    rho_water * depth_water * area, area = GLL weight * half edge length * s (the
+    axisymmetric line integral of the surface normal). The normal's polar angle is 0 (flat
+    surface) plus, with tilt > 0, a seeded random angle in [0, tilt] per point, which makes
+    the s-z coupling of the ocean-loaded mass non-zero."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    wgll = np.array([0.1, 49.0 / 90.0, 32.0 / 45.0, 49.0 / 90.0, 0.1])
+    h_s = width / nx
+    pts, _ = structured_points(nx, nz)
+    area = {}
+    for i in range(nx):
+        e = i * nz + (nz - 1)
+        for ip in range(5):
+            p = int(pts[e, ip * 5 + 4])
+            area[p] = area.get(p, 0.0) + wgll[ip] * 0.5 * h_s * max(m.sp_coords[p, 0], 0.0)
+    keep = sorted(p for p in area if area[p] > 0.0)
+    mo = np.array([rho_water * depth_water * area[p] for p in keep])
+    th = rng.uniform(0.0, tilt, len(keep)) if tilt > 0 else np.zeros(len(keep))
+    m.ocean_load = (np.array(keep, np.int32), mo, th)
+    return m
+
+
+def with_mass3d(m, amp=0.05, seed=0, exclude=()):
+    """A copy of `m` whose solid points with nr >= 2 (except `exclude`) carry 3-D masses
+    (Mass3D): the point's mass times (1 + amp * U(-1, 1)) per slice, seeded."""
+    import copy
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = copy.copy(m)
+    ex = set(int(p) for p in exclude)
+    nr = np.asarray(m.sp_nr)
+    mass = np.asarray(m.sp_mass, dtype=np.float64)
+    mnr = np.ones(len(nr), np.int32)
+    moff = np.zeros(len(nr), np.int64)
+    vals = []
+    o = 0
+    for p in range(len(nr)):
+        moff[p] = o
+        if nr[p] >= 2 and p not in ex:
+            mnr[p] = nr[p]
+            vals.append(mass[p] * (1.0 + amp * rng.uniform(-1.0, 1.0, nr[p])))
+            o += nr[p]
+        else:
+            vals.append(mass[p:p + 1])
+            o += 1
+    out.sp_mass_nr = mnr
+    out.sp_mass_off = moff
+    out.sp_mass = np.concatenate(vals)
+    return out
+
+
 # ---------------------------------------------------------- microbenchmark ---
 def microbench_model(n_elem=200000, nr_max=64, seed=1, rheology="tiso", attenuation="full",
                      is3d=True, nsls=3, aspect=1.25, s_offset=1.0e6, h=2.0e3, axial_column=False,

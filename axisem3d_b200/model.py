@@ -117,6 +117,8 @@ class Model:
     cl_fluid: Optional[dict] = None               # point, rho_vp, area
     sponge_solid: Optional[tuple] = None          # (points, gamma)
     sponge_fluid: Optional[tuple] = None
+    # MassOceanLoad1D on solid surface points: (points, ocean mass, normal polar angle)
+    ocean_load: Optional[tuple] = None
     meta: dict = field(default_factory=dict)
     meta_rho: Optional[np.ndarray] = None          # (ne, 25) density at element points (generators)
 
@@ -268,6 +270,13 @@ class Model:
                 c.theta = k(name + "_th", d["theta"], _f64, C.c_double)
             return c
 
+        def ocean():
+            if not self.ocean_load:
+                return (None, None, None)
+            pt, mo, th = _i32(self.ocean_load[0]), _f64(self.ocean_load[1]), _f64(self.ocean_load[2])
+            keep["oc_pt"], keep["oc_mo"], keep["oc_th"] = pt, mo, th
+            return (pt, mo, th)
+
         def sponge(name, t):
             if not t:
                 return (None, None)
@@ -278,4 +287,5 @@ class Model:
         return {"sp": sp, "fp": fp, "se": se, "fe": fe, "sf": sf, "ms": ms, "fs": fs, "st": st,
                 "cl_s": clay("cls", self.cl_solid, True), "cl_f": clay("clf", self.cl_fluid, False),
                 "sg_s": sponge("sgs", self.sponge_solid), "sg_f": sponge("sgf", self.sponge_fluid),
+                "ocean": ocean(),
                 "keep": keep}

@@ -65,6 +65,10 @@ class Solver:
             if pt is not None and len(pt):
                 self._check(self.lib.axg_set_sponge(h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
                                                     g.ctypes.data_as(L.P_f64)))
+        pt, mo, th = s["ocean"]
+        if pt is not None and len(pt):
+            self._check(self.lib.axg_set_ocean_load(h, len(pt), pt.ctypes.data_as(L.P_i32),
+                                                    mo.ctypes.data_as(L.P_f64), th.ctypes.data_as(L.P_f64)))
         for cls, team in (team_sizes or {}).items():
             self._check(self.lib.axg_set_team_size(h, int(cls), int(team)))
         self._check(self.lib.axg_finalize(h))

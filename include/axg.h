@@ -256,6 +256,13 @@ int  axg_set_clayton(axg_solver *h, int32_t solid, const axg_clayton *c);
    Domain::applyBC_AfterComputingAccel: accel -= 2 gamma veloc + gamma^2 displ */
 int  axg_set_sponge(axg_solver *h, int32_t solid, int32_t count, const int32_t *point,
                     const double *gamma);
+/* MassOceanLoad1D (point/mass/MassOceanLoad1D.hpp, built in GLLPoint.cpp:66-73) on solid
+   surface points under an ocean:
+   in computeStiffToAccel the point's own mass acts along the surface and mass + mass_ocean
+   across it, the surface normal at polar angle theta; each point at most once, points with
+   1-D masses only (a 3-D ocean load returns AXG_E_UNSUPPORTED) */
+int  axg_set_ocean_load(axg_solver *h, int32_t count, const int32_t *point, const double *mass_ocean,
+                        const double *theta);
 /* builds buckets, uploads to HBM; must precede any time-loop call */
 int  axg_finalize(axg_solver *h);
 

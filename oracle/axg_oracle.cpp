@@ -24,6 +24,7 @@
 #include "../include/axg.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -274,6 +275,9 @@ struct PointSet {
     std::vector<int> nr, nu, off;
     std::vector<int> mass_nr;
     std::vector<std::vector<R>> inv_mass;    // 1 or nr values
+    std::vector<double> mass1;               // 1-D mass (double), for MassOceanLoad1D
+    std::vector<int> ocean;                  // index into ocean_c, -1 = none
+    std::vector<std::array<R, 4>> ocean_c;   // (ss, zz, sz, pp)
     std::vector<uint8_t> axial, surface;
     std::vector<Cx<R>> stiff, displ, veloc, accel;
     size_t total = 0;
@@ -281,7 +285,7 @@ struct PointSet {
                const double *mass, const uint8_t *ax, const uint8_t *surf, int nd) {
         n = count; ndim = nd;
         nr.assign(nr_, nr_ + n); nu.resize(n); off.resize(n);
-        mass_nr.resize(n); inv_mass.resize(n);
+        mass_nr.resize(n); inv_mass.resize(n); mass1.assign(n, 0.0); ocean.assign(n, -1); ocean_c.clear();
         axial.assign(n, 0); surface.assign(n, 0);
         size_t o = 0;
         for (int p = 0; p < n; p++) {
@@ -291,6 +295,7 @@ struct PointSet {
             inv_mass[p].resize(mass_nr[p]);
             // Mass1D / Mass3D store (Real)(1 / mass)  (Mass1D.hpp:19-21, Mass3D.hpp:19-20)
             for (int k = 0; k < mass_nr[p]; k++) inv_mass[p][k] = (R)(1.0 / mass[mo + k]);
+            mass1[p] = mass[mo];
             if (ax) axial[p] = ax[p];
             if (surf) surface[p] = surf[p];
         }
@@ -379,6 +384,7 @@ struct OracleBase {
     virtual void set_stations(const axg_stations *, int) = 0;
     virtual void set_clayton(int solid, const axg_clayton *) = 0;
     virtual void set_sponge(int solid, int n, const int32_t *pt, const double *g) = 0;
+    virtual void set_ocean_load(int n, const int32_t *pt, const double *mo, const double *theta) = 0;
     virtual void apply_sources(int tstep) = 0;
     virtual void compute_stiffness(int nthreads) = 0;
     virtual void bc_before() = 0;
@@ -620,6 +626,18 @@ struct Oracle : OracleBase {
             } else {
                 clf.push_back({c->point[i], (R)(c->area[i] / c->rho_vp[i])});
             }
+        }
+    }
+    // MassOceanLoad1D constructor (coefficients in double, cast); after set_solid_points
+    void set_ocean_load(int n, const int32_t *pt, const double *mo, const double *theta) override {
+        for (int i = 0; i < n; i++) {
+            const int p = pt[i];
+            const double mass = sp.mass1[p], mv = mass + mo[i];
+            const double ct = std::cos(theta[i]), st = std::sin(theta[i]);
+            sp.ocean[p] = (int)sp.ocean_c.size();
+            sp.ocean_c.push_back({(R)(1. / mass * ct * ct + 1. / mv * st * st),
+                                  (R)(1. / mass * st * st + 1. / mv * ct * ct),
+                                  (R)((1. / mv - 1. / mass) * ct * st), (R)(1 / mass)});
         }
     }
     void set_sponge(int solid, int n, const int32_t *pt, const double *g) override {
@@ -1028,7 +1046,16 @@ struct Oracle : OracleBase {
             int nu = ps.nu[p], nr = ps.nr[p];
             if (nr % 2 == 0)
                 for (int c = 0; c < nd; c++) f[(nu - 1) * nd + c].imag(0);
-            if (ps.mass_nr[p] == 1) {
+            if (ps.ocean.size() && ps.ocean[p] >= 0) {
+                // MassOceanLoad1D::computeAccel (MassOceanLoad1D.hpp)
+                const std::array<R, 4> &c = ps.ocean_c[ps.ocean[p]];
+                for (int a = 0; a < nu; a++) {
+                    const Cx<R> s0 = f[a * 3 + 0];
+                    f[a * 3 + 0] = c[0] * s0 + c[2] * f[a * 3 + 2];
+                    f[a * 3 + 2] = c[2] * s0 + c[1] * f[a * 3 + 2];
+                    f[a * 3 + 1] *= c[3];
+                }
+            } else if (ps.mass_nr[p] == 1) {
                 R im = ps.inv_mass[p][0];
                 for (int q = 0; q < nu * nd; q++) f[q] *= im;
             } else {
@@ -1209,6 +1236,7 @@ int axo_set_force_sources(void *h, const axg_force_sources *s) { AXO_TRY(static_
 int axo_set_stations(void *h, const axg_stations *s, int interval) { AXO_TRY(static_cast<OracleBase *>(h)->set_stations(s, interval)) }
 int axo_set_clayton(void *h, int solid, const axg_clayton *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton(solid, c)) }
 int axo_set_sponge(void *h, int solid, int n, const int32_t *pt, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge(solid, n, pt, g)) }
+int axo_set_ocean_load(void *h, int n, const int32_t *pt, const double *mo, const double *theta) { AXO_TRY(static_cast<OracleBase *>(h)->set_ocean_load(n, pt, mo, theta)) }
 int axo_apply_sources(void *h, int tstep) { AXO_TRY(static_cast<OracleBase *>(h)->apply_sources(tstep)) }
 int axo_compute_stiffness(void *h, int nthreads) { AXO_TRY(static_cast<OracleBase *>(h)->compute_stiffness(nthreads)) }
 int axo_bc_before(void *h) { AXO_TRY(static_cast<OracleBase *>(h)->bc_before()) }

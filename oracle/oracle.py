@@ -52,6 +52,7 @@ def lib():
             "axo_apply_sources": (C.c_int, [V, C.c_int]),
             "axo_set_clayton": (C.c_int, [V, C.c_int, C.POINTER(L.axg_clayton)]),
             "axo_set_sponge": (C.c_int, [V, C.c_int, C.c_int, L.P_i32, L.P_f64]),
+            "axo_set_ocean_load": (C.c_int, [V, C.c_int, L.P_i32, L.P_f64, L.P_f64]),
             "axo_compute_stiffness": (C.c_int, [V, C.c_int]),
             "axo_bc_before": (C.c_int, [V]),
             "axo_bc_after": (C.c_int, [V]),
@@ -108,6 +109,10 @@ class Oracle:
             if pt is not None and len(pt):
                 self._chk(self.O.axo_set_sponge(self.h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
                                                 g.ctypes.data_as(L.P_f64)))
+        pt, mo, th = s["ocean"]
+        if pt is not None and len(pt):
+            self._chk(self.O.axo_set_ocean_load(self.h, len(pt), pt.ctypes.data_as(L.P_i32),
+                                                mo.ctypes.data_as(L.P_f64), th.ctypes.data_as(L.P_f64)))
 
     def _chk(self, rc):
         if rc != 0:

@@ -362,3 +362,73 @@ def test_fluid_clayton_and_sponges_parity(built, precision):
         for solid in (True, False):
             assert rel(s.get_field("displ", solid=solid), o.get_field("displ", solid=solid)) <= tol
             assert rel(s.get_field("veloc", solid=solid), o.get_field("veloc", solid=solid)) <= tol
+
+
+def _mass3d_ocean_model():
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=6, nz=6, nr=6,
+                                attenuation=dict(meshgen.default_sls(3), qkappa=57823.0, qmu=100.0))
+    meshgen.add_ocean_load(m, 6, 6, 100e3, tilt=0.3, seed=1)
+    return meshgen.with_mass3d(m, amp=0.05, seed=2, exclude=m.ocean_load[0])
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("fp32", 1e-5), ("mixed", 1e-5)])
+def test_mass3d_and_ocean_load_parity(built, precision, tol):
+    """Mass3D points (per-slice masses: slices -> x 1/M_k -> Fourier, Mass3D.cpp:41-68) and
+    MassOceanLoad1D surface points with tilted normals: five full steps vs the oracle."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = _mass3d_ocean_model()
+    u0 = meshgen.random_displacement(m, seed=8) * 1e-3
+    o = O.Oracle(m, "fp64")
+    o.set_field(u0, "displ")
+    o.run(5)
+    with Solver(m, precision) as s:
+        s.set_field(u0, "displ")
+        s.run(5)
+        for f in ("displ", "veloc", "accel"):
+            assert rel(s.get_field(f), o.get_field(f)) <= tol, (f, rel(s.get_field(f), o.get_field(f)))
+
+
+def test_mass3d_and_ocean_load_hooks_equal_graph(built):
+    """The per-hook path (boundary conditions after assembly, then 1/M, as separate calls)
+    gives the graph's steps on Mass3D and ocean-loaded points (FP64)."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = _mass3d_ocean_model()
+    u0 = meshgen.random_displacement(m, seed=9) * 1e-3
+    out = []
+    for mode in ("graph", "hooks"):
+        with Solver(m, "fp64") as s:
+            s.set_field(u0, "displ")
+            if mode == "hooks":
+                for t in range(4):
+                    s.apply_sources(t)
+                    s.compute_stiffness()
+                    s.apply_bc_before_assembly()
+                    s.record_stations(t)
+                    s.apply_bc_after_assembly()
+                    s.stiff_to_accel()
+                    s.newmark_update()
+            else:
+                s.run(4)
+            out.append((s.get_field("displ"), s.get_field("veloc")))
+    assert rel(out[1][0], out[0][0]) <= 1e-13 and rel(out[1][1], out[0][1]) <= 1e-13
+
+
+def test_ocean_load_errors(built):
+    """Ocean load on a Mass3D point, twice on one point, or out of range: host-side errors."""
+    from axisem3d_b200 import _lib as L, meshgen
+    from axisem3d_b200.solver import Solver, EngineError
+    m = meshgen.cartesian_model(nx=3, nz=3, nr=4)
+    meshgen.add_ocean_load(m, 3, 3, 100e3)
+    bad3d = meshgen.with_mass3d(m, seed=1)          # ocean points get 3-D masses too
+    with pytest.raises(EngineError) as ei:
+        Solver(bad3d, "fp32")
+    assert ei.value.code == L.AXG_E_UNSUPPORTED and "MassOceanLoad3D" in str(ei.value)
+    pt, mo, th = m.ocean_load
+    m.ocean_load = (np.concatenate([pt, pt[:1]]), np.concatenate([mo, mo[:1]]), np.concatenate([th, th[:1]]))
+    with pytest.raises(EngineError) as ei:
+        Solver(m, "fp32")
+    assert ei.value.code == L.AXG_E_ARG and "twice" in str(ei.value)

@@ -266,3 +266,27 @@ def test_absorbing_boundaries_drain_energy():
         late.append(np.linalg.norm(o.get_field("veloc")))
         assert np.isfinite(late[-1])
     assert late[1] < 0.6 * late[0], late
+
+
+def test_ocean_and_mass3d_reduce_to_mass1d():
+    """MassOceanLoad1D with no ocean mass, and Mass3D with the same mass on every slice,
+    act as Mass1D (to rounding): five steps of the oracle in FP64."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    base = meshgen.cartesian_model(nx=5, nz=5, nr=6)
+    u0 = meshgen.random_displacement(base, seed=4) * 1e-3
+
+    def run(m):
+        o = O.Oracle(m, "fp64")
+        o.set_field(u0, "displ")
+        o.run(5)
+        return o.get_field("displ")
+
+    ref = run(base)
+    oc = meshgen.cartesian_model(nx=5, nz=5, nr=6)
+    meshgen.add_ocean_load(oc, 5, 5, 100e3, tilt=0.4, seed=3)
+    oc.ocean_load = (oc.ocean_load[0], np.zeros(len(oc.ocean_load[0])), oc.ocean_load[2])
+    m3 = meshgen.with_mass3d(base, amp=0.0, seed=1)
+    for m in (oc, m3):
+        d = run(m)
+        assert np.linalg.norm(d - ref) <= 1e-13 * np.linalg.norm(ref)
