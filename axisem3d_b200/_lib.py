@@ -88,6 +88,11 @@ class axg_clayton(C.Structure):
                 ("area", P_f64), ("theta", P_f64)]
 
 
+class axg_clayton3d(C.Structure):
+    _fields_ = [("count", C.c_int32), ("point", P_i32), ("offset", P_i64), ("nvalues", C.c_int64),
+                ("rho_vp", P_f64), ("rho_vs", P_f64), ("area", P_f64), ("normal", P_f64)]
+
+
 # name -> (restype, argtypes) of every entry point declared in include/axg.h
 H = C.c_void_p
 SIGNATURES = {
@@ -106,6 +111,8 @@ SIGNATURES = {
     "axg_set_clayton": (C.c_int, [H, C.c_int32, C.POINTER(axg_clayton)]),
     "axg_set_sponge": (C.c_int, [H, C.c_int32, C.c_int32, P_i32, P_f64]),
     "axg_set_ocean_load": (C.c_int, [H, C.c_int32, P_i32, P_f64, P_f64]),
+    "axg_set_clayton3d": (C.c_int, [H, C.c_int32, C.POINTER(axg_clayton3d)]),
+    "axg_set_sponge3d": (C.c_int, [H, C.c_int32, C.c_int32, P_i32, P_i64, C.c_int64, P_f64]),
     "axg_finalize": (C.c_int, [H]),
     "axg_apply_sources": (C.c_int, [H, C.c_int32]),
     "axg_compute_stiffness": (C.c_int, [H]),

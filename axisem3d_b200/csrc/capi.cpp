@@ -302,6 +302,38 @@ int axg_set_sponge(axg_solver *h, int32_t solid, int32_t count, const int32_t *p
     });
 }
 
+int axg_set_clayton3d(axg_solver *h, int32_t solid, const axg_clayton3d *c) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!c || c->count < 0 || c->nvalues < 0 ||
+            (c->count && (!c->point || !c->offset || !c->rho_vp || !c->area ||
+                          (solid && (!c->rho_vs || !c->normal)))))
+            throw axg::Error(AXG_E_ARG, "ClaytonSolid3D || missing array.");
+        axg::HostClayton3D &x = solid ? h->model.cl3_s : h->model.cl3_f;
+        x.count = c->count;
+        x.pt = copy(c->point, c->count);
+        x.off = copy(c->offset, c->count);
+        x.rvp = copy(c->rho_vp, c->nvalues);
+        x.rvs = solid ? copy(c->rho_vs, c->nvalues) : std::vector<double>();
+        x.area = copy(c->area, c->nvalues);
+        x.normal = solid ? copy(c->normal, (size_t)c->nvalues * 3) : std::vector<double>();
+    });
+}
+
+int axg_set_sponge3d(axg_solver *h, int32_t solid, int32_t count, const int32_t *point, const int64_t *offset,
+                     int64_t nvalues, const double *gamma) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (count < 0 || nvalues < 0 || (count && (!point || !offset || !gamma)))
+            throw axg::Error(AXG_E_ARG, "Sponge || missing array.");
+        axg::HostSponge3D &x = solid ? h->model.sg3_s : h->model.sg3_f;
+        x.count = count;
+        x.pt = copy(point, count);
+        x.off = copy(offset, count);
+        x.gamma = copy(gamma, nvalues);
+    });
+}
+
 int axg_set_ocean_load(axg_solver *h, int32_t count, const int32_t *point, const double *mass_ocean,
                        const double *theta) {
     return guarded(h, [&] {
@@ -365,6 +397,34 @@ int axg_finalize(axg_solver *h) {
                     throw axg::Error(AXG_E_UNSUPPORTED, "MassOceanLoad3D || 3-D ocean load is not supported.");
                 if (!(m.ocean.mass_ocean[i] >= 0))
                     throw axg::Error(AXG_E_ARG, "MassOceanLoad1D || negative ocean mass.");
+            }
+        }
+        // 3-D conditions: nr values of the point from each offset
+        for (int solid = 1; solid >= 0; solid--) {
+            const axg::HostPoints &P = solid ? m.sp : m.fp;
+            const axg::HostClayton3D &c = solid ? m.cl3_s : m.cl3_f;
+            for (int i = 0; i < c.count; i++) {
+                const int p = c.pt[i];
+                if (p < 0 || p >= P.count)
+                    throw axg::Error(AXG_E_ARG, "ClaytonSolid3D || point index out of range.");
+                if (c.off[i] < 0 || c.off[i] + P.nr[p] > (int64_t)c.rvp.size())
+                    throw axg::Error(AXG_E_ARG, "ClaytonSolid3D::checkCompatibility || Incompatible sizes.");
+                for (int k = 0; k < P.nr[p]; k++)
+                    if (!(c.rvp[c.off[i] + k] > 0))
+                        throw axg::Error(AXG_E_ARG, "ClaytonFluid3D || rho vp must be positive.");
+            }
+            const axg::HostSponge3D &g = solid ? m.sg3_s : m.sg3_f;
+            const axg::HostSponge &g1 = solid ? m.sg_s : m.sg_f;
+            std::vector<char> seen(P.count, 0);
+            for (int i = 0; i < g1.count; i++)
+                if (g1.pt[i] >= 0 && g1.pt[i] < P.count) seen[g1.pt[i]] = 1;
+            for (int i = 0; i < g.count; i++) {
+                const int p = g.pt[i];
+                if (p < 0 || p >= P.count) throw axg::Error(AXG_E_ARG, "Sponge || point index out of range.");
+                if (seen[p]) throw axg::Error(AXG_E_ARG, "Sponge || point listed twice.");
+                seen[p] = 1;
+                if (g.off[i] < 0 || g.off[i] + P.nr[p] > (int64_t)g.gamma.size())
+                    throw axg::Error(AXG_E_ARG, "Sponge::Sponge || Incompatible sizes.");
             }
         }
         // one Sponge per point (GLLPoint::release averages the boundaries' gammas first)

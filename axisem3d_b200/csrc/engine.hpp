@@ -71,6 +71,20 @@ struct HostClayton {
     std::vector<double> rvp, rvs, area, theta;
 };
 
+struct HostClayton3D {
+    int count = 0;
+    std::vector<int> pt;
+    std::vector<int64_t> off;
+    std::vector<double> rvp, rvs, area, normal;
+};
+
+struct HostSponge3D {
+    int count = 0;
+    std::vector<int> pt;
+    std::vector<int64_t> off;
+    std::vector<double> gamma;
+};
+
 struct HostOcean {
     int count = 0;
     std::vector<int> pt;
@@ -85,6 +99,8 @@ struct HostSponge {
 
 struct HostModel {
     HostClayton cl_s, cl_f;
+    HostClayton3D cl3_s, cl3_f;
+    HostSponge3D sg3_s, sg3_f;
     HostOcean ocean;
     HostSponge sg_s, sg_f;
     HostPoints sp, fp;

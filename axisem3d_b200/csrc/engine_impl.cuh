@@ -101,6 +101,13 @@ class Engine final : public EngineBase {
         DBuf<cx_t<float>> cd, cv;
     };
 
+    // per-slice absorbing-boundary data (3-D Clayton, 3-D sponge) of one point set
+    struct Abc3D {
+        int n = 0;
+        DBuf<int> pt, first;
+        DBuf<int64_t> coff;
+        DBuf<T> c;
+    };
     struct SolidBucket {
         int rheo, att, is3d, rtz, cls, team, tpc, qc, nr_max, n, grid = 1;
         size_t team_bytes;
@@ -164,6 +171,11 @@ public:
                 nrmax = std::max(nrmax, hp->nr[p]);
                 if (hp->mass_nr.size() && hp->mass_nr[p] > 1) nrs.push_back(hp->nr[p]);
             }
+        // and the points of 3-D absorbing boundaries
+        for (int i = 0; i < m.cl3_s.count; i++) nrs.push_back(m.sp.nr[m.cl3_s.pt[i]]);
+        for (int i = 0; i < m.cl3_f.count; i++) nrs.push_back(m.fp.nr[m.cl3_f.pt[i]]);
+        for (int i = 0; i < m.sg3_s.count; i++) nrs.push_back(m.sp.nr[m.sg3_s.pt[i]]);
+        for (int i = 0; i < m.sg3_f.count; i++) nrs.push_back(m.fp.nr[m.sg3_f.pt[i]]);
         std::vector<int> twoff;
         tw_.upload(twiddle_pool<T>(nrs, nrmax, twoff));
         tw_off_.upload(twoff);
@@ -1077,21 +1089,91 @@ private:
         };
         sponge(m.sg_s, sp_.n, sg_s_);
         sponge(m.sg_f, fp_.n, sg_f_);
+        // 3-D Clayton (ClaytonSolid3D / ClaytonFluid3D constructors: in double, cast), grouped
+        // per point in the given order, per-slice coefficients of each condition in a pool
+        auto clay3 = [&](const HostClayton3D &h, const HostPoints &hp, bool solid, Abc3D &out) {
+            out.n = 0;
+            if (!h.count) return;
+            std::vector<int> idx(h.count);
+            for (int i = 0; i < h.count; i++) idx[i] = i;
+            std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return h.pt[x] < h.pt[y]; });
+            std::vector<int> u, first;
+            std::vector<int64_t> coff;
+            std::vector<T> c;
+            for (int k = 0; k < h.count; k++) {
+                const int i = idx[k], p = h.pt[i], nr = hp.nr[p];
+                if (k == 0 || p != h.pt[idx[k - 1]]) { u.push_back(p); first.push_back(k); }
+                coff.push_back((int64_t)c.size());
+                for (int j = 0; j < nr; j++) {
+                    const int64_t q = h.off[i] + j;
+                    if (solid) {
+                        const double rsa = h.rvs[q] * h.area[q];
+                        const double sk = std::sqrt((h.rvp[q] - h.rvs[q]) * h.area[q]);
+                        c.push_back((T)rsa);
+                        for (int d = 0; d < 3; d++) c.push_back((T)(sk * h.normal[q * 3 + d]));
+                    } else {
+                        c.push_back((T)(h.area[q] / h.rvp[q]));
+                    }
+                }
+            }
+            first.push_back(h.count);
+            out.n = (int)u.size();
+            out.pt.upload(u); out.first.upload(first); out.coff.upload(coff); out.c.upload(c);
+        };
+        clay3(m.cl3_s, m.sp, true, cl3_s_);
+        clay3(m.cl3_f, m.fp, false, cl3_f_);
+        auto sponge3 = [&](const HostSponge3D &h, const HostPoints &hp, Abc3D &out) {
+            out.n = h.count;
+            if (!h.count) return;
+            std::vector<int64_t> goff;
+            std::vector<T> g;
+            for (int i = 0; i < h.count; i++) {
+                goff.push_back((int64_t)g.size());
+                for (int j = 0; j < hp.nr[h.pt[i]]; j++) g.push_back((T)h.gamma[h.off[i] + j]);
+            }
+            out.pt.upload(h.pt); out.coff.upload(goff); out.c.upload(g);
+        };
+        sponge3(m.sg3_s, m.sp, sg3_s_);
+        sponge3(m.sg3_f, m.fp, sg3_f_);
     }
 
     void launch_clayton() {
         for (int solid = 1; solid >= 0; solid--) {
-            const int n = solid ? cls_n_ : clf_n_;
-            if (!n) continue;
             PointDev &P = solid ? sp_ : fp_;
-            ClaytonArgs<T, D> a;
-            a.n = n; a.ndim = P.ndim; a.pt = solid ? cls_pt_.p : clf_pt_.p; a.off = P.off.p; a.nu = P.nu.p;
-            a.first = solid ? cls_first_.p : clf_first_.p;
-            a.c = solid ? cls_c_.p : clf_c_.p; a.veloc = P.veloc.p; a.stiff = P.stiff.p;
-            a.nwave = nwave_; a.fstride = (size_t)P.total * P.ndim;
-            clayton_kernel<T, D><<<(n * 32 + 255) / 256, 256, 0, stream_>>>(a);
-            post_launch();
+            const int n = solid ? cls_n_ : clf_n_;
+            if (n) {
+                ClaytonArgs<T, D> a;
+                a.n = n; a.ndim = P.ndim; a.pt = solid ? cls_pt_.p : clf_pt_.p; a.off = P.off.p; a.nu = P.nu.p;
+                a.first = solid ? cls_first_.p : clf_first_.p;
+                a.c = solid ? cls_c_.p : clf_c_.p; a.veloc = P.veloc.p; a.stiff = P.stiff.p;
+                a.nwave = nwave_; a.fstride = (size_t)P.total * P.ndim;
+                clayton_kernel<T, D><<<(n * 32 + 255) / 256, 256, 0, stream_>>>(a);
+                post_launch();
+            }
+            Abc3D &c3 = solid ? cl3_s_ : cl3_f_;
+            if (c3.n) {
+                Clayton3DArgs<T, D> a;
+                a.n = c3.n; a.ndim = P.ndim; a.pt = c3.pt.p; a.first = c3.first.p; a.coff = c3.coff.p;
+                a.c = c3.c.p; a.nr = P.nr.p; a.off = P.off.p; a.tw = tw_.p; a.tw_off = tw_off_.p;
+                a.veloc = P.veloc.p; a.stiff = P.stiff.p; a.nr_max = P.nr_max; a.nwave = nwave_;
+                a.fstride = (size_t)P.total * P.ndim;
+                const int wpb = 4;
+                clayton3d_kernel<T, D><<<(c3.n * nwave_ + wpb - 1) / wpb, 32 * wpb,
+                                         (size_t)wpb * 6 * P.nr_max * sizeof(T), stream_>>>(a);
+                post_launch();
+            }
         }
+    }
+
+    void launch_sponge3d(PointDev &P, Abc3D &g) {
+        Sponge3DArgs<T, D> a;
+        a.n = g.n; a.ndim = P.ndim; a.pt = g.pt.p; a.goff = g.coff.p; a.gamma = g.c.p; a.nr = P.nr.p;
+        a.off = P.off.p; a.tw = tw_.p; a.tw_off = tw_off_.p; a.veloc = P.veloc.p; a.displ = P.displ.p;
+        a.stiff = P.stiff.p; a.nr_max = P.nr_max; a.nwave = nwave_; a.fstride = (size_t)P.total * P.ndim;
+        const int wpb = 4;
+        sponge3d_kernel<T, D><<<(g.n * nwave_ + wpb - 1) / wpb, 32 * wpb, (size_t)wpb * 3 * P.nr_max * sizeof(T),
+                                stream_>>>(a);
+        post_launch();
     }
 
     void build_sources(const HostSources &ms, const HostSources &fs) {
@@ -1332,6 +1414,16 @@ private:
             a.nwave = nwave_;
             a.sponge = solid ? sg_s_.p : sg_f_.p;
             int threads = 256, blocks = (int)(((int64_t)P.total * nwave_ + threads - 1) / threads);
+            Abc3D &g3 = solid ? sg3_s_ : sg3_f_;
+            if (g3.n && (mask & 2)) {
+                // a 3-D sponge acts on the acceleration in slices between 1/M and the update
+                a.mask = mask & 3;
+                point_update_kernel<T, D, COMP><<<blocks, threads, 0, stream_>>>(a);
+                post_launch();
+                launch_sponge3d(P, g3);
+                if (!(mask & 4)) continue;
+                a.mask = 4;
+            }
             point_update_kernel<T, D, COMP><<<blocks, threads, 0, stream_>>>(a);
             post_launch();
         }
@@ -1412,6 +1504,7 @@ private:
     int nwave_ = 1;
     int64_t state_wave_ = 0;
     int cls_n_ = 0, clf_n_ = 0;
+    Abc3D cl3_s_, cl3_f_, sg3_s_, sg3_f_;
     int ocean_n_ = 0;
     DBuf<int> ocean_pt_;
     DBuf<T> ocean_c_;

@@ -224,6 +224,142 @@ __global__ void mass3d_kernel(const Mass3DArgs<T> a) {
 // MIXED (T = float, D = double): increments formed in double, optionally
 // accumulated with compensated (Kahan) summation; a float copy of d feeds the
 // elements.
+// ------------------------------------------------- 3-D absorbing boundaries ---
+// Warp-level computeC2R / computeR2C of one component of one point (SolverFFTW.hpp:101-172
+// conventions: c2r doubles every mode above 0 and ignores the imaginary parts of the DC and
+// Nyquist terms; r2c scales by 1/nr and halves the Nyquist term), lanes over slices / modes.
+template <class T, class V>
+__device__ __forceinline__ void warp_c2r(const V *f, int stride, int nu, int nr, const T *twc, const T *tws,
+                                         T *r, int lane) {
+    for (int k = lane; k < nr; k += 32) {
+        T acc = (T)f[0].x;
+        int j = 0;
+        for (int al = 1; al < nu; al++) {
+            j += k;
+            j = j >= nr ? j - nr : j;
+            const V v = f[(size_t)al * stride];
+            acc += (T)2 * ((T)v.x * twc[j] - (T)v.y * tws[j]);
+        }
+        r[k] = acc;
+    }
+}
+template <class T>
+__device__ __forceinline__ cx_t<T> r2c_mode(const T *r, int nr, int al, const T *twc, const T *tws) {
+    const T inv_nr = (T)1 / (T)nr;
+    T re = 0, im = 0;
+    int j = 0;
+    const int step = al % nr;
+    for (int k = 0; k < nr; k++) {
+        const T x = r[k] * inv_nr;
+        re += x * twc[j];
+        im -= x * tws[j];
+        j += step;
+        j = j >= nr ? j - nr : j;
+    }
+    if (al == 0) im = 0;
+    if ((nr & 1) == 0 && al == nr / 2) { re *= (T)0.5; im = 0; }
+    return mk<T>(re, im);
+}
+
+// ClaytonSolid3D::apply (ABC/ClaytonSolid3D.cpp): a = rsa v + (v . k) k in slices,
+// stiff -= R2C(a); ClaytonFluid3D::apply (ABC/ClaytonFluid3D.cpp): a = (area / rho vp) v.
+// One warp per point; its conditions (one per boundary) in the order given.
+template <class T, class D>
+struct Clayton3DArgs {
+    int n, ndim;                 // distinct points
+    const int *pt, *first;       // conditions of point i: first[i] .. first[i+1]-1
+    const int64_t *coff;         // per condition: offset of its per-slice coefficients
+    const T *c;                  // solid: [nr][4] (rsa, k_s, k_phi, k_z); fluid: [nr]
+    const int *nr, *off;
+    const T *tw; const int *tw_off;
+    const cx_t<D> *veloc;
+    cx_t<T> *stiff;
+    int nr_max, nwave;
+    size_t fstride;
+};
+
+template <class T, class D>
+__global__ void clayton3d_kernel(const Clayton3DArgs<T, D> a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int w = threadIdx.x / 32, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * (blockDim.x / 32) + w;
+    if (item >= a.n * a.nwave) return;
+    const int i = item % a.n, wf = item / a.n;
+    const int p = a.pt[i], nr = a.nr[p], nu = nr / 2 + 1, nd = a.ndim;
+    T *vr = reinterpret_cast<T *>(sm) + (size_t)w * 2 * 3 * a.nr_max;   // [nd][nr_max] velocity slices
+    T *ar = vr + (size_t)3 * a.nr_max;                                  // [nd][nr_max] result slices
+    const T *twc = a.tw + a.tw_off[nr], *tws = twc + nr;
+    const cx_t<D> *v = a.veloc + (size_t)wf * a.fstride + (size_t)a.off[p] * nd;
+    cx_t<T> *f = a.stiff + (size_t)wf * a.fstride + (size_t)a.off[p] * nd;
+    for (int c = 0; c < nd; c++) warp_c2r<T, cx_t<D>>(v + c, nd, nu, nr, twc, tws, vr + (size_t)c * a.nr_max, lane);
+    __syncwarp();
+    for (int q = a.first[i]; q < a.first[i + 1]; q++) {
+        const T *cf = a.c + a.coff[q];
+        for (int k = lane; k < nr; k += 32) {
+            if (nd == 3) {
+                const T v0 = vr[k], v1 = vr[a.nr_max + k], v2 = vr[2 * a.nr_max + k];
+                const T rsa = cf[4 * k], k0 = cf[4 * k + 1], k1 = cf[4 * k + 2], k2 = cf[4 * k + 3];
+                const T dot = v0 * k0 + v1 * k1 + v2 * k2;
+                ar[k] = rsa * v0 + dot * k0;
+                ar[a.nr_max + k] = rsa * v1 + dot * k1;
+                ar[2 * a.nr_max + k] = rsa * v2 + dot * k2;
+            } else {
+                ar[k] = vr[k] * cf[k];
+            }
+        }
+        __syncwarp();
+        for (int al = lane; al < nu; al += 32)
+            for (int c = 0; c < nd; c++) {
+                const cx_t<T> x = r2c_mode<T>(ar + (size_t)c * a.nr_max, nr, al, twc, tws);
+                f[(size_t)al * nd + c] = csub(f[(size_t)al * nd + c], x);
+            }
+        __syncwarp();
+    }
+}
+
+// Sponge::apply, 3-D branch (ABC/Sponge.hpp:74-98): in slices, accel -= 2 gamma veloc +
+// gamma^2 displ, then back to Fourier; after the mass term. One warp per point.
+template <class T, class D>
+struct Sponge3DArgs {
+    int n, ndim;
+    const int *pt;
+    const int64_t *goff;         // per point: offset of its nr gammas
+    const T *gamma;
+    const int *nr, *off;
+    const T *tw; const int *tw_off;
+    const cx_t<D> *veloc, *displ;
+    cx_t<T> *stiff;
+    int nr_max, nwave;
+    size_t fstride;
+};
+
+template <class T, class D>
+__global__ void sponge3d_kernel(const Sponge3DArgs<T, D> a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int w = threadIdx.x / 32, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * (blockDim.x / 32) + w;
+    if (item >= a.n * a.nwave) return;
+    const int i = item % a.n, wf = item / a.n;
+    const int p = a.pt[i], nr = a.nr[p], nu = nr / 2 + 1, nd = a.ndim;
+    T *sr = reinterpret_cast<T *>(sm) + (size_t)w * 3 * a.nr_max;      // stiff, veloc, displ slices
+    T *vr = sr + a.nr_max, *ur = vr + a.nr_max;
+    const T *twc = a.tw + a.tw_off[nr], *tws = twc + nr;
+    const T *g = a.gamma + a.goff[i];
+    const size_t o = (size_t)wf * a.fstride + (size_t)a.off[p] * nd;
+    cx_t<T> *f = a.stiff + o;
+    const T two = 2;
+    for (int c = 0; c < nd; c++) {
+        warp_c2r<T, cx_t<T>>(f + c, nd, nu, nr, twc, tws, sr, lane);
+        warp_c2r<T, cx_t<D>>(a.veloc + o + c, nd, nu, nr, twc, tws, vr, lane);
+        warp_c2r<T, cx_t<D>>(a.displ + o + c, nd, nu, nr, twc, tws, ur, lane);
+        __syncwarp();
+        for (int k = lane; k < nr; k += 32) sr[k] -= (two * g[k]) * vr[k] + (g[k] * g[k]) * ur[k];
+        __syncwarp();
+        for (int al = lane; al < nu; al += 32) f[(size_t)al * nd + c] = r2c_mode<T>(sr, nr, al, twc, tws);
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------- ocean load ---
 // MassOceanLoad1D::computeAccel (point/mass/MassOceanLoad1D.hpp): the point's own mass acts
 // along the surface, mass + ocean mass across it; one warp per point, lanes over modes,

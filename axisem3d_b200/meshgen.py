@@ -412,6 +412,48 @@ def add_ocean_load(m, nx, nz, width, rho_water=1020.0, depth_water=3000.0, tilt=
     return m
 
 
+def add_absorbing3d(m, rho=3300.0, vp=8000.0, vs=4500.0, pert=0.05, sponge_width=0.02, seed=0):
+    """3-D absorbing boundaries on the outer surface of a spherical shell (points at the
+    largest radius): ClaytonSolid3D conditions with rho vp and rho vs varying by +-pert over
+    the nr slices of each point and a radial normal tilted towards phi by a small seeded
+    angle per slice; and 3-D sponges (nr gammas, seeded variation over the slices) on the
+    points within sponge_width of the outer radius. Synthetic: for parity of the 3-D
+    boundary terms, not a calibrated absorbing layer."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    r = np.hypot(m.sp_coords[:, 0], m.sp_coords[:, 1])
+    rmax = r.max()
+    surf = np.nonzero(r > rmax * (1 - 1e-9))[0].astype(np.int32)
+    nr = np.asarray(m.sp_nr)
+    off, rvp, rvs, area, nrm = [], [], [], [], []
+    o = 0
+    for p in surf:
+        n = int(nr[p])
+        off.append(o)
+        o += n
+        k = np.arange(n)
+        wobble = 1.0 + pert * np.sin(2 * np.pi * k / n + rng.uniform(0, 2 * np.pi))
+        rvp.append(rho * vp * wobble)
+        rvs.append(rho * vs * wobble)
+        area.append(np.full(n, 1e6 * (1.0 + m.sp_coords[p, 0] / rmax)))
+        th = math.atan2(m.sp_coords[p, 0], m.sp_coords[p, 1])
+        tilt = rng.uniform(-0.1, 0.1, n)
+        v = np.stack([np.sin(th) * np.cos(tilt), np.sin(tilt), np.cos(th) * np.cos(tilt)], axis=1)
+        nrm.append(v / np.linalg.norm(v, axis=1, keepdims=True))
+    m.cl3_solid = {"point": surf, "offset": np.array(off, np.int64), "rho_vp": np.concatenate(rvp),
+                   "rho_vs": np.concatenate(rvs), "area": np.concatenate(area), "normal": np.concatenate(nrm)}
+    near = np.nonzero(r > rmax * (1 - sponge_width))[0].astype(np.int32)
+    goff, g = [], []
+    o = 0
+    for p in near:
+        n = int(nr[p])
+        goff.append(o)
+        o += n
+        x = (r[p] - rmax * (1 - sponge_width)) / (rmax * sponge_width)
+        g.append(0.05 * x * (1.0 + 0.2 * rng.uniform(-1, 1, n)))
+    m.sponge3d_solid = (near, np.array(goff, np.int64), np.concatenate(g))
+    return m
+
+
 def with_mass3d(m, amp=0.05, seed=0, exclude=()):
     """A copy of `m` whose solid points with nr >= 2 (except `exclude`) carry 3-D masses
     (Mass3D): the point's mass times (1 + amp * U(-1, 1)) per slice, seeded."""

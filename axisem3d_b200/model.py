@@ -119,6 +119,12 @@ class Model:
     sponge_fluid: Optional[tuple] = None
     # MassOceanLoad1D on solid surface points: (points, ocean mass, normal polar angle)
     ocean_load: Optional[tuple] = None
+    # 3-D absorbing boundaries: Clayton dicts with point, offset and per-slice rho_vp,
+    # rho_vs, area, normal [n][3] (solid); sponges as (points, offsets, per-slice gamma)
+    cl3_solid: Optional[dict] = None
+    cl3_fluid: Optional[dict] = None
+    sponge3d_solid: Optional[tuple] = None
+    sponge3d_fluid: Optional[tuple] = None
     meta: dict = field(default_factory=dict)
     meta_rho: Optional[np.ndarray] = None          # (ne, 25) density at element points (generators)
 
@@ -270,6 +276,29 @@ class Model:
                 c.theta = k(name + "_th", d["theta"], _f64, C.c_double)
             return c
 
+        def clay3(name, d, solid):
+            c = L.axg_clayton3d()
+            if not d:
+                c.count = 0
+                return c
+            c.count = len(d["point"])
+            c.point = k(name + "_pt", d["point"], _i32, C.c_int32)
+            c.offset = k(name + "_off", d["offset"], _i64, C.c_int64)
+            c.nvalues = len(d["rho_vp"])
+            c.rho_vp = k(name + "_rvp", d["rho_vp"], _f64, C.c_double)
+            c.area = k(name + "_area", d["area"], _f64, C.c_double)
+            if solid:
+                c.rho_vs = k(name + "_rvs", d["rho_vs"], _f64, C.c_double)
+                c.normal = k(name + "_nrm", np.asarray(d["normal"]).ravel(), _f64, C.c_double)
+            return c
+
+        def sponge3(name, t):
+            if not t:
+                return (None, None, None)
+            pt, off, g = _i32(t[0]), _i64(t[1]), _f64(t[2])
+            keep[name + "_pt"], keep[name + "_off"], keep[name + "_g"] = pt, off, g
+            return (pt, off, g)
+
         def ocean():
             if not self.ocean_load:
                 return (None, None, None)
@@ -288,4 +317,6 @@ class Model:
                 "cl_s": clay("cls", self.cl_solid, True), "cl_f": clay("clf", self.cl_fluid, False),
                 "sg_s": sponge("sgs", self.sponge_solid), "sg_f": sponge("sgf", self.sponge_fluid),
                 "ocean": ocean(),
+                "cl3_s": clay3("c3s", self.cl3_solid, True), "cl3_f": clay3("c3f", self.cl3_fluid, False),
+                "sg3_s": sponge3("g3s", self.sponge3d_solid), "sg3_f": sponge3("g3f", self.sponge3d_fluid),
                 "keep": keep}

@@ -65,6 +65,14 @@ class Solver:
             if pt is not None and len(pt):
                 self._check(self.lib.axg_set_sponge(h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
                                                     g.ctypes.data_as(L.P_f64)))
+        for solid, key in ((1, "cl3_s"), (0, "cl3_f")):
+            if s[key].count:
+                self._check(self.lib.axg_set_clayton3d(h, solid, C.byref(s[key])))
+        for solid, (pt, off, g) in ((1, s["sg3_s"]), (0, s["sg3_f"])):
+            if pt is not None and len(pt):
+                self._check(self.lib.axg_set_sponge3d(h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
+                                                      off.ctypes.data_as(L.P_i64), len(g),
+                                                      g.ctypes.data_as(L.P_f64)))
         pt, mo, th = s["ocean"]
         if pt is not None and len(pt):
             self._check(self.lib.axg_set_ocean_load(h, len(pt), pt.ctypes.data_as(L.P_i32),

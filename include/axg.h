@@ -231,6 +231,20 @@ typedef struct axg_clayton {
     const double  *theta;         /* polar angle of the normal (solid only)            */
 } axg_clayton;
 
+/* 3-D Clayton-Engquist conditions (ClaytonSolid3D / ClaytonFluid3D, built in GLLPoint.cpp:148-190
+   when the point's properties or normal vary with phi): per condition nr values (nr of its point)
+   from offset[i] in every per-slice array */
+typedef struct axg_clayton3d {
+    int32_t        count;
+    const int32_t *point;
+    const int64_t *offset;        /* first per-slice value of condition i                 */
+    int64_t        nvalues;       /* length of rho_vp / rho_vs / area (normal: 3x)         */
+    const double  *rho_vp;
+    const double  *rho_vs;        /* solid only                                           */
+    const double  *area;          /* length of the boundary normal per slice              */
+    const double  *normal;        /* solid only: unit normal (s, phi, z) per slice, [nvalues][3] */
+} axg_clayton3d;
+
 typedef struct axg_solver axg_solver;
 
 /* ---- lifetime ---- */
@@ -256,6 +270,14 @@ int  axg_set_clayton(axg_solver *h, int32_t solid, const axg_clayton *c);
    Domain::applyBC_AfterComputingAccel: accel -= 2 gamma veloc + gamma^2 displ */
 int  axg_set_sponge(axg_solver *h, int32_t solid, int32_t count, const int32_t *point,
                     const double *gamma);
+/* 3-D Clayton conditions: applied after the 1-D ones of axg_set_clayton, in the order
+   listed per point (stiff -= R2C(C(C2R(veloc))) per condition) */
+int  axg_set_clayton3d(axg_solver *h, int32_t solid, const axg_clayton3d *c);
+/* 3-D Kosloff sponge (Sponge.hpp, nr gammas per point, the 3-D constructor): on the
+   acceleration in slices, accel -= 2 gamma veloc + gamma^2 displ; gamma[offset[i] ..
+   offset[i] + nr - 1] for point[i]; a point carries a 1-D or a 3-D sponge, not both */
+int  axg_set_sponge3d(axg_solver *h, int32_t solid, int32_t count, const int32_t *point,
+                      const int64_t *offset, int64_t nvalues, const double *gamma);
 /* MassOceanLoad1D (point/mass/MassOceanLoad1D.hpp, built in GLLPoint.cpp:66-73) on solid
    surface points under an ocean:
    in computeStiffToAccel the point's own mass acts along the surface and mass + mass_ocean

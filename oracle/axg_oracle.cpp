@@ -385,6 +385,8 @@ struct OracleBase {
     virtual void set_clayton(int solid, const axg_clayton *) = 0;
     virtual void set_sponge(int solid, int n, const int32_t *pt, const double *g) = 0;
     virtual void set_ocean_load(int n, const int32_t *pt, const double *mo, const double *theta) = 0;
+    virtual void set_clayton3d(int solid, const axg_clayton3d *c) = 0;
+    virtual void set_sponge3d(int solid, int n, const int32_t *pt, const int64_t *off, const double *g) = 0;
     virtual void apply_sources(int tstep) = 0;
     virtual void compute_stiffness(int nthreads) = 0;
     virtual void bc_before() = 0;
@@ -425,6 +427,11 @@ struct Oracle : OracleBase {
     std::vector<ClaytonS> cls;
     std::vector<ClaytonF> clf;
     std::vector<std::pair<int, R>> sgs, sgf;
+    // 3-D Clayton (per slice: rsa, k_s, k_phi, k_z for solid points; area / rho vp for fluid)
+    struct Clayton3 { int p; std::vector<R> c; };
+    std::vector<Clayton3> cl3s, cl3f;
+    struct Sponge3 { int p; std::vector<R> g; };
+    std::vector<Sponge3> sg3s, sg3f;
 
     explicit Oracle(const axg_config *c) : cfg(*c) {
         for (int i = 0; i < P; i++)
@@ -626,6 +633,36 @@ struct Oracle : OracleBase {
             } else {
                 clf.push_back({c->point[i], (R)(c->area[i] / c->rho_vp[i])});
             }
+        }
+    }
+    // ClaytonSolid3D / ClaytonFluid3D constructors (in double, cast); after the points
+    void set_clayton3d(int solid, const axg_clayton3d *c) override {
+        for (int i = 0; i < c->count; i++) {
+            const int p = c->point[i];
+            const int nr = solid ? sp.nr[p] : fp.nr[p];
+            Clayton3 x{p, {}};
+            for (int k = 0; k < nr; k++) {
+                const int64_t q = c->offset[i] + k;
+                if (solid) {
+                    const double sk = std::sqrt((c->rho_vp[q] - c->rho_vs[q]) * c->area[q]);
+                    x.c.push_back((R)(c->rho_vs[q] * c->area[q]));
+                    for (int d = 0; d < 3; d++) x.c.push_back((R)(sk * c->normal[q * 3 + d]));
+                } else {
+                    x.c.push_back((R)(c->area[q] / c->rho_vp[q]));
+                }
+            }
+            prepare_twiddle(nr);
+            (solid ? cl3s : cl3f).push_back(std::move(x));
+        }
+    }
+    // Sponge 3-D constructor: gamma cast to Real
+    void set_sponge3d(int solid, int n, const int32_t *pt, const int64_t *off, const double *g) override {
+        for (int i = 0; i < n; i++) {
+            const int nr = solid ? sp.nr[pt[i]] : fp.nr[pt[i]];
+            Sponge3 x{pt[i], {}};
+            for (int k = 0; k < nr; k++) x.g.push_back((R)g[off[i] + k]);
+            prepare_twiddle(nr);
+            (solid ? sg3s : sg3f).push_back(std::move(x));
         }
     }
     // MassOceanLoad1D constructor (coefficients in double, cast); after set_solid_points
@@ -996,6 +1033,39 @@ struct Oracle : OracleBase {
         for (auto &c : clf)
             for (int a = 0; a < fp.nu[c.p]; a++)
                 fp.stiff[(size_t)fp.off[c.p] + a] -= fp.veloc[(size_t)fp.off[c.p] + a] * c.c;
+        // ClaytonSolid3D::apply / ClaytonFluid3D::apply (ABC/ClaytonSolid3D.cpp, ClaytonFluid3D.cpp)
+        for (int solid = 1; solid >= 0; solid--) {
+            PointSet<R> &ps = solid ? sp : fp;
+            const int nd = ps.ndim;
+            for (auto &c : (solid ? cl3s : cl3f)) {
+                const int nr = ps.nr[c.p], nu = ps.nu[c.p];
+                const Twiddle<R> &t = twiddle(nr);
+                Cx<R> *f = &ps.stiff[(size_t)ps.off[c.p] * nd];
+                const Cx<R> *v = &ps.veloc[(size_t)ps.off[c.p] * nd];
+                std::vector<Cx<R>> cb(nu);
+                std::vector<R> vr((size_t)nd * nr), ar((size_t)nd * nr);
+                for (int d = 0; d < nd; d++) {
+                    for (int a = 0; a < nu; a++) cb[a] = v[a * nd + d];
+                    c2r(cb.data(), nu, &vr[(size_t)d * nr], nr, t);
+                }
+                for (int k = 0; k < nr; k++) {
+                    if (nd == 3) {
+                        const R *q = &c.c[(size_t)4 * k];
+                        const R v0 = vr[k], v1 = vr[nr + k], v2 = vr[2 * nr + k];
+                        const R dot = v0 * q[1] + v1 * q[2] + v2 * q[3];
+                        ar[k] = q[0] * v0 + dot * q[1];
+                        ar[nr + k] = q[0] * v1 + dot * q[2];
+                        ar[2 * nr + k] = q[0] * v2 + dot * q[3];
+                    } else {
+                        ar[k] = vr[k] * c.c[k];
+                    }
+                }
+                for (int d = 0; d < nd; d++) {
+                    r2c(&ar[(size_t)d * nr], nr, cb.data(), nu, t);
+                    for (int a = 0; a < nu; a++) f[a * nd + d] -= cb[a];
+                }
+            }
+        }
         for (auto &c : sf) {
             int nus = sp.nu[c.s], nuf = fp.nu[c.f];
             int nu = std::min(nus, nuf);
@@ -1088,6 +1158,29 @@ struct Oracle : OracleBase {
             size_t o = (size_t)fp.off[g.first];
             for (int q = 0; q < fp.nu[g.first]; q++)
                 fp.stiff[o + q] -= (two * g.second) * fp.veloc[o + q] + (g.second * g.second) * fp.displ[o + q];
+        }
+        // Sponge::apply, 3-D branch (ABC/Sponge.hpp:74-98)
+        for (int solid = 1; solid >= 0; solid--) {
+            PointSet<R> &ps = solid ? sp : fp;
+            const int nd = ps.ndim;
+            for (auto &g : (solid ? sg3s : sg3f)) {
+                const int nr = ps.nr[g.p], nu = ps.nu[g.p];
+                const Twiddle<R> &t = twiddle(nr);
+                const size_t o = (size_t)ps.off[g.p] * nd;
+                std::vector<Cx<R>> cb(nu);
+                std::vector<R> sr(nr), vr(nr), ur(nr);
+                for (int d = 0; d < nd; d++) {
+                    for (int a = 0; a < nu; a++) cb[a] = ps.stiff[o + a * nd + d];
+                    c2r(cb.data(), nu, sr.data(), nr, t);
+                    for (int a = 0; a < nu; a++) cb[a] = ps.veloc[o + a * nd + d];
+                    c2r(cb.data(), nu, vr.data(), nr, t);
+                    for (int a = 0; a < nu; a++) cb[a] = ps.displ[o + a * nd + d];
+                    c2r(cb.data(), nu, ur.data(), nr, t);
+                    for (int k = 0; k < nr; k++) sr[k] -= (two * g.g[k]) * vr[k] + (g.g[k] * g.g[k]) * ur[k];
+                    r2c(sr.data(), nr, cb.data(), nu, t);
+                    for (int a = 0; a < nu; a++) ps.stiff[o + a * nd + d] = cb[a];
+                }
+            }
         }
     }
 
@@ -1237,6 +1330,8 @@ int axo_set_stations(void *h, const axg_stations *s, int interval) { AXO_TRY(sta
 int axo_set_clayton(void *h, int solid, const axg_clayton *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton(solid, c)) }
 int axo_set_sponge(void *h, int solid, int n, const int32_t *pt, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge(solid, n, pt, g)) }
 int axo_set_ocean_load(void *h, int n, const int32_t *pt, const double *mo, const double *theta) { AXO_TRY(static_cast<OracleBase *>(h)->set_ocean_load(n, pt, mo, theta)) }
+int axo_set_clayton3d(void *h, int solid, const axg_clayton3d *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton3d(solid, c)) }
+int axo_set_sponge3d(void *h, int solid, int n, const int32_t *pt, const int64_t *off, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge3d(solid, n, pt, off, g)) }
 int axo_apply_sources(void *h, int tstep) { AXO_TRY(static_cast<OracleBase *>(h)->apply_sources(tstep)) }
 int axo_compute_stiffness(void *h, int nthreads) { AXO_TRY(static_cast<OracleBase *>(h)->compute_stiffness(nthreads)) }
 int axo_bc_before(void *h) { AXO_TRY(static_cast<OracleBase *>(h)->bc_before()) }

@@ -53,6 +53,8 @@ def lib():
             "axo_set_clayton": (C.c_int, [V, C.c_int, C.POINTER(L.axg_clayton)]),
             "axo_set_sponge": (C.c_int, [V, C.c_int, C.c_int, L.P_i32, L.P_f64]),
             "axo_set_ocean_load": (C.c_int, [V, C.c_int, L.P_i32, L.P_f64, L.P_f64]),
+            "axo_set_clayton3d": (C.c_int, [V, C.c_int, C.POINTER(L.axg_clayton3d)]),
+            "axo_set_sponge3d": (C.c_int, [V, C.c_int, C.c_int, L.P_i32, L.P_i64, L.P_f64]),
             "axo_compute_stiffness": (C.c_int, [V, C.c_int]),
             "axo_bc_before": (C.c_int, [V]),
             "axo_bc_after": (C.c_int, [V]),
@@ -109,6 +111,13 @@ class Oracle:
             if pt is not None and len(pt):
                 self._chk(self.O.axo_set_sponge(self.h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
                                                 g.ctypes.data_as(L.P_f64)))
+        for solid, key in ((1, "cl3_s"), (0, "cl3_f")):
+            if s[key].count:
+                self._chk(self.O.axo_set_clayton3d(self.h, solid, C.byref(s[key])))
+        for solid, (pt, off, g) in ((1, s["sg3_s"]), (0, s["sg3_f"])):
+            if pt is not None and len(pt):
+                self._chk(self.O.axo_set_sponge3d(self.h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
+                                                  off.ctypes.data_as(L.P_i64), g.ctypes.data_as(L.P_f64)))
         pt, mo, th = s["ocean"]
         if pt is not None and len(pt):
             self._chk(self.O.axo_set_ocean_load(self.h, len(pt), pt.ctypes.data_as(L.P_i32),

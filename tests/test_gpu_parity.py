@@ -432,3 +432,86 @@ def test_ocean_load_errors(built):
     with pytest.raises(EngineError) as ei:
         Solver(m, "fp32")
     assert ei.value.code == L.AXG_E_ARG and "twice" in str(ei.value)
+
+
+def _abc3d_model():
+    from axisem3d_b200 import meshgen
+    m = meshgen.spherical_model(n_theta=16, n_solid_layers=4, n_fluid_layers=2, nr_max=24, three_d=True)
+    meshgen.add_absorbing3d(m, seed=3)
+    # ClaytonFluid3D on a seeded subset of fluid points (synthetic values: parity only)
+    rng = np.random.default_rng(11)
+    fpt = np.sort(rng.choice(len(m.fp_nr), size=len(m.fp_nr) // 5, replace=False)).astype(np.int32)
+    nr = np.asarray(m.fp_nr)[fpt]
+    off = np.concatenate([[0], np.cumsum(nr)[:-1]]).astype(np.int64)
+    tot = int(nr.sum())
+    mass = np.asarray(m.fp_mass)[np.repeat(fpt, nr)]
+    m.cl3_fluid = {"point": fpt, "offset": off, "rho_vp": np.full(tot, 1.0e7),
+                   "area": 0.05 * mass * 1.0e7 / m.dt * rng.uniform(0.5, 1.5, tot)}
+    return m
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("fp32", 1e-5), ("mixed", 1e-5)])
+def test_absorbing3d_parity(built, precision, tol):
+    """ClaytonSolid3D (per-slice impedances, tilted normals) on the outer surface of a 3-D
+    shell, ClaytonFluid3D on fluid points and 3-D sponges (nr gammas per point): five full
+    steps vs the oracle."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = _abc3d_model()
+    us = meshgen.random_displacement(m, seed=3) * 1e-9
+    uf = meshgen.random_displacement(m, seed=4, solid=False) * 1e-9
+    o = O.Oracle(m, "fp64")
+    for which in ("displ", "veloc"):
+        o.set_field(us, which)
+        o.set_field(uf, which, solid=False)
+    o.run(5)
+    with Solver(m, precision) as s:
+        for which in ("displ", "veloc"):
+            s.set_field(us, which)
+            s.set_field(uf, which, solid=False)
+        s.run(5)
+        for solid in (True, False):
+            for f in ("displ", "veloc"):
+                got, ref = s.get_field(f, solid=solid), o.get_field(f, solid=solid)
+                assert rel(got, ref) <= tol, (solid, f, rel(got, ref))
+
+
+def test_absorbing3d_hooks_equal_graph_and_errors(built):
+    """The per-hook path equals the graph with 3-D boundaries (FP64); a point with a 1-D and
+    a 3-D sponge, and per-slice arrays too short for a point's nr, are host-side errors."""
+    from axisem3d_b200 import _lib as L, meshgen
+    from axisem3d_b200.solver import Solver, EngineError
+    m = _abc3d_model()
+    us = meshgen.random_displacement(m, seed=5) * 1e-9
+    out = []
+    for mode in ("graph", "hooks"):
+        with Solver(m, "fp64") as s:
+            s.set_field(us, "displ")
+            s.set_field(us, "veloc")
+            if mode == "hooks":
+                for t in range(4):
+                    s.apply_sources(t)
+                    s.compute_stiffness()
+                    s.apply_bc_before_assembly()
+                    s.record_stations(t)
+                    s.apply_bc_after_assembly()
+                    s.stiff_to_accel()
+                    s.newmark_update()
+            else:
+                s.run(4)
+            out.append((s.get_field("displ"), s.get_field("veloc")))
+    assert rel(out[1][0], out[0][0]) <= 1e-13 and rel(out[1][1], out[0][1]) <= 1e-13
+    both = _abc3d_model()
+    p0 = both.sponge3d_solid[0][:1]
+    both.sponge_solid = (p0, np.array([0.01]))
+    with pytest.raises(EngineError) as ei:
+        Solver(both, "fp32")
+    assert ei.value.code == L.AXG_E_ARG and "twice" in str(ei.value)
+    short = _abc3d_model()
+    c = dict(short.cl3_solid)
+    c["offset"] = c["offset"] + 1
+    short.cl3_solid = c
+    with pytest.raises(EngineError) as ei:
+        Solver(short, "fp32")
+    assert ei.value.code == L.AXG_E_ARG and "Incompatible sizes" in str(ei.value)
