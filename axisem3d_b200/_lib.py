@@ -93,6 +93,14 @@ class axg_clayton3d(C.Structure):
                 ("rho_vp", P_f64), ("rho_vs", P_f64), ("area", P_f64), ("normal", P_f64)]
 
 
+class axg_scanning(C.Structure):
+    _fields_ = [("tol_fourier_h1", C.c_double), ("rel_tol_h1", C.c_double), ("abs_tol_h1", C.c_double),
+                ("max_num_peaks", C.c_int32), ("interval", C.c_int32), ("n_solid", C.c_int32),
+                ("solid_points", P_i32), ("n_fluid", C.c_int32), ("fluid_points", P_i32)]
+
+
+AXG_SCAN_MAX_PEAKS = 32
+
 # name -> (restype, argtypes) of every entry point declared in include/axg.h
 H = C.c_void_p
 SIGNATURES = {
@@ -112,6 +120,8 @@ SIGNATURES = {
     "axg_set_sponge": (C.c_int, [H, C.c_int32, C.c_int32, P_i32, P_f64]),
     "axg_set_ocean_load": (C.c_int, [H, C.c_int32, P_i32, P_f64, P_f64]),
     "axg_set_clayton3d": (C.c_int, [H, C.c_int32, C.POINTER(axg_clayton3d)]),
+    "axg_set_scanning": (C.c_int, [H, C.POINTER(axg_scanning)]),
+    "axg_scanning_nr": (C.c_int, [H, P_i32, P_i32]),
     "axg_set_sponge3d": (C.c_int, [H, C.c_int32, C.c_int32, P_i32, P_i64, C.c_int64, P_f64]),
     "axg_finalize": (C.c_int, [H]),
     "axg_apply_sources": (C.c_int, [H, C.c_int32]),

@@ -334,6 +334,32 @@ int axg_set_sponge3d(axg_solver *h, int32_t solid, int32_t count, const int32_t 
     });
 }
 
+int axg_set_scanning(axg_solver *h, const axg_scanning *sc) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!sc) throw axg::Error(AXG_E_ARG, "WavefieldScanning || missing parameters.");
+        if (sc->interval < 1 || sc->max_num_peaks < 1 || !(sc->tol_fourier_h1 > 0) || !(sc->rel_tol_h1 >= 0) ||
+            !(sc->abs_tol_h1 >= 0))
+            throw axg::Error(AXG_E_ARG, "WavefieldScanning || invalid parameters.");
+        if ((sc->n_solid > 0 && !sc->solid_points) || (sc->n_fluid > 0 && !sc->fluid_points))
+            throw axg::Error(AXG_E_ARG, "WavefieldScanning || missing point list.");
+        axg::HostScanning &x = h->model.scan;
+        x.enabled = true;
+        x.tol_fourier_h1 = sc->tol_fourier_h1; x.rel_tol_h1 = sc->rel_tol_h1; x.abs_tol_h1 = sc->abs_tol_h1;
+        x.max_peaks = sc->max_num_peaks; x.interval = sc->interval;
+        x.all_solid = sc->n_solid < 0; x.all_fluid = sc->n_fluid < 0;
+        x.solid_pts = sc->n_solid > 0 ? copy(sc->solid_points, sc->n_solid) : std::vector<int>();
+        x.fluid_pts = sc->n_fluid > 0 ? copy(sc->fluid_points, sc->n_fluid) : std::vector<int>();
+    });
+}
+
+int axg_scanning_nr(axg_solver *h, int32_t *solid_nr, int32_t *fluid_nr) {
+    return guarded(h, [&] {
+        if (!h->finalized) throw axg::Error(AXG_E_STATE, "axg_scanning_nr || axg_finalize not called.");
+        h->eng->scanning_nr(solid_nr, fluid_nr);
+    });
+}
+
 int axg_set_ocean_load(axg_solver *h, int32_t count, const int32_t *point, const double *mass_ocean,
                        const double *theta) {
     return guarded(h, [&] {
@@ -425,6 +451,16 @@ int axg_finalize(axg_solver *h) {
                 seen[p] = 1;
                 if (g.off[i] < 0 || g.off[i] + P.nr[p] > (int64_t)g.gamma.size())
                     throw axg::Error(AXG_E_ARG, "Sponge::Sponge || Incompatible sizes.");
+            }
+        }
+        for (int solid = 1; solid >= 0; solid--) {
+            const std::vector<int> &pts = solid ? m.scan.solid_pts : m.scan.fluid_pts;
+            const int np = solid ? m.sp.count : m.fp.count;
+            std::vector<char> seen(np, 0);
+            for (int p : pts) {
+                if (p < 0 || p >= np) throw axg::Error(AXG_E_ARG, "WavefieldScanning || point index out of range.");
+                if (seen[p]) throw axg::Error(AXG_E_ARG, "WavefieldScanning || point listed twice.");
+                seen[p] = 1;
             }
         }
         // one Sponge per point (GLLPoint::release averages the boundaries' gammas first)

@@ -85,6 +85,14 @@ struct HostSponge3D {
     std::vector<double> gamma;
 };
 
+struct HostScanning {
+    bool enabled = false;
+    double tol_fourier_h1 = 0, rel_tol_h1 = 0, abs_tol_h1 = 0;
+    int max_peaks = 1, interval = 1;
+    bool all_solid = false, all_fluid = false;
+    std::vector<int> solid_pts, fluid_pts;
+};
+
 struct HostOcean {
     int count = 0;
     std::vector<int> pt;
@@ -102,6 +110,7 @@ struct HostModel {
     HostClayton3D cl3_s, cl3_f;
     HostSponge3D sg3_s, sg3_f;
     HostOcean ocean;
+    HostScanning scan;
     HostSponge sg_s, sg_f;
     HostPoints sp, fp;
     HostSolidElements se;
@@ -147,6 +156,8 @@ public:
     virtual void stiffness_noalloc(const void *sx, void *sf, const void *fx, void *ff, void *scratch,
                                    size_t cap) = 0;
     virtual int device() const = 0;
+    // Point::reportScanningNr per point (-1: not scanned)
+    virtual void scanning_nr(int32_t *solid_nr, int32_t *fluid_nr) = 0;
 };
 
 // device address of the library's fixed no-allocation scratch on `device` (looked up

@@ -184,6 +184,7 @@ public:
         if (cfg_.autotune && !cfg_.plain) autotune();
         build_coupling(m.sf);
         build_abc(m);
+        build_scanning(m);
         build_sources(m.ms, m.fs);
         build_stations(m.st);
         step_dev_.alloc(1);
@@ -213,6 +214,7 @@ public:
         ensure_capacity(tstep + 1);
         set_step(tstep);
         launch_stations();
+        launch_scan();
     }
 
     void run(int nsteps, bool graph) override {
@@ -1165,6 +1167,84 @@ private:
         }
     }
 
+    static_assert(AXG_SCAN_CAP == AXG_SCAN_MAX_PEAKS, "scanning capacity must match the header");
+    void build_scanning(const HostModel &m) {
+        if (!m.scan.enabled) return;
+        if (nwave_ != 1) throw Error(AXG_E_UNSUPPORTED, "WavefieldScanning || one wavefield per handle.");
+        auto one = [&](bool all, const std::vector<int> &pts, const PointDev &P, ScanDev &S) {
+            S.h_pt.clear();
+            if (all) for (int p = 0; p < P.n; p++) S.h_pt.push_back(p);
+            else S.h_pt = pts;
+            S.n = (int)S.h_pt.size();
+            if (!S.n) return;
+            const size_t mm = (size_t)S.n * P.ndim;
+            S.pt.upload(S.h_pt);
+            S.cnt.alloc(mm); S.cnt.zero(stream_);
+            S.nu1.alloc(mm * AXG_SCAN_CAP); S.nu1.zero(stream_);
+            S.h2p.alloc(mm); S.h2p.zero(stream_);
+            S.h2pp.alloc(mm); S.h2pp.zero(stream_);
+            S.key.alloc(mm * AXG_SCAN_CAP); S.key.zero(stream_);
+        };
+        one(m.scan.all_solid, m.scan.solid_pts, sp_, scan_s_);
+        one(m.scan.all_fluid, m.scan.fluid_pts, fp_, scan_f_);
+    }
+
+    // Domain::doScanning (Domain.cpp:466-490) at the device's current step
+    void launch_scan() {
+        const HostScanning &h = model_.scan;
+        if (!h.enabled) return;
+        for (int solid = 1; solid >= 0; solid--) {
+            ScanDev &S = solid ? scan_s_ : scan_f_;
+            PointDev &P = solid ? sp_ : fp_;
+            if (!S.n) continue;
+            ScanArgs<T, D> a;
+            a.n = S.n; a.ndim = P.ndim; a.pt = S.pt.p; a.off = P.off.p; a.nr = P.nr.p; a.displ = P.displ.p;
+            // WavefieldScanning stores squared tolerances in double; doScanning takes Real
+            a.tol_fourier_h2 = (T)(h.tol_fourier_h1 * h.tol_fourier_h1);
+            a.rel_tol_h2 = (T)(h.rel_tol_h1 * h.rel_tol_h1);
+            a.abs_tol_h2 = (T)(h.abs_tol_h1 * h.abs_tol_h1);
+            a.max_peaks = std::min(h.max_peaks, AXG_SCAN_CAP);
+            a.interval = h.interval;
+            a.step = step_dev_.p;
+            a.h2p = S.h2p.p; a.h2pp = S.h2pp.p; a.cnt = S.cnt.p; a.key = S.key.p; a.nu1 = S.nu1.p;
+            const int m = S.n * P.ndim;
+            scan_kernel<T, D><<<(m + 255) / 256, 256, 0, stream_>>>(a);
+            post_launch();
+        }
+    }
+
+    void scanning_nr(int32_t *solid_nr, int32_t *fluid_nr) override {
+        need();
+        for (int solid = 1; solid >= 0; solid--) {
+            int32_t *out = solid ? solid_nr : fluid_nr;
+            if (!out) continue;
+            PointDev &P = solid ? sp_ : fp_;
+            ScanDev &S = solid ? scan_s_ : scan_f_;
+            for (int p = 0; p < P.n; p++) out[p] = -1;
+            if (!S.n) continue;
+            const size_t mm = (size_t)S.n * P.ndim;
+            std::vector<int> cnt(mm), nu1(mm * AXG_SCAN_CAP);
+            AXG_CUDA(cudaStreamSynchronize(stream_));
+            AXG_CUDA(cudaMemcpy(cnt.data(), S.cnt.p, mm * sizeof(int), cudaMemcpyDeviceToHost));
+            AXG_CUDA(cudaMemcpy(nu1.data(), S.nu1.p, mm * AXG_SCAN_CAP * sizeof(int), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < S.n; i++) {
+                const int p = S.h_pt[i];
+                int best = 1;
+                for (int c = 0; c < P.ndim; c++) {
+                    const size_t t = (size_t)i * P.ndim + c;
+                    int r = 1;   // reportScanningNr: 1 without candidates
+                    if (cnt[t] > 0) {
+                        int nu = 0;
+                        for (int k = 0; k < cnt[t]; k++) nu = std::max(nu, nu1[(size_t)k * mm + t]);
+                        r = std::min(nu * 2 + 1, P.h_nr[p]);
+                    }
+                    best = std::max(best, r);
+                }
+                out[p] = best;
+            }
+        }
+    }
+
     void launch_sponge3d(PointDev &P, Abc3D &g) {
         Sponge3DArgs<T, D> a;
         a.n = g.n; a.ndim = P.ndim; a.pt = g.pt.p; a.goff = g.coff.p; a.gamma = g.c.p; a.nr = P.nr.p;
@@ -1435,6 +1515,7 @@ private:
         launch_clayton();
         launch_coupling();
         launch_stations();
+        launch_scan();
         launch_points(7);
         advance_step_kernel<T><<<1, 1, 0, stream_>>>(step_dev_.p);
         post_launch();
@@ -1505,6 +1586,13 @@ private:
     int64_t state_wave_ = 0;
     int cls_n_ = 0, clf_n_ = 0;
     Abc3D cl3_s_, cl3_f_, sg3_s_, sg3_f_;
+    struct ScanDev {
+        int n = 0;
+        std::vector<int> h_pt;
+        DBuf<int> pt, cnt, nu1;
+        DBuf<T> h2p, h2pp, key;
+    };
+    ScanDev scan_s_, scan_f_;
     int ocean_n_ = 0;
     DBuf<int> ocean_pt_;
     DBuf<T> ocean_c_;

@@ -360,6 +360,108 @@ __global__ void sponge3d_kernel(const Sponge3DArgs<T, D> a) {
     }
 }
 
+// ------------------------------------------------------- wavefield scanning ---
+// Scanning1D::doScanning (point/Point.hpp:106-174) on the displacement of one component of
+// one point, every `interval` steps: energy peaks of the Fourier series (H2 norm) and the
+// number of modes each needs; the reference's std::map of candidates (ascending H2 keys)
+// is a sorted array of at most AXG_SCAN_CAP entries per component.
+#ifndef AXG_SCAN_CAP
+#define AXG_SCAN_CAP 32
+#endif
+template <class T, class D>
+struct ScanArgs {
+    int n, ndim;                 // scanned points; components per point
+    const int *pt, *off, *nr;
+    const cx_t<D> *displ;
+    T tol_fourier_h2, rel_tol_h2, abs_tol_h2;
+    int max_peaks, interval;
+    const int *step;
+    T *h2p, *h2pp;               // [n * ndim]
+    int *cnt;                    // [n * ndim]
+    T *key;                      // [AXG_SCAN_CAP][n * ndim]
+    int *nu1;                    // [AXG_SCAN_CAP][n * ndim]
+};
+
+template <class T, class D>
+__global__ void scan_kernel(const ScanArgs<T, D> a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = a.n * a.ndim;
+    if (t >= m || (*a.step) % a.interval != 0) return;
+    const int i = t / a.ndim, c = t - i * a.ndim;
+    const int p = a.pt[i], nu = a.nr[p] / 2 + 1;
+    const cx_t<D> *f = a.displ + (size_t)a.off[p] * a.ndim + c;
+    // l2 and h2 norms (the series in the working precision)
+    T l2 = 0;
+    for (int al = 0; al < nu; al++) {
+        const T x = (T)f[(size_t)al * a.ndim].x, y = (T)f[(size_t)al * a.ndim].y;
+        l2 += x * x + y * y;
+    }
+    const T x0 = (T)f[0].x, y0 = (T)f[0].y;
+    const T h2 = (T)((double)l2 - .5 * (double)(x0 * x0 + y0 * y0));
+    int n = a.cnt[t];
+    const T max_h2 = n > 0 ? a.key[(size_t)(n - 1) * m + t] : (T)0;
+    const T hp = a.h2p[t], hpp = a.h2pp[t];
+    a.h2pp[t] = hp;
+    a.h2p[t] = h2;
+    if (!(h2 > a.abs_tol_h2 && h2 > a.rel_tol_h2 * max_h2 && hp > h2 && hp > hpp)) return;
+    // smallest number of modes whose truncation error is below tol * H2
+    const T abs_fourier = h2 * a.tol_fourier_h2;
+    int new_nu1 = 1;
+    T head = 0;
+    for (; new_nu1 < nu; new_nu1++) {
+        const T x = (T)f[(size_t)(new_nu1 - 1) * a.ndim].x, y = (T)f[(size_t)(new_nu1 - 1) * a.ndim].y;
+        head += x * x + y * y;
+        if (l2 - head < abs_fourier) break;
+    }
+    T *key = a.key + t;
+    int *nv = a.nu1 + t;
+    int hit = -1;
+    for (int k = 0; k < n; k++)
+        if (key[(size_t)k * m] == h2) { hit = k; break; }
+    if (hit >= 0) {
+        nv[(size_t)hit * m] = max(nv[(size_t)hit * m], new_nu1);
+    } else {
+        if (max_h2 < h2) {
+            // drop the keys below rel_tol * H2 (map::erase(begin, lower_bound(rel_tol * H2)))
+            const T cut = a.rel_tol_h2 * h2;
+            int drop = 0;
+            while (drop < n && key[(size_t)drop * m] < cut) drop++;
+            for (int k = drop; k < n; k++) {
+                key[(size_t)(k - drop) * m] = key[(size_t)k * m];
+                nv[(size_t)(k - drop) * m] = nv[(size_t)k * m];
+            }
+            n -= drop;
+        }
+        // insert in ascending order; at capacity, inserting and then erasing the smallest key
+        // (the map's steps) keeps the set as it is when the new key is the smallest
+        if (n == AXG_SCAN_CAP) {
+            if (h2 < key[0]) { a.cnt[t] = n; return; }
+            for (int k = 1; k < n; k++) {
+                key[(size_t)(k - 1) * m] = key[(size_t)k * m];
+                nv[(size_t)(k - 1) * m] = nv[(size_t)k * m];
+            }
+            n--;
+        }
+        int pos = n;
+        while (pos > 0 && key[(size_t)(pos - 1) * m] > h2) {
+            key[(size_t)pos * m] = key[(size_t)(pos - 1) * m];
+            nv[(size_t)pos * m] = nv[(size_t)(pos - 1) * m];
+            pos--;
+        }
+        key[(size_t)pos * m] = h2;
+        nv[(size_t)pos * m] = new_nu1;
+        n++;
+    }
+    if (n > a.max_peaks) {
+        for (int k = 1; k < n; k++) {
+            key[(size_t)(k - 1) * m] = key[(size_t)k * m];
+            nv[(size_t)(k - 1) * m] = nv[(size_t)k * m];
+        }
+        n--;
+    }
+    a.cnt[t] = n;
+}
+
 // ------------------------------------------------------------- ocean load ---
 // MassOceanLoad1D::computeAccel (point/mass/MassOceanLoad1D.hpp): the point's own mass acts
 // along the surface, mass + ocean mass across it; one warp per point, lanes over modes,

@@ -121,6 +121,9 @@ class Model:
     ocean_load: Optional[tuple] = None
     # 3-D absorbing boundaries: Clayton dicts with point, offset and per-slice rho_vp,
     # rho_vs, area, normal [n][3] (solid); sponges as (points, offsets, per-slice gamma)
+    # wavefield scanning: dict(tol_fourier_h1, rel_tol_h1, abs_tol_h1, max_num_peaks, interval,
+    # solid_points=None (all), fluid_points=None (all))
+    scanning: Optional[dict] = None
     cl3_solid: Optional[dict] = None
     cl3_fluid: Optional[dict] = None
     sponge3d_solid: Optional[tuple] = None
@@ -299,6 +302,22 @@ class Model:
             keep[name + "_pt"], keep[name + "_off"], keep[name + "_g"] = pt, off, g
             return (pt, off, g)
 
+        def scan():
+            d = self.scanning
+            if not d:
+                return None
+            c = L.axg_scanning()
+            c.tol_fourier_h1, c.rel_tol_h1, c.abs_tol_h1 = d["tol_fourier_h1"], d["rel_tol_h1"], d["abs_tol_h1"]
+            c.max_num_peaks, c.interval = int(d["max_num_peaks"]), int(d["interval"])
+            for key, nk, pk in (("solid_points", "n_solid", "scs"), ("fluid_points", "n_fluid", "scf")):
+                pts = d.get(key)
+                if pts is None:
+                    setattr(c, nk, -1)
+                else:
+                    setattr(c, nk, len(pts))
+                    setattr(c, key, k(pk, pts, _i32, C.c_int32))
+            return c
+
         def ocean():
             if not self.ocean_load:
                 return (None, None, None)
@@ -316,7 +335,7 @@ class Model:
         return {"sp": sp, "fp": fp, "se": se, "fe": fe, "sf": sf, "ms": ms, "fs": fs, "st": st,
                 "cl_s": clay("cls", self.cl_solid, True), "cl_f": clay("clf", self.cl_fluid, False),
                 "sg_s": sponge("sgs", self.sponge_solid), "sg_f": sponge("sgf", self.sponge_fluid),
-                "ocean": ocean(),
+                "ocean": ocean(), "scan": scan(),
                 "cl3_s": clay3("c3s", self.cl3_solid, True), "cl3_f": clay3("c3f", self.cl3_fluid, False),
                 "sg3_s": sponge3("g3s", self.sponge3d_solid), "sg3_f": sponge3("g3f", self.sponge3d_fluid),
                 "keep": keep}

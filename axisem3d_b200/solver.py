@@ -73,6 +73,8 @@ class Solver:
                 self._check(self.lib.axg_set_sponge3d(h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
                                                       off.ctypes.data_as(L.P_i64), len(g),
                                                       g.ctypes.data_as(L.P_f64)))
+        if s["scan"] is not None:
+            self._check(self.lib.axg_set_scanning(h, C.byref(s["scan"])))
         pt, mo, th = s["ocean"]
         if pt is not None and len(pt):
             self._check(self.lib.axg_set_ocean_load(h, len(pt), pt.ctypes.data_as(L.P_i32),
@@ -110,6 +112,14 @@ class Solver:
 
     def compute_stiffness(self):
         self._check(self.lib.axg_compute_stiffness(self.h))
+
+    def scanning_nr(self):
+        """Point::reportScanningNr of every solid and fluid point (-1: not scanned)."""
+        ns, nf = len(self.model.sp_nr), len(self.model.fp_nr)
+        a = np.zeros(max(ns, 1), np.int32)
+        b = np.zeros(max(nf, 1), np.int32)
+        self._check(self.lib.axg_scanning_nr(self.h, a.ctypes.data_as(L.P_i32), b.ctypes.data_as(L.P_i32)))
+        return a[:ns], b[:nf]
 
     def compute_stiffness_noalloc(self, solid_x, solid_f, fluid_x=None, fluid_f=None):
         """f -= K x for caller-owned device buffers (integer device addresses, complex in the

@@ -245,6 +245,22 @@ typedef struct axg_clayton3d {
     const double  *normal;        /* solid only: unit normal (s, phi, z) per slice, [nvalues][3] */
 } axg_clayton3d;
 
+/* wavefield scanning (WavefieldScanning.cpp:40-90 parameters; Scanning1D, Point.hpp:106-198):
+   every `interval` steps the displacement of each scanned point is checked for energy peaks
+   and the number of Fourier modes each peak needs; axg_scanning_nr reports the resulting nr */
+typedef struct axg_scanning {
+    double         tol_fourier_h1;  /* threshold_Fourier_convergence                      */
+    double         rel_tol_h1;      /* relative_amplitude_skipped                          */
+    double         abs_tol_h1;      /* absolute_amplitude_skipped                          */
+    int32_t        max_num_peaks;   /* peaks kept per component (at most AXG_SCAN_MAX_PEAKS) */
+    int32_t        interval;        /* time steps between two scans                        */
+    int32_t        n_solid;         /* scanned solid points; -1 = all                      */
+    const int32_t *solid_points;
+    int32_t        n_fluid;         /* scanned fluid points; -1 = all                      */
+    const int32_t *fluid_points;
+} axg_scanning;
+#define AXG_SCAN_MAX_PEAKS 32
+
 typedef struct axg_solver axg_solver;
 
 /* ---- lifetime ---- */
@@ -278,6 +294,15 @@ int  axg_set_clayton3d(axg_solver *h, int32_t solid, const axg_clayton3d *c);
    offset[i] + nr - 1] for point[i]; a point carries a 1-D or a 3-D sponge, not both */
 int  axg_set_sponge3d(axg_solver *h, int32_t solid, int32_t count, const int32_t *point,
                       const int64_t *offset, int64_t nvalues, const double *gamma);
+/* enables wavefield scanning (Domain::doScanning, Domain.cpp:466-490) during axg_run and
+   axg_record_stations; before axg_finalize; one wavefield per handle. A max_num_peaks above
+   AXG_SCAN_MAX_PEAKS keeps the AXG_SCAN_MAX_PEAKS largest peaks (the reference keeps up to
+   max_num_peaks) */
+int  axg_set_scanning(axg_solver *h, const axg_scanning *s);
+/* Point::reportScanningNr per point (solid: the largest over the three components):
+   min(2 nu + 1, nr) of the peaks found, 1 where no peak passed, -1 for unscanned points;
+   solid_nr [solid points], fluid_nr [fluid points] (either may be NULL) */
+int  axg_scanning_nr(axg_solver *h, int32_t *solid_nr, int32_t *fluid_nr);
 /* MassOceanLoad1D (point/mass/MassOceanLoad1D.hpp, built in GLLPoint.cpp:66-73) on solid
    surface points under an ocean:
    in computeStiffToAccel the point's own mass acts along the surface and mass + mass_ocean

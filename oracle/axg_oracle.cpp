@@ -27,6 +27,7 @@
 #include <array>
 #include <cmath>
 #include <complex>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -386,6 +387,8 @@ struct OracleBase {
     virtual void set_sponge(int solid, int n, const int32_t *pt, const double *g) = 0;
     virtual void set_ocean_load(int n, const int32_t *pt, const double *mo, const double *theta) = 0;
     virtual void set_clayton3d(int solid, const axg_clayton3d *c) = 0;
+    virtual void set_scanning(const axg_scanning *s) = 0;
+    virtual void scanning_nr(int32_t *s, int32_t *f) = 0;
     virtual void set_sponge3d(int solid, int n, const int32_t *pt, const int64_t *off, const double *g) = 0;
     virtual void apply_sources(int tstep) = 0;
     virtual void compute_stiffness(int nthreads) = 0;
@@ -1203,7 +1206,102 @@ struct Oracle : OracleBase {
     }
 
     // StationSolid::record, displacement channel (StationSolid.cpp:58-66, Station.hpp:53-72)
+    // ---------------- wavefield scanning (Scanning1D, Point.hpp:106-198) ----------------
+    struct Scan1D {
+        R h2p = 0, h2pp = 0;
+        std::map<R, int> cand;
+    };
+    bool scan_on = false;
+    R scan_tf = 0, scan_rel = 0, scan_abs = 0;
+    int scan_peaks = 1, scan_interval = 1;
+    std::vector<int> scan_pts[2];            // [fluid, solid]
+    std::vector<std::vector<Scan1D>> scan_st[2];
+    void set_scanning(const axg_scanning *s) override {
+        scan_on = true;
+        scan_tf = (R)(s->tol_fourier_h1 * s->tol_fourier_h1);
+        scan_rel = (R)(s->rel_tol_h1 * s->rel_tol_h1);
+        scan_abs = (R)(s->abs_tol_h1 * s->abs_tol_h1);
+        scan_peaks = std::min(s->max_num_peaks, AXG_SCAN_MAX_PEAKS);
+        scan_interval = s->interval;
+        for (int solid = 1; solid >= 0; solid--) {
+            const PointSet<R> &ps = solid ? sp : fp;
+            const int n = solid ? s->n_solid : s->n_fluid;
+            const int32_t *pts = solid ? s->solid_points : s->fluid_points;
+            scan_pts[solid].clear();
+            if (n < 0) for (int p = 0; p < ps.n; p++) scan_pts[solid].push_back(p);
+            else for (int i = 0; i < n; i++) scan_pts[solid].push_back(pts[i]);
+            scan_st[solid].assign(scan_pts[solid].size(), std::vector<Scan1D>(ps.ndim));
+        }
+    }
+    static void scan_one(Scan1D &sc, const Cx<R> *f, int stride, int nu, R tf, R rel, R abs_, int peaks) {
+        R l2 = 0;
+        for (int a = 0; a < nu; a++) l2 += f[a * stride].real() * f[a * stride].real() + f[a * stride].imag() * f[a * stride].imag();
+        const R n0 = f[0].real() * f[0].real() + f[0].imag() * f[0].imag();
+        const R h2 = (R)((double)l2 - .5 * (double)n0);
+        const R maxh2 = sc.cand.empty() ? (R)0 : sc.cand.rbegin()->first;
+        if (!(h2 > abs_ && h2 > rel * maxh2 && sc.h2p > h2 && sc.h2p > sc.h2pp)) {
+            sc.h2pp = sc.h2p;
+            sc.h2p = h2;
+            return;
+        }
+        const R absf = h2 * tf;
+        int nn = 1;
+        R head = 0;
+        for (; nn < nu; nn++) {
+            head += f[(nn - 1) * stride].real() * f[(nn - 1) * stride].real() +
+                    f[(nn - 1) * stride].imag() * f[(nn - 1) * stride].imag();
+            if (l2 - head < absf) break;
+        }
+        auto it = sc.cand.find(h2);
+        if (it != sc.cand.end()) {
+            it->second = std::max(it->second, nn);
+        } else {
+            if (maxh2 < h2) sc.cand.erase(sc.cand.begin(), sc.cand.lower_bound(rel * h2));
+            sc.cand.insert({h2, nn});
+        }
+        if ((int)sc.cand.size() > peaks) sc.cand.erase(sc.cand.begin());
+        sc.h2pp = sc.h2p;
+        sc.h2p = h2;
+    }
+    void scan(int tstep) {
+        if (!scan_on || tstep % scan_interval != 0) return;
+        for (int solid = 1; solid >= 0; solid--) {
+            PointSet<R> &ps = solid ? sp : fp;
+            for (size_t i = 0; i < scan_pts[solid].size(); i++) {
+                const int p = scan_pts[solid][i];
+                for (int c = 0; c < ps.ndim; c++)
+                    scan_one(scan_st[solid][i][c], &ps.displ[(size_t)ps.off[p] * ps.ndim + c], ps.ndim, ps.nu[p],
+                             scan_tf, scan_rel, scan_abs, scan_peaks);
+            }
+        }
+    }
+    void scanning_nr(int32_t *out_s, int32_t *out_f) override {
+        for (int solid = 1; solid >= 0; solid--) {
+            int32_t *out = solid ? out_s : out_f;
+            if (!out) continue;
+            PointSet<R> &ps = solid ? sp : fp;
+            for (int p = 0; p < ps.n; p++) out[p] = -1;
+            if (!scan_on) continue;
+            for (size_t i = 0; i < scan_pts[solid].size(); i++) {
+                const int p = scan_pts[solid][i];
+                int best = 1;
+                for (int c = 0; c < ps.ndim; c++) {
+                    const Scan1D &sc = scan_st[solid][i][c];
+                    int r = 1;
+                    if (!sc.cand.empty()) {
+                        int nu = 0;
+                        for (auto &kv : sc.cand) nu = std::max(nu, kv.second);
+                        r = std::min(nu * 2 + 1, ps.nr[p]);
+                    }
+                    best = std::max(best, r);
+                }
+                out[p] = best;
+            }
+        }
+    }
+
     void record(int tstep) override {
+        scan(tstep);
         if (st.empty() || tstep % rec_interval != 0) return;
         size_t base = seis.size();
         seis.resize(base + st.size() * 3);
@@ -1330,6 +1428,8 @@ int axo_set_stations(void *h, const axg_stations *s, int interval) { AXO_TRY(sta
 int axo_set_clayton(void *h, int solid, const axg_clayton *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton(solid, c)) }
 int axo_set_sponge(void *h, int solid, int n, const int32_t *pt, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge(solid, n, pt, g)) }
 int axo_set_ocean_load(void *h, int n, const int32_t *pt, const double *mo, const double *theta) { AXO_TRY(static_cast<OracleBase *>(h)->set_ocean_load(n, pt, mo, theta)) }
+int axo_set_scanning(void *h, const axg_scanning *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_scanning(s)) }
+int axo_scanning_nr(void *h, int32_t *s, int32_t *f) { AXO_TRY(static_cast<OracleBase *>(h)->scanning_nr(s, f)) }
 int axo_set_clayton3d(void *h, int solid, const axg_clayton3d *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton3d(solid, c)) }
 int axo_set_sponge3d(void *h, int solid, int n, const int32_t *pt, const int64_t *off, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge3d(solid, n, pt, off, g)) }
 int axo_apply_sources(void *h, int tstep) { AXO_TRY(static_cast<OracleBase *>(h)->apply_sources(tstep)) }

@@ -54,6 +54,8 @@ def lib():
             "axo_set_sponge": (C.c_int, [V, C.c_int, C.c_int, L.P_i32, L.P_f64]),
             "axo_set_ocean_load": (C.c_int, [V, C.c_int, L.P_i32, L.P_f64, L.P_f64]),
             "axo_set_clayton3d": (C.c_int, [V, C.c_int, C.POINTER(L.axg_clayton3d)]),
+            "axo_set_scanning": (C.c_int, [V, C.POINTER(L.axg_scanning)]),
+            "axo_scanning_nr": (C.c_int, [V, L.P_i32, L.P_i32]),
             "axo_set_sponge3d": (C.c_int, [V, C.c_int, C.c_int, L.P_i32, L.P_i64, L.P_f64]),
             "axo_compute_stiffness": (C.c_int, [V, C.c_int]),
             "axo_bc_before": (C.c_int, [V]),
@@ -118,6 +120,8 @@ class Oracle:
             if pt is not None and len(pt):
                 self._chk(self.O.axo_set_sponge3d(self.h, solid, len(pt), pt.ctypes.data_as(L.P_i32),
                                                   off.ctypes.data_as(L.P_i64), g.ctypes.data_as(L.P_f64)))
+        if s["scan"] is not None:
+            self._chk(self.O.axo_set_scanning(self.h, C.byref(s["scan"])))
         pt, mo, th = s["ocean"]
         if pt is not None and len(pt):
             self._chk(self.O.axo_set_ocean_load(self.h, len(pt), pt.ctypes.data_as(L.P_i32),
@@ -161,6 +165,13 @@ class Oracle:
 
     def run(self, nsteps):
         self._chk(self.O.axo_run(self.h, int(nsteps), int(self.threads)))
+
+    def scanning_nr(self):
+        ns, nf = len(self.model.sp_nr), len(self.model.fp_nr)
+        a = np.zeros(max(ns, 1), np.int32)
+        b = np.zeros(max(nf, 1), np.int32)
+        self._chk(self.O.axo_scanning_nr(self.h, a.ctypes.data_as(self.L.P_i32), b.ctypes.data_as(self.L.P_i32)))
+        return a[:ns], b[:nf]
 
     def reset_attenuation(self):
         self._chk(self.O.axo_reset_attenuation(self.h))

@@ -290,3 +290,27 @@ def test_ocean_and_mass3d_reduce_to_mass1d():
     for m in (oc, m3):
         d = run(m)
         assert np.linalg.norm(d - ref) <= 1e-13 * np.linalg.norm(ref)
+
+
+def test_scanning_peak_and_mode_count():
+    """Scanning1D on a prescribed history: a displacement whose Fourier series fills modes
+    0..3 equally, with amplitudes 1, 2, 3, 2, 1 at five scans, has one energy peak (found at
+    the scan after the maximum) that needs 4 modes: every point reports nr = 2 * 4 + 1."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=3, nz=3, nr=16)
+    m.ms_elem = np.zeros(0, np.int32)
+    m.ms_nu = np.zeros(0, np.int32)
+    m.ms_pat_off = np.zeros(0, np.int64)
+    m.ms_pattern = np.zeros(0, np.complex128)
+    m.ms_stf = []
+    m.scanning = dict(tol_fourier_h1=1e-2, rel_tol_h1=0.1, abs_tol_h1=1e-12, max_num_peaks=10, interval=1)
+    o = O.Oracle(m, "fp64")
+    nu = 16 // 2 + 1
+    pattern = np.zeros((len(m.sp_nr), nu, 3), np.complex128)
+    pattern[:, :4, :] = 1.0 + 0.5j
+    for t, amp in enumerate((1.0, 2.0, 3.0, 2.0, 1.0)):
+        o.set_field((amp * pattern).ravel(), "displ")
+        o.record_stations(t)
+    s_nr, _ = o.scanning_nr()
+    assert np.all(s_nr == 9), np.unique(s_nr)
