@@ -119,6 +119,7 @@ SIGNATURES = {
     "axg_set_clayton": (C.c_int, [H, C.c_int32, C.POINTER(axg_clayton)]),
     "axg_set_sponge": (C.c_int, [H, C.c_int32, C.c_int32, P_i32, P_f64]),
     "axg_set_ocean_load": (C.c_int, [H, C.c_int32, P_i32, P_f64, P_f64]),
+    "axg_set_ocean_load3d": (C.c_int, [H, C.c_int32, P_i32, P_i64, C.c_int64, P_f64, P_f64]),
     "axg_set_clayton3d": (C.c_int, [H, C.c_int32, C.POINTER(axg_clayton3d)]),
     "axg_set_scanning": (C.c_int, [H, C.POINTER(axg_scanning)]),
     "axg_scanning_nr": (C.c_int, [H, P_i32, P_i32]),

@@ -374,6 +374,21 @@ int axg_set_ocean_load(axg_solver *h, int32_t count, const int32_t *point, const
     });
 }
 
+int axg_set_ocean_load3d(axg_solver *h, int32_t count, const int32_t *point, const int64_t *offset,
+                         int64_t nvalues, const double *mass_ocean, const double *normal) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (count < 0 || nvalues < 0 || (count && (!point || !offset || !mass_ocean || !normal)))
+            throw axg::Error(AXG_E_ARG, "MassOceanLoad3D || missing array.");
+        axg::HostOcean3D &x = h->model.ocean3;
+        x.count = count;
+        x.pt = copy(point, count);
+        x.off = copy(offset, count);
+        x.mass_ocean = copy(mass_ocean, nvalues);
+        x.normal = copy(normal, (size_t)nvalues * 3);
+    });
+}
+
 int axg_finalize(axg_solver *h) {
     return guarded(h, [&] {
         need_open(h);
@@ -420,9 +435,24 @@ int axg_finalize(axg_solver *h) {
                 if (seen[p]) throw axg::Error(AXG_E_ARG, "MassOceanLoad1D || point listed twice.");
                 seen[p] = 1;
                 if (m.sp.mass_nr.size() && m.sp.mass_nr[p] > 1)
-                    throw axg::Error(AXG_E_UNSUPPORTED, "MassOceanLoad3D || 3-D ocean load is not supported.");
+                    throw axg::Error(AXG_E_ARG, "MassOceanLoad1D || a Mass3D point needs a 3-D ocean load.");
                 if (!(m.ocean.mass_ocean[i] >= 0))
                     throw axg::Error(AXG_E_ARG, "MassOceanLoad1D || negative ocean mass.");
+            }
+            for (int i = 0; i < m.ocean3.count; i++) {
+                const int p = m.ocean3.pt[i];
+                if (p < 0 || p >= m.sp.count)
+                    throw axg::Error(AXG_E_ARG, "MassOceanLoad3D || point index out of range.");
+                if (seen[p]) throw axg::Error(AXG_E_ARG, "MassOceanLoad3D || point listed twice.");
+                seen[p] = 1;
+                const int nr = m.sp.nr[p];
+                if (m.sp.mass_nr.size() && m.sp.mass_nr[p] > 1 && m.sp.mass_nr[p] != nr)
+                    throw axg::Error(AXG_E_ARG, "MassOceanLoad3D::checkCompatibility || Incompatible sizes.");
+                if (m.ocean3.off[i] < 0 || m.ocean3.off[i] + nr > (int64_t)m.ocean3.mass_ocean.size())
+                    throw axg::Error(AXG_E_ARG, "MassOceanLoad3D::checkCompatibility || Incompatible sizes.");
+                for (int k = 0; k < nr; k++)
+                    if (!(m.ocean3.mass_ocean[m.ocean3.off[i] + k] >= 0))
+                        throw axg::Error(AXG_E_ARG, "MassOceanLoad3D || negative ocean mass.");
             }
         }
         // 3-D conditions: nr values of the point from each offset

@@ -99,6 +99,13 @@ struct HostOcean {
     std::vector<double> mass_ocean, theta;
 };
 
+struct HostOcean3D {
+    int count = 0;
+    std::vector<int> pt;
+    std::vector<int64_t> off;
+    std::vector<double> mass_ocean, normal;
+};
+
 struct HostSponge {
     int count = 0;
     std::vector<int> pt;
@@ -110,6 +117,7 @@ struct HostModel {
     HostClayton3D cl3_s, cl3_f;
     HostSponge3D sg3_s, sg3_f;
     HostOcean ocean;
+    HostOcean3D ocean3;
     HostScanning scan;
     HostSponge sg_s, sg_f;
     HostPoints sp, fp;

@@ -176,6 +176,7 @@ public:
         for (int i = 0; i < m.cl3_f.count; i++) nrs.push_back(m.fp.nr[m.cl3_f.pt[i]]);
         for (int i = 0; i < m.sg3_s.count; i++) nrs.push_back(m.sp.nr[m.sg3_s.pt[i]]);
         for (int i = 0; i < m.sg3_f.count; i++) nrs.push_back(m.fp.nr[m.sg3_f.pt[i]]);
+        for (int i = 0; i < m.ocean3.count; i++) nrs.push_back(m.sp.nr[m.ocean3.pt[i]]);
         std::vector<int> twoff;
         tw_.upload(twiddle_pool<T>(nrs, nrmax, twoff));
         tw_off_.upload(twoff);
@@ -646,6 +647,7 @@ private:
     // -------------------------------------------------------- points ---
     // MassOceanLoad1D constructor (MassOceanLoad1D.hpp): coefficients in double, cast
     void build_ocean(const HostModel &m) {
+        build_ocean3d(m);
         ocean_n_ = m.ocean.count;
         if (!ocean_n_) return;
         std::vector<T> c((size_t)4 * ocean_n_);
@@ -663,6 +665,39 @@ private:
         ocean_pt_.upload(m.ocean.pt);
         ocean_c_.upload(c);
         sp_.flags.upload(sp_.h_flags);
+    }
+
+    // MassOceanLoad3D constructor (MassOceanLoad3D.cpp): 1/m and k = sqrt(m0 / (m (m + m0))) n
+    // per slice, in double, cast; these points leave the Mass3D list (their kernel does 1/M)
+    void build_ocean3d(const HostModel &m) {
+        ocean3_n_ = m.ocean3.count;
+        if (!ocean3_n_) return;
+        std::vector<T> c;
+        std::vector<int64_t> coff;
+        for (int i = 0; i < ocean3_n_; i++) {
+            const int p = m.ocean3.pt[i], nr = m.sp.nr[p];
+            const int mnr = m.sp.mass_nr.size() ? m.sp.mass_nr[p] : 1;
+            const int64_t mo = m.sp.mass_off.size() ? m.sp.mass_off[p] : p;
+            coff.push_back((int64_t)c.size());
+            for (int k = 0; k < nr; k++) {
+                const double mass = m.sp.mass[mo + (mnr > 1 ? k : 0)];
+                const int64_t q = m.ocean3.off[i] + k;
+                const double m0 = m.ocean3.mass_ocean[q];
+                const double sk = std::sqrt(m0 / (mass * (mass + m0)));
+                c.push_back((T)(1.0 / mass));
+                for (int d = 0; d < 3; d++) c.push_back((T)(sk * m.ocean3.normal[q * 3 + d]));
+            }
+            sp_.h_flags[p] = (uint8_t)((sp_.h_flags[p] & ~PT_MASS3D) | PT_OCEAN);
+        }
+        ocean3_pt_.upload(m.ocean3.pt);
+        ocean3_coff_.upload(coff);
+        ocean3_c_.upload(c);
+        sp_.flags.upload(sp_.h_flags);
+        std::vector<int> pt3d;
+        for (int p = 0; p < sp_.n; p++)
+            if (sp_.h_flags[p] & PT_MASS3D) pt3d.push_back(p);
+        sp_.n3d = (int)pt3d.size();
+        sp_.pt3d.upload(pt3d);
     }
 
     void build_points(const HostPoints &h, PointDev &P, bool solid) {
@@ -1470,6 +1505,17 @@ private:
                 mass3d_kernel<T><<<(P.n3d * nwave_ + wpb - 1) / wpb, 32 * wpb, wpb * P.nr_max * sizeof(T), stream_>>>(a);
                 post_launch();
             }
+            if (solid && ocean3_n_ && (mask & 3)) {
+                Ocean3DArgs<T> o;
+                o.n = ocean3_n_; o.pt = ocean3_pt_.p; o.coff = ocean3_coff_.p; o.c = ocean3_c_.p;
+                o.nr = P.nr.p; o.off = P.off.p; o.flags = P.flags.p; o.tw = tw_.p; o.tw_off = tw_off_.p;
+                o.stiff = P.stiff.p; o.nr_max = P.nr_max; o.nwave = nwave_;
+                o.fstride = (size_t)P.total * P.ndim; o.mask = mask;
+                const int wpb = 4;
+                ocean3d_kernel<T><<<(ocean3_n_ * nwave_ + wpb - 1) / wpb, 32 * wpb,
+                                    (size_t)wpb * 3 * P.nr_max * sizeof(T), stream_>>>(o);
+                post_launch();
+            }
             if (solid && ocean_n_ && (mask & 3)) {
                 OceanArgs<T> o;
                 o.n = ocean_n_; o.pt = ocean_pt_.p; o.c = ocean_c_.p; o.nr = P.nr.p; o.off = P.off.p;
@@ -1593,7 +1639,10 @@ private:
         DBuf<T> h2p, h2pp, key;
     };
     ScanDev scan_s_, scan_f_;
-    int ocean_n_ = 0;
+    int ocean_n_ = 0, ocean3_n_ = 0;
+    DBuf<int> ocean3_pt_;
+    DBuf<int64_t> ocean3_coff_;
+    DBuf<T> ocean3_c_;
     DBuf<int> ocean_pt_;
     DBuf<T> ocean_c_;
     DBuf<int> cls_pt_, clf_pt_, cls_first_, clf_first_;

@@ -504,6 +504,59 @@ __global__ void ocean_mass_kernel(const OceanArgs<T> a) {
     }
 }
 
+// MassOceanLoad3D::computeAccel (point/mass/MassOceanLoad3D.cpp): in slices,
+// a = F / m - (F . k) k; one warp per point, after its boundary conditions
+template <class T>
+struct Ocean3DArgs {
+    int n;
+    const int *pt;
+    const int64_t *coff;         // per point: offset of its [nr][4] (1/m, k_s, k_phi, k_z)
+    const T *c;
+    const int *nr, *off;
+    const uint8_t *flags;
+    const T *tw; const int *tw_off;
+    cx_t<T> *stiff;
+    int nr_max, nwave;
+    size_t fstride;
+    int mask;
+};
+
+template <class T>
+__global__ void ocean3d_kernel(const Ocean3DArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int w = threadIdx.x / 32, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * (blockDim.x / 32) + w;
+    if (item >= a.n * a.nwave) return;
+    const int i = item % a.n, wf = item / a.n;
+    const int p = a.pt[i], nr = a.nr[p], nu = nr / 2 + 1;
+    cx_t<T> *f = a.stiff + (size_t)wf * a.fstride + (size_t)a.off[p] * 3;
+    if (a.mask & 1) {
+        for (int al = lane; al < nu; al += 32) {
+            cx_t<T> v[3] = {f[al * 3], f[al * 3 + 1], f[al * 3 + 2]};
+            point_bc<T>(v, 3, al, nu, nr, a.flags[p], true);
+            f[al * 3] = v[0]; f[al * 3 + 1] = v[1]; f[al * 3 + 2] = v[2];
+        }
+        __syncwarp();
+    }
+    if (!(a.mask & 2)) return;
+    T *fr = reinterpret_cast<T *>(sm) + (size_t)w * 3 * a.nr_max;   // [3][nr_max] slices
+    const T *twc = a.tw + a.tw_off[nr], *tws = twc + nr;
+    const T *cf = a.c + a.coff[i];
+    for (int c = 0; c < 3; c++) warp_c2r<T, cx_t<T>>(f + c, 3, nu, nr, twc, tws, fr + (size_t)c * a.nr_max, lane);
+    __syncwarp();
+    for (int k = lane; k < nr; k += 32) {
+        const T f0 = fr[k], f1 = fr[a.nr_max + k], f2 = fr[2 * a.nr_max + k];
+        const T im = cf[4 * k], k0 = cf[4 * k + 1], k1 = cf[4 * k + 2], k2 = cf[4 * k + 3];
+        const T dot = f0 * k0 + f1 * k1 + f2 * k2;
+        fr[k] = im * f0 - dot * k0;
+        fr[a.nr_max + k] = im * f1 - dot * k1;
+        fr[2 * a.nr_max + k] = im * f2 - dot * k2;
+    }
+    __syncwarp();
+    for (int al = lane; al < nu; al += 32)
+        for (int c = 0; c < 3; c++) f[al * 3 + c] = r2c_mode<T>(fr + (size_t)c * a.nr_max, nr, al, twc, tws);
+}
+
 template <class T, class D>
 struct PointArgs {
     int nmodes;                  // sum nu

@@ -454,6 +454,30 @@ def add_absorbing3d(m, rho=3300.0, vp=8000.0, vs=4500.0, pert=0.05, sponge_width
     return m
 
 
+def add_ocean_load3d(m, nx, nz, width, rho_water=1020.0, depth_water=3000.0, amp=0.2, tilt=0.2, seed=0):
+    """MassOceanLoad3D on the surface points of a cartesian_model grid: the water depth varies
+    by +-amp over the nr slices of each point (a seeded phase), and the unit normal tilts by a
+    seeded angle of up to `tilt` towards s and phi per slice; area as in add_ocean_load."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    add_ocean_load(m, nx, nz, width, rho_water, depth_water)
+    pts, mo1, _ = m.ocean_load
+    m.ocean_load = None
+    nr = np.asarray(m.sp_nr)
+    off, mo, nrm = [], [], []
+    o = 0
+    for p, m0 in zip(pts, mo1):
+        n = int(nr[p])
+        off.append(o)
+        o += n
+        k = np.arange(n)
+        mo.append(m0 * (1.0 + amp * np.sin(2 * np.pi * k / n + rng.uniform(0, 2 * np.pi))))
+        a, b = rng.uniform(-tilt, tilt, n), rng.uniform(-tilt, tilt, n)
+        v = np.stack([np.sin(a), np.sin(b), np.cos(a) * np.cos(b)], axis=1)
+        nrm.append(v / np.linalg.norm(v, axis=1, keepdims=True))
+    m.ocean_load3d = (np.asarray(pts, np.int32), np.array(off, np.int64), np.concatenate(mo), np.concatenate(nrm))
+    return m
+
+
 def with_mass3d(m, amp=0.05, seed=0, exclude=()):
     """A copy of `m` whose solid points with nr >= 2 (except `exclude`) carry 3-D masses
     (Mass3D): the point's mass times (1 + amp * U(-1, 1)) per slice, seeded."""

@@ -119,6 +119,8 @@ class Model:
     sponge_fluid: Optional[tuple] = None
     # MassOceanLoad1D on solid surface points: (points, ocean mass, normal polar angle)
     ocean_load: Optional[tuple] = None
+    # MassOceanLoad3D: (points, offsets, per-slice ocean mass, per-slice unit normal [n][3])
+    ocean_load3d: Optional[tuple] = None
     # 3-D absorbing boundaries: Clayton dicts with point, offset and per-slice rho_vp,
     # rho_vs, area, normal [n][3] (solid); sponges as (points, offsets, per-slice gamma)
     # wavefield scanning: dict(tol_fourier_h1, rel_tol_h1, abs_tol_h1, max_num_peaks, interval,
@@ -318,6 +320,14 @@ class Model:
                     setattr(c, key, k(pk, pts, _i32, C.c_int32))
             return c
 
+        def ocean3():
+            if not self.ocean_load3d:
+                return None
+            t = self.ocean_load3d
+            pt, off, mo, nrm = _i32(t[0]), _i64(t[1]), _f64(t[2]), _f64(np.asarray(t[3]).ravel())
+            keep["o3_pt"], keep["o3_off"], keep["o3_mo"], keep["o3_n"] = pt, off, mo, nrm
+            return (pt, off, mo, nrm)
+
         def ocean():
             if not self.ocean_load:
                 return (None, None, None)
@@ -335,7 +345,7 @@ class Model:
         return {"sp": sp, "fp": fp, "se": se, "fe": fe, "sf": sf, "ms": ms, "fs": fs, "st": st,
                 "cl_s": clay("cls", self.cl_solid, True), "cl_f": clay("clf", self.cl_fluid, False),
                 "sg_s": sponge("sgs", self.sponge_solid), "sg_f": sponge("sgf", self.sponge_fluid),
-                "ocean": ocean(), "scan": scan(),
+                "ocean": ocean(), "scan": scan(), "ocean3": ocean3(),
                 "cl3_s": clay3("c3s", self.cl3_solid, True), "cl3_f": clay3("c3f", self.cl3_fluid, False),
                 "sg3_s": sponge3("g3s", self.sponge3d_solid), "sg3_f": sponge3("g3f", self.sponge3d_fluid),
                 "keep": keep}

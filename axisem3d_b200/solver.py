@@ -75,6 +75,11 @@ class Solver:
                                                       g.ctypes.data_as(L.P_f64)))
         if s["scan"] is not None:
             self._check(self.lib.axg_set_scanning(h, C.byref(s["scan"])))
+        if s["ocean3"] is not None:
+            pt, off, mo, nrm = s["ocean3"]
+            self._check(self.lib.axg_set_ocean_load3d(h, len(pt), pt.ctypes.data_as(L.P_i32),
+                                                      off.ctypes.data_as(L.P_i64), len(mo),
+                                                      mo.ctypes.data_as(L.P_f64), nrm.ctypes.data_as(L.P_f64)))
         pt, mo, th = s["ocean"]
         if pt is not None and len(pt):
             self._check(self.lib.axg_set_ocean_load(h, len(pt), pt.ctypes.data_as(L.P_i32),

@@ -307,9 +307,15 @@ int  axg_scanning_nr(axg_solver *h, int32_t *solid_nr, int32_t *fluid_nr);
    surface points under an ocean:
    in computeStiffToAccel the point's own mass acts along the surface and mass + mass_ocean
    across it, the surface normal at polar angle theta; each point at most once, points with
-   1-D masses only (a 3-D ocean load returns AXG_E_UNSUPPORTED) */
+   1-D masses only (a Mass3D point takes axg_set_ocean_load3d) */
 int  axg_set_ocean_load(axg_solver *h, int32_t count, const int32_t *point, const double *mass_ocean,
                         const double *theta);
+/* MassOceanLoad3D (point/mass/MassOceanLoad3D.cpp, built in GLLPoint.cpp:74-87) where the
+   ocean mass or the surface normal varies with phi: per slice, accel = F / m - (F . k) k with
+   k = sqrt(m0 / (m (m + m0))) n; m = the point's own masses (1-D or Mass3D), m0 and the unit
+   normal (s, phi, z) given per slice: nr values of mass_ocean (3 nr of normal) from offset[i] */
+int  axg_set_ocean_load3d(axg_solver *h, int32_t count, const int32_t *point, const int64_t *offset,
+                          int64_t nvalues, const double *mass_ocean, const double *normal);
 /* builds buckets, uploads to HBM; must precede any time-loop call */
 int  axg_finalize(axg_solver *h);
 

@@ -279,6 +279,9 @@ struct PointSet {
     std::vector<double> mass1;               // 1-D mass (double), for MassOceanLoad1D
     std::vector<int> ocean;                  // index into ocean_c, -1 = none
     std::vector<std::array<R, 4>> ocean_c;   // (ss, zz, sz, pp)
+    std::vector<int> ocean3;                 // index into ocean3_c, -1 = none
+    std::vector<std::vector<R>> ocean3_c;    // [nr][4]: 1/m, k_s, k_phi, k_z
+    std::vector<std::vector<double>> mass3;  // the point's masses per slice (or one)
     std::vector<uint8_t> axial, surface;
     std::vector<Cx<R>> stiff, displ, veloc, accel;
     size_t total = 0;
@@ -287,6 +290,7 @@ struct PointSet {
         n = count; ndim = nd;
         nr.assign(nr_, nr_ + n); nu.resize(n); off.resize(n);
         mass_nr.resize(n); inv_mass.resize(n); mass1.assign(n, 0.0); ocean.assign(n, -1); ocean_c.clear();
+        ocean3.assign(n, -1); ocean3_c.clear(); mass3.assign(n, {});
         axial.assign(n, 0); surface.assign(n, 0);
         size_t o = 0;
         for (int p = 0; p < n; p++) {
@@ -297,6 +301,7 @@ struct PointSet {
             // Mass1D / Mass3D store (Real)(1 / mass)  (Mass1D.hpp:19-21, Mass3D.hpp:19-20)
             for (int k = 0; k < mass_nr[p]; k++) inv_mass[p][k] = (R)(1.0 / mass[mo + k]);
             mass1[p] = mass[mo];
+            mass3[p].assign(mass + mo, mass + mo + mass_nr[p]);
             if (ax) axial[p] = ax[p];
             if (surf) surface[p] = surf[p];
         }
@@ -386,6 +391,8 @@ struct OracleBase {
     virtual void set_clayton(int solid, const axg_clayton *) = 0;
     virtual void set_sponge(int solid, int n, const int32_t *pt, const double *g) = 0;
     virtual void set_ocean_load(int n, const int32_t *pt, const double *mo, const double *theta) = 0;
+    virtual void set_ocean_load3d(int n, const int32_t *pt, const int64_t *off, const double *mo,
+                                  const double *normal) = 0;
     virtual void set_clayton3d(int solid, const axg_clayton3d *c) = 0;
     virtual void set_scanning(const axg_scanning *s) = 0;
     virtual void scanning_nr(int32_t *s, int32_t *f) = 0;
@@ -666,6 +673,24 @@ struct Oracle : OracleBase {
             for (int k = 0; k < nr; k++) x.g.push_back((R)g[off[i] + k]);
             prepare_twiddle(nr);
             (solid ? sg3s : sg3f).push_back(std::move(x));
+        }
+    }
+    // MassOceanLoad3D constructor (MassOceanLoad3D.cpp: in double, cast); after set_solid_points
+    void set_ocean_load3d(int n, const int32_t *pt, const int64_t *off, const double *mo,
+                          const double *normal) override {
+        for (int i = 0; i < n; i++) {
+            const int p = pt[i], nr = sp.nr[p];
+            std::vector<R> c;
+            for (int k = 0; k < nr; k++) {
+                const double mass = sp.mass3[p][sp.mass_nr[p] > 1 ? k : 0];
+                const double m0 = mo[off[i] + k];
+                const double sk = std::sqrt(m0 / (mass * (mass + m0)));
+                c.push_back((R)(1.0 / mass));
+                for (int d = 0; d < 3; d++) c.push_back((R)(sk * normal[(off[i] + k) * 3 + d]));
+            }
+            sp.ocean3[p] = (int)sp.ocean3_c.size();
+            sp.ocean3_c.push_back(std::move(c));
+            prepare_twiddle(nr);
         }
     }
     // MassOceanLoad1D constructor (coefficients in double, cast); after set_solid_points
@@ -1119,7 +1144,29 @@ struct Oracle : OracleBase {
             int nu = ps.nu[p], nr = ps.nr[p];
             if (nr % 2 == 0)
                 for (int c = 0; c < nd; c++) f[(nu - 1) * nd + c].imag(0);
-            if (ps.ocean.size() && ps.ocean[p] >= 0) {
+            if (ps.ocean3.size() && ps.ocean3[p] >= 0) {
+                // MassOceanLoad3D::computeAccel (MassOceanLoad3D.cpp)
+                const std::vector<R> &c = ps.ocean3_c[ps.ocean3[p]];
+                const Twiddle<R> &t = twiddle(nr);
+                std::vector<Cx<R>> cb(nu);
+                std::vector<R> fr((size_t)3 * nr);
+                for (int d = 0; d < 3; d++) {
+                    for (int a = 0; a < nu; a++) cb[a] = f[a * 3 + d];
+                    c2r(cb.data(), nu, &fr[(size_t)d * nr], nr, t);
+                }
+                for (int k = 0; k < nr; k++) {
+                    const R f0 = fr[k], f1 = fr[nr + k], f2 = fr[2 * nr + k];
+                    const R *q = &c[(size_t)4 * k];
+                    const R dot = f0 * q[1] + f1 * q[2] + f2 * q[3];
+                    fr[k] = q[0] * f0 - dot * q[1];
+                    fr[nr + k] = q[0] * f1 - dot * q[2];
+                    fr[2 * nr + k] = q[0] * f2 - dot * q[3];
+                }
+                for (int d = 0; d < 3; d++) {
+                    r2c(&fr[(size_t)d * nr], nr, cb.data(), nu, t);
+                    for (int a = 0; a < nu; a++) f[a * 3 + d] = cb[a];
+                }
+            } else if (ps.ocean.size() && ps.ocean[p] >= 0) {
                 // MassOceanLoad1D::computeAccel (MassOceanLoad1D.hpp)
                 const std::array<R, 4> &c = ps.ocean_c[ps.ocean[p]];
                 for (int a = 0; a < nu; a++) {
@@ -1428,6 +1475,7 @@ int axo_set_stations(void *h, const axg_stations *s, int interval) { AXO_TRY(sta
 int axo_set_clayton(void *h, int solid, const axg_clayton *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton(solid, c)) }
 int axo_set_sponge(void *h, int solid, int n, const int32_t *pt, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge(solid, n, pt, g)) }
 int axo_set_ocean_load(void *h, int n, const int32_t *pt, const double *mo, const double *theta) { AXO_TRY(static_cast<OracleBase *>(h)->set_ocean_load(n, pt, mo, theta)) }
+int axo_set_ocean_load3d(void *h, int n, const int32_t *pt, const int64_t *off, const double *mo, const double *nrm) { AXO_TRY(static_cast<OracleBase *>(h)->set_ocean_load3d(n, pt, off, mo, nrm)) }
 int axo_set_scanning(void *h, const axg_scanning *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_scanning(s)) }
 int axo_scanning_nr(void *h, int32_t *s, int32_t *f) { AXO_TRY(static_cast<OracleBase *>(h)->scanning_nr(s, f)) }
 int axo_set_clayton3d(void *h, int solid, const axg_clayton3d *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton3d(solid, c)) }

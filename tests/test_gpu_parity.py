@@ -418,7 +418,7 @@ def test_mass3d_and_ocean_load_hooks_equal_graph(built):
 
 
 def test_ocean_load_errors(built):
-    """Ocean load on a Mass3D point, twice on one point, or out of range: host-side errors."""
+    """A 1-D ocean load on a Mass3D point, or twice on one point: host-side errors."""
     from axisem3d_b200 import _lib as L, meshgen
     from axisem3d_b200.solver import Solver, EngineError
     m = meshgen.cartesian_model(nx=3, nz=3, nr=4)
@@ -426,7 +426,7 @@ def test_ocean_load_errors(built):
     bad3d = meshgen.with_mass3d(m, seed=1)          # ocean points get 3-D masses too
     with pytest.raises(EngineError) as ei:
         Solver(bad3d, "fp32")
-    assert ei.value.code == L.AXG_E_UNSUPPORTED and "MassOceanLoad3D" in str(ei.value)
+    assert ei.value.code == L.AXG_E_ARG and "3-D ocean load" in str(ei.value)
     pt, mo, th = m.ocean_load
     m.ocean_load = (np.concatenate([pt, pt[:1]]), np.concatenate([mo, mo[:1]]), np.concatenate([th, th[:1]]))
     with pytest.raises(EngineError) as ei:
@@ -567,3 +567,42 @@ def test_wavefield_scanning_prescribed_history(built, precision):
             s.record_stations(t)
         s_nr, _ = s.scanning_nr()
     assert np.all(s_nr == 9), np.unique(s_nr)
+
+
+def _ocean3d_model():
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=6, nz=6, nr=6,
+                                attenuation=dict(meshgen.default_sls(3), qkappa=57823.0, qmu=100.0))
+    meshgen.add_ocean_load3d(m, 6, 6, 100e3, seed=2)
+    return meshgen.with_mass3d(m, amp=0.05, seed=2)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("fp32", 1e-5), ("mixed", 1e-5)])
+def test_ocean_load3d_parity(built, precision, tol):
+    """MassOceanLoad3D (per-slice ocean masses and tilted normals) on surface points whose own
+    masses are 3-D: five full steps vs the oracle; the per-hook path equals the graph."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = _ocean3d_model()
+    u0 = meshgen.random_displacement(m, seed=8) * 1e-3
+    o = O.Oracle(m, "fp64")
+    o.set_field(u0, "displ")
+    o.run(5)
+    with Solver(m, precision) as s:
+        s.set_field(u0, "displ")
+        s.run(5)
+        for f in ("displ", "veloc", "accel"):
+            assert rel(s.get_field(f), o.get_field(f)) <= tol, (f, rel(s.get_field(f), o.get_field(f)))
+    if precision == "fp64":
+        with Solver(m, "fp64") as s:
+            s.set_field(u0, "displ")
+            for t in range(5):
+                s.apply_sources(t)
+                s.compute_stiffness()
+                s.apply_bc_before_assembly()
+                s.record_stations(t)
+                s.apply_bc_after_assembly()
+                s.stiff_to_accel()
+                s.newmark_update()
+            assert rel(s.get_field("displ"), o.get_field("displ")) <= tol

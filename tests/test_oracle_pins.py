@@ -314,3 +314,27 @@ def test_scanning_peak_and_mode_count():
         o.record_stations(t)
     s_nr, _ = o.scanning_nr()
     assert np.all(s_nr == 9), np.unique(s_nr)
+
+
+def test_ocean_load3d_reduces_to_1d():
+    """MassOceanLoad3D with the same ocean mass on every slice and a vertical normal equals
+    MassOceanLoad1D with theta = 0 (to rounding): five oracle steps in FP64."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    m1 = meshgen.cartesian_model(nx=5, nz=5, nr=6)
+    meshgen.add_ocean_load(m1, 5, 5, 100e3)
+    m3 = meshgen.cartesian_model(nx=5, nz=5, nr=6)
+    pts, mo, _ = m1.ocean_load
+    nr = np.asarray(m3.sp_nr)[pts]
+    off = np.concatenate([[0], np.cumsum(nr)[:-1]]).astype(np.int64)
+    nrm = np.zeros((int(nr.sum()), 3))
+    nrm[:, 2] = 1.0
+    m3.ocean_load3d = (pts, off, np.repeat(mo, nr), nrm)
+    u0 = meshgen.random_displacement(m1, seed=4) * 1e-3
+    out = []
+    for m in (m1, m3):
+        o = O.Oracle(m, "fp64")
+        o.set_field(u0, "displ")
+        o.run(5)
+        out.append(o.get_field("displ"))
+    assert np.linalg.norm(out[1] - out[0]) <= 1e-12 * np.linalg.norm(out[0])
