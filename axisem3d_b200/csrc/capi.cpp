@@ -334,6 +334,21 @@ int axg_set_sponge3d(axg_solver *h, int32_t solid, int32_t count, const int32_t 
     });
 }
 
+int axg_set_prt(axg_solver *h, int32_t count, const int32_t *element, const int64_t *offset,
+                const uint8_t *is3d_prt, int64_t nvalues, const double *x) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (count < 0 || nvalues < 0 || (count && (!element || !offset || !is3d_prt || !x)))
+            throw axg::Error(AXG_E_ARG, "PRT || missing array.");
+        axg::HostPrt &p = h->model.prt;
+        p.count = count;
+        p.elem = copy(element, count);
+        p.off = copy(offset, count);
+        p.x3d = copy(is3d_prt, count);
+        p.x = copy(x, nvalues);
+    });
+}
+
 int axg_set_scanning(axg_solver *h, const axg_scanning *sc) {
     return guarded(h, [&] {
         need_open(h);
@@ -491,6 +506,22 @@ int axg_finalize(axg_solver *h) {
                 if (p < 0 || p >= np) throw axg::Error(AXG_E_ARG, "WavefieldScanning || point index out of range.");
                 if (seen[p]) throw axg::Error(AXG_E_ARG, "WavefieldScanning || point listed twice.");
                 seen[p] = 1;
+            }
+        }
+        {
+            // PRT: one per element, sizes, 3-D factors on 3-D elements only
+            std::vector<char> seen(m.se.count, 0);
+            for (int i = 0; i < m.prt.count; i++) {
+                const int e = m.prt.elem[i];
+                if (e < 0 || e >= m.se.count) throw axg::Error(AXG_E_ARG, "PRT || element index out of range.");
+                if (seen[e]) throw axg::Error(AXG_E_ARG, "PRT || element listed twice.");
+                seen[e] = 1;
+                const bool e3d = m.se.is3d.size() && m.se.is3d[e];
+                if (m.prt.x3d[i] && !e3d)
+                    throw axg::Error(AXG_E_ARG, "PRT::checkCompatibility || 3-D PRT on a 1-D element.");
+                const int64_t ns = m.prt.x3d[i] ? m.se.nr[e] : 1;
+                if (m.prt.off[i] < 0 || m.prt.off[i] + 5 * ns * 25 > (int64_t)m.prt.x.size())
+                    throw axg::Error(AXG_E_ARG, "PRT::checkCompatibility || Incompatible sizes.");
             }
         }
         // one Sponge per point (GLLPoint::release averages the boundaries' gammas first)

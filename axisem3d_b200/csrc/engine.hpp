@@ -85,6 +85,14 @@ struct HostSponge3D {
     std::vector<double> gamma;
 };
 
+struct HostPrt {
+    int count = 0;
+    std::vector<int> elem;
+    std::vector<int64_t> off;
+    std::vector<uint8_t> x3d;
+    std::vector<double> x;       // per element from off: [5][nslice][25] X0..X3, |J|
+};
+
 struct HostScanning {
     bool enabled = false;
     double tol_fourier_h1 = 0, rel_tol_h1 = 0, abs_tol_h1 = 0;
@@ -119,6 +127,7 @@ struct HostModel {
     HostOcean ocean;
     HostOcean3D ocean3;
     HostScanning scan;
+    HostPrt prt;
     HostSponge sg_s, sg_f;
     HostPoints sp, fp;
     HostSolidElements se;

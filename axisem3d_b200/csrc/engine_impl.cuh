@@ -12,6 +12,7 @@
 #include "adjoint_kernel.cuh"
 #include "fluid_kernel.cuh"
 #include "point_kernels.cuh"
+#include "prt_kernel.cuh"
 #include "solid_kernel.cuh"
 
 #include <algorithm>
@@ -117,6 +118,12 @@ class Engine final : public EngineBase {
         DBuf<int64_t> mod_off, att_off, state_off;
         double bytes = 0, flops = 0;
         void (*kernel)(const SolidArgs<T, AT>, int, int, int, size_t) = nullptr;
+        // particle relabelling (undulated geometry): its own kernel and factors
+        int prt = 0;
+        DBuf<T> xpool;
+        DBuf<int64_t> xoff;
+        DBuf<uint8_t> x3d;
+        void (*pkernel)(const PrtArgs<T, AT>, int, int, int, size_t) = nullptr;
     };
     struct FluidBucket {
         int is3d, cls, team, tpc, nr_max, n;
@@ -544,9 +551,7 @@ public:
             a.nwave = 1;
             a.fstride = 0;
             a.sstride = 0;
-            b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc,
-                                                                              b.tpc, b.team_bytes);
-            post_launch();
+            launch_solid_args(b, a);
         }
         for (auto &bp : fb_) {
             FluidBucket &b = *bp;
@@ -571,6 +576,7 @@ private:
         const HostSolidElements &h = model_.se;
         if (fp_.n > 0) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || fluid elements are not differentiated.");
         if (nwave_ != 1) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || one wavefield per handle.");
+        if (model_.prt.count) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || PRT elements are not differentiated.");
         for (int e = 0; e < h.count; e++) {
             bool ok = h.rheo[e] == AXG_ISO && !(h.is3d.size() && h.is3d[e]) &&
                       !(h.att.size() && h.att[e] != AXG_ATT_NONE);
@@ -791,25 +797,55 @@ private:
         }
     }
 
+    using PrtKernel = void (*)(const PrtArgs<T, AT>, int, int, int, size_t);
+    template <int RHEO, int ATT>
+    static PrtKernel pick_prt2(bool is3d, bool rtz) {
+        if (is3d) return rtz ? solid_prt_kernel<T, AT, RHEO, ATT, true, true> : solid_prt_kernel<T, AT, RHEO, ATT, true, false>;
+        return rtz ? solid_prt_kernel<T, AT, RHEO, ATT, false, true> : solid_prt_kernel<T, AT, RHEO, ATT, false, false>;
+    }
+    template <int RHEO>
+    static PrtKernel pick_prt1(int att, bool is3d, bool rtz) {
+        switch (att) {
+            case ATT_NONE: return pick_prt2<RHEO, ATT_NONE>(is3d, rtz);
+            case ATT_FULL: return pick_prt2<RHEO, ATT_FULL>(is3d, rtz);
+            default: return pick_prt2<RHEO, ATT_CG4>(is3d, rtz);
+        }
+    }
+    static PrtKernel pick_prt(int rheo, int att, bool is3d, bool rtz) {
+        switch (rheo) {
+            case RHEO_ISO: return pick_prt1<RHEO_ISO>(att, is3d, rtz);
+            case RHEO_TISO: return pick_prt1<RHEO_TISO>(att, is3d, rtz);
+            default: return pick_prt1<RHEO_ANISO>(att, is3d, rtz);
+        }
+    }
+
     int nmod_of(int rheo) const { return rheo == RHEO_ISO ? 2 : rheo == RHEO_TISO ? 5 : 21; }
 
     void build_solid_buckets(const HostSolidElements &h) {
-        // group elements by (rheology, attenuation, 1-D/3-D, RTZ, nr class)
-        std::map<std::tuple<int, int, int, int, int>, std::vector<int>> groups;
+        // group elements by (rheology, attenuation, 1-D/3-D, RTZ, nr class, PRT)
+        const HostPrt &hp = model_.prt;
+        std::vector<int> prt_of(h.count, -1);
+        for (int i = 0; i < hp.count; i++) prt_of[hp.elem[i]] = i;
+        std::map<std::tuple<int, int, int, int, int, int>, std::vector<int>> groups;
         for (int e = 0; e < h.count; e++) {
             int att = h.att.size() ? h.att[e] : ATT_NONE;
             int is3d = h.is3d.size() ? h.is3d[e] : 0;
             int rtz = h.rtz.size() ? h.rtz[e] : 0;
-            if (h.rheo[e] == RHEO_ISO) rtz = 0;   // isotropic rheology is frame invariant
+            const int prt = prt_of[e] >= 0 ? 1 : 0;
+            // isotropic rheology is frame invariant; with PRT the RTZ frame carries the factors
+            if (h.rheo[e] == RHEO_ISO && !prt) rtz = 0;
             if (att != ATT_NONE && cfg_.nsls <= 0)
                 throw Error(AXG_E_ARG, "Attenuation::checkCompatibility || nsls must be > 0.");
-            groups[{h.rheo[e], att, is3d, rtz, cfg_.plain ? 0 : nr_class(h.nr[e])}].push_back(e);
+            groups[{h.rheo[e], att, is3d, rtz, cfg_.plain ? 0 : nr_class(h.nr[e]), prt}].push_back(e);
         }
         int64_t state_total = 0;
         std::vector<std::vector<int64_t>> state_offs;
         for (auto &kv : groups) {
             auto b = std::make_unique<SolidBucket>();
-            std::tie(b->rheo, b->att, b->is3d, b->rtz, b->cls) = kv.first;
+            std::tie(b->rheo, b->att, b->is3d, b->rtz, b->cls, b->prt) = kv.first;
+            std::vector<T> xpool;
+            std::vector<int64_t> xoff;
+            std::vector<uint8_t> x3d;
             const std::vector<int> &ids = kv.second;
             b->n = (int)ids.size();
             b->nr_max = 1;
@@ -869,6 +905,21 @@ private:
                     bytes += 2.0 * (cfg_.nsls + 1) * 6 * slots * sa * nwave_;   // state read + write
                 }
                 if (b->rtz) bytes += 25 * s;                              // theta
+                if (b->prt) {
+                    // PRT factors X0..X3 and their |J|-scaled copies (PRT.hpp constructor: the
+                    // products formed in double, then cast)
+                    const int i = prt_of[e];
+                    const int xns = hp.x3d[i] ? enr : 1;
+                    const double *x = &hp.x[hp.off[i]];
+                    const size_t xs = (size_t)xns * 25;
+                    xoff.push_back((int64_t)xpool.size());
+                    x3d.push_back(hp.x3d[i]);
+                    for (int c = 0; c < 4; c++)
+                        for (size_t j = 0; j < xs; j++) xpool.push_back((T)x[c * xs + j]);
+                    for (int c = 0; c < 4; c++)
+                        for (size_t j = 0; j < xs; j++) xpool.push_back((T)(x[c * xs + j] * x[4 * xs + j]));
+                    bytes += 8.0 * xs * s;
+                }
                 flops += nwave_ * (double)enu * 25 * (2 * 3 * 10 * 4 + 60);   // gradient
                 flops += nwave_ * (double)enu * 25 * (2 * 3 * 10 * 4 + 60);   // quadrature
                 double pw = nm == 2 ? 16 : nm == 5 ? 22 : 72;             // stress per point
@@ -892,7 +943,12 @@ private:
             b->mod.upload(mod); b->attmod.upload(attm);
             b->mod_off.upload(moff); b->att_off.upload(aoff);
             state_offs.push_back(soff);
-            b->kernel = pick_solid(b->rheo, b->att, b->is3d, b->rtz, cfg_.nsls);
+            if (b->prt) {
+                b->xpool.upload(xpool); b->xoff.upload(xoff); b->x3d.upload(x3d);
+                b->pkernel = pick_prt(b->rheo, b->att, b->is3d, b->rtz);
+            } else {
+                b->kernel = pick_solid(b->rheo, b->att, b->is3d, b->rtz, cfg_.nsls);
+            }
             configure_bucket(*b);
             sb_.push_back(std::move(b));
         }
@@ -908,12 +964,17 @@ private:
     void configure_bucket(SolidBucket &b, int team_req = 0) {
         int team = team_req ? team_req
                             : (cfg_.plain ? 256 : (team_override_[b.cls] ? team_override_[b.cls] : default_team(b.cls)));
-        // shared memory per team; split the 25 points of the slice phase if needed
+        // shared memory per team (the PRT kernel holds 9 gradient components instead of 6)
+        auto bytes_of = [&](int q) {
+            return b.prt ? prt_layout<T>(b.nr_max, q).total : team_layout<T>(b.nr_max, q).total;
+        };
+        const void *kfn = b.prt ? (const void *)b.pkernel : (const void *)b.kernel;
+        // split the 25 points of the slice phase if needed
         const size_t budget = 200 * 1024;
         int qc = 25;
-        TeamLayout L = team_layout<T>(b.nr_max, qc);
-        while (L.total > budget / 1 && qc > 1) { qc = (qc + 1) / 2; L = team_layout<T>(b.nr_max, qc); }
-        if (L.total > budget)
+        size_t total = bytes_of(qc);
+        while (total > budget && qc > 1) { qc = (qc + 1) / 2; total = bytes_of(qc); }
+        if (total > budget)
             throw Error(AXG_E_UNSUPPORTED, "SolidElement::expandWorkspace || nr too large for shared memory.");
 #if AXG_QC_FOR_TWO_CTAS
         // a one-element CTA too large for two per SM: smaller point chunks of the slice phase
@@ -922,24 +983,24 @@ private:
         if (team >= 128 && b.is3d) {
             const size_t two_per_sm = 110 * 1024;
             int qn = qc;
-            TeamLayout Ln = L;
-            while (qn > 5 && Ln.total > two_per_sm) {
-                const TeamLayout Lh = team_layout<T>(b.nr_max, (qn + 1) / 2);
-                if (Lh.total >= Ln.total) break;
+            size_t tn = total;
+            while (qn > 5 && tn > two_per_sm) {
+                const size_t th = bytes_of((qn + 1) / 2);
+                if (th >= tn) break;
                 qn = (qn + 1) / 2;
-                Ln = Lh;
+                tn = th;
             }
-            if (Ln.total <= two_per_sm) { qc = qn; L = Ln; }
+            if (tn <= two_per_sm) { qc = qn; total = tn; }
         }
 #endif
         b.qc = qc;
-        b.team_bytes = L.total;
+        b.team_bytes = total;
         b.team = team;
         int tpc = std::max(1, 256 / team);
-        while (tpc > 1 && (size_t)tpc * L.total > budget) tpc--;
+        while (tpc > 1 && (size_t)tpc * total > budget) tpc--;
         if (team > 32) tpc = std::min(tpc, 15);
         b.tpc = tpc;
-        raise_smem_limit((const void *)b.kernel, tpc * L.total);
+        raise_smem_limit(kfn, tpc * total);
         // one CTA per group of tpc elements: measured faster on B200 than a persistent grid
         // (the hardware scheduler refills an SM as soon as any CTA ends, which hides the
         // tail of uneven nr better than a fixed walk). AXG_PERSISTENT_GRID restores the
@@ -947,9 +1008,8 @@ private:
         b.grid = (b.n + tpc - 1) / tpc;
 #ifdef AXG_PERSISTENT_GRID
         int per_sm = 0;
-        AXG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b.kernel, team * tpc,
-                                                               tpc * L.total));
-        if (!cfg_.plain)
+        AXG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, team * tpc, tpc * total));
+        if (!cfg_.plain && !b.prt)
             b.grid = std::max(1, std::min(b.grid, std::max(1, per_sm) * prop_.multiProcessorCount));
 #endif
     }
@@ -1441,10 +1501,23 @@ private:
             a.nwave = nwave_;
             a.fstride = (size_t)sp_.total * 3;
             a.sstride = (size_t)state_wave_;
-            b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc,
-                                                                              b.tpc, b.team_bytes);
-            post_launch();
+            launch_solid_args(b, a);
         }
+    }
+
+    // one solid bucket's kernel with the given arguments (the PRT kernel takes the bucket's
+    // factors on top)
+    void launch_solid_args(SolidBucket &b, const SolidArgs<T, AT> &a) {
+        if (b.prt) {
+            PrtArgs<T, AT> pa;
+            pa.s = a; pa.x = b.xpool.p; pa.x_off = b.xoff.p; pa.x3d = b.x3d.p;
+            b.pkernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(pa, b.nr_max, b.qc, b.tpc,
+                                                                               b.team_bytes);
+        } else {
+            b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc, b.tpc,
+                                                                              b.team_bytes);
+        }
+        post_launch();
     }
 
     void launch_fluid() {

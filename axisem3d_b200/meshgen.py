@@ -478,6 +478,32 @@ def add_ocean_load3d(m, nx, nz, width, rho_water=1020.0, depth_water=3000.0, amp
     return m
 
 
+def add_prt(m, elements=None, amp=0.05, three_d=False, seed=0):
+    """Particle-relabelling factors on `elements` (default: every solid element): J^-1
+    components X0 = 1 + a, X1 = b, X2 = c, X3 = 1 + d and |J| = 1 / (X0 X3), with a, b, c, d
+    seeded and of size `amp` per point (and per slice with three_d, which needs 3-D
+    elements). Synthetic: a smooth near-identity relabelling for parity of the PRT path."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ne = m.n_solid_elements
+    el = np.arange(ne, dtype=np.int32) if elements is None else np.asarray(elements, np.int32)
+    off, x3, xs = [], [], []
+    o = 0
+    for e in el:
+        ns = int(m.se_nr[e]) if three_d else 1
+        X0 = 1.0 + amp * rng.uniform(-1, 1, (ns, 25))
+        X1 = amp * rng.uniform(-1, 1, (ns, 25))
+        X2 = amp * rng.uniform(-1, 1, (ns, 25))
+        X3 = 1.0 + amp * rng.uniform(-1, 1, (ns, 25))
+        XJ = 1.0 / (X0 * X3)
+        off.append(o)
+        x3.append(1 if three_d else 0)
+        xs.append(np.stack([X0, X1, X2, X3, XJ]).ravel())
+        o += 5 * ns * 25
+    m.prt = {"element": el, "offset": np.array(off, np.int64), "is3d_prt": np.array(x3, np.uint8),
+             "x": np.concatenate(xs)}
+    return m
+
+
 def with_mass3d(m, amp=0.05, seed=0, exclude=()):
     """A copy of `m` whose solid points with nr >= 2 (except `exclude`) carry 3-D masses
     (Mass3D): the point's mass times (1 + amp * U(-1, 1)) per slice, seeded."""

@@ -126,6 +126,9 @@ class Model:
     # wavefield scanning: dict(tol_fourier_h1, rel_tol_h1, abs_tol_h1, max_num_peaks, interval,
     # solid_points=None (all), fluid_points=None (all))
     scanning: Optional[dict] = None
+    # PRT (undulated geometry): dict(element, offset, is3d_prt, x) with x per element
+    # [5][nslice][25] (X0..X3, |J|) from offset
+    prt: Optional[dict] = None
     cl3_solid: Optional[dict] = None
     cl3_fluid: Optional[dict] = None
     sponge3d_solid: Optional[tuple] = None
@@ -320,6 +323,16 @@ class Model:
                     setattr(c, key, k(pk, pts, _i32, C.c_int32))
             return c
 
+        def prt():
+            d = self.prt
+            if not d:
+                return None
+            e, off = _i32(d["element"]), _i64(d["offset"])
+            x3 = np.ascontiguousarray(d["is3d_prt"], dtype=np.uint8)
+            x = _f64(np.asarray(d["x"]).ravel())
+            keep["prt_e"], keep["prt_off"], keep["prt_x3"], keep["prt_x"] = e, off, x3, x
+            return (e, off, x3, x)
+
         def ocean3():
             if not self.ocean_load3d:
                 return None
@@ -345,7 +358,7 @@ class Model:
         return {"sp": sp, "fp": fp, "se": se, "fe": fe, "sf": sf, "ms": ms, "fs": fs, "st": st,
                 "cl_s": clay("cls", self.cl_solid, True), "cl_f": clay("clf", self.cl_fluid, False),
                 "sg_s": sponge("sgs", self.sponge_solid), "sg_f": sponge("sgf", self.sponge_fluid),
-                "ocean": ocean(), "scan": scan(), "ocean3": ocean3(),
+                "ocean": ocean(), "scan": scan(), "ocean3": ocean3(), "prt": prt(),
                 "cl3_s": clay3("c3s", self.cl3_solid, True), "cl3_f": clay3("c3f", self.cl3_fluid, False),
                 "sg3_s": sponge3("g3s", self.sponge3d_solid), "sg3_f": sponge3("g3f", self.sponge3d_fluid),
                 "keep": keep}

@@ -303,6 +303,14 @@ int  axg_set_scanning(axg_solver *h, const axg_scanning *s);
    min(2 nu + 1, nr) of the peaks found, 1 where no peak passed, -1 for unscanned points;
    solid_nr [solid points], fluid_nr [fluid points] (either may be NULL) */
 int  axg_scanning_nr(axg_solver *h, int32_t *solid_nr, int32_t *fluid_nr);
+/* particle relabelling transformation on solid elements under topography (PRT, PRT/PRT.hpp;
+   SolidElement::displToStiff's PRT branch, SolidElement.cpp:113-161): element[i] takes the
+   J^-1 components X0..X3 and |J| (PRT constructor arguments) from x[offset[i]...] as
+   [5][nslice][25] doubles, nslice = 1 (is3d_prt[i] = 0) or the element's nr (a 3-D PRT, which
+   needs a 3-D element, axg_solid_elements.is3d); nvalues = length of x. On a spherical element
+   (rtz) the 9-component gradient is taken to the RTZ frame first whatever the rheology. */
+int  axg_set_prt(axg_solver *h, int32_t count, const int32_t *element, const int64_t *offset,
+                 const uint8_t *is3d_prt, int64_t nvalues, const double *x);
 /* MassOceanLoad1D (point/mass/MassOceanLoad1D.hpp, built in GLLPoint.cpp:66-73) on solid
    surface points under an ocean:
    in computeStiffToAccel the point's own mass acts along the surface and mass + mass_ocean

@@ -33,6 +33,7 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -196,6 +197,38 @@ struct Grad {
         quad_overS(A1, f[1], integrate);
         quad_overS(A2, f[2], integrate);
     }
+    // computeGrad9 (GradientQuadrature.hpp:181-205): ui_j with j = d/ds, 1/s terms, d/dz
+    void grad9(const CM<R> u[3], CM<R> g[9], int alpha) const {
+        dSdZ(u[0], g[0], g[2]);
+        dSdZ(u[1], g[3], g[5]);
+        dSdZ(u[2], g[6], g[8]);
+        CM<R> A0, A1, A2;
+        for (int i = 0; i < P; i++)
+            for (int j = 0; j < P; j++) {
+                A0.a[i][j] = ia(alpha, u[0].a[i][j]) - u[1].a[i][j];
+                A1.a[i][j] = ia(alpha, u[1].a[i][j]) + u[0].a[i][j];
+                A2.a[i][j] = ia(alpha, u[2].a[i][j]);
+            }
+        overS(A0, g[1], false);
+        overS(A1, g[4], false);
+        overS(A2, g[7], false);
+    }
+    // computeQuad9 (GradientQuadrature.hpp:258-292)
+    void quad9(const CM<R> s[9], CM<R> f[3], int alpha) const {
+        quad_dSdZ(s[0], s[2], f[0], true);
+        quad_dSdZ(s[3], s[5], f[1], true);
+        quad_dSdZ(s[6], s[8], f[2], true);
+        CM<R> A0, A1, A2;
+        for (int i = 0; i < P; i++)
+            for (int j = 0; j < P; j++) {
+                A0.a[i][j] = ia(alpha, s[1].a[i][j]) - s[4].a[i][j];
+                A1.a[i][j] = ia(alpha, s[4].a[i][j]) + s[1].a[i][j];
+                A2.a[i][j] = ia(alpha, s[7].a[i][j]);
+            }
+        quad_overS(A0, f[0], true);
+        quad_overS(A1, f[1], true);
+        quad_overS(A2, f[2], true);
+    }
     // computeGrad3 (GradientQuadrature.hpp:163-175)
     void grad3(const CM<R> &p, CM<R> q[3], int alpha) const {
         dSdZ(p, q[0], q[2]);
@@ -327,6 +360,9 @@ struct SolidElem {
     std::vector<R> dstressC;       // [nr][6][npa]
     std::vector<R> memC;           // [nsls][nr][6][npa]
     R sin1[N], cos1[N], sin2[N], cos2[N];
+    // PRT: X0..X3 then X0|J|..X3|J|, [8][xns][25]
+    int prt = 0, prt3 = 0;
+    std::vector<R> X;
 };
 
 template <class R>
@@ -395,6 +431,7 @@ struct OracleBase {
                                   const double *normal) = 0;
     virtual void set_clayton3d(int solid, const axg_clayton3d *c) = 0;
     virtual void set_scanning(const axg_scanning *s) = 0;
+    virtual void set_prt(int n, const int32_t *elem, const int64_t *off, const uint8_t *x3d, const double *x) = 0;
     virtual void scanning_nr(int32_t *s, int32_t *f) = 0;
     virtual void set_sponge3d(int solid, int n, const int32_t *pt, const int64_t *off, const double *g) = 0;
     virtual void apply_sources(int tstep) = 0;
@@ -645,6 +682,22 @@ struct Oracle : OracleBase {
             }
         }
     }
+    // PRT constructor (PRT.hpp): X0..X3 cast, X_k |J| formed in double then cast
+    void set_prt(int n, const int32_t *elem, const int64_t *off, const uint8_t *x3d, const double *x) override {
+        for (int i = 0; i < n; i++) {
+            SolidElem<R> &el = se[elem[i]];
+            el.prt = 1;
+            el.prt3 = x3d[i];
+            const size_t xs = (size_t)(el.prt3 ? el.nr : 1) * N;
+            const double *xv = x + off[i];
+            el.X.resize(8 * xs);
+            for (int c = 0; c < 4; c++)
+                for (size_t j = 0; j < xs; j++) {
+                    el.X[c * xs + j] = (R)xv[c * xs + j];
+                    el.X[(4 + c) * xs + j] = (R)(xv[c * xs + j] * xv[4 * xs + j]);
+                }
+        }
+    }
     // ClaytonSolid3D / ClaytonFluid3D constructors (in double, cast); after the points
     void set_clayton3d(int solid, const axg_clayton3d *c) override {
         for (int i = 0; i < c->count; i++) {
@@ -843,9 +896,179 @@ struct Oracle : OracleBase {
         s[5] = s[5] * c1 + t3 * s1;
     }
 
+    // PRT::sphericalToUndulated6 / undulatedToSpherical6 (PRT/PRT.hpp)
+    template <class V>
+    static void sph2und(const V g[9], V u[6], R X0, R X1, R X2, R X3) {
+        u[0] = g[0] * X0 + g[2] * X1;
+        u[1] = g[4] * X0 + g[5] * X2;
+        u[2] = g[8] * X3;
+        u[3] = g[7] * X0 + g[8] * X2 + g[5] * X3;
+        u[4] = g[6] * X0 + g[8] * X1 + g[2] * X3;
+        u[5] = (g[3] + g[1]) * X0 + g[5] * X1 + g[2] * X2;
+    }
+    template <class V>
+    static void und2sph(const V u[6], V g[9], R X0, R X1, R X2, R X3) {
+        g[0] = u[0] * X0;
+        g[1] = u[5] * X0;
+        g[2] = u[0] * X1 + u[4] * X3 + u[5] * X2;
+        g[3] = g[1];
+        g[4] = u[1] * X0;
+        g[5] = u[1] * X2 + u[3] * X3 + u[5] * X1;
+        g[6] = u[4] * X0;
+        g[7] = u[3] * X0;
+        g[8] = u[2] * X3 + u[3] * X2 + u[4] * X1;
+    }
+    // CoordTransformSpherical::transformSPZ_RTZ9 / transformRTZ_SPZ9 (CoordTransformSpherical.hpp:102-183)
+    static void rtz9(Cx<R> n[9], R s1, R c1, R s2, R c2, bool to_rtz) {
+        const R half = (R).5;
+        const Cx<R> s08 = n[0] + n[8], d08 = n[0] - n[8], s26 = n[2] + n[6], d26 = n[2] - n[6];
+        if (to_rtz) {
+            n[0] = (s08 + d08 * c2 - s26 * s2) * half;
+            n[2] = (d26 + s26 * c2 + d08 * s2) * half;
+        } else {
+            n[0] = (s08 + d08 * c2 + s26 * s2) * half;
+            n[2] = (d26 + s26 * c2 - d08 * s2) * half;
+        }
+        n[6] = n[2] - d26;
+        n[8] = s08 - n[0];
+        const Cx<R> t1 = n[1], t3 = n[3];
+        if (to_rtz) {
+            n[1] = t1 * c1 - n[7] * s1;
+            n[7] = n[7] * c1 + t1 * s1;
+            n[3] = t3 * c1 - n[5] * s1;
+            n[5] = n[5] * c1 + t3 * s1;
+        } else {
+            n[1] = t1 * c1 + n[7] * s1;
+            n[7] = n[7] * c1 - t1 * s1;
+            n[3] = t3 * c1 + n[5] * s1;
+            n[5] = n[5] * c1 - t3 * s1;
+        }
+    }
+    // attenuation of one (point, mode) (complex V) or (point, slice) (real V) of an element's
+    // state, the same steps as solid_element's
+    template <class V>
+    void att_at(SolidElem<R> &el, int a_or_k, int q, const V e[6], V s[6]) {
+        static const int cg4pt[4] = {6, 8, 16, 18};
+        const int npa = el.att == AXG_ATT_CG4 ? 4 : N;
+        int kk = q;
+        if (el.att == AXG_ATT_CG4) {
+            kk = -1;
+            for (int j = 0; j < 4; j++)
+                if (cg4pt[j] == q) kk = j;
+            if (kk < 0) return;
+        }
+        V dst[6], mem[AXG_MAX_SLS * 6];
+        if constexpr (std::is_same<V, Cx<R>>::value) {
+            const size_t memStride = (size_t)el.nu * 6 * npa;
+            for (int d = 0; d < 6; d++) {
+                dst[d] = el.dstressF[((size_t)a_or_k * 6 + d) * npa + kk];
+                for (int l = 0; l < cfg.nsls; l++) mem[l * 6 + d] = el.memF[l * memStride + ((size_t)a_or_k * 6 + d) * npa + kk];
+            }
+            attenuate(e, s, dst, mem, 6, el.dlam[kk], el.dmu[kk], el.dmu2[kk]);
+            for (int d = 0; d < 6; d++) {
+                el.dstressF[((size_t)a_or_k * 6 + d) * npa + kk] = dst[d];
+                for (int l = 0; l < cfg.nsls; l++) el.memF[l * memStride + ((size_t)a_or_k * 6 + d) * npa + kk] = mem[l * 6 + d];
+            }
+        } else {
+            const size_t memStride = (size_t)el.nr * 6 * npa;
+            for (int d = 0; d < 6; d++) {
+                dst[d] = el.dstressC[((size_t)a_or_k * 6 + d) * npa + kk];
+                for (int l = 0; l < cfg.nsls; l++) mem[l * 6 + d] = el.memC[l * memStride + ((size_t)a_or_k * 6 + d) * npa + kk];
+            }
+            const size_t ao = (size_t)a_or_k * npa + kk;
+            attenuate(e, s, dst, mem, 6, el.dlam[ao], el.dmu[ao], el.dmu2[ao]);
+            for (int d = 0; d < 6; d++) {
+                el.dstressC[((size_t)a_or_k * 6 + d) * npa + kk] = dst[d];
+                for (int l = 0; l < cfg.nsls; l++) el.memC[l * memStride + ((size_t)a_or_k * 6 + d) * npa + kk] = mem[l * 6 + d];
+            }
+        }
+    }
+    // SolidElement::displToStiff, PRT branch (SolidElement.cpp:113-161)
+    void solid_element_prt(SolidElem<R> &el, std::vector<Cx<R>> &elemStiff) {
+        const int nu = el.nu, nr = el.nr;
+        std::vector<CM<R>> U((size_t)nu * 3), G((size_t)nu * 9);
+        for (int q = 0; q < N; q++) {
+            int p = el.pts[q];
+            for (int a = 0; a < nu; a++)
+                for (int c = 0; c < 3; c++)
+                    U[(size_t)a * 3 + c].a[q / P][q % P] =
+                        a < sp.nu[p] ? sp.displ[((size_t)sp.off[p] + a) * 3 + c] : Cx<R>(0);
+        }
+        Grad<R> g{el.ops, gm};
+        for (int a = 0; a < nu; a++) g.grad9(&U[(size_t)a * 3], &G[(size_t)a * 9], a);
+        auto at = [&](int a, int d, int q) -> Cx<R> & { return G[(size_t)a * 9 + d].a[q / P][q % P]; };
+        if (el.rtz)
+            for (int a = 0; a < nu; a++)
+                for (int q = 0; q < N; q++) {
+                    Cx<R> n[9];
+                    for (int d = 0; d < 9; d++) n[d] = at(a, d, q);
+                    rtz9(n, el.sin1[q], el.cos1[q], el.sin2[q], el.cos2[q], true);
+                    for (int d = 0; d < 9; d++) at(a, d, q) = n[d];
+                }
+        const int xns = el.prt3 ? nr : 1;
+        const size_t xs = (size_t)xns * N;
+        auto X = [&](int c, int k, int q) { return el.X[c * xs + (size_t)k * N + q]; };
+        if (!el.is3d) {
+            for (int a = 0; a < nu; a++)
+                for (int q = 0; q < N; q++) {
+                    Cx<R> n[9], eu[6], su[6];
+                    for (int d = 0; d < 9; d++) n[d] = at(a, d, q);
+                    sph2und(n, eu, X(0, 0, q), X(1, 0, q), X(2, 0, q), X(3, 0, q));
+                    elastic(el, 0, q, eu, su);
+                    if (el.att != AXG_ATT_NONE) att_at(el, a, q, eu, su);
+                    und2sph(su, n, X(4, 0, q), X(5, 0, q), X(6, 0, q), X(7, 0, q));
+                    for (int d = 0; d < 9; d++) at(a, d, q) = n[d];
+                }
+        } else {
+            const Twiddle<R> &t = twiddle(nr);
+            std::vector<R> gc((size_t)nr * 9 * N);
+            std::vector<Cx<R>> cbuf(nu);
+            std::vector<R> rbuf(nr);
+            for (int d = 0; d < 9; d++)
+                for (int q = 0; q < N; q++) {
+                    for (int a = 0; a < nu; a++) cbuf[a] = at(a, d, q);
+                    c2r(cbuf.data(), nu, rbuf.data(), nr, t);
+                    for (int k = 0; k < nr; k++) gc[((size_t)k * 9 + d) * N + q] = rbuf[k];
+                }
+            for (int k = 0; k < nr; k++)
+                for (int q = 0; q < N; q++) {
+                    R n[9], eu[6], su[6];
+                    for (int d = 0; d < 9; d++) n[d] = gc[((size_t)k * 9 + d) * N + q];
+                    const int kx = el.prt3 ? k : 0;
+                    sph2und(n, eu, X(0, kx, q), X(1, kx, q), X(2, kx, q), X(3, kx, q));
+                    elastic(el, k, q, eu, su);
+                    if (el.att != AXG_ATT_NONE) att_at(el, k, q, eu, su);
+                    und2sph(su, n, X(4, kx, q), X(5, kx, q), X(6, kx, q), X(7, kx, q));
+                    for (int d = 0; d < 9; d++) gc[((size_t)k * 9 + d) * N + q] = n[d];
+                }
+            for (int d = 0; d < 9; d++)
+                for (int q = 0; q < N; q++) {
+                    for (int k = 0; k < nr; k++) rbuf[k] = gc[((size_t)k * 9 + d) * N + q];
+                    r2c(rbuf.data(), nr, cbuf.data(), nu, t);
+                    for (int a = 0; a < nu; a++) at(a, d, q) = cbuf[a];
+                }
+        }
+        if (el.rtz)
+            for (int a = 0; a < nu; a++)
+                for (int q = 0; q < N; q++) {
+                    Cx<R> n[9];
+                    for (int d = 0; d < 9; d++) n[d] = at(a, d, q);
+                    rtz9(n, el.sin1[q], el.cos1[q], el.sin2[q], el.cos2[q], false);
+                    for (int d = 0; d < 9; d++) at(a, d, q) = n[d];
+                }
+        elemStiff.resize((size_t)nu * 3 * N);
+        for (int a = 0; a < nu; a++) {
+            CM<R> f[3];
+            g.quad9(&G[(size_t)a * 9], f, a);
+            for (int c = 0; c < 3; c++)
+                for (int q = 0; q < N; q++) elemStiff[((size_t)a * 3 + c) * N + q] = f[c].a[q / P][q % P];
+        }
+    }
+
     // ----------------------- SolidElement::computeStiff -----------------------
     void solid_element(SolidElem<R> &el, std::vector<Cx<R>> &elemStiff,
                        std::vector<CM<R>> &S, std::vector<CM<R>> &E) {
+        if (el.prt) { solid_element_prt(el, elemStiff); return; }
         int nu = el.nu, nr = el.nr;
         // collectDisplFromPoints (SolidElement.cpp:101-109, SolidPoint.hpp:82-98)
         std::vector<CM<R>> U((size_t)nu * 3);
@@ -1476,6 +1699,7 @@ int axo_set_clayton(void *h, int solid, const axg_clayton *c) { AXO_TRY(static_c
 int axo_set_sponge(void *h, int solid, int n, const int32_t *pt, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge(solid, n, pt, g)) }
 int axo_set_ocean_load(void *h, int n, const int32_t *pt, const double *mo, const double *theta) { AXO_TRY(static_cast<OracleBase *>(h)->set_ocean_load(n, pt, mo, theta)) }
 int axo_set_ocean_load3d(void *h, int n, const int32_t *pt, const int64_t *off, const double *mo, const double *nrm) { AXO_TRY(static_cast<OracleBase *>(h)->set_ocean_load3d(n, pt, off, mo, nrm)) }
+int axo_set_prt(void *h, int n, const int32_t *e, const int64_t *off, const uint8_t *x3d, const double *x) { AXO_TRY(static_cast<OracleBase *>(h)->set_prt(n, e, off, x3d, x)) }
 int axo_set_scanning(void *h, const axg_scanning *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_scanning(s)) }
 int axo_scanning_nr(void *h, int32_t *s, int32_t *f) { AXO_TRY(static_cast<OracleBase *>(h)->scanning_nr(s, f)) }
 int axo_set_clayton3d(void *h, int solid, const axg_clayton3d *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton3d(solid, c)) }

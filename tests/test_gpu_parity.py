@@ -606,3 +606,73 @@ def test_ocean_load3d_parity(built, precision, tol):
                 s.stiff_to_accel()
                 s.newmark_update()
             assert rel(s.get_field("displ"), o.get_field("displ")) <= tol
+
+
+PRT_GPU = {
+    "cart_iso_1d_full": (lambda m: m.cartesian_model(nx=5, nz=4, nr=8, attenuation=dict(
+        m.default_sls(3), qkappa=57823.0, qmu=120.0)), False),
+    "tiso_3d_full_prt3d": (lambda m: m.microbench_model(n_elem=60, nr_max=32, seed=22, axial_column=True), True),
+    "tiso_3d_full_prt1d": (lambda m: m.microbench_model(n_elem=60, nr_max=32, seed=23), False),
+    "sph_aniso_rtz": (lambda m: m.spherical_model(n_theta=16, n_solid_layers=4, n_fluid_layers=2, nr_max=24,
+                                                  rheology="aniso", attenuation=None), False),
+    "sph_iso_rtz_cg4": (lambda m: m.spherical_model(n_theta=16, n_solid_layers=4, n_fluid_layers=2,
+                                                    nr_max=24), False),
+}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
+@pytest.mark.parametrize("case", sorted(PRT_GPU))
+def test_prt_stiffness_parity(built, case, precision):
+    """Solid elements with particle relabelling (1-D and 3-D factors, on the axis, RTZ frame,
+    FULL / CG4 attenuation): two stiffness evaluations vs the oracle, the tolerances of the
+    other stiffness tests."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    build, three_d = PRT_GPU[case]
+    m = build(meshgen)
+    meshgen.add_prt(m, amp=0.05, three_d=three_d, seed=4)
+    u = meshgen.random_displacement(m, seed=5)
+    uf = meshgen.random_displacement(m, seed=6, solid=False) if len(m.fp_nr) else None
+    ref = []
+    o = O.Oracle(m, "fp64")
+    o.set_field(u, "displ")
+    if uf is not None:
+        o.set_field(uf, "displ", solid=False)
+    for _ in range(2):
+        o.set_field(np.zeros_like(u), "stiff")
+        o.compute_stiffness()
+        ref.append(o.get_field("stiff"))
+    with Solver(m, precision) as s:
+        s.set_field(u, "displ")
+        if uf is not None:
+            s.set_field(uf, "displ", solid=False)
+        for k in range(2):
+            s.set_field(np.zeros_like(u), "stiff")
+            s.compute_stiffness()
+            got = s.get_field("stiff")
+            assert rel(got, ref[k]) <= TOL_STIFF[precision], (k, rel(got, ref[k]))
+
+
+def test_prt_full_steps_and_errors(built):
+    """Five full steps of a PRT model (mixed precision) vs the oracle; a 3-D PRT on a 1-D
+    element and a PRT on an element listed twice are host-side errors."""
+    import oracle as O
+    from axisem3d_b200 import _lib as L, meshgen
+    from axisem3d_b200.solver import Solver, EngineError
+    m = meshgen.cartesian_model(nx=6, nz=6, nr=5,
+                                attenuation=dict(meshgen.default_sls(3), qkappa=57823.0, qmu=100.0))
+    meshgen.add_prt(m, elements=np.arange(0, 36, 2), amp=0.05, seed=7)
+    u0 = meshgen.random_displacement(m, seed=8) * 1e-3
+    o = O.Oracle(m, "fp64")
+    o.set_field(u0, "displ")
+    o.run(5)
+    with Solver(m, "mixed") as s:
+        s.set_field(u0, "displ")
+        s.run(5)
+        assert rel(s.get_field("displ"), o.get_field("displ")) <= 1e-5
+    bad = meshgen.cartesian_model(nx=3, nz=3, nr=5)
+    meshgen.add_prt(bad, three_d=True)
+    with pytest.raises(EngineError) as ei:
+        Solver(bad, "fp32")
+    assert ei.value.code == L.AXG_E_ARG and "3-D PRT on a 1-D element" in str(ei.value)

@@ -338,3 +338,55 @@ def test_ocean_load3d_reduces_to_1d():
         o.run(5)
         out.append(o.get_field("displ"))
     assert np.linalg.norm(out[1] - out[0]) <= 1e-12 * np.linalg.norm(out[0])
+
+
+PRT_CASES = {
+    # name: (model builder, 3-D PRT factors)
+    "cartesian_iso_1d_full": (lambda m: m.cartesian_model(nx=4, nz=4, nr=6, attenuation=dict(
+        m.default_sls(3), qkappa=57823.0, qmu=120.0)), False),
+    "tiso_3d_full_prt3d": (lambda m: m.microbench_model(n_elem=40, nr_max=24, seed=21), True),
+    "sph_aniso_rtz": (lambda m: m.spherical_model(n_theta=16, n_solid_layers=4, n_fluid_layers=2, nr_max=24,
+                                                  rheology="aniso", attenuation=None), False),
+}
+
+
+@pytest.mark.parametrize("name", sorted(PRT_CASES))
+def test_identity_prt_equals_no_prt(built, name):
+    """PRT factors of the identity (X0 = X3 = |J| = 1, X1 = X2 = 0) give the stiffness of the
+    same elements without PRT (two evaluations, attenuation memory included): the
+    9-component gradient, RTZ and quadrature of the PRT branch against the 6-component ones."""
+    import copy
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    build, three_d = PRT_CASES[name]
+    m = build(meshgen)
+    u = meshgen.random_displacement(m, seed=5)
+    mi = copy.copy(m)
+    meshgen.add_prt(mi, amp=0.0, three_d=three_d)
+    out = []
+    for mm in (m, mi):
+        o = O.Oracle(mm, "fp64")
+        o.set_field(u, "displ")
+        for _ in range(2):
+            o.set_field(np.zeros_like(u), "stiff")
+            o.compute_stiffness()
+        out.append(o.get_field("stiff"))
+    assert np.linalg.norm(out[1] - out[0]) <= 1e-14 * np.linalg.norm(out[0])
+
+
+def test_prt_stiffness_is_self_adjoint(built):
+    """With PRT factors (undulatedToSpherical6 scaled by |J| is the transpose of
+    sphericalToUndulated6), the stiffness stays self-adjoint under the azimuthal weights."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=4, nz=4, nr=5)
+    meshgen.add_prt(m, amp=0.08, seed=9)
+    o = O.Oracle(m, "fp64")
+    u = meshgen.random_displacement(m, seed=11)
+    v = meshgen.random_displacement(m, seed=12)
+    nu = np.asarray(m.sp_nr) // 2 + 1
+    w = np.repeat(np.concatenate([np.where(np.arange(k) == 0, 1.0, 2.0) for k in nu]), 3)
+    ku, kv = _stiff(o, u), _stiff(o, v)
+    a = np.sum(w * np.real(np.conj(v) * ku))
+    b = np.sum(w * np.real(np.conj(u) * kv))
+    assert abs(a - b) <= 1e-12 * np.linalg.norm(ku) * np.linalg.norm(v) * 4
