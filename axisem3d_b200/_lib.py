@@ -123,6 +123,7 @@ SIGNATURES = {
     "axg_set_clayton3d": (C.c_int, [H, C.c_int32, C.POINTER(axg_clayton3d)]),
     "axg_set_scanning": (C.c_int, [H, C.POINTER(axg_scanning)]),
     "axg_set_prt": (C.c_int, [H, C.c_int32, P_i32, P_i64, P_u8, C.c_int64, P_f64]),
+    "axg_set_prt_fluid": (C.c_int, [H, C.c_int32, P_i32, P_i64, P_u8, C.c_int64, P_f64, P_f64]),
     "axg_scanning_nr": (C.c_int, [H, P_i32, P_i32]),
     "axg_set_sponge3d": (C.c_int, [H, C.c_int32, C.c_int32, P_i32, P_i64, C.c_int64, P_f64]),
     "axg_finalize": (C.c_int, [H]),

@@ -349,6 +349,22 @@ int axg_set_prt(axg_solver *h, int32_t count, const int32_t *element, const int6
     });
 }
 
+int axg_set_prt_fluid(axg_solver *h, int32_t count, const int32_t *element, const int64_t *offset,
+                      const uint8_t *is3d_prt, int64_t nvalues, const double *x, const double *theta) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (count < 0 || nvalues < 0 || (count && (!element || !offset || !is3d_prt || !x)))
+            throw axg::Error(AXG_E_ARG, "PRT || missing array.");
+        axg::HostPrt &p = h->model.prt_f;
+        p.count = count;
+        p.elem = copy(element, count);
+        p.off = copy(offset, count);
+        p.x3d = copy(is3d_prt, count);
+        p.x = copy(x, nvalues);
+        p.theta = theta ? copy(theta, (size_t)count * 25) : std::vector<double>();
+    });
+}
+
 int axg_set_scanning(axg_solver *h, const axg_scanning *sc) {
     return guarded(h, [&] {
         need_open(h);
@@ -508,19 +524,22 @@ int axg_finalize(axg_solver *h) {
                 seen[p] = 1;
             }
         }
-        {
+        for (int solid = 1; solid >= 0; solid--) {
             // PRT: one per element, sizes, 3-D factors on 3-D elements only
-            std::vector<char> seen(m.se.count, 0);
-            for (int i = 0; i < m.prt.count; i++) {
-                const int e = m.prt.elem[i];
-                if (e < 0 || e >= m.se.count) throw axg::Error(AXG_E_ARG, "PRT || element index out of range.");
+            const axg::HostPrt &pr = solid ? m.prt : m.prt_f;
+            const int ne = solid ? m.se.count : m.fe.count;
+            std::vector<char> seen(ne, 0);
+            for (int i = 0; i < pr.count; i++) {
+                const int e = pr.elem[i];
+                if (e < 0 || e >= ne) throw axg::Error(AXG_E_ARG, "PRT || element index out of range.");
                 if (seen[e]) throw axg::Error(AXG_E_ARG, "PRT || element listed twice.");
                 seen[e] = 1;
-                const bool e3d = m.se.is3d.size() && m.se.is3d[e];
-                if (m.prt.x3d[i] && !e3d)
+                const std::vector<uint8_t> &is3d = solid ? m.se.is3d : m.fe.is3d;
+                const bool e3d = is3d.size() && is3d[e];
+                if (pr.x3d[i] && !e3d)
                     throw axg::Error(AXG_E_ARG, "PRT::checkCompatibility || 3-D PRT on a 1-D element.");
-                const int64_t ns = m.prt.x3d[i] ? m.se.nr[e] : 1;
-                if (m.prt.off[i] < 0 || m.prt.off[i] + 5 * ns * 25 > (int64_t)m.prt.x.size())
+                const int64_t ns = pr.x3d[i] ? (solid ? m.se.nr[e] : m.fe.nr[e]) : 1;
+                if (pr.off[i] < 0 || pr.off[i] + 5 * ns * 25 > (int64_t)pr.x.size())
                     throw axg::Error(AXG_E_ARG, "PRT::checkCompatibility || Incompatible sizes.");
             }
         }

@@ -91,6 +91,7 @@ struct HostPrt {
     std::vector<int64_t> off;
     std::vector<uint8_t> x3d;
     std::vector<double> x;       // per element from off: [5][nslice][25] X0..X3, |J|
+    std::vector<double> theta;   // fluid elements: [count][25] theta of the RTZ frame (empty: none)
 };
 
 struct HostScanning {
@@ -127,7 +128,7 @@ struct HostModel {
     HostOcean ocean;
     HostOcean3D ocean3;
     HostScanning scan;
-    HostPrt prt;
+    HostPrt prt, prt_f;
     HostSponge sg_s, sg_f;
     HostPoints sp, fp;
     HostSolidElements se;

@@ -126,7 +126,10 @@ class Engine final : public EngineBase {
         void (*pkernel)(const PrtArgs<T, AT>, int, int, int, size_t) = nullptr;
     };
     struct FluidBucket {
-        int is3d, cls, team, tpc, nr_max, n;
+        int is3d, cls, team, tpc, nr_max, n, prt = 0;
+        DBuf<T> xpool, trig;
+        DBuf<int64_t> xoff;
+        DBuf<uint8_t> x3d;
         size_t team_bytes;
         DBuf<int> nr, pts;
         DBuf<uint8_t> axial;
@@ -563,6 +566,7 @@ public:
             a.gmat = gmat_.p;
             a.nwave = 1;
             a.fstride = 0;
+            a.x = b.xpool.p; a.x_off = b.xoff.p; a.x3d = b.x3d.p; a.trig = b.trig.p;
             int blocks = (b.n + b.tpc - 1) / b.tpc;
             b.kernel<<<blocks, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.tpc,
                                                                               b.team_bytes);
@@ -1063,12 +1067,21 @@ private:
     // ------------------------------------------------------- fluid buckets ---
     using FluidKernel = void (*)(const FluidArgs<T>, int, int, size_t);
     void build_fluid_buckets(const HostFluidElements &h) {
-        std::map<std::tuple<int, int>, std::vector<int>> groups;
-        for (int e = 0; e < h.count; e++)
-            groups[{h.is3d.size() ? h.is3d[e] : 0, cfg_.plain ? 0 : nr_class(h.nr[e])}].push_back(e);
+        // group by (1-D/3-D, nr class, PRT mode: 0 none, 1 PRT, 2 PRT in the RTZ frame)
+        const HostPrt &hp = model_.prt_f;
+        std::vector<int> prt_of(h.count, -1);
+        for (int i = 0; i < hp.count; i++) prt_of[hp.elem[i]] = i;
+        std::map<std::tuple<int, int, int>, std::vector<int>> groups;
+        for (int e = 0; e < h.count; e++) {
+            const int mode = prt_of[e] < 0 ? 0 : (hp.theta.empty() ? 1 : 2);
+            groups[{h.is3d.size() ? h.is3d[e] : 0, cfg_.plain ? 0 : nr_class(h.nr[e]), mode}].push_back(e);
+        }
         for (auto &kv : groups) {
             auto b = std::make_unique<FluidBucket>();
-            std::tie(b->is3d, b->cls) = kv.first;
+            std::tie(b->is3d, b->cls, b->prt) = kv.first;
+            std::vector<T> xpool, trig;
+            std::vector<int64_t> xoff;
+            std::vector<uint8_t> x3d;
             const std::vector<int> &ids = kv.second;
             b->n = (int)ids.size();
             b->nr_max = 1;
@@ -1099,6 +1112,27 @@ private:
                 for (int i = 0; i < ns * 25; i++) K.push_back((T)mm[i]);
                 double s = sizeof(T);
                 bytes += 6 * 25 * s + 25 * 4 + 8 + (double)ns * 25 * s;
+                if (b->prt) {
+                    const int i = prt_of[e];
+                    const int xns = hp.x3d[i] ? enr : 1;
+                    const size_t xs = (size_t)xns * 25;
+                    const double *x = &hp.x[hp.off[i]];
+                    xoff.push_back((int64_t)xpool.size());
+                    x3d.push_back(hp.x3d[i]);
+                    for (int c = 0; c < 4; c++)
+                        for (size_t j = 0; j < xs; j++) xpool.push_back((T)x[c * xs + j]);
+                    for (int c = 0; c < 4; c++)
+                        for (size_t j = 0; j < xs; j++) xpool.push_back((T)(x[c * xs + j] * x[4 * xs + j]));
+                    bytes += 8.0 * xs * s;
+                    if (b->prt == 2) {
+                        // CoordTransformSpherical constructor: sin / cos of theta, cast
+                        for (int q = 0; q < 25; q++) trig.push_back((T)std::sin(hp.theta[(size_t)i * 25 + q]));
+                        for (int q = 0; q < 25; q++) trig.push_back((T)std::cos(hp.theta[(size_t)i * 25 + q]));
+                    }
+                } else {
+                    xoff.push_back(0);
+                    x3d.push_back(0);
+                }
                 flops += (double)enu * 25 * 2 * (10 * 4 + 20);
                 if (b->is3d) flops += 2.0 * 75 * enr * enu * 4;
             }
@@ -1108,8 +1142,17 @@ private:
             b->geom.upload(geom);
             if (K.empty()) K.push_back((T)0);
             b->K.upload(K); b->K_off.upload(koff);
-            b->kernel = b->is3d ? (FluidKernel)fluid_stiffness_kernel<T, true>
-                                : (FluidKernel)fluid_stiffness_kernel<T, false>;
+            if (xpool.empty()) xpool.push_back((T)0);
+            if (trig.empty()) trig.push_back((T)0);
+            b->xpool.upload(xpool); b->xoff.upload(xoff); b->x3d.upload(x3d); b->trig.upload(trig);
+            if (b->is3d)
+                b->kernel = b->prt == 0 ? (FluidKernel)fluid_stiffness_kernel<T, true, 0>
+                          : b->prt == 1 ? (FluidKernel)fluid_stiffness_kernel<T, true, 1>
+                                        : (FluidKernel)fluid_stiffness_kernel<T, true, 2>;
+            else
+                b->kernel = b->prt == 0 ? (FluidKernel)fluid_stiffness_kernel<T, false, 0>
+                          : b->prt == 1 ? (FluidKernel)fluid_stiffness_kernel<T, false, 1>
+                                        : (FluidKernel)fluid_stiffness_kernel<T, false, 2>;
             int team = cfg_.plain ? 256 : (team_override_[b->cls] ? team_override_[b->cls] : default_team(b->cls));
             TeamLayout L = fluid_layout<T>(b->nr_max);
             if (L.total > 200 * 1024)
@@ -1530,6 +1573,7 @@ private:
             a.gmat = gmat_.p;
             a.nwave = nwave_;
             a.fstride = (size_t)fp_.total;
+            a.x = b.xpool.p; a.x_off = b.xoff.p; a.x3d = b.x3d.p; a.trig = b.trig.p;
             int blocks = (b.n + b.tpc - 1) / b.tpc;
             b.kernel<<<blocks, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.tpc,
                                                                               b.team_bytes);

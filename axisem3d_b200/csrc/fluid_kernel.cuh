@@ -31,7 +31,41 @@ struct FluidArgs {
     const T *gmat;
     int nwave;
     size_t fstride;
+    // particle relabelling (PRT kernels only): per element [8][nsl][25] X0..X3, X0|J|..X3|J|,
+    // nsl = nr where x3d, else 1; trig [n][2][25] sin, cos of theta (RTZ frame)
+    const T *x;
+    const int64_t *x_off;
+    const uint8_t *x3d;
+    const T *trig;
 };
+
+// PRT::sphericalToUndulated3 / undulatedToSpherical3 (PRT/PRT.hpp:313-371), as written there:
+// the phi row of the forward map takes X1 (the solid map's takes X2)
+template <class V, class R>
+__device__ __forceinline__ void prt_sph_to_und3(const V g[3], V u[3], R X0, R X1, R X2, R X3) {
+    (void)X2;
+    u[0] = cadd(cscale(g[0], X0), cscale(g[2], X1));
+    u[1] = cadd(cscale(g[1], X0), cscale(g[2], X1));
+    u[2] = cscale(g[2], X3);
+}
+template <class V, class R>
+__device__ __forceinline__ void prt_und_to_sph3(const V u[3], V g[3], R X0, R X1, R X2, R X3) {
+    g[0] = cscale(u[0], X0);
+    g[1] = cscale(u[1], X0);
+    g[2] = cadd(cadd(cscale(u[0], X1), cscale(u[1], X2)), cscale(u[2], X3));
+}
+// CoordTransformSpherical::transformSPZ_RTZ3 / transformRTZ_SPZ3 (CoordTransformSpherical.hpp:54-100)
+template <bool TO_RTZ, class V, class T>
+__device__ __forceinline__ void rtz3(V g[3], T s1, T c1) {
+    const V u0 = g[0];
+    if (TO_RTZ) {
+        g[0] = csub(cscale(u0, c1), cscale(g[2], s1));
+        g[2] = cadd(cscale(g[2], c1), cscale(u0, s1));
+    } else {
+        g[0] = cadd(cscale(u0, c1), cscale(g[2], s1));
+        g[2] = csub(cscale(g[2], c1), cscale(u0, s1));
+    }
+}
 
 template <class T>
 __host__ __device__ inline TeamLayout fluid_layout(int nr_max) {
@@ -42,7 +76,7 @@ __host__ __device__ inline TeamLayout fluid_layout(int nr_max) {
     size_t o = 0;
     auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
     L.geom = o; o = al(o + 10 * 25 * sizeof(T));
-    L.trig = o;
+    L.trig = o; o = al(o + 2 * 25 * sizeof(T));
     L.ipt = o;  o = al(o + 3 * 25 * sizeof(int));
     L.tw = o;   o = al(o + 2 * (size_t)nr_max * sizeof(T));
     L.regA = o; o = al(o + 3 * (size_t)L.nu_max * 25 * 2 * sizeof(T));   // q[a][3][25]
@@ -53,7 +87,8 @@ __host__ __device__ inline TeamLayout fluid_layout(int nr_max) {
     return L;
 }
 
-template <class T, bool IS3D>
+// PRT: 0 = none, 1 = particle relabelling, 2 = particle relabelling in the RTZ frame
+template <class T, bool IS3D, int PRT>
 __global__ void __launch_bounds__(256)
 fluid_stiffness_kernel(const FluidArgs<T> a, const int nr_max, const int teams_per_cta,
                        const size_t team_bytes) {
@@ -73,6 +108,7 @@ fluid_stiffness_kernel(const FluidArgs<T> a, const int nr_max, const int teams_p
     const TeamLayout L = fluid_layout<T>(nr_max);
     unsigned char *base = smem_raw + (size_t)team * team_bytes;
     T *sGeo = reinterpret_cast<T *>(base + L.geom);
+    T *sTrig = reinterpret_cast<T *>(base + L.trig);
     int *sPt = reinterpret_cast<int *>(base + L.ipt);
     int *sOff = sPt + 25;
     int *sNu = sPt + 50;
@@ -91,6 +127,14 @@ fluid_stiffness_kernel(const FluidArgs<T> a, const int nr_max, const int teams_p
         const bool axial = a.axial[e] != 0;
         const T *Gxi = axial ? sGlj : sGll;
         for (int i = lane; i < 250; i += TEAM) sGeo[i] = a.geom[(size_t)e * 250 + i];
+        if constexpr (PRT == 2)
+            for (int i = lane; i < 50; i += TEAM) sTrig[i] = a.trig[(size_t)e * 50 + i];
+        const T *xp = nullptr;
+        int xns = 1;
+        if constexpr (PRT > 0) {
+            xp = a.x + a.x_off[e];
+            xns = a.x3d[e] ? nr : 1;
+        }
         for (int i = lane; i < 25; i += TEAM) {
             int p = a.pts[(size_t)e * 25 + i];
             sPt[i] = p;
@@ -139,10 +183,21 @@ fluid_stiffness_kernel(const FluidArgs<T> a, const int nr_max, const int teams_p
                 }
                 g[1] = cadd(cscale(ax, ze), cscale(ay, zx));
             }
+            if constexpr (PRT == 2) rtz3<true>(g, sTrig[q], sTrig[25 + q]);
             if constexpr (!IS3D) {
+                // Acoustic::strainToStress_FR, through the PRT maps when relabelled
                 const T K = __ldg(a.K + koff + q);
+                if constexpr (PRT > 0) {
+                    C u[3];
+                    prt_sph_to_und3(g, u, xp[q], xp[25 + q], xp[50 + q], xp[75 + q]);
 #pragma unroll
-                for (int c = 0; c < 3; c++) g[c] = cscale(g[c], K);
+                    for (int c = 0; c < 3; c++) u[c] = cscale(u[c], K);
+                    prt_und_to_sph3(u, g, xp[100 + q], xp[125 + q], xp[150 + q], xp[175 + q]);
+                    if constexpr (PRT == 2) rtz3<false>(g, sTrig[q], sTrig[25 + q]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) g[c] = cscale(g[c], K);
+                }
             }
 #pragma unroll
             for (int c = 0; c < 3; c++) rA[(al * 3 + c) * 25 + q] = g[c];
@@ -167,8 +222,21 @@ fluid_stiffness_kernel(const FluidArgs<T> a, const int nr_max, const int teams_p
                     }
                 }
                 const T K = __ldg(a.K + koff + (size_t)k * 25 + q);
+                if constexpr (PRT > 0) {
+                    const size_t xs = (size_t)xns * 25, xo = (size_t)(xns > 1 ? k : 0) * 25 + q;
+                    re1<T> gv[3], u[3];
 #pragma unroll
-                for (int c = 0; c < 3; c++) rBr[((size_t)k * 3 + c) * 25 + q] = acc[c] * K;
+                    for (int c = 0; c < 3; c++) gv[c].x = acc[c];
+                    prt_sph_to_und3(gv, u, xp[xo], xp[xs + xo], xp[2 * xs + xo], xp[3 * xs + xo]);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) u[c].x = u[c].x * K;
+                    prt_und_to_sph3(u, gv, xp[4 * xs + xo], xp[5 * xs + xo], xp[6 * xs + xo], xp[7 * xs + xo]);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) rBr[((size_t)k * 3 + c) * 25 + q] = gv[c].x;
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) rBr[((size_t)k * 3 + c) * 25 + q] = acc[c] * K;
+                }
             }
             team_sync(team, TEAM);
             for (int i = lane; i < nu * 25; i += TEAM) {
@@ -186,13 +254,17 @@ fluid_stiffness_kernel(const FluidArgs<T> a, const int nr_max, const int teams_p
                     }
                     j += step; j = j >= nr ? j - nr : j;
                 }
+                C out[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     T r = re[c], m = im[c];
                     if (al == 0) m = 0;
                     if ((nr & 1) == 0 && al == nr / 2) { r *= (T)0.5; m = 0; }
-                    rA[(al * 3 + c) * 25 + q] = mk<T>(r, m);
+                    out[c] = mk<T>(r, m);
                 }
+                if constexpr (PRT == 2) rtz3<false>(out, sTrig[q], sTrig[25 + q]);
+#pragma unroll
+                for (int c = 0; c < 3; c++) rA[(al * 3 + c) * 25 + q] = out[c];
             }
             team_sync(team, TEAM);
         }

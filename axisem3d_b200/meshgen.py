@@ -478,6 +478,30 @@ def add_ocean_load3d(m, nx, nz, width, rho_water=1020.0, depth_water=3000.0, amp
     return m
 
 
+def add_prt_fluid(m, amp=0.05, three_d=False, seed=0, rtz=True):
+    """add_prt's synthetic factors on every fluid element (3-D factors need 3-D fluid
+    elements); with rtz, the polar angle of each element point (fe_theta of a spherical
+    model) selects the RTZ frame."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ne = len(m.fe_nr)
+    off, x3, xs = [], [], []
+    o = 0
+    for e in range(ne):
+        ns = int(m.fe_nr[e]) if three_d else 1
+        X0 = 1.0 + amp * rng.uniform(-1, 1, (ns, 25))
+        X1 = amp * rng.uniform(-1, 1, (ns, 25))
+        X2 = amp * rng.uniform(-1, 1, (ns, 25))
+        X3 = 1.0 + amp * rng.uniform(-1, 1, (ns, 25))
+        off.append(o)
+        x3.append(1 if three_d else 0)
+        xs.append(np.stack([X0, X1, X2, X3, 1.0 / (X0 * X3)]).ravel())
+        o += 5 * ns * 25
+    th = np.asarray(m.fe_theta) if rtz else None
+    m.prt_fluid = {"element": np.arange(ne, dtype=np.int32), "offset": np.array(off, np.int64),
+                   "is3d_prt": np.array(x3, np.uint8), "x": np.concatenate(xs), "theta": th}
+    return m
+
+
 def add_prt(m, elements=None, amp=0.05, three_d=False, seed=0):
     """Particle-relabelling factors on `elements` (default: every solid element): J^-1
     components X0 = 1 + a, X1 = b, X2 = c, X3 = 1 + d and |J| = 1 / (X0 X3), with a, b, c, d
@@ -978,6 +1002,7 @@ def spherical_model(n_theta=96, n_solid_layers=24, n_fluid_layers=2, r_cmb=3480e
         m.nsls, m.att_alpha, m.att_beta, m.att_gamma = len(a), a, b, g
     m.fe_nr = enr[sel_f]
     m.fe_pts = fid[pts[sel_f]].astype(np.int32)
+    m.fe_theta = np.arctan2(szp[sel_f, 0, :], szp[sel_f, 1, :])
     m.fe_axial = axial[sel_f]
     m.fe_geom = geom[sel_f]
     m.fe_is3d = np.zeros(len(sel_f), np.uint8)

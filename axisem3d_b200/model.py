@@ -79,6 +79,7 @@ class Model:
     # fluid elements
     fe_nr: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     fe_pts: np.ndarray = field(default_factory=lambda: np.zeros((0, 25), np.int32))
+    fe_theta: Optional[np.ndarray] = None         # (n, 25) polar angle (not used by the engine)
     fe_axial: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint8))
     fe_geom: np.ndarray = field(default_factory=lambda: np.zeros((0, 6, 25)))
     fe_is3d: Optional[np.ndarray] = None
@@ -129,6 +130,8 @@ class Model:
     # PRT (undulated geometry): dict(element, offset, is3d_prt, x) with x per element
     # [5][nslice][25] (X0..X3, |J|) from offset
     prt: Optional[dict] = None
+    # the same for fluid elements, plus theta [n][25] for the RTZ frame (None: cartesian)
+    prt_fluid: Optional[dict] = None
     cl3_solid: Optional[dict] = None
     cl3_fluid: Optional[dict] = None
     sponge3d_solid: Optional[tuple] = None
@@ -323,15 +326,16 @@ class Model:
                     setattr(c, key, k(pk, pts, _i32, C.c_int32))
             return c
 
-        def prt():
-            d = self.prt
+        def prt(d, name):
             if not d:
                 return None
             e, off = _i32(d["element"]), _i64(d["offset"])
             x3 = np.ascontiguousarray(d["is3d_prt"], dtype=np.uint8)
             x = _f64(np.asarray(d["x"]).ravel())
-            keep["prt_e"], keep["prt_off"], keep["prt_x3"], keep["prt_x"] = e, off, x3, x
-            return (e, off, x3, x)
+            th = _f64(np.asarray(d["theta"]).ravel()) if d.get("theta") is not None else None
+            keep[name + "_e"], keep[name + "_off"], keep[name + "_x3"], keep[name + "_x"] = e, off, x3, x
+            keep[name + "_th"] = th
+            return (e, off, x3, x, th)
 
         def ocean3():
             if not self.ocean_load3d:
@@ -358,7 +362,7 @@ class Model:
         return {"sp": sp, "fp": fp, "se": se, "fe": fe, "sf": sf, "ms": ms, "fs": fs, "st": st,
                 "cl_s": clay("cls", self.cl_solid, True), "cl_f": clay("clf", self.cl_fluid, False),
                 "sg_s": sponge("sgs", self.sponge_solid), "sg_f": sponge("sgf", self.sponge_fluid),
-                "ocean": ocean(), "scan": scan(), "ocean3": ocean3(), "prt": prt(),
+                "ocean": ocean(), "scan": scan(), "ocean3": ocean3(), "prt": prt(self.prt, "prt"), "prt_f": prt(self.prt_fluid, "prtf"),
                 "cl3_s": clay3("c3s", self.cl3_solid, True), "cl3_f": clay3("c3f", self.cl3_fluid, False),
                 "sg3_s": sponge3("g3s", self.sponge3d_solid), "sg3_f": sponge3("g3f", self.sponge3d_fluid),
                 "keep": keep}

@@ -76,9 +76,15 @@ class Solver:
         if s["scan"] is not None:
             self._check(self.lib.axg_set_scanning(h, C.byref(s["scan"])))
         if s["prt"] is not None:
-            e, off, x3, x = s["prt"]
+            e, off, x3, x, _ = s["prt"]
             self._check(self.lib.axg_set_prt(h, len(e), e.ctypes.data_as(L.P_i32), off.ctypes.data_as(L.P_i64),
                                              x3.ctypes.data_as(L.P_u8), len(x), x.ctypes.data_as(L.P_f64)))
+        if s["prt_f"] is not None:
+            e, off, x3, x, th = s["prt_f"]
+            self._check(self.lib.axg_set_prt_fluid(h, len(e), e.ctypes.data_as(L.P_i32),
+                                                   off.ctypes.data_as(L.P_i64), x3.ctypes.data_as(L.P_u8), len(x),
+                                                   x.ctypes.data_as(L.P_f64),
+                                                   th.ctypes.data_as(L.P_f64) if th is not None else None))
         if s["ocean3"] is not None:
             pt, off, mo, nrm = s["ocean3"]
             self._check(self.lib.axg_set_ocean_load3d(h, len(pt), pt.ctypes.data_as(L.P_i32),

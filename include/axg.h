@@ -311,6 +311,11 @@ int  axg_scanning_nr(axg_solver *h, int32_t *solid_nr, int32_t *fluid_nr);
    (rtz) the 9-component gradient is taken to the RTZ frame first whatever the rheology. */
 int  axg_set_prt(axg_solver *h, int32_t count, const int32_t *element, const int64_t *offset,
                  const uint8_t *is3d_prt, int64_t nvalues, const double *x);
+/* the same for fluid elements (FluidElement::displToStiff's PRT branch, FluidElement.cpp:101-148);
+   theta [count][25] (the polar angle of each element point, for the RTZ frame of spherical
+   meshes) or NULL on cartesian meshes */
+int  axg_set_prt_fluid(axg_solver *h, int32_t count, const int32_t *element, const int64_t *offset,
+                       const uint8_t *is3d_prt, int64_t nvalues, const double *x, const double *theta);
 /* MassOceanLoad1D (point/mass/MassOceanLoad1D.hpp, built in GLLPoint.cpp:66-73) on solid
    surface points under an ocean:
    in computeStiffToAccel the point's own mass acts along the surface and mass + mass_ocean

@@ -372,6 +372,10 @@ struct FluidElem {
     Ops<R> ops;
     int is3d, nslice;
     std::vector<R> K;              // [nslice][25]
+    // PRT: X0..X3 then X0|J|..X3|J| [8][xns][25]; RTZ frame sin / cos of theta
+    int prt = 0, prt3 = 0, rtz = 0;
+    std::vector<R> X;
+    R sin1[N], cos1[N];
 };
 
 template <class R>
@@ -431,6 +435,8 @@ struct OracleBase {
                                   const double *normal) = 0;
     virtual void set_clayton3d(int solid, const axg_clayton3d *c) = 0;
     virtual void set_scanning(const axg_scanning *s) = 0;
+    virtual void set_prt_fluid(int n, const int32_t *elem, const int64_t *off, const uint8_t *x3d, const double *x,
+                               const double *theta) = 0;
     virtual void set_prt(int n, const int32_t *elem, const int64_t *off, const uint8_t *x3d, const double *x) = 0;
     virtual void scanning_nr(int32_t *s, int32_t *f) = 0;
     virtual void set_sponge3d(int solid, int n, const int32_t *pt, const int64_t *off, const double *g) = 0;
@@ -695,6 +701,28 @@ struct Oracle : OracleBase {
                 for (size_t j = 0; j < xs; j++) {
                     el.X[c * xs + j] = (R)xv[c * xs + j];
                     el.X[(4 + c) * xs + j] = (R)(xv[c * xs + j] * xv[4 * xs + j]);
+                }
+        }
+    }
+    void set_prt_fluid(int n, const int32_t *elem, const int64_t *off, const uint8_t *x3d, const double *x,
+                       const double *theta) override {
+        for (int i = 0; i < n; i++) {
+            FluidElem<R> &el = fe[elem[i]];
+            el.prt = 1;
+            el.prt3 = x3d[i];
+            const size_t xs = (size_t)(el.prt3 ? el.nr : 1) * N;
+            const double *xv = x + off[i];
+            el.X.resize(8 * xs);
+            for (int c = 0; c < 4; c++)
+                for (size_t j = 0; j < xs; j++) {
+                    el.X[c * xs + j] = (R)xv[c * xs + j];
+                    el.X[(4 + c) * xs + j] = (R)(xv[c * xs + j] * xv[4 * xs + j]);
+                }
+            el.rtz = theta != nullptr;
+            if (theta)
+                for (int q = 0; q < N; q++) {
+                    el.sin1[q] = (R)std::sin(theta[(size_t)i * N + q]);
+                    el.cos1[q] = (R)std::cos(theta[(size_t)i * N + q]);
                 }
         }
     }
@@ -1191,8 +1219,102 @@ struct Oracle : OracleBase {
         }
     }
 
+    // PRT::sphericalToUndulated3 / undulatedToSpherical3 (PRT.hpp:313-371) as written there
+    template <class V>
+    static void sph2und3(const V g[3], V u[3], R X0, R X1, R X2, R X3) {
+        (void)X2;
+        u[0] = g[0] * X0 + g[2] * X1;
+        u[1] = g[1] * X0 + g[2] * X1;
+        u[2] = g[2] * X3;
+    }
+    template <class V>
+    static void und2sph3(const V u[3], V g[3], R X0, R X1, R X2, R X3) {
+        g[0] = u[0] * X0;
+        g[1] = u[1] * X0;
+        g[2] = u[0] * X1 + u[1] * X2 + u[2] * X3;
+    }
+    // transformSPZ_RTZ3 / transformRTZ_SPZ3 (CoordTransformSpherical.hpp:54-100)
+    static void rtz3(Cx<R> g[3], R s1, R c1, bool to_rtz) {
+        const Cx<R> u0 = g[0];
+        if (to_rtz) { g[0] = u0 * c1 - g[2] * s1; g[2] = g[2] * c1 + u0 * s1; }
+        else { g[0] = u0 * c1 + g[2] * s1; g[2] = g[2] * c1 - u0 * s1; }
+    }
+    // FluidElement::displToStiff, PRT branch (FluidElement.cpp:101-148)
+    void fluid_element_prt(const FluidElem<R> &el, std::vector<Cx<R>> &elemStiff) {
+        const int nu = el.nu, nr = el.nr;
+        std::vector<CM<R>> X(nu), Q((size_t)nu * 3);
+        for (int q = 0; q < N; q++) {
+            int p = el.pts[q];
+            for (int a = 0; a < nu; a++)
+                X[a].a[q / P][q % P] = a < fp.nu[p] ? fp.displ[(size_t)fp.off[p] + a] : Cx<R>(0);
+        }
+        Grad<R> g{el.ops, gm};
+        for (int a = 0; a < nu; a++) g.grad3(X[a], &Q[(size_t)a * 3], a);
+        auto at = [&](int a, int c, int q) -> Cx<R> & { return Q[(size_t)a * 3 + c].a[q / P][q % P]; };
+        if (el.rtz)
+            for (int a = 0; a < nu; a++)
+                for (int q = 0; q < N; q++) {
+                    Cx<R> v[3] = {at(a, 0, q), at(a, 1, q), at(a, 2, q)};
+                    rtz3(v, el.sin1[q], el.cos1[q], true);
+                    for (int c = 0; c < 3; c++) at(a, c, q) = v[c];
+                }
+        const int xns = el.prt3 ? nr : 1;
+        const size_t xs = (size_t)xns * N;
+        auto XF = [&](int c, int k, int q) { return el.X[c * xs + (size_t)k * N + q]; };
+        if (!el.is3d) {
+            for (int a = 0; a < nu; a++)
+                for (int q = 0; q < N; q++) {
+                    Cx<R> v[3] = {at(a, 0, q), at(a, 1, q), at(a, 2, q)}, u[3];
+                    sph2und3(v, u, XF(0, 0, q), XF(1, 0, q), XF(2, 0, q), XF(3, 0, q));
+                    for (int c = 0; c < 3; c++) u[c] *= el.K[q];
+                    und2sph3(u, v, XF(4, 0, q), XF(5, 0, q), XF(6, 0, q), XF(7, 0, q));
+                    for (int c = 0; c < 3; c++) at(a, c, q) = v[c];
+                }
+        } else {
+            const Twiddle<R> &t = twiddle(nr);
+            std::vector<R> gc((size_t)nr * 3 * N);
+            std::vector<Cx<R>> cbuf(nu);
+            std::vector<R> rbuf(nr);
+            for (int c = 0; c < 3; c++)
+                for (int q = 0; q < N; q++) {
+                    for (int a = 0; a < nu; a++) cbuf[a] = at(a, c, q);
+                    c2r(cbuf.data(), nu, rbuf.data(), nr, t);
+                    for (int k = 0; k < nr; k++) gc[((size_t)k * 3 + c) * N + q] = rbuf[k];
+                }
+            for (int k = 0; k < nr; k++)
+                for (int q = 0; q < N; q++) {
+                    const int kx = el.prt3 ? k : 0;
+                    R v[3] = {gc[((size_t)k * 3) * N + q], gc[((size_t)k * 3 + 1) * N + q], gc[((size_t)k * 3 + 2) * N + q]}, u[3];
+                    sph2und3(v, u, XF(0, kx, q), XF(1, kx, q), XF(2, kx, q), XF(3, kx, q));
+                    for (int c = 0; c < 3; c++) u[c] *= el.K[(size_t)k * N + q];
+                    und2sph3(u, v, XF(4, kx, q), XF(5, kx, q), XF(6, kx, q), XF(7, kx, q));
+                    for (int c = 0; c < 3; c++) gc[((size_t)k * 3 + c) * N + q] = v[c];
+                }
+            for (int c = 0; c < 3; c++)
+                for (int q = 0; q < N; q++) {
+                    for (int k = 0; k < nr; k++) rbuf[k] = gc[((size_t)k * 3 + c) * N + q];
+                    r2c(rbuf.data(), nr, cbuf.data(), nu, t);
+                    for (int a = 0; a < nu; a++) at(a, c, q) = cbuf[a];
+                }
+        }
+        if (el.rtz)
+            for (int a = 0; a < nu; a++)
+                for (int q = 0; q < N; q++) {
+                    Cx<R> v[3] = {at(a, 0, q), at(a, 1, q), at(a, 2, q)};
+                    rtz3(v, el.sin1[q], el.cos1[q], false);
+                    for (int c = 0; c < 3; c++) at(a, c, q) = v[c];
+                }
+        elemStiff.resize((size_t)nu * N);
+        for (int a = 0; a < nu; a++) {
+            CM<R> f;
+            g.quad3(&Q[(size_t)a * 3], f, a);
+            for (int q = 0; q < N; q++) elemStiff[(size_t)a * N + q] = f.a[q / P][q % P];
+        }
+    }
+
     // ----------------------- FluidElement::computeStiff -----------------------
     void fluid_element(const FluidElem<R> &el, std::vector<Cx<R>> &elemStiff) {
+        if (el.prt) { fluid_element_prt(el, elemStiff); return; }
         int nu = el.nu, nr = el.nr;
         std::vector<CM<R>> X(nu), Q((size_t)nu * 3);
         for (int q = 0; q < N; q++) {
@@ -1700,6 +1822,7 @@ int axo_set_sponge(void *h, int solid, int n, const int32_t *pt, const double *g
 int axo_set_ocean_load(void *h, int n, const int32_t *pt, const double *mo, const double *theta) { AXO_TRY(static_cast<OracleBase *>(h)->set_ocean_load(n, pt, mo, theta)) }
 int axo_set_ocean_load3d(void *h, int n, const int32_t *pt, const int64_t *off, const double *mo, const double *nrm) { AXO_TRY(static_cast<OracleBase *>(h)->set_ocean_load3d(n, pt, off, mo, nrm)) }
 int axo_set_prt(void *h, int n, const int32_t *e, const int64_t *off, const uint8_t *x3d, const double *x) { AXO_TRY(static_cast<OracleBase *>(h)->set_prt(n, e, off, x3d, x)) }
+int axo_set_prt_fluid(void *h, int n, const int32_t *e, const int64_t *off, const uint8_t *x3d, const double *x, const double *th) { AXO_TRY(static_cast<OracleBase *>(h)->set_prt_fluid(n, e, off, x3d, x, th)) }
 int axo_set_scanning(void *h, const axg_scanning *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_scanning(s)) }
 int axo_scanning_nr(void *h, int32_t *s, int32_t *f) { AXO_TRY(static_cast<OracleBase *>(h)->scanning_nr(s, f)) }
 int axo_set_clayton3d(void *h, int solid, const axg_clayton3d *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton3d(solid, c)) }

@@ -56,6 +56,7 @@ def lib():
             "axo_set_clayton3d": (C.c_int, [V, C.c_int, C.POINTER(L.axg_clayton3d)]),
             "axo_set_scanning": (C.c_int, [V, C.POINTER(L.axg_scanning)]),
             "axo_set_prt": (C.c_int, [V, C.c_int, L.P_i32, L.P_i64, L.P_u8, L.P_f64]),
+            "axo_set_prt_fluid": (C.c_int, [V, C.c_int, L.P_i32, L.P_i64, L.P_u8, L.P_f64, L.P_f64]),
             "axo_set_ocean_load3d": (C.c_int, [V, C.c_int, L.P_i32, L.P_i64, L.P_f64, L.P_f64]),
             "axo_scanning_nr": (C.c_int, [V, L.P_i32, L.P_i32]),
             "axo_set_sponge3d": (C.c_int, [V, C.c_int, C.c_int, L.P_i32, L.P_i64, L.P_f64]),
@@ -125,9 +126,15 @@ class Oracle:
         if s["scan"] is not None:
             self._chk(self.O.axo_set_scanning(self.h, C.byref(s["scan"])))
         if s["prt"] is not None:
-            e, off, x3, x = s["prt"]
+            e, off, x3, x, _ = s["prt"]
             self._chk(self.O.axo_set_prt(self.h, len(e), e.ctypes.data_as(L.P_i32), off.ctypes.data_as(L.P_i64),
                                          x3.ctypes.data_as(L.P_u8), x.ctypes.data_as(L.P_f64)))
+        if s["prt_f"] is not None:
+            e, off, x3, x, th = s["prt_f"]
+            self._chk(self.O.axo_set_prt_fluid(self.h, len(e), e.ctypes.data_as(L.P_i32),
+                                               off.ctypes.data_as(L.P_i64), x3.ctypes.data_as(L.P_u8),
+                                               x.ctypes.data_as(L.P_f64),
+                                               th.ctypes.data_as(L.P_f64) if th is not None else None))
         if s["ocean3"] is not None:
             pt, off, mo, nrm = s["ocean3"]
             self._chk(self.O.axo_set_ocean_load3d(self.h, len(pt), pt.ctypes.data_as(L.P_i32),

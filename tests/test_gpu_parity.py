@@ -676,3 +676,35 @@ def test_prt_full_steps_and_errors(built):
     with pytest.raises(EngineError) as ei:
         Solver(bad, "fp32")
     assert ei.value.code == L.AXG_E_ARG and "3-D PRT on a 1-D element" in str(ei.value)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
+@pytest.mark.parametrize("three_d", [False, True])
+def test_fluid_prt_parity(built, precision, three_d):
+    """Fluid elements with PRT factors in the RTZ frame of a spherical shell (1-D elements
+    with 1-D factors; 3-D elements with per-slice K and 3-D factors): fluid stiffness vs the
+    oracle."""
+    import copy
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.spherical_model(n_theta=16, n_solid_layers=4, n_fluid_layers=2, nr_max=24)
+    if three_d:
+        nr = np.asarray(m.fe_nr)
+        K = np.asarray(m.fe_moduli).reshape(-1, 25)
+        m = copy.copy(m)
+        m.fe_is3d = np.ones(len(nr), np.uint8)
+        m.fe_moduli = np.concatenate([
+            (np.tile(K[e], (nr[e], 1)) * (1 + 0.02 * np.sin(np.arange(nr[e])))[:, None]).ravel()
+            for e in range(len(nr))])
+        m.fe_mat_off = np.concatenate([[0], np.cumsum(nr * 25)[:-1]]).astype(np.int64)
+    meshgen.add_prt_fluid(m, amp=0.05, three_d=three_d, seed=2)
+    uf = meshgen.random_displacement(m, seed=6, solid=False)
+    o = O.Oracle(m, "fp64")
+    o.set_field(uf, "displ", solid=False)
+    o.compute_stiffness()
+    ref = o.get_field("stiff", solid=False)
+    with Solver(m, precision) as s:
+        s.set_field(uf, "displ", solid=False)
+        s.compute_stiffness()
+        assert rel(s.get_field("stiff", solid=False), ref) <= TOL_STIFF[precision]

@@ -390,3 +390,36 @@ def test_prt_stiffness_is_self_adjoint(built):
     a = np.sum(w * np.real(np.conj(v) * ku))
     b = np.sum(w * np.real(np.conj(u) * kv))
     assert abs(a - b) <= 1e-12 * np.linalg.norm(ku) * np.linalg.norm(v) * 4
+
+
+def _fluid3d(m):
+    import copy
+    m3 = copy.copy(m)
+    nr = np.asarray(m.fe_nr)
+    K = np.asarray(m.fe_moduli).reshape(-1, 25)
+    m3.fe_is3d = np.ones(len(nr), np.uint8)
+    m3.fe_moduli = np.concatenate([
+        (np.tile(K[e], (nr[e], 1)) * (1 + 0.02 * np.sin(np.arange(nr[e])))[:, None]).ravel()
+        for e in range(len(nr))])
+    m3.fe_mat_off = np.concatenate([[0], np.cumsum(nr * 25)[:-1]]).astype(np.int64)
+    return m3
+
+
+@pytest.mark.parametrize("three_d", [False, True])
+def test_identity_fluid_prt_equals_no_prt(built, three_d):
+    """Identity PRT factors on the fluid elements of a spherical shell (RTZ frame on) give the
+    fluid stiffness without PRT; 3-D fluid elements with per-slice K and 3-D factors too."""
+    import copy
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    m = meshgen.spherical_model(n_theta=16, n_solid_layers=4, n_fluid_layers=2, nr_max=24)
+    if three_d:
+        m = _fluid3d(m)
+    uf = meshgen.random_displacement(m, seed=6, solid=False)
+    out = []
+    for mm in (m, meshgen.add_prt_fluid(copy.copy(m), amp=0.0, three_d=three_d)):
+        o = O.Oracle(mm, "fp64")
+        o.set_field(uf, "displ", solid=False)
+        o.compute_stiffness()
+        out.append(o.get_field("stiff", solid=False))
+    assert np.linalg.norm(out[1] - out[0]) <= 1e-14 * np.linalg.norm(out[0])
