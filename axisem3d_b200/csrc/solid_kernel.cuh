@@ -68,6 +68,29 @@ constexpr int KP = AXG_KP;   // slice pairs per thread in the paired Fourier -> 
 constexpr int KB = AXG_KB;   // slices per thread in the Fourier -> slice transform
 constexpr int AB = AXG_AB;   // modes per thread in the slice -> Fourier transform
 
+// The SLS state is read once and written once per step: with AXG_STREAM_STATE its loads and
+// stores carry the streaming cache hint (evict first), so that it does not push the moduli and
+// the point fields out of L2.
+#ifndef AXG_STREAM_STATE
+#define AXG_STREAM_STATE 0
+#endif
+template <class AT>
+__device__ __forceinline__ AT state_ld(const AT *p) {
+#if AXG_STREAM_STATE
+    return __ldcs(p);
+#else
+    return *p;
+#endif
+}
+template <class AT>
+__device__ __forceinline__ void state_st(AT *p, AT v) {
+#if AXG_STREAM_STATE
+    __stcs(p, v);
+#else
+    *p = v;
+#endif
+}
+
 template <class T, class AT>
 struct SolidArgs {
     int n_elem;
@@ -639,11 +662,11 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                             dl = __ldg(am + slot);
                             dmu = __ldg(am + nslot + slot);
 #pragma unroll
-                            for (int d = 0; d < 6; d++) ds[d] = st[d * nslot + slot];
+                            for (int d = 0; d < 6; d++) ds[d] = state_ld(st + d * nslot + slot);
 #pragma unroll
                             for (int l = 0; l < NSR; l++)
 #pragma unroll
-                                for (int d = 0; d < 6; d++) mem[l][d] = st[(6 + l * 6 + d) * nslot + slot];
+                                for (int d = 0; d < 6; d++) mem[l][d] = state_ld(st + (6 + l * 6 + d) * nslot + slot);
                         }
                     }
                     T acc[6];
@@ -686,11 +709,11 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
 #pragma unroll
                             for (int d = 0; d < 6; d++) sg[d].x = s6[d];
 #pragma unroll
-                            for (int d = 0; d < 6; d++) st[d * nslot + slot] = ds[d];
+                            for (int d = 0; d < 6; d++) state_st(st + d * nslot + slot, ds[d]);
 #pragma unroll
                             for (int l = 0; l < NSR; l++)
 #pragma unroll
-                                for (int d = 0; d < 6; d++) st[(6 + l * 6 + d) * nslot + slot] = mem[l][d];
+                                for (int d = 0; d < 6; d++) state_st(st + (6 + l * 6 + d) * nslot + slot, mem[l][d]);
                         }
                     }
 #pragma unroll
