@@ -16,7 +16,7 @@ AXG_FP64, AXG_FP32, AXG_MIXED = 0, 1, 2
 AXG_ISO, AXG_TISO, AXG_ANISO = 0, 1, 2
 AXG_ATT_NONE, AXG_ATT_FULL, AXG_ATT_CG4 = 0, 1, 2
 AXG_FIELD_STIFF, AXG_FIELD_DISPL, AXG_FIELD_VELOC, AXG_FIELD_ACCEL = 0, 1, 2, 3
-AXG_MAP_LINEAR, AXG_MAP_SPHERICAL = 0, 1
+AXG_MAP_LINEAR, AXG_MAP_SPHERICAL, AXG_MAP_SEMI_SPHERICAL = 0, 1, 2
 AXG_MAX_SLS = 8
 
 PRECISIONS = {"fp64": AXG_FP64, "fp32": AXG_FP32, "mixed": AXG_MIXED}
@@ -157,6 +157,7 @@ SIGNATURES = {
     "axg_spectral_tables": (C.c_int, [P_f64] * 6),
     "axg_quad_geometry": (C.c_int, [C.c_int32, P_f64, C.c_int32, P_f64, P_f64]),
     "axg_quad_geometry_batch": (C.c_int, [C.c_int32, C.c_int32, P_f64, P_u8, P_f64, P_f64]),
+    "axg_quad_map": (C.c_int, [C.c_int32, P_f64, C.c_double, C.c_double, P_f64]),
     "axg_quad_dt": (C.c_int, [P_f64, C.c_double, P_f64]),
     "axg_att_alpha_beta_gamma": (C.c_int, [C.c_int32, P_f64, P_f64, C.c_double, P_f64, P_f64, P_f64]),
     "axg_att_moduli": (C.c_int, [C.c_int32, P_f64, P_f64, C.c_double, C.c_double, C.c_double,

@@ -219,6 +219,60 @@ void map_spherical(const double *n, int co, double xi0, double eta0, double &s, 
     J.J11 = a10 * Q[1] + a11 * Q[3];
 }
 
+// MappingSemiSpherical (mapping/MappingSemiSpherical.hpp): one curved outer edge (equal
+// nodal radii, the larger ones), the opposite edge straight; rotated by Q2 like the spherical
+// mapping, blended linearly between the straight edge and the arc.
+int curved_outer_semi(const double *n) {
+    double r[4], e[4];
+    for (int k = 0; k < 4; k++) r[k] = std::hypot(n[2 * k], n[2 * k + 1]);
+    for (int k = 0; k < 4; k++) {
+        int k1 = (k + 1) % 4;
+        e[k] = std::hypot(n[2 * k] - n[2 * k1], n[2 * k + 1] - n[2 * k1 + 1]);
+    }
+    double tol = std::min(std::min(e[0], e[1]), std::min(e[2], e[3])) * 1e-3;
+    if (std::fabs(r[0] - r[1]) < tol && r[0] > r[2]) return 0;
+    if (std::fabs(r[1] - r[2]) < tol && r[1] > r[3]) return 1;
+    if (std::fabs(r[2] - r[3]) < tol && r[2] > r[0]) return 2;
+    if (std::fabs(r[3] - r[0]) < tol && r[3] > r[1]) return 3;
+    return -1;
+}
+
+void map_semi_spherical(const double *n, int co, double xi0, double eta0, double &s, double &z,
+                        Jac &J) {
+    const double *Q = kQ2[co];
+    double sq_n[4], zq_n[4], t_n[4];
+    for (int k = 0; k < 4; k++) {
+        sq_n[k] = Q[0] * n[2 * k] + Q[1] * n[2 * k + 1];
+        zq_n[k] = Q[2] * n[2 * k] + Q[3] * n[2 * k + 1];
+        t_n[k] = M_PI * .5 - std::atan2(zq_n[k], sq_n[k]);
+    }
+    double xi = Q[0] * xi0 + Q[1] * eta0, eta = Q[2] * xi0 + Q[3] * eta0;
+    const int i0 = cycle4(co - 2), i1 = cycle4(co - 1), i2 = cycle4(co), i3 = cycle4(co + 1);
+    double s0 = sq_n[i0], z0 = zq_n[i0], s1 = sq_n[i1], z1 = zq_n[i1];
+    double r2 = std::hypot(sq_n[i2], zq_n[i2]);
+    double t2 = t_n[i2], t3 = t_n[i3];
+    angles_close(t3, t2);
+    double s01 = ((1. - xi) * s0 + (1. + xi) * s1) * .5;
+    double z01 = ((1. - xi) * z0 + (1. + xi) * z1) * .5;
+    double t32 = ((1. - xi) * t3 + (1. + xi) * t2) * .5;
+    double etam = (1. - eta) * .5, r2p = (1. + eta) * r2 * .5;
+    double s01_xi = (s1 - s0) * .5, z01_xi = (z1 - z0) * .5, t32_xi = (t2 - t3) * .5;
+    double sq = etam * s01 + r2p * std::sin(t32);
+    double zq = etam * z01 + r2p * std::cos(t32);
+    double j00 = etam * s01_xi + r2p * std::cos(t32) * t32_xi;
+    double j10 = etam * z01_xi - r2p * std::sin(t32) * t32_xi;
+    double j01 = -.5 * s01 + r2 * .5 * std::sin(t32);
+    double j11 = -.5 * z01 + r2 * .5 * std::cos(t32);
+    s = Q[0] * sq + Q[2] * zq;
+    z = Q[1] * sq + Q[3] * zq;
+    double a00 = Q[0] * j00 + Q[2] * j10, a01 = Q[0] * j01 + Q[2] * j11;
+    double a10 = Q[1] * j00 + Q[3] * j10, a11 = Q[1] * j01 + Q[3] * j11;
+    J.J00 = a00 * Q[0] + a01 * Q[2];
+    J.J01 = a00 * Q[1] + a01 * Q[3];
+    J.J10 = a10 * Q[0] + a11 * Q[2];
+    J.J11 = a10 * Q[1] + a11 * Q[3];
+}
+
 }  // namespace
 }  // namespace axg
 
@@ -244,6 +298,9 @@ int axg_quad_geometry(int32_t mapping, const double *nodal_sz, int32_t axial,
     if (mapping == AXG_MAP_SPHERICAL) {
         co = curved_outer(nodal_sz);
         if (co < 0) return AXG_E_ARG;   // "Error identifying curved outer edge."
+    } else if (mapping == AXG_MAP_SEMI_SPHERICAL) {
+        co = curved_outer_semi(nodal_sz);
+        if (co < 0) return AXG_E_ARG;
     } else if (mapping != AXG_MAP_LINEAR) {
         return AXG_E_ARG;
     }
@@ -259,7 +316,8 @@ int axg_quad_geometry(int32_t mapping, const double *nodal_sz, int32_t axial,
             double s, z;
             Jac J;
             if (mapping == AXG_MAP_LINEAR) map_linear(nodal_sz, xi, eta, s, z, J);
-            else map_spherical(nodal_sz, co, xi, eta, s, z, J);
+            else if (mapping == AXG_MAP_SPHERICAL) map_spherical(nodal_sz, co, xi, eta, s, z, J);
+            else map_semi_spherical(nodal_sz, co, xi, eta, s, z, J);
             double det = J.J00 * J.J11 - J.J01 * J.J10;
             double f = w_xi[ipol] * t.wGLL[jpol] * det;
             if (axial) f *= (ipol == 0) ? J.J00 : s / (1. + xi);
@@ -272,6 +330,29 @@ int axg_quad_geometry(int32_t mapping, const double *nodal_sz, int32_t axial,
             inv_s[q] = (axial && ipol == 0) ? 0. : 1. / s;
             if (out_sz) { out_sz[q] = s; out_sz[25 + q] = z; }
         }
+    return AXG_OK;
+}
+
+// Mapping::mapping and Mapping::jacobian at one (xi, eta): out = s, z, J00, J01, J10, J11
+int axg_quad_map(int32_t mapping, const double *nodal_sz, double xi, double eta, double *out) {
+    if (!nodal_sz || !out) return AXG_E_ARG;
+    double s, z;
+    Jac J;
+    if (mapping == AXG_MAP_LINEAR) {
+        map_linear(nodal_sz, xi, eta, s, z, J);
+    } else if (mapping == AXG_MAP_SPHERICAL) {
+        int co = curved_outer(nodal_sz);
+        if (co < 0) return AXG_E_ARG;
+        map_spherical(nodal_sz, co, xi, eta, s, z, J);
+    } else if (mapping == AXG_MAP_SEMI_SPHERICAL) {
+        int co = curved_outer_semi(nodal_sz);
+        if (co < 0) return AXG_E_ARG;
+        map_semi_spherical(nodal_sz, co, xi, eta, s, z, J);
+    } else {
+        return AXG_E_ARG;
+    }
+    out[0] = s; out[1] = z;
+    out[2] = J.J00; out[3] = J.J01; out[4] = J.J10; out[5] = J.J11;
     return AXG_OK;
 }
 

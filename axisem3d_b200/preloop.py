@@ -1,0 +1,1219 @@
+"""The preloop: an Exodus mesh and the reference's input files -> a `Model` for the engine.
+
+This follows the reference's preloop (SOLVER/src/main.cpp:60-640) in its order and rules:
+geodesy (preloop/exodus/geodesy.{hpp,cpp}), absorbing boundaries (exodus/ABC.cpp), the Nr
+field (nr_field/NrField*.cpp, ExodusMesh::formNrAtNodes), quads (se_model/quad/Quad.cpp:
+mapping, material, integral factor, normals, dt), materials (quad/physical/Material.cpp,
+AttBuilder.cpp), GLL points and their boundaries (se_model/gll/GLLPoint.{hpp,cpp}), the time
+step (SE_Model::computeDt), sources (preloop/source/Source.cpp, Mechanism.cpp, core STF.cpp)
+and station groups (preloop/output/StationOutput.cpp).
+
+Supported inputs: 1-D models from the Exodus radial profile (isotropic or transversely
+isotropic, fluid layers, attenuation NONE / FULL / CG4), Cartesian and spherical meshes with
+all three mappings, Clayton and sponge boundaries, constant Nr (bounded by the in-plane
+resolution, rounded to FFT-friendly sizes), moment-tensor and force sources with Gaussian
+source-time functions anywhere in the solid, and solid station groups recording displacement
+(channels U, U1, U2, U3, U_NORM in the spz, RTZ, ENZ or xyz frame). Anything else named in the
+inputs (3-D models, other Nr fields, fluid-pressure sources, file STFs, strain / stress /
+curl channels, fluid stations, element output) raises `PreloopError` naming it.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import _lib as L
+from .exodus import ExodusMesh
+from .inparam import Inparam
+from .meshgen import (cg4_correct, geometry_batch, iso_with_attenuation, lagrange, round_dt, tables,
+                      tiso_with_attenuation, weights_cg4)
+from .model import STF, Model
+from .solver import att_alpha_beta_gamma, quad_dt
+
+EPS = np.finfo(np.float64).eps
+# vicinity::constants (mesh/topology/vicinity.hpp), nPol = 4
+NODE_IPNT = (0, 20, 24, 4)
+EDGE_IPNT = ((0, 5, 10, 15, 20), (20, 21, 22, 23, 24), (24, 19, 14, 9, 4), (4, 3, 2, 1, 0))
+# exodus element_type -> this package's mapping codes
+MAPPING = {0: L.AXG_MAP_SPHERICAL, 1: L.AXG_MAP_LINEAR, 2: L.AXG_MAP_SEMI_SPHERICAL}
+
+
+class PreloopError(RuntimeError):
+    """An input the preloop cannot use; messages follow "Class::method || text"."""
+
+
+def cround(x):
+    """C++ round(): halves away from zero."""
+    return np.sign(x) * np.floor(np.abs(x) + 0.5)
+
+
+# ------------------------------------------------------------------ Nr field ---
+def is_lucky(n: int) -> bool:
+    """NrField::isLuckyNumber: largest prime factor <= 13, at most one factor 11 or 13."""
+    num = n
+    for p in (2, 3, 5, 7, 11, 13):
+        while num % p == 0:
+            num //= p
+    if num != 1:
+        return False
+    e = 0
+    num = n
+    while num % 11 == 0:
+        num //= 11
+        e += 1
+    while num % 13 == 0:
+        num //= 13
+        e += 1
+    return e <= 1
+
+
+def next_lucky(n: int) -> int:
+    """NrField::nextLuckyNumber: the smallest lucky number >= n."""
+    m = max(int(n), 1)
+    while not is_lucky(m):
+        m += 1
+    return m
+
+
+# ------------------------------------------------------------------- geodesy ---
+class Geodesy:
+    """geodesy::setup and the transforms of geodesy.hpp."""
+
+    FLATTENING = {"SPHERE": 0., "WGS84": 1. / 298.257223563, "GRS80": 1. / 298.257222101,
+                  "SPECFEM3D_GLOBE": 1. / 299.8}
+
+    def __init__(self, mesh: ExodusMesh, inp: Inparam):
+        self.cartesian = mesh.is_cartesian
+        self.outer_radius = mesh.mesh_surface
+        self.inner_radius = mesh.mesh_bottom
+        self.outer_solid_radius = mesh.solid_surface
+        key = "geodesy:flattening_on_surface"
+        fl = inp.model.get(key)
+        try:
+            f = self.FLATTENING[fl] if fl in self.FLATTENING else float(fl)
+        except ValueError:
+            raise PreloopError("geodesy::setup || Invalid %s: %s" % (key, fl))
+        if f < EPS or self.cartesian:
+            f = 0.
+        self.outer_flattening = f
+        self.ellip_r = mesh.ellipticity[0].copy()
+        self.ellip_f = mesh.ellipticity[1] * f
+        gz = inp.model.get("geodesy:lat_lon_north_pole_mesh")
+        if gz == "SOURCE":
+            name = inp.source.get("list_of_sources:{0}")
+            root = "list_of_sources:[0]:%s:location" % name
+            try:
+                lat = inp.source.get_bounded(root + ":latitude_longitude:[0]", -90., 90.)
+                lon = inp.source.get_bounded(root + ":latitude_longitude:[1]", -180., 180.)
+            except Exception:
+                raise PreloopError("geodesy::setup || Error determining the geographic location of the "
+                                   "first || source in list_of_sources in inparam.source.yaml; || "
+                                   "location:latitude_longitude must be presented.")
+            if inp.source.contains(root + ":depth"):
+                depth = inp.source.get_bounded(root + ":depth", 0., self.outer_radius)
+                solid = inp.source.get(root + ":depth_below_solid_surface", bool)
+                r = (self.outer_solid_radius if solid else self.outer_radius) - depth
+            else:
+                r = inp.source.get_bounded(root + ":radius", 0., self.outer_radius)
+        else:
+            lat = inp.model.get_bounded("geodesy:lat_lon_north_pole_mesh:[0]", -90., 90.)
+            lon = inp.model.get_bounded("geodesy:lat_lon_north_pole_mesh:[1]", -180., 180.)
+            r = self.outer_radius
+        self.llr_axis = np.array([lat, lon, r])
+        th, ph, _ = self.llr2tpr(self.llr_axis[None, :], True)[0]
+        Q = np.array([[math.cos(th) * math.cos(ph), -math.sin(ph), math.sin(th) * math.cos(ph)],
+                      [math.cos(th) * math.sin(ph), math.cos(ph), math.sin(th) * math.sin(ph)],
+                      [-math.sin(th), 0., math.cos(th)]])
+        self.src2geo = Q.T
+
+    def flattening(self, r):
+        """geodesy::computeFlattening: the ellipticity curve, clamped at its ends."""
+        r = np.atleast_1d(np.asarray(r, dtype=np.float64))
+        R, F = self.ellip_r, self.ellip_f
+        tol = (R[-1] - R[0]) * EPS
+        out = np.empty_like(r)
+        for k, x in enumerate(r):
+            if x < R[0] - tol or x > R[-1] + tol:
+                out[k] = F[-1] if x > R[-1] else F[0]
+                continue
+            i1 = int(np.searchsorted(R, x, side="right"))
+            i1 = 1 if i1 == 0 else (len(R) - 1 if i1 == len(R) else i1)
+            i0 = i1 - 1
+            f1 = (x - R[i0]) / (R[i1] - R[i0])
+            out[k] = F[i0] * (1. - f1) + F[i1] * f1
+        return out
+
+    def llr2tpr(self, llr, ellipticity):
+        llr = np.atleast_2d(llr)
+        tpr = np.empty_like(llr, dtype=np.float64)
+        t = np.radians(llr[:, 0])
+        if ellipticity:
+            t = np.arctan(np.tan(t) * (self.flattening(llr[:, 2]) - 1.) ** 2)
+        tpr[:, 0] = np.pi / 2. - t
+        tpr[:, 1] = np.radians(llr[:, 1])
+        tpr[:, 2] = llr[:, 2]
+        return tpr
+
+    def tpr2llr(self, tpr, ellipticity):
+        tpr = np.atleast_2d(tpr)
+        llr = np.empty_like(tpr, dtype=np.float64)
+        lat = np.pi / 2. - tpr[:, 0]
+        if ellipticity:
+            lat = np.arctan(np.tan(lat) / (self.flattening(tpr[:, 2]) - 1.) ** 2)
+        llr[:, 0] = np.degrees(lat)
+        llr[:, 1] = np.degrees(tpr[:, 1])
+        llr[:, 2] = tpr[:, 2]
+        return llr
+
+    @staticmethod
+    def _xy2sphi(x, y, undefined):
+        s = np.hypot(x, y)
+        with np.errstate(invalid="ignore"):
+            p = np.where((np.abs(x) < EPS) & (np.abs(y) < EPS), undefined, np.arctan2(y, x))
+        return s, p
+
+    def llr2spz(self, llr, ellipticity):
+        tpr = self.llr2tpr(llr, ellipticity)
+        xyz = np.stack([tpr[:, 2] * np.sin(tpr[:, 0]) * np.cos(tpr[:, 1]),
+                        tpr[:, 2] * np.sin(tpr[:, 0]) * np.sin(tpr[:, 1]),
+                        tpr[:, 2] * np.cos(tpr[:, 0])], axis=1)
+        src = xyz @ self.src2geo.T
+        err = np.finfo(np.float64).min
+        s, p = self._xy2sphi(src[:, 0], src[:, 1], err)
+        p = np.where(p < err * .9, tpr[:, 1], p)
+        return np.stack([s, p, src[:, 2]], axis=1)
+
+    def spz2llr(self, spz, ellipticity, lon360):
+        spz = np.atleast_2d(spz)
+        xyz = np.stack([spz[:, 0] * np.cos(spz[:, 1]), spz[:, 0] * np.sin(spz[:, 1]), spz[:, 2]], axis=1)
+        geo = xyz @ self.src2geo
+        err = np.finfo(np.float64).min
+        s, p = self._xy2sphi(geo[:, 0], geo[:, 1], err)
+        p = np.where(p < err * .9, spz[:, 1], p)
+        r = np.hypot(s, geo[:, 2])
+        t = np.where(r < EPS, 0., np.arccos(np.clip(geo[:, 2] / np.maximum(r, EPS), -1., 1.)))
+        llr = self.tpr2llr(np.stack([t, p, r], axis=1), ellipticity)
+        llr[:, 2] = np.hypot(spz[:, 0], spz[:, 2])
+        if lon360:
+            llr[:, 1] = np.where(llr[:, 1] < 0., llr[:, 1] + 360., llr[:, 1])
+        else:
+            llr[:, 1] = np.where(llr[:, 1] > 180., llr[:, 1] - 360., llr[:, 1])
+        return llr
+
+    def back_azimuth(self, llr, ellipticity):
+        """geodesy::backAzimuth."""
+        src = self.llr2tpr(self.llr_axis[None, :], ellipticity)[0]
+        d, e = math.sin(src[1]), -math.cos(src[1])
+        f, c = -math.sin(src[0]), math.cos(src[0])
+        a, b = f * e, -f * d
+        tpr = self.llr2tpr(llr, ellipticity)
+        dd, ee = np.sin(tpr[:, 1]), -np.cos(tpr[:, 1])
+        ff, cc = -np.sin(tpr[:, 0]), np.cos(tpr[:, 0])
+        gg, hh = -cc * ee, cc * dd
+        x = (a - gg) ** 2 + (b - hh) ** 2 + (c - ff) ** 2 - 2.
+        y = (a - dd) ** 2 + (b - ee) ** 2 + c * c - 2.
+        return self._xy2sphi(x, y, 0.)[1]
+
+
+def sz2rtheta(s, z):
+    """geodesy::sz2rtheta: r and the polar angle acos(z / r) (0 at r = 0)."""
+    r = np.hypot(s, z)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        t = np.where(r < EPS, 0., np.arccos(np.clip(z / np.maximum(r, EPS), -1., 1.)))
+    return r, t
+
+
+# ----------------------------------------------------------------------- ABC ---
+@dataclass
+class ABC:
+    """ABC::buildInparam: the boundaries the user asked for and the mesh has."""
+    user_keys: List[str] = field(default_factory=list)
+    keys: List[str] = field(default_factory=list)
+    clayton: bool = False
+    sponge: bool = False
+    outer_span: dict = field(default_factory=dict)
+    expr_solid: str = ""
+    expr_fluid: str = ""
+    t0: float = 0.0
+
+    def u0(self, span, vp, vs, rho, fluid):
+        """ABC::getU0Solid / getU0Fluid: the user's gamma expression."""
+        expr = self.expr_fluid if fluid else self.expr_solid
+        env = {"VP": vp, "RHO": rho, "SPAN": span, "T0": self.t0, "exp": np.exp, "sqrt": np.sqrt,
+               "log": np.log, "abs": np.abs, "sin": np.sin, "cos": np.cos, "tan": np.tan, "pi": math.pi,
+               "pow": np.power, "min": np.minimum, "max": np.maximum}
+        if not fluid:
+            env["VS"] = vs
+        try:
+            return np.asarray(eval(expr.replace("^", "**"), {"__builtins__": {}}, env), dtype=np.float64)
+        except Exception as ex:
+            raise PreloopError("ABC::buildInparam || Error evaluating Kosloff_Kosloff::gamma_expr_%s: %s"
+                               % ("fluid" if fluid else "solid", ex))
+
+
+def build_abc(mesh: ExodusMesh, inp: Inparam) -> ABC:
+    gm = inp.model
+    root = "absorbing_boundary"
+    abc = ABC()
+    abc.user_keys = gm.get_vector(root + ":boundaries")
+    if not abc.user_keys:
+        return abc
+    if len(abc.user_keys) > 3:
+        raise PreloopError("ABC::buildInparam || Parameter absorbing_boundary:boundaries || "
+                           "cannot contain more than three entities.")
+    if len(set(abc.user_keys)) != len(abc.user_keys):
+        raise PreloopError("ABC::buildInparam || Parameter absorbing_boundary:boundaries || "
+                           "cannot contain duplicated entities.")
+    for k in abc.user_keys:
+        if k not in ("RIGHT", "BOTTOM", "TOP"):
+            raise PreloopError("ABC::buildInparam || Parameter absorbing_boundary:boundaries || "
+                               "contains an invalid entity: " + k)
+    abc.clayton = gm.get(root + ":enable_Clayton_Enquist", bool)
+    root += ":Kosloff_Kosloff"
+    abc.sponge = gm.get(root + ":enable", bool)
+    if not abc.clayton and not abc.sponge:
+        raise PreloopError("ABC::buildInparam || Both Clayton-Enquist and Kosloff-Kosloff are disabled.")
+    rel = []
+    if abc.sponge:
+        rel = gm.get_vector(root + ":relative_spans", float)
+        if len(rel) != len(abc.user_keys):
+            raise PreloopError("ABC::buildInparam || The number of Kosloff_Kosloff::relative_spans || "
+                               "does not match the number of boundaries.")
+        if min(rel) < .01 or max(rel) > .25:
+            raise PreloopError("ABC::buildInparam || Kosloff_Kosloff:relative_spans must range "
+                               "between 0.01 and 0.25.")
+        abc.expr_solid = gm.get(root + ":gamma_expr_solid")
+        abc.expr_fluid = gm.get(root + ":gamma_expr_fluid")
+    for i, k in enumerate(abc.user_keys):
+        present, outer, span = mesh.boundary_info_abc(k)
+        if present:
+            abc.keys.append(k)
+            if abc.sponge:
+                abc.outer_span[k] = (outer, rel[i] * span)
+    if abc.sponge:
+        abc.t0 = mesh.global_variables["minimum_period"]
+    return abc
+
+
+# ------------------------------------------------------------------- Nr field ---
+def nodal_nr(mesh: ExodusMesh, inp: Inparam, lucky: bool) -> np.ndarray:
+    """Nr at the mesh nodes (NrField::buildInparam, ExodusMesh::formNrAtNodes)."""
+    kind = inp.nr.get_options("type_Nr", {"CONSTANT": "CONSTANT", "ANALYTICAL": "ANALYTICAL",
+                                          "POINTWISE": "POINTWISE", "STRUCTURED": "STRUCTURED"})
+    if kind != "CONSTANT":
+        raise PreloopError("NrField::buildInparam || type_Nr = %s is not supported by this build; "
+                           "use CONSTANT." % kind)
+    nr = np.full(mesh.num_nodes, inp.nr.get_bounded("constant", 1, None, int), np.int64)
+    if inp.nr.get("bound_Nr_by_inplane", bool):
+        conn, xy = mesh.connectivity, mesh.coords
+        edges = np.zeros(mesh.num_quads)
+        for a in range(4):
+            b = (a + 1) % 4
+            edges += np.hypot(*(xy[conn[:, a]] - xy[conn[:, b]]).T)
+        tot = np.zeros(mesh.num_nodes)
+        cnt = np.zeros(mesh.num_nodes)
+        for a in range(4):
+            np.add.at(tot, conn[:, a], edges)
+            np.add.at(cnt, conn[:, a], 1.)
+        ave = tot / np.maximum(cnt * 4 * 4, 1.)
+        circ = 2. * np.pi * xy[:, 0]
+        upper = np.maximum(cround(circ / np.where(ave > 0, ave, 1.)), 1).astype(np.int64)
+        upper = np.where(xy[:, 0] < mesh.global_variables["dist_tolerance"], 5, upper)
+        nr = np.minimum(nr, upper)
+    if lucky:
+        nr = np.array([next_lucky(int(n)) for n in nr], np.int64)
+    if nr.min() < 1:
+        raise PreloopError("ExodusMesh::formNrAtNodes || Nr must be positive.")
+    return nr
+
+
+def gll_shape(axial: np.ndarray) -> np.ndarray:
+    """spectrals::interpolateGLL: (nq, 4, 25) bilinear shape functions at the element points."""
+    t = tables()
+    out = np.zeros((len(axial), 4, 25))
+    for ax in (0, 1):
+        xi = np.repeat(t["pGLJ"] if ax else t["pGLL"], 5)
+        eta = np.tile(t["pGLL"], 5)
+        lsf = np.stack([(1 - xi) * (1 - eta), (1 + xi) * (1 - eta), (1 + xi) * (1 + eta),
+                        (1 - xi) * (1 + eta)]) / 4.
+        out[np.asarray(axial) == ax] = lsf
+    return out
+
+
+# ------------------------------------------------------------------ the build ---
+@dataclass
+class StationGroup:
+    """One station group of inparam.output.yaml after location (StationOutput::release)."""
+    name: str
+    keys: List[str]
+    channels: List[str]
+    frame: str
+    interval: int
+    tmin: float
+    tmax: float
+    fmt: str
+    buffer_size: int
+    first: int                                  # index of the group's first station in the model
+    theta: np.ndarray = None
+    baz: np.ndarray = None
+    phi: np.ndarray = None
+
+
+@dataclass
+class Simulation:
+    """What the preloop hands to the time loop."""
+    model: Model
+    nsteps: int
+    t0: float
+    dt: float
+    groups: List[StationGroup]
+    mesh: ExodusMesh
+    cartesian: bool
+    info: dict
+
+
+def _read_stf(gm, root, name, dt):
+    """STF::buildInparam (core/source/elem_src/stf/STF.cpp:19-40), GaussianSTF."""
+    cls = gm.get(root + ":class_name")
+    if cls != "GaussianSTF":
+        raise PreloopError("STF::buildInparam || class_name %s is not supported by this build "
+                           "(GaussianSTF only). || Source name: %s" % (cls, name))
+    hdur = gm.get_bounded(root + ":half_duration", 0.)
+    hdur = max(hdur, dt * 5.)                     # dt * 5 as the minimum
+    decay = gm.get_bounded(root + ":decay_factor", 0.)
+    shift = gm.get(root + ":time_shift", float)
+    order = gm.get_options(root + ":use_derivative_integral",
+                           {"ERF": -1, "GAUSSIAN": 0, "FIRST_DERIVATIVE": 1, "RICKER": 2})
+    return STF(half_duration=hdur, decay_factor=decay, time_shift=shift, derivative_order=order)
+
+
+class _Quads:
+    """Per-quad geometry, boundaries and material in arrays over all quads."""
+
+    def __init__(self, mesh: ExodusMesh, inp: Inparam, geo: Geodesy, abc: ABC, lucky: bool):
+        self.mesh = mesh
+        nq = mesh.num_quads
+        conn = mesh.connectivity
+        self.nodal = mesh.coords[conn].reshape(nq, 8)
+        self.axial = np.array([mesh.left_side(q) >= 0 for q in range(nq)], np.uint8)
+        self.fluid = mesh.is_fluid.astype(bool)
+        self.sides = {"LEFT": [mesh.left_side(q) for q in range(nq)],
+                      "RIGHT": [mesh.right_side(q) for q in range(nq)],
+                      "BOTTOM": [mesh.bottom_side(q) for q in range(nq)],
+                      "TOP": [mesh.top_side(q) for q in range(nq)],
+                      "SOLID_FLUID": [mesh.side("solid_fluid_boundary", q) for q in range(nq)]}
+        # mapping: operands and point coordinates
+        self.geom = np.zeros((nq, 6, 25))
+        self.sz = np.zeros((nq, 2, 25))
+        for gt, mp in MAPPING.items():
+            sel = np.nonzero(mesh.geometry_type == gt)[0]
+            if len(sel):
+                try:
+                    g, s = geometry_batch(self.nodal[sel], self.axial[sel], mp)
+                except RuntimeError:
+                    raise PreloopError("Quad::Quad || Error identifying curved outer edge "
+                                       "(element_type %d)." % gt)
+                self.geom[sel], self.sz[sel] = g, s
+        unknown = set(np.unique(mesh.geometry_type).tolist()) - set(MAPPING)
+        if unknown:
+            raise PreloopError("Quad::Quad || Unknown element_type %s." % sorted(unknown))
+        # Jacobian at the points, recovered from the operands (exact inverse of the stored form)
+        a, b, c, d = self.geom[:, 0], self.geom[:, 1], self.geom[:, 2], self.geom[:, 3]
+        det = 1. / (a * d - b * c)
+        self.J = np.stack([a * det, -b * det, -c * det, d * det], axis=-1).reshape(nq, 25, 2, 2)
+        # point Nr: nodal Nr interpolated to the points and rounded (Quad::Quad)
+        nnr = nodal_nr(mesh, inp, lucky)
+        shp = gll_shape(self.axial)
+        self.pnr = cround(np.einsum("qk,qkp->qp", nnr[conn].astype(np.float64), shp)).astype(np.int64)
+        if lucky:
+            self.pnr = np.vectorize(next_lucky)(self.pnr)
+        self._material(mesh, geo, shp)
+
+    def _material(self, mesh, geo, shp):
+        """Material::Material: the radial profile at the nodes, then at the points."""
+        rc = mesh.radial_coords
+        tol = mesh.global_variables["dist_tolerance"]
+        xy = self.nodal.reshape(-1, 4, 2)
+        r = xy[:, :, 1] if geo.cartesian else np.hypot(xy[:, :, 0], xy[:, :, 1])
+        center = r.mean(axis=1)
+        i1 = np.searchsorted(rc, center, side="right")
+        i1 = np.where(i1 == 0, 1, np.where(i1 == len(rc), len(rc) - 1, i1))
+        i0 = i1 - 1
+        r0 = rc[i0] - tol
+        r1 = rc[i1] + tol
+        nodal = {}
+        for name, vals in mesh.radial_variables.items():
+            v0, v1 = vals[i0], vals[i1]
+            nodal[name] = ((v1 - v0) / (r1 - r0))[:, None] * (r - r0[:, None]) + v0[:, None]
+        vs_key = "VS" if "VS" in nodal else "VSV"
+        fluid_mat = np.max(nodal[vs_key], axis=1) < EPS
+        if "VSH" in nodal:
+            fluid_mat |= np.max(nodal["VSH"], axis=1) < EPS
+        if np.any(fluid_mat != self.fluid):
+            q = int(np.nonzero(fluid_mat != self.fluid)[0][0])
+            raise PreloopError("Material::getMass || Incompatible solid/fluid flags. || Element %d" % q)
+        tiso = "VPV" in nodal
+        iso_e = np.ones(len(center), bool)
+        if tiso:
+            nrm = lambda v: np.sqrt(np.sum(v * v, axis=1))     # noqa: E731
+            iso_e = ((nrm(nodal["VPV"] - nodal["VPH"]) < nrm(nodal["VPV"]) * EPS) &
+                     (nrm(nodal["VSV"] - nodal["VSH"]) < nrm(nodal["VSV"]) * EPS) &
+                     (nrm(nodal["ETA"] - 1.) < 2. * EPS))
+        self.iso = iso_e
+        self.tiso = tiso
+        pt = {k: np.einsum("qk,qkp->qp", v, shp) for k, v in nodal.items()}
+        self.prop = pt
+        rho = pt["RHO"]
+        if tiso:
+            vp_iso, vs_iso = pt["VPV"], pt["VSV"]
+            self.vmax = np.where(iso_e[:, None], vp_iso, np.maximum(pt["VPV"], pt["VPH"]))
+            self.vp_c = np.where(iso_e[:, None], vp_iso, pt["VPV"])
+            self.vs_c = np.where(iso_e[:, None], vs_iso, pt["VSV"])
+        else:
+            self.vmax = pt["VP"]
+            self.vp_c, self.vs_c = pt["VP"], pt["VS"]
+        self.rho = rho
+
+    def normals(self, q, edge):
+        """Quad::computeNormal: (points, (5, 2) normals) of one edge."""
+        t = tables()
+        ax = bool(self.axial[q])
+        out = np.zeros((5, 2))
+        pts = EDGE_IPNT[edge]
+        for ip, p in enumerate(pts):
+            J = self.J[q, p]
+            if edge == 0:
+                n = np.array([J[1, 0], -J[0, 0]])
+            elif edge == 1:
+                n = np.array([J[1, 1], -J[0, 1]])
+            elif edge == 2:
+                n = np.array([-J[1, 0], J[0, 0]])
+            else:
+                n = np.array([-J[1, 1], J[0, 1]])
+            ipol, jpol = p // 5, p % 5
+            if ax:
+                if edge % 2 != 0:
+                    raise PreloopError("Quad::computeNormal || Impossible.")
+                n = n * t["wGLJ"][ipol]
+            else:
+                n = n * t["wGLL"][ipol if edge % 2 == 0 else jpol]
+            s = self.sz[q, 0, p]
+            if ax:
+                n = n * (J[0, 0] if ipol == 0 else s / (1. + t["pGLJ"][ipol]))
+            else:
+                n = n * s
+            out[ip] = n
+        return list(pts), out
+
+
+def _gll_numbering(conn: np.ndarray) -> np.ndarray:
+    """Global GLL point of every (quad, point), from the mesh topology: vertices by node,
+    edge points by (sorted node pair, position from the lower node), the rest per quad."""
+    nq = len(conn)
+    keys = {}
+    out = np.zeros((nq, 25), np.int64)
+    edge_nodes = ((0, 1), (1, 2), (2, 3), (3, 0))
+    where = {}
+    for e, pts in enumerate(EDGE_IPNT):
+        for k, p in enumerate(pts[1:4]):
+            where[p] = (e, k + 1)
+    for q in range(nq):
+        c = conn[q]
+        for p in range(25):
+            if p in NODE_IPNT:
+                key = ("v", int(c[NODE_IPNT.index(p)]))
+            elif p in where:
+                e, k = where[p]
+                na, nb = int(c[edge_nodes[e][0]]), int(c[edge_nodes[e][1]])
+                key = ("e", na, nb, k) if na < nb else ("e", nb, na, 4 - k)
+            else:
+                key = ("i", q, p)
+            g = keys.get(key)
+            if g is None:
+                g = len(keys)
+                keys[key] = g
+            out[q, p] = g
+    return out
+
+
+def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_channels: bool = False
+          ) -> Simulation:
+    """Run the preloop on one input directory. skip_unsupported_channels: drop station channels
+    this build does not record (strain, curl, ...) instead of raising; a group left without
+    channels is dropped, and info["skipped_channels"] names them."""
+    inp = Inparam(input_dir)
+    mesh = ExodusMesh(inp.path(inp.model.get("model1D:exodus_mesh")))
+    if inp.model.contains("list_of_3D_models") and inp.model.get_vector("list_of_3D_models"):
+        raise PreloopError("Model3D::buildInparam || 3-D models are not supported by this build.")
+    geo = Geodesy(mesh, inp)
+    abc = build_abc(mesh, inp)
+    lucky = inp.advanced.get("develop:fftw_lucky_numbers", bool) \
+        if inp.advanced.contains("develop:fftw_lucky_numbers") else True
+    quads = _Quads(mesh, inp, geo, abc, lucky)
+    nq = mesh.num_quads
+    tol = mesh.global_variables["dist_tolerance"]
+
+    # ---- time step (SE_Model::computeDt, main.cpp:431-470)
+    courant = inp.source.get_bounded("time_axis:Courant_number", 0.0)
+    dts = np.empty(nq)
+    for q in range(nq):
+        f = 1.
+        if quads.sides["SOLID_FLUID"][q] != -1:
+            f = .9
+        if abc.clayton and any(quads.sides[k][q] != -1 for k in abc.keys):
+            f = .5
+        dts[q] = quad_dt(quads.sz[q], float(np.max(quads.vmax[q]))) * f * courant
+    dt_mesh = round_dt(float(dts.min()))
+    enforced = inp.source.get("time_axis:enforced_dt")
+    dt = dt_mesh if enforced == "NONE" or float(enforced) < EPS else float(enforced)
+
+    # ---- attenuation (main.cpp:482-499, AttBuilder)
+    att = inp.model.get_options("attenuation", {"NONE": -1, "FULL": 0, "CG4": 1})
+    sls = None
+    if att >= 0 and mesh.has_attenuation:
+        gv = mesh.global_variables
+        n = int(gv["nr_lin_solids"])
+        sls = {"w": np.array([gv["attenuation_w_%d" % i] for i in range(n)]),
+               "y": np.array([gv["attenuation_y_%d" % i] for i in range(n)]),
+               "fmin": gv["attenuation_f_min"], "fmax": gv["attenuation_f_max"],
+               "fref": gv["attenuation_f_ref"]}
+        fmesh = 1. / gv["minimum_period"]
+        if fmesh < sls["fmin"] or fmesh > sls["fmax"]:
+            raise PreloopError("AttBuilder::AttBuilder || Mesh frequency lies out of attenuation band.")
+
+    # ---- GLL points
+    gll = _gll_numbering(mesh.connectivity)
+    ngll = int(gll.max()) + 1
+    coords = np.zeros((ngll, 2))
+    coords[gll.ravel(), 0] = quads.sz[:, 0, :].ravel()
+    coords[gll.ravel(), 1] = quads.sz[:, 1, :].ravel()
+    dev = np.abs(coords[gll, 0] - quads.sz[:, 0, :]) + np.abs(coords[gll, 1] - quads.sz[:, 1, :])
+    if dev.max() > tol:
+        raise PreloopError("LocalMesh::buildElementGLL || Non-conforming mesh: GLL points of "
+                           "neighbouring elements differ by %g." % dev.max())
+    pnr = np.zeros(ngll, np.int64)
+    np.maximum.at(pnr, gll.ravel(), quads.pnr.ravel())
+    solid_q = np.nonzero(~quads.fluid)[0]
+    fluid_q = np.nonzero(quads.fluid)[0]
+    sp_used = np.unique(gll[solid_q].ravel()) if len(solid_q) else np.zeros(0, np.int64)
+    fp_used = np.unique(gll[fluid_q].ravel()) if len(fluid_q) else np.zeros(0, np.int64)
+    sid = -np.ones(ngll, np.int64)
+    fid = -np.ones(ngll, np.int64)
+    sid[sp_used] = np.arange(len(sp_used))
+    fid[fp_used] = np.arange(len(fp_used))
+    ifact = quads.geom[:, 5, :]
+    smass = np.zeros(len(sp_used))
+    np.add.at(smass, sid[gll[solid_q]].ravel(), (quads.rho[solid_q] * ifact[solid_q]).ravel())
+    fmass = np.zeros(len(fp_used))
+    if len(fluid_q):
+        kappa = quads.rho[fluid_q] * quads.vp_c[fluid_q] ** 2
+        np.add.at(fmass, fid[gll[fluid_q]].ravel(), (ifact[fluid_q] / kappa).ravel())
+
+    # ---- boundaries of the points (Quad::setupGLL, GLLPoint::release)
+    axial_pt = np.zeros(ngll, bool)
+    surface_pt = np.zeros(ngll, bool)
+    normal = np.zeros((ngll, 2))
+    cl_s, cl_f = [], []
+    gamma_sum = np.zeros(ngll)
+    gamma_cnt = np.zeros(ngll, np.int64)
+    for q in range(nq):
+        if quads.axial[q]:
+            for p in EDGE_IPNT[quads.sides["LEFT"][q]]:
+                axial_pt[gll[q, p]] = True
+        if quads.sides["TOP"][q] != -1:
+            for p in EDGE_IPNT[quads.sides["TOP"][q]]:
+                surface_pt[gll[q, p]] = True
+        if quads.sides["SOLID_FLUID"][q] != -1:
+            pts, nsf = quads.normals(q, quads.sides["SOLID_FLUID"][q])
+            for p, n in zip(pts, nsf):
+                normal[gll[q, p]] += n / 2. if quads.fluid[q] else -n / 2.
+        if abc.clayton:
+            for key in abc.keys:
+                edge = quads.sides[key][q]
+                if edge == -1:
+                    continue
+                pts, nab = quads.normals(q, edge)
+                for p, n in zip(pts, nab):
+                    g = gll[q, p]
+                    area = float(np.hypot(n[0], n[1]))
+                    if area <= 0.:
+                        continue
+                    rv = quads.rho[q, p] * quads.vp_c[q, p]
+                    if quads.fluid[q]:
+                        cl_f.append((fid[g], rv, area))
+                    else:
+                        _, th = sz2rtheta(n[0], n[1])
+                        cl_s.append((sid[g], rv, quads.rho[q, p] * quads.vs_c[q, p], area, float(th)))
+        if abc.sponge:
+            for p in range(25):
+                gmax = 0.
+                dmin = 1.
+                s_, z_ = quads.sz[q, 0, p], quads.sz[q, 1, p]
+                for key in abc.keys:
+                    outer, span = abc.outer_span[key]
+                    if geo.cartesian:
+                        coord = s_ if key == "RIGHT" else z_
+                        r_ = z_
+                    else:
+                        r_, t_ = sz2rtheta(s_, z_)
+                        coord = float(t_) if key == "RIGHT" else float(r_)
+                    dist = (outer - coord) / span
+                    if dist > dmin:
+                        continue
+                    dmin = dist
+                    pattern = math.cos(math.pi / 2. * dist) ** 2
+                    if not geo.cartesian and key == "RIGHT":
+                        span = span * float(r_)
+                    gmax = float(abc.u0(abs(span), quads.vp_c[q, p], quads.vs_c[q, p], quads.rho[q, p],
+                                        bool(quads.fluid[q]))) * pattern
+                if abs(gmax) > EPS:
+                    g = gll[q, p]
+                    gamma_sum[g] += gmax
+                    gamma_cnt[g] += 1
+
+    # ---- model
+    m = Model(dt=dt)
+    m.sp_nr = pnr[sp_used].astype(np.int32)
+    m.sp_mass = smass
+    m.sp_axial = axial_pt[sp_used].astype(np.uint8)
+    m.sp_coords = coords[sp_used]
+    m.fp_nr = pnr[fp_used].astype(np.int32)
+    m.fp_mass = fmass
+    m.fp_axial = axial_pt[fp_used].astype(np.uint8)
+    fsurf = surface_pt & ("TOP" not in abc.keys)
+    m.fp_surface = fsurf[fp_used].astype(np.uint8)
+    # solid elements
+    ns = len(solid_q)
+    enr = np.array([int(pnr[gll[q]].max()) for q in range(nq)], np.int64)
+    theta = sz2rtheta(quads.sz[:, 0, :], quads.sz[:, 1, :])[1]
+    m.se_nr = enr[solid_q].astype(np.int32)
+    m.se_pts = sid[gll[solid_q]].astype(np.int32)
+    m.se_axial = quads.axial[solid_q]
+    m.se_geom = quads.geom[solid_q]
+    m.se_is3d = np.zeros(ns, np.uint8)
+    m.se_theta = theta[solid_q]
+    rheo = np.where(quads.iso[solid_q], L.AXG_ISO, L.AXG_TISO).astype(np.int32)
+    m.se_rheo = rheo
+    m.se_rtz = ((rheo == L.AXG_TISO) & (not geo.cartesian)).astype(np.uint8)
+    nmod = np.where(rheo == L.AXG_ISO, 2, 5)
+    mat_off = np.zeros(ns, np.int64)
+    if ns:
+        mat_off[1:] = np.cumsum(nmod * 25)[:-1]
+    moduli = np.zeros(int(np.sum(nmod * 25)))
+    P = quads.prop
+    rho_s = quads.rho[solid_q]
+    if quads.tiso:
+        A = rho_s * P["VPH"][solid_q] ** 2
+        Cm = rho_s * P["VPV"][solid_q] ** 2
+        Lm = rho_s * P["VSV"][solid_q] ** 2
+        N = rho_s * P["VSH"][solid_q] ** 2
+        F = P["ETA"][solid_q] * (A - 2. * Lm)
+    mu = rho_s * quads.vs_c[solid_q] ** 2
+    lam = rho_s * quads.vp_c[solid_q] ** 2 - 2. * mu
+    npa = 4 if att == 1 else 25
+    if sls is not None:
+        qk, qm = P["QKAPPA"][solid_q], P["QMU"][solid_q]
+        att_mod = np.zeros(ns * 2 * npa)
+        wcg4 = weights_cg4(ifact[solid_q]) if att == 1 else None
+    iso_sel = np.nonzero(rheo == L.AXG_ISO)[0]
+    ti_sel = np.nonzero(rheo == L.AXG_TISO)[0]
+    dl_all = np.zeros((ns, npa))
+    dm_all = np.zeros((ns, npa))
+    if len(iso_sel):
+        l_, m_ = lam[iso_sel], mu[iso_sel]
+        if sls is not None and att == 0:
+            l_, m_, dl, dm = iso_with_attenuation(l_, m_, qk[iso_sel], qm[iso_sel], sls)
+            dl_all[iso_sel], dm_all[iso_sel] = dl, dm
+        elif sls is not None:
+            kp = (l_ + (2. / 3.) * m_)[:, None, :]
+            kp2, mu2, dl4, dm4 = cg4_correct(kp, m_[:, None, :], qk[iso_sel][:, None, :],
+                                             qm[iso_sel][:, None, :], wcg4[iso_sel], sls)
+            l_, m_ = (kp2 - (2. / 3.) * mu2)[:, 0], mu2[:, 0]
+            dl_all[iso_sel], dm_all[iso_sel] = dl4[:, 0], dm4[:, 0]
+        for k, e in enumerate(iso_sel):
+            moduli[mat_off[e]:mat_off[e] + 25] = l_[k]
+            moduli[mat_off[e] + 25:mat_off[e] + 50] = m_[k]
+    if len(ti_sel):
+        a_, c_, f_, l_, n_ = (x[ti_sel] for x in (A, Cm, F, Lm, N))
+        if sls is not None and att == 0:
+            a_, c_, f_, l_, n_, dl, dm = tiso_with_attenuation(a_, c_, f_, l_, n_, qk[ti_sel], qm[ti_sel], sls)
+            dl_all[ti_sel], dm_all[ti_sel] = dl, dm
+        elif sls is not None:
+            kp = (a_ * 4. + c_ + f_ * 4. - n_ * 4.) / 9.
+            mu0 = (a_ + c_ - f_ * 2. + l_ * 6. + n_ * 5.) / 15.
+            kp2, mu2, dl4, dm4 = cg4_correct(kp[:, None, :], mu0[:, None, :], qk[ti_sel][:, None, :],
+                                             qm[ti_sel][:, None, :], wcg4[ti_sel], sls)
+            kp2, mu2 = kp2[:, 0], mu2[:, 0]
+            a_ = a_ - (kp + 4. / 3. * mu0) + (kp2 + 4. / 3. * mu2)
+            c_ = c_ - (kp + 4. / 3. * mu0) + (kp2 + 4. / 3. * mu2)
+            f_ = f_ - (kp - 2. / 3. * mu0) + (kp2 - 2. / 3. * mu2)
+            l_ = l_ - mu0 + mu2
+            n_ = n_ - mu0 + mu2
+            dl_all[ti_sel], dm_all[ti_sel] = dl4[:, 0], dm4[:, 0]
+        for k, e in enumerate(ti_sel):
+            for j, v in enumerate((a_, c_, f_, l_, n_)):
+                moduli[mat_off[e] + 25 * j:mat_off[e] + 25 * (j + 1)] = v[k]
+    m.se_mat_off = mat_off
+    m.se_moduli = moduli
+    if sls is not None and ns:
+        m.se_att = np.full(ns, L.AXG_ATT_CG4 if att == 1 else L.AXG_ATT_FULL, np.int32)
+        m.se_att_off = np.arange(ns, dtype=np.int64) * 2 * npa
+        att_mod = np.concatenate([dl_all, dm_all], axis=1).ravel()
+        m.se_att_moduli = att_mod
+        a, b, g = att_alpha_beta_gamma(sls["w"], sls["y"], dt)
+        m.nsls, m.att_alpha, m.att_beta, m.att_gamma = len(a), a, b, g
+    # fluid elements: K = 1 / rho (Material::createAcoustic)
+    nf = len(fluid_q)
+    m.fe_nr = enr[fluid_q].astype(np.int32)
+    m.fe_pts = fid[gll[fluid_q]].astype(np.int32) if nf else np.zeros((0, 25), np.int32)
+    m.fe_axial = quads.axial[fluid_q]
+    m.fe_geom = quads.geom[fluid_q]
+    m.fe_is3d = np.zeros(nf, np.uint8)
+    m.fe_theta = theta[fluid_q]
+    m.fe_mat_off = np.arange(nf, dtype=np.int64) * 25
+    m.fe_moduli = (1. / quads.rho[fluid_q]).ravel() if nf else np.zeros(0)
+    # solid-fluid coupling
+    iface = np.intersect1d(sp_used, fp_used)
+    m.sf_solid = sid[iface].astype(np.int32)
+    m.sf_fluid = fid[iface].astype(np.int32)
+    m.sf_nsu = normal[iface, 0].copy()
+    m.sf_nzu = normal[iface, 1].copy()
+    m.sf_nsa = normal[iface, 0].copy()
+    m.sf_nza = normal[iface, 1].copy()
+    m.sf_mass_fluid = fmass[fid[iface]] if len(iface) else np.zeros(0)
+    # absorbing boundaries
+    if cl_s:
+        a_ = np.array(cl_s)
+        m.cl_solid = {"point": a_[:, 0].astype(np.int32), "rho_vp": a_[:, 1], "rho_vs": a_[:, 2],
+                      "area": a_[:, 3], "theta": a_[:, 4]}
+    if cl_f:
+        a_ = np.array(cl_f)
+        m.cl_fluid = {"point": a_[:, 0].astype(np.int32), "rho_vp": a_[:, 1], "area": a_[:, 2]}
+    if abc.sponge:
+        gam = np.where(gamma_cnt > 0, gamma_sum / np.maximum(gamma_cnt, 1), 0.)
+        sel_s = sp_used[gamma_cnt[sp_used] > 0]
+        sel_f = fp_used[gamma_cnt[fp_used] > 0]
+        if len(sel_s):
+            m.sponge_solid = (sid[sel_s].astype(np.int32), gam[sel_s])
+        if len(sel_f):
+            m.sponge_fluid = (fid[sel_f].astype(np.int32), gam[sel_f])
+
+    # ---- sources (Source::release) and the time axis (main.cpp:580-620)
+    ctx = _Locator(mesh, quads, geo, gll, solid_q, fluid_q)
+    t_min0 = _release_sources(inp, m, ctx, geo, enr, solid_q, dt)
+    t1 = inp.source.get_bounded("time_axis:record_length", 0.)
+    nmax = inp.advanced.get("develop:max_num_time_steps", int) \
+        if inp.advanced.contains("develop:max_num_time_steps") else 0
+    if nmax <= 0:
+        nmax = np.iinfo(np.int64).max
+    if max_steps is not None:
+        nmax = min(nmax, max_steps)
+    step0 = math.floor(t_min0 / dt)
+    step1 = math.ceil(t1 / dt)
+    nstep = int(min(step1 - step0 + 1, nmax))
+    m.t0 = step0 * dt
+    skipped = [] if skip_unsupported_channels else None
+    groups = _release_stations(inp, m, ctx, geo, dt, m.t0, m.t0 + (nstep - 1) * dt, nstep, enr, solid_q,
+                               skipped)
+    m.meta = {"workload": "exodus %s (%d solid + %d fluid quads, %s)" %
+              (mesh.summary()["file"], ns, nf, mesh.records.get("model", "")),
+              "dt_mesh": dt_mesh}
+    info = {"dt_mesh": dt_mesh, "dt": dt, "nsteps": nstep, "t0": m.t0, "t1": step1 * dt,
+            "abc_keys": abc.keys, "attenuation": ["NONE", "FULL", "CG4"][att + 1] if sls is not None else "NONE",
+            "nr_range": (int(pnr.min()), int(pnr.max())), "skipped_channels": skipped or [],
+            "stability_interval": inp.advanced.get("verbose:stability_interval", int)
+            if inp.advanced.contains("verbose:stability_interval") else 0}
+    return Simulation(model=m, nsteps=nstep, t0=m.t0, dt=dt, groups=groups, mesh=mesh,
+                      cartesian=geo.cartesian, info=info)
+
+
+# --------------------------------------------------------- location in the mesh ---
+class _Locator:
+    """SE_Model::locateInplane and computeInplaneFactor."""
+
+    def __init__(self, mesh, quads, geo, gll, solid_q, fluid_q):
+        self.quads = quads
+        self.geo = geo
+        self.centers = quads.nodal.reshape(-1, 4, 2).mean(axis=1)
+        self.solid_q, self.fluid_q = solid_q, fluid_q
+        self.solid_index = -np.ones(mesh.num_quads, np.int64)
+        self.solid_index[solid_q] = np.arange(len(solid_q))
+        xy = mesh.coords
+        tol = mesh.global_variables["dist_tolerance"]
+        self.tol = tol
+        self.range_s = (xy[:, 0].min() - tol, xy[:, 0].max() + tol)
+        self.range_z = (xy[:, 1].min() - tol, xy[:, 1].max() + tol)
+        r, t = sz2rtheta(xy[:, 0], xy[:, 1])
+        self.range_r = (r.min() - tol, r.max() + tol)
+        self.range_t = (t.min(), t.max())
+        nodes = quads.nodal.reshape(-1, 4, 2)
+        e = np.stack([np.hypot(*(nodes[:, a] - nodes[:, (a + 1) % 4]).T) for a in range(4)], axis=1)
+        self.min_edge = e.min(axis=1)
+
+    def _map(self, q, xi, eta):
+        """Mapping::mapping and jacobian at one (xi, eta) of quad q."""
+        mp = MAPPING[int(self.quads.mesh.geometry_type[q])]
+        return _map_point(mp, self.quads.nodal[q], xi, eta)
+
+    def inverse(self, q, s, z, max_iter=10, tolerance=1e-9):
+        """Mapping::inverseMapping: Newton from (0, 0)."""
+        xe = np.zeros(2)
+        target = np.array([s, z])
+        it = 0
+        for it in range(max_iter):
+            p, J = self._map(q, xe[0], xe[1])
+            d = target - p
+            if np.hypot(d[0], d[1]) < tolerance * self.min_edge[q]:
+                break
+            xe = xe + np.linalg.solve(J, d)
+        else:
+            return None
+        b = 1. + tolerance * 20.
+        if xe.min() > -b and xe.max() < b:
+            return xe
+        return None
+
+    def locate(self, s, z, fluid):
+        if not (self.range_s[0] <= s <= self.range_s[1] and self.range_z[0] <= z <= self.range_z[1]):
+            return -1, None
+        r, t = sz2rtheta(s, z)
+        if (r < self.range_r[0] or r > self.range_r[1] or t * r < self.range_t[0] * r - self.tol or
+                t * r > self.range_t[1] * r + self.tol):
+            return -1, None
+        cand = self.fluid_q if fluid else self.solid_q
+        d = np.hypot(self.centers[cand, 0] - s, self.centers[cand, 1] - z)
+        for k in np.argsort(d, kind="stable")[:30]:
+            q = int(cand[k])
+            xe = self.inverse(q, s, z)
+            if xe is not None:
+                return q, xe
+        return -1, None
+
+    def weights(self, q, xe):
+        t = tables()
+        wx = lagrange(t["pGLJ"] if self.quads.axial[q] else t["pGLL"], xe[0])
+        we = lagrange(t["pGLL"], xe[1])
+        return np.outer(wx, we).ravel()
+
+
+def _map_point(mp, nodal, xi, eta):
+    """One point of a mapping and its Jacobian (axg_quad_map)."""
+    lib = L.lib()
+    nod = np.ascontiguousarray(nodal, dtype=np.float64)
+    out = np.zeros(6)
+    rc = lib.axg_quad_map(int(mp), nod.ctypes.data_as(L.P_f64), float(xi), float(eta),
+                          out.ctypes.data_as(L.P_f64))
+    if rc != L.AXG_OK:
+        raise PreloopError("Mapping::mapping || Error identifying curved outer edge.")
+    return out[:2], out[2:].reshape(2, 2)
+
+
+def _compute_spz(geo, crd, source_centered, xy, ellipticity, use_depth, depth_solid, enforce_axis):
+    """Source::computeSPZ without undulation (no 3-D geometric models in this build)."""
+    crd = np.array(crd, dtype=np.float64)
+    if use_depth:
+        R = geo.outer_solid_radius if depth_solid else geo.outer_radius
+        crd[2] = R - crd[2]
+    if enforce_axis:
+        crd[0] = crd[1] = 0.
+    elif source_centered:
+        if xy:
+            x, y = crd[0], crd[1]
+            crd[0] = math.hypot(x, y)
+            crd[1] = 0. if crd[0] < EPS else math.atan2(y, x)
+        elif not geo.cartesian:
+            r, th = crd[2], crd[0]
+            crd[0], crd[2] = r * math.sin(th), r * math.cos(th)
+    else:
+        crd = geo.llr2spz(crd[None, :], ellipticity)[0]
+        if geo.cartesian:
+            r, t = sz2rtheta(crd[0], crd[2])
+            un = np.array([float(t) * float(r), crd[1], float(r)])
+            if un[2] < un[0] * 10.:
+                raise PreloopError("Source::computeSPZ || Invalid geographic location in Cartesian mesh.")
+            crd = un
+    return crd
+
+
+def _qzsp(geo, spz, axial, source_centered, crd_in, use_depth, depth_solid, ellipticity):
+    """Source::computeQzsp: rotation from the input frame to (z, s, phi)."""
+    Q = np.eye(3)
+    if axial:
+        return Q
+    if not source_centered:
+        llr = np.array(crd_in, dtype=np.float64)
+        if use_depth:
+            R = geo.outer_solid_radius if depth_solid else geo.outer_radius
+            llr[2] = R - llr[2]
+        baz = float(geo.back_azimuth(llr[None, :], ellipticity)[0])
+        Q[1, 1] = Q[2, 2] = math.cos(baz)
+        Q[1, 2] = -math.sin(baz)
+        Q[2, 1] = math.sin(baz)
+    if not geo.cartesian:
+        th = float(sz2rtheta(spz[0], spz[2])[1])
+        Qt = np.eye(3)
+        Qt[0, 0] = Qt[1, 1] = math.cos(th)
+        Qt[0, 1] = -math.sin(th)
+        Qt[1, 0] = math.sin(th)
+        Q = Q @ Qt
+    return Q
+
+
+def _release_sources(inp, m, ctx, geo, enr, solid_q, dt):
+    gm = inp.source
+    n = gm.get("list_of_sources:[?]", int) if gm.contains("list_of_sources") and \
+        gm._walk("list_of_sources") else 0
+    ms, fs = [], []
+    t0 = np.inf
+    north_source = inp.model.get("geodesy:lat_lon_north_pole_mesh") == "SOURCE"
+    for k in range(n):
+        name = gm.get("list_of_sources:{%d}" % k)
+        root = "list_of_sources:[%d]:%s" % (k, name)
+        rl = root + ":location"
+        axial, centered, ellip = False, False, True
+        crd = np.zeros(3)
+        if gm.contains(rl + ":latitude_longitude"):
+            if gm.get(rl + ":latitude_longitude") == "ON_AXIS":
+                axial = True
+            else:
+                crd[0] = gm.get_bounded(rl + ":latitude_longitude:[0]", -90., 90.)
+                crd[1] = gm.get_bounded(rl + ":latitude_longitude:[1]", -180., 180.)
+                ellip = gm.get(rl + ":ellipticity", bool)
+        elif gm.contains(rl + ":distance_azimuth"):
+            if gm.get(rl + ":distance_azimuth") == "ON_AXIS":
+                axial = True
+            else:
+                centered = True
+                crd[0] = gm.get_bounded(rl + ":distance_azimuth:[0]", 0., None if geo.cartesian else math.pi)
+                crd[1] = gm.get_bounded(rl + ":distance_azimuth:[1]", 0., 2. * math.pi)
+        else:
+            raise PreloopError("Source::buildInparam || Either location:latitude_longitude or || "
+                               "location:distance_azimuth must exist. || Source name: " + name)
+        if k == 0 and north_source:
+            axial = True
+        use_depth, depth_solid = False, False
+        if gm.contains(rl + ":depth"):
+            use_depth = True
+            crd[2] = gm.get(rl + ":depth", float)
+            depth_solid = gm.get(rl + ":depth_below_solid_surface", bool)
+        elif gm.contains(rl + ":radius"):
+            crd[2] = gm.get(rl + ":radius", float)
+        else:
+            raise PreloopError("Source::buildInparam || Either location:radius or location:depth must "
+                               "exist. || Source name: " + name)
+        rm = root + ":mechanism"
+        mtype = gm.get_options(rm + ":type", {"MOMENT_TENSOR": "M", "FORCE_VECTOR": "F",
+                                              "FLUID_PRESSURE": "P"})
+        if mtype == "P":
+            raise PreloopError("Mechanism::release || FLUID_PRESSURE sources are not supported by this "
+                               "build. || Source name: " + name)
+        data = np.array(gm.get_vector(rm + ":data", float)) * gm.get(rm + ":unit", float)
+        spz = _compute_spz(geo, crd, centered, False, ellip, use_depth, depth_solid, axial)
+        q, xe = ctx.locate(spz[0], spz[2], False)
+        if q < 0:
+            raise PreloopError("Source::release || Error locating source in mesh. || "
+                               "Source index = %d || Source name  = %s" % (k, name))
+        w = ctx.weights(q, xe)
+        stf = _read_stf(gm, root + ":source_time_function", name, dt)
+        t0 = min(t0, -stf.half_duration * 2.5 + stf.time_shift)
+        Q = _qzsp(geo, spz, axial, centered, crd, use_depth, depth_solid, ellip)
+        nu_1 = int(enr[q]) // 2 + 1
+        e = int(ctx.solid_index[q])
+        pat = _pattern(mtype, data, Q, axial, w, float(spz[1]), nu_1, bool(ctx.quads.axial[q]))
+        (ms if mtype == "M" else fs).append((e, pat, stf))
+    if n == 0:
+        t0 = 0.
+    for lst, pre in ((ms, "ms"), (fs, "fs")):
+        if not lst:
+            continue
+        setattr(m, pre + "_elem", np.array([x[0] for x in lst], np.int32))
+        setattr(m, pre + "_nu", np.array([x[1].shape[0] for x in lst], np.int32))
+        off = np.zeros(len(lst), np.int64)
+        sizes = [x[1].size for x in lst]
+        off[1:] = np.cumsum(sizes)[:-1]
+        setattr(m, pre + "_pat_off", off)
+        setattr(m, pre + "_pattern", np.concatenate([x[1].ravel() for x in lst]))
+        setattr(m, pre + "_stf", [x[2] for x in lst])
+    return t0
+
+
+def _pattern(mtype, data, Q, on_axis, w, phi, nu_1, axial_quad):
+    """Mechanism::release (Mechanism.cpp:42-222) for moment tensors and force vectors."""
+    ephi = lambda a: np.exp(1. * a * (-1j * phi))         # noqa: E731
+    if mtype == "F":
+        f = Q @ data[:3]
+        fs_, fp_, fz_ = f[1] * w, f[2] * w, f[0] * w
+        nu = min(nu_1, 2) if on_axis else nu_1
+        pat = np.zeros((nu, 3, 25), np.complex128)
+        if not on_axis:
+            for a in range(nu):
+                pat[a, 0], pat[a, 1], pat[a, 2] = ephi(a) * fs_, ephi(a) * fp_, ephi(a) * fz_
+        if axial_quad:
+            pat[:, :, 0:5] = 0.
+            pat[0, 2, 0:5] = fz_[0:5]
+            if nu >= 2:
+                pat[1, 0, 0:5] = (fs_[0:5] - 1j * fp_[0:5]) / 2.
+                pat[1, 1, 0:5] = 1j * pat[1, 0, 0:5]
+            pat /= 2. * np.pi
+        return pat
+    mt = np.zeros((3, 3))
+    mt[0, 0], mt[1, 1], mt[2, 2] = data[0], data[1], data[2]
+    mt[0, 1] = mt[1, 0] = data[3]
+    mt[0, 2] = mt[2, 0] = data[4]
+    mt[1, 2] = mt[2, 1] = data[5]
+    mt = Q @ mt @ Q.T
+    mss, mpp, mzz = mt[1, 1] * w, mt[2, 2] * w, mt[0, 0] * w
+    mpz, msz, msp = mt[0, 2] * w, mt[0, 1] * w, mt[1, 2] * w
+    nu = min(nu_1, 3) if on_axis else nu_1
+    pat = np.zeros((nu, 6, 25), np.complex128)
+    if not on_axis:
+        for a in range(nu):
+            for d, v in enumerate((mss, mpp, mzz, mpz, msz, msp)):
+                pat[a, d] = ephi(a) * v
+    if axial_quad:
+        pat[:, :, 0:5] = 0.
+        pat[0, 0, 0:5] = pat[0, 1, 0:5] = (mss[0:5] + mpp[0:5]) / 2.
+        pat[0, 2, 0:5] = mzz[0:5]
+        if nu >= 2:
+            pat[1, 4, 0:5] = (msz[0:5] - 1j * mpz[0:5]) / 2.
+            pat[1, 3, 0:5] = 1j * pat[1, 4, 0:5]
+        if nu >= 3:
+            pat[2, 0, 0:5] = (mss[0:5] - mpp[0:5] - 2. * 1j * msp[0:5]) / 4.
+            pat[2, 1, 0:5] = -pat[2, 0, 0:5]
+            pat[2, 5, 0:5] = 1j * pat[2, 0, 0:5]
+        pat /= 2. * np.pi
+    return pat
+
+
+# ----------------------------------------------------------------- stations ---
+U_CHANNELS = {"U1": ("U1", "U"), "U2": ("U2", "U"), "U3": ("U3", "U"), "U_NORM": ("U_NORM", "|U|")}
+STD_ORDER = ("U1", "U2", "U3", "U_NORM")
+
+
+def standard_channels(user, skipped=None):
+    """channel::solid::ChannelOptions for displacement channels; other channels raise, or are
+    listed in `skipped` when a list is given."""
+    out = []
+    for uch in user:
+        found = False
+        for std in STD_ORDER:
+            if uch in U_CHANNELS[std]:
+                out.append(std)
+                found = True
+        if not found:
+            if skipped is None:
+                raise PreloopError("channel::solid::ChannelOptions::ChannelOptions || Channel %s is not "
+                                   "supported by this build (displacement channels only)." % uch)
+            skipped.append(uch)
+    return [c for c in STD_ORDER if c in set(out)]
+
+
+def _release_stations(inp, m, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, solid_q, skipped=None):
+    gm = inp.output
+    groups = []
+    if not gm.contains("list_of_station_groups") or not gm._walk("list_of_station_groups"):
+        _set_stations(m, [], [], [], 1)
+        return groups
+    n = gm.get("list_of_station_groups:[?]", int)
+    st_e, st_w, st_phi = [], [], []
+    names = set()
+    intervals = []
+    for g in range(n):
+        name = gm.get("list_of_station_groups:{%d}" % g)
+        if name in names:
+            raise PreloopError("StationOutput::release || Station group name must be unique. || "
+                               "Duplicated station group name: " + name)
+        names.add(name)
+        root = "list_of_station_groups:[%d]:%s" % (g, name)
+        rl = root + ":locations"
+        fname = gm.get(rl + ":station_file")
+        h = gm.get(rl + ":horizontal_x1_x2")
+        centered = {"LATITUDE_LONGITUDE": False, "DISTANCE_AZIMUTH": True, "XY_CARTESIAN": True}[h]
+        xy = h == "XY_CARTESIAN"
+        use_depth = gm.get_options(rl + ":vertical_x3", {"RADIUS": False, "DEPTH": True})
+        ellip = gm.get(rl + ":ellipticity", bool) if not centered else False
+        depth_solid = gm.get(rl + ":depth_below_solid_surface", bool) if use_depth else False
+        rw = root + ":wavefields"
+        frame = gm.get_options(rw + ":coordinate_frame", {"spz": "spz", "RTZ": "RTZ", "ENZ": "ENZ",
+                                                          "xyz": "xyz"})
+        if gm.get_options(rw + ":medium", {"SOLID": False, "FLUID": True}):
+            raise PreloopError("StationOutput::release || Fluid station groups are not supported by "
+                               "this build. || Station group name: " + name)
+        chans = standard_channels(gm.get_vector(rw + ":channels"), skipped)
+        if not chans:
+            continue
+        rt = root + ":temporal"
+        sp = gm.get(rt + ":sampling_period")
+        if sp == "DT":
+            period = dt
+        elif sp.startswith("DTx"):
+            period = dt * int(sp[3:])
+        else:
+            period = float(sp)
+        tmin, tmax = tmin_simu, tmax_simu
+        if gm.get(rt + ":time_window") != "FULL":
+            tmin = max(tmin_simu, gm.get(rt + ":time_window:[0]", float))
+            tmax = min(tmax_simu, gm.get(rt + ":time_window:[1]", float))
+        rf = root + ":file_options"
+        fmt = gm.get_options(rf + ":format", {"ASCII_STATION": "ASCII_STATION",
+                                              "ASCII_CHANNEL": "ASCII_CHANNEL", "NETCDF": "NETCDF"})
+        bsize = gm.get_bounded(rf + ":buffer_size", 1, None, int)
+        keys, crds = [], []
+        with open(inp.path(fname)) as f:
+            for line in f:
+                words = line.split()
+                if not words or words[0].startswith("#"):
+                    continue
+                if len(words) not in (5, 6):
+                    raise PreloopError("StationOutput::release || Input file for stations must contain "
+                                       "five or six columns. || Ascii file: %s || Station group name: %s"
+                                       % (fname, name))
+                key = words[1] + "." + words[0]
+                if key in keys:
+                    raise PreloopError("StationOutput::release || Station key must be unique. || "
+                                       "Duplicated station key: %s || Station group name: %s" % (key, name))
+                keys.append(key)
+                crds.append([float(words[2]), float(words[3]), float(words[-1])])
+        intv = int(period / dt)
+        intv = 1 if intv == 0 else intv
+        if intv < 0:
+            intv = np.iinfo(np.int32).max
+        nrec = sum(1 for t in range(0, nsteps, intv)
+                   if tmin - dt / 2. <= tmin_simu + t * dt <= tmax + dt / 2.)
+        if nrec == 0:
+            raise PreloopError("StationOutput::release || No time step to record in the given time "
+                               "window. ||Station group name: " + name)
+        grp = StationGroup(name=name, keys=keys, channels=chans, frame=frame, interval=intv,
+                           tmin=tmin - dt / 2., tmax=tmax + dt / 2., fmt=fmt, buffer_size=bsize,
+                           first=len(st_e))
+        th, baz, phi = [], [], []
+        for key, c in zip(keys, crds):
+            spz = _compute_spz(geo, c, centered, xy, ellip, use_depth, depth_solid, False)
+            q, xe = ctx.locate(spz[0], spz[2], False)
+            if q < 0:
+                raise PreloopError("StationOutput::release || Error locating station in mesh. || "
+                                   "Station key: %s || Station group name: %s" % (key, name))
+            st_e.append(int(ctx.solid_index[q]))
+            st_w.append(ctx.weights(q, xe))
+            st_phi.append(float(spz[1]))
+            th.append(float(sz2rtheta(spz[0], spz[2])[1]))
+            llr = geo.spz2llr(spz[None, :], True, False)
+            baz.append(float(geo.back_azimuth(llr, True)[0]))
+            phi.append(float(spz[1]))
+        grp.theta, grp.baz, grp.phi = np.array(th), np.array(baz), np.array(phi)
+        intervals.append(intv)
+        groups.append(grp)
+    interval = int(np.gcd.reduce(intervals)) if intervals else 1
+    interval = max(1, min(interval, nsteps))
+    _set_stations(m, st_e, st_w, st_phi, interval)
+    return groups
+
+
+def _set_stations(m, st_e, st_w, st_phi, interval):
+    m.st_elem = np.array(st_e, np.int32)
+    m.st_w = np.array(st_w).reshape(-1, 25)
+    m.st_phi = np.array(st_phi, np.float64)
+    m.st_interval = int(interval)

@@ -91,6 +91,7 @@ extern "C" {
 /* mapping of a quad (SOLVER/src/preloop/se_model/quad/mapping) */
 #define AXG_MAP_LINEAR    0   /* MappingLinear.hpp    */
 #define AXG_MAP_SPHERICAL 1   /* MappingSpherical.hpp */
+#define AXG_MAP_SEMI_SPHERICAL 2   /* MappingSemiSpherical.hpp */
 
 #define AXG_MAX_SLS 8
 
@@ -437,6 +438,10 @@ int  axg_spectral_tables(double *xgll, double *xglj, double *wgll, double *wglj,
    counter-clockwise from (xi,eta)=(-1,-1)); out_geometry[6*25], out_sz[2*25] */
 int  axg_quad_geometry(int32_t mapping, const double *nodal_sz, int32_t axial,
                        double *out_geometry, double *out_sz);
+/* one point of a quad's mapping and its Jacobian d(s,z)/d(xi,eta): out[6] = s, z, J00, J01,
+ * J10, J11 (Mapping::mapping, Mapping::jacobian; mapping/Mapping.hpp, MappingLinear.hpp,
+ * MappingSpherical.hpp, MappingSemiSpherical.hpp) */
+int  axg_quad_map(int32_t mapping, const double *nodal_sz, double xi, double eta, double *out);
 /* axg_quad_geometry over n quads: nodal_sz [n*8], axial [n], out [n*150], [n*50] */
 int  axg_quad_geometry_batch(int32_t n, int32_t mapping, const double *nodal_sz,
                              const uint8_t *axial, double *out_geometry, double *out_sz);

@@ -1,0 +1,271 @@
+"""CPU tests of mesh and input ingestion (hdf5, exodus, inparam, preloop, output).
+
+Pins, in order of strength:
+  - a Cartesian Exodus fixture (the box of meshgen.cartesian_model, written as an Exodus file)
+    gives the model meshgen builds directly: masses, operands, moduli, source pattern and
+    station weights to round-off, and the oracle's seismograms of both models agree to 1e-10;
+  - the reference's own example meshes (read when the reference tree is present): all open, and
+    the PREM global mesh integrates to Earth's mass without the outer core;
+  - a spherical shell fixture: closed-form solid volume, axis and interface counts;
+  - geodesy identities, output file round trips and the error paths of unsupported inputs.
+"""
+import glob
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import exodus_fixture as fx  # noqa: E402
+
+REF = "/root/reference/examples"
+have_ref = pytest.mark.skipif(not os.path.isdir(REF), reason="reference examples not present")
+
+NX, NZ, W, H, R = 10, 8, 100e3, 80e3, 6371e3
+
+
+def _box_dir(tmp, attenuation=None, storage="element_nodes"):
+    from axisem3d_b200 import meshgen
+    ref = meshgen.cartesian_model(nx=NX, nz=NZ, width=W, height=H, nr=5, nstations=5, source_depth=10e3,
+                                  attenuation=attenuation)
+    desc = fx.cartesian_box(NX, NZ, W, H, 2700.0, 5800.0, 3460.0, surface=R, storage=storage,
+                            attenuation=attenuation, minimum_period=1.0)
+    st = [("S%d" % k, "XX", W * k / 5, 0.0, 0.0) for k in range(1, 6)]
+    d = fx.write_inputs(str(tmp), desc, nr=5, depth=10e3, mt=ref.meta["moment"], hdur=1.0, decay=math.pi,
+                        order="RICKER", courant=0.6, record_length=1.0, stations=st,
+                        attenuation="FULL" if attenuation else "NONE")
+    return d, ref
+
+
+def _point_perm(m, ref):
+    rmap = {(round(c[0], 3), round(c[1] + R, 3)): i for i, c in enumerate(ref.sp_coords)}
+    return np.array([rmap[(round(c[0], 3), round(c[1], 3))] for c in m.sp_coords])
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("storage", ["element_nodes", "elements"])
+def test_box_exodus_gives_the_meshgen_model(tmp_path, storage):
+    from axisem3d_b200 import preloop
+    d, ref = _box_dir(tmp_path, storage=storage)
+    m = preloop.build(d).model
+    perm = _point_perm(m, ref)
+    assert m.dt == ref.dt
+    assert np.array_equal(perm[m.se_pts], ref.se_pts)
+    assert np.array_equal(m.sp_axial, ref.sp_axial[perm]) and np.array_equal(m.sp_nr, ref.sp_nr[perm])
+    assert _rel(m.sp_mass, ref.sp_mass[perm]) < 1e-12
+    assert _rel(m.se_geom, ref.se_geom) < 1e-12
+    assert _rel(m.se_moduli, ref.se_moduli) < 1e-14
+    assert np.array_equal(m.ms_elem, ref.ms_elem) and _rel(m.ms_pattern, ref.ms_pattern) < 1e-14
+    assert m.ms_stf == ref.ms_stf
+    assert np.array_equal(m.st_elem, ref.st_elem) and _rel(m.st_w, ref.st_w) < 1e-14
+
+
+def test_box_with_full_attenuation_gives_the_meshgen_model(tmp_path):
+    from axisem3d_b200 import meshgen, preloop
+    sls = dict(meshgen.default_sls(3, fmin=0.1, fmax=2.0), qkappa=57823.0, qmu=120.0)
+    d, ref = _box_dir(tmp_path, attenuation=sls)
+    m = preloop.build(d).model
+    assert m.dt == ref.dt
+    assert _rel(m.se_moduli, ref.se_moduli) < 1e-13
+    assert _rel(m.se_att_moduli, ref.se_att_moduli) < 1e-13
+    assert np.allclose(m.att_alpha, ref.att_alpha, rtol=0, atol=1e-15)
+    assert np.allclose(m.att_beta, ref.att_beta, rtol=1e-13) and np.allclose(m.att_gamma, ref.att_gamma, rtol=1e-13)
+
+
+def test_box_seismograms_of_both_models_agree_in_the_oracle(built, tmp_path):
+    import oracle as O
+    from axisem3d_b200 import preloop
+    d, ref = _box_dir(tmp_path)
+    m = preloop.build(d).model
+    ref.t0 = m.t0            # the preloop starts at floor(t0 / dt) dt, as main.cpp does
+    out = []
+    for mod in (m, ref):
+        o = O.Oracle(mod, "fp64")
+        o.run(60)
+        out.append(o.seismograms())
+        o.close()
+    assert np.abs(out[1]).max() > 0
+    assert _rel(out[0], out[1]) < 1e-10
+
+
+def _shell_dir(tmp, rho_solid=None):
+    from axisem3d_b200 import meshgen
+    r_edges = [3480e3, 3540e3, 3600e3, 4200e3, 4800e3, 5400e3, 6000e3, 6371e3]
+    layers = [dict(RHO=9900., VP=8000., VS=0., QMU=0., QKAPPA=57823.)] * 2 + \
+        [dict(RHO=rho_solid or 5500. - 300 * k, VP=13000. - 600 * k, VS=7000. - 300 * k, QMU=300.,
+              QKAPPA=57823.) for k in range(5)]
+    sls = meshgen.default_sls(3, fmin=1 / 80., fmax=1 / 5.)
+    desc = fx.spherical_shell(24, r_edges, 2, layers, attenuation=sls, minimum_period=20.0,
+                              discontinuities=[3480e3, 3600e3, 6371e3])
+    st = [("S%02d" % k, "XX", 90. - 170. * k / 9, 0.0, 0.0) for k in range(1, 9)]
+    return fx.write_inputs(str(tmp), desc, nr=8, depth=100e3, mt=(1e20, -2e19, 3e19, 5e19, -4e19, 1e19),
+                           hdur=10.0, decay=1.628, order="RICKER", courant=0.6, record_length=200., stations=st,
+                           horizontal="LATITUDE_LONGITUDE", frame="RTZ", attenuation="CG4",
+                           boundaries=["BOTTOM", "RIGHT"], clayton=True, sponge=True, spans=[0.05, 0.05],
+                           lucky=True, bound_nr=True), r_edges
+
+
+def test_shell_volume_axis_and_interface(tmp_path):
+    from axisem3d_b200 import preloop
+    d, r_edges = _shell_dir(tmp_path, rho_solid=4000.0)
+    sim = preloop.build(d)
+    m = sim.model
+    # solid mass = rho * 4/3 pi (R^3 - r_sf^3); the points carry it divided by 2 pi
+    vol = 4. / 3. * math.pi * (r_edges[-1] ** 3 - r_edges[2] ** 3)
+    assert abs(m.sp_mass.sum() * 2 * math.pi / (4000.0 * vol) - 1.0) < 1e-6
+    # both axis columns are axial (the south one after the side-3 rotation)
+    assert int(m.se_axial.sum()) == 2 * 5 and int(m.fe_axial.sum()) == 2 * 2
+    assert len(m.sf_solid) == 4 * 24 + 1
+    # Clayton on the fluid bottom, sponge over the lowest 5 % of the radius span
+    assert m.cl_fluid is not None and m.cl_solid is None
+    assert m.sponge_fluid is not None and m.sponge_solid is not None
+    assert sim.info["abc_keys"] == ["BOTTOM"] and sim.info["attenuation"] == "CG4"
+    # station longitude 0 -> phi 0; theta = epicentral distance
+    g = sim.groups[0]
+    assert np.allclose(g.phi, 0.0) and np.allclose(g.theta, np.radians(170. * np.arange(1, 9) / 9), atol=1e-12)
+
+
+@have_ref
+def test_reference_meshes_open():
+    from axisem3d_b200 import hdf5
+    from axisem3d_b200.exodus import ExodusMesh
+    files = sorted(set(glob.glob(REF + "/**/*.e", recursive=True)))
+    assert len(files) >= 10
+    for f in files:
+        h = hdf5.File(f)
+        for ds in h.datasets.values():
+            ds.read()
+        m = ExodusMesh(f)
+        assert m.connectivity.min() == 0 and m.connectivity.max() == m.num_nodes - 1
+        assert len(m.radial_coords) >= 2
+
+
+@have_ref
+def test_reference_prem_mesh_mass():
+    """PREM: Earth 5.974e24 kg minus the outer core 1.841e24 kg in the solid elements."""
+    from axisem3d_b200 import preloop
+    sim = preloop.build(REF + "/01_S362ANI_EMC_global/input1D", skip_unsupported_channels=True)
+    m = sim.model
+    assert abs(m.sp_mass.sum() * 2 * math.pi / 4.133e24 - 1.0) < 3e-3
+    assert sim.info["skipped_channels"] == ["E_I1", "R3"]
+    assert len(m.ms_elem) == 1 and m.ms_nu[0] == 3 and m.ms_stf[0].derivative_order == -1
+
+
+def test_unsupported_inputs_raise(tmp_path):
+    from axisem3d_b200 import preloop
+    d, _ = _box_dir(tmp_path)
+    p = os.path.join(d, "inparam.output.yaml")
+    with open(p) as f:
+        txt = f.read()
+    with open(p, "w") as f:
+        f.write(txt.replace("channels: [U]", "channels: [U, E_I1]"))
+    with pytest.raises(preloop.PreloopError, match="E_I1"):
+        preloop.build(d)
+    assert preloop.build(d, skip_unsupported_channels=True).info["skipped_channels"] == ["E_I1"]
+    p = os.path.join(d, "inparam.model.yaml")
+    with open(p) as f:
+        txt = f.read()
+    with open(p, "w") as f:
+        f.write(txt.replace("list_of_3D_models: []", "list_of_3D_models: [crust]"))
+    with pytest.raises(preloop.PreloopError, match="3-D models"):
+        preloop.build(d)
+
+
+def test_lucky_numbers():
+    from axisem3d_b200.preloop import is_lucky, next_lucky
+    assert [n for n in range(1, 30) if not is_lucky(n)] == [17, 19, 23, 29]
+    assert not is_lucky(11 * 13) and is_lucky(11 * 8) and not is_lucky(11 * 11)
+    assert next_lucky(17) == 18 and next_lucky(127) == 128
+
+
+def test_geodesy_round_trip_and_back_azimuth(tmp_path):
+    from axisem3d_b200.exodus import ExodusMesh
+    from axisem3d_b200.inparam import Inparam
+    from axisem3d_b200.preloop import Geodesy
+    d, _ = _shell_dir(tmp_path)
+    p = os.path.join(d, "inparam.source.yaml")
+    with open(p) as f:
+        txt = f.read()
+    with open(p, "w") as f:
+        f.write(txt.replace("latitude_longitude: [90., 0.]", "latitude_longitude: [37.91, -77.93]"))
+    inp = Inparam(d)
+    geo = Geodesy(ExodusMesh(os.path.join(d, "mesh.e")), inp)
+    rng = np.random.default_rng(3)
+    llr = np.stack([rng.uniform(-80, 80, 20), rng.uniform(-170, 170, 20), np.full(20, 6.0e6)], axis=1)
+    spz = geo.llr2spz(llr, True)
+    back = geo.spz2llr(spz, True, False)
+    assert np.allclose(back[:, :2], llr[:, :2], atol=1e-9) and np.allclose(back[:, 2], 6.0e6)
+    # back azimuth against the spherical-trigonometry formula (no flattening on a sphere)
+    la1, lo1 = np.radians(37.91), np.radians(-77.93)
+    la2, lo2 = np.radians(llr[:, 0]), np.radians(llr[:, 1])
+    baz = np.arctan2(np.sin(lo1 - lo2) * np.cos(la1),
+                     np.cos(la2) * np.sin(la1) - np.sin(la2) * np.cos(la1) * np.cos(lo1 - lo2))
+    got = geo.back_azimuth(llr, True)
+    assert np.allclose(np.angle(np.exp(1j * (got - baz))), 0.0, atol=1e-9)
+
+
+def test_semi_spherical_quad_area():
+    """sum of ifact / s over the points = the area of a quad with one curved edge."""
+    from axisem3d_b200 import _lib as L, meshgen
+    r0, r1, t0, t1 = 1000.0, 1500.0, 0.3, 0.5
+    # straight inner edge, curved outer edge (nodes 2-3 on r1)
+    n = np.array([r0 * math.sin(t0), r0 * math.cos(t0), r0 * math.sin(t1), r0 * math.cos(t1),
+                  r1 * math.sin(t1), r1 * math.cos(t1), r1 * math.sin(t0), r1 * math.cos(t0)])
+    g, sz = meshgen.geometry_batch(n[None, :], np.zeros(1, np.uint8), L.AXG_MAP_SEMI_SPHERICAL)
+    area = float(np.sum(g[0, 5] / sz[0, 0]))
+    exact = 0.5 * r1 * r1 * (t1 - t0) - 0.5 * r0 * r0 * math.sin(t1 - t0)
+    assert abs(area / exact - 1.0) < 1e-9
+    # corners map onto the nodes
+    out = np.zeros(6)
+    for k, (xi, eta) in enumerate([(-1, -1), (1, -1), (1, 1), (-1, 1)]):
+        assert L.lib().axg_quad_map(L.AXG_MAP_SEMI_SPHERICAL, n.ctypes.data_as(L.P_f64), xi, eta,
+                                    out.ctypes.data_as(L.P_f64)) == 0
+        assert np.allclose(out[:2], n[2 * k:2 * k + 2], atol=1e-9)
+
+
+def test_output_formats_round_trip(tmp_path):
+    from scipy.io import netcdf_file
+    from axisem3d_b200 import output
+    from axisem3d_b200.preloop import StationGroup
+    rng = np.random.default_rng(0)
+    data = rng.normal(size=(3, 2, 37))
+    times = np.arange(37) * 0.25 - 2.0
+    for fmt in ("ASCII_STATION", "ASCII_CHANNEL", "NETCDF"):
+        g = StationGroup(name="g_" + fmt, keys=["XX.A", "XX.B", "YY.C"], channels=["U1", "U3"], frame="RTZ",
+                         interval=1, tmin=-9e9, tmax=9e9, fmt=fmt, buffer_size=10, first=0)
+        output.write_group(str(tmp_path), g, times, data, 16)
+        gd = tmp_path / "stations" / g.name
+        if fmt == "NETCDF":
+            nc = netcdf_file(str(gd / "axisem3d_synthetics.nc.rank0"), "r", mmap=False)
+            assert np.allclose(nc.variables["data_wave"][:], data)
+            assert np.allclose(nc.variables["data_time"][:], times)
+            nc.close()
+            continue
+        assert np.allclose(np.loadtxt(gd / "data_time.ascii"), times)
+        if fmt == "ASCII_STATION":
+            for k, key in enumerate(g.keys):
+                assert np.allclose(np.loadtxt(gd / (key + ".ascii")), data[k].T, rtol=1e-15)
+        else:
+            for c, ch in enumerate(g.channels):
+                assert np.allclose(np.loadtxt(gd / "dir_rank0" / (ch + ".ascii")), data[:, c].T, rtol=1e-15)
+            assert (gd / "dir_rank0" / "list_station.info").read_text().split() == g.keys
+
+
+def test_rotation_frames():
+    from axisem3d_b200.output import rotate_displacement
+    # a purely radial (outward) displacement at colatitude theta: spz = (sin, 0, cos)
+    th = np.array([0.3, 1.1])
+    u = np.stack([np.sin(th), np.zeros(2), np.cos(th)], axis=1)[:, None, :]
+    rtz = rotate_displacement(u, "RTZ", th, np.zeros(2), np.zeros(2), False)
+    assert np.allclose(rtz[:, 0], [[0, 0, 1], [0, 0, 1]], atol=1e-15)
+    # ENZ with back azimuth 0 (source due north): R points south, T east
+    e = np.array([[[1.0, 0.0, 0.0]]])
+    enz = rotate_displacement(e, "ENZ", np.array([0.0]), np.array([0.0]), np.array([0.0]), False)
+    assert np.allclose(enz[0, 0], [0, -1, 0], atol=1e-15)
