@@ -764,12 +764,12 @@ private:
 
     // ------------------------------------------------------- solid buckets ---
     using SolidKernel = void (*)(const SolidArgs<T, AT>, int, int, int, size_t);
-    // NS: the register-resident slice path is built for 3 and 5 SLS (3-D elements);
-    // other counts and 1-D elements take the generic path
+    // NS: the register-resident SLS recursions are built for 3 and 5 SLS (3-D slices and
+    // 1-D Fourier slots); other counts take the generic path
     template <int RHEO, int ATT, bool IS3D, bool RTZ>
     static SolidKernel pick4(int nsls) {
 #ifndef AXG_GENERIC_SLS_ONLY
-        if constexpr (IS3D && ATT != ATT_NONE) {
+        if constexpr (ATT != ATT_NONE) {
             if (nsls == 3) return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 3>;
             if (nsls == 5) return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 5>;
         }

@@ -362,14 +362,80 @@ __device__ __forceinline__ void attenuate_regs(const AT *alpha, const AT *beta, 
     for (int d = 0; d < 6; d++) s[d] = (T)sv[d];
 }
 
+// SLS recursion on one complex Fourier-space slot of a 1-D element, state in registers. The
+// recursion is linear and acts on each stress component separately, on the real and the
+// imaginary parts alike, so the slot runs in four passes: (real, imaginary) x (components
+// 0-2, which share the trace of the strain, and 3-5). Each pass loads its 3 + 3 NS state
+// words at once (independent loads whose latencies overlap), updates them in registers with
+// the steps and order of attenuate_regs, and stores them back. Same layout and results as
+// attenuate<T, AT, true>: part w of state word j of the slot is at (j * nslot + slot) * 2 + w.
+template <int NS, class T, class AT>
+__device__ __forceinline__ void attenuate_cplx_regs(const SolidArgs<T, AT> &a, AT *state, size_t nslot,
+                                                    size_t slot, const cx_t<T> e[6], cx_t<T> s[6], T dl,
+                                                    T dm) {
+    const AT lam = (AT)dl, mu = (AT)dm, mu2 = mu + mu;
+#pragma unroll 1
+    for (int pass = 0; pass < 4; pass++) {
+        const int w = pass & 1, d0 = (pass >> 1) * 3;
+        AT *base = state + w;
+        AT ds[3], mem[NS][3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) ds[c] = base[((d0 + c) * nslot + slot) * 2];
+#pragma unroll
+        for (int l = 0; l < NS; l++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) mem[l][c] = base[((6 + l * 6 + d0 + c) * nslot + slot) * 2];
+        // new dstress of these components (Isotropic::strainToStress with dlambda, dmu)
+        AT dn[3];
+        if (d0 == 0) {
+            const AT e0 = (AT)(w ? e[0].y : e[0].x), e1 = (AT)(w ? e[1].y : e[1].x),
+                     e2 = (AT)(w ? e[2].y : e[2].x);
+            const AT sii = (e0 + e1 + e2) * lam;
+            dn[0] = sii + e0 * mu2;
+            dn[1] = sii + e1 * mu2;
+            dn[2] = sii + e2 * mu2;
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++) dn[c] = (AT)(w ? e[3 + c].y : e[3 + c].x) * mu;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            AT sv = (AT)(w ? s[d0 + c].y : s[d0 + c].x);
+#pragma unroll
+            for (int l = 0; l < NS; l++) {
+                sv -= mem[l][c];
+                mem[l][c] = a.alpha[l] * mem[l][c] + a.beta[l] * ds[c];
+            }
+#pragma unroll
+            for (int l = 0; l < NS; l++) mem[l][c] += a.gamma[l] * dn[c];
+            if (w) s[d0 + c].y = (T)sv;
+            else s[d0 + c].x = (T)sv;
+            base[((d0 + c) * nslot + slot) * 2] = dn[c];
+        }
+#pragma unroll
+        for (int l = 0; l < NS; l++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) base[((6 + l * 6 + d0 + c) * nslot + slot) * 2] = mem[l][c];
+    }
+}
+
+// 1-D elements: the register-resident recursion for 3 and 5 SLS, the generic one otherwise
+template <int NS, class T, class AT>
+__device__ __forceinline__ void attenuate_1d(const SolidArgs<T, AT> &a, AT *state, size_t nslot, size_t slot,
+                                             const cx_t<T> e[6], cx_t<T> s[6], T dl, T dm) {
+    if constexpr (NS > 0) attenuate_cplx_regs<NS, T, AT>(a, state, nslot, slot, e, s, dl, dm);
+    else attenuate<T, AT, true>(a, state, nslot, slot, e, s, dl, dm);
+}
+
 __device__ __forceinline__ int cg4_slot(int q) {
     // (1,1) (1,3) (3,1) (3,3) -> 0..3, else -1
     return q == 6 ? 0 : q == 8 ? 1 : q == 16 ? 2 : q == 18 ? 3 : -1;
 }
 
 // ----------------------------------------------------------------- kernel ---
-// NS: compile-time number of SLS for the register-resident slice path (3-D
-// elements); 0 = the generic path with the count read at run time
+// NS: compile-time number of SLS for the register-resident recursions (the slice path of 3-D
+// elements, the Fourier-space path of 1-D elements); 0 = the generic path with the count
+// read at run time
 template <class T, class AT, int RHEO, int ATT, bool IS3D, bool RTZ, int NS>
 __global__ void __launch_bounds__(256, AXG_SOLID_MIN_BLOCKS)
 solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_max,
@@ -524,21 +590,21 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             if constexpr (RTZ) {
                 spz_to_rtz6(eps, sTrig[q], sTrig[25 + q], sTrig[50 + q], sTrig[75 + q]);
             }
-            if constexpr (!IS3D) {
+            if constexpr (!IS3D && !(ATT != ATT_NONE && NS > 0)) {
                 // strainToStress_FR with 1-D moduli
                 C sig[6];
                 elastic_at<RHEO>(a.mod + moff, 1, 0, q, eps, sig);
                 if constexpr (ATT == ATT_FULL) {
                     const int64_t ao = a.att_off[e];
                     AT *st = statew + a.state_off[e];
-                    attenuate<T, AT, true>(a, st, (size_t)nu * 25, (size_t)al * 25 + q, eps, sig,
+                    attenuate_1d<NS, T, AT>(a, st, (size_t)nu * 25, (size_t)al * 25 + q, eps, sig,
                                            a.attmod[ao + q], a.attmod[ao + 25 + q]);
                 } else if constexpr (ATT == ATT_CG4) {
                     const int k4 = cg4_slot(q);
                     if (k4 >= 0) {
                         const int64_t ao = a.att_off[e];
                         AT *st = statew + a.state_off[e];
-                        attenuate<T, AT, true>(a, st, (size_t)nu * 4, (size_t)al * 4 + k4, eps, sig,
+                        attenuate_1d<NS, T, AT>(a, st, (size_t)nu * 4, (size_t)al * 4 + k4, eps, sig,
                                                a.attmod[ao + k4], a.attmod[ao + 4 + k4]);
                     }
                 }
@@ -553,6 +619,47 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             }
         }
         team_sync(team, TEAM);
+
+        // ---------------- 1-D attenuation: stress pass, SLS state in registers ----------------
+        // strainToStress_FR on the strain left in region A, then the SLS recursion of each
+        // attenuating slot with its whole state loaded at once; with CG4 the recursion runs on
+        // threads mapped to the 4 CG4 points of each mode only
+        if constexpr (!IS3D && ATT != ATT_NONE && NS > 0) {
+            const int64_t ao = a.att_off[e];
+            AT *st = statew + a.state_off[e];
+            auto stress_slot = [&](int al, int q, bool att, size_t nslot, size_t slot, T dl, T dm) {
+                C ev[6], sig[6];
+#pragma unroll
+                for (int d = 0; d < 6; d++) ev[d] = rA[(al * 6 + d) * 25 + q];
+                elastic_at<RHEO>(a.mod + moff, 1, 0, q, ev, sig);
+                if (att) attenuate_cplx_regs<NS, T, AT>(a, st, nslot, slot, ev, sig, dl, dm);
+                if constexpr (RTZ) {
+                    rtz_to_spz6(sig, sTrig[q], sTrig[25 + q], sTrig[50 + q], sTrig[75 + q]);
+                }
+#pragma unroll
+                for (int d = 0; d < 6; d++) rA[(al * 6 + d) * 25 + q] = sig[d];
+            };
+            if constexpr (ATT == ATT_FULL) {
+                for (int i = lane; i < nu * 25; i += TEAM) {
+                    const int al = i / 25, q = i - al * 25;
+                    stress_slot(al, q, true, (size_t)nu * 25, (size_t)i, a.attmod[ao + q], a.attmod[ao + 25 + q]);
+                }
+            } else {
+                // CG4 points (1,1) (1,3) (3,1) (3,3) = 6, 8, 16, 18 of each mode
+                for (int i = lane; i < nu * 4; i += TEAM) {
+                    const int al = i >> 2, k4 = i & 3;
+                    const int q = 6 + 2 * (k4 & 1) + 10 * (k4 >> 1);
+                    stress_slot(al, q, true, (size_t)nu * 4, (size_t)i, a.attmod[ao + k4], a.attmod[ao + 4 + k4]);
+                }
+                // the other 21 points of each mode: elastic only
+                for (int i = lane; i < nu * 21; i += TEAM) {
+                    const int al = i / 21, j = i - al * 21;
+                    const int q = j + (j >= 6) + (j >= 7) + (j >= 14) + (j >= 15);
+                    stress_slot(al, q, false, 0, 0, (T)0, (T)0);
+                }
+            }
+            team_sync(team, TEAM);
+        }
 
         // ---------------- 3-D material: slices ----------------
         if constexpr (IS3D) {
