@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
     p.add_argument("--adjoint-steps", type=int, default=4000)
     p.add_argument("--ensemble", type=int, default=64, help="sources of the ensemble leg (0 = skip)")
+    p.add_argument("--no-oned", action="store_true", help="skip the 1-D (in-Fourier) leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     return p.parse_args()
 
@@ -343,7 +344,39 @@ def run_ours(args, world, rank, local):
     if args.ensemble > 0:
         log("ensemble")
         out["ensemble"] = ensemble_timing(args, local, stream, world)
+    if not args.no_oned:
+        log("1-D leg")
+        out["oned"] = oned_timing(args, local, stream, world)
     return out
+
+
+def oned_timing(args, local, stream, world):
+    """The same microbenchmark with per-(element, point) moduli: every element takes the 1-D
+    path (stress and SLS attenuation in Fourier space, no phi transforms), in the bench
+    precision; step rate and the stiffness kernels against the HBM roofline."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.microbench_model(n_elem=args.elements, nr_max=args.nr_max, seed=5, is3d=False)
+    U = m.updates_per_step()
+    k = max(10, args.steps)
+    with Solver(m, args.precision, device=local) as s:
+        s.set_stream(stream.cuda_stream)
+        s.set_field(meshgen.random_displacement(m, seed=6) * 1e-6, "displ")
+        s.run(3)
+        t = dist_max(time_steps(s, k, stream), world)
+        s.set_timing(True)
+        s.run(5, graph=False)
+        kms, kn = s.stiffness_time()
+        s.set_timing(False)
+        b, _ = s.stiffness_cost()
+    kms = kms / max(kn, 1)
+    peak, kind = measured_peaks()
+    gbs = b / (kms / 1e3) / 1e9
+    return {"workload": "stiffness microbenchmark, 1-D moduli (Fourier-space path): %d quads, nr "
+                        "log-uniform [1,%d], TI, 3 SLS FULL" % (m.n_solid_elements, args.nr_max),
+            "updates_per_step": int(U), "value": U * k * world / t, "ms_per_step": t / k * 1e3,
+            "stiffness_ms": kms, "stiffness_bytes": b, "stiffness_GBps": gbs,
+            "stiffness_frac_of_" + kind + "_hbm": gbs / peak}
 
 
 def ensemble_timing(args, local, stream, world):
@@ -482,6 +515,8 @@ def main():
             line["adjoint"] = r["adjoint"]
         if "ensemble" in r:
             line["ensemble"] = r["ensemble"]
+        if "oned" in r:
+            line["oned"] = r["oned"]
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
