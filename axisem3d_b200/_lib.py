@@ -141,6 +141,8 @@ SIGNATURES = {
     "axg_set_field": (C.c_int, [H, C.c_int32, C.c_int32, P_f64]),
     "axg_field_size": (C.c_int, [H, C.c_int32, P_i64]),
     "axg_get_seismograms": (C.c_int, [H, P_f64, P_i32]),
+    "axg_get_station_gradients": (C.c_int, [H, P_f64, P_i32]),
+    "axg_set_station_gradient": (C.c_int, [H, C.c_int32]),
     "axg_forward_checkpointed": (C.c_int, [H, C.c_int32, C.c_int32]),
     "axg_adjoint_run": (C.c_int, [H, P_f64, P_f64, P_f64, P_f64, P_f64]),
     "axg_field_raw_bytes": (C.c_int, [H, C.c_int32, C.c_int32, P_i64]),

@@ -273,6 +273,13 @@ int axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interv
     });
 }
 
+int axg_set_station_gradient(axg_solver *h, int32_t enable) {
+    return guarded(h, [&] {
+        need_open(h);
+        h->model.st.gradient = enable ? 1 : 0;
+    });
+}
+
 int axg_set_clayton(axg_solver *h, int32_t solid, const axg_clayton *c) {
     return guarded(h, [&] {
         need_open(h);
@@ -647,6 +654,12 @@ int axg_get_field_raw(axg_solver *h, int32_t solid, int32_t which, void *host, i
 int axg_get_seismograms(axg_solver *h, double *host_out, int32_t *nrecords) {
     return guarded(h, [&] {
         int n = h->eng->get_seismograms(host_out);
+        if (nrecords) *nrecords = n;
+    });
+}
+int axg_get_station_gradients(axg_solver *h, double *host_out, int32_t *nrecords) {
+    return guarded(h, [&] {
+        int n = h->eng->get_station_gradients(host_out);
         if (nrecords) *nrecords = n;
     });
 }

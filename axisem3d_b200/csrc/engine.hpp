@@ -61,6 +61,7 @@ struct HostSources {
 
 struct HostStations {
     int count = 0, interval = 1;
+    int gradient = 0;               // also record the 9-component displacement gradient
     std::vector<int> elem;
     std::vector<double> w, phi;
 };
@@ -157,6 +158,7 @@ public:
     virtual void set_field_raw(int solid, int which, const void *host, int64_t bytes) = 0;
     virtual void get_field_raw(int solid, int which, void *host, int64_t bytes) = 0;
     virtual int get_seismograms(double *out) = 0;
+    virtual int get_station_gradients(double *out) = 0;
     virtual void synchronize() = 0;
     virtual int64_t launches() const = 0;
     virtual void set_timing(bool on) = 0;

@@ -355,6 +355,19 @@ public:
                                 cudaMemcpyDeviceToHost));
         return nrec;
     }
+    int get_station_gradients(double *out) override {
+        need();
+        if (!model_.st.gradient)
+            throw Error(AXG_E_ARG, "StationSolid::record || station gradients were not requested "
+                                   "(axg_set_station_gradient before axg_finalize).");
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        int nrec = 0;
+        if (st_n_ > 0) nrec = std::min(seis_cap_, (step_ + st_interval_ - 1) / st_interval_);
+        if (out && nrec > 0)
+            AXG_CUDA(cudaMemcpy(out, seis_grad_.p, (size_t)nrec * nwave_ * st_n_ * 9 * sizeof(double),
+                                cudaMemcpyDeviceToHost));
+        return nrec;
+    }
     void synchronize() override { AXG_CUDA(cudaStreamSynchronize(stream_)); }
     int64_t launches() const override { return launches_; }
     void set_timing(bool on) override {
@@ -1427,7 +1440,7 @@ private:
             e_nr_.upload(h.nr); e_pts_.upload(h.pts);
             std::vector<uint8_t> ax(h.axial.begin(), h.axial.end());
             e_axial_.upload(ax);
-            if (ms_n_) e_geom_.upload(g);
+            if (ms_n_ || model_.st.gradient) e_geom_.upload(g);
         }
     }
 
@@ -1462,6 +1475,17 @@ private:
                                              cudaMemcpyDeviceToDevice, stream_));
                 AXG_CUDA(cudaStreamSynchronize(stream_));
                 std::swap(seis_.p, nb.p); std::swap(seis_.n, nb.n);
+                if (model_.st.gradient) {
+                    DBuf<double> ng;
+                    ng.alloc((size_t)cap * nwave_ * st_n_ * 9);
+                    ng.zero(stream_);
+                    if (seis_cap_)
+                        AXG_CUDA(cudaMemcpyAsync(ng.p, seis_grad_.p,
+                                                 (size_t)seis_cap_ * nwave_ * st_n_ * 9 * sizeof(double),
+                                                 cudaMemcpyDeviceToDevice, stream_));
+                    AXG_CUDA(cudaStreamSynchronize(stream_));
+                    std::swap(seis_grad_.p, ng.p); std::swap(seis_grad_.n, ng.n);
+                }
                 seis_cap_ = cap;
                 changed = true;
             }
@@ -1602,9 +1626,20 @@ private:
         a.displ = elem_displ(sp_); a.out = seis_.p; a.interval = st_interval_;
         a.max_rec = seis_cap_; a.step = step_dev_.p;
         a.nwave = nwave_; a.fstride = (size_t)sp_.total * 3;
-        int threads = 128, blocks = (st_n_ * 3 * nwave_ + threads - 1) / threads;
+        const int threads = 128;                          // four stations per block
+        const int blocks = (int)(((size_t)st_n_ * nwave_ * 32 + threads - 1) / threads);
         station_kernel<T><<<blocks, threads, 0, stream_>>>(a);
         post_launch();
+        if (model_.st.gradient) {
+            StationGradArgs<T> g;
+            g.nst = st_n_; g.elem = st_el_.p; g.w = st_w_.p; g.phi = st_phi_.p;
+            g.e_nr = e_nr_.p; g.e_pts = e_pts_.p; g.e_axial = e_axial_.p; g.e_geom = e_geom_.p;
+            g.gmat = gmat_.p; g.pt_off = sp_.off.p; g.pt_nu = sp_.nu.p; g.displ = elem_displ(sp_);
+            g.out = seis_grad_.p; g.interval = st_interval_; g.max_rec = seis_cap_; g.step = step_dev_.p;
+            g.nwave = nwave_; g.fstride = (size_t)sp_.total * 3;
+            station_grad_kernel<T><<<blocks, threads, 0, stream_>>>(g);
+            post_launch();
+        }
     }
 
     void launch_points(int mask) {
@@ -1773,7 +1808,7 @@ private:
     int st_n_ = 0, st_interval_ = 1, seis_cap_ = 0;
     DBuf<int> st_el_;
     DBuf<T> st_w_, st_phi_;
-    DBuf<double> seis_;
+    DBuf<double> seis_, seis_grad_;
     DBuf<int> step_dev_, nonfinite_;
 };
 

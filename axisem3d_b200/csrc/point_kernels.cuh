@@ -812,39 +812,166 @@ struct StationArgs {
     size_t fstride;
 };
 
+// one warp per (station, wavefield): the lanes take the (point, mode) pairs of the element,
+// modes fastest (consecutive modes of a point are consecutive in memory, so the loads
+// coalesce, and small nr still fills the warp); each lane adds the weighted terms of its
+// pairs to the synthesis at phi, and a warp sum gives the three components
 template <class T>
 __global__ void station_kernel(const StationArgs<T> a) {
-    const int tt = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tt >= a.nst * 3 * a.nwave) return;
+    const int warp = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= a.nst * a.nwave) return;              // whole warps leave together
     const int step = *a.step;
     if (step < 0 || a.out == nullptr || step % a.interval != 0) return;
     const int rec = step / a.interval;
     if (rec >= a.max_rec) return;
-    const int wf = tt / (a.nst * 3), t = tt % (a.nst * 3);
-    const int s = t / 3, c = t % 3;
+    const int wf = warp / a.nst, s = warp - wf * a.nst;
     const cx_t<T> *displ = a.displ + (size_t)wf * a.fstride;
     const int e = a.elem[s];
     const int nu = a.e_nr[e] / 2 + 1;
     const T phi = a.phi[s];
-    T acc = 0;
-    for (int al = 0; al < nu; al++) {
-        cx_t<T> x = mk<T>(0, 0);
-        for (int q = 0; q < 25; q++) {
-            const T w = a.w[(size_t)s * 25 + q];
-            if (w == (T)0) continue;
-            const int p = a.e_pts[(size_t)e * 25 + q];
-            if (al < a.pt_nu[p]) x = cadd(x, cscale(displ[(size_t)(a.pt_off[p] + al) * 3 + c], w));
-        }
+    T acc[3] = {0, 0, 0};
+    for (int i = lane; i < nu * 25; i += 32) {
+        const int q = i / nu, al = i - q * nu;
+        const T w = a.w[(size_t)s * 25 + q];
+        if (w == (T)0) continue;
+        const int p = a.e_pts[(size_t)e * 25 + q];
+        if (al >= a.pt_nu[p]) continue;
+        const cx_t<T> *src = displ + (size_t)(a.pt_off[p] + al) * 3;
         if (al == 0) {
-            acc += x.x;
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[c] += w * src[c].x;
         } else {
             T sn, cs;
             if constexpr (sizeof(T) == 4) sincosf((T)al * phi, &sn, &cs);
             else sincos((T)al * phi, &sn, &cs);
-            acc += (T)2 * (cs * x.x - sn * x.y);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const cx_t<T> x = src[c];
+                acc[c] += (T)2 * w * (cs * x.x - sn * x.y);
+            }
         }
     }
-    a.out[(((size_t)rec * a.nwave + wf) * a.nst + s) * 3 + c] = (double)acc;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], off);
+    if (lane == 0) {
+        double *o = a.out + (((size_t)rec * a.nwave + wf) * a.nst + s) * 3;
+#pragma unroll
+        for (int c = 0; c < 3; c++) o[c] = (double)acc[c];
+    }
+}
+
+// displacement gradient at the stations (SolidElement::getNablaField without PRT, then
+// Station::interpolate): one warp per (station, wavefield), lanes over the (point, mode)
+// pairs; each lane forms d_j u_i (computeGrad9: index 3 i + j, s / phi / z) at its point
+// from the element's 5 x 5 operators, with the L'Hopital row on the axis, and adds its
+// weighted terms of the synthesis at phi; a warp sum gives the nine components
+template <class T>
+struct StationGradArgs {
+    int nst;
+    const int *elem;
+    const T *w, *phi;
+    const int *e_nr, *e_pts;
+    const uint8_t *e_axial;
+    const T *e_geom;          // [ne][250]: dsdxii, dsdeta, dzdxii, dzdeta, 1/s, ... (25 each)
+    const T *gmat;            // [2][25]: G_GLL, G_GLJ
+    const int *pt_off, *pt_nu;
+    const cx_t<T> *displ;
+    double *out;              // [nrec][nwave][nst][9]
+    int interval, max_rec;
+    const int *step;
+    int nwave;
+    size_t fstride;
+};
+
+template <class T>
+__global__ void station_grad_kernel(const StationGradArgs<T> a) {
+    using C = cx_t<T>;
+    const int warp = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= a.nst * a.nwave) return;              // whole warps leave together
+    const int step = *a.step;
+    if (step < 0 || a.out == nullptr || step % a.interval != 0) return;
+    const int rec = step / a.interval;
+    if (rec >= a.max_rec) return;
+    const int wf = warp / a.nst, s = warp - wf * a.nst;
+    const C *displ = a.displ + (size_t)wf * a.fstride;
+    const int e = a.elem[s];
+    const int nu = a.e_nr[e] / 2 + 1;
+    const bool axial = a.e_axial[e] != 0;
+    const T *Gxi = axial ? a.gmat + 25 : a.gmat, *Gll = a.gmat;
+    const T *geo = a.e_geom + (size_t)e * 250;
+    const int *pts = a.e_pts + (size_t)e * 25;
+    const T phi = a.phi[s];
+    T acc[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) acc[k] = 0;
+    for (int i = lane; i < nu * 25; i += 32) {
+        const int q = i / nu, al = i - q * nu;
+        const T w = a.w[(size_t)s * 25 + q];
+        if (w == (T)0) continue;
+        const int ii = q / 5, jj = q - ii * 5;
+        auto U = [&](int pq, int c) -> C {
+            const int p = pts[pq];
+            return al < a.pt_nu[p] ? displ[(size_t)(a.pt_off[p] + al) * 3 + c] : mk<T>(0, 0);
+        };
+        const T alf = (T)al;
+        // A_c = (i alpha u0 - u1, i alpha u1 + u0, i alpha u2) at point pq
+        auto A = [&](int pq, int c) -> C {
+            const C u0 = U(pq, 0), u1 = U(pq, 1), u2 = U(pq, 2);
+            return c == 0 ? csub(cia(alf, u0), u1) : c == 1 ? cadd(cia(alf, u1), u0) : cia(alf, u2);
+        };
+        const T sx = geo[q], se = geo[25 + q], zx = geo[50 + q], ze = geo[75 + q], is = geo[100 + q];
+        C g[9];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            C x = mk<T>(0, 0), y = mk<T>(0, 0);
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                const C uc = U(k * 5 + jj, c), ur = U(ii * 5 + k, c);
+                const T gx = Gxi[k * 5 + ii], gy = Gll[k * 5 + jj];
+                x.x += gx * uc.x; x.y += gx * uc.y;
+                y.x += ur.x * gy; y.y += ur.y * gy;
+            }
+            g[c * 3 + 0] = cadd(cscale(x, ze), cscale(y, zx));        // d/ds
+            g[c * 3 + 2] = cadd(cscale(x, se), cscale(y, sx));        // d/dz
+            g[c * 3 + 1] = cscale(A(q, c), is);                       // (1/s) d/dphi terms
+        }
+        if (axial && ii == 0) {
+            // L'Hopital on the axis: A / s replaced by dA/ds
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                C ax = mk<T>(0, 0), ay = mk<T>(0, 0);
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    ax = cadd(ax, cscale(A(k * 5 + jj, c), Gxi[k * 5 + 0]));
+                    ay = cadd(ay, cscale(A(k, c), Gll[k * 5 + jj]));
+                }
+                g[c * 3 + 1] = cadd(g[c * 3 + 1], cadd(cscale(ax, ze), cscale(ay, zx)));
+            }
+        }
+        if (al == 0) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) acc[k] += w * g[k].x;
+        } else {
+            T sn, cs;
+            if constexpr (sizeof(T) == 4) sincosf(alf * phi, &sn, &cs);
+            else sincos(alf * phi, &sn, &cs);
+#pragma unroll
+            for (int k = 0; k < 9; k++) acc[k] += (T)2 * w * (cs * g[k].x - sn * g[k].y);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], off);
+    if (lane == 0) {
+        double *o = a.out + (((size_t)rec * a.nwave + wf) * a.nst + s) * 9;
+#pragma unroll
+        for (int k = 0; k < 9; k++) o[k] = (double)acc[k];
+    }
 }
 
 // element-facing float copy of a double displacement (mixed precision)

@@ -113,6 +113,7 @@ class Model:
     st_w: np.ndarray = field(default_factory=lambda: np.zeros((0, 25)))
     st_phi: np.ndarray = field(default_factory=lambda: np.zeros(0))
     st_interval: int = 1
+    st_gradient: bool = False                     # also record d_j u_i at the stations
     # absorbing boundaries (Clayton 1-D coefficients; sponge gamma per point)
     cl_solid: Optional[dict] = None               # point, rho_vp, rho_vs, area, theta
     cl_fluid: Optional[dict] = None               # point, rho_vp, area

@@ -34,36 +34,124 @@ def _rotate(V, k, angle):
     V[..., j] = -vi * s + V[..., j] * c
 
 
-def rotate_displacement(u_spz, frame, theta, baz, phi, cartesian):
-    """u_spz: [station, time, 3] -> the requested frame (a new array)."""
-    u = np.array(u_spz, dtype=np.float64, copy=True)
+def _rotate9(T, k, angle):
+    """Station::rotate for 3 x 3 tensors stored as 9 (index 3 row + column): rows, then columns."""
+    i = k - 2 if k + 1 > 2 else k + 1
+    j = k - 1 if k + 2 > 2 else k + 2
+    c, s = np.cos(angle), np.sin(angle)
+    for n in range(3):
+        I, J = i * 3 + n, j * 3 + n
+        ti = T[..., I].copy()
+        T[..., I] = ti * c + T[..., J] * s
+        T[..., J] = -ti * s + T[..., J] * c
+    for p in range(3):
+        I, J = p * 3 + i, p * 3 + j
+        ti = T[..., I].copy()
+        T[..., I] = ti * c + T[..., J] * s
+        T[..., J] = -ti * s + T[..., J] * c
+
+
+# Voigt (0 5 4 / 5 1 3 / 4 3 2) <-> 3 x 3 (Station::rotate for 6-component fields)
+_V2T = (0, 5, 4, 5, 1, 3, 4, 3, 2)
+_T2V = (0, 4, 8, 5, 2, 1)
+
+
+def _rotate6(S, k, angle):
+    T = S[..., list(_V2T)].copy()
+    _rotate9(T, k, angle)
+    S[...] = T[..., list(_T2V)]
+
+
+def rotate_field(f, frame, theta, baz, phi, cartesian):
+    """Station::rotateField for a field recorded in (s, phi, z): f [station, time, D] with D = 3
+    (vectors), 6 (Voigt tensors) or 9 (full tensors); returns a new array in the frame."""
+    f = np.array(f, dtype=np.float64, copy=True)
+    rot = {3: _rotate, 6: _rotate6, 9: _rotate9}[f.shape[-1]]
     th = np.asarray(theta)[:, None]
     bz = (np.asarray(baz) + math.pi * .5)[:, None]
     ph = np.asarray(phi)[:, None]
     if cartesian:
         if frame == "ENZ":
-            _rotate(u, 2, bz)
+            rot(f, 2, bz)
         elif frame == "xyz":
-            _rotate(u, 2, -ph)
+            rot(f, 2, -ph)
     else:
         if frame == "RTZ":
-            _rotate(u, 1, th)
+            rot(f, 1, th)
         elif frame == "ENZ":
-            _rotate(u, 1, th)
-            _rotate(u, 2, bz)
+            rot(f, 1, th)
+            rot(f, 2, bz)
         elif frame == "xyz":
-            _rotate(u, 2, -ph)
-    return u
+            rot(f, 2, -ph)
+    return f
+
+
+def rotate_displacement(u_spz, frame, theta, baz, phi, cartesian):
+    """u_spz: [station, time, 3] -> the requested frame (a new array)."""
+    return rotate_field(u_spz, frame, theta, baz, phi, cartesian)
+
+
+def strain_from_gradient(g):
+    """computeGrad6 from computeGrad9 (GradientQuadrature.hpp:177-232): Voigt strain with
+    engineering shear, E = (G0, G4, G8, G5 + G7, G2 + G6, G1 + G3)."""
+    return np.stack([g[..., 0], g[..., 4], g[..., 8], g[..., 5] + g[..., 7], g[..., 2] + g[..., 6],
+                     g[..., 1] + g[..., 3]], axis=-1)
+
+
+def curl_from_gradient(g):
+    """SolidElement::getCurlField (SolidElement.cpp:525-533): (G7 - G5, G2 - G6, G3 - G1)."""
+    return np.stack([g[..., 7] - g[..., 5], g[..., 2] - g[..., 6], g[..., 3] - g[..., 1]], axis=-1)
 
 
 def channel_data(u, channels):
-    """[station, time, 3] in the output frame -> [station, channel, time]."""
+    """Displacement channels of u [station, time, 3], already in the output frame ->
+    [station, channel, time]."""
     cols = []
     for ch in channels:
         if ch == "U_NORM":
             cols.append(np.sqrt(np.sum(u * u, axis=2)))
         else:
             cols.append(u[:, :, int(ch[1]) - 1])
+    return np.stack(cols, axis=1)
+
+
+def group_channels(u_spz, g_spz, channels, frame, theta, baz, phi, cartesian):
+    """[station, channel, time] of one group from the (s, phi, z) displacement [station,
+    time, 3] and gradient [station, time, 9] (None when no G / E / R channel is asked)."""
+    need = {c[0] for c in channels}
+    f = {}
+    if "U" in need:
+        f["U"] = rotate_field(u_spz, frame, theta, baz, phi, cartesian)
+    if "G" in need:
+        f["G"] = rotate_field(g_spz, frame, theta, baz, phi, cartesian)
+    if "E" in need:
+        e = strain_from_gradient(g_spz)
+        e[..., 3:] *= .5
+        e = rotate_field(e, frame, theta, baz, phi, cartesian)
+        e[..., 3:] *= 2.
+        f["E"] = e
+    if "R" in need:
+        f["R"] = rotate_field(curl_from_gradient(g_spz), frame, theta, baz, phi, cartesian)
+    cols = []
+    for ch in channels:
+        x = f[ch[0]]
+        if ch in ("U_NORM", "R_NORM"):
+            cols.append(np.sqrt(np.sum(x * x, axis=2)))
+        elif ch == "G_I1":
+            cols.append(x[:, :, 0] + x[:, :, 4] + x[:, :, 8])
+        elif ch == "E_I1":
+            cols.append(x[:, :, 0] + x[:, :, 1] + x[:, :, 2])
+        elif ch == "E_J2":
+            i1 = x[:, :, 0] + x[:, :, 1] + x[:, :, 2]
+            i2 = (x[:, :, 0] * x[:, :, 1] + x[:, :, 1] * x[:, :, 2] + x[:, :, 2] * x[:, :, 0] -
+                  x[:, :, 3] ** 2 - x[:, :, 4] ** 2 - x[:, :, 5] ** 2)
+            cols.append(i1 * i1 / 3. - i2)
+        elif ch[0] == "G":
+            cols.append(x[:, :, (int(ch[1]) - 1) * 3 + int(ch[2]) - 1])
+        elif ch[0] == "E":
+            cols.append(x[:, :, {"11": 0, "22": 1, "33": 2, "23": 3, "31": 4, "12": 5}[ch[1:]]])
+        else:
+            cols.append(x[:, :, int(ch[1]) - 1])
     return np.stack(cols, axis=1)
 
 

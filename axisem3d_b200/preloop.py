@@ -1089,26 +1089,43 @@ def _pattern(mtype, data, Q, on_axis, w, phi, nu_1, axial_quad):
 
 
 # ----------------------------------------------------------------- stations ---
-U_CHANNELS = {"U1": ("U1", "U"), "U2": ("U2", "U"), "U3": ("U3", "U"), "U_NORM": ("U_NORM", "|U|")}
-STD_ORDER = ("U1", "U2", "U3", "U_NORM")
+# channel::solid::gChannelMap (core/output/channel.hpp:37-73): standard name, the names a user
+# may give, field; kept in the map's order. Stress channels (S*) need the stress of the
+# element at the station and are not recorded by this build.
+SOLID_CHANNELS = (
+    ("U1", ("U1", "U"), "U"), ("U2", ("U2", "U"), "U"), ("U3", ("U3", "U"), "U"),
+    ("U_NORM", ("U_NORM", "|U|"), "U"),
+    ("G11", ("G11", "G"), "G"), ("G12", ("G12", "G"), "G"), ("G13", ("G13", "G"), "G"),
+    ("G21", ("G21", "G"), "G"), ("G22", ("G22", "G"), "G"), ("G23", ("G23", "G"), "G"),
+    ("G31", ("G31", "G"), "G"), ("G32", ("G32", "G"), "G"), ("G33", ("G33", "G"), "G"),
+    ("G_I1", ("G_I1", "Gii"), "G"),
+    ("E11", ("E11", "E"), "E"), ("E22", ("E22", "E"), "E"), ("E33", ("E33", "E"), "E"),
+    ("E23", ("E23", "E", "E32"), "E"), ("E31", ("E31", "E", "E13"), "E"), ("E12", ("E12", "E", "E21"), "E"),
+    ("E_I1", ("E_I1", "Eii"), "E"), ("E_J2", ("E_J2",), "E"),
+    ("R1", ("R1", "R"), "R"), ("R2", ("R2", "R"), "R"), ("R3", ("R3", "R"), "R"),
+    ("R_NORM", ("R_NORM", "|R|"), "R"),
+)
+UNSUPPORTED_CHANNELS = ("S11", "S22", "S33", "S23", "S32", "S31", "S13", "S12", "S21", "S", "S_I1", "Sii",
+                        "S_J2")
 
 
 def standard_channels(user, skipped=None):
-    """channel::solid::ChannelOptions for displacement channels; other channels raise, or are
-    listed in `skipped` when a list is given."""
-    out = []
+    """channel::solid::ChannelOptions: the user's channels as standard names in the map's
+    order; stress channels raise, or are listed in `skipped` when a list is given."""
+    out = set()
     for uch in user:
         found = False
-        for std in STD_ORDER:
-            if uch in U_CHANNELS[std]:
-                out.append(std)
+        for std, names, _ in SOLID_CHANNELS:
+            if uch in names:
+                out.add(std)
                 found = True
         if not found:
-            if skipped is None:
-                raise PreloopError("channel::solid::ChannelOptions::ChannelOptions || Channel %s is not "
-                                   "supported by this build (displacement channels only)." % uch)
+            if skipped is None or uch not in UNSUPPORTED_CHANNELS:
+                raise PreloopError("channel::solid::ChannelOptions::ChannelOptions || %s: %s" %
+                                   ("Stress channels are not supported by this build"
+                                    if uch in UNSUPPORTED_CHANNELS else "Unknown channel for solid", uch))
             skipped.append(uch)
-    return [c for c in STD_ORDER if c in set(out)]
+    return [std for std, _, _ in SOLID_CHANNELS if std in out]
 
 
 def _release_stations(inp, m, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, solid_q, skipped=None):
@@ -1204,6 +1221,8 @@ def _release_stations(inp, m, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, s
             baz.append(float(geo.back_azimuth(llr, True)[0]))
             phi.append(float(spz[1]))
         grp.theta, grp.baz, grp.phi = np.array(th), np.array(baz), np.array(phi)
+        if any(c[0] in "GER" for c in chans):
+            m.st_gradient = True
         intervals.append(intv)
         groups.append(grp)
     interval = int(np.gcd.reduce(intervals)) if intervals else 1

@@ -42,13 +42,14 @@ def run(input_dir: str, output_dir: Optional[str] = None, precision: str = "fp32
         s.synchronize()
         res.seconds_loop = time.perf_counter() - t
         seis = s.seismograms() if len(sim.model.st_elem) else np.zeros((0, 0, 3))
+        grad = s.station_gradients() if sim.model.st_gradient and len(sim.model.st_elem) else None
     wave_precision = 16 if precision == "fp64" else 8
     for g in sim.groups:
         steps, rows = output.group_records(g, sim.nsteps, sim.t0, sim.dt, sim.model.st_interval)
         sl = slice(g.first, g.first + len(g.keys))
         u = np.transpose(seis[rows][:, sl, :], (1, 0, 2))          # [station, time, 3]
-        u = output.rotate_displacement(u, g.frame, g.theta, g.baz, g.phi, sim.cartesian)
-        data = output.channel_data(u, g.channels)
+        gs = np.transpose(grad[rows][:, sl, :], (1, 0, 2)) if grad is not None else None
+        data = output.group_channels(u, gs, g.channels, g.frame, g.theta, g.baz, g.phi, sim.cartesian)
         times = sim.t0 + steps * sim.dt
         res.traces[g.name] = (times, data)
         if output_dir is not None:

@@ -58,6 +58,8 @@ class Solver:
             self._check(self.lib.axg_set_force_sources(h, C.byref(s["fs"])))
         if s["st"].count:
             self._check(self.lib.axg_set_stations(h, C.byref(s["st"]), int(model.st_interval)))
+            if getattr(model, "st_gradient", False):
+                self._check(self.lib.axg_set_station_gradient(h, 1))
         for solid, key in ((1, "cl_s"), (0, "cl_f")):
             if s[key].count:
                 self._check(self.lib.axg_set_clayton(h, solid, C.byref(s[key])))
@@ -218,6 +220,18 @@ class Solver:
         out = np.zeros((n.value, nw, ns, 3))
         if n.value and ns:
             self._check(self.lib.axg_get_seismograms(self.h, out.ctypes.data_as(L.P_f64), C.byref(n)))
+        return out[:, 0] if nw == 1 else out
+
+    def station_gradients(self):
+        """(nrecords, nstations, 9) displacement gradient d_j u_i (index 3 i + j, s / phi / z)
+        at the stations; with batched wavefields (nrecords, nwave, nstations, 9)."""
+        n = C.c_int32()
+        self._check(self.lib.axg_get_station_gradients(self.h, None, C.byref(n)))
+        ns = len(self.model.st_elem)
+        nw = max(1, int(self.model.nwave))
+        out = np.zeros((n.value, nw, ns, 9))
+        if n.value and ns:
+            self._check(self.lib.axg_get_station_gradients(self.h, out.ctypes.data_as(L.P_f64), C.byref(n)))
         return out[:, 0] if nw == 1 else out
 
     # -------------------------------------------------------- differentiation ---

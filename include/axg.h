@@ -279,6 +279,13 @@ int  axg_set_solid_fluid(axg_solver *h, const axg_solid_fluid *c);
 int  axg_set_moment_sources(axg_solver *h, const axg_moment_sources *s);
 int  axg_set_force_sources(axg_solver *h, const axg_force_sources *s);
 int  axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interval);
+/* also record the displacement gradient at the stations (StationSolid::record with the
+   G / E / R channels, StationSolid.cpp:58-91; SolidElement::getNablaField, :410-446): the
+   nine components d_j u_i of GradientQuadrature::computeGrad9 (index 3 i + j, i and j in
+   s, phi, z order; GradientQuadrature.hpp:177-202), interpolated at each station like the
+   displacement; strain and curl are linear in it. For elements without particle
+   relabelling. Set before axg_finalize. */
+int  axg_set_station_gradient(axg_solver *h, int32_t enable);
 /* Clayton-Engquist conditions (GLLPoint.cpp:148-190 builds one ClaytonSolid1D /
    ClaytonFluid1D per point and boundary key); a point on two boundaries is listed once per
    boundary, and its conditions are applied in the order listed */
@@ -385,6 +392,9 @@ int  axg_set_field_raw(axg_solver *h, int32_t solid, int32_t which, const void *
 int  axg_get_field_raw(axg_solver *h, int32_t solid, int32_t which, void *host, int64_t bytes);
 /* seismograms recorded so far: [nrecords][nwave][nstations][3] doubles, SPZ components */
 int  axg_get_seismograms(axg_solver *h, double *host_out, int32_t *nrecords);
+/* station gradients recorded so far: [nrecords][nwave][nstations][9] doubles (after
+   axg_set_station_gradient(h, 1)) */
+int  axg_get_station_gradients(axg_solver *h, double *host_out, int32_t *nrecords);
 int  axg_synchronize(axg_solver *h);
 
 /* ---- diagnostics ---- */

@@ -65,8 +65,8 @@ def _oracle_traces(sim):
     for g in sim.groups:
         steps, rows = output.group_records(g, sim.nsteps, sim.t0, sim.dt, sim.model.st_interval)
         u = np.transpose(seis[rows][:, g.first:g.first + len(g.keys), :], (1, 0, 2))
-        u = output.rotate_displacement(u, g.frame, g.theta, g.baz, g.phi, sim.cartesian)
-        out[g.name] = (sim.t0 + steps * sim.dt, output.channel_data(u, g.channels))
+        out[g.name] = (sim.t0 + steps * sim.dt,
+                       output.group_channels(u, None, g.channels, g.frame, g.theta, g.baz, g.phi, sim.cartesian))
     return out
 
 
@@ -104,3 +104,88 @@ def test_simulation_max_steps(built, tmp_path):
     assert res.sim.nsteps == 17
     t, w = next(iter(res.traces.values()))
     assert len(t) == 17 and w.shape[-1] == 17
+
+
+def _grad9_at_stations(m, field):
+    """computeGrad9 (GradientQuadrature.hpp:177-202, L'Hopital rows :421-459) of the field at
+    the points of each station's element, interpolated like the displacement
+    (Station::interpolate): [station, 9]. Also returns the interpolated displacement."""
+    from axisem3d_b200.solver import spectral_tables
+    t = spectral_tables()
+    gll, glj = t["gGLL"].reshape(5, 5), t["gGLJ"].reshape(5, 5)      # [k, i] = l_k'(x_i)
+    nu_p = np.asarray(m.sp_nr) // 2 + 1
+    off = np.concatenate([[0], np.cumsum(nu_p)[:-1]])
+    f = field.reshape(-1, 3)
+    out_g, out_u = [], []
+    for s, e in enumerate(m.st_elem):
+        nu = int(m.se_nr[e]) // 2 + 1
+        pts = m.se_pts[e]
+        U = np.zeros((nu, 3, 5, 5), np.complex128)
+        for q in range(25):
+            p = pts[q]
+            n = min(nu, nu_p[p])
+            U[:n, :, q // 5, q % 5] = f[off[p]:off[p] + n]
+        gx = glj if m.se_axial[e] else gll
+        X = np.einsum("ki,ackj->acij", gx, U)
+        Y = np.einsum("kj,acik->acij", gll, U)
+        sx, se, zx, ze, inv_s = (m.se_geom[e, k].reshape(5, 5) for k in range(5))
+        al = np.arange(nu)[:, None, None]
+        A = np.stack([1j * al * U[:, 0] - U[:, 1], 1j * al * U[:, 1] + U[:, 0], 1j * al * U[:, 2]], axis=1)
+        g = np.zeros((nu, 9, 5, 5), np.complex128)
+        for c in range(3):
+            g[:, c * 3 + 0] = X[:, c] * ze + Y[:, c] * zx
+            g[:, c * 3 + 2] = X[:, c] * se + Y[:, c] * sx
+            g[:, c * 3 + 1] = A[:, c] * inv_s
+        if m.se_axial[e]:
+            ax = np.einsum("k,ackj->acj", gx[:, 0], A)
+            ay = np.einsum("kj,ack->acj", gll, A[:, :, 0, :])
+            for c in range(3):
+                g[:, c * 3 + 1, 0, :] += ax[:, c] * ze[0] + ay[:, c] * zx[0]
+        w = m.st_w[s].reshape(5, 5)
+        z = np.where(np.arange(nu) == 0, 1.0, 2.0) * np.exp(1j * np.arange(nu) * m.st_phi[s])
+        out_g.append(np.real(np.einsum("a,akij,ij->k", z, g, w)))
+        out_u.append(np.real(np.einsum("a,akij,ij->k", z, U, w)))
+    return np.array(out_g), np.array(out_u)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_station_gradient_matches_numpy_restatement(built, tmp_path, precision):
+    """Gradient records against computeGrad9 restated in numpy on the oracle's displacement,
+    for stations on the surface, inside the box and on the axis (the L'Hopital row)."""
+    import oracle as O
+    from axisem3d_b200 import preloop
+    from axisem3d_b200.solver import Solver
+    d = _box(str(tmp_path / "input"))
+    with open(os.path.join(d, "STATIONS.txt"), "a") as f:
+        f.write("AX XX 0.0 0.0 0.0 30000.0\n")         # on the axis, 30 km deep
+        f.write("IN XX 37000.0 0.0 0.0 41000.0\n")     # inside an element
+    p = os.path.join(d, "inparam.output.yaml")
+    with open(p) as f:
+        txt = f.read()
+    with open(p, "w") as f:
+        f.write(txt.replace("channels: [U]", "channels: [U, G, E_I1, R]"))
+    sim = preloop.build(d, max_steps=40)
+    m = sim.model
+    assert m.st_gradient
+    with Solver(m, precision) as s:
+        s.run(sim.nsteps)
+        grad = s.station_gradients()
+        seis = s.seismograms()
+    o = O.Oracle(m, "fp64")
+    ref_g, ref_u = [], []
+    for k in range(sim.nsteps):
+        g, u = _grad9_at_stations(m, o.get_field("displ"))
+        ref_g.append(g)
+        ref_u.append(u)
+        o.run(1)
+    o_seis = o.seismograms()
+    o.close()
+    ref_g, ref_u = np.array(ref_g), np.array(ref_u)
+    # the restatement reproduces the oracle's own station displacement (timing and weights)
+    assert np.abs(ref_u - o_seis).max() <= 1e-12 * np.abs(o_seis).max()
+    assert np.abs(ref_g).max() > 0
+    tol = 1e-10 if precision == "fp64" else 1e-4
+    for k in range(len(m.st_elem)):
+        err = np.linalg.norm(grad[:, k] - ref_g[:, k]) / np.linalg.norm(ref_g)
+        assert err <= tol, (k, err)
+    assert np.linalg.norm(seis - o_seis) / np.linalg.norm(o_seis) <= tol

@@ -154,7 +154,7 @@ def test_reference_prem_mesh_mass():
     sim = preloop.build(REF + "/01_S362ANI_EMC_global/input1D", skip_unsupported_channels=True)
     m = sim.model
     assert abs(m.sp_mass.sum() * 2 * math.pi / 4.133e24 - 1.0) < 3e-3
-    assert sim.info["skipped_channels"] == ["E_I1", "R3"]
+    assert sim.info["skipped_channels"] == [] and m.st_gradient     # E_I1 and R3 need gradients
     assert len(m.ms_elem) == 1 and m.ms_nu[0] == 3 and m.ms_stf[0].derivative_order == -1
 
 
@@ -165,10 +165,11 @@ def test_unsupported_inputs_raise(tmp_path):
     with open(p) as f:
         txt = f.read()
     with open(p, "w") as f:
-        f.write(txt.replace("channels: [U]", "channels: [U, E_I1]"))
-    with pytest.raises(preloop.PreloopError, match="E_I1"):
+        f.write(txt.replace("channels: [U]", "channels: [U, E_I1, S11]"))
+    with pytest.raises(preloop.PreloopError, match="S11"):
         preloop.build(d)
-    assert preloop.build(d, skip_unsupported_channels=True).info["skipped_channels"] == ["E_I1"]
+    sim = preloop.build(d, skip_unsupported_channels=True)
+    assert sim.info["skipped_channels"] == ["S11"] and sim.groups[0].channels == ["U1", "U2", "U3", "E_I1"]
     p = os.path.join(d, "inparam.model.yaml")
     with open(p) as f:
         txt = f.read()
@@ -256,6 +257,28 @@ def test_output_formats_round_trip(tmp_path):
             for c, ch in enumerate(g.channels):
                 assert np.allclose(np.loadtxt(gd / "dir_rank0" / (ch + ".ascii")), data[:, c].T, rtol=1e-15)
             assert (gd / "dir_rank0" / "list_station.info").read_text().split() == g.keys
+
+
+def test_tensor_rotation_identities():
+    """Rotated gradients are R G R^T, and the strain of the rotated gradient is the rotated
+    strain (the Voigt round trip of Station::rotate for 6-component fields)."""
+    from axisem3d_b200 import output
+    rng = np.random.default_rng(1)
+    g = rng.normal(size=(2, 4, 9))
+    u = rng.normal(size=(2, 4, 3))
+    th, baz, phi = np.array([0.3, 1.2]), np.array([0.5, -0.7]), np.array([0.1, 0.2])
+    for frame in ("RTZ", "ENZ", "xyz"):
+        gr = output.rotate_field(g, frame, th, baz, phi, False)
+        ur = output.rotate_field(u, frame, th, baz, phi, False)
+        for k in range(2):
+            R = output.rotate_field(np.eye(3)[None], frame, th[k:k + 1], baz[k:k + 1], phi[k:k + 1], False)[0].T
+            assert np.allclose(ur[k], u[k] @ R.T)
+            assert np.allclose(gr[k].reshape(4, 3, 3), R @ g[k].reshape(4, 3, 3) @ R.T)
+        e = output.strain_from_gradient(g)
+        e[..., 3:] *= .5
+        er = output.rotate_field(e, frame, th, baz, phi, False)
+        er[..., 3:] *= 2.
+        assert np.allclose(er, output.strain_from_gradient(gr))
 
 
 def test_rotation_frames():
