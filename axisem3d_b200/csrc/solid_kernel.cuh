@@ -509,6 +509,14 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
         const C *displw = a.displ + (size_t)w * a.fstride;
         C *stiffw = a.stiff + (size_t)w * a.fstride;
         AT *statew = a.state + (size_t)w * a.sstride;
+#if AXG_PREFETCH_SLICES
+        if constexpr (!IS3D && ATT != ATT_NONE && NS > 0) {
+            // the SLS state of this 1-D element starts moving into L2 now, so that the stress
+            // pass after the gather and the gradient finds it there
+            constexpr int NPA_ = ATT == ATT_CG4 ? 4 : 25;
+            prefetch_l2(statew + a.state_off[e], (size_t)(6 + 6 * NS) * nu * NPA_ * 2 * sizeof(AT), lane, TEAM);
+        }
+#endif
         // ---------------- gather displacement: U[a][c][q] in region B ----------------
         for (int i = lane; i < nu * 25; i += TEAM) {
             const int q = i / nu, al = i - q * nu;
