@@ -31,6 +31,7 @@ from .inparam import Inparam
 from .meshgen import (cg4_correct, geometry_batch, iso_with_attenuation, lagrange, round_dt, tables,
                       tiso_with_attenuation, weights_cg4)
 from .model import STF, Model
+from .models3d import Model3DError, build_models
 from .solver import att_alpha_beta_gamma, quad_dt
 
 EPS = np.finfo(np.float64).eps
@@ -398,6 +399,7 @@ class _Quads:
         nq = mesh.num_quads
         conn = mesh.connectivity
         self.nodal = mesh.coords[conn].reshape(nq, 8)
+        self.nodal_xy = self.nodal.reshape(nq, 4, 2)
         self.axial = np.array([mesh.left_side(q) >= 0 for q in range(nq)], np.uint8)
         self.fluid = mesh.is_fluid.astype(bool)
         self.sides = {"LEFT": [mesh.left_side(q) for q in range(nq)],
@@ -465,7 +467,14 @@ class _Quads:
         self.iso = iso_e
         self.tiso = tiso
         pt = {k: np.einsum("qk,qkp->qp", v, shp) for k, v in nodal.items()}
+        if tiso:
+            pt.setdefault("VP", pt["VPV"].copy())
+            pt.setdefault("VS", pt["VSV"].copy())
         self.prop = pt
+        # getPointwiseNodal: the 1-D values the REF1D / REF_PERTURB kinds refer to
+        self.prop1d = {k: v.copy() for k, v in pt.items()}
+        # per quad, the properties that vary in phi: {q: {key: [25 arrays of nr_p values]}}
+        self.p3 = {}
         rho = pt["RHO"]
         if tiso:
             vp_iso, vs_iso = pt["VPV"], pt["VSV"]
@@ -476,6 +485,137 @@ class _Quads:
             self.vmax = pt["VP"]
             self.vp_c, self.vs_c = pt["VP"], pt["VS"]
         self.rho = rho
+
+    def refresh_derived(self):
+        """rho, the velocities used by boundaries and dt, and vmax from the current 1-D values."""
+        P = self.prop
+        self.rho = P["RHO"]
+        if self.tiso:
+            iso = self.iso[:, None]
+            self.vmax = np.where(iso, P["VP"], np.maximum(P["VPV"], P["VPH"]))
+            self.vp_c = np.where(iso, P["VP"], P["VPV"])
+            self.vs_c = np.where(iso, P["VS"], P["VSV"])
+        else:
+            self.vmax, self.vp_c, self.vs_c = P["VP"], P["VP"], P["VS"]
+
+    def vmax_3d(self, q):
+        """Material::getMaxVelocity over all slices of a quad with 3-D properties."""
+        nr_e = int(self.pnr[q].max())
+        if self.fluid[q] or self.iso[q]:
+            return float(np.max(self.elemental(q, "VP", nr_e)))
+        return float(max(np.max(self.elemental(q, "VPV", nr_e)), np.max(self.elemental(q, "VPH", nr_e))))
+
+    # ---------------- 3-D properties (Material::addProperty3D, PhysicalProperty) ----------------
+    def pointwise(self, q, key):
+        """PhysicalProperty::getPointwise: 25 arrays (1 value, or nr_p values on phi slices)."""
+        d = self.p3.get(q, {})
+        if key in d:
+            return d[key]
+        return [self.prop[key][q, p:p + 1] for p in range(25)]
+
+    def set_pointwise(self, q, key, arrs):
+        """PhysicalProperty::setGLL with tryReduceTo1D."""
+        from .models3d import try_reduce_1d
+        if try_reduce_1d(arrs):
+            self.prop[key][q, :] = [a[0] for a in arrs]
+            self.p3.get(q, {}).pop(key, None)
+        else:
+            self.p3.setdefault(q, {})[key] = [np.asarray(a, dtype=np.float64) for a in arrs]
+
+    def elemental(self, q, key, nr_e):
+        """PhysicalProperty::getElemental: (1, 25) or (nr_e, 25) by linInterpPhi per point."""
+        from .models3d import lin_interp_phi
+        d = self.p3.get(q, {})
+        if key not in d:
+            return self.prop[key][q][None, :]
+        return np.stack([lin_interp_phi(a, nr_e) for a in d[key]], axis=1)
+
+    def is3d(self, q):
+        return bool(self.p3.get(q))
+
+    def _ensure_tiso_keys(self):
+        for k, src in (("VPV", "VP"), ("VPH", "VP"), ("VSV", "VS"), ("VSH", "VS")):
+            if k not in self.prop:
+                self.prop[k] = self.prop[src].copy()
+                self.prop1d[k] = self.prop1d[src].copy()
+        if "ETA" not in self.prop:
+            self.prop["ETA"] = np.ones_like(self.prop["RHO"])
+            self.prop1d["ETA"] = np.ones_like(self.prop["RHO"])
+        self.tiso = True
+
+    def _evolve_iso_tiso(self, q):
+        """Material::evolveISO_TISO: VPV = VPH = VP, VSV = VSH = VS, ETA = 1."""
+        self._ensure_tiso_keys()
+        for k, src in (("VPV", "VP"), ("VPH", "VP"), ("VSV", "VS"), ("VSH", "VS")):
+            self.prop1d[k][q] = self.prop1d[src][q]
+            self.prop[k][q] = self.prop[src][q]
+            d = self.p3.get(q, {})
+            if src in d:
+                d[k] = [a.copy() for a in d[src]]
+        self.prop["ETA"][q] = 1.
+        self.prop1d["ETA"][q] = 1.
+        self.iso[q] = False
+
+    def apply_model(self, md, geo):
+        """Volumetric3D::applyTo + Material::addProperty3D for every quad in the model's scope."""
+        for q in range(len(self.axial)):
+            res = md.properties(self.nodal_xy[q], self.sz[q], self.pnr[q], geo)
+            if res is None:
+                continue
+            ok, vals = res
+            for j, (key, _, _, ref) in enumerate(md.props):
+                keys = [key]
+                if self.fluid[q]:
+                    if key not in ("RHO", "VP"):
+                        raise PreloopError("Material::getProperty || Unacceptable property key: %s||Rheology "
+                                           "type: FLUID || Model name: %s" % (key, md.name))
+                elif not self.iso[q] and key in ("VP", "VS"):
+                    keys = [key + "V", key + "H"]
+                elif self.iso[q] and key in ("VPV", "VPH", "VSV", "VSH", "ETA"):
+                    self._evolve_iso_tiso(q)
+                if key in ("QMU", "QKAPPA") and key not in self.prop:
+                    raise PreloopError("Material::getProperty || Unacceptable property key: %s (the mesh "
+                                       "has no attenuation) || Model name: %s" % (key, md.name))
+                for k in keys:
+                    cur = self.pointwise(q, k)
+                    nod = self.prop1d[k][q]
+                    new = []
+                    for p in range(25):
+                        v = vals[p][:, j]
+                        if ref == "ABS":
+                            x = v.copy()
+                        elif ref == "REF1D":
+                            x = (v + 1.) * nod[p]
+                        elif ref == "REF3D":
+                            x = (v + 1.) * cur[p]
+                        else:
+                            x = (v + 1.) * (cur[p] - nod[p]) + nod[p]
+                        c = np.broadcast_to(cur[p], x.shape)
+                        new.append(np.where(ok[p], x, c))
+                    self.set_pointwise(q, k, new)
+
+    def finished3d(self):
+        """Material::finished3D: a TISO quad touched by 3-D models whose V and H velocities
+        agree and ETA is 1 becomes ISO."""
+        for q in list(self.p3):
+            if self.fluid[q] or self.iso[q]:
+                continue
+            nr_e = int(self.pnr[q].max())
+            g = {k: self.elemental(q, k, nr_e) for k in ("VPV", "VPH", "VSV", "VSH", "ETA")}
+            n = lambda x: float(np.linalg.norm(x))          # noqa: E731
+            b = lambda x, y: np.broadcast_arrays(x, y)        # noqa: E731
+            vpv, vph = b(g["VPV"], g["VPH"])
+            vsv, vsh = b(g["VSV"], g["VSH"])
+            if (n(vpv - vph) < n(vpv) * EPS and n(vsv - vsh) < n(vsv) * EPS and
+                    n(g["ETA"] - 1.) < n(g["ETA"]) * EPS):
+                self.iso[q] = True
+                self.prop["VP"][q] = self.prop["VPV"][q]
+                self.prop["VS"][q] = self.prop["VSV"][q]
+                d = self.p3.get(q, {})
+                if "VPV" in d:
+                    d["VP"] = d["VPV"]
+                if "VSV" in d:
+                    d["VS"] = d["VSV"]
 
     def normals(self, q, edge):
         """Quad::computeNormal: (points, (5, 2) normals) of one edge."""
@@ -546,14 +686,22 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     channels is dropped, and info["skipped_channels"] names them."""
     inp = Inparam(input_dir)
     mesh = ExodusMesh(inp.path(inp.model.get("model1D:exodus_mesh")))
-    if inp.model.contains("list_of_3D_models") and inp.model.get_vector("list_of_3D_models"):
-        raise PreloopError("Model3D::buildInparam || 3-D models are not supported by this build.")
     geo = Geodesy(mesh, inp)
     abc = build_abc(mesh, inp)
     lucky = inp.advanced.get("develop:fftw_lucky_numbers", bool) \
         if inp.advanced.contains("develop:fftw_lucky_numbers") else True
     quads = _Quads(mesh, inp, geo, abc, lucky)
     nq = mesh.num_quads
+    # ---- 3-D models (Model3D::buildInparam, SE_Model: applyTo, finishing3D / finished3D)
+    try:
+        models = build_models(inp, geo.cartesian)
+        for md in models:
+            quads.apply_model(md, geo)
+    except Model3DError as ex:
+        raise PreloopError(str(ex))
+    quads.finished3d()
+    quads.refresh_derived()
+    q3d = np.array([quads.is3d(q) for q in range(nq)], bool)
     tol = mesh.global_variables["dist_tolerance"]
 
     # ---- time step (SE_Model::computeDt, main.cpp:431-470)
@@ -565,7 +713,8 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
             f = .9
         if abc.clayton and any(quads.sides[k][q] != -1 for k in abc.keys):
             f = .5
-        dts[q] = quad_dt(quads.sz[q], float(np.max(quads.vmax[q]))) * f * courant
+        vmax = quads.vmax_3d(q) if q3d[q] else float(np.max(quads.vmax[q]))
+        dts[q] = quad_dt(quads.sz[q], vmax) * f * courant
     dt_mesh = round_dt(float(dts.min()))
     enforced = inp.source.get("time_axis:enforced_dt")
     dt = dt_mesh if enforced == "NONE" or float(enforced) < EPS else float(enforced)
@@ -605,12 +754,27 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     sid[sp_used] = np.arange(len(sp_used))
     fid[fp_used] = np.arange(len(fp_used))
     ifact = quads.geom[:, 5, :]
+    s1d, f1d = solid_q[~q3d[solid_q]], fluid_q[~q3d[fluid_q]]
     smass = np.zeros(len(sp_used))
-    np.add.at(smass, sid[gll[solid_q]].ravel(), (quads.rho[solid_q] * ifact[solid_q]).ravel())
+    np.add.at(smass, sid[gll[s1d]].ravel(), (quads.rho[s1d] * ifact[s1d]).ravel())
     fmass = np.zeros(len(fp_used))
-    if len(fluid_q):
-        kappa = quads.rho[fluid_q] * quads.vp_c[fluid_q] ** 2
-        np.add.at(fmass, fid[gll[fluid_q]].ravel(), (ifact[fluid_q] / kappa).ravel())
+    if len(f1d):
+        kappa = quads.rho[f1d] * quads.vp_c[f1d] ** 2
+        np.add.at(fmass, fid[gll[f1d]].ravel(), (ifact[f1d] / kappa).ravel())
+    # quads with 3-D properties add per-slice masses (Mass3D where a point's mass varies)
+    smass3, fmass3 = {}, {}
+    for q in np.nonzero(q3d)[0]:
+        rho = quads.pointwise(q, "RHO")
+        vp = quads.pointwise(q, "VP") if quads.fluid[q] else None
+        for p in range(25):
+            if quads.fluid[q]:
+                mval = ifact[q, p] / (np.broadcast_arrays(rho[p], vp[p])[0] * vp[p] ** 2)
+                tgt, idx = fmass3, int(fid[gll[q, p]])
+            else:
+                mval = rho[p] * ifact[q, p]
+                tgt, idx = smass3, int(sid[gll[q, p]])
+            prev = tgt.get(idx)
+            tgt[idx] = mval.copy() if prev is None else prev + mval
 
     # ---- boundaries of the points (Quad::setupGLL, GLLPoint::release)
     axial_pt = np.zeros(ngll, bool)
@@ -630,6 +794,9 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
             pts, nsf = quads.normals(q, quads.sides["SOLID_FLUID"][q])
             for p, n in zip(pts, nsf):
                 normal[gll[q, p]] += n / 2. if quads.fluid[q] else -n / 2.
+        if q3d[q] and abc.clayton and any(quads.sides[k][q] != -1 for k in abc.keys):
+            raise PreloopError("Quad::setupGLL || Clayton boundaries on elements with 3-D properties "
+                               "are not supported by this build (quad %d)." % q)
         if abc.clayton:
             for key in abc.keys:
                 edge = quads.sides[key][q]
@@ -670,6 +837,9 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
                     gmax = float(abc.u0(abs(span), quads.vp_c[q, p], quads.vs_c[q, p], quads.rho[q, p],
                                         bool(quads.fluid[q]))) * pattern
                 if abs(gmax) > EPS:
+                    if q3d[q]:
+                        raise PreloopError("Quad::setupGLL || Sponge layers on elements with 3-D "
+                                           "properties are not supported by this build (quad %d)." % q)
                     g = gll[q, p]
                     gamma_sum[g] += gmax
                     gamma_cnt[g] += 1
@@ -677,11 +847,16 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     # ---- model
     m = Model(dt=dt)
     m.sp_nr = pnr[sp_used].astype(np.int32)
-    m.sp_mass = smass
+    m.sp_mass, m.sp_mass_nr, m.sp_mass_off = _mass_layout(smass, smass3)
     m.sp_axial = axial_pt[sp_used].astype(np.uint8)
     m.sp_coords = coords[sp_used]
     m.fp_nr = pnr[fp_used].astype(np.int32)
-    m.fp_mass = fmass
+    m.fp_mass, m.fp_mass_nr, m.fp_mass_off = _mass_layout(fmass, fmass3)
+    if fmass3 and len(np.intersect1d(sp_used, fp_used)):
+        iface_f = set(int(x) for x in fid[np.intersect1d(sp_used, fp_used)])
+        if any(k in iface_f and np.ptp(v + fmass[k]) > 0 for k, v in fmass3.items()):
+            raise PreloopError("GLLPoint::release || Solid-fluid coupling with 3-D fluid masses is not "
+                               "supported by this build.")
     m.fp_axial = axial_pt[fp_used].astype(np.uint8)
     fsurf = surface_pt & ("TOP" not in abc.keys)
     m.fp_surface = fsurf[fp_used].astype(np.uint8)
@@ -693,16 +868,25 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     m.se_pts = sid[gll[solid_q]].astype(np.int32)
     m.se_axial = quads.axial[solid_q]
     m.se_geom = quads.geom[solid_q]
-    m.se_is3d = np.zeros(ns, np.uint8)
     m.se_theta = theta[solid_q]
     rheo = np.where(quads.iso[solid_q], L.AXG_ISO, L.AXG_TISO).astype(np.int32)
     m.se_rheo = rheo
     m.se_rtz = ((rheo == L.AXG_TISO) & (not geo.cartesian)).astype(np.uint8)
     nmod = np.where(rheo == L.AXG_ISO, 2, 5)
+    # elements whose moduli vary in phi (op1D_3D::regularize1D): per-slice operands
+    rows = np.ones(ns, np.int64)
+    for k in np.nonzero(q3d[solid_q])[0]:
+        q = solid_q[k]
+        keys = (("RHO", "VP", "VS") if rheo[k] == L.AXG_ISO else
+                ("RHO", "VPV", "VPH", "VSV", "VSH", "ETA")) + (("QMU", "QKAPPA") if sls is not None else ())
+        if any(kk in quads.p3.get(q, {}) for kk in keys):
+            rows[k] = enr[q]
+    is3 = rows > 1
+    m.se_is3d = is3.astype(np.uint8)
     mat_off = np.zeros(ns, np.int64)
     if ns:
-        mat_off[1:] = np.cumsum(nmod * 25)[:-1]
-    moduli = np.zeros(int(np.sum(nmod * 25)))
+        mat_off[1:] = np.cumsum(nmod * rows * 25)[:-1]
+    moduli = np.zeros(int(np.sum(nmod * rows * 25)))
     P = quads.prop
     rho_s = quads.rho[solid_q]
     if quads.tiso:
@@ -718,8 +902,8 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
         qk, qm = P["QKAPPA"][solid_q], P["QMU"][solid_q]
         att_mod = np.zeros(ns * 2 * npa)
         wcg4 = weights_cg4(ifact[solid_q]) if att == 1 else None
-    iso_sel = np.nonzero(rheo == L.AXG_ISO)[0]
-    ti_sel = np.nonzero(rheo == L.AXG_TISO)[0]
+    iso_sel = np.nonzero((rheo == L.AXG_ISO) & ~is3)[0]
+    ti_sel = np.nonzero((rheo == L.AXG_TISO) & ~is3)[0]
     dl_all = np.zeros((ns, npa))
     dm_all = np.zeros((ns, npa))
     if len(iso_sel):
@@ -756,12 +940,63 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
         for k, e in enumerate(ti_sel):
             for j, v in enumerate((a_, c_, f_, l_, n_)):
                 moduli[mat_off[e] + 25 * j:mat_off[e] + 25 * (j + 1)] = v[k]
+    # 3-D elements, one at a time (Material::createIsotropic / createTISO on (nr, 25) arrays)
+    att3 = {}
+    for k in np.nonzero(is3)[0]:
+        q = solid_q[k]
+        R = int(rows[k])
+        E = lambda key: np.broadcast_to(quads.elemental(q, key, R), (R, 25)).astype(np.float64)  # noqa: E731
+        rho = E("RHO")
+        if sls is not None:
+            qk3, qm3 = E("QKAPPA"), E("QMU")
+        if rheo[k] == L.AXG_ISO:
+            vp, vs = E("VP"), E("VS")
+            mu3 = rho * vs ** 2
+            lam3 = rho * vp ** 2 - 2. * mu3
+            if sls is not None and att == 0:
+                lam3, mu3, dl, dm = iso_with_attenuation(lam3, mu3, qk3, qm3, sls)
+                att3[k] = (dl, dm)
+            elif sls is not None:
+                kp = lam3 + (2. / 3.) * mu3
+                kp2, mu2, dl4, dm4 = cg4_correct(kp[None], mu3[None], qk3[None], qm3[None], wcg4[k:k + 1], sls)
+                lam3, mu3 = (kp2 - (2. / 3.) * mu2)[0], mu2[0]
+                att3[k] = (dl4[0], dm4[0])
+            mods = (lam3, mu3)
+        else:
+            A3, C3 = rho * E("VPH") ** 2, rho * E("VPV") ** 2
+            L3, N3 = rho * E("VSV") ** 2, rho * E("VSH") ** 2
+            F3 = E("ETA") * (A3 - 2. * L3)
+            if sls is not None and att == 0:
+                A3, C3, F3, L3, N3, dl, dm = tiso_with_attenuation(A3, C3, F3, L3, N3, qk3, qm3, sls)
+                att3[k] = (dl, dm)
+            elif sls is not None:
+                kp = (A3 * 4. + C3 + F3 * 4. - N3 * 4.) / 9.
+                mu0 = (A3 + C3 - F3 * 2. + L3 * 6. + N3 * 5.) / 15.
+                kp2, mu2, dl4, dm4 = cg4_correct(kp[None], mu0[None], qk3[None], qm3[None], wcg4[k:k + 1], sls)
+                kp2, mu2 = kp2[0], mu2[0]
+                A3 = A3 - (kp + 4. / 3. * mu0) + (kp2 + 4. / 3. * mu2)
+                C3 = C3 - (kp + 4. / 3. * mu0) + (kp2 + 4. / 3. * mu2)
+                F3 = F3 - (kp - 2. / 3. * mu0) + (kp2 - 2. / 3. * mu2)
+                L3 = L3 - mu0 + mu2
+                N3 = N3 - mu0 + mu2
+                att3[k] = (dl4[0], dm4[0])
+            mods = (A3, C3, F3, L3, N3)
+        for j, v in enumerate(mods):
+            moduli[mat_off[k] + j * R * 25:mat_off[k] + (j + 1) * R * 25] = v.ravel()
     m.se_mat_off = mat_off
     m.se_moduli = moduli
     if sls is not None and ns:
         m.se_att = np.full(ns, L.AXG_ATT_CG4 if att == 1 else L.AXG_ATT_FULL, np.int32)
-        m.se_att_off = np.arange(ns, dtype=np.int64) * 2 * npa
-        att_mod = np.concatenate([dl_all, dm_all], axis=1).ravel()
+        asz = 2 * rows * npa
+        att_off = np.zeros(ns, np.int64)
+        att_off[1:] = np.cumsum(asz)[:-1]
+        att_mod = np.zeros(int(np.sum(asz)))
+        for k in range(ns):
+            R = int(rows[k])
+            dl, dm = att3[k] if k in att3 else (dl_all[k], dm_all[k])
+            att_mod[att_off[k]:att_off[k] + R * npa] = np.asarray(dl).ravel()
+            att_mod[att_off[k] + R * npa:att_off[k] + 2 * R * npa] = np.asarray(dm).ravel()
+        m.se_att_off = att_off
         m.se_att_moduli = att_mod
         a, b, g = att_alpha_beta_gamma(sls["w"], sls["y"], dt)
         m.nsls, m.att_alpha, m.att_beta, m.att_gamma = len(a), a, b, g
@@ -771,10 +1006,16 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     m.fe_pts = fid[gll[fluid_q]].astype(np.int32) if nf else np.zeros((0, 25), np.int32)
     m.fe_axial = quads.axial[fluid_q]
     m.fe_geom = quads.geom[fluid_q]
-    m.fe_is3d = np.zeros(nf, np.uint8)
     m.fe_theta = theta[fluid_q]
-    m.fe_mat_off = np.arange(nf, dtype=np.int64) * 25
-    m.fe_moduli = (1. / quads.rho[fluid_q]).ravel() if nf else np.zeros(0)
+    frows = np.array([int(enr[q]) if "RHO" in quads.p3.get(q, {}) else 1 for q in fluid_q], np.int64)
+    m.fe_is3d = (frows > 1).astype(np.uint8)
+    fe_off = np.zeros(nf, np.int64)
+    if nf:
+        fe_off[1:] = np.cumsum(frows * 25)[:-1]
+    m.fe_mat_off = fe_off
+    m.fe_moduli = (np.concatenate([(1. / np.broadcast_to(quads.elemental(q, "RHO", int(frows[k])),
+                                                          (int(frows[k]), 25))).ravel()
+                                   for k, q in enumerate(fluid_q)]) if nf else np.zeros(0))
     # solid-fluid coupling
     iface = np.intersect1d(sp_used, fp_used)
     m.sf_solid = sid[iface].astype(np.int32)
@@ -828,6 +1069,29 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
             if inp.advanced.contains("verbose:stability_interval") else 0}
     return Simulation(model=m, nsteps=nstep, t0=m.t0, dt=dt, groups=groups, mesh=mesh,
                       cartesian=geo.cartesian, info=info)
+
+
+def _mass_layout(mass1d, mass3d):
+    """Point masses: 1-D values plus the per-slice contributions of elements with 3-D density
+    (GLLPoint::addMass); (values, per-point count, offsets), the last two None when every
+    point's mass is 1-D (Mass1D) and per-point nr values where it varies (Mass3D)."""
+    out, nr, off = [], np.ones(len(mass1d), np.int32), np.zeros(len(mass1d), np.int64)
+    any3 = False
+    o = 0
+    for p in range(len(mass1d)):
+        v = mass3d.get(p)
+        tot = np.array([mass1d[p]]) if v is None else v + mass1d[p]
+        if len(tot) > 1 and np.linalg.norm(tot - tot[0]) > np.linalg.norm(tot) * EPS:
+            any3 = True
+        else:
+            tot = tot[:1]
+        off[p] = o
+        nr[p] = len(tot)
+        out.append(tot)
+        o += len(tot)
+    if not any3:
+        return np.array([x[0] for x in out]), None, None
+    return np.concatenate(out), nr, off
 
 
 # --------------------------------------------------------- location in the mesh ---

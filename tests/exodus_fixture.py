@@ -299,3 +299,50 @@ def write_inputs(d, mesh_desc, nr=5, depth=10e3, mt=(1e18, 0, 0, 0, 0, 0), hdur=
         for name, net, x1, x2, dep in stations:
             f.write("%s %s %.17g %.17g 0.0 %.17g\n" % (name, net, x1, x2, dep))
     return d
+
+
+def write_grid_v3d(path, coords, data, order):
+    """A StructuredGridV3D NetCDF-3 file: coords {name: values} (in the model's coordinate
+    order), data {name: array over the coords in that order}, stored with its axes permuted
+    to `order` (names of the coords in file order)."""
+    from scipy.io import netcdf_file
+    nc = netcdf_file(path, "w", version=2)
+    names = list(coords)
+    for n in names:
+        nc.createDimension(n, len(coords[n]))
+        v = nc.createVariable(n, "d", (n,))
+        v[:] = coords[n]
+    perm = [names.index(n) for n in order]
+    for k, a in data.items():
+        v = nc.createVariable(k, "d", tuple(order))
+        v[:] = np.transpose(np.asarray(a, np.float64), perm)
+    nc.close()
+
+
+def model3d_yaml(name, fname, horizontal, vertical, nc_vars, data_rank, props, length_unit="km",
+                 angle_unit="degree", depth_solid="true", ellipticity="false", whole_element="false"):
+    """One list_of_3D_models entry; props: (key, nc_var, factor, reference_kind) rows."""
+    lines = ["    - %s:" % name, "        activated: true", "        class_name: StructuredGridV3D",
+             "        nc_data_file: %s" % fname, "        coordinates:",
+             "            horizontal: %s" % horizontal, "            vertical: %s" % vertical,
+             "            ellipticity: %s" % ellipticity,
+             "            depth_below_solid_surface: %s" % depth_solid,
+             "            nc_variables: [%s]" % ", ".join(nc_vars),
+             "            data_rank: [%s]" % ", ".join(str(r) for r in data_rank),
+             "            length_unit: %s" % length_unit, "            angle_unit: %s" % angle_unit,
+             "            undulated_geometry: false", "            whole_element_inplane: %s" % whole_element,
+             "        properties:"]
+    for key, var, factor, kind in props:
+        lines += ["            - %s:" % key, "                nc_var: %s" % var,
+                  "                factor: %r" % factor, "                reference_kind: %s" % kind]
+    lines.append("        store_grid_only_on_leaders: true")
+    return "\n".join(lines) + "\n"
+
+
+def add_3d_models(d, entries):
+    """Replace the empty list_of_3D_models of an input directory by the given entries."""
+    p = os.path.join(d, "inparam.model.yaml")
+    with open(p) as f:
+        txt = f.read()
+    with open(p, "w") as f:
+        f.write(txt.replace("list_of_3D_models: []", "list_of_3D_models:\n" + "".join(entries)))

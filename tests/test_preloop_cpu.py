@@ -95,7 +95,7 @@ def test_box_seismograms_of_both_models_agree_in_the_oracle(built, tmp_path):
     assert _rel(out[0], out[1]) < 1e-10
 
 
-def _shell_dir(tmp, rho_solid=None):
+def _shell_dir(tmp, rho_solid=None, attenuation="CG4"):
     from axisem3d_b200 import meshgen
     r_edges = [3480e3, 3540e3, 3600e3, 4200e3, 4800e3, 5400e3, 6000e3, 6371e3]
     layers = [dict(RHO=9900., VP=8000., VS=0., QMU=0., QKAPPA=57823.)] * 2 + \
@@ -107,7 +107,7 @@ def _shell_dir(tmp, rho_solid=None):
     st = [("S%02d" % k, "XX", 90. - 170. * k / 9, 0.0, 0.0) for k in range(1, 9)]
     return fx.write_inputs(str(tmp), desc, nr=8, depth=100e3, mt=(1e20, -2e19, 3e19, 5e19, -4e19, 1e19),
                            hdur=10.0, decay=1.628, order="RICKER", courant=0.6, record_length=200., stations=st,
-                           horizontal="LATITUDE_LONGITUDE", frame="RTZ", attenuation="CG4",
+                           horizontal="LATITUDE_LONGITUDE", frame="RTZ", attenuation=attenuation,
                            boundaries=["BOTTOM", "RIGHT"], clayton=True, sponge=True, spans=[0.05, 0.05],
                            lucky=True, bound_nr=True), r_edges
 
@@ -174,8 +174,9 @@ def test_unsupported_inputs_raise(tmp_path):
     with open(p) as f:
         txt = f.read()
     with open(p, "w") as f:
-        f.write(txt.replace("list_of_3D_models: []", "list_of_3D_models: [crust]"))
-    with pytest.raises(preloop.PreloopError, match="3-D models"):
+        f.write(txt.replace("list_of_3D_models: []", "list_of_3D_models:\n    - moho:\n        activated: true\n"
+                                                      "        class_name: StructuredGridG3D\n"))
+    with pytest.raises(preloop.PreloopError, match="StructuredGridG3D"):
         preloop.build(d)
 
 
@@ -292,3 +293,121 @@ def test_rotation_frames():
     e = np.array([[[1.0, 0.0, 0.0]]])
     enz = rotate_displacement(e, "ENZ", np.array([0.0]), np.array([0.0]), np.array([0.0]), False)
     assert np.allclose(enz[0, 0], [0, -1, 0], atol=1e-15)
+
+
+# ------------------------------------------------------------------ 3-D models ---
+def _lin_box(x, y, d):
+    return 0.01 + 2e-4 * x - 3e-4 * y + 4e-4 * d        # per km
+
+
+def _lin_rho(x, y, d):
+    return -0.02 + 1e-4 * x + 2e-4 * d
+
+
+def _box3d_dir(tmp, props=None, fluid_vs=False):
+    desc = fx.cartesian_box(NX, NZ, W, H, 2700.0, 5800.0, 3460.0, surface=R)
+    st = [("S%d" % k, "XX", W * k / 5, 0.0, 0.0) for k in range(1, 6)]
+    d = fx.write_inputs(str(tmp), desc, nr=5, depth=10e3, mt=(1e18, -3e17, 2e17, 4e17, -1e17, 5e17),
+                        record_length=2.0, stations=st)
+    x = np.linspace(-120., 120., 7)
+    y = np.linspace(-120., 120., 5)
+    dep = np.linspace(0., 90., 4)
+    X, Y, D = np.meshgrid(x, y, dep, indexing="ij")
+    fx.write_grid_v3d(os.path.join(d, "m3d.nc"), {"x": x, "y": y, "depth": dep},
+                      {"dvs": _lin_box(X, Y, D), "drho": _lin_rho(X, Y, D)}, ["depth", "x", "y"])
+    props = props or [("VS", "dvs", 1.0, "REF1D"), ("RHO", "drho", 0.5, "REF1D")]
+    fx.add_3d_models(d, [fx.model3d_yaml("blob", "m3d.nc", "XY_CARTESIAN", "DEPTH", ["x", "y", "depth"],
+                                         [1, 2, 0], props)])
+    return d
+
+
+def test_3d_model_moduli_and_masses_are_exact(tmp_path):
+    """A grid linear in (x, y, depth) is interpolated exactly: every slice of every element
+    carries rho (1 + 0.5 drho) and vs (1 + dvs) of the 1-D values, and the points carry the
+    per-slice masses (Mass3D)."""
+    from axisem3d_b200 import preloop
+    d = _box3d_dir(tmp_path)
+    m = preloop.build(d).model
+    m1 = preloop.build(_box_dir(tmp_path / "plain")[0]).model
+    assert m.se_is3d.all() and m.sp_mass_nr is not None
+    for e in (0, 37, 79):
+        nr = int(m.se_nr[e])
+        off = m.se_mat_off[e]
+        lam = m.se_moduli[off:off + nr * 25].reshape(nr, 25)
+        mu = m.se_moduli[off + nr * 25:off + 2 * nr * 25].reshape(nr, 25)
+        pts = m.se_pts[e]
+        s_, z_ = m.sp_coords[pts, 0], m.sp_coords[pts, 1]
+        phi = 2 * np.pi * np.arange(nr) / nr
+        xx = s_[None] * np.cos(phi)[:, None] / 1e3
+        yy = s_[None] * np.sin(phi)[:, None] / 1e3
+        dd = (R - z_)[None] / 1e3
+        rho = 2700.0 * (1 + 0.5 * _lin_rho(xx, yy, dd))
+        mu_ref = rho * (3460.0 * (1 + _lin_box(xx, yy, dd))) ** 2
+        assert np.allclose(mu, mu_ref, rtol=1e-13)
+        assert np.allclose(lam, rho * 5800.0 ** 2 - 2 * mu_ref, rtol=1e-13)
+    # Mass3D: the per-slice density times the summed integral factors (1-D mass / 2700)
+    perm = {(round(c[0], 3), round(c[1], 3)): i for i, c in enumerate(m1.sp_coords)}
+    for p in range(0, len(m.sp_nr), 97):
+        nr = int(m.sp_mass_nr[p])
+        vals = m.sp_mass[m.sp_mass_off[p]:m.sp_mass_off[p] + nr]
+        s_, z_ = m.sp_coords[p]
+        phi = 2 * np.pi * np.arange(nr) / nr
+        rho = 2700.0 * (1 + 0.5 * _lin_rho(s_ * np.cos(phi) / 1e3, s_ * np.sin(phi) / 1e3, (R - z_) / 1e3))
+        ref = rho * m1.sp_mass[perm[(round(s_, 3), round(z_, 3))]] / 2700.0
+        assert np.allclose(vals, ref if nr > 1 else ref[:1], rtol=1e-12)
+
+
+def test_3d_model_lat_lon_and_iso_to_tiso(tmp_path):
+    """LATITUDE_LONGITUDE / DEPTH grid on the shell (mesh pole at the source at the north
+    pole, so latitude = 90 - theta and longitude = phi): a VSH model on isotropic elements
+    turns them transversely isotropic (VSV = VS, VSH = VS (1 + dv)); the fluid layer and the
+    deepest mantle lie outside the grid and stay 1-D."""
+    from axisem3d_b200 import _lib as L, preloop
+    d, r_edges = _shell_dir(tmp_path / "in", attenuation="NONE")
+    lat = np.linspace(-90., 90., 7)
+    lon = np.linspace(-180., 180., 9)
+    dep = np.linspace(0., 2000., 5)
+    LA, LO, DE = np.meshgrid(lat, lon, dep, indexing="ij")
+    dv = 0.02 + 1e-4 * LA - 5e-5 * LO + 1e-5 * DE
+    fx.write_grid_v3d(os.path.join(d, "ll.nc"), {"lat": lat, "lon": lon, "dep": dep}, {"dv": dv},
+                      ["lat", "lon", "dep"])
+    fx.add_3d_models(d, [fx.model3d_yaml("sh", "ll.nc", "LATITUDE_LONGITUDE", "DEPTH", ["lat", "lon", "dep"],
+                                         [0, 1, 2], [("VSH", "dv", 1.0, "REF1D")])])
+    sim = preloop.build(d)
+    m = sim.model
+    ti = m.se_rheo == L.AXG_TISO
+    assert ti.any() and m.se_is3d[ti].all() and not m.se_is3d[~ti].any()
+    assert not m.fe_is3d.any()
+    # N = rho VSH^2 on the slices of one TI element against the closed form
+    e = int(np.nonzero(ti)[0][len(np.nonzero(ti)[0]) // 2])
+    nr = int(m.se_nr[e])
+    off = m.se_mat_off[e]
+    pts = m.se_pts[e]
+    s_, z_ = m.sp_coords[pts, 0], m.sp_coords[pts, 1]
+    r_ = np.hypot(s_, z_)
+    th = np.degrees(np.arccos(z_ / r_))
+    phi = 2 * np.pi * np.arange(nr) / nr
+    lo = np.degrees(np.where(phi > np.pi, phi - 2 * np.pi, phi))
+    dvr = 0.02 + 1e-4 * (90. - th)[None] - 5e-5 * lo[:, None] + 1e-5 * ((6371e3 - r_) / 1e3)[None]
+    Lm = m.se_moduli[off + 3 * nr * 25:off + 4 * nr * 25].reshape(nr, 25)
+    N = m.se_moduli[off + 4 * nr * 25:off + 5 * nr * 25].reshape(nr, 25)
+    inside = ((6371e3 - r_) / 1e3) <= 2000.0                 # points below the grid keep 1-D values
+    ref = np.where(inside[None], (1 + dvr) ** 2, 1.0)
+    assert inside.any() and (~inside).any()
+    assert np.allclose(N / Lm, ref, rtol=1e-12)
+
+
+def test_3d_model_errors(tmp_path):
+    from axisem3d_b200 import preloop
+    d = _box3d_dir(tmp_path / "c", props=[("C11", "dvs", 1.0, "ABS")])
+    with pytest.raises(preloop.PreloopError, match="Cij"):
+        preloop.build(d)
+    # a VS model reaching into the fluid layer of the shell
+    d2, _ = _shell_dir(tmp_path / "s")
+    lat, lon, dep = np.linspace(-90., 90., 3), np.linspace(-180., 180., 3), np.linspace(0., 3000., 3)
+    fx.write_grid_v3d(os.path.join(d2, "ll.nc"), {"lat": lat, "lon": lon, "dep": dep},
+                      {"dv": np.full((3, 3, 3), 0.01)}, ["lat", "lon", "dep"])
+    fx.add_3d_models(d2, [fx.model3d_yaml("deep", "ll.nc", "LATITUDE_LONGITUDE", "DEPTH", ["lat", "lon", "dep"],
+                                          [0, 1, 2], [("VS", "dv", 1.0, "REF1D")])])
+    with pytest.raises(preloop.PreloopError, match="Unacceptable property key: VS"):
+        preloop.build(d2)
