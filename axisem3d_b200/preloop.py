@@ -466,6 +466,9 @@ class _Quads:
                      (nrm(nodal["ETA"] - 1.) < 2. * EPS))
         self.iso = iso_e
         self.tiso = tiso
+        self.node_vals = nodal                       # the 4 nodal values of every property
+        self.shp = shp
+        self.gll_keys = {}                           # per quad, the keys a 3-D model has set
         pt = {k: np.einsum("qk,qkp->qp", v, shp) for k, v in nodal.items()}
         if tiso:
             pt.setdefault("VP", pt["VPV"].copy())
@@ -498,6 +501,33 @@ class _Quads:
         else:
             self.vmax, self.vp_c, self.vs_c = P["VP"], P["VP"], P["VS"]
 
+    def abc_rho_vp_vs(self, q):
+        """Material::getPointwiseRhoVpVs (Material.cpp:249-305): rho, vp, vs per point (25
+        arrays of 1 or nr_p values) for Clayton and sponge conditions. TI elements use the
+        Voigt averages of kappa and mu; with nodal-only properties (NodalPhysicalProperty
+        arithmetic on the 4 nodes) they are formed on the nodes and then interpolated."""
+        rho = self.pointwise(q, "RHO")
+        if self.fluid[q]:
+            return rho, self.pointwise(q, "VP"), [np.zeros(1)] * 25
+        if self.iso[q]:
+            return rho, self.pointwise(q, "VP"), self.pointwise(q, "VS")
+
+        def voigt(r, vph, vpv, vsv, vsh, eta):
+            A, C, Lm, N = r * vph ** 2, r * vpv ** 2, r * vsv ** 2, r * vsh ** 2
+            F = eta * (A - Lm * 2.)
+            kp = (A * 4. + C + F * 4. - N * 4.) / 9.
+            mu = (A + C - F * 2. + Lm * 6. + N * 5.) / 15.
+            return np.sqrt((kp + mu * (4. / 3.)) / r), np.sqrt(mu / r)
+
+        keys = ("RHO", "VPH", "VPV", "VSV", "VSH", "ETA")
+        if not (self.gll_keys.get(q, set()) & set(keys)):
+            vp_n, vs_n = voigt(*(self.node_vals[k][q] for k in keys))
+            vp, vs = vp_n @ self.shp[q], vs_n @ self.shp[q]
+            return rho, [vp[p:p + 1] for p in range(25)], [vs[p:p + 1] for p in range(25)]
+        pw = [self.pointwise(q, k) for k in keys]
+        out = [voigt(*np.broadcast_arrays(*(x[p] for x in pw))) for p in range(25)]
+        return rho, [o[0] for o in out], [o[1] for o in out]
+
     def vmax_3d(self, q):
         """Material::getMaxVelocity over all slices of a quad with 3-D properties."""
         nr_e = int(self.pnr[q].max())
@@ -516,6 +546,7 @@ class _Quads:
     def set_pointwise(self, q, key, arrs):
         """PhysicalProperty::setGLL with tryReduceTo1D."""
         from .models3d import try_reduce_1d
+        self.gll_keys.setdefault(q, set()).add(key)
         if try_reduce_1d(arrs):
             self.prop[key][q, :] = [a[0] for a in arrs]
             self.p3.get(q, {}).pop(key, None)
@@ -549,11 +580,19 @@ class _Quads:
         for k, src in (("VPV", "VP"), ("VPH", "VP"), ("VSV", "VS"), ("VSH", "VS")):
             self.prop1d[k][q] = self.prop1d[src][q]
             self.prop[k][q] = self.prop[src][q]
+            if k not in self.node_vals:
+                self.node_vals[k] = self.node_vals[src].copy()
+            self.node_vals[k][q] = self.node_vals[src][q]
             d = self.p3.get(q, {})
             if src in d:
                 d[k] = [a.copy() for a in d[src]]
+            if src in self.gll_keys.get(q, set()):
+                self.gll_keys[q].add(k)
         self.prop["ETA"][q] = 1.
         self.prop1d["ETA"][q] = 1.
+        if "ETA" not in self.node_vals:
+            self.node_vals["ETA"] = np.ones_like(self.node_vals["RHO"])
+        self.node_vals["ETA"][q] = 1.
         self.iso[q] = False
 
     def apply_model(self, md, geo):
@@ -780,9 +819,10 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     axial_pt = np.zeros(ngll, bool)
     surface_pt = np.zeros(ngll, bool)
     normal = np.zeros((ngll, 2))
-    cl_s, cl_f = [], []
+    cl_s, cl_f, cl3_s, cl3_f = [], [], [], []
     gamma_sum = np.zeros(ngll)
     gamma_cnt = np.zeros(ngll, np.int64)
+    gamma3 = {}                                   # points whose gamma varies in phi
     for q in range(nq):
         if quads.axial[q]:
             for p in EDGE_IPNT[quads.sides["LEFT"][q]]:
@@ -794,9 +834,8 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
             pts, nsf = quads.normals(q, quads.sides["SOLID_FLUID"][q])
             for p, n in zip(pts, nsf):
                 normal[gll[q, p]] += n / 2. if quads.fluid[q] else -n / 2.
-        if q3d[q] and abc.clayton and any(quads.sides[k][q] != -1 for k in abc.keys):
-            raise PreloopError("Quad::setupGLL || Clayton boundaries on elements with 3-D properties "
-                               "are not supported by this build (quad %d)." % q)
+        if abc.clayton or abc.sponge:
+            a_rho, a_vp, a_vs = quads.abc_rho_vp_vs(q)
         if abc.clayton:
             for key in abc.keys:
                 edge = quads.sides[key][q]
@@ -808,15 +847,25 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
                     area = float(np.hypot(n[0], n[1]))
                     if area <= 0.:
                         continue
-                    rv = quads.rho[q, p] * quads.vp_c[q, p]
-                    if quads.fluid[q]:
-                        cl_f.append((fid[g], rv, area))
+                    rvp = a_rho[p] * a_vp[p]
+                    rvs = np.broadcast_arrays(a_rho[p], a_vs[p])[0] * a_vs[p]
+                    if len(rvp) == 1 and len(rvs) == 1:
+                        # ClaytonSolid1D / ClaytonFluid1D
+                        if quads.fluid[q]:
+                            cl_f.append((fid[g], float(rvp[0]), area))
+                        else:
+                            _, th = sz2rtheta(n[0], n[1])
+                            cl_s.append((sid[g], float(rvp[0]), float(rvs[0]), area, float(th)))
                     else:
-                        _, th = sz2rtheta(n[0], n[1])
-                        cl_s.append((sid[g], rv, quads.rho[q, p] * quads.vs_c[q, p], area, float(th)))
+                        # ClaytonSolid3D / ClaytonFluid3D: per slice of the point
+                        nrp = int(pnr[g])
+                        unit = np.array([n[0] / area, 0., n[1] / area])
+                        ent = (int(fid[g] if quads.fluid[q] else sid[g]), np.broadcast_to(rvp, (nrp,)).copy(),
+                               np.broadcast_to(rvs, (nrp,)).copy(), np.full(nrp, area), np.tile(unit, (nrp, 1)))
+                        (cl3_f if quads.fluid[q] else cl3_s).append(ent)
         if abc.sponge:
             for p in range(25):
-                gmax = 0.
+                gmax = np.zeros(1)
                 dmin = 1.
                 s_, z_ = quads.sz[q, 0, p], quads.sz[q, 1, p]
                 for key in abc.keys:
@@ -834,15 +883,16 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
                     pattern = math.cos(math.pi / 2. * dist) ** 2
                     if not geo.cartesian and key == "RIGHT":
                         span = span * float(r_)
-                    gmax = float(abc.u0(abs(span), quads.vp_c[q, p], quads.vs_c[q, p], quads.rho[q, p],
-                                        bool(quads.fluid[q]))) * pattern
-                if abs(gmax) > EPS:
-                    if q3d[q]:
-                        raise PreloopError("Quad::setupGLL || Sponge layers on elements with 3-D "
-                                           "properties are not supported by this build (quad %d)." % q)
+                    vp, vs, rho = np.broadcast_arrays(a_vp[p], a_vs[p], a_rho[p])
+                    gmax = np.atleast_1d(abc.u0(abs(span), vp, vs, rho, bool(quads.fluid[q]))) * pattern
+                if np.linalg.norm(gmax) > EPS:
                     g = gll[q, p]
-                    gamma_sum[g] += gmax
                     gamma_cnt[g] += 1
+                    if len(gmax) == 1 and g not in gamma3:
+                        gamma_sum[g] += gmax[0]
+                    else:
+                        prev = gamma3.get(g, np.zeros(1))
+                        gamma3[g] = prev + gmax
 
     # ---- model
     m = Model(dt=dt)
@@ -1033,14 +1083,30 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     if cl_f:
         a_ = np.array(cl_f)
         m.cl_fluid = {"point": a_[:, 0].astype(np.int32), "rho_vp": a_[:, 1], "area": a_[:, 2]}
+    for ents, attr in ((cl3_s, "cl3_solid"), (cl3_f, "cl3_fluid")):
+        if ents:
+            off = np.concatenate([[0], np.cumsum([len(e[1]) for e in ents])[:-1]]).astype(np.int64)
+            d3 = {"point": np.array([e[0] for e in ents], np.int32), "offset": off,
+                  "rho_vp": np.concatenate([e[1] for e in ents]), "area": np.concatenate([e[3] for e in ents])}
+            if attr == "cl3_solid":
+                d3["rho_vs"] = np.concatenate([e[2] for e in ents])
+                d3["normal"] = np.concatenate([e[4] for e in ents])
+            setattr(m, attr, d3)
     if abc.sponge:
+        # Sponge: the average over the contributing elements (GLLPoint::release), 1-D or per slice
+        for g in list(gamma3):
+            gamma3[g] = np.broadcast_to(gamma3[g] + gamma_sum[g], (int(pnr[g]),)) / gamma_cnt[g]
         gam = np.where(gamma_cnt > 0, gamma_sum / np.maximum(gamma_cnt, 1), 0.)
-        sel_s = sp_used[gamma_cnt[sp_used] > 0]
-        sel_f = fp_used[gamma_cnt[fp_used] > 0]
-        if len(sel_s):
-            m.sponge_solid = (sid[sel_s].astype(np.int32), gam[sel_s])
-        if len(sel_f):
-            m.sponge_fluid = (fid[sel_f].astype(np.int32), gam[sel_f])
+        for used, idx, one, three in ((sp_used, sid, "sponge_solid", "sponge3d_solid"),
+                                      (fp_used, fid, "sponge_fluid", "sponge3d_fluid")):
+            sel = used[(gamma_cnt[used] > 0) & np.array([g not in gamma3 for g in used], bool)]
+            sel3 = [g for g in used if g in gamma3]
+            if len(sel):
+                setattr(m, one, (idx[sel].astype(np.int32), gam[sel]))
+            if sel3:
+                off = np.concatenate([[0], np.cumsum([len(gamma3[g]) for g in sel3])[:-1]]).astype(np.int64)
+                setattr(m, three, (idx[np.array(sel3)].astype(np.int32), off,
+                                   np.concatenate([gamma3[g] for g in sel3])))
 
     # ---- sources (Source::release) and the time axis (main.cpp:580-620)
     ctx = _Locator(mesh, quads, geo, gll, solid_q, fluid_q)

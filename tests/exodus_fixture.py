@@ -163,7 +163,7 @@ def spherical_shell(n_theta, r_edges, n_fluid, layers, storage="elements", atten
         sides["solid_fluid_boundary"] = (sf_e, sf_s)
     lay = np.array([j for i in range(n_theta) for j in range(nl)])
     ev = {"element_type": np.zeros(nq), "fluid": (lay < n_fluid).astype(float)}
-    keys = ["RHO", "VP", "VS"] + (["QMU", "QKAPPA"] if attenuation is not None else [])
+    keys = [k for k in layers[0] if attenuation is not None or k not in ("QMU", "QKAPPA")]
     for k in keys:
         vals = np.array([layers[j][k] for j in lay], np.float64)
         if storage == "element_nodes":

@@ -229,3 +229,26 @@ def test_simulation_with_3d_models_matches_oracle(built, tmp_path, case, precisi
         assert np.array_equal(t, t_ref) and np.abs(w_ref).max() > 0
         err = float(np.linalg.norm(w - w_ref) / np.linalg.norm(w_ref))
         assert err <= TOL[precision], (name, err)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_3d_model_at_absorbing_boundaries_matches_oracle(built, tmp_path, precision):
+    """A 3-D model reaching the box's Clayton (right, bottom) and sponge layers: 3-D Clayton
+    conditions and 3-D sponge gammas from the preloop, against the oracle."""
+    from axisem3d_b200 import meshgen, simulation
+    sls = dict(meshgen.default_sls(3, fmin=0.1, fmax=2.0), qkappa=57823.0, qmu=120.0)
+    desc = fx.cartesian_box(10, 8, 100e3, 80e3, 2700.0, 5800.0, 3460.0, attenuation=sls, minimum_period=1.0)
+    st = [("S%d" % k, "XX", 100e3 * k / 5, 0.0, 0.0) for k in range(1, 6)]
+    d = fx.write_inputs(str(tmp_path / "input"), desc, nr=5, depth=10e3, mt=(1e18, -3e17, 2e17, 4e17, -1e17, 5e17),
+                        hdur=1.0, decay=math.pi, order="RICKER", courant=0.6, record_length=8.0, stations=st,
+                        attenuation="FULL", boundaries=["RIGHT", "BOTTOM"], clayton=True, sponge=True,
+                        spans=[0.1, 0.1])
+    d = _with_3d(d, "box")
+    res = simulation.run(d, None, precision=precision)
+    m = res.sim.model
+    assert m.cl3_solid is not None and m.sponge3d_solid is not None
+    ref = _oracle_traces(res.sim)
+    for name, (t_ref, w_ref) in ref.items():
+        t, w = res.traces[name]
+        err = float(np.linalg.norm(w - w_ref) / np.linalg.norm(w_ref))
+        assert err <= TOL[precision], (name, err)

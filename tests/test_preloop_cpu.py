@@ -411,3 +411,23 @@ def test_3d_model_errors(tmp_path):
                                           [0, 1, 2], [("VS", "dv", 1.0, "REF1D")])])
     with pytest.raises(preloop.PreloopError, match="Unacceptable property key: VS"):
         preloop.build(d2)
+
+
+def test_ti_absorbing_boundaries_use_voigt_velocities(tmp_path):
+    """Material::getPointwiseRhoVpVs: Clayton rho vp / rho vs of a transversely isotropic
+    element are the Voigt averages of kappa and mu, not VPV / VSV (homogeneous TI layers, so
+    the nodal interpolation is exact)."""
+    from axisem3d_b200 import preloop
+    r_edges = [5000e3, 5500e3, 6000e3, 6371e3]
+    lay = dict(RHO=3300., VPV=8000., VPH=8400., VSV=4400., VSH=4700., ETA=0.9)
+    desc = fx.spherical_shell(12, r_edges, 0, [lay] * 3, discontinuities=[5000e3, 6371e3])
+    d = fx.write_inputs(str(tmp_path), desc, nr=4, depth=100e3, record_length=20., boundaries=["BOTTOM"],
+                        clayton=True, sponge=False, spans=[0.05])
+    m = preloop.build(d).model
+    A, C, Lm, N = (lay["RHO"] * lay[k] ** 2 for k in ("VPH", "VPV", "VSV", "VSH"))
+    F = lay["ETA"] * (A - 2 * Lm)
+    kp = (4 * A + C + 4 * F - 4 * N) / 9.
+    mu = (A + C - 2 * F + 6 * Lm + 5 * N) / 15.
+    assert m.cl_solid is not None
+    assert np.allclose(m.cl_solid["rho_vp"], np.sqrt((kp + 4. / 3. * mu) * lay["RHO"]), rtol=1e-12)
+    assert np.allclose(m.cl_solid["rho_vs"], np.sqrt(mu * lay["RHO"]), rtol=1e-12)
