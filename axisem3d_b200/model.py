@@ -62,6 +62,7 @@ class Model:
     fp_mass_off: Optional[np.ndarray] = None
     fp_axial: Optional[np.ndarray] = None
     fp_surface: Optional[np.ndarray] = None
+    fp_coords: Optional[np.ndarray] = None        # (n, 2) s, z (not used by the engine)
     # solid elements
     se_nr: np.ndarray = None
     se_pts: np.ndarray = None                     # (ne, 25)

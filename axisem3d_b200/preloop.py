@@ -300,14 +300,90 @@ def build_abc(mesh: ExodusMesh, inp: Inparam) -> ABC:
 
 
 # ------------------------------------------------------------------- Nr field ---
-def nodal_nr(mesh: ExodusMesh, inp: Inparam, lucky: bool) -> np.ndarray:
+def _nr_field(mesh: ExodusMesh, inp: Inparam, geo) -> np.ndarray:
+    """NrField::buildInparam and getNrAtPoints at the mesh nodes: CONSTANT, ANALYTICAL (the
+    depth-dependent default of NrFieldAnalytical.cpp), STRUCTURED (NrFieldStructured.cpp) or
+    POINTWISE (NrFieldPointwise.cpp, inverse-distance average of the 4 nearest control points)."""
+    from .models3d import Model3DError, StructuredGrid, _read_nc
+    gm = inp.nr
+    kind = gm.get_options("type_Nr", {"CONSTANT": "CONSTANT", "ANALYTICAL": "ANALYTICAL",
+                                      "POINTWISE": "POINTWISE", "STRUCTURED": "STRUCTURED"})
+    xy = mesh.coords
+    n = mesh.num_nodes
+    if kind == "CONSTANT":
+        return np.full(n, gm.get_bounded("constant", 1, None, int), np.int64)
+    if kind == "ANALYTICAL":
+        code = "depth-dependent (AxiSEM3D default)"
+        if gm.get("analytical:code_ID") != code:
+            raise PreloopError("NrFieldAnalytical::NrFieldAnalytical || Inconsistent code ID's: || in "
+                               "inparam.nr.yaml:       %s ||in NrFieldAnalytical.cpp: %s"
+                               % (gm.get("analytical:code_ID"), code))
+        root = "analytical:depth_dependent_AxiSEM3D_default"
+        dep = np.array(gm.get_vector(root + ":control_depths", float))
+        nrs = np.array(gm.get_vector(root + ":Nr_at_control_depths", float))
+        if len(dep) != len(nrs):
+            raise PreloopError("NrFieldAnalytical::NrFieldAnalytical || Depths and Nr's do not pair up.")
+        if len(dep) < 2:
+            raise PreloopError("NrFieldAnalytical::NrFieldAnalytical || Insufficient control depths, at "
+                               "least 2.")
+        if np.any(np.diff(dep) <= 0):
+            raise PreloopError("NrFieldAnalytical::NrFieldAnalytical || Depths must be ascendingly sorted.")
+        depth = geo.outer_radius - (xy[:, 1] if geo.cartesian else np.hypot(xy[:, 0], xy[:, 1]))
+        tol = (dep[-1] - dep[0]) * EPS
+        if np.any(depth < dep[0] - tol) or np.any(depth > dep[-1] + tol):
+            raise PreloopError("NrFieldAnalytical::getNrAtPoints || Target depth is out of range.")
+        i1 = np.searchsorted(dep, depth, side="right")
+        i1 = np.where(i1 == 0, 1, np.where(i1 == len(dep), len(dep) - 1, i1))
+        f1 = (depth - dep[i1 - 1]) / (dep[i1] - dep[i1 - 1])
+        return cround(nrs[i1 - 1] * (1. - f1) + nrs[i1] * f1).astype(np.int64)
+    if kind == "STRUCTURED":
+        fname = inp.path(gm.get("structured:nc_data_file"))
+        out_val = gm.get("structured:value_out_of_range", int)
+        names = ("structured_s", "structured_z") if geo.cartesian else ("structured_r", "structured_t")
+        try:
+            grid = StructuredGrid(fname, list(names), [("structured_Nr", 1.)], [0, 1])
+        except Model3DError as ex:
+            raise PreloopError(str(ex))
+        grid.data = cround(grid.data)                     # StructuredGrid<2, int>
+        if geo.cartesian:
+            crd = xy
+        else:
+            r, t = sz2rtheta(xy[:, 0], xy[:, 1])
+            crd = np.stack([r, t], axis=1)
+        v, ok, _ = grid.compute(crd)
+        return np.where(ok, cround(v[:, 0]), out_val).astype(np.int64)
+    # POINTWISE
+    fname = inp.path(gm.get("pointwise:nc_data_file"))
+    factor = gm.get("pointwise:multip_factor", float)
+    try:
+        nc = _read_nc(fname)
+        sz = np.asarray(nc["pointwise_sz"], np.float64).reshape(-1, 2)
+        nrc = np.asarray(nc["pointwise_Nr"], np.float64).reshape(-1)
+    except (KeyError, Model3DError) as ex:
+        raise PreloopError("NrFieldPointwise::NrFieldPointwise || %s: %s" % (fname, ex))
+    from scipy.spatial import cKDTree
+    tree = cKDTree(sz)
+    k = min(4, len(sz))
+    dist, idx = tree.query(xy, k=k)
+    dist, idx = dist.reshape(n, k), idx.reshape(n, k)
+    tol = mesh.global_variables["dist_tolerance"]
+    out = np.empty(n, np.int64)
+    for i in range(n):
+        exact = np.nonzero(dist[i] < tol)[0]
+        if len(exact):
+            v = nrc[idx[i, exact[0]]]
+        else:
+            w = 1. / dist[i]
+            v = cround(np.sum(nrc[idx[i]] * w) / np.sum(w))
+        out[i] = int(cround(v * factor))
+    return out
+
+
+def nodal_nr(mesh: ExodusMesh, inp: Inparam, lucky: bool, geo=None) -> np.ndarray:
     """Nr at the mesh nodes (NrField::buildInparam, ExodusMesh::formNrAtNodes)."""
-    kind = inp.nr.get_options("type_Nr", {"CONSTANT": "CONSTANT", "ANALYTICAL": "ANALYTICAL",
-                                          "POINTWISE": "POINTWISE", "STRUCTURED": "STRUCTURED"})
-    if kind != "CONSTANT":
-        raise PreloopError("NrField::buildInparam || type_Nr = %s is not supported by this build; "
-                           "use CONSTANT." % kind)
-    nr = np.full(mesh.num_nodes, inp.nr.get_bounded("constant", 1, None, int), np.int64)
+    nr = _nr_field(mesh, inp, geo)
+    if nr.min() < 1:
+        raise PreloopError("ExodusMesh::formNrAtNodes || Nr must be positive.")
     if inp.nr.get("bound_Nr_by_inplane", bool):
         conn, xy = mesh.connectivity, mesh.coords
         edges = np.zeros(mesh.num_quads)
@@ -326,8 +402,6 @@ def nodal_nr(mesh: ExodusMesh, inp: Inparam, lucky: bool) -> np.ndarray:
         nr = np.minimum(nr, upper)
     if lucky:
         nr = np.array([next_lucky(int(n)) for n in nr], np.int64)
-    if nr.min() < 1:
-        raise PreloopError("ExodusMesh::formNrAtNodes || Nr must be positive.")
     return nr
 
 
@@ -427,7 +501,7 @@ class _Quads:
         det = 1. / (a * d - b * c)
         self.J = np.stack([a * det, -b * det, -c * det, d * det], axis=-1).reshape(nq, 25, 2, 2)
         # point Nr: nodal Nr interpolated to the points and rounded (Quad::Quad)
-        nnr = nodal_nr(mesh, inp, lucky)
+        nnr = nodal_nr(mesh, inp, lucky, geo)
         shp = gll_shape(self.axial)
         self.pnr = cround(np.einsum("qk,qkp->qp", nnr[conn].astype(np.float64), shp)).astype(np.int64)
         if lucky:
@@ -908,6 +982,7 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
             raise PreloopError("GLLPoint::release || Solid-fluid coupling with 3-D fluid masses is not "
                                "supported by this build.")
     m.fp_axial = axial_pt[fp_used].astype(np.uint8)
+    m.fp_coords = coords[fp_used]
     fsurf = surface_pt & ("TOP" not in abc.keys)
     m.fp_surface = fsurf[fp_used].astype(np.uint8)
     # solid elements
@@ -1108,6 +1183,29 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
                 setattr(m, three, (idx[np.array(sel3)].astype(np.int32), off,
                                    np.concatenate([gamma3[g] for g in sel3])))
 
+    # ---- wavefield scanning (WavefieldScanning::setup, SE_Model::initScanningOnPoints)
+    scan_file = None
+    rs = "wavefield_scanning"
+    if inp.nr.contains(rs + ":enable_scanning") and inp.nr.get(rs + ":enable_scanning", bool):
+        gm = inp.nr
+        nspp = gm.get_bounded(rs + ":advanced:num_steps_per_mesh_period", 4, None, int)
+        interval = max(int(cround(mesh.global_variables["minimum_period"] / nspp / dt)), 1)
+        iface_g = set(np.intersect1d(sp_used, fp_used).tolist())
+        if gm.get(rs + ":advanced:vertex_only", bool):
+            vs_ = sorted({int(sid[gll[q, p]]) for q in solid_q for p in NODE_IPNT})
+            vf_ = sorted({int(fid[gll[q, p]]) for q in fluid_q for p in NODE_IPNT
+                          if int(gll[q, p]) not in iface_g})
+        else:
+            vs_ = list(range(len(sp_used)))
+            vf_ = [int(fid[g]) for g in fp_used if int(g) not in iface_g]
+        m.scanning = {"tol_fourier_h1": gm.get_bounded(rs + ":threshold_Fourier_convergence", 1e-4, 1e-1),
+                      "rel_tol_h1": gm.get_bounded(rs + ":relative_amplitude_skipped", 0., 1.),
+                      "abs_tol_h1": gm.get_bounded(rs + ":advanced:absolute_amplitude_skipped", 1e-14, 1e-10),
+                      "max_num_peaks": gm.get_bounded(rs + ":advanced:max_num_peaks", 1, None, int),
+                      "interval": interval, "solid_points": np.array(vs_, np.int32),
+                      "fluid_points": np.array(vf_, np.int32)}
+        scan_file = gm.get(rs + ":output_file")
+
     # ---- sources (Source::release) and the time axis (main.cpp:580-620)
     ctx = _Locator(mesh, quads, geo, gll, solid_q, fluid_q)
     t_min0 = _release_sources(inp, m, ctx, geo, enr, solid_q, dt)
@@ -1131,6 +1229,7 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     info = {"dt_mesh": dt_mesh, "dt": dt, "nsteps": nstep, "t0": m.t0, "t1": step1 * dt,
             "abc_keys": abc.keys, "attenuation": ["NONE", "FULL", "CG4"][att + 1] if sls is not None else "NONE",
             "nr_range": (int(pnr.min()), int(pnr.max())), "skipped_channels": skipped or [],
+            "scanning_file": scan_file,
             "stability_interval": inp.advanced.get("verbose:stability_interval", int)
             if inp.advanced.contains("verbose:stability_interval") else 0}
     return Simulation(model=m, nsteps=nstep, t0=m.t0, dt=dt, groups=groups, mesh=mesh,

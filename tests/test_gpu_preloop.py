@@ -252,3 +252,54 @@ def test_3d_model_at_absorbing_boundaries_matches_oracle(built, tmp_path, precis
         t, w = res.traces[name]
         err = float(np.linalg.norm(w - w_ref) / np.linalg.norm(w_ref))
         assert err <= TOL[precision], (name, err)
+
+
+SCAN_NR_YAML = """type_Nr: CONSTANT
+bound_Nr_by_inplane: false
+constant: 8
+wavefield_scanning:
+    enable_scanning: true
+    output_file: scan_nr.nc
+    threshold_Fourier_convergence: 1e-2
+    relative_amplitude_skipped: 0.1
+    advanced:
+        absolute_amplitude_skipped: 1e-12
+        max_num_peaks: 10
+        vertex_only: true
+        num_steps_per_mesh_period: 12
+"""
+
+
+def test_scanning_file_and_pointwise_nr_round_trip(built, tmp_path):
+    """Wavefield scanning from inparam.nr.yaml writes the reference's scanning file
+    (pointwise_sz, pointwise_Nr, starting_Nr_for_scanning) with the oracle's scanned Nr; a
+    second preloop reads it as a POINTWISE Nr field and puts those values on the vertices."""
+    import oracle as O
+    from scipy.io import netcdf_file
+    from axisem3d_b200 import preloop, simulation
+    d = _box(str(tmp_path / "input"))
+    with open(os.path.join(d, "inparam.nr.yaml"), "w") as f:
+        f.write(SCAN_NR_YAML)
+    out = str(tmp_path / "output")
+    res = simulation.run(d, out, precision="fp64")
+    m = res.sim.model
+    assert m.scanning is not None
+    nc = netcdf_file(os.path.join(out, "scan_nr.nc"), "r", mmap=False)
+    sz = np.array(nc.variables["pointwise_sz"][:])
+    nr_scan = np.array(nc.variables["pointwise_Nr"][:])
+    nr0 = np.array(nc.variables["starting_Nr_for_scanning"][:])
+    nc.close()
+    o = O.Oracle(m, "fp64")
+    o.run(res.sim.nsteps)
+    ref_s, _ = o.scanning_nr()
+    o.close()
+    pts = m.scanning["solid_points"]
+    assert len(nr_scan) == len(pts) and np.all(nr0 == 8)
+    assert np.array_equal(nr_scan, ref_s[pts]) and nr_scan.max() > 1
+    with open(os.path.join(d, "inparam.nr.yaml"), "w") as f:
+        f.write("type_Nr: POINTWISE\nbound_Nr_by_inplane: false\npointwise:\n    nc_data_file: %s\n"
+                "    multip_factor: 1.\n" % os.path.join(out, "scan_nr.nc"))
+    m2 = preloop.build(d).model
+    look = {(round(c[0], 3), round(c[1], 3)): k for k, c in enumerate(m2.sp_coords)}
+    got = np.array([m2.sp_nr[look[(round(a, 3), round(b, 3))]] for a, b in sz])
+    assert np.array_equal(got, nr_scan)

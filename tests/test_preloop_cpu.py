@@ -431,3 +431,61 @@ def test_ti_absorbing_boundaries_use_voigt_velocities(tmp_path):
     assert m.cl_solid is not None
     assert np.allclose(m.cl_solid["rho_vp"], np.sqrt((kp + 4. / 3. * mu) * lay["RHO"]), rtol=1e-12)
     assert np.allclose(m.cl_solid["rho_vs"], np.sqrt(mu * lay["RHO"]), rtol=1e-12)
+
+
+# ------------------------------------------------------------------ Nr fields ---
+def _set_nr(d, text):
+    with open(os.path.join(d, "inparam.nr.yaml"), "w") as f:
+        f.write(text)
+
+
+def test_nr_fields(tmp_path):
+    """ANALYTICAL (linear in depth between control depths), STRUCTURED (bilinear on an (s, z)
+    grid, out-of-range value outside) and POINTWISE (inverse-distance average of the 4
+    nearest control points, exact on a control point) at the mesh nodes."""
+    from axisem3d_b200 import preloop
+    from axisem3d_b200.exodus import ExodusMesh
+    from axisem3d_b200.inparam import Inparam
+    d, _ = _box_dir(tmp_path)
+    mesh = ExodusMesh(os.path.join(d, "mesh.e"))
+    depth = R - mesh.coords[:, 1]
+    _set_nr(d, "type_Nr: ANALYTICAL\nbound_Nr_by_inplane: false\nanalytical:\n"
+               "    code_ID: depth-dependent (AxiSEM3D default)\n    depth_dependent_AxiSEM3D_default:\n"
+               "        control_depths: [0., 40e3, 80e3]\n        Nr_at_control_depths: [40, 20, 8]\n")
+    geo = preloop.Geodesy(mesh, Inparam(d))
+    nr = preloop._nr_field(mesh, Inparam(d), geo)
+    ref = np.where(depth <= 40e3, 40 - 20 * depth / 40e3, 20 - 12 * (depth - 40e3) / 40e3)
+    assert np.array_equal(nr, np.floor(ref + 0.5).astype(int))
+    # structured: Nr = 10 + s/1e4 + z-offset term on a grid covering half the box
+    s_ax, z_ax = np.linspace(0., 50e3, 6), np.linspace(R - 80e3, R, 5)
+    S, Z = np.meshgrid(s_ax, z_ax, indexing="ij")
+    from scipy.io import netcdf_file
+    nc = netcdf_file(os.path.join(d, "nr.nc"), "w", version=2)
+    nc.createDimension("ns", 6)
+    nc.createDimension("nz", 5)
+    for n, a, dim in (("structured_s", s_ax, "ns"), ("structured_z", z_ax, "nz")):
+        v = nc.createVariable(n, "d", (dim,))
+        v[:] = a
+    v = nc.createVariable("structured_Nr", "d", ("ns", "nz"))
+    v[:] = 10 + S / 1e4 + (R - Z) / 2e4
+    nc.close()
+    _set_nr(d, "type_Nr: STRUCTURED\nbound_Nr_by_inplane: false\nstructured:\n    nc_data_file: nr.nc\n"
+               "    value_out_of_range: 3\n")
+    nr = preloop._nr_field(mesh, Inparam(d), geo)
+    s_, z_ = mesh.coords[:, 0], mesh.coords[:, 1]
+    inside = s_ <= 50e3 + 1e-6
+    assert np.all(nr[~inside] == 3)
+    assert np.array_equal(nr[inside], np.floor(10 + s_[inside] / 1e4 + (R - z_[inside]) / 2e4 + 0.5).astype(int))
+    # pointwise: control points on every mesh node carry 7 + node index % 5
+    nc = netcdf_file(os.path.join(d, "pw.nc"), "w", version=2)
+    nc.createDimension("dim_point", mesh.num_nodes)
+    nc.createDimension("dim_sz", 2)
+    v = nc.createVariable("pointwise_sz", "d", ("dim_point", "dim_sz"))
+    v[:] = mesh.coords
+    v = nc.createVariable("pointwise_Nr", "i", ("dim_point",))
+    v[:] = 7 + np.arange(mesh.num_nodes) % 5
+    nc.close()
+    _set_nr(d, "type_Nr: POINTWISE\nbound_Nr_by_inplane: false\npointwise:\n    nc_data_file: pw.nc\n"
+               "    multip_factor: 2.\n")
+    nr = preloop._nr_field(mesh, Inparam(d), geo)
+    assert np.array_equal(nr, 2 * (7 + np.arange(mesh.num_nodes) % 5))
