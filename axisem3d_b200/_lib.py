@@ -148,6 +148,9 @@ SIGNATURES = {
     "axg_field_raw_bytes": (C.c_int, [H, C.c_int32, C.c_int32, P_i64]),
     "axg_set_field_raw": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_int64]),
     "axg_get_field_raw": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_int64]),
+    "axg_set_element_record": (C.c_int, [H, C.c_int32, P_i32, P_i32, P_i32, C.c_int32, C.c_int32]),
+    "axg_element_record_words": (C.c_int, [H, P_i64]),
+    "axg_get_element_records": (C.c_int, [H, C.c_int32, C.c_int32, P_f64]),
     "axg_synchronize": (C.c_int, [H]),
     "axg_launch_count": (C.c_int, [H, P_i64]),
     "axg_set_timing": (C.c_int, [H, C.c_int32]),

@@ -663,6 +663,22 @@ int axg_get_station_gradients(axg_solver *h, double *host_out, int32_t *nrecords
         if (nrecords) *nrecords = n;
     });
 }
+int axg_set_element_record(axg_solver *h, int32_t n, const int32_t *elem, const int32_t *gll,
+                           const int32_t *kind, int32_t interval, int32_t ring) {
+    return guarded(h, [&] {
+        if (!h->finalized) throw axg::Error(AXG_E_STATE, "axg_set_element_record || axg_finalize not called.");
+        h->eng->set_element_record(n, elem, gll, kind, interval, ring);
+    });
+}
+int axg_element_record_words(const axg_solver *h, int64_t *words) {
+    if (!h || !words) return AXG_E_ARG;
+    if (!h->finalized) return AXG_E_STATE;
+    *words = h->eng->element_record_words();
+    return AXG_OK;
+}
+int axg_get_element_records(axg_solver *h, int32_t rec_first, int32_t nrec, double *host_out) {
+    return guarded(h, [&] { h->eng->get_element_records(rec_first, nrec, host_out); });
+}
 int axg_synchronize(axg_solver *h) {
     return guarded(h, [&] { h->eng->synchronize(); });
 }

@@ -159,6 +159,10 @@ public:
     virtual void get_field_raw(int solid, int which, void *host, int64_t bytes) = 0;
     virtual int get_seismograms(double *out) = 0;
     virtual int get_station_gradients(double *out) = 0;
+    virtual void set_element_record(int n, const int *elem, const int *gll, const int *kind, int interval,
+                                    int ring) = 0;
+    virtual int64_t element_record_words() const = 0;
+    virtual void get_element_records(int rec_first, int nrec, double *out) = 0;
     virtual void synchronize() = 0;
     virtual int64_t launches() const = 0;
     virtual void set_timing(bool on) = 0;

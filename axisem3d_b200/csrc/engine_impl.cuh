@@ -225,6 +225,7 @@ public:
         ensure_capacity(tstep + 1);
         set_step(tstep);
         launch_stations();
+        launch_element_record();
         launch_scan();
     }
 
@@ -367,6 +368,59 @@ public:
             AXG_CUDA(cudaMemcpy(out, seis_grad_.p, (size_t)nrec * nwave_ * st_n_ * 9 * sizeof(double),
                                 cudaMemcpyDeviceToHost));
         return nrec;
+    }
+    // ----------------------------------------------------- element output ---
+    void set_element_record(int n, const int *elem, const int *gll, const int *kind, int interval,
+                            int ring) override {
+        need();
+        if (n < 0 || interval < 1 || ring < 1 || (n && (!elem || !gll || !kind)))
+            throw Error(AXG_E_ARG, "ElementOpGroup::ElementOpGroup || bad element-record arguments.");
+        const HostSolidElements &h = model_.se;
+        std::vector<int64_t> off(std::max(n, 1), 0);
+        int64_t words = 0;
+        bool grad = false;
+        for (int i = 0; i < n; i++) {
+            if (elem[i] < 0 || elem[i] >= h.count || gll[i] < 0 || gll[i] > 24 || kind[i] < 0 || kind[i] > 1)
+                throw Error(AXG_E_ARG, "ElementOpSolid::ElementOpSolid || element, GLL point or kind out of range.");
+            off[i] = words;
+            words += (int64_t)(h.nr[elem[i]] / 2 + 1) * (kind[i] ? 9 : 3);
+            grad = grad || kind[i] == 1;
+        }
+        if (grad)
+            for (int i = 0; i < model_.prt.count; i++)
+                for (int k = 0; k < n; k++)
+                    if (kind[k] == 1 && elem[k] == model_.prt.elem[i])
+                        throw Error(AXG_E_ARG, "SolidElement::getNablaField || gradient output of an "
+                                               "element under particle relabelling is not supported.");
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        er_n_ = n; er_words_ = words; er_interval_ = interval; er_ring_ = ring;
+        er_elem_.upload(std::vector<int>(elem, elem + n));
+        er_gll_.upload(std::vector<int>(gll, gll + n));
+        er_kind_.upload(std::vector<int>(kind, kind + n));
+        er_off_.upload(off);
+        er_out_.alloc((size_t)ring * nwave_ * (size_t)std::max<int64_t>(words, 1));
+        er_out_.zero(stream_);
+        if (n) upload_elem_tables(grad);
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+    }
+    int64_t element_record_words() const override { return er_words_; }
+    void get_element_records(int rec_first, int nrec, double *out) override {
+        need();
+        if (!er_n_) throw Error(AXG_E_STATE, "ElementOpGroup::dumpToFile || no element record was set.");
+        const int last = step_ > 0 ? (step_ - 1) / er_interval_ : -1;
+        if (nrec < 0 || rec_first < 0 || rec_first + nrec - 1 > last || rec_first <= last - er_ring_ ||
+            (nrec && !out))
+            throw Error(AXG_E_ARG, "ElementOpGroup::dumpToFile || records not in the device ring.");
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        const size_t per = (size_t)nwave_ * (size_t)er_words_;
+        std::vector<C> h(per);
+        for (int r = 0; r < nrec; r++) {
+            const int slot = (rec_first + r) % er_ring_;
+            AXG_CUDA(cudaMemcpy(h.data(), er_out_.p + (size_t)slot * per, per * sizeof(C), cudaMemcpyDeviceToHost));
+            double *o = out + (size_t)r * per * 2;
+            for (size_t i = 0; i < per; i++) { o[2 * i] = (double)h[i].x; o[2 * i + 1] = (double)h[i].y; }
+        }
     }
     void synchronize() override { AXG_CUDA(cudaStreamSynchronize(stream_)); }
     int64_t launches() const override { return launches_; }
@@ -1427,20 +1481,29 @@ private:
             if (ms.elem[i] < 0 || ms.elem[i] >= model_.se.count)
                 throw Error(AXG_E_ARG, "SolidMoment::SolidMoment || element index out of range.");
         // element lookup tables in original order for the source kernels
+        if (ms_n_ || fs_n_ || model_.st.count) upload_elem_tables(ms_n_ || model_.st.gradient);
+    }
+
+    // solid-element tables in the model's order for the source, station and element-record
+    // kernels: nr, points, axial flags and, when asked, the geometry [e][250] (the first
+    // five 25-rows of the element's geometry, then the same scaled by the last row)
+    void upload_elem_tables(bool geom) {
         const HostSolidElements &h = model_.se;
-        std::vector<T> g((size_t)h.count * 250);
-        for (int e = 0; e < h.count; e++)
-            for (int c = 0; c < 5; c++)
-                for (int q = 0; q < 25; q++) {
-                    g[(size_t)e * 250 + c * 25 + q] = (T)h.geom[(size_t)e * 150 + c * 25 + q];
-                    g[(size_t)e * 250 + 125 + c * 25 + q] =
-                        (T)(h.geom[(size_t)e * 150 + c * 25 + q] * h.geom[(size_t)e * 150 + 125 + q]);
-                }
-        if (ms_n_ || fs_n_ || model_.st.count) {
+        if (!e_nr_.n && h.count) {
             e_nr_.upload(h.nr); e_pts_.upload(h.pts);
             std::vector<uint8_t> ax(h.axial.begin(), h.axial.end());
             e_axial_.upload(ax);
-            if (ms_n_ || model_.st.gradient) e_geom_.upload(g);
+        }
+        if (geom && !e_geom_.n && h.count) {
+            std::vector<T> g((size_t)h.count * 250);
+            for (int e = 0; e < h.count; e++)
+                for (int c = 0; c < 5; c++)
+                    for (int q = 0; q < 25; q++) {
+                        g[(size_t)e * 250 + c * 25 + q] = (T)h.geom[(size_t)e * 150 + c * 25 + q];
+                        g[(size_t)e * 250 + 125 + c * 25 + q] =
+                            (T)(h.geom[(size_t)e * 150 + c * 25 + q] * h.geom[(size_t)e * 150 + 125 + q]);
+                    }
+            e_geom_.upload(g);
         }
     }
 
@@ -1642,6 +1705,20 @@ private:
         }
     }
 
+    void launch_element_record() {
+        if (!er_n_) return;
+        ElemRecordArgs<T> a;
+        a.n = er_n_; a.elem = er_elem_.p; a.gll = er_gll_.p; a.kind = er_kind_.p; a.off = er_off_.p;
+        a.words = er_words_; a.e_nr = e_nr_.p; a.e_pts = e_pts_.p; a.e_axial = e_axial_.p;
+        a.e_geom = e_geom_.p; a.gmat = gmat_.p; a.pt_off = sp_.off.p; a.pt_nu = sp_.nu.p;
+        a.displ = elem_displ(sp_); a.out = er_out_.p; a.interval = er_interval_; a.ring = er_ring_;
+        a.step = step_dev_.p; a.nwave = nwave_; a.fstride = (size_t)sp_.total * 3;
+        const int threads = 256;                          // eight entries per block
+        const int blocks = (int)(((size_t)er_n_ * nwave_ * 32 + threads - 1) / threads);
+        element_record_kernel<T><<<blocks, threads, 0, stream_>>>(a);
+        post_launch();
+    }
+
     void launch_points(int mask) {
         for (int solid = 1; solid >= 0; solid--) {
             PointDev &P = solid ? sp_ : fp_;
@@ -1713,6 +1790,7 @@ private:
         launch_clayton();
         launch_coupling();
         launch_stations();
+        launch_element_record();
         launch_scan();
         launch_points(7);
         advance_step_kernel<T><<<1, 1, 0, stream_>>>(step_dev_.p);
@@ -1809,6 +1887,11 @@ private:
     DBuf<int> st_el_;
     DBuf<T> st_w_, st_phi_;
     DBuf<double> seis_, seis_grad_;
+    int er_n_ = 0, er_interval_ = 1, er_ring_ = 1;
+    int64_t er_words_ = 0;
+    DBuf<int> er_elem_, er_gll_, er_kind_;
+    DBuf<int64_t> er_off_;
+    DBuf<C> er_out_;
     DBuf<int> step_dev_, nonfinite_;
 };
 

@@ -886,6 +886,54 @@ struct StationGradArgs {
     size_t fstride;
 };
 
+// computeGrad9 (GradientQuadrature.hpp:177-202) of Fourier order al at GLL point q of one
+// element, with the L'Hopital rows on the axis (:421-459): g[c * 3 + d] = d_d u_c, d = (s, phi, z)
+template <class T>
+__device__ __forceinline__ void grad9_point(const cx_t<T> *displ, const int *pts, const int *pt_off,
+                                            const int *pt_nu, const T *geo, const T *Gxi, const T *Gll,
+                                            bool axial, int q, int al, cx_t<T> g[9]) {
+    using C = cx_t<T>;
+    const int ii = q / 5, jj = q - ii * 5;
+    auto U = [&](int pq, int c) -> C {
+        const int p = pts[pq];
+        return al < pt_nu[p] ? displ[(size_t)(pt_off[p] + al) * 3 + c] : mk<T>(0, 0);
+    };
+    const T alf = (T)al;
+    // A_c = (i alpha u0 - u1, i alpha u1 + u0, i alpha u2) at point pq
+    auto A = [&](int pq, int c) -> C {
+        const C u0 = U(pq, 0), u1 = U(pq, 1), u2 = U(pq, 2);
+        return c == 0 ? csub(cia(alf, u0), u1) : c == 1 ? cadd(cia(alf, u1), u0) : cia(alf, u2);
+    };
+    const T sx = geo[q], se = geo[25 + q], zx = geo[50 + q], ze = geo[75 + q], is = geo[100 + q];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        C x = mk<T>(0, 0), y = mk<T>(0, 0);
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            const C uc = U(k * 5 + jj, c), ur = U(ii * 5 + k, c);
+            const T gx = Gxi[k * 5 + ii], gy = Gll[k * 5 + jj];
+            x.x += gx * uc.x; x.y += gx * uc.y;
+            y.x += ur.x * gy; y.y += ur.y * gy;
+        }
+        g[c * 3 + 0] = cadd(cscale(x, ze), cscale(y, zx));        // d/ds
+        g[c * 3 + 2] = cadd(cscale(x, se), cscale(y, sx));        // d/dz
+        g[c * 3 + 1] = cscale(A(q, c), is);                       // (1/s) d/dphi terms
+    }
+    if (axial && ii == 0) {
+        // L'Hopital on the axis: A / s replaced by dA/ds
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            C ax = mk<T>(0, 0), ay = mk<T>(0, 0);
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                ax = cadd(ax, cscale(A(k * 5 + jj, c), Gxi[k * 5 + 0]));
+                ay = cadd(ay, cscale(A(k, c), Gll[k * 5 + jj]));
+            }
+            g[c * 3 + 1] = cadd(g[c * 3 + 1], cadd(cscale(ax, ze), cscale(ay, zx)));
+        }
+    }
+}
+
 template <class T>
 __global__ void station_grad_kernel(const StationGradArgs<T> a) {
     using C = cx_t<T>;
@@ -912,50 +960,13 @@ __global__ void station_grad_kernel(const StationGradArgs<T> a) {
         const int q = i / nu, al = i - q * nu;
         const T w = a.w[(size_t)s * 25 + q];
         if (w == (T)0) continue;
-        const int ii = q / 5, jj = q - ii * 5;
-        auto U = [&](int pq, int c) -> C {
-            const int p = pts[pq];
-            return al < a.pt_nu[p] ? displ[(size_t)(a.pt_off[p] + al) * 3 + c] : mk<T>(0, 0);
-        };
-        const T alf = (T)al;
-        // A_c = (i alpha u0 - u1, i alpha u1 + u0, i alpha u2) at point pq
-        auto A = [&](int pq, int c) -> C {
-            const C u0 = U(pq, 0), u1 = U(pq, 1), u2 = U(pq, 2);
-            return c == 0 ? csub(cia(alf, u0), u1) : c == 1 ? cadd(cia(alf, u1), u0) : cia(alf, u2);
-        };
-        const T sx = geo[q], se = geo[25 + q], zx = geo[50 + q], ze = geo[75 + q], is = geo[100 + q];
         C g[9];
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            C x = mk<T>(0, 0), y = mk<T>(0, 0);
-#pragma unroll
-            for (int k = 0; k < 5; k++) {
-                const C uc = U(k * 5 + jj, c), ur = U(ii * 5 + k, c);
-                const T gx = Gxi[k * 5 + ii], gy = Gll[k * 5 + jj];
-                x.x += gx * uc.x; x.y += gx * uc.y;
-                y.x += ur.x * gy; y.y += ur.y * gy;
-            }
-            g[c * 3 + 0] = cadd(cscale(x, ze), cscale(y, zx));        // d/ds
-            g[c * 3 + 2] = cadd(cscale(x, se), cscale(y, sx));        // d/dz
-            g[c * 3 + 1] = cscale(A(q, c), is);                       // (1/s) d/dphi terms
-        }
-        if (axial && ii == 0) {
-            // L'Hopital on the axis: A / s replaced by dA/ds
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                C ax = mk<T>(0, 0), ay = mk<T>(0, 0);
-#pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    ax = cadd(ax, cscale(A(k * 5 + jj, c), Gxi[k * 5 + 0]));
-                    ay = cadd(ay, cscale(A(k, c), Gll[k * 5 + jj]));
-                }
-                g[c * 3 + 1] = cadd(g[c * 3 + 1], cadd(cscale(ax, ze), cscale(ay, zx)));
-            }
-        }
+        grad9_point<T>(displ, pts, a.pt_off, a.pt_nu, geo, Gxi, Gll, axial, q, al, g);
         if (al == 0) {
 #pragma unroll
             for (int k = 0; k < 9; k++) acc[k] += w * g[k].x;
         } else {
+            const T alf = (T)al;
             T sn, cs;
             if constexpr (sizeof(T) == 4) sincosf(alf * phi, &sn, &cs);
             else sincos(alf * phi, &sn, &cs);
@@ -971,6 +982,69 @@ __global__ void station_grad_kernel(const StationGradArgs<T> a) {
         double *o = a.out + (((size_t)rec * a.nwave + wf) * a.nst + s) * 9;
 #pragma unroll
         for (int k = 0; k < 9; k++) o[k] = (double)acc[k];
+    }
+}
+
+// Element-wise output (ElementOpSolid::record, core/output/element-wise/element/ElementOpSolid.cpp:
+// 48-80, before its RTZ transform and channel forming): at every step that is a multiple of the
+// interval, the Fourier coefficients of orders alpha < nr/2 + 1 of the element (the element's
+// nu_1, collectDisplFromPoints) of the displacement (kind 0: 3 components) or of its gradient
+// (kind 1: 9 components, computeGrad9) at one GLL point of one solid element, into slot
+// (step / interval) % ring of a device ring of records, [ring][nwave][words], the entry's
+// words at off[entry] with orders slowest and components fastest.
+template <class T>
+struct ElemRecordArgs {
+    int n;
+    const int *elem, *gll, *kind;
+    const int64_t *off;
+    int64_t words;
+    const int *e_nr, *e_pts;
+    const uint8_t *e_axial;
+    const T *e_geom;
+    const T *gmat;
+    const int *pt_off, *pt_nu;
+    const cx_t<T> *displ;
+    cx_t<T> *out;
+    int interval, ring;
+    const int *step;
+    int nwave;
+    size_t fstride;
+};
+
+// one warp per (entry, wavefield); displacement entries: the lanes take consecutive
+// (order, component) words, which are consecutive in the point's field and in the record
+// (coalesced copy); gradient entries: one order per lane, all nine components
+template <class T>
+__global__ void element_record_kernel(const ElemRecordArgs<T> a) {
+    using C = cx_t<T>;
+    const int warp = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= a.n * a.nwave) return;                // whole warps leave together
+    const int step = *a.step;
+    if (step < 0 || step % a.interval != 0) return;
+    const int slot = (step / a.interval) % a.ring;
+    const int wf = warp / a.n, k = warp - wf * a.n;
+    const C *displ = a.displ + (size_t)wf * a.fstride;
+    C *out = a.out + ((size_t)slot * a.nwave + wf) * (size_t)a.words + (size_t)a.off[k];
+    const int e = a.elem[k], q = a.gll[k];
+    const int nu = a.e_nr[e] / 2 + 1;
+    const int *pts = a.e_pts + (size_t)e * 25;
+    if (a.kind[k] == 0) {
+        const int p = pts[q];
+        const int pnu = a.pt_nu[p];
+        const C *src = displ + (size_t)a.pt_off[p] * 3;
+        for (int i = lane; i < nu * 3; i += 32)
+            out[i] = i / 3 < pnu ? src[i] : mk<T>(0, 0);
+    } else {
+        const bool axial = a.e_axial[e] != 0;
+        const T *Gxi = axial ? a.gmat + 25 : a.gmat, *Gll = a.gmat;
+        const T *geo = a.e_geom + (size_t)e * 250;
+        for (int al = lane; al < nu; al += 32) {
+            C g[9];
+            grad9_point<T>(displ, pts, a.pt_off, a.pt_nu, geo, Gxi, Gll, axial, q, al, g);
+#pragma unroll
+            for (int c = 0; c < 9; c++) out[(size_t)al * 9 + c] = g[c];
+        }
     }
 }
 

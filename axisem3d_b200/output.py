@@ -221,3 +221,159 @@ def group_records(group, nsteps, t0, dt, engine_interval):
              if group.tmin <= t0 + t * dt <= group.tmax]
     rows = [t // engine_interval for t in steps]
     return np.array(steps, np.int64), np.array(rows, np.int64)
+
+
+# ------------------------------------------------------------ element groups ---
+# Element-wise output (core/output/element-wise): ElementOpSolid::record (ElementOpSolid.cpp:48-80)
+# takes the element's Fourier coefficients at the chosen GLL points to the output frame,
+# ElementOp::recordToElem (ElementOp.hpp:26-68) lays them out as real rows (Fourier: row 0 the
+# real part of order 0, rows 2 alpha - 1 and 2 alpha the real and imaginary parts of order
+# alpha, cut at na = nr; azimuths: the series summed at each phi, 2 exp(i alpha phi) for
+# alpha > 0), and ElementOp::dumpToIO (ElementOp.hpp:70-176) forms the channels on those rows.
+
+
+def _rotate_complex(f, theta, cartesian):
+    """(s, phi, z) -> RTZ of complex coefficients f [point, order, D] (theta per point):
+    CoordTransformSpherical::transformSPZ_RTZ3 / 9 / 6 applied to real and imaginary parts;
+    identity in a Cartesian mesh (CoordTransformCartesian)."""
+    if cartesian:
+        return f
+    zero = np.zeros(len(theta))
+    re = rotate_field(f.real, "RTZ", theta, zero, zero, False)
+    im = rotate_field(f.imag, "RTZ", theta, zero, zero, False)
+    return re + 1j * im
+
+
+def element_fields(u, g, need, frame, theta, cartesian):
+    """Fields of one set of elements in the output frame from the complex coefficients of the
+    displacement u [point, order, 3] and gradient g [point, order, 9] (either may be None):
+    SolidElement::getDisplField / getNablaField / getStrainField / getCurlField
+    (SolidElement.cpp:396-546, the branch without particle relabelling)."""
+    rtz = frame == "RTZ"
+    out = {}
+    if "U" in need:
+        out["U"] = _rotate_complex(u, theta, cartesian) if rtz else u
+    if "G" in need:
+        out["G"] = _rotate_complex(g, theta, cartesian) if rtz else g
+    if "E" in need:
+        e = strain_from_gradient(g)
+        if rtz and not cartesian:
+            e = e.copy()
+            e[..., 3:] *= .5
+            e = _rotate_complex(e, theta, cartesian)
+            e[..., 3:] *= 2.
+        out["E"] = e
+    if "R" in need:
+        r = curl_from_gradient(g)
+        out["R"] = _rotate_complex(r, theta, cartesian) if rtz else r
+    return out
+
+
+def fourier_rows(c, na, phis):
+    """ElementOp::recordToElem: complex coefficients c [..., order, D] -> real rows
+    [..., na, D] (Fourier layout when phis is empty, else the series at each azimuth)."""
+    nu = c.shape[-2]
+    if len(phis) == 0:
+        rows = np.empty(c.shape[:-2] + (2 * nu - 1, c.shape[-1]))
+        rows[..., 0, :] = c[..., 0, :].real
+        rows[..., 1::2, :] = c[..., 1:, :].real
+        rows[..., 2::2, :] = c[..., 1:, :].imag
+        return rows[..., :na, :]
+    al = np.arange(nu)
+    z = np.where(al == 0, 1.0, 2.0)[None, :] * np.exp(1j * np.outer(np.asarray(phis), al))   # [phi, order]
+    return np.real(np.einsum("pa,...ad->...pd", z, c))
+
+
+def element_channels(rows, channels):
+    """ElementOp::dumpToIO on rows {field: [..., na, D]} -> [..., na, channel]. As in the
+    reference's element output, G_I1 adds the first three gradient components and E_J2 takes
+    I1^2 / 3 - (E11 E22 + E22 E33 + E33 E11) + (E23 E31 + E31 E12 + E12 E23)."""
+    cols = []
+    for ch in channels:
+        x = rows[ch[0]]
+        if ch in ("U_NORM", "R_NORM"):
+            cols.append(np.sqrt(np.sum(x * x, axis=-1)))
+        elif ch in ("G_I1", "E_I1"):
+            cols.append(x[..., 0] + x[..., 1] + x[..., 2])
+        elif ch == "E_J2":
+            i1 = x[..., 0] + x[..., 1] + x[..., 2]
+            cols.append(i1 * i1 / 3. - (x[..., 0] * x[..., 1] + x[..., 1] * x[..., 2] + x[..., 2] * x[..., 0]) +
+                        (x[..., 3] * x[..., 4] + x[..., 4] * x[..., 5] + x[..., 5] * x[..., 3]))
+        elif ch[0] == "G":
+            cols.append(x[..., (int(ch[1]) - 1) * 3 + int(ch[2]) - 1])
+        elif ch[0] == "E":
+            cols.append(x[..., {"11": 0, "22": 1, "33": 2, "23": 3, "31": 4, "12": 5}[ch[1:]]])
+        else:
+            cols.append(x[..., int(ch[1]) - 1])
+    return np.stack(cols, axis=-1)
+
+
+class ElementGroupWriter:
+    """ElementIO_NetCDF (core/output/element-wise/io/ElementIO_NetCDF.cpp:14-249): the file
+    <output>/elements/<group>/axisem3d_synthetics.nc.rank0 with data_time [dim_time], one
+    data_wave__NaG=<nag> [dim_element__NaG=<nag>, dim_na__NaG=<nag>, dim_GLL, dim_channel,
+    dim_time] per na-grid value, list_channel, list_element__NaG=<nag> (element tags),
+    list_na_grid, list_element_na [dim_element, 5] and list_element_coords [dim_element,
+    dim_GLL, 2]. No file when the group has no element. Rows at and above an element's na in
+    its na-grid block are zero."""
+
+    def __init__(self, out_dir, group, wave_dtype):
+        from .ncwrite import NC3File
+        self.group = group
+        self.line = 0
+        self.nc = None
+        ne = len(group.elems)
+        if ne == 0:
+            return
+        gdir = os.path.join(out_dir, "elements", group.name)
+        os.makedirs(gdir, exist_ok=True)
+        nc = NC3File(os.path.join(gdir, "axisem3d_synthetics.nc.rank0"))
+        nt, npnts, nch = group.nrec, group.npnts, len(group.channels)
+        nc.add("data_time", [("dim_time", nt)], np.float64)
+        self.members = []
+        for nag in group.na_grid:
+            sel = np.nonzero(group.elem_na[:, 2] == nag)[0]
+            self.members.append(sel)
+            s = "%d" % nag
+            nc.add("data_wave__NaG=" + s, [("dim_element__NaG=" + s, len(sel)), ("dim_na__NaG=" + s, int(nag)),
+                                            ("dim_GLL", npnts), ("dim_channel", nch), ("dim_time", nt)], wave_dtype)
+        lc = max(len(c) for c in group.channels)
+        nc.add("list_channel", [("dim_channel", nch), ("dim_channel_str_length", lc)], "S1")
+        for nag, sel in zip(group.na_grid, self.members):
+            s = "%d" % nag
+            nc.add("list_element__NaG=" + s, [("dim_element__NaG=" + s, len(sel))], np.int32)
+        nc.add("list_na_grid", [("dim_na_grid", len(group.na_grid))], np.int32)
+        nc.add("list_element_na", [("dim_element", ne), ("dim_5", 5)], np.int32)
+        nc.add("list_element_coords", [("dim_element", ne), ("dim_GLL", npnts), ("dim_2", 2)], np.float64)
+        nc.create()
+        nc.var("list_channel")[:] = np.array([list(c.ljust(lc, "\0")) for c in group.channels], "S1")
+        for nag, sel in zip(group.na_grid, self.members):
+            nc.var("list_element__NaG=%d" % nag)[:] = group.tags[sel]
+        nc.var("list_na_grid")[:] = group.na_grid
+        nc.var("list_element_na")[:] = group.elem_na
+        nc.var("list_element_coords")[:] = group.coords
+        nc.flush()
+        self.nc = nc
+
+    def write(self, times, data):
+        """times [b]; data: per element [na, npnts, channel, b] (a list in group order)."""
+        b = len(times)
+        if self.nc is None or b == 0:
+            return
+        g = self.group
+        t0 = self.line
+        self.nc.var("data_time")[t0:t0 + b] = times
+        for nag, sel in zip(g.na_grid, self.members):
+            blk = np.zeros((len(sel), int(nag), g.npnts, len(g.channels), b))
+            for i, k in enumerate(sel):
+                na = int(g.na[k])
+                blk[i, :na] = data[k]
+            self.nc.var("data_wave__NaG=%d" % nag)[..., t0:t0 + b] = blk
+        self.line += b
+        if g.flush:
+            self.nc.flush()
+
+    def close(self):
+        if self.nc is not None:
+            self.nc.close()
+            self.nc = None

@@ -448,6 +448,7 @@ class Simulation:
     mesh: ExodusMesh
     cartesian: bool
     info: dict
+    element_groups: List["ElementGroup"] = field(default_factory=list)
 
 
 def _read_stf(gm, root, name, dt):
@@ -1223,6 +1224,8 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     skipped = [] if skip_unsupported_channels else None
     groups = _release_stations(inp, m, ctx, geo, dt, m.t0, m.t0 + (nstep - 1) * dt, nstep, enr, solid_q,
                                skipped)
+    egroups = _release_elements(inp, quads, coords, gll, ctx, geo, dt, m.t0, m.t0 + (nstep - 1) * dt, nstep,
+                                enr, mesh.global_variables["dist_tolerance"])
     m.meta = {"workload": "exodus %s (%d solid + %d fluid quads, %s)" %
               (mesh.summary()["file"], ns, nf, mesh.records.get("model", "")),
               "dt_mesh": dt_mesh}
@@ -1233,7 +1236,7 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
             "stability_interval": inp.advanced.get("verbose:stability_interval", int)
             if inp.advanced.contains("verbose:stability_interval") else 0}
     return Simulation(model=m, nsteps=nstep, t0=m.t0, dt=dt, groups=groups, mesh=mesh,
-                      cartesian=geo.cartesian, info=info)
+                      cartesian=geo.cartesian, info=info, element_groups=egroups)
 
 
 def _mass_layout(mass1d, mass3d):
@@ -1657,6 +1660,180 @@ def _release_stations(inp, m, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, s
     interval = int(np.gcd.reduce(intervals)) if intervals else 1
     interval = max(1, min(interval, nsteps))
     _set_stations(m, st_e, st_w, st_phi, interval)
+    return groups
+
+
+# ---------------------------------------------------------- element groups ---
+# vicinity::constants::gEdgeIPnt (preloop/spectral/vicinity.hpp): GLL points along each edge
+EDGE_IPNT = ((0, 5, 10, 15, 20), (20, 21, 22, 23, 24), (24, 19, 14, 9, 4), (4, 3, 2, 1, 0))
+
+
+@dataclass
+class ElementGroup:
+    """One element group (ElementOutput::buildInparam, preloop/output/ElementOutput.cpp:27-143,
+    and ElementOutput::release :276-400, ElementOpGroup::initialize, core/output/element-wise/
+    element/ElementOpGroup.hpp:66-150)."""
+    name: str
+    channels: List[str]
+    frame: str                      # spz or RTZ
+    interval: int
+    tmin: float                     # the window already widened by dt / 2
+    tmax: float
+    buffer_size: int
+    flush: bool
+    npnts: int                      # GLL points per element
+    phis: np.ndarray                # azimuths (phi_list, then lat_lon_list); empty = Fourier
+    tags: np.ndarray                # mesh quad index of each element
+    elems: np.ndarray               # solid-element index in the model
+    ipnts: np.ndarray               # [element, npnts] GLL point (ipol * 5 + jpol)
+    coords: np.ndarray              # [element, npnts, 2] (s, z) of the points
+    theta: np.ndarray               # [element, npnts] polar angle of the points (RTZ)
+    nr: np.ndarray                  # nr of each element
+    na: np.ndarray                  # element nr (Fourier) or the number of azimuths
+    na_grid: np.ndarray
+    elem_na: np.ndarray             # [element, 5]: tag, na, na-grid value, index in it, global index
+    nrec: int = 0
+
+
+def _na_grid(na, na_space):
+    """ElementOpGroup::initialize (ElementOpGroup.hpp:96-118): from the largest na down, keep
+    an na only when it is at least na_space below the last kept one."""
+    srt = sorted(set(int(x) for x in na))
+    grid = []
+    if srt:
+        grid.append(srt[-1])
+        for v in srt[-2::-1]:
+            if v <= grid[-1] - na_space:
+                grid.append(v)
+    return np.array(sorted(set(grid)), np.int64)
+
+
+def _release_elements(inp, quads, coords, gll, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, dist_tol):
+    """ElementOutput::release (ElementOutput.cpp:276-480) for solid groups; fluid groups and
+    stress channels raise."""
+    gm = inp.output
+    key = "list_of_element_groups"
+    if not gm.contains(key) or not gm._walk(key):
+        return []
+    groups, names = [], set()
+    nq = len(quads.fluid)
+    centers = quads.nodal_xy.mean(axis=1)                          # [quad, (s, z)]
+    if geo.cartesian:
+        cR, cZ = centers[:, 0], centers[:, 1]
+    else:
+        r, t = sz2rtheta(centers[:, 0], centers[:, 1])
+        cR, cZ = t, r
+    for gi in range(gm.get(key + ":[?]", int)):
+        name = gm.get(key + ":{%d}" % gi)
+        root = key + ":[%d]:%s" % (gi, name)
+        re_ = root + ":elements"
+        minR, maxR = gm.get(re_ + ":horizontal_range:[0]", float), gm.get(re_ + ":horizontal_range:[1]", float)
+        minZ, maxZ = gm.get(re_ + ":vertical_range:[0]", float), gm.get(re_ + ":vertical_range:[1]", float)
+        ri = root + ":inplane"
+        edge_dim = gm.get_options(ri + ":edge_dimension", {"HORIZONTAL": 0, "VERTICAL": 1, "BOTH": -1})
+        edge_pos = gm.get(ri + ":edge_position", float) if edge_dim >= 0 else 0.
+        if gm.get(ri + ":GLL_points_one_edge") == "FULL":
+            ipols = list(range(5))
+        else:
+            ipols = sorted(set(int(x) for x in gm.get_vector(ri + ":GLL_points_one_edge")))
+        if not ipols:
+            raise PreloopError("ElementOutput::buildInparam || elements:GLL_points_one_edge cannot be empty.")
+        if ipols[0] < 0 or ipols[-1] > 4:
+            raise PreloopError("ElementOutput::buildInparam || elements:GLL_points_one_edge must be "
+                               "ranged between 0 and 4.")
+        ra = root + ":azimuthal"
+        phis = [gm.get_bounded(ra + ":phi_list:[%d]" % k, 0., 2. * math.pi)
+                for k in range(gm.get(ra + ":phi_list:[?]", int))]
+        lats, lons = [], []
+        for k in range(gm.get(ra + ":lat_lon_list:[?]", int)):
+            lats.append(gm.get_bounded(ra + ":lat_lon_list:[%d]:[0]" % k, -90., 90.))
+            lons.append(gm.get_bounded(ra + ":lat_lon_list:[%d]:[1]" % k, -180., 180.))
+        na_space = gm.get_bounded(ra + ":na_space", 1, None, int)
+        rw = root + ":wavefields"
+        frame = gm.get_options(rw + ":coordinate_frame", {"spz": "spz", "RTZ": "RTZ"})
+        fluid = gm.get_options(rw + ":medium", {"SOLID": False, "FLUID": True})
+        if fluid:
+            raise PreloopError("ElementOutput::release || Fluid element groups are not supported by "
+                               "this build. || Element group name: " + name)
+        chans = standard_channels(gm.get_vector(rw + ":channels"))
+        rt = root + ":temporal"
+        sp = gm.get(rt + ":sampling_period")
+        period = dt if sp == "DT" else dt * int(sp[3:]) if sp.startswith("DTx") else float(sp)
+        tmin, tmax = tmin_simu, tmax_simu
+        if gm.get(rt + ":time_window") != "FULL":
+            tmin = max(tmin_simu, gm.get(rt + ":time_window:[0]", float))
+            tmax = min(tmax_simu, gm.get(rt + ":time_window:[1]", float))
+        rf = root + ":file_options"
+        bsize = gm.get_bounded(rf + ":buffer_size", 1, None, int)
+        flush = gm.get(rf + ":flush", bool)
+        if name in names:
+            raise PreloopError("ElementOutput::release || Element group name must be unique. || "
+                               "Duplicated element group name: " + name)
+        names.add(name)
+        # elements by the (R, Z) of their centers (theta and r in a spherical mesh)
+        sel = [q for q in range(nq) if minR < cR[q] < maxR and minZ < cZ[q] < maxZ and
+               bool(quads.fluid[q]) == fluid]
+        use, ipnts = [], []
+        if edge_dim < 0:
+            uni = [i * 5 + j for i in ipols for j in ipols]
+            use = sel
+            ipnts = [uni] * len(sel)
+        else:
+            for q in sel:
+                sz = quads.nodal_xy[q].T                                  # [2, 4]
+                if geo.cartesian:
+                    RZ = sz
+                else:
+                    r4, t4 = sz2rtheta(sz[0], sz[1])
+                    RZ = np.stack([t4, r4])
+                if edge_dim == 0 and not geo.cartesian:
+                    rmean = RZ[1].mean()
+                    x = RZ[0] * rmean
+                    xmin, xmax = edge_pos * rmean - dist_tol, edge_pos * rmean + dist_tol
+                else:
+                    x = RZ[edge_dim]
+                    xmin, xmax = edge_pos - dist_tol, edge_pos + dist_tol
+                for ie in range(4):
+                    je = 0 if ie == 3 else ie + 1
+                    if xmin < x[ie] < xmax and xmin < x[je] < xmax:
+                        use.append(q)
+                        ipnts.append([EDGE_IPNT[ie][i] for i in ipols])
+                        break
+        # azimuths: phi_list, then the lat_lon_list at the surface
+        if lats:
+            llr = np.stack([lats, lons, np.full(len(lats), geo.outer_radius)], axis=1)
+            phis = phis + list(geo.llr2spz(llr, True)[:, 1])
+        intv = int(period / dt)
+        intv = 1 if intv == 0 else intv
+        if intv < 0:
+            intv = np.iinfo(np.int32).max
+        nrec = sum(1 for t in range(0, nsteps, intv)
+                   if tmin - dt / 2. <= tmin_simu + t * dt <= tmax + dt / 2.)
+        if nrec == 0:
+            raise PreloopError("ElementOutput::release || No time step to record in the given time "
+                               "window. ||Element group name: " + name)
+        npnts = len(ipols) ** 2 if edge_dim < 0 else len(ipols)
+        use = np.array(use, np.int64)
+        ip = np.array(ipnts, np.int64).reshape(len(use), npnts)
+        tags = use.astype(np.int64)
+        elems = ctx.solid_index[use].astype(np.int64) if len(use) else np.zeros(0, np.int64)
+        pts = gll[use[:, None], ip] if len(use) else np.zeros((0, npnts), np.int64)
+        crd = coords[pts] if len(use) else np.zeros((0, npnts, 2))
+        theta = sz2rtheta(crd[..., 0], crd[..., 1])[1] if len(use) else np.zeros((0, npnts))
+        nr = enr[use].astype(np.int64) if len(use) else np.zeros(0, np.int64)
+        na = nr.copy() if not phis else np.full(len(use), len(phis), np.int64)
+        grid = _na_grid(na, na_space)
+        info = np.zeros((len(use), 5), np.int64)
+        count = np.zeros(len(grid), np.int64)
+        for k in range(len(use)):
+            gidx = int(np.searchsorted(grid, na[k]))
+            info[k] = (tags[k], na[k], grid[gidx], count[gidx], count[gidx])
+            count[gidx] += 1
+        groups.append(ElementGroup(name=name, channels=chans, frame=frame, interval=intv, tmin=tmin - dt / 2.,
+                                   tmax=tmax + dt / 2., buffer_size=bsize, flush=flush, npnts=npnts,
+                                   phis=np.array(phis, np.float64), tags=tags, elems=elems, ipnts=ip,
+                                   coords=crd, theta=theta, nr=nr, na=na, na_grid=grid, elem_na=info,
+                                   nrec=nrec))
     return groups
 
 

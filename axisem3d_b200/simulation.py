@@ -26,6 +26,112 @@ class Result:
     traces: dict = field(default_factory=dict)     # group -> (times, [station, channel, time])
     seconds_preloop: float = 0.0
     seconds_loop: float = 0.0
+    seconds_element_output: float = 0.0
+    element_files: dict = field(default_factory=dict)   # element group -> file (None: no element)
+    element_data: dict = field(default_factory=dict)    # element group -> [(times, per element)]
+
+
+class ElementRecorder:
+    """The element groups of one run (ElementOpGroup::record / dumpToFile, core/output/
+    element-wise/element/ElementOpGroup.hpp:197-236): the engine keeps the Fourier
+    coefficients of every group's points in a device ring (axg_set_element_record, one
+    interval for all groups, the gcd of theirs); after each chunk of steps that fills the ring
+    at most once, the host takes the chunk's records, keeps each group's own steps and time
+    window, forms its channels and writes them to the group's file."""
+
+    RING_BYTES = 256 << 20
+
+    def __init__(self, solver, sim, out_dir, wave_dtype):
+        self.s, self.sim = solver, sim
+        self.groups = [g for g in sim.element_groups]
+        nr = np.asarray(sim.model.se_nr, np.int64)
+        elem, gll, kind = [], [], []
+        self.layout = []            # per group: {kind: [element, point] entry numbers}
+        for g in self.groups:
+            need = {c[0] for c in g.channels}
+            d = {}
+            for kd, on in ((0, "U" in need), (1, bool(need & set("GER")))):
+                if not on or len(g.elems) == 0:
+                    continue
+                idx = np.arange(len(elem), len(elem) + len(g.elems) * g.npnts).reshape(len(g.elems), g.npnts)
+                elem += np.repeat(g.elems, g.npnts).tolist()
+                gll += g.ipnts.ravel().tolist()
+                kind += [kd] * (len(g.elems) * g.npnts)
+                d[kd] = idx
+            self.layout.append(d)
+        elem, kind = np.array(elem, np.int64), np.array(kind, np.int64)
+        width = (nr[elem] // 2 + 1) * np.where(kind == 1, 9, 3) if len(elem) else np.zeros(0, np.int64)
+        self.off = np.concatenate([[0], np.cumsum(width)[:-1]]).astype(np.int64) if len(elem) else width
+        words = int(width.sum())
+        self.interval = int(np.gcd.reduce([g.interval for g in self.groups])) if self.groups else 1
+        self.interval = max(1, min(self.interval, sim.nsteps))
+        total = (sim.nsteps + self.interval - 1) // self.interval
+        per = max(1, words) * max(1, int(sim.model.nwave)) * (16 if solver.precision == "fp64" else 8)
+        self.ring = int(max(1, min(total, self.RING_BYTES // per)))
+        self.active = len(elem) > 0
+        if self.active:
+            w = solver.set_element_record(elem, gll, kind, self.interval, self.ring)
+            assert w == words
+        self.chunk_steps = self.ring * self.interval
+        self.next_rec = 0
+        self.writers = [output.ElementGroupWriter(out_dir, g, wave_dtype) if out_dir is not None else None
+                        for g in self.groups]
+        self.data = [[] for _ in self.groups]      # kept when no output directory is given
+
+    def _coeffs(self, recs, g, idx, D):
+        """[element][record, point, order, D] complex coefficients of one kind."""
+        out = []
+        for k, e in enumerate(g.elems):
+            nu = int(g.nr[k]) // 2 + 1
+            cols = self.off[idx[k]][:, None] + np.arange(nu * D)[None, :]       # [point, nu * D]
+            out.append(recs[:, cols].reshape(len(recs), g.npnts, nu, D))
+        return out
+
+    def drain(self, step):
+        """Take the records of steps below `step` that are not taken yet."""
+        if not self.active:
+            return
+        last = (step - 1) // self.interval
+        if last < self.next_rec:
+            return
+        recs = self.s.element_records(self.next_rec, last - self.next_rec + 1)
+        if recs.ndim == 3:
+            recs = recs[:, 0]
+        rec_ids = np.arange(self.next_rec, last + 1)
+        self.next_rec = last + 1
+        sim = self.sim
+        for gi, g in enumerate(self.groups):
+            if len(g.elems) == 0:
+                continue
+            steps = rec_ids * self.interval
+            t = sim.t0 + steps * sim.dt
+            keep = (steps % g.interval == 0) & (t >= g.tmin) & (t <= g.tmax)
+            if not keep.any():
+                continue
+            r = recs[keep]
+            need = {c[0] for c in g.channels}
+            lay = self.layout[gi]
+            us = self._coeffs(r, g, lay[0], 3) if 0 in lay else None
+            gs = self._coeffs(r, g, lay[1], 9) if 1 in lay else None
+            per_elem = []
+            for k in range(len(g.elems)):
+                th = np.broadcast_to(g.theta[k], (len(r), g.npnts)).reshape(-1)
+                u = us[k].reshape(-1, *us[k].shape[2:]) if us is not None else None
+                gg = gs[k].reshape(-1, *gs[k].shape[2:]) if gs is not None else None
+                f = output.element_fields(u, gg, need, g.frame, th, sim.cartesian)
+                rows = {key: output.fourier_rows(v, int(g.na[k]), g.phis).reshape(len(r), g.npnts, -1, v.shape[-1])
+                        for key, v in f.items()}
+                ch = output.element_channels(rows, g.channels)                  # [rec, point, na, channel]
+                per_elem.append(np.transpose(ch, (2, 1, 3, 0)))                 # [na, point, channel, rec]
+            if self.writers[gi] is not None:
+                self.writers[gi].write(t[keep], per_elem)
+            else:
+                self.data[gi].append((t[keep], per_elem))
+
+    def close(self):
+        for w in self.writers:
+            if w is not None:
+                w.close()
 
 
 def write_scanning(path, model, solid_nr, fluid_nr):
@@ -60,17 +166,36 @@ def run(input_dir: str, output_dir: Optional[str] = None, precision: str = "fp32
     res = Result(sim=sim, seconds_preloop=time.perf_counter() - t)
     if stability_interval is None:
         stability_interval = sim.info["stability_interval"]
+    wave_precision = 16 if precision == "fp64" else 8
     with Solver(sim.model, precision, device=device, stability_interval=stability_interval) as s:
+        rec = None
+        if sim.element_groups:
+            rec = ElementRecorder(s, sim, output_dir, np.float64 if precision == "fp64" else np.float32)
         t = time.perf_counter()
-        s.run(sim.nsteps)
-        s.synchronize()
-        res.seconds_loop = time.perf_counter() - t
+        if rec is None or not rec.active:
+            s.run(sim.nsteps)
+            s.synchronize()
+        else:
+            done = 0
+            while done < sim.nsteps:
+                n = min(rec.chunk_steps, sim.nsteps - done)
+                s.run(n)
+                done += n
+                t1 = time.perf_counter()
+                rec.drain(done)
+                res.seconds_element_output += time.perf_counter() - t1
+        res.seconds_loop = time.perf_counter() - t - res.seconds_element_output
+        if rec is not None:
+            rec.close()
+            for g, w in zip(rec.groups, rec.writers):
+                res.element_files[g.name] = (os.path.join(output_dir, "elements", g.name, "axisem3d_synthetics.nc.rank0")
+                                             if w is not None and len(g.elems) else None)
+            res.element_data = {g.name: d for g, d in zip(rec.groups, rec.data)}
         seis = s.seismograms() if len(sim.model.st_elem) else np.zeros((0, 0, 3))
         scan = s.scanning_nr() if sim.model.scanning else None
         grad = s.station_gradients() if sim.model.st_gradient and len(sim.model.st_elem) else None
     if scan is not None and output_dir is not None and sim.info.get("scanning_file"):
         write_scanning(os.path.join(output_dir, sim.info["scanning_file"]), sim.model, *scan)
-    wave_precision = 16 if precision == "fp64" else 8
     for g in sim.groups:
         steps, rows = output.group_records(g, sim.nsteps, sim.t0, sim.dt, sim.model.st_interval)
         sl = slice(g.first, g.first + len(g.keys))

@@ -234,6 +234,33 @@ class Solver:
             self._check(self.lib.axg_get_station_gradients(self.h, out.ctypes.data_as(L.P_f64), C.byref(n)))
         return out[:, 0] if nw == 1 else out
 
+    def set_element_record(self, elem, gll, kind, interval, ring):
+        """Record, every `interval` steps into a device ring of `ring` records, the Fourier
+        coefficients (orders < nr/2 + 1 of the element) of the displacement (kind 0) or its
+        gradient (kind 1) at GLL point gll[i] of solid element elem[i]."""
+        e = np.ascontiguousarray(elem, np.int32)
+        g = np.ascontiguousarray(gll, np.int32)
+        k = np.ascontiguousarray(kind, np.int32)
+        if not (len(e) == len(g) == len(k)):
+            raise ValueError("elem, gll and kind differ in length")
+        self._check(self.lib.axg_set_element_record(self.h, len(e), e.ctypes.data_as(L.P_i32),
+                                                    g.ctypes.data_as(L.P_i32), k.ctypes.data_as(L.P_i32),
+                                                    int(interval), int(ring)))
+        w = C.c_int64()
+        self._check(self.lib.axg_element_record_words(self.h, C.byref(w)))
+        self._er_words = int(w.value)
+        return self._er_words
+
+    def element_records(self, rec_first, nrec):
+        """Records rec_first .. rec_first + nrec - 1 as complex [nrec, nwave, words]
+        (without the wavefield axis for one wavefield)."""
+        nw = max(1, int(self.model.nwave))
+        out = np.zeros((int(nrec), nw, self._er_words, 2))
+        self._check(self.lib.axg_get_element_records(self.h, int(rec_first), int(nrec),
+                                                     out.ctypes.data_as(L.P_f64)))
+        c = out[..., 0] + 1j * out[..., 1]
+        return c[:, 0] if nw == 1 else c
+
     # -------------------------------------------------------- differentiation ---
     def forward_checkpointed(self, nsteps, interval=100):
         """nsteps forward steps keeping a device checkpoint every `interval` steps."""

@@ -395,6 +395,22 @@ int  axg_get_seismograms(axg_solver *h, double *host_out, int32_t *nrecords);
 /* station gradients recorded so far: [nrecords][nwave][nstations][9] doubles (after
    axg_set_station_gradient(h, 1)) */
 int  axg_get_station_gradients(axg_solver *h, double *host_out, int32_t *nrecords);
+/* Element-wise output (ElementOpGroup::record, core/output/element-wise/element/ElementOpGroup.hpp:
+   197-215, and ElementOpSolid::record, ElementOpSolid.cpp:48-80, before the RTZ transform and the
+   channels, which the host forms): after axg_finalize, entry i names GLL point gll[i] (ipol * 5 +
+   jpol) of solid element elem[i] and a kind, 0 = the displacement (3 components), 1 = its gradient
+   computeGrad9 (9 components, g[c * 3 + d] = d_d u_c, d = s, phi, z). At every step that is a
+   multiple of `interval` the Fourier coefficients of orders 0 .. nr/2 of the element are kept in
+   a device ring of `ring` records (record r = step / interval in slot r % ring), so a caller
+   that reads them back at least every ring records (buffer_size) never loses one. One record
+   per wavefield holds axg_element_record_words complex words: the entries in order, each as
+   [order][component]. A new call replaces the previous entries. */
+int  axg_set_element_record(axg_solver *h, int32_t n, const int32_t *elem, const int32_t *gll,
+                            const int32_t *kind, int32_t interval, int32_t ring);
+int  axg_element_record_words(const axg_solver *h, int64_t *words);
+/* records rec_first .. rec_first + nrec - 1, which must all be in the ring, into host_out as
+   [nrec][nwave][words][re, im] doubles */
+int  axg_get_element_records(axg_solver *h, int32_t rec_first, int32_t nrec, double *host_out);
 int  axg_synchronize(axg_solver *h);
 
 /* ---- diagnostics ---- */

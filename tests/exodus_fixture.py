@@ -346,3 +346,43 @@ def add_3d_models(d, entries):
         txt = f.read()
     with open(p, "w") as f:
         f.write(txt.replace("list_of_3D_models: []", "list_of_3D_models:\n" + "".join(entries)))
+
+
+ELEMENT_GROUP_YAML = """    - {name}:
+        elements:
+            horizontal_range: [{hmin!r}, {hmax!r}]
+            vertical_range: [{vmin!r}, {vmax!r}]
+        inplane:
+            edge_dimension: {edge_dim}
+            edge_position: {edge_pos!r}
+            GLL_points_one_edge: {gll}
+        azimuthal:
+            phi_list: [{phis}]
+            lat_lon_list: [{latlon}]
+            na_space: {na_space}
+        wavefields:
+            coordinate_frame: {frame}
+            medium: SOLID
+            channels: [{channels}]
+        temporal:
+            sampling_period: {period}
+            time_window: {window}
+        file_options:
+            buffer_size: {buffer}
+            flush: true
+"""
+
+
+def add_element_groups(d, groups):
+    """Replace list_of_element_groups in d/inparam.output.yaml; groups: dicts with the keys of
+    ELEMENT_GROUP_YAML (defaults: whole mesh, BOTH, FULL, Fourier, spz, [U], DT, FULL)."""
+    base = dict(hmin=-1e30, hmax=1e30, vmin=-1e30, vmax=1e30, edge_dim="BOTH", edge_pos=0.0, gll="FULL",
+                phis="", latlon="", na_space=1, frame="spz", channels="U", period="DT", window="FULL",
+                buffer=100)
+    txt = "list_of_element_groups:\n" + "".join(ELEMENT_GROUP_YAML.format(**dict(base, **g)) for g in groups)
+    p = os.path.join(d, "inparam.output.yaml")
+    with open(p) as f:
+        cur = f.read()
+    i = cur.index("list_of_element_groups:")
+    with open(p, "w") as f:
+        f.write(cur[:i] + txt)

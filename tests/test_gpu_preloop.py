@@ -106,41 +106,50 @@ def test_simulation_max_steps(built, tmp_path):
     assert len(t) == 17 and w.shape[-1] == 17
 
 
-def _grad9_at_stations(m, field):
-    """computeGrad9 (GradientQuadrature.hpp:177-202, L'Hopital rows :421-459) of the field at
-    the points of each station's element, interpolated like the displacement
-    (Station::interpolate): [station, 9]. Also returns the interpolated displacement."""
+def _element_displ_grad(m, field, e):
+    """The displacement U [order, 3, 5, 5] of solid element e (orders < nr/2 + 1 of the
+    element, collectDisplFromPoints) and its computeGrad9 (GradientQuadrature.hpp:177-202,
+    L'Hopital rows :421-459) g [order, 9, 5, 5], g[c * 3 + d] = d_d u_c, from the point field."""
     from axisem3d_b200.solver import spectral_tables
     t = spectral_tables()
     gll, glj = t["gGLL"].reshape(5, 5), t["gGLJ"].reshape(5, 5)      # [k, i] = l_k'(x_i)
     nu_p = np.asarray(m.sp_nr) // 2 + 1
     off = np.concatenate([[0], np.cumsum(nu_p)[:-1]])
     f = field.reshape(-1, 3)
+    nu = int(m.se_nr[e]) // 2 + 1
+    pts = m.se_pts[e]
+    U = np.zeros((nu, 3, 5, 5), np.complex128)
+    for q in range(25):
+        p = pts[q]
+        n = min(nu, nu_p[p])
+        U[:n, :, q // 5, q % 5] = f[off[p]:off[p] + n]
+    gx = glj if m.se_axial[e] else gll
+    X = np.einsum("ki,ackj->acij", gx, U)
+    Y = np.einsum("kj,acik->acij", gll, U)
+    sx, se, zx, ze, inv_s = (m.se_geom[e, k].reshape(5, 5) for k in range(5))
+    al = np.arange(nu)[:, None, None]
+    A = np.stack([1j * al * U[:, 0] - U[:, 1], 1j * al * U[:, 1] + U[:, 0], 1j * al * U[:, 2]], axis=1)
+    g = np.zeros((nu, 9, 5, 5), np.complex128)
+    for c in range(3):
+        g[:, c * 3 + 0] = X[:, c] * ze + Y[:, c] * zx
+        g[:, c * 3 + 2] = X[:, c] * se + Y[:, c] * sx
+        g[:, c * 3 + 1] = A[:, c] * inv_s
+    if m.se_axial[e]:
+        ax = np.einsum("k,ackj->acj", gx[:, 0], A)
+        ay = np.einsum("kj,ack->acj", gll, A[:, :, 0, :])
+        for c in range(3):
+            g[:, c * 3 + 1, 0, :] += ax[:, c] * ze[0] + ay[:, c] * zx[0]
+    return U, g
+
+
+def _grad9_at_stations(m, field):
+    """computeGrad9 of the field at the points of each station's element, interpolated like
+    the displacement (Station::interpolate): [station, 9]. Also returns the interpolated
+    displacement."""
     out_g, out_u = [], []
     for s, e in enumerate(m.st_elem):
-        nu = int(m.se_nr[e]) // 2 + 1
-        pts = m.se_pts[e]
-        U = np.zeros((nu, 3, 5, 5), np.complex128)
-        for q in range(25):
-            p = pts[q]
-            n = min(nu, nu_p[p])
-            U[:n, :, q // 5, q % 5] = f[off[p]:off[p] + n]
-        gx = glj if m.se_axial[e] else gll
-        X = np.einsum("ki,ackj->acij", gx, U)
-        Y = np.einsum("kj,acik->acij", gll, U)
-        sx, se, zx, ze, inv_s = (m.se_geom[e, k].reshape(5, 5) for k in range(5))
-        al = np.arange(nu)[:, None, None]
-        A = np.stack([1j * al * U[:, 0] - U[:, 1], 1j * al * U[:, 1] + U[:, 0], 1j * al * U[:, 2]], axis=1)
-        g = np.zeros((nu, 9, 5, 5), np.complex128)
-        for c in range(3):
-            g[:, c * 3 + 0] = X[:, c] * ze + Y[:, c] * zx
-            g[:, c * 3 + 2] = X[:, c] * se + Y[:, c] * sx
-            g[:, c * 3 + 1] = A[:, c] * inv_s
-        if m.se_axial[e]:
-            ax = np.einsum("k,ackj->acj", gx[:, 0], A)
-            ay = np.einsum("kj,ack->acj", gll, A[:, :, 0, :])
-            for c in range(3):
-                g[:, c * 3 + 1, 0, :] += ax[:, c] * ze[0] + ay[:, c] * zx[0]
+        U, g = _element_displ_grad(m, field, e)
+        nu = U.shape[0]
         w = m.st_w[s].reshape(5, 5)
         z = np.where(np.arange(nu) == 0, 1.0, 2.0) * np.exp(1j * np.arange(nu) * m.st_phi[s])
         out_g.append(np.real(np.einsum("a,akij,ij->k", z, g, w)))
