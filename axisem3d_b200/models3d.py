@@ -21,6 +21,7 @@ import math
 import numpy as np
 
 EPS = np.finfo(np.float64).eps
+DEPS = 1e-12                  # numerical::dEpsilon, the reference's tolerance for 1-D / zero tests
 
 
 class Model3DError(RuntimeError):
@@ -132,8 +133,170 @@ class StructuredGrid:
         return out, ok, dim_out
 
 
+# ------------------------------------------------ sg_tools and Model3D helpers ---
+def _horizontal(gm, rc, name, cartesian):
+    """sg_tools::inparamHorizontal: (source_centered, xy, ellipticity)."""
+    h = gm.get(rc + ":horizontal")
+    if h == "DISTANCE_AZIMUTH":
+        return True, False, False
+    if h == "XY_CARTESIAN":
+        if not cartesian:
+            raise Model3DError("sg_tools::inparamHorizontal || XY_CARTESIAN is incompatible with a "
+                               "spherical mesh.")
+        return True, True, False
+    if h == "LATITUDE_LONGITUDE":
+        return False, False, gm.get(rc + ":ellipticity", bool)
+    raise Model3DError("sg_tools::inparamHorizontal || Parameter coordinates:horizontal must be "
+                       "DISTANCE_AZIMUTH, || XY_CARTESIAN or LATITUDE_LONGITUDE. || Model name: " + name)
+
+
+def _vertical(gm, rc, name):
+    """sg_tools::inparamVertical: (use_depth, depth_below_solid_surface)."""
+    v = gm.get(rc + ":vertical")
+    if v == "DEPTH":
+        return True, gm.get(rc + ":depth_below_solid_surface", bool)
+    if v == "RADIUS":
+        return False, False
+    raise Model3DError("sg_tools::inparamVertical || Parameter coordinates:vertical must be either "
+                       "RADIUS or DEPTH. || Model name: " + name)
+
+
+def _var_rank(gm, rc, name, n):
+    """sg_tools::inparamVarRank<n>: coordinate variable names and the data rank."""
+    vars_ = gm.get_vector(rc + ":nc_variables")
+    rank = gm.get_vector(rc + ":data_rank", int)
+    if len(vars_) != n or len(rank) != n:
+        raise Model3DError("sg_tools::inparamVarRank || The size of coordinates:nc_variables and "
+                           "coordinates:data_rank must be %d. || Model name: %s" % (n, name))
+    return vars_, rank
+
+
+def _units(gm, rc, xy):
+    """sg_tools::inparamUnits: (length unit, angle unit)."""
+    lu = gm.get(rc + ":length_unit")
+    length = {"m": 1., "km": 1e3}[lu] if lu in ("m", "km") else gm.get(rc + ":length_unit", float)
+    angle = 1.0
+    if not xy:
+        angle = gm.get_options(rc + ":angle_unit", {"degree": math.pi / 180., "radian": 1.})
+    return length, angle
+
+
+def _construct_units(g, source_centered, xy, vertical, length, angle, cartesian):
+    """sg_tools::constructUnits on the grid coordinates g (in place): horizontal axes to
+    metres / radians (source-centred) or degrees (geographic), the vertical axis to metres."""
+    if source_centered:
+        if cartesian:
+            g[0] *= length
+            g[1] *= (length if xy else angle)
+        else:
+            g[0] *= angle
+            g[1] *= angle
+    else:
+        g[0] *= angle / (math.pi / 180.)
+        g[1] *= angle / (math.pi / 180.)
+    if vertical:
+        g[2] *= length
+
+
+def _lon360(g, name):
+    """sg_tools::constructLon360: longitudes in [0, 360] rather than [-180, 180]."""
+    lon = g[1]
+    if lon[0] < 0. - DEPS and lon[-1] > 180. + DEPS:
+        raise Model3DError("sg_tools::constructLon360 || Longitude range must be either "
+                           "[-180, 180] or [0, 360]. || Model name = " + name)
+    return bool(lon[-1] > 180. + DEPS)
+
+
+def inplane_scope(sz, geo, check_r, rmin, rmax, check_z, zmin, zmax, use_depth, depth_solid):
+    """Model3D::inplaneScope (models3D/Model3D.hpp:69-109) on (s, z) rows: the quad may touch
+    the model's horizontal (theta or s) and vertical (r / z or depth) ranges."""
+    if not check_r and not check_z:
+        return True
+    sz = np.atleast_2d(sz)
+    if geo.cartesian:
+        a, b = sz[:, 0], sz[:, 1]
+    else:
+        r = np.hypot(sz[:, 0], sz[:, 1])
+        t = np.where(r < DEPS, 0., np.arccos(np.clip(sz[:, 1] / np.maximum(r, DEPS), -1., 1.)))
+        a, b = t, r
+    if check_r and (a.max() < rmin or a.min() > rmax):
+        return False
+    if check_z:
+        if use_depth:
+            R = geo.outer_solid_radius if depth_solid else geo.outer_radius
+            b = R - b
+        if b.max() < zmin or b.min() > zmax:
+            return False
+    return True
+
+
+def to_model(spz, geo, source_centered, xy, ellipticity, lon360, use_depth, depth_solid, name):
+    """Model3D::coordsFromMeshToModel (Model3D.hpp:111-175): mesh (s, phi, z) rows to the
+    model's coordinates (theta, phi, r), (x, y, z), (s, phi, z) or (lat, lon, r), with depth
+    for r when the model uses depth."""
+    spz = np.atleast_2d(spz)
+    if source_centered:
+        if geo.cartesian:
+            crd = spz.copy()
+            if xy:
+                crd[:, 0] = spz[:, 0] * np.cos(spz[:, 1])
+                crd[:, 1] = spz[:, 0] * np.sin(spz[:, 1])
+        else:
+            r = np.hypot(spz[:, 0], spz[:, 2])
+            t = np.where(r < DEPS, 0., np.arccos(np.clip(spz[:, 2] / np.maximum(r, DEPS), -1., 1.)))
+            crd = np.stack([t, spz[:, 1], r], axis=1)
+    else:
+        if geo.cartesian:
+            if np.any(spz[:, 2] < spz[:, 0] * 10.):
+                raise Model3DError("Model3D::coordsFromMeshToModel || Invalid geographic location in "
+                                   "Cartesian mesh. || Model name = " + name)
+            t = spz[:, 0] / spz[:, 2]
+            bend = np.stack([spz[:, 2] * np.sin(t), spz[:, 1], spz[:, 2] * np.cos(t)], axis=1)
+            crd = geo.spz2llr(bend, ellipticity, lon360)
+        else:
+            crd = geo.spz2llr(spz, ellipticity, lon360)
+    if use_depth:
+        R = geo.outer_solid_radius if depth_solid else geo.outer_radius
+        crd = crd.copy()
+        crd[:, 2] = R - crd[:, 2]
+    return crd
+
+
+def element_spz(point_sz, point_nr, und=None, cartesian=True):
+    """Model3D::computeElemSPZ (Model3D.cpp:16-66): the (s, phi, z) of every (point, slice)
+    of a quad, slices at phi = 2 pi k / nr of each point; with `und` (per-point undulation,
+    1 or nr values) the points move by it along z (Cartesian) or along r (spherical)."""
+    rows = []
+    for p in range(25):
+        nr = int(point_nr[p])
+        phi = np.linspace(0., 2. * np.pi / nr * (nr - 1), nr) if nr > 1 else np.zeros(1)
+        s0, z0 = point_sz[0, p], point_sz[1, p]
+        s, z = np.full(nr, s0), np.full(nr, z0)
+        if und is not None:
+            u = np.broadcast_to(np.asarray(und[p], np.float64), (nr,))
+            if cartesian:
+                z = z + u
+            else:
+                r = math.hypot(s0, z0)
+                th = 0. if r < DEPS else math.acos(z0 / r)
+                s = s + u * math.sin(th)
+                z = z + u * math.cos(th)
+        rows.append(np.stack([s, phi, z], axis=1))
+    return np.concatenate(rows, axis=0)
+
+
+def _split(vals, point_nr, npts=25):
+    out, r0 = [], 0
+    for p in range(npts):
+        nr = int(point_nr[p])
+        out.append(vals[r0:r0 + nr])
+        r0 += nr
+    return out
+
+
 class StructuredGridV3D:
     """One `list_of_3D_models` entry of class StructuredGridV3D."""
+    kind = "volumetric"
 
     REF_KINDS = ("ABS", "REF1D", "REF3D", "REF_PERTURB")
     PROPERTIES = ("RHO", "VP", "VS", "VPV", "VPH", "VSV", "VSH", "ETA", "QMU", "QKAPPA")
@@ -141,41 +304,12 @@ class StructuredGridV3D:
     def __init__(self, name, gm, root, inp_path, cartesian):
         self.name = name
         rc = root + ":coordinates"
-        h = gm.get(rc + ":horizontal")
-        if h == "DISTANCE_AZIMUTH":
-            self.source_centered, self.xy, self.ellipticity = True, False, False
-        elif h == "XY_CARTESIAN":
-            if not cartesian:
-                raise Model3DError("sg_tools::inparamHorizontal || XY_CARTESIAN is incompatible with a "
-                                   "spherical mesh.")
-            self.source_centered, self.xy, self.ellipticity = True, True, False
-        elif h == "LATITUDE_LONGITUDE":
-            self.source_centered, self.xy = False, False
-            self.ellipticity = gm.get(rc + ":ellipticity", bool)
-        else:
-            raise Model3DError("sg_tools::inparamHorizontal || Parameter coordinates:horizontal must be "
-                               "DISTANCE_AZIMUTH, || XY_CARTESIAN or LATITUDE_LONGITUDE. || Model name: "
-                               + name)
-        v = gm.get(rc + ":vertical")
-        if v == "DEPTH":
-            self.use_depth = True
-            self.depth_solid = gm.get(rc + ":depth_below_solid_surface", bool)
-        elif v == "RADIUS":
-            self.use_depth, self.depth_solid = False, False
-        else:
-            raise Model3DError("sg_tools::inparamVertical || Parameter coordinates:vertical must be either "
-                               "RADIUS or DEPTH. || Model name: " + name)
-        vars_ = gm.get_vector(rc + ":nc_variables")
-        rank = gm.get_vector(rc + ":data_rank", int)
-        if len(vars_) != 3 or len(rank) != 3:
-            raise Model3DError("sg_tools::inparamVarRank || The size of coordinates:nc_variables and "
-                               "coordinates:data_rank must be 3. || Model name: " + name)
-        lu = gm.get(rc + ":length_unit")
-        length = {"m": 1., "km": 1e3}[lu] if lu in ("m", "km") else gm.get(rc + ":length_unit", float)
-        angle = 1.0
-        if not self.xy:
-            angle = gm.get_options(rc + ":angle_unit", {"degree": math.pi / 180., "radian": 1.})
+        self.source_centered, self.xy, self.ellipticity = _horizontal(gm, rc, name, cartesian)
+        self.use_depth, self.depth_solid = _vertical(gm, rc, name)
+        vars_, rank = _var_rank(gm, rc, name, 3)
+        length, angle = _units(gm, rc, self.xy)
         undulated = gm.get(rc + ":undulated_geometry", bool)
+        self.undulated = undulated
         if undulated and self.use_depth:
             raise Model3DError("StructuredGridV3D::StructuredGridV3D || Cannot use depth as vertical "
                                "coordinate in undulated geometry. || Model name = " + name)
@@ -195,87 +329,28 @@ class StructuredGridV3D:
             self.props.append((key, gm.get(rpi + ":nc_var"), gm.get(rpi + ":factor", float), ref))
         fname = gm.get(root + ":nc_data_file")
         self.grid = StructuredGrid(inp_path(fname), vars_, [(p[1], p[2]) for p in self.props], rank)
-        # sg_tools::constructUnits
-        g = self.grid.coords
-        if self.source_centered:
-            if cartesian:
-                g[0] *= length
-                g[1] *= (length if self.xy else angle)
-            else:
-                g[0] *= angle
-                g[1] *= angle
-        else:
-            g[0] *= angle / (math.pi / 180.)
-            g[1] *= angle / (math.pi / 180.)
-        g[2] *= length
-        self.lon360 = False
-        if not self.source_centered:
-            lon = g[1]
-            if lon[0] < 0. - EPS and lon[-1] > 180. + EPS:
-                raise Model3DError("sg_tools::constructLon360 || Longitude range must be either "
-                                   "[-180, 180] or [0, 360]. || Model name = " + name)
-            self.lon360 = bool(lon[-1] > 180. + EPS)
+        _construct_units(self.grid.coords, self.source_centered, self.xy, True, length, angle, cartesian)
+        self.lon360 = False if self.source_centered else _lon360(self.grid.coords, name)
 
-    # Model3D::inplaneScope on (s, z) columns
     def _inplane_scope(self, sz, geo):
-        check_r = self.source_centered and not self.xy
         g = self.grid.coords
-        if geo.cartesian:
-            a, b = sz[:, 0], sz[:, 1]
-        else:
-            r = np.hypot(sz[:, 0], sz[:, 1])
-            t = np.where(r < EPS, 0., np.arccos(np.clip(sz[:, 1] / np.maximum(r, EPS), -1., 1.)))
-            a, b = t, r
-        if check_r and (a.max() < g[0][0] or a.min() > g[0][-1]):
-            return False
-        if self.use_depth:
-            R = geo.outer_solid_radius if self.depth_solid else geo.outer_radius
-            b = R - b
-        if b.max() < g[2][0] or b.min() > g[2][-1]:
-            return False
-        return True
+        return inplane_scope(sz, geo, self.source_centered and not self.xy, g[0][0], g[0][-1], True, g[2][0],
+                             g[2][-1], self.use_depth, self.depth_solid)
 
-    # Model3D::coordsFromMeshToModel
     def _to_model(self, spz, geo):
-        if self.source_centered:
-            if geo.cartesian:
-                crd = spz.copy()
-                if self.xy:
-                    crd[:, 0] = spz[:, 0] * np.cos(spz[:, 1])
-                    crd[:, 1] = spz[:, 0] * np.sin(spz[:, 1])
-            else:
-                r = np.hypot(spz[:, 0], spz[:, 2])
-                t = np.where(r < EPS, 0., np.arccos(np.clip(spz[:, 2] / np.maximum(r, EPS), -1., 1.)))
-                crd = np.stack([t, spz[:, 1], r], axis=1)
-        else:
-            if geo.cartesian:
-                if np.any(spz[:, 2] < spz[:, 0] * 10.):
-                    raise Model3DError("Model3D::coordsFromMeshToModel || Invalid geographic location in "
-                                       "Cartesian mesh. || Model name = " + self.name)
-                t = spz[:, 0] / spz[:, 2]
-                bend = np.stack([spz[:, 2] * np.sin(t), spz[:, 1], spz[:, 2] * np.cos(t)], axis=1)
-                crd = geo.spz2llr(bend, self.ellipticity, self.lon360)
-            else:
-                crd = geo.spz2llr(spz, self.ellipticity, self.lon360)
-        if self.use_depth:
-            R = geo.outer_solid_radius if self.depth_solid else geo.outer_radius
-            crd = crd.copy()
-            crd[:, 2] = R - crd[:, 2]
-        return crd
+        return to_model(spz, geo, self.source_centered, self.xy, self.ellipticity, self.lon360, self.use_depth,
+                        self.depth_solid, self.name)
 
-    def properties(self, nodal_sz, point_sz, point_nr, geo):
+    def properties(self, nodal_sz, point_sz, point_nr, geo, und=None):
         """StructuredGridV3D::getProperties for one quad: (in_scope [25][nr_p] bool,
-        values [25][nr_p][nprop]) per point, or None when the quad is out of the model."""
+        values [25][nr_p][nprop]) per point, or None when the quad is out of the model.
+        `und`: the quad's undulation per point, used when the model asks for the
+        undulated geometry."""
         if self.center and not self._inplane_scope(nodal_sz.mean(axis=0)[None, :], geo):
             return None
         if not self._inplane_scope(nodal_sz, geo):
             return None
-        rows = []
-        for p in range(25):
-            nr = int(point_nr[p])
-            phi = np.linspace(0., 2. * np.pi / nr * (nr - 1), nr) if nr > 1 else np.zeros(1)
-            rows.append(np.stack([np.full(nr, point_sz[0, p]), phi, np.full(nr, point_sz[1, p])], axis=1))
-        spz = np.concatenate(rows, axis=0)
+        spz = element_spz(point_sz, point_nr, und if self.undulated else None, geo.cartesian)
         crd = self._to_model(spz, geo)
         vals, ok, dim_out = self.grid.compute(crd)
         if self.center:
@@ -297,6 +372,118 @@ class StructuredGridV3D:
         return out_ok, out_v
 
 
+class StructuredGridG3D:
+    """A geometric 3-D model (models3D/geometric/StructuredGridG3D.cpp): an undulation
+    map on a 2-D grid applied between two radii (or depths) min < interface < max, ramped
+    linearly from 0 at min and max to the map's value at the interface."""
+    kind = "geometric"
+
+    def __init__(self, name, gm, root, inp_path, cartesian):
+        self.name = name
+        rc = root + ":coordinates"
+        self.source_centered, self.xy, self.ellipticity = _horizontal(gm, rc, name, cartesian)
+        self.use_depth, self.depth_solid = _vertical(gm, rc, name)
+        vars_, rank = _var_rank(gm, rc, name, 2)
+        length, angle = _units(gm, rc, self.xy)
+        rr = root + ":undulation_range"
+        interface = gm.get(rr + ":interface", float)
+        lo, hi = gm.get(rr + ":min_max:[0]", float), gm.get(rr + ":min_max:[1]", float)
+        if interface >= hi or interface <= lo:
+            raise Model3DError("Geometric3D::buildInparam || undulation_range:interface must lie within "
+                               "undulation_range:min_max. || Model name: %s || Class name: StructuredGridG3D"
+                               % name)
+        self.interface, self.min, self.max = interface * length, lo * length, hi * length
+        ru = root + ":undulation_data"
+        self.grid = StructuredGrid(inp_path(gm.get(root + ":nc_data_file")), vars_,
+                                   [(gm.get(ru + ":nc_var"), gm.get(ru + ":factor", float))], rank)
+        _construct_units(self.grid.coords, self.source_centered, self.xy, False, length, angle, cartesian)
+        self.lon360 = False if self.source_centered else _lon360(self.grid.coords, name)
+
+    def at(self, spz, geo):
+        """StructuredGridG3D::getUndulation on (s, phi, z) rows: (undulation, any in scope)."""
+        crd = to_model(spz, geo, self.source_centered, self.xy, self.ellipticity, self.lon360, self.use_depth,
+                       self.depth_solid, self.name)
+        und = np.zeros(len(crd))
+        rd = crd[:, 2]
+        vals, ok, _ = self.grid.compute(crd[:, :2])
+        inr = (rd >= self.min) & (rd <= self.max) & ok
+        v = vals[:, 0]
+        below = rd < self.interface
+        ramp = np.where(below, v / (self.interface - self.min) * (rd - self.min),
+                        v / (self.max - self.interface) * (self.max - rd))
+        und[inr] = ramp[inr]
+        return und, bool(inr.any())
+
+    def undulation(self, nodal_sz, point_sz, point_nr, geo):
+        """Per-point undulation of one quad, or None when it is out of the model."""
+        g = self.grid.coords
+        if not inplane_scope(nodal_sz, geo, self.source_centered and not self.xy, g[0][0], g[0][-1], True,
+                             self.min, self.max, self.use_depth, self.depth_solid):
+            return None
+        und, any_in = self.at(element_spz(point_sz, point_nr), geo)
+        return _split(und, point_nr) if any_in else None
+
+
+class Ellipticity:
+    """The Ellipticity geometric model (models3D/geometric/Ellipticity.cpp): every point
+    moves from its radius r to the ellipsoid of flattening f(r) through it, a b / sqrt((a
+    cos t)^2 + (b sin t)^2) - r with b = (1 - f)^(2/3) r and a = b / (1 - f), t the
+    geographic colatitude; nothing on a Cartesian mesh or with zero flattening."""
+    kind = "geometric"
+
+    def __init__(self, name):
+        self.name = name
+
+    def at(self, spz, geo):
+        if geo.cartesian or geo.outer_flattening < DEPS:
+            return np.zeros(len(np.atleast_2d(spz))), False
+        llr = to_model(spz, geo, False, False, False, False, False, False, self.name)
+        tpr = geo.llr2tpr(llr, False)
+        r, t = tpr[:, 2], tpr[:, 0]
+        f = geo.flattening(r)
+        b = (1. - f) ** (2. / 3.) * r
+        a = b / (1. - f)
+        tmp = (a * np.cos(t)) ** 2 + (b * np.sin(t)) ** 2
+        return a * b / np.maximum(np.sqrt(tmp), DEPS) - r, True
+
+    def undulation(self, nodal_sz, point_sz, point_nr, geo):
+        und, any_in = self.at(element_spz(point_sz, point_nr), geo)
+        return _split(und, point_nr) if any_in else None
+
+
+class StructuredGridO3D:
+    """An ocean-load 3-D model (models3D/ocean_load/StructuredGridO3D.cpp): sum(rho * depth)
+    of the water column on a 2-D grid, taken where it is positive."""
+    kind = "ocean"
+
+    def __init__(self, name, gm, root, inp_path, cartesian):
+        self.name = name
+        rc = root + ":coordinates"
+        self.source_centered, self.xy, self.ellipticity = _horizontal(gm, rc, name, cartesian)
+        vars_, rank = _var_rank(gm, rc, name, 2)
+        length, angle = _units(gm, rc, self.xy)
+        rd = root + ":data_sum_rho_depth"
+        self.grid = StructuredGrid(inp_path(gm.get(root + ":nc_data_file")), vars_,
+                                   [(gm.get(rd + ":nc_var"), gm.get(rd + ":factor", float))], rank)
+        _construct_units(self.grid.coords, self.source_centered, self.xy, False, length, angle, cartesian)
+        self.lon360 = False if self.source_centered else _lon360(self.grid.coords, name)
+
+    def sum_rho_depth(self, nodal_sz, edge_spz, edge_nr, geo):
+        """StructuredGridO3D::getSumRhoDepth on the 5 surface-edge points of one quad (rows
+        of (s, phi, z), 1 per slice): per-point arrays, or None when out of the model."""
+        g = self.grid.coords
+        if not inplane_scope(nodal_sz, geo, self.source_centered and not self.xy, g[0][0], g[0][-1], False,
+                             0., 0., False, False):
+            return None
+        crd = to_model(edge_spz, geo, self.source_centered, self.xy, self.ellipticity, self.lon360, False, False,
+                       self.name)
+        vals, ok, _ = self.grid.compute(crd[:, :2])
+        v = np.where(ok & (vals[:, 0] > 0.), vals[:, 0], 0.)
+        if not np.any(ok & (vals[:, 0] > 0.)):
+            return None
+        return _split(v, edge_nr, 5)
+
+
 def build_models(inp, cartesian):
     """Model3D::buildInparam: the activated entries of list_of_3D_models, in order."""
     gm = inp.model
@@ -309,10 +496,20 @@ def build_models(inp, cartesian):
         if not gm.get(root + ":activated", bool):
             continue
         cls = gm.get(root + ":class_name")
-        if cls != "StructuredGridV3D":
+        if cls == "StructuredGridV3D":
+            models.append(StructuredGridV3D(name, gm, root, inp.path, cartesian))
+        elif cls == "StructuredGridG3D":
+            models.append(StructuredGridG3D(name, gm, root, inp.path, cartesian))
+        elif cls == "Ellipticity":
+            if any(isinstance(m, Ellipticity) for m in models):
+                raise Model3DError("Geometric3D::buildInparam || Ellipticity model cannot be added more "
+                                   "than once.")
+            models.append(Ellipticity(name))
+        elif cls == "StructuredGridO3D":
+            models.append(StructuredGridO3D(name, gm, root, inp.path, cartesian))
+        else:
             raise Model3DError("Model3D::buildInparam || 3-D model class %s is not supported by this "
-                               "build (StructuredGridV3D only). || Model name: %s" % (cls, name))
-        models.append(StructuredGridV3D(name, gm, root, inp.path, cartesian))
+                               "build. || Model name: %s" % (cls, name))
     return models
 
 
@@ -336,7 +533,7 @@ def try_reduce_1d(arrs):
     """PhysicalProperty::tryReduceTo1D on the 25 per-point arrays: 1-D if every point is
     constant in phi (relative to its norm)."""
     for a in arrs:
-        if np.linalg.norm(a - a[0]) > np.linalg.norm(a) * EPS:
+        if np.linalg.norm(a - a[0]) > np.linalg.norm(a) * DEPS:
             return False
     return True
 

@@ -31,10 +31,11 @@ from .inparam import Inparam
 from .meshgen import (cg4_correct, geometry_batch, iso_with_attenuation, lagrange, round_dt, tables,
                       tiso_with_attenuation, weights_cg4)
 from .model import STF, Model
-from .models3d import Model3DError, build_models
+from .models3d import Model3DError, build_models, lin_interp_phi
 from .solver import att_alpha_beta_gamma, quad_dt
 
 EPS = np.finfo(np.float64).eps
+DEPS = 1e-12                  # numerical::dEpsilon, the reference's tolerance for 1-D / zero tests
 # vicinity::constants (mesh/topology/vicinity.hpp), nPol = 4
 NODE_IPNT = (0, 20, 24, 4)
 EDGE_IPNT = ((0, 5, 10, 15, 20), (20, 21, 22, 23, 24), (24, 19, 14, 9, 4), (4, 3, 2, 1, 0))
@@ -97,7 +98,7 @@ class Geodesy:
             f = self.FLATTENING[fl] if fl in self.FLATTENING else float(fl)
         except ValueError:
             raise PreloopError("geodesy::setup || Invalid %s: %s" % (key, fl))
-        if f < EPS or self.cartesian:
+        if f < DEPS or self.cartesian:
             f = 0.
         self.outer_flattening = f
         self.ellip_r = mesh.ellipticity[0].copy()
@@ -173,7 +174,7 @@ class Geodesy:
     def _xy2sphi(x, y, undefined):
         s = np.hypot(x, y)
         with np.errstate(invalid="ignore"):
-            p = np.where((np.abs(x) < EPS) & (np.abs(y) < EPS), undefined, np.arctan2(y, x))
+            p = np.where((np.abs(x) < DEPS) & (np.abs(y) < DEPS), undefined, np.arctan2(y, x))
         return s, p
 
     def llr2spz(self, llr, ellipticity):
@@ -195,7 +196,7 @@ class Geodesy:
         s, p = self._xy2sphi(geo[:, 0], geo[:, 1], err)
         p = np.where(p < err * .9, spz[:, 1], p)
         r = np.hypot(s, geo[:, 2])
-        t = np.where(r < EPS, 0., np.arccos(np.clip(geo[:, 2] / np.maximum(r, EPS), -1., 1.)))
+        t = np.where(r < DEPS, 0., np.arccos(np.clip(geo[:, 2] / np.maximum(r, DEPS), -1., 1.)))
         llr = self.tpr2llr(np.stack([t, p, r], axis=1), ellipticity)
         llr[:, 2] = np.hypot(spz[:, 0], spz[:, 2])
         if lon360:
@@ -223,7 +224,7 @@ def sz2rtheta(s, z):
     """geodesy::sz2rtheta: r and the polar angle acos(z / r) (0 at r = 0)."""
     r = np.hypot(s, z)
     with np.errstate(invalid="ignore", divide="ignore"):
-        t = np.where(r < EPS, 0., np.arccos(np.clip(z / np.maximum(r, EPS), -1., 1.)))
+        t = np.where(r < DEPS, 0., np.arccos(np.clip(z / np.maximum(r, DEPS), -1., 1.)))
     return r, t
 
 
@@ -526,9 +527,9 @@ class _Quads:
             v0, v1 = vals[i0], vals[i1]
             nodal[name] = ((v1 - v0) / (r1 - r0))[:, None] * (r - r0[:, None]) + v0[:, None]
         vs_key = "VS" if "VS" in nodal else "VSV"
-        fluid_mat = np.max(nodal[vs_key], axis=1) < EPS
+        fluid_mat = np.max(nodal[vs_key], axis=1) < DEPS
         if "VSH" in nodal:
-            fluid_mat |= np.max(nodal["VSH"], axis=1) < EPS
+            fluid_mat |= np.max(nodal["VSH"], axis=1) < DEPS
         if np.any(fluid_mat != self.fluid):
             q = int(np.nonzero(fluid_mat != self.fluid)[0][0])
             raise PreloopError("Material::getMass || Incompatible solid/fluid flags. || Element %d" % q)
@@ -536,9 +537,9 @@ class _Quads:
         iso_e = np.ones(len(center), bool)
         if tiso:
             nrm = lambda v: np.sqrt(np.sum(v * v, axis=1))     # noqa: E731
-            iso_e = ((nrm(nodal["VPV"] - nodal["VPH"]) < nrm(nodal["VPV"]) * EPS) &
-                     (nrm(nodal["VSV"] - nodal["VSH"]) < nrm(nodal["VSV"]) * EPS) &
-                     (nrm(nodal["ETA"] - 1.) < 2. * EPS))
+            iso_e = ((nrm(nodal["VPV"] - nodal["VPH"]) < nrm(nodal["VPV"]) * DEPS) &
+                     (nrm(nodal["VSV"] - nodal["VSH"]) < nrm(nodal["VSV"]) * DEPS) &
+                     (nrm(nodal["ETA"] - 1.) < 2. * DEPS))
         self.iso = iso_e
         self.tiso = tiso
         self.node_vals = nodal                       # the 4 nodal values of every property
@@ -602,6 +603,14 @@ class _Quads:
         pw = [self.pointwise(q, k) for k in keys]
         out = [voigt(*np.broadcast_arrays(*(x[p] for x in pw))) for p in range(25)]
         return rho, [o[0] for o in out], [o[1] for o in out]
+
+    def vmax_slices(self, q):
+        """Material::getMaxVelocity: the largest velocity of each slice of a 3-D quad."""
+        nr_e = int(self.pnr[q].max())
+        if self.fluid[q] or self.iso[q]:
+            return np.max(self.elemental(q, "VP", nr_e), axis=1)
+        return np.maximum(np.max(self.elemental(q, "VPV", nr_e), axis=1),
+                          np.max(self.elemental(q, "VPH", nr_e), axis=1))
 
     def vmax_3d(self, q):
         """Material::getMaxVelocity over all slices of a quad with 3-D properties."""
@@ -670,10 +679,12 @@ class _Quads:
         self.node_vals["ETA"][q] = 1.
         self.iso[q] = False
 
-    def apply_model(self, md, geo):
-        """Volumetric3D::applyTo + Material::addProperty3D for every quad in the model's scope."""
+    def apply_model(self, md, geo, und=None):
+        """Volumetric3D::applyTo + Material::addProperty3D for every quad in the model's scope
+        (on the undulated geometry when the model asks for it)."""
         for q in range(len(self.axial)):
-            res = md.properties(self.nodal_xy[q], self.sz[q], self.pnr[q], geo)
+            uq = und.pointwise(q) if und is not None and q in und.und else None
+            res = md.properties(self.nodal_xy[q], self.sz[q], self.pnr[q], geo, uq)
             if res is None:
                 continue
             ok, vals = res
@@ -720,8 +731,8 @@ class _Quads:
             b = lambda x, y: np.broadcast_arrays(x, y)        # noqa: E731
             vpv, vph = b(g["VPV"], g["VPH"])
             vsv, vsh = b(g["VSV"], g["VSH"])
-            if (n(vpv - vph) < n(vpv) * EPS and n(vsv - vsh) < n(vsv) * EPS and
-                    n(g["ETA"] - 1.) < n(g["ETA"]) * EPS):
+            if (n(vpv - vph) < n(vpv) * DEPS and n(vsv - vsh) < n(vsv) * DEPS and
+                    n(g["ETA"] - 1.) < n(g["ETA"]) * DEPS):
                 self.iso[q] = True
                 self.prop["VP"][q] = self.prop["VPV"][q]
                 self.prop["VS"][q] = self.prop["VSV"][q]
@@ -761,6 +772,212 @@ class _Quads:
                 n = n * s
             out[ip] = n
         return list(pts), out
+
+
+# ------------------------------------------------------------- undulation ---
+class _Undulation:
+    """Undulation (preloop/se_model/quad/physical/Undulation.cpp) of the quads that geometric
+    3-D models touch: the radial (spherical) or vertical (Cartesian) displacement dZ of each
+    (point, slice), its gradient in (R, T, Z), and what follows from it: the particle
+    relabelling transformation, the Jacobian on the mass, 3-D normals and the slice-wise
+    coordinates for dt."""
+
+    def __init__(self, quads, cartesian):
+        self.q = quads
+        self.cartesian = cartesian
+        self.und = {}            # quad -> 25 arrays (1 value, or nr_p values on phi slices)
+        self._rtz = {}
+
+    def add(self, q, arrs):
+        """PhysicalProperty::addGLL: add per point (1-D + per-slice broadcast), then
+        tryReduceTo1D."""
+        from .models3d import try_reduce_1d
+        cur = self.und.get(q)
+        out = []
+        for p in range(25):
+            a = np.asarray(arrs[p], dtype=np.float64)
+            if cur is not None:
+                c = cur[p]
+                n = max(len(a), len(c))
+                a = np.broadcast_to(c, (n,)) + np.broadcast_to(a, (n,))
+            out.append(np.array(a, dtype=np.float64))
+        if try_reduce_1d(out):
+            out = [a[:1].copy() for a in out]
+        self.und[q] = out
+        self._rtz.pop(q, None)
+
+    def pointwise(self, q):
+        return self.und[q]
+
+    def elemental(self, q):
+        """PhysicalProperty::getElemental: [max nr of the arrays, 25] by linInterpPhi."""
+        from .models3d import lin_interp_phi
+        a = self.und[q]
+        nr = max(len(x) for x in a)
+        return np.stack([lin_interp_phi(x, nr) for x in a], axis=1)
+
+    def is3d(self, q):
+        return q in self.und and max(len(x) for x in self.und[q]) > 1
+
+    def rtz(self, q):
+        """Undulation::finished3D: [nr, 3, 25] = (dZ/dR, dZ/dT, dZ/dZ) on the element's
+        slices: the gradient (computeGrad3) of dZ's Fourier series, back on the slices and,
+        on a spherical mesh, from (s, z) to (R, Z) with each point's theta."""
+        if q in self._rtz:
+            return self._rtz[q]
+        from .solver import spectral_tables
+        t = spectral_tables()
+        gll, glj = t["gGLL"].reshape(5, 5), t["gGLJ"].reshape(5, 5)      # [k, i] = l_k'(x_i)
+        dz = self.elemental(q)                                           # [nr, 25]
+        nr = len(dz)
+        c = np.fft.rfft(dz, axis=0) / nr                                 # [nu, 25]
+        nu = c.shape[0]
+        P = c.reshape(nu, 5, 5)
+        ax = bool(self.q.axial[q])
+        gx = glj if ax else gll
+        X = np.einsum("ki,akj->aij", gx, P)
+        Y = np.einsum("kj,aik->aij", gll, P)
+        sx, se, zx, ze = (self.q.geom[q, k].reshape(5, 5) for k in range(4))
+        inv_s = self.q.geom[q, 4].reshape(5, 5)
+        al = np.arange(nu)[:, None, None]
+        A = 1j * al * P
+        g = np.zeros((nu, 3, 5, 5), np.complex128)
+        g[:, 0] = X * ze + Y * zx
+        g[:, 2] = X * se + Y * sx
+        g[:, 1] = A * inv_s
+        if ax:
+            axv = np.einsum("k,akj->aj", gx[:, 0], A)
+            ayv = np.einsum("kj,ak->aj", gll, A[:, 0, :])
+            g[:, 1, 0, :] = axv * ze[0] + ayv * zx[0]
+        d = np.fft.irfft(g.reshape(nu, 3, 25) * nr, n=nr, axis=0) if nr > 1 else g.reshape(1, 3, 25).real.copy()
+        if not self.cartesian:
+            th = sz2rtheta(self.q.sz[q, 0], self.q.sz[q, 1])[1]
+            ct, st = np.cos(th), np.sin(th)
+            ds, dzz = d[:, 0].copy(), d[:, 2].copy()
+            d[:, 0] = ds * ct - dzz * st
+            d[:, 2] = dzz * ct + ds * st
+        self._rtz[q] = d
+        return d
+
+    def _j0(self, q, p, dz, j3):
+        if self.cartesian:
+            return np.ones_like(j3)
+        Z = math.hypot(self.q.sz[q, 0, p], self.q.sz[q, 1, p])
+        return 1. + dz / Z if Z > DEPS else j3
+
+    def mass_jacobian(self, q):
+        """Undulation::getMassJacobian: J0^2 J3 per point (1 or nr_p values)."""
+        from .models3d import lin_interp_phi
+        d = self.rtz(q)
+        out = []
+        for p in range(25):
+            dz = self.und[q][p]
+            j3 = 1. + lin_interp_phi(d[:, 2, p], len(dz))
+            j0 = self._j0(q, p, dz, j3)
+            J = j0 ** 2 * j3
+            if J.min() < DEPS:
+                raise PreloopError("Undulation::getMassJacobian || Negative Jacobian or distorted element "
+                                   "occurred.")
+            out.append(J)
+        return out
+
+    def prt(self, q):
+        """Undulation::createPRT: [5, nr, 25] = X0 = 1/J0, X1 = -J1/(J0 J3), X2 = -J2/(J0 J3),
+        X3 = 1/J3 and |J| = J0^2 J3 on the element's slices."""
+        d = self.rtz(q)
+        dz = self.elemental(q)
+        j1, j2, j3 = d[:, 0], d[:, 1], 1. + d[:, 2]
+        if self.cartesian:
+            j0 = np.ones_like(j3)
+        else:
+            Z = np.broadcast_to(np.hypot(self.q.sz[q, 0], self.q.sz[q, 1]), j3.shape)
+            j0 = np.where(Z > DEPS, 1. + dz / np.where(Z > DEPS, Z, 1.), j3)
+        xj = j0 ** 2 * j3
+        if xj.min() < DEPS:
+            raise PreloopError("Undulation::createPRT || Negative Jacobian or distorted element occurred.")
+        return np.stack([1. / j0, -j1 / (j0 * j3), -j2 / (j0 * j3), 1. / j3, xj])
+
+    def normal3d(self, q, n1d, p):
+        """Undulation::computeNormal3D: the (s, phi, z) normal [nr_p, 3] of an edge point."""
+        from .models3d import lin_interp_phi
+        if q not in self.und:
+            return np.array([[n1d[0], 0., n1d[1]]])
+        d = self.rtz(q)
+        dz = self.und[q][p]
+        n = len(dz)
+        j1, j2 = lin_interp_phi(d[:, 0, p], n), lin_interp_phi(d[:, 1, p], n)
+        j3 = 1. + lin_interp_phi(d[:, 2, p], n)
+        j0 = self._j0(q, p, dz, j3)
+        k0, k1, k2, k3 = j3 * j0, -j1 * j0, -j2 * j0, j0 * j0
+        nR, nZ = n1d[0], n1d[1]
+        if not self.cartesian:
+            th = float(sz2rtheta(self.q.sz[q, 0, p], self.q.sz[q, 1, p])[1])
+            st, ct = math.sin(th), math.cos(th)
+            nR, nZ = n1d[0] * ct - n1d[1] * st, n1d[1] * ct + n1d[0] * st
+        out = np.stack([k1 * nZ + k0 * nR, k2 * nZ, k3 * nZ], axis=1)
+        if not self.cartesian:
+            r = out.copy()
+            out[:, 0] = r[:, 0] * ct + r[:, 2] * st
+            out[:, 2] = r[:, 2] * ct - r[:, 0] * st
+        return out
+
+    def slices_sz(self, q):
+        """Quad::computeDt: the point coordinates on each slice of dZ."""
+        dz = self.elemental(q)
+        out = []
+        for k in range(len(dz)):
+            sz = self.q.sz[q].copy()
+            if self.cartesian:
+                sz[1] += dz[k]
+            else:
+                th = sz2rtheta(self.q.sz[q, 0], self.q.sz[q, 1])[1]
+                sz[0] += dz[k] * np.sin(th)
+                sz[1] += dz[k] * np.cos(th)
+            out.append(sz)
+        return out
+
+    def total(self, models, spz, geo):
+        """SE_Model::getTotalUndulation at one (s, phi, z)."""
+        return float(sum(md.at(np.asarray(spz, np.float64)[None, :], geo)[0][0] for md in models))
+
+    def to_reference(self, models, spz, geo, tol):
+        """SE_Model::undulatedToReference: bisection on the reference radius (or z) whose
+        undulated position is the given one."""
+        if not models:
+            return spz
+        spz = np.array(spz, dtype=np.float64)
+        if self.cartesian:
+            st = ct = 0.
+            und_r = spz[2]
+        else:
+            th = float(sz2rtheta(spz[0], spz[2])[1])
+            st, ct = math.sin(th), math.cos(th)
+            und_r = math.hypot(spz[0], spz[2])
+
+        def put(R, x):
+            if self.cartesian:
+                x[2] = R
+            else:
+                x[0], x[2] = R * st, R * ct
+
+        ref = spz.copy()
+        if und_r < geo.inner_radius:
+            put(geo.inner_radius, ref)
+        if und_r > geo.outer_radius:
+            put(geo.outer_radius, ref)
+        current = ref[2] if self.cartesian else math.hypot(ref[0], ref[2])
+        upper, lower = geo.outer_radius, geo.inner_radius
+        for _ in range(101):
+            diff = self.total(models, ref, geo) + current - und_r
+            if abs(diff) < tol:
+                return ref
+            if diff > 0.:
+                upper = current
+            else:
+                lower = current
+            current = .5 * (lower + upper)
+            put(current, ref)
+        raise PreloopError("SE_Model::undulatedToReference || Failed to find reference radius.")
 
 
 def _gll_numbering(conn: np.ndarray) -> np.ndarray:
@@ -807,15 +1024,30 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     quads = _Quads(mesh, inp, geo, abc, lucky)
     nq = mesh.num_quads
     # ---- 3-D models (Model3D::buildInparam, SE_Model: applyTo, finishing3D / finished3D)
+    # geometric models (Geometric3D::applyTo) add undulation on the reference geometry;
+    # volumetric models may read the undulated one; ocean-load models act on the surface
+    und = _Undulation(quads, geo.cartesian)
+    geo_models, ocean_models = [], []
     try:
         models = build_models(inp, geo.cartesian)
         for md in models:
-            quads.apply_model(md, geo)
+            if md.kind == "volumetric":
+                quads.apply_model(md, geo, und)
+            elif md.kind == "geometric":
+                geo_models.append(md)
+                for q in range(nq):
+                    arrs = md.undulation(quads.nodal_xy[q], quads.sz[q], quads.pnr[q], geo)
+                    if arrs is not None:
+                        und.add(q, arrs)
+            else:
+                ocean_models.append(md)
     except Model3DError as ex:
         raise PreloopError(str(ex))
     quads.finished3d()
     quads.refresh_derived()
     q3d = np.array([quads.is3d(q) for q in range(nq)], bool)
+    has_und = np.array([q in und.und for q in range(nq)], bool)
+    und3d = np.array([und.is3d(q) for q in range(nq)], bool)
     tol = mesh.global_variables["dist_tolerance"]
 
     # ---- time step (SE_Model::computeDt, main.cpp:431-470)
@@ -827,11 +1059,19 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
             f = .9
         if abc.clayton and any(quads.sides[k][q] != -1 for k in abc.keys):
             f = .5
+        if has_und[q]:
+            # slice by slice on the undulated coordinates (Quad::computeDt)
+            vs = quads.vmax_slices(q) if q3d[q] else np.array([float(np.max(quads.vmax[q]))])
+            szs = und.slices_sz(q)
+            n = max(len(vs), len(szs))
+            dts[q] = min(quad_dt(szs[0 if len(szs) == 1 else k], vs[0 if len(vs) == 1 else k])
+                         for k in range(n)) * f * courant
+            continue
         vmax = quads.vmax_3d(q) if q3d[q] else float(np.max(quads.vmax[q]))
         dts[q] = quad_dt(quads.sz[q], vmax) * f * courant
     dt_mesh = round_dt(float(dts.min()))
     enforced = inp.source.get("time_axis:enforced_dt")
-    dt = dt_mesh if enforced == "NONE" or float(enforced) < EPS else float(enforced)
+    dt = dt_mesh if enforced == "NONE" or float(enforced) < DEPS else float(enforced)
 
     # ---- attenuation (main.cpp:482-499, AttBuilder)
     att = inp.model.get_options("attenuation", {"NONE": -1, "FULL": 0, "CG4": 1})
@@ -868,7 +1108,8 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     sid[sp_used] = np.arange(len(sp_used))
     fid[fp_used] = np.arange(len(fp_used))
     ifact = quads.geom[:, 5, :]
-    s1d, f1d = solid_q[~q3d[solid_q]], fluid_q[~q3d[fluid_q]]
+    qm3 = q3d | has_und                         # quads whose masses go point by point
+    s1d, f1d = solid_q[~qm3[solid_q]], fluid_q[~qm3[fluid_q]]
     smass = np.zeros(len(sp_used))
     np.add.at(smass, sid[gll[s1d]].ravel(), (quads.rho[s1d] * ifact[s1d]).ravel())
     fmass = np.zeros(len(fp_used))
@@ -877,9 +1118,10 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
         np.add.at(fmass, fid[gll[f1d]].ravel(), (ifact[f1d] / kappa).ravel())
     # quads with 3-D properties add per-slice masses (Mass3D where a point's mass varies)
     smass3, fmass3 = {}, {}
-    for q in np.nonzero(q3d)[0]:
+    for q in np.nonzero(qm3)[0]:
         rho = quads.pointwise(q, "RHO")
         vp = quads.pointwise(q, "VP") if quads.fluid[q] else None
+        jac = und.mass_jacobian(q) if has_und[q] else None
         for p in range(25):
             if quads.fluid[q]:
                 mval = ifact[q, p] / (np.broadcast_arrays(rho[p], vp[p])[0] * vp[p] ** 2)
@@ -887,14 +1129,24 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
             else:
                 mval = rho[p] * ifact[q, p]
                 tgt, idx = smass3, int(sid[gll[q, p]])
+            if jac is not None:
+                mval = mval * jac[p]
             prev = tgt.get(idx)
             tgt[idx] = mval.copy() if prev is None else prev + mval
+    # per-point contributions constant in phi are 1-D masses after all
+    for tgt, one in ((smass3, smass), (fmass3, fmass)):
+        for idx in list(tgt):
+            v = np.atleast_1d(tgt[idx])
+            if len(v) == 1 or np.linalg.norm(v - v[0]) <= np.linalg.norm(v) * DEPS:
+                one[idx] += v[0]
+                del tgt[idx]
 
     # ---- boundaries of the points (Quad::setupGLL, GLLPoint::release)
     axial_pt = np.zeros(ngll, bool)
     surface_pt = np.zeros(ngll, bool)
     normal = np.zeros((ngll, 2))
     cl_s, cl_f, cl3_s, cl3_f = [], [], [], []
+    ocean_pts = {}                                # point -> [summed top normal [n][3], sum rho depth]
     gamma_sum = np.zeros(ngll)
     gamma_cnt = np.zeros(ngll, np.int64)
     gamma3 = {}                                   # points whose gamma varies in phi
@@ -905,9 +1157,18 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
         if quads.sides["TOP"][q] != -1:
             for p in EDGE_IPNT[quads.sides["TOP"][q]]:
                 surface_pt[gll[q, p]] = True
+            if ocean_models and not quads.fluid[q]:
+                _ocean_on_quad(q, quads, und, ocean_models, geo, gll, ocean_pts)
         if quads.sides["SOLID_FLUID"][q] != -1:
             pts, nsf = quads.normals(q, quads.sides["SOLID_FLUID"][q])
             for p, n in zip(pts, nsf):
+                if has_und[q]:
+                    n3 = und.normal3d(q, n, p)
+                    if len(n3) > 1 and np.linalg.norm(n3 - n3[0]) > np.linalg.norm(n3) * DEPS:
+                        raise PreloopError("GLLPoint::release || A solid-fluid boundary with undulation that "
+                                           "varies in azimuth (SolidFluidCoupling3D) is not supported by "
+                                           "this build.")
+                    n = np.array([n3[0, 0], n3[0, 2]])
                 normal[gll[q, p]] += n / 2. if quads.fluid[q] else -n / 2.
         if abc.clayton or abc.sponge:
             a_rho, a_vp, a_vs = quads.abc_rho_vp_vs(q)
@@ -919,12 +1180,25 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
                 pts, nab = quads.normals(q, edge)
                 for p, n in zip(pts, nab):
                     g = gll[q, p]
+                    n3 = None
+                    if has_und[q]:
+                        n3 = und.normal3d(q, n, p)
+                        if len(n3) == 1 or np.linalg.norm(n3 - n3[0]) <= np.linalg.norm(n3) * DEPS:
+                            n, n3 = np.array([n3[0, 0], n3[0, 2]]), None
                     area = float(np.hypot(n[0], n[1]))
-                    if area <= 0.:
+                    if area <= 0. and n3 is None:
                         continue
                     rvp = a_rho[p] * a_vp[p]
                     rvs = np.broadcast_arrays(a_rho[p], a_vs[p])[0] * a_vs[p]
-                    if len(rvp) == 1 and len(rvs) == 1:
+                    if n3 is not None:
+                        # ClaytonSolid3D / ClaytonFluid3D with the undulated normal of each slice
+                        nrp = int(pnr[g])
+                        n3 = np.broadcast_to(n3, (nrp, 3)) if len(n3) == 1 else n3
+                        ar = np.linalg.norm(n3, axis=1)
+                        ent = (int(fid[g] if quads.fluid[q] else sid[g]), np.broadcast_to(rvp, (nrp,)).copy(),
+                               np.broadcast_to(rvs, (nrp,)).copy(), ar.copy(), n3 / ar[:, None])
+                        (cl3_f if quads.fluid[q] else cl3_s).append(ent)
+                    elif len(rvp) == 1 and len(rvs) == 1:
                         # ClaytonSolid1D / ClaytonFluid1D
                         if quads.fluid[q]:
                             cl_f.append((fid[g], float(rvp[0]), area))
@@ -960,7 +1234,7 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
                         span = span * float(r_)
                     vp, vs, rho = np.broadcast_arrays(a_vp[p], a_vs[p], a_rho[p])
                     gmax = np.atleast_1d(abc.u0(abs(span), vp, vs, rho, bool(quads.fluid[q]))) * pattern
-                if np.linalg.norm(gmax) > EPS:
+                if np.linalg.norm(gmax) > DEPS:
                     g = gll[q, p]
                     gamma_cnt[g] += 1
                     if len(gmax) == 1 and g not in gamma3:
@@ -986,6 +1260,8 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     m.fp_coords = coords[fp_used]
     fsurf = surface_pt & ("TOP" not in abc.keys)
     m.fp_surface = fsurf[fp_used].astype(np.uint8)
+    if ocean_pts:
+        _release_ocean(m, ocean_pts, sid)
     # solid elements
     ns = len(solid_q)
     enr = np.array([int(pnr[gll[q]].max()) for q in range(nq)], np.int64)
@@ -1001,11 +1277,11 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     nmod = np.where(rheo == L.AXG_ISO, 2, 5)
     # elements whose moduli vary in phi (op1D_3D::regularize1D): per-slice operands
     rows = np.ones(ns, np.int64)
-    for k in np.nonzero(q3d[solid_q])[0]:
+    for k in np.nonzero(q3d[solid_q] | und3d[solid_q])[0]:
         q = solid_q[k]
         keys = (("RHO", "VP", "VS") if rheo[k] == L.AXG_ISO else
                 ("RHO", "VPV", "VPH", "VSV", "VSH", "ETA")) + (("QMU", "QKAPPA") if sls is not None else ())
-        if any(kk in quads.p3.get(q, {}) for kk in keys):
+        if any(kk in quads.p3.get(q, {}) for kk in keys) or und3d[q]:
             rows[k] = enr[q]
     is3 = rows > 1
     m.se_is3d = is3.astype(np.uint8)
@@ -1133,7 +1409,7 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     m.fe_axial = quads.axial[fluid_q]
     m.fe_geom = quads.geom[fluid_q]
     m.fe_theta = theta[fluid_q]
-    frows = np.array([int(enr[q]) if "RHO" in quads.p3.get(q, {}) else 1 for q in fluid_q], np.int64)
+    frows = np.array([int(enr[q]) if "RHO" in quads.p3.get(q, {}) or und3d[q] else 1 for q in fluid_q], np.int64)
     m.fe_is3d = (frows > 1).astype(np.uint8)
     fe_off = np.zeros(nf, np.int64)
     if nf:
@@ -1151,6 +1427,28 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     m.sf_nsa = normal[iface, 0].copy()
     m.sf_nza = normal[iface, 1].copy()
     m.sf_mass_fluid = fmass[fid[iface]] if len(iface) else np.zeros(0)
+    # particle relabelling (Undulation::createPRT) on every quad a geometric model touched
+    for sel, attr, local in ((solid_q, "prt", None), (fluid_q, "prt_fluid", None)):
+        els = [k for k, q in enumerate(sel) if has_und[q]]
+        if not els:
+            continue
+        xs, offs, is3 = [], [], []
+        o = 0
+        for k in els:
+            q = sel[k]
+            x = und.prt(q)                                          # [5, nr, 25]
+            if x.shape[1] > 1 and x.shape[1] != enr[q]:
+                x = np.stack([np.stack([lin_interp_phi(x[c, :, p], int(enr[q])) for p in range(25)], axis=1)
+                              for c in range(5)])
+            offs.append(o)
+            is3.append(1 if x.shape[1] > 1 else 0)
+            xs.append(x.ravel())
+            o += x.size
+        d = {"element": np.array(els, np.int32), "offset": np.array(offs, np.int64),
+             "is3d_prt": np.array(is3, np.uint8), "x": np.concatenate(xs)}
+        if attr == "prt_fluid" and not geo.cartesian:
+            d["theta"] = np.stack([m.fe_theta[k] for k in els])
+        setattr(m, attr, d)
     # absorbing boundaries
     if cl_s:
         a_ = np.array(cl_s)
@@ -1209,7 +1507,8 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
 
     # ---- sources (Source::release) and the time axis (main.cpp:580-620)
     ctx = _Locator(mesh, quads, geo, gll, solid_q, fluid_q)
-    t_min0 = _release_sources(inp, m, ctx, geo, enr, solid_q, dt)
+    und_ctx = (und, geo_models, tol)
+    t_min0 = _release_sources(inp, m, ctx, geo, enr, solid_q, dt, und_ctx)
     t1 = inp.source.get_bounded("time_axis:record_length", 0.)
     nmax = inp.advanced.get("develop:max_num_time_steps", int) \
         if inp.advanced.contains("develop:max_num_time_steps") else 0
@@ -1223,7 +1522,7 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     m.t0 = step0 * dt
     skipped = [] if skip_unsupported_channels else None
     groups = _release_stations(inp, m, ctx, geo, dt, m.t0, m.t0 + (nstep - 1) * dt, nstep, enr, solid_q,
-                               skipped)
+                               skipped, und_ctx)
     egroups = _release_elements(inp, quads, coords, gll, ctx, geo, dt, m.t0, m.t0 + (nstep - 1) * dt, nstep,
                                 enr, mesh.global_variables["dist_tolerance"])
     m.meta = {"workload": "exodus %s (%d solid + %d fluid quads, %s)" %
@@ -1239,6 +1538,73 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
                       cartesian=geo.cartesian, info=info, element_groups=egroups)
 
 
+def _ocean_on_quad(q, quads, und, models, geo, gll, ocean_pts):
+    """OceanLoad3D::applyTo and Quad::setupGLL's ocean part for one quad with a surface
+    edge: sum(rho * depth) of the models at the edge points' slices (reference geometry),
+    and each point's top normal (undulated), summed over the quads that share it."""
+    from .models3d import try_reduce_1d
+    edge = quads.sides["TOP"][q]
+    ipnts = EDGE_IPNT[edge]
+    nr = [int(quads.pnr[q][p]) for p in ipnts]
+    rows = []
+    for p, n in zip(ipnts, nr):
+        phi = np.linspace(0., 2. * np.pi / n * (n - 1), n) if n > 1 else np.zeros(1)
+        rows.append(np.stack([np.full(n, quads.sz[q, 0, p]), phi, np.full(n, quads.sz[q, 1, p])], axis=1))
+    spz = np.concatenate(rows, axis=0)
+    tot = None
+    for md in models:
+        v = md.sum_rho_depth(quads.nodal_xy[q], spz, nr, geo)
+        if v is None:
+            continue
+        tot = v if tot is None else [a + b for a, b in zip(tot, v)]
+    if tot is None:
+        return
+    if try_reduce_1d(tot):
+        tot = [a[:1] for a in tot]
+    pts, n2 = quads.normals(q, edge)
+    for ip, p in enumerate(pts):
+        n3 = und.normal3d(q, n2[ip], p)
+        g = int(gll[q, p])
+        cur = ocean_pts.get(g)
+        if cur is None:
+            ocean_pts[g] = [n3.copy(), tot[ip]]
+        else:
+            k = max(len(cur[0]), len(n3))
+            cur[0] = np.broadcast_to(cur[0], (k, 3)) + np.broadcast_to(n3, (k, 3))
+            cur[1] = tot[ip]
+
+
+def _release_ocean(m, ocean_pts, sid):
+    """GLLPoint::release for solid points under an ocean (GLLPoint.cpp:55-90):
+    MassOceanLoad1D where the mass, sum(rho * depth) and the top normal are all 1-D, else
+    MassOceanLoad3D with the ocean mass sum(rho * depth) |n| and the unit normal per slice."""
+    one, three = [], []
+    for g in sorted(ocean_pts):
+        i = int(sid[g])
+        if i < 0:
+            continue
+        ntop, srd = ocean_pts[g]
+        if len(ntop) > 1 and np.linalg.norm(ntop - ntop[0]) <= np.linalg.norm(ntop) * DEPS:
+            ntop = ntop[:1]
+        mass1d = m.sp_mass_nr is None or int(m.sp_mass_nr[i]) == 1
+        nrp = int(m.sp_nr[i])
+        if mass1d and len(srd) == 1 and len(ntop) == 1:
+            r, t = sz2rtheta(ntop[0, 0], ntop[0, 2])
+            one.append((i, float(srd[0]) * float(r), float(t)))
+        else:
+            area = np.linalg.norm(ntop, axis=1)
+            mo = np.broadcast_to(srd, (nrp,)) * np.broadcast_to(area, (nrp,))
+            unit = np.broadcast_to(ntop / area[:, None], (nrp, 3)).copy()
+            three.append((i, mo, unit))
+    if one:
+        m.ocean_load = (np.array([x[0] for x in one], np.int32), np.array([x[1] for x in one]),
+                        np.array([x[2] for x in one]))
+    if three:
+        off = np.concatenate([[0], np.cumsum([len(x[1]) for x in three])[:-1]]).astype(np.int64)
+        m.ocean_load3d = (np.array([x[0] for x in three], np.int32), off, np.concatenate([x[1] for x in three]),
+                          np.concatenate([x[2] for x in three]))
+
+
 def _mass_layout(mass1d, mass3d):
     """Point masses: 1-D values plus the per-slice contributions of elements with 3-D density
     (GLLPoint::addMass); (values, per-point count, offsets), the last two None when every
@@ -1249,7 +1615,7 @@ def _mass_layout(mass1d, mass3d):
     for p in range(len(mass1d)):
         v = mass3d.get(p)
         tot = np.array([mass1d[p]]) if v is None else v + mass1d[p]
-        if len(tot) > 1 and np.linalg.norm(tot - tot[0]) > np.linalg.norm(tot) * EPS:
+        if len(tot) > 1 and np.linalg.norm(tot - tot[0]) > np.linalg.norm(tot) * DEPS:
             any3 = True
         else:
             tot = tot[:1]
@@ -1343,8 +1709,30 @@ def _map_point(mp, nodal, xi, eta):
     return out[:2], out[2:].reshape(2, 2)
 
 
-def _compute_spz(geo, crd, source_centered, xy, ellipticity, use_depth, depth_solid, enforce_axis):
-    """Source::computeSPZ without undulation (no 3-D geometric models in this build)."""
+def _compute_spz(geo, crd, source_centered, xy, ellipticity, use_depth, depth_solid, enforce_axis, und_ctx=None):
+    """Source::computeSPZ (preloop/source/Source.cpp:97-191). und_ctx = (undulation, geometric
+    models, distance tolerance) when the location is given in the undulated geometry: a depth
+    is then taken below the undulated surface, and the point is mapped back to the
+    reference geometry (SE_Model::undulatedToReference)."""
+    crd_in = np.array(crd, dtype=np.float64)
+    spz = _compute_spz_ref(geo, crd, source_centered, xy, ellipticity, use_depth, depth_solid, enforce_axis)
+    if und_ctx is None or not und_ctx[1]:
+        return spz
+    und, models, tol = und_ctx
+    if use_depth:
+        R = geo.outer_solid_radius if depth_solid else geo.outer_radius
+        if geo.cartesian:
+            spz[2] = R
+            spz[2] = R + und.total(models, spz, geo) - crd_in[2]
+        else:
+            th = float(sz2rtheta(spz[0], spz[2])[1])
+            spz[0], spz[2] = R * math.sin(th), R * math.cos(th)
+            r = R + und.total(models, spz, geo) - crd_in[2]
+            spz[0], spz[2] = r * math.sin(th), r * math.cos(th)
+    return und.to_reference(models, spz, geo, tol)
+
+
+def _compute_spz_ref(geo, crd, source_centered, xy, ellipticity, use_depth, depth_solid, enforce_axis):
     crd = np.array(crd, dtype=np.float64)
     if use_depth:
         R = geo.outer_solid_radius if depth_solid else geo.outer_radius
@@ -1355,7 +1743,7 @@ def _compute_spz(geo, crd, source_centered, xy, ellipticity, use_depth, depth_so
         if xy:
             x, y = crd[0], crd[1]
             crd[0] = math.hypot(x, y)
-            crd[1] = 0. if crd[0] < EPS else math.atan2(y, x)
+            crd[1] = 0. if crd[0] < DEPS else math.atan2(y, x)
         elif not geo.cartesian:
             r, th = crd[2], crd[0]
             crd[0], crd[2] = r * math.sin(th), r * math.cos(th)
@@ -1394,7 +1782,7 @@ def _qzsp(geo, spz, axial, source_centered, crd_in, use_depth, depth_solid, elli
     return Q
 
 
-def _release_sources(inp, m, ctx, geo, enr, solid_q, dt):
+def _release_sources(inp, m, ctx, geo, enr, solid_q, dt, und_ctx=None):
     gm = inp.source
     n = gm.get("list_of_sources:[?]", int) if gm.contains("list_of_sources") and \
         gm._walk("list_of_sources") else 0
@@ -1443,7 +1831,9 @@ def _release_sources(inp, m, ctx, geo, enr, solid_q, dt):
             raise PreloopError("Mechanism::release || FLUID_PRESSURE sources are not supported by this "
                                "build. || Source name: " + name)
         data = np.array(gm.get_vector(rm + ":data", float)) * gm.get(rm + ":unit", float)
-        spz = _compute_spz(geo, crd, centered, False, ellip, use_depth, depth_solid, axial)
+        undulated = gm.get(rl + ":undulated_geometry", bool) if gm.contains(rl + ":undulated_geometry") else False
+        spz = _compute_spz(geo, crd, centered, False, ellip, use_depth, depth_solid, axial,
+                           und_ctx if undulated else None)
         q, xe = ctx.locate(spz[0], spz[2], False)
         if q < 0:
             raise PreloopError("Source::release || Error locating source in mesh. || "
@@ -1560,7 +1950,8 @@ def standard_channels(user, skipped=None):
     return [std for std, _, _ in SOLID_CHANNELS if std in out]
 
 
-def _release_stations(inp, m, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, solid_q, skipped=None):
+def _release_stations(inp, m, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, solid_q, skipped=None,
+                      und_ctx=None):
     gm = inp.output
     groups = []
     if not gm.contains("list_of_station_groups") or not gm._walk("list_of_station_groups"):
@@ -1585,6 +1976,7 @@ def _release_stations(inp, m, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, s
         use_depth = gm.get_options(rl + ":vertical_x3", {"RADIUS": False, "DEPTH": True})
         ellip = gm.get(rl + ":ellipticity", bool) if not centered else False
         depth_solid = gm.get(rl + ":depth_below_solid_surface", bool) if use_depth else False
+        undulated = gm.get(rl + ":undulated_geometry", bool) if gm.contains(rl + ":undulated_geometry") else False
         rw = root + ":wavefields"
         frame = gm.get_options(rw + ":coordinate_frame", {"spz": "spz", "RTZ": "RTZ", "ENZ": "ENZ",
                                                           "xyz": "xyz"})
@@ -1640,7 +2032,8 @@ def _release_stations(inp, m, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, s
                            first=len(st_e))
         th, baz, phi = [], [], []
         for key, c in zip(keys, crds):
-            spz = _compute_spz(geo, c, centered, xy, ellip, use_depth, depth_solid, False)
+            spz = _compute_spz(geo, c, centered, xy, ellip, use_depth, depth_solid, False,
+                               und_ctx if undulated else None)
             q, xe = ctx.locate(spz[0], spz[2], False)
             if q < 0:
                 raise PreloopError("StationOutput::release || Error locating station in mesh. || "

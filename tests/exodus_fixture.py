@@ -339,6 +339,40 @@ def model3d_yaml(name, fname, horizontal, vertical, nc_vars, data_rank, props, l
     return "\n".join(lines) + "\n"
 
 
+def geometric_yaml(name, fname, horizontal, vertical, nc_vars, data_rank, var, interface, lo, hi, factor=1.0,
+                   length_unit="m", angle_unit="radian", depth_solid="false", ellipticity="false"):
+    """One StructuredGridG3D entry of list_of_3D_models (undulation map between lo and hi)."""
+    return "\n".join([
+        "    - %s:" % name, "        activated: true", "        class_name: StructuredGridG3D",
+        "        nc_data_file: %s" % fname, "        coordinates:",
+        "            horizontal: %s" % horizontal, "            vertical: %s" % vertical,
+        "            ellipticity: %s" % ellipticity, "            depth_below_solid_surface: %s" % depth_solid,
+        "            nc_variables: [%s]" % ", ".join(nc_vars),
+        "            data_rank: [%s]" % ", ".join(str(r) for r in data_rank),
+        "            length_unit: %s" % length_unit, "            angle_unit: %s" % angle_unit,
+        "        undulation_range:", "            interface: %r" % interface, "            min_max: [%r, %r]" % (lo, hi),
+        "        undulation_data:", "            nc_var: %s" % var, "            factor: %r" % factor,
+        "        store_grid_only_on_leaders: true"]) + "\n"
+
+
+def ocean_yaml(name, fname, horizontal, nc_vars, data_rank, var, factor=1.0, length_unit="m",
+               angle_unit="radian", ellipticity="false"):
+    """One StructuredGridO3D entry of list_of_3D_models (sum of rho * depth)."""
+    return "\n".join([
+        "    - %s:" % name, "        activated: true", "        class_name: StructuredGridO3D",
+        "        nc_data_file: %s" % fname, "        coordinates:",
+        "            horizontal: %s" % horizontal, "            ellipticity: %s" % ellipticity,
+        "            nc_variables: [%s]" % ", ".join(nc_vars),
+        "            data_rank: [%s]" % ", ".join(str(r) for r in data_rank),
+        "            length_unit: %s" % length_unit, "            angle_unit: %s" % angle_unit,
+        "        data_sum_rho_depth:", "            nc_var: %s" % var, "            factor: %r" % factor,
+        "        store_grid_only_on_leaders: true"]) + "\n"
+
+
+def ellipticity_yaml(name):
+    return "    - %s:\n        activated: true\n        class_name: Ellipticity\n" % name
+
+
 def add_3d_models(d, entries):
     """Replace the empty list_of_3D_models of an input directory by the given entries."""
     p = os.path.join(d, "inparam.model.yaml")

@@ -312,3 +312,61 @@ def test_scanning_file_and_pointwise_nr_round_trip(built, tmp_path):
     look = {(round(c[0], 3), round(c[1], 3)): k for k, c in enumerate(m2.sp_coords)}
     got = np.array([m2.sp_nr[look[(round(a, 3), round(b, 3))]] for a, b in sz])
     assert np.array_equal(got, nr_scan)
+
+
+def _with_geometry(d, case):
+    """Add geometric (undulation) and ocean-load 3-D models to a box or shell input directory:
+    box: a Moho-like undulation 300 cos(phi) m between 10 and 70 km depth and an ocean whose
+    sum(rho * depth) varies with phi; shell: a latitude / longitude undulation between 100
+    and 800 km depth and an ocean on half of the globe; shell_ellipticity: WGS84 flattening
+    with the Ellipticity model."""
+    if case == "box":
+        s = np.linspace(0, 200e3, 11)
+        ph = np.linspace(0, 2 * np.pi, 9)
+        fx.write_grid_v3d(os.path.join(d, "und.nc"), {"s": s, "phi": ph},
+                          {"dz": 300.0 * np.cos(ph)[None, :] * np.ones((11, 1))}, ["s", "phi"])
+        fx.write_grid_v3d(os.path.join(d, "sea.nc"), {"s": s, "phi": ph},
+                          {"srd": 4e6 * (1 + 0.5 * np.sin(ph))[None, :] * np.ones((11, 1))}, ["s", "phi"])
+        fx.add_3d_models(d, [fx.geometric_yaml("moho", "und.nc", "DISTANCE_AZIMUTH", "DEPTH", ["s", "phi"], [0, 1],
+                                               "dz", 40e3, 10e3, 70e3),
+                             fx.ocean_yaml("sea", "sea.nc", "DISTANCE_AZIMUTH", ["s", "phi"], [0, 1], "srd")])
+    elif case == "shell":
+        lat, lon = np.linspace(-90, 90, 19), np.linspace(-180, 180, 37)
+        fx.write_grid_v3d(os.path.join(d, "moho.nc"), {"lat": lat, "lon": lon},
+                          {"dz": 2000.0 * np.cos(np.radians(lat))[:, None] * np.sin(np.radians(lon))[None, :]},
+                          ["lat", "lon"])
+        fx.write_grid_v3d(os.path.join(d, "sea.nc"), {"lat": lat, "lon": lon},
+                          {"srd": np.maximum(0, 4e6 * np.sin(np.radians(lon)))[None, :] * np.ones((19, 1))},
+                          ["lat", "lon"])
+        fx.add_3d_models(d, [fx.geometric_yaml("moho", "moho.nc", "LATITUDE_LONGITUDE", "DEPTH", ["lat", "lon"],
+                                               [0, 1], "dz", 400e3, 100e3, 800e3, angle_unit="degree"),
+                             fx.ocean_yaml("sea", "sea.nc", "LATITUDE_LONGITUDE", ["lat", "lon"], [0, 1], "srd",
+                                           angle_unit="degree")])
+    else:
+        fx.add_3d_models(d, [fx.ellipticity_yaml("ellipticity")])
+        p = os.path.join(d, "inparam.model.yaml")
+        with open(p) as f:
+            txt = f.read()
+        with open(p, "w") as f:
+            f.write(txt.replace("flattening_on_surface: SPHERE", "flattening_on_surface: WGS84"))
+    return d
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["box", "shell", "shell_ellipticity"])
+def test_simulation_with_geometric_and_ocean_models_matches_oracle(built, tmp_path, case, precision):
+    """Undulated geometry through the whole path: particle relabelling (1-D and 3-D, solid
+    and fluid elements), the PRT Jacobian on the masses, 3-D ocean loads, slice-wise dt."""
+    from axisem3d_b200 import simulation
+    d = _with_geometry((_box if case == "box" else _shell)(str(tmp_path / "input")), case)
+    res = simulation.run(d, None, precision=precision)
+    m = res.sim.model
+    assert m.prt is not None and len(m.prt["element"]) > 0
+    if case != "shell_ellipticity":
+        assert m.prt["is3d_prt"].any() and m.ocean_load3d is not None
+    ref = _oracle_traces(res.sim)
+    for name, (t_ref, w_ref) in ref.items():
+        t, w = res.traces[name]
+        assert np.array_equal(t, t_ref) and np.abs(w_ref).max() > 0
+        err = float(np.linalg.norm(w - w_ref) / np.linalg.norm(w_ref))
+        assert err <= TOL[precision], (name, err)

@@ -175,8 +175,8 @@ def test_unsupported_inputs_raise(tmp_path):
         txt = f.read()
     with open(p, "w") as f:
         f.write(txt.replace("list_of_3D_models: []", "list_of_3D_models:\n    - moho:\n        activated: true\n"
-                                                      "        class_name: StructuredGridG3D\n"))
-    with pytest.raises(preloop.PreloopError, match="StructuredGridG3D"):
+                                                      "        class_name: SphericalHarmonicsG3D\n"))
+    with pytest.raises(preloop.PreloopError, match="SphericalHarmonicsG3D is not supported"):
         preloop.build(d)
 
 
