@@ -79,6 +79,11 @@ class axg_force_sources(C.Structure):
                 ("pattern", P_f64), ("stf", C.POINTER(axg_stf)), ("wavefield", P_i32)]
 
 
+class axg_pressure_sources(C.Structure):
+    _fields_ = [("count", C.c_int32), ("element", P_i32), ("nu", P_i32), ("pattern_offset", P_i64),
+                ("pattern", P_f64), ("stf", C.POINTER(axg_stf)), ("wavefield", P_i32)]
+
+
 class axg_stations(C.Structure):
     _fields_ = [("count", C.c_int32), ("element", P_i32), ("weights", P_f64), ("phi", P_f64)]
 
@@ -115,6 +120,7 @@ SIGNATURES = {
     "axg_set_solid_fluid": (C.c_int, [H, C.POINTER(axg_solid_fluid)]),
     "axg_set_moment_sources": (C.c_int, [H, C.POINTER(axg_moment_sources)]),
     "axg_set_force_sources": (C.c_int, [H, C.POINTER(axg_force_sources)]),
+    "axg_set_pressure_sources": (C.c_int, [H, C.POINTER(axg_pressure_sources)]),
     "axg_set_stations": (C.c_int, [H, C.POINTER(axg_stations), C.c_int32]),
     "axg_set_clayton": (C.c_int, [H, C.c_int32, C.POINTER(axg_clayton)]),
     "axg_set_sponge": (C.c_int, [H, C.c_int32, C.c_int32, P_i32, P_f64]),

@@ -259,6 +259,15 @@ int axg_set_force_sources(axg_solver *h, const axg_force_sources *s) {
     });
 }
 
+int axg_set_pressure_sources(axg_solver *h, const axg_pressure_sources *s) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (!s) throw axg::Error(AXG_E_ARG, "FluidPressure || null description.");
+        sources_from(h->model.ps, s->count, s->element, s->nu, s->pattern_offset, s->pattern, s->stf,
+                     s->wavefield, std::max(1, h->cfg.nwave), 1, "FluidPressure::FluidPressure");
+    });
+}
+
 int axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interval) {
     return guarded(h, [&] {
         need_open(h);

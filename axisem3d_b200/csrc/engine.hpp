@@ -135,7 +135,7 @@ struct HostModel {
     HostSolidElements se;
     HostFluidElements fe;
     HostCoupling sf;
-    HostSources ms, fs;
+    HostSources ms, fs, ps;          // moment, force, fluid pressure
     HostStations st;
 };
 

@@ -197,6 +197,7 @@ public:
         build_abc(m);
         build_scanning(m);
         build_sources(m.ms, m.fs);
+        build_pressure_sources(m.ps);
         build_stations(m.st);
         step_dev_.alloc(1);
         step_dev_.zero(stream_);
@@ -1461,6 +1462,21 @@ private:
         post_launch();
     }
 
+    void build_pressure_sources(const HostSources &ps) {
+        ps_n_ = ps.count;
+        if (!ps_n_) return;
+        for (int i = 0; i < ps.count; i++)
+            if (ps.elem[i] < 0 || ps.elem[i] >= model_.fe.count)
+                throw Error(AXG_E_ARG, "FluidPressure::FluidPressure || element index out of range.");
+        ps_el_.upload(ps.elem); ps_nu_.upload(ps.nu); ps_wave_.upload(ps.wave);
+        std::vector<int64_t> off(ps.pat_off.begin(), ps.pat_off.end());
+        ps_po_.upload(off);
+        std::vector<C> p(std::max<size_t>(ps.pattern.size() / 2, 1), mk<T>(0, 0));
+        for (size_t i = 0; i < ps.pattern.size() / 2; i++) p[i] = mk<T>((T)ps.pattern[2 * i], (T)ps.pattern[2 * i + 1]);
+        ps_pat_.upload(p);
+        fe_pts_.upload(model_.fe.pts);
+    }
+
     void build_sources(const HostSources &ms, const HostSources &fs) {
         auto conv = [](const HostSources &h, DBuf<int> &el, DBuf<int> &nu, DBuf<int64_t> &po,
                        DBuf<C> &pat) {
@@ -1521,7 +1537,7 @@ private:
     // STF table and seismogram buffer large enough for steps [0, nsteps)
     void ensure_capacity(int nsteps) {
         bool changed = false;
-        if ((ms_n_ || fs_n_) && nsteps > stf_cap_) {
+        if ((ms_n_ || fs_n_ || ps_n_) && nsteps > stf_cap_) {
             int cap = std::max(nsteps, 2 * stf_cap_);
             fill_stf(cap);
             changed = true;
@@ -1570,15 +1586,18 @@ private:
     }
     void fill_stf(int cap) {
         // t accumulated as NewmarkTimeScheme::solve does (t += mDt)
-        std::vector<T> ms((size_t)cap * std::max(ms_n_, 1)), fs((size_t)cap * std::max(fs_n_, 1));
+        std::vector<T> ms((size_t)cap * std::max(ms_n_, 1)), fs((size_t)cap * std::max(fs_n_, 1)),
+            ps((size_t)cap * std::max(ps_n_, 1));
         double t = cfg_.t0;
         for (int k = 0; k < cap; k++) {
             for (int i = 0; i < ms_n_; i++) ms[(size_t)k * ms_n_ + i] = (T)stf_value(model_.ms.stf[i], t);
             for (int i = 0; i < fs_n_; i++) fs[(size_t)k * fs_n_ + i] = (T)stf_value(model_.fs.stf[i], t);
+            for (int i = 0; i < ps_n_; i++) ps[(size_t)k * ps_n_ + i] = (T)stf_value(model_.ps.stf[i], t);
             t += cfg_.dt;
         }
         ms_stf_.upload(ms);
         fs_stf_.upload(fs);
+        ps_stf_.upload(ps);
         stf_cap_ = cap;
     }
 
@@ -1605,6 +1624,18 @@ private:
             force_source_kernel<T><<<fs_n_, 128, 0, stream_>>>(a);
             post_launch();
         }
+    }
+
+    void launch_pressure_sources() {
+        if (stf_cap_ <= 0)
+            throw Error(AXG_E_STATE, "Domain::applySources || source-time table not allocated.");
+        ForceArgs<T> a;
+        a.nsrc = ps_n_; a.elem = ps_el_.p; a.nu = ps_nu_.p; a.pat_off = ps_po_.p;
+        a.pattern = ps_pat_.p; a.stf = ps_stf_.p; a.stf_steps = stf_cap_; a.step = step_dev_.p;
+        a.e_pts = fe_pts_.p; a.pt_off = fp_.off.p; a.pt_nu = fp_.nu.p; a.stiff = fp_.stiff.p;
+        a.wave = ps_wave_.p; a.fstride = (size_t)fp_.total;
+        pressure_source_kernel<T><<<ps_n_, 128, 0, stream_>>>(a);
+        post_launch();
     }
 
     void launch_stiffness() {
@@ -1770,12 +1801,15 @@ private:
             a.sponge = solid ? sg_s_.p : sg_f_.p;
             int threads = 256, blocks = (int)(((int64_t)P.total * nwave_ + threads - 1) / threads);
             Abc3D &g3 = solid ? sg3_s_ : sg3_f_;
-            if (g3.n && (mask & 2)) {
-                // a 3-D sponge acts on the acceleration in slices between 1/M and the update
+            const bool press = !solid && ps_n_ && (mask & 2);
+            if ((g3.n || press) && (mask & 2)) {
+                // a 3-D sponge and fluid pressure sources act on the acceleration between
+                // 1/M and the update
                 a.mask = mask & 3;
                 point_update_kernel<T, D, COMP><<<blocks, threads, 0, stream_>>>(a);
                 post_launch();
-                launch_sponge3d(P, g3);
+                if (g3.n) launch_sponge3d(P, g3);
+                if (press) launch_pressure_sources();
                 if (!(mask & 4)) continue;
                 a.mask = 4;
             }
@@ -1881,6 +1915,11 @@ private:
     DBuf<C> ms_pat_, fs_pat_;
     DBuf<T> ms_stf_, fs_stf_;
     DBuf<int> e_nr_, e_pts_;
+    int ps_n_ = 0;
+    DBuf<int> ps_el_, ps_nu_, ps_wave_, fe_pts_;
+    DBuf<int64_t> ps_po_;
+    DBuf<C> ps_pat_;
+    DBuf<T> ps_stf_;
     DBuf<uint8_t> e_axial_;
     DBuf<T> e_geom_;
     int st_n_ = 0, st_interval_ = 1, seis_cap_ = 0;

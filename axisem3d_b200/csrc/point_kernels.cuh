@@ -794,6 +794,27 @@ __global__ void force_source_kernel(const ForceArgs<T> a) {
     }
 }
 
+// FluidPressure::apply (core/source/elem_src/fluid/FluidPressure.cpp) -> FluidPoint::
+// addPressureSource (FluidPoint.hpp:113-119): pattern [nu][25] x STF(t) added to the fluid
+// points' acceleration after the mass term (FluidPoint::computeStiffToAccel, FluidPoint.cpp:
+// 42-48), modes below the point's nu; same arguments as the force sources, one component
+template <class T>
+__global__ void pressure_source_kernel(const ForceArgs<T> a) {
+    const int s = blockIdx.x;
+    if (s >= a.nsrc || a.stf_steps <= 0 || a.stf == nullptr) return;
+    const int e = a.elem[s];
+    const int st = max(0, min(*a.step, a.stf_steps - 1));
+    const T v = a.stf[(size_t)st * a.nsrc + s];
+    for (int i = threadIdx.x; i < a.nu[s] * 25; i += blockDim.x) {
+        const int al = i / 25, q = i % 25;
+        const int p = a.e_pts[(size_t)e * 25 + q];
+        if (al >= a.pt_nu[p]) continue;
+        const cx_t<T> pv = a.pattern[a.pat_off[s] + (size_t)al * 25 + q];
+        atomic_add_cx(a.stiff + (size_t)a.wave[s] * a.fstride + (size_t)(a.pt_off[p] + al),
+                      mk<T>(pv.x * v, pv.y * v));
+    }
+}
+
 // ----------------------------------------------------------------- stations ---
 template <class T>
 struct StationArgs {

@@ -108,6 +108,13 @@ class Model:
     fs_pattern: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex128))
     fs_stf: List[STF] = field(default_factory=list)
     fs_wave: Optional[np.ndarray] = None
+    # FluidPressure sources on fluid elements: pattern [nu][25] complex per source
+    ps_elem: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    ps_nu: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    ps_pat_off: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    ps_pattern: np.ndarray = field(default_factory=lambda: np.zeros(0, np.complex128))
+    ps_stf: List[STF] = field(default_factory=list)
+    ps_wave: Optional[np.ndarray] = None
     nwave: int = 1                                # independent wavefields on this mesh
     # stations
     st_elem: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
@@ -268,6 +275,7 @@ class Model:
 
         ms = sources("ms", L.axg_moment_sources, 6)
         fs = sources("fs", L.axg_force_sources, 3)
+        ps = sources("ps", L.axg_pressure_sources, 1)
 
         st = L.axg_stations()
         st.count = len(self.st_elem)
@@ -361,7 +369,7 @@ class Model:
             keep[name + "_pt"], keep[name + "_g"] = pt, g
             return (pt, g)
 
-        return {"sp": sp, "fp": fp, "se": se, "fe": fe, "sf": sf, "ms": ms, "fs": fs, "st": st,
+        return {"sp": sp, "fp": fp, "se": se, "fe": fe, "sf": sf, "ms": ms, "fs": fs, "ps": ps, "st": st,
                 "cl_s": clay("cls", self.cl_solid, True), "cl_f": clay("clf", self.cl_fluid, False),
                 "sg_s": sponge("sgs", self.sponge_solid), "sg_f": sponge("sgf", self.sponge_fluid),
                 "ocean": ocean(), "scan": scan(), "ocean3": ocean3(), "prt": prt(self.prt, "prt"), "prt_f": prt(self.prt_fluid, "prtf"),

@@ -1639,6 +1639,8 @@ class _Locator:
         self.solid_q, self.fluid_q = solid_q, fluid_q
         self.solid_index = -np.ones(mesh.num_quads, np.int64)
         self.solid_index[solid_q] = np.arange(len(solid_q))
+        self.fluid_index = -np.ones(mesh.num_quads, np.int64)
+        self.fluid_index[fluid_q] = np.arange(len(fluid_q))
         xy = mesh.coords
         tol = mesh.global_variables["dist_tolerance"]
         self.tol = tol
@@ -1786,7 +1788,7 @@ def _release_sources(inp, m, ctx, geo, enr, solid_q, dt, und_ctx=None):
     gm = inp.source
     n = gm.get("list_of_sources:[?]", int) if gm.contains("list_of_sources") and \
         gm._walk("list_of_sources") else 0
-    ms, fs = [], []
+    ms, fs, ps = [], [], []
     t0 = np.inf
     north_source = inp.model.get("geodesy:lat_lon_north_pole_mesh") == "SOURCE"
     for k in range(n):
@@ -1827,14 +1829,11 @@ def _release_sources(inp, m, ctx, geo, enr, solid_q, dt, und_ctx=None):
         rm = root + ":mechanism"
         mtype = gm.get_options(rm + ":type", {"MOMENT_TENSOR": "M", "FORCE_VECTOR": "F",
                                               "FLUID_PRESSURE": "P"})
-        if mtype == "P":
-            raise PreloopError("Mechanism::release || FLUID_PRESSURE sources are not supported by this "
-                               "build. || Source name: " + name)
         data = np.array(gm.get_vector(rm + ":data", float)) * gm.get(rm + ":unit", float)
         undulated = gm.get(rl + ":undulated_geometry", bool) if gm.contains(rl + ":undulated_geometry") else False
         spz = _compute_spz(geo, crd, centered, False, ellip, use_depth, depth_solid, axial,
                            und_ctx if undulated else None)
-        q, xe = ctx.locate(spz[0], spz[2], False)
+        q, xe = ctx.locate(spz[0], spz[2], mtype == "P")
         if q < 0:
             raise PreloopError("Source::release || Error locating source in mesh. || "
                                "Source index = %d || Source name  = %s" % (k, name))
@@ -1843,12 +1842,12 @@ def _release_sources(inp, m, ctx, geo, enr, solid_q, dt, und_ctx=None):
         t0 = min(t0, -stf.half_duration * 2.5 + stf.time_shift)
         Q = _qzsp(geo, spz, axial, centered, crd, use_depth, depth_solid, ellip)
         nu_1 = int(enr[q]) // 2 + 1
-        e = int(ctx.solid_index[q])
+        e = int(ctx.fluid_index[q] if mtype == "P" else ctx.solid_index[q])
         pat = _pattern(mtype, data, Q, axial, w, float(spz[1]), nu_1, bool(ctx.quads.axial[q]))
-        (ms if mtype == "M" else fs).append((e, pat, stf))
+        {"M": ms, "F": fs, "P": ps}[mtype].append((e, pat, stf))
     if n == 0:
         t0 = 0.
-    for lst, pre in ((ms, "ms"), (fs, "fs")):
+    for lst, pre in ((ms, "ms"), (fs, "fs"), (ps, "ps")):
         if not lst:
             continue
         setattr(m, pre + "_elem", np.array([x[0] for x in lst], np.int32))
@@ -1863,8 +1862,21 @@ def _release_sources(inp, m, ctx, geo, enr, solid_q, dt, und_ctx=None):
 
 
 def _pattern(mtype, data, Q, on_axis, w, phi, nu_1, axial_quad):
-    """Mechanism::release (Mechanism.cpp:42-222) for moment tensors and force vectors."""
+    """Mechanism::release (Mechanism.cpp:42-222) for fluid pressures, force vectors and moment
+    tensors."""
     ephi = lambda a: np.exp(1. * a * (-1j * phi))         # noqa: E731
+    if mtype == "P":
+        p = data[0] * w
+        nu = min(nu_1, 1) if on_axis else nu_1
+        pat = np.zeros((nu, 25), np.complex128)
+        if not on_axis:
+            for a in range(nu):
+                pat[a] = ephi(a) * p
+        if axial_quad:
+            pat[:, 0:5] = 0.
+            pat[0, 0:5] = p[0:5]
+            pat /= 2. * np.pi
+        return pat
     if mtype == "F":
         f = Q @ data[:3]
         fs_, fp_, fz_ = f[1] * w, f[2] * w, f[0] * w

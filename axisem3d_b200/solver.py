@@ -56,6 +56,8 @@ class Solver:
             self._check(self.lib.axg_set_moment_sources(h, C.byref(s["ms"])))
         if s["fs"].count:
             self._check(self.lib.axg_set_force_sources(h, C.byref(s["fs"])))
+        if s["ps"].count:
+            self._check(self.lib.axg_set_pressure_sources(h, C.byref(s["ps"])))
         if s["st"].count:
             self._check(self.lib.axg_set_stations(h, C.byref(s["st"]), int(model.st_interval)))
             if getattr(model, "st_gradient", False):

@@ -213,6 +213,21 @@ typedef struct axg_force_sources {
     const int32_t *wavefield;     /* [count]; NULL = 0 */
 } axg_force_sources;
 
+/* fluid-pressure sources (FluidPressure, core/source/elem_src/fluid/FluidPressure.cpp, with
+   the pattern of Mechanism::release, preloop/source/Mechanism.cpp:59-86): each step the
+   fluid points of the element get pattern * STF(t) added to their acceleration after the
+   mass term (FluidPoint::computeStiffToAccel, FluidPoint.cpp:42-48), modes below the
+   point's nu */
+typedef struct axg_pressure_sources {
+    int32_t        count;
+    const int32_t *element;       /* fluid element index */
+    const int32_t *nu;
+    const int64_t *pattern_offset;
+    const double  *pattern;       /* per source [nu][25] complex */
+    const axg_stf *stf;
+    const int32_t *wavefield;     /* [count]; NULL = 0 */
+} axg_pressure_sources;
+
 /* stations: in-plane Lagrange weights and azimuth (Station.hpp:53-72) */
 typedef struct axg_stations {
     int32_t        count;
@@ -278,6 +293,7 @@ int  axg_set_fluid_elements(axg_solver *h, const axg_fluid_elements *e);
 int  axg_set_solid_fluid(axg_solver *h, const axg_solid_fluid *c);
 int  axg_set_moment_sources(axg_solver *h, const axg_moment_sources *s);
 int  axg_set_force_sources(axg_solver *h, const axg_force_sources *s);
+int  axg_set_pressure_sources(axg_solver *h, const axg_pressure_sources *s);
 int  axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interval);
 /* also record the displacement gradient at the stations (StationSolid::record with the
    G / E / R channels, StationSolid.cpp:58-91; SolidElement::getNablaField, :410-446): the

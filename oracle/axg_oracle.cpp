@@ -391,6 +391,13 @@ struct ForceSrc {
     axg_stf stf;
 };
 
+template <class R>
+struct PressureSrc {
+    int elem, nu;
+    std::vector<Cx<R>> pattern;    // [nu][25]
+    axg_stf stf;
+};
+
 struct Station {
     int elem;
     double w[N];
@@ -427,6 +434,7 @@ struct OracleBase {
     virtual void set_solid_fluid(const axg_solid_fluid *) = 0;
     virtual void set_moment_sources(const axg_moment_sources *) = 0;
     virtual void set_force_sources(const axg_force_sources *) = 0;
+    virtual void set_pressure_sources(const axg_pressure_sources *) = 0;
     virtual void set_stations(const axg_stations *, int) = 0;
     virtual void set_clayton(int solid, const axg_clayton *) = 0;
     virtual void set_sponge(int solid, int n, const int32_t *pt, const double *g) = 0;
@@ -469,6 +477,8 @@ struct Oracle : OracleBase {
     std::vector<Couple> sf;
     std::vector<MomentSrc<R>> msrc;
     std::vector<ForceSrc<R>> fsrc;
+    std::vector<PressureSrc<R>> psrc;
+    std::vector<Cx<R>> pressure;          // FluidPoint mPressureSource, per fluid point mode
     std::vector<Station> st;
     int rec_interval = 1;
     std::vector<double> seis;   // [nrec][nst][3]
@@ -665,6 +675,17 @@ struct Oracle : OracleBase {
             fsrc[i].stf = s->stf[i];
         }
     }
+    void set_pressure_sources(const axg_pressure_sources *s) override {
+        psrc.resize(s->count);
+        for (int i = 0; i < s->count; i++) {
+            psrc[i].elem = s->element[i]; psrc[i].nu = s->nu[i];
+            psrc[i].pattern.resize((size_t)psrc[i].nu * N);
+            const double *pp = s->pattern + 2 * s->pattern_offset[i];
+            for (size_t q = 0; q < psrc[i].pattern.size(); q++)
+                psrc[i].pattern[q] = Cx<R>((R)pp[2 * q], (R)pp[2 * q + 1]);
+            psrc[i].stf = s->stf[i];
+        }
+    }
     void set_stations(const axg_stations *s, int interval) override {
         st.resize(s->count);
         for (int i = 0; i < s->count; i++) {
@@ -799,6 +820,18 @@ struct Oracle : OracleBase {
     }
     void apply_sources(int tstep) override {
         double t = time_of(tstep);
+        // FluidPressure::apply -> FluidElement::addPressureSource -> FluidPoint::
+        // addPressureSource (FluidPoint.hpp:113-119): kept until computeStiffToAccel
+        if (!psrc.empty() && pressure.size() != fp.total) pressure.assign(fp.total, Cx<R>(0, 0));
+        for (auto &s : psrc) {
+            FluidElem<R> &el = fe[s.elem];
+            R v = (R)stf_value(s.stf, t);
+            for (int q = 0; q < N; q++) {
+                int p = el.pts[q];
+                int numin = std::min(fp.nu[p], s.nu);
+                for (int a = 0; a < numin; a++) pressure[(size_t)fp.off[p] + a] += s.pattern[(size_t)a * N + q] * v;
+            }
+        }
         // SolidMoment::apply -> SolidElement::addMomentSource (SolidElement.cpp:273-356)
         for (auto &s : msrc) {
             SolidElem<R> &el = se[s.elem];
@@ -1543,6 +1576,12 @@ struct Oracle : OracleBase {
     void stiff_to_accel() override {
         points_to_accel(sp);
         points_to_accel(fp);
+        // FluidPoint::computeStiffToAccel (FluidPoint.cpp:42-48): the pressure source is added
+        // to the new acceleration and zeroed for the next step
+        for (size_t i = 0; i < pressure.size(); i++) {
+            fp.stiff[i] += pressure[i];
+            pressure[i] = Cx<R>(0, 0);
+        }
         const R two = 2;
         for (auto &g : sgs) {
             size_t o = (size_t)sp.off[g.first] * 3;
@@ -1816,6 +1855,7 @@ int axo_set_fluid_elements(void *h, const axg_fluid_elements *e) { AXO_TRY(stati
 int axo_set_solid_fluid(void *h, const axg_solid_fluid *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_solid_fluid(c)) }
 int axo_set_moment_sources(void *h, const axg_moment_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_moment_sources(s)) }
 int axo_set_force_sources(void *h, const axg_force_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_force_sources(s)) }
+int axo_set_pressure_sources(void *h, const axg_pressure_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_pressure_sources(s)) }
 int axo_set_stations(void *h, const axg_stations *s, int interval) { AXO_TRY(static_cast<OracleBase *>(h)->set_stations(s, interval)) }
 int axo_set_clayton(void *h, int solid, const axg_clayton *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton(solid, c)) }
 int axo_set_sponge(void *h, int solid, int n, const int32_t *pt, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge(solid, n, pt, g)) }

@@ -48,6 +48,7 @@ def lib():
             "axo_set_solid_fluid": (C.c_int, [V, C.POINTER(L.axg_solid_fluid)]),
             "axo_set_moment_sources": (C.c_int, [V, C.POINTER(L.axg_moment_sources)]),
             "axo_set_force_sources": (C.c_int, [V, C.POINTER(L.axg_force_sources)]),
+            "axo_set_pressure_sources": (C.c_int, [V, C.POINTER(L.axg_pressure_sources)]),
             "axo_set_stations": (C.c_int, [V, C.POINTER(L.axg_stations), C.c_int]),
             "axo_apply_sources": (C.c_int, [V, C.c_int]),
             "axo_set_clayton": (C.c_int, [V, C.c_int, C.POINTER(L.axg_clayton)]),
@@ -108,6 +109,8 @@ class Oracle:
         self._chk(self.O.axo_set_solid_fluid(self.h, C.byref(s["sf"])))
         self._chk(self.O.axo_set_moment_sources(self.h, C.byref(s["ms"])))
         self._chk(self.O.axo_set_force_sources(self.h, C.byref(s["fs"])))
+        if s["ps"].count:
+            self._chk(self.O.axo_set_pressure_sources(self.h, C.byref(s["ps"])))
         self._chk(self.O.axo_set_stations(self.h, C.byref(s["st"]), int(model.st_interval)))
         for solid, key in ((1, "cl_s"), (0, "cl_f")):
             if s[key].count:

@@ -147,3 +147,18 @@ def test_geometric_model_errors(built, tmp_path):
     d = _box_with(_box(str(tmp_path / "input2")), [fx.ellipticity_yaml("a"), fx.ellipticity_yaml("b")])
     with pytest.raises(preloop.PreloopError, match="cannot be added more than once"):
         preloop.build(d, max_steps=10)
+
+
+def test_fluid_pressure_pattern_on_the_axis(built, tmp_path):
+    """Mechanism::release (Mechanism.cpp:59-86) for a pressure on the axis: a monopole on
+    the element's axis points, P w / (2 pi), in the fluid element that holds it."""
+    from axisem3d_b200 import preloop
+    from test_gpu_preloop import _pressure_source
+    sim = preloop.build(_pressure_source(_shell(str(tmp_path / "input"))), max_steps=10)
+    m = sim.model
+    assert len(m.ps_elem) == 1 and len(m.ms_elem) == 0 and len(m.fs_elem) == 0
+    e = int(m.ps_elem[0])
+    assert m.fe_axial[e] == 1 and m.ps_nu[0] == 1
+    pat = m.ps_pattern.reshape(1, 25)
+    assert np.all(pat[0, 5:] == 0) and np.all(pat.imag == 0)
+    assert abs(pat[0].real.sum() * 2. * math.pi / 1e12 - 1.) < 1e-9

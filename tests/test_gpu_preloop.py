@@ -370,3 +370,36 @@ def test_simulation_with_geometric_and_ocean_models_matches_oracle(built, tmp_pa
         assert np.array_equal(t, t_ref) and np.abs(w_ref).max() > 0
         err = float(np.linalg.norm(w - w_ref) / np.linalg.norm(w_ref))
         assert err <= TOL[precision], (name, err)
+
+
+def _pressure_source(d, depth=2831e3):
+    """Turn the input's moment tensor into a FLUID_PRESSURE source inside the fluid layer."""
+    p = os.path.join(d, "inparam.source.yaml")
+    with open(p) as f:
+        txt = f.read()
+    i = txt.index("depth:")
+    j = txt.index("\n", i)
+    txt = txt[:i] + "depth: %r" % depth + txt[j:]
+    i = txt.index("type: MOMENT_TENSOR")
+    j = txt.index("unit:", i)
+    txt = txt[:i] + "type: FLUID_PRESSURE\n            data: [1e12]\n            " + txt[j:]
+    with open(p, "w") as f:
+        f.write(txt)
+    return d
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fluid_pressure_source_matches_oracle(built, tmp_path, precision):
+    """FLUID_PRESSURE (Mechanism::release's pressure pattern, FluidPressure::apply) in the
+    shell's fluid layer: the pressure goes to the fluid acceleration after the mass term."""
+    from axisem3d_b200 import simulation
+    d = _pressure_source(_shell(str(tmp_path / "input")))
+    res = simulation.run(d, None, precision=precision)
+    m = res.sim.model
+    assert len(m.ps_elem) == 1 and len(m.ms_elem) == 0
+    ref = _oracle_traces(res.sim)
+    for name, (t_ref, w_ref) in ref.items():
+        t, w = res.traces[name]
+        assert np.array_equal(t, t_ref) and np.abs(w_ref).max() > 0
+        err = float(np.linalg.norm(w - w_ref) / np.linalg.norm(w_ref))
+        assert err <= TOL[precision], (name, err)
