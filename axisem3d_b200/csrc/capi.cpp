@@ -268,6 +268,30 @@ int axg_set_pressure_sources(axg_solver *h, const axg_pressure_sources *s) {
     });
 }
 
+int axg_set_stf_table(axg_solver *h, int32_t kind, int32_t index, int32_t n, const double *times,
+                      const double *values, int32_t padding, double left, double right, int32_t pad_first) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (kind < 0 || kind > 2 || !times || !values)
+            throw axg::Error(AXG_E_ARG, "STF::buildInparam || bad STF table arguments.");
+        axg::HostSources &src = kind == 0 ? h->model.ms : kind == 1 ? h->model.fs : h->model.ps;
+        if (index < 0 || index >= src.count)
+            throw axg::Error(AXG_E_ARG, "STF::buildInparam || source index out of range.");
+        if (n < 2)
+            throw axg::Error(AXG_E_ARG, "StreamSTF::StreamSTF || Insufficient time points, at least 2.");
+        for (int i = 1; i < n; i++)
+            if (!(times[i] > times[i - 1]))
+                throw axg::Error(AXG_E_ARG, "StreamSTF::StreamSTF || Time points are not ascendingly sorted.");
+        axg::HostStfTable tb;
+        tb.t.assign(times, times + n);
+        tb.v.assign(values, values + n);
+        tb.padding = padding != 0;
+        tb.left = left; tb.right = right;
+        tb.pad_first = pad_first != 0;
+        src.table[index] = tb;
+    });
+}
+
 int axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interval) {
     return guarded(h, [&] {
         need_open(h);

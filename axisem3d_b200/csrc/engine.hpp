@@ -8,6 +8,8 @@
 #include <stdexcept>
 #include <string>
 #include <vector>
+#include <map>
+#include <algorithm>
 
 namespace axg {
 
@@ -51,12 +53,44 @@ struct HostCoupling {
     std::vector<double> nsu, nzu, nsa, nza, mf;
 };
 
+// StreamSTF / NetCDF_STF table (core/source/elem_src/stf/StreamSTF.cpp, NetCDF_STF.cpp)
+struct HostStfTable {
+    std::vector<double> t, v;
+    int padding = 0;               // 0: out of range is an error; 1: left / right values
+    double left = 0, right = 0;
+    int pad_first = 0;             // NetCDF_STF: padding tested before the interpolation
+};
+
+// StreamSTF::getValue / NetCDF_STF::getValue with vector_tools::linearInterpSorted (range x
+// 1e-12 tolerance): samples in Real, combined in double, cast to Real
+template <class T>
+inline T stf_table_value(const HostStfTable &tb, double time) {
+    const size_t n = tb.t.size();
+    if (tb.pad_first && tb.padding) {
+        if (time < tb.t.front()) return (T)tb.left;
+        if (time > tb.t.back()) return (T)tb.right;
+    }
+    const double tol = (tb.t.back() - tb.t.front()) * 1e-12;
+    if (time < tb.t.front() - tol || time > tb.t.back() + tol) {
+        if (!tb.padding)
+            throw Error(AXG_E_ARG, "StreamSTF::getValue || Time is out of range with padding disabled.");
+        return (T)(time < tb.t.front() ? tb.left : tb.right);
+    }
+    size_t i1 = (size_t)(std::upper_bound(tb.t.begin(), tb.t.end(), time) - tb.t.begin());
+    if (i1 == 0) i1++;
+    else if (i1 == n) i1--;
+    const size_t i0 = i1 - 1;
+    const double f1 = (time - tb.t[i0]) / (tb.t[i1] - tb.t[i0]), f0 = 1. - f1;
+    return (T)(f0 * (double)(T)tb.v[i0] + f1 * (double)(T)tb.v[i1]);
+}
+
 struct HostSources {
     int count = 0;
     std::vector<int> elem, nu, wave;
     std::vector<int64_t> pat_off;
     std::vector<double> pattern;   // (re, im) pairs
     std::vector<axg_stf> stf;
+    std::map<int, HostStfTable> table;   // sources whose STF is a table
 };
 
 struct HostStations {

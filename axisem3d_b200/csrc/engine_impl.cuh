@@ -1571,6 +1571,10 @@ private:
         }
         if (changed && graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
     }
+    static T src_stf(const HostSources &h, int i, double t) {
+        auto it = h.table.find(i);
+        return it == h.table.end() ? (T)stf_value(h.stf[i], t) : stf_table_value<T>(it->second, t);
+    }
     static double stf_value(const axg_stf &s, double time) {
         // GaussianSTF::getValue (GaussianSTF.hpp:35-58)
         const double invSqrtPi = 1. / std::sqrt(M_PI);
@@ -1590,9 +1594,9 @@ private:
             ps((size_t)cap * std::max(ps_n_, 1));
         double t = cfg_.t0;
         for (int k = 0; k < cap; k++) {
-            for (int i = 0; i < ms_n_; i++) ms[(size_t)k * ms_n_ + i] = (T)stf_value(model_.ms.stf[i], t);
-            for (int i = 0; i < fs_n_; i++) fs[(size_t)k * fs_n_ + i] = (T)stf_value(model_.fs.stf[i], t);
-            for (int i = 0; i < ps_n_; i++) ps[(size_t)k * ps_n_ + i] = (T)stf_value(model_.ps.stf[i], t);
+            for (int i = 0; i < ms_n_; i++) ms[(size_t)k * ms_n_ + i] = src_stf(model_.ms, i, t);
+            for (int i = 0; i < fs_n_; i++) fs[(size_t)k * fs_n_ + i] = src_stf(model_.fs, i, t);
+            for (int i = 0; i < ps_n_; i++) ps[(size_t)k * ps_n_ + i] = src_stf(model_.ps, i, t);
             t += cfg_.dt;
         }
         ms_stf_.upload(ms);

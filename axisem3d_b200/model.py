@@ -33,11 +33,24 @@ def _f64(a):
 
 @dataclass
 class STF:
-    """GaussianSTF parameters (GaussianSTF.hpp:35-58)."""
-    half_duration: float
-    decay_factor: float
-    time_shift: float
+    """GaussianSTF parameters (GaussianSTF.hpp:35-58), or a StreamSTF / NetCDF_STF table:
+    `table` = (times, values), padding 0 (none) or 1 (left / right values), and pad_first
+    for NetCDF_STF's order of tests."""
+    half_duration: float = 0.0
+    decay_factor: float = 0.0
+    time_shift: float = 0.0
     derivative_order: int = 2
+    table: Optional[tuple] = None
+    padding: int = 0
+    left: float = 0.0
+    right: float = 0.0
+    pad_first: int = 0
+
+    def start_time(self):
+        """STF::getStartTime: -2.5 half durations + shift (Gaussian) or the first time."""
+        if self.table is not None:
+            return float(self.table[0][0])
+        return -self.half_duration * 2.5 + self.time_shift
 
 
 @dataclass

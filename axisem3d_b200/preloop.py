@@ -452,12 +452,52 @@ class Simulation:
     element_groups: List["ElementGroup"] = field(default_factory=list)
 
 
-def _read_stf(gm, root, name, dt):
-    """STF::buildInparam (core/source/elem_src/stf/STF.cpp:19-40), GaussianSTF."""
+def _read_stf(gm, root, name, dt, path=None):
+    """STF::buildInparam (core/source/elem_src/stf/STF.cpp:19-70): GaussianSTF, or a table
+    from StreamSTF (two ascii columns, '#' comments) or NetCDF_STF (two variables)."""
     cls = gm.get(root + ":class_name")
+    if cls in ("StreamSTF", "NetCDF_STF"):
+        pad = gm.get(root + ":padding")
+        padding, left, right = 0, 0., 0.
+        if pad == "FIRST_LAST":
+            padding = 1
+        elif pad != "NONE":
+            padding = 1
+            left, right = gm.get(root + ":padding:[0]", float), gm.get(root + ":padding:[1]", float)
+        if cls == "StreamSTF":
+            fname = path(gm.get(root + ":ascii_data_file"))
+            t, v = [], []
+            with open(fname) as f:
+                for line in f:
+                    w = line.split()
+                    if not w or w[0].startswith("#"):
+                        continue
+                    if len(w) != 2:
+                        raise PreloopError("StreamSTF::StreamSTF || Input file for STF must contain two "
+                                           "columns. || Ascii file: " + fname)
+                    t.append(float(w[0]))
+                    v.append(float(w[1]))
+            where = "StreamSTF::StreamSTF"
+        else:
+            from .models3d import _read_nc
+            fname = path(gm.get(root + ":nc_data_file"))
+            nc = _read_nc(fname)
+            t = list(np.asarray(nc[gm.get(root + ":nc_var_times")], np.float64).ravel())
+            v = list(np.asarray(nc[gm.get(root + ":nc_var_data")], np.float64).ravel())
+            where = "NetCDF_STF::NetCDF_STF"
+            if len(t) != len(v):
+                raise PreloopError(where + " || Times and values have different lengths. || NetCDF file: " + fname)
+        if len(t) < 2:
+            raise PreloopError(where + " || Insufficient time points, at least 2. || File: " + fname)
+        if np.any(np.diff(t) <= 0):
+            raise PreloopError(where + " || Time points are not ascendingly sorted. || File: " + fname)
+        if pad == "FIRST_LAST":
+            left, right = v[0], v[-1]
+        return STF(table=(np.array(t), np.array(v)), padding=padding, left=left, right=right,
+                   pad_first=int(cls == "NetCDF_STF"))
     if cls != "GaussianSTF":
-        raise PreloopError("STF::buildInparam || class_name %s is not supported by this build "
-                           "(GaussianSTF only). || Source name: %s" % (cls, name))
+        raise PreloopError("STF::buildInparam || Unknown class of source-time function. || Source name: "
+                           "%s || STF class name: %s" % (name, cls))
     hdur = gm.get_bounded(root + ":half_duration", 0.)
     hdur = max(hdur, dt * 5.)                     # dt * 5 as the minimum
     decay = gm.get_bounded(root + ":decay_factor", 0.)
@@ -1838,8 +1878,8 @@ def _release_sources(inp, m, ctx, geo, enr, solid_q, dt, und_ctx=None):
             raise PreloopError("Source::release || Error locating source in mesh. || "
                                "Source index = %d || Source name  = %s" % (k, name))
         w = ctx.weights(q, xe)
-        stf = _read_stf(gm, root + ":source_time_function", name, dt)
-        t0 = min(t0, -stf.half_duration * 2.5 + stf.time_shift)
+        stf = _read_stf(gm, root + ":source_time_function", name, dt, inp.path)
+        t0 = min(t0, stf.start_time())
         Q = _qzsp(geo, spz, axial, centered, crd, use_depth, depth_solid, ellip)
         nu_1 = int(enr[q]) // 2 + 1
         e = int(ctx.fluid_index[q] if mtype == "P" else ctx.solid_index[q])

@@ -58,6 +58,13 @@ class Solver:
             self._check(self.lib.axg_set_force_sources(h, C.byref(s["fs"])))
         if s["ps"].count:
             self._check(self.lib.axg_set_pressure_sources(h, C.byref(s["ps"])))
+        for kind, lst in enumerate((model.ms_stf, model.fs_stf, model.ps_stf)):
+            for i, st in enumerate(lst):
+                if getattr(st, "table", None) is not None:
+                    tt = np.ascontiguousarray(st.table[0], np.float64)
+                    vv = np.ascontiguousarray(st.table[1], np.float64)
+                    self._check(self.lib.axg_set_stf_table(h, kind, i, len(tt), tt.ctypes.data_as(L.P_f64), vv.ctypes.data_as(L.P_f64),
+                        int(st.padding), float(st.left), float(st.right), int(st.pad_first)))
         if s["st"].count:
             self._check(self.lib.axg_set_stations(h, C.byref(s["st"]), int(model.st_interval)))
             if getattr(model, "st_gradient", False):

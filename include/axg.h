@@ -294,6 +294,13 @@ int  axg_set_solid_fluid(axg_solver *h, const axg_solid_fluid *c);
 int  axg_set_moment_sources(axg_solver *h, const axg_moment_sources *s);
 int  axg_set_force_sources(axg_solver *h, const axg_force_sources *s);
 int  axg_set_pressure_sources(axg_solver *h, const axg_pressure_sources *s);
+/* StreamSTF / NetCDF_STF (core/source/elem_src/stf/StreamSTF.cpp:63-93, NetCDF_STF.cpp:
+   92-140): source `index` of `kind` (0 moment, 1 force, 2 pressure) takes its STF by linear
+   interpolation in n (times, values), times ascending; outside them an error (padding 0) or
+   left / right (padding 1, FIRST_LAST passes the first and last values); pad_first 1 tests
+   the padding before the interpolation as NetCDF_STF does. Call after the sources. */
+int  axg_set_stf_table(axg_solver *h, int32_t kind, int32_t index, int32_t n, const double *times,
+                       const double *values, int32_t padding, double left, double right, int32_t pad_first);
 int  axg_set_stations(axg_solver *h, const axg_stations *s, int32_t record_interval);
 /* also record the displacement gradient at the stations (StationSolid::record with the
    G / E / R channels, StationSolid.cpp:58-91; SolidElement::getNablaField, :410-446): the

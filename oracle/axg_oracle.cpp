@@ -419,6 +419,34 @@ double stf_value(const axg_stf &s, double time) {
     throw std::runtime_error("GaussianSTF::getValue || Unsupported derivative order.");
 }
 
+// StreamSTF::getValue (StreamSTF.cpp:63-93) / NetCDF_STF::getValue (NetCDF_STF.cpp:92-140),
+// vector_tools::linearInterpSorted (vector_tools.hpp:23-66): samples in Real, combined in
+// double
+struct StfTable {
+    std::vector<double> t, v;
+    int padding = 0, pad_first = 0;
+    double left = 0, right = 0;
+};
+template <class R>
+R stf_table_value(const StfTable &tb, double time) {
+    const size_t n = tb.t.size();
+    if (tb.pad_first && tb.padding) {
+        if (time < tb.t.front()) return (R)tb.left;
+        if (time > tb.t.back()) return (R)tb.right;
+    }
+    const double tol = (tb.t.back() - tb.t.front()) * 1e-12;
+    if (time < tb.t.front() - tol || time > tb.t.back() + tol) {
+        if (!tb.padding) throw std::runtime_error("StreamSTF::getValue || Time is out of range with padding disabled.");
+        return (R)(time < tb.t.front() ? tb.left : tb.right);
+    }
+    size_t i1 = (size_t)(std::upper_bound(tb.t.begin(), tb.t.end(), time) - tb.t.begin());
+    if (i1 == 0) i1++;
+    else if (i1 == n) i1--;
+    const size_t i0 = i1 - 1;
+    const double f1 = (time - tb.t[i0]) / (tb.t[i1] - tb.t[i0]), f0 = 1. - f1;
+    return (R)(f0 * (double)(R)tb.v[i0] + f1 * (double)(R)tb.v[i1]);
+}
+
 int nmod_of(int rheo) { return rheo == AXG_ISO ? 2 : (rheo == AXG_TISO ? 5 : 21); }
 
 // ---------------------------------------------------------------------------
@@ -435,6 +463,8 @@ struct OracleBase {
     virtual void set_moment_sources(const axg_moment_sources *) = 0;
     virtual void set_force_sources(const axg_force_sources *) = 0;
     virtual void set_pressure_sources(const axg_pressure_sources *) = 0;
+    virtual void set_stf_table(int kind, int index, int n, const double *t, const double *v, int padding,
+                               double left, double right, int pad_first) = 0;
     virtual void set_stations(const axg_stations *, int) = 0;
     virtual void set_clayton(int solid, const axg_clayton *) = 0;
     virtual void set_sponge(int solid, int n, const int32_t *pt, const double *g) = 0;
@@ -478,6 +508,19 @@ struct Oracle : OracleBase {
     std::vector<MomentSrc<R>> msrc;
     std::vector<ForceSrc<R>> fsrc;
     std::vector<PressureSrc<R>> psrc;
+    std::map<int, StfTable> stf_tab[3];   // moment, force, pressure sources with a table STF
+    R src_stf(int kind, int i, const axg_stf &g, double t) const {
+        auto it = stf_tab[kind].find(i);
+        return it == stf_tab[kind].end() ? (R)stf_value(g, t) : stf_table_value<R>(it->second, t);
+    }
+    void set_stf_table(int kind, int index, int n, const double *t, const double *v, int padding, double left,
+                       double right, int pad_first) override {
+        StfTable tb;
+        tb.t.assign(t, t + n);
+        tb.v.assign(v, v + n);
+        tb.padding = padding; tb.left = left; tb.right = right; tb.pad_first = pad_first;
+        stf_tab[kind][index] = tb;
+    }
     std::vector<Cx<R>> pressure;          // FluidPoint mPressureSource, per fluid point mode
     std::vector<Station> st;
     int rec_interval = 1;
@@ -823,9 +866,10 @@ struct Oracle : OracleBase {
         // FluidPressure::apply -> FluidElement::addPressureSource -> FluidPoint::
         // addPressureSource (FluidPoint.hpp:113-119): kept until computeStiffToAccel
         if (!psrc.empty() && pressure.size() != fp.total) pressure.assign(fp.total, Cx<R>(0, 0));
-        for (auto &s : psrc) {
+        for (size_t si = 0; si < psrc.size(); si++) {
+            auto &s = psrc[si];
             FluidElem<R> &el = fe[s.elem];
-            R v = (R)stf_value(s.stf, t);
+            R v = src_stf(2, (int)si, s.stf, t);
             for (int q = 0; q < N; q++) {
                 int p = el.pts[q];
                 int numin = std::min(fp.nu[p], s.nu);
@@ -833,9 +877,10 @@ struct Oracle : OracleBase {
             }
         }
         // SolidMoment::apply -> SolidElement::addMomentSource (SolidElement.cpp:273-356)
-        for (auto &s : msrc) {
+        for (size_t si = 0; si < msrc.size(); si++) {
+            auto &s = msrc[si];
             SolidElem<R> &el = se[s.elem];
-            R v = (R)stf_value(s.stf, t);
+            R v = src_stf(0, (int)si, s.stf, t);
             int nu_co = std::min(el.nu, s.nu);
             std::vector<CM<R>> stress(6);
             Grad<R> g{el.ops, gm};
@@ -854,9 +899,10 @@ struct Oracle : OracleBase {
             }
         }
         // SolidForce::apply -> SolidPoint::addForceSource (SolidPoint.hpp:112-119)
-        for (auto &s : fsrc) {
+        for (size_t si = 0; si < fsrc.size(); si++) {
+            auto &s = fsrc[si];
             SolidElem<R> &el = se[s.elem];
-            R v = (R)stf_value(s.stf, t);
+            R v = src_stf(1, (int)si, s.stf, t);
             for (int q = 0; q < N; q++) {
                 int p = el.pts[q];
                 int numin = std::min(sp.nu[p], s.nu);
@@ -1856,6 +1902,10 @@ int axo_set_solid_fluid(void *h, const axg_solid_fluid *c) { AXO_TRY(static_cast
 int axo_set_moment_sources(void *h, const axg_moment_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_moment_sources(s)) }
 int axo_set_force_sources(void *h, const axg_force_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_force_sources(s)) }
 int axo_set_pressure_sources(void *h, const axg_pressure_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_pressure_sources(s)) }
+int axo_set_stf_table(void *h, int kind, int index, int n, const double *t, const double *v, int padding, double left,
+                      double right, int pad_first) {
+    AXO_TRY(static_cast<OracleBase *>(h)->set_stf_table(kind, index, n, t, v, padding, left, right, pad_first))
+}
 int axo_set_stations(void *h, const axg_stations *s, int interval) { AXO_TRY(static_cast<OracleBase *>(h)->set_stations(s, interval)) }
 int axo_set_clayton(void *h, int solid, const axg_clayton *c) { AXO_TRY(static_cast<OracleBase *>(h)->set_clayton(solid, c)) }
 int axo_set_sponge(void *h, int solid, int n, const int32_t *pt, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge(solid, n, pt, g)) }

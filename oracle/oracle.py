@@ -49,6 +49,8 @@ def lib():
             "axo_set_moment_sources": (C.c_int, [V, C.POINTER(L.axg_moment_sources)]),
             "axo_set_force_sources": (C.c_int, [V, C.POINTER(L.axg_force_sources)]),
             "axo_set_pressure_sources": (C.c_int, [V, C.POINTER(L.axg_pressure_sources)]),
+            "axo_set_stf_table": (C.c_int, [V, C.c_int, C.c_int, C.c_int, L.P_f64, L.P_f64, C.c_int, C.c_double,
+                                            C.c_double, C.c_int]),
             "axo_set_stations": (C.c_int, [V, C.POINTER(L.axg_stations), C.c_int]),
             "axo_apply_sources": (C.c_int, [V, C.c_int]),
             "axo_set_clayton": (C.c_int, [V, C.c_int, C.POINTER(L.axg_clayton)]),
@@ -111,6 +113,13 @@ class Oracle:
         self._chk(self.O.axo_set_force_sources(self.h, C.byref(s["fs"])))
         if s["ps"].count:
             self._chk(self.O.axo_set_pressure_sources(self.h, C.byref(s["ps"])))
+        for kind, lst in enumerate((model.ms_stf, model.fs_stf, model.ps_stf)):
+            for i, st in enumerate(lst):
+                if getattr(st, "table", None) is not None:
+                    tt = np.ascontiguousarray(st.table[0], np.float64)
+                    vv = np.ascontiguousarray(st.table[1], np.float64)
+                    self._chk(self.O.axo_set_stf_table(self.h, kind, i, len(tt), tt.ctypes.data_as(L.P_f64), vv.ctypes.data_as(L.P_f64),
+                        int(st.padding), float(st.left), float(st.right), int(st.pad_first)))
         self._chk(self.O.axo_set_stations(self.h, C.byref(s["st"]), int(model.st_interval)))
         for solid, key in ((1, "cl_s"), (0, "cl_f")):
             if s[key].count:

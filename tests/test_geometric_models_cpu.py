@@ -162,3 +162,20 @@ def test_fluid_pressure_pattern_on_the_axis(built, tmp_path):
     pat = m.ps_pattern.reshape(1, 25)
     assert np.all(pat[0, 5:] == 0) and np.all(pat.imag == 0)
     assert abs(pat[0].real.sum() * 2. * math.pi / 1e12 - 1.) < 1e-9
+
+
+def test_table_stf_parsing_and_errors(built, tmp_path):
+    """STF::buildInparam for StreamSTF / NetCDF_STF: padding modes and the file checks."""
+    from axisem3d_b200 import preloop
+    from test_gpu_preloop import _table_stf
+    d, t, v = _table_stf(_box(str(tmp_path / "a")), "StreamSTF", "[0.5, -0.25]")
+    st = preloop.build(d, max_steps=5).model.ms_stf[0]
+    assert (st.padding, st.left, st.right, st.pad_first) == (1, 0.5, -0.25, 0)
+    assert np.array_equal(st.table[0], t) and np.allclose(st.table[1], v, rtol=0, atol=1e-15)
+    d, t, v = _table_stf(_box(str(tmp_path / "b")), "NetCDF_STF", "NONE")
+    st = preloop.build(d, max_steps=5).model.ms_stf[0]
+    assert (st.padding, st.pad_first) == (0, 1)
+    with open(os.path.join(str(tmp_path / "a"), "stf.txt"), "a") as f:
+        f.write("1.0 2.0 3.0\n")
+    with pytest.raises(preloop.PreloopError, match="two columns"):
+        preloop.build(str(tmp_path / "a"), max_steps=5)

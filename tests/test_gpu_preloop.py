@@ -403,3 +403,49 @@ def test_fluid_pressure_source_matches_oracle(built, tmp_path, precision):
         assert np.array_equal(t, t_ref) and np.abs(w_ref).max() > 0
         err = float(np.linalg.norm(w - w_ref) / np.linalg.norm(w_ref))
         assert err <= TOL[precision], (name, err)
+
+
+def _table_stf(d, cls="StreamSTF", padding="FIRST_LAST"):
+    """Replace the Gaussian STF of the input's source by a table: a Ricker-like wavelet
+    sampled every 0.37 s (not a multiple of dt), as an ascii file or a NetCDF file."""
+    t = np.arange(-3.0, 9.0, 0.37)
+    v = (1. - 2. * (math.pi * 0.8 * (t - 1.)) ** 2) * np.exp(-(math.pi * 0.8 * (t - 1.)) ** 2)
+    if cls == "StreamSTF":
+        with open(os.path.join(d, "stf.txt"), "w") as f:
+            f.write("# time value\n")
+            for a, b in zip(t, v):
+                f.write("%.17g %.17g\n" % (a, b))
+        spec = "class_name: StreamSTF\n            ascii_data_file: stf.txt\n"
+    else:
+        fx.write_grid_v3d(os.path.join(d, "stf.nc"), {"time": t}, {"stf": v}, ["time"])
+        spec = ("class_name: NetCDF_STF\n            nc_data_file: stf.nc\n            nc_var_times: time\n"
+                "            nc_var_data: stf\n            chunk_size: NONE\n")
+    p = os.path.join(d, "inparam.source.yaml")
+    with open(p) as f:
+        txt = f.read()
+    i = txt.index("class_name: GaussianSTF")
+    j = txt.index("use_derivative_integral:", i)
+    j = txt.index("\n", j) + 1
+    txt = txt[:i] + spec + "            padding: %s\n" % padding + txt[j:]
+    with open(p, "w") as f:
+        f.write(txt)
+    return d, t, v
+
+
+@pytest.mark.parametrize("cls", ["StreamSTF", "NetCDF_STF"])
+def test_table_stf_matches_oracle(built, tmp_path, cls):
+    """StreamSTF / NetCDF_STF: the table is interpolated at the accumulated step times (in
+    the engine's STF table and in the oracle alike); the run starts at the first sample."""
+    from axisem3d_b200 import simulation
+    d, t, v = _table_stf(_box(str(tmp_path / "input")), cls)
+    res = simulation.run(d, None, precision="fp64", max_steps=60)
+    sim = res.sim
+    st = sim.model.ms_stf[0]
+    assert st.table is not None and st.padding == 1 and st.pad_first == int(cls == "NetCDF_STF")
+    assert sim.t0 == math.floor(t[0] / sim.dt) * sim.dt
+    ref = _oracle_traces(sim)
+    for name, (t_ref, w_ref) in ref.items():
+        tt, w = res.traces[name]
+        assert np.array_equal(tt, t_ref) and np.abs(w_ref).max() > 0
+        err = float(np.linalg.norm(w - w_ref) / np.linalg.norm(w_ref))
+        assert err <= TOL["fp64"], (name, err)
