@@ -1,18 +1,21 @@
-"""Volumetric 3-D models on structured grids (the reference's StructuredGridV3D), for the
-preloop.
+"""3-D models on structured grids for the preloop: volumetric (StructuredGridV3D), geometric
+(StructuredGridG3D, Ellipticity) and ocean-load (StructuredGridO3D) models of the reference.
 
 Follows SOLVER/src/models3D: Model3D::buildInparam and computeElemSPZ (Model3D.cpp),
 Volumetric3D::buildInparam (volumetric/Volumetric3D.cpp:135-200), StructuredGridV3D
-(volumetric/StructuredGridV3D.cpp: constructor, getProperties), sg_tools.hpp (inparam
-parsing, units, longitude range), Model3D.hpp (inplaneScope, coordsFromMeshToModel) and
-StructuredGrid.hpp (reading with the data-rank shuffle; multilinear interpolation with
-vector_tools::linearInterpSorted factors). The properties a grid returns are applied to
-the quads by preloop.py as Material::addProperty3D does.
+(volumetric/StructuredGridV3D.cpp: constructor, getProperties), Geometric3D::buildInparam
+(geometric/Geometric3D.cpp:115-190), StructuredGridG3D::getUndulation, Ellipticity::
+getUndulation, OceanLoad3D::buildInparam and StructuredGridO3D::getSumRhoDepth, sg_tools.hpp
+(inparam parsing, units, longitude range), Model3D.hpp (inplaneScope, coordsFromMeshToModel)
+and StructuredGrid.hpp (reading with the data-rank shuffle; multilinear interpolation with
+vector_tools::linearInterpSorted factors). What a model returns is applied to the quads by
+preloop.py: properties as Material::addProperty3D does, undulation as Undulation::
+addUndulation, sum(rho * depth) as OceanLoad::addSumRhoDepth.
 
 Supported: horizontal LATITUDE_LONGITUDE / DISTANCE_AZIMUTH / XY_CARTESIAN, vertical DEPTH /
-RADIUS, length and angle units, whole_element_inplane, reference kinds ABS / REF1D / REF3D /
-REF_PERTURB, properties RHO, VP, VS, VPV, VPH, VSV, VSH, ETA, QMU, QKAPPA. Cij properties,
-geometric and ocean-load 3-D models raise `Model3DError`.
+RADIUS, length and angle units, whole_element_inplane, undulated_geometry, reference kinds
+ABS / REF1D / REF3D / REF_PERTURB, properties RHO, VP, VS, VPV, VPH, VSV, VSH, ETA, QMU,
+QKAPPA. Cij properties raise `Model3DError`.
 """
 from __future__ import annotations
 
@@ -62,7 +65,7 @@ class _LazyH5(dict):
 class StructuredGrid:
     """StructuredGrid<D, double>: coordinates, data [nvar, n0, n1, ...] and multilinear
     interpolation; a coordinate outside its axis (beyond the end by more than the range
-    times machine epsilon) is out of range."""
+    times 1e-12, as vector_tools::linearInterpSorted allows) is out of range."""
 
     def __init__(self, path, coord_vars, data_info, shuffle):
         if sorted(shuffle) != list(range(len(coord_vars))):
@@ -105,7 +108,7 @@ class StructuredGrid:
         i0s, f1s = [], []
         for d in range(D):
             c = self.coords[d]
-            tol = (c[-1] - c[0]) * EPS
+            tol = (c[-1] - c[0]) * DEPS                # vector_tools::linearInterpSorted
             x = crd[:, d]
             bad = (x < c[0] - tol) | (x > c[-1] + tol)
             dim_out = np.where(ok & bad, d, dim_out)
