@@ -121,6 +121,7 @@ SIGNATURES = {
     "axg_set_moment_sources": (C.c_int, [H, C.POINTER(axg_moment_sources)]),
     "axg_set_force_sources": (C.c_int, [H, C.POINTER(axg_force_sources)]),
     "axg_set_pressure_sources": (C.c_int, [H, C.POINTER(axg_pressure_sources)]),
+    "axg_set_solid_fluid3d": (C.c_int, [H, C.c_int32, P_i32, P_i32, P_i64, C.c_int64, P_f64, P_f64, P_f64]),
     "axg_set_stf_table": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, P_f64, P_f64, C.c_int32, C.c_double,
                                      C.c_double, C.c_int32]),
     "axg_set_stations": (C.c_int, [H, C.POINTER(axg_stations), C.c_int32]),

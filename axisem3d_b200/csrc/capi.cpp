@@ -431,6 +431,29 @@ int axg_scanning_nr(axg_solver *h, int32_t *solid_nr, int32_t *fluid_nr) {
     });
 }
 
+int axg_set_solid_fluid3d(axg_solver *h, int32_t count, const int32_t *solid_point, const int32_t *fluid_point,
+                          const int64_t *offset, int64_t nvalues, const double *normal_u, const double *normal_a,
+                          const double *mass_fluid) {
+    return guarded(h, [&] {
+        need_open(h);
+        if (count < 0 || nvalues < 0 ||
+            (count && (!solid_point || !fluid_point || !offset || !normal_u || !normal_a || !mass_fluid)))
+            throw axg::Error(AXG_E_ARG, "SolidFluidCoupling3D || missing array.");
+        axg::HostCoupling3D &x = h->model.sf3;
+        x.count = count;
+        x.sp = copy(solid_point, count);
+        x.fp = copy(fluid_point, count);
+        x.off = copy(offset, count);
+        x.nu3.resize((size_t)nvalues * 3);
+        x.na3.resize((size_t)nvalues * 3);
+        for (int64_t k = 0; k < nvalues; k++)
+            for (int c = 0; c < 3; c++) {
+                x.nu3[(size_t)k * 3 + c] = normal_u[(size_t)k * 3 + c];
+                x.na3[(size_t)k * 3 + c] = normal_a[(size_t)k * 3 + c] / mass_fluid[k];
+            }
+    });
+}
+
 int axg_set_ocean_load(axg_solver *h, int32_t count, const int32_t *point, const double *mass_ocean,
                        const double *theta) {
     return guarded(h, [&] {

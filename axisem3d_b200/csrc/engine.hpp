@@ -84,6 +84,13 @@ inline T stf_table_value(const HostStfTable &tb, double time) {
     return (T)(f0 * (double)(T)tb.v[i0] + f1 * (double)(T)tb.v[i1]);
 }
 
+struct HostCoupling3D {
+    int count = 0;
+    std::vector<int> sp, fp;
+    std::vector<int64_t> off;
+    std::vector<double> nu3, na3;    // [n][3] unassembled normal, assembled normal / fluid mass
+};
+
 struct HostSources {
     int count = 0;
     std::vector<int> elem, nu, wave;
@@ -169,6 +176,7 @@ struct HostModel {
     HostSolidElements se;
     HostFluidElements fe;
     HostCoupling sf;
+    HostCoupling3D sf3;
     HostSources ms, fs, ps;          // moment, force, fluid pressure
     HostStations st;
 };

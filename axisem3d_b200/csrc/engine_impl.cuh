@@ -187,6 +187,7 @@ public:
         for (int i = 0; i < m.sg3_s.count; i++) nrs.push_back(m.sp.nr[m.sg3_s.pt[i]]);
         for (int i = 0; i < m.sg3_f.count; i++) nrs.push_back(m.fp.nr[m.sg3_f.pt[i]]);
         for (int i = 0; i < m.ocean3.count; i++) nrs.push_back(m.sp.nr[m.ocean3.pt[i]]);
+        for (int i = 0; i < m.sf3.count; i++) nrs.push_back(m.sp.nr[m.sf3.sp[i]]);
         std::vector<int> twoff;
         tw_.upload(twiddle_pool<T>(nrs, nrmax, twoff));
         tw_off_.upload(twoff);
@@ -194,6 +195,7 @@ public:
         build_fluid_buckets(m.fe);
         if (cfg_.autotune && !cfg_.plain) autotune();
         build_coupling(m.sf);
+        build_coupling3d(m);
         build_abc(m);
         build_scanning(m);
         build_sources(m.ms, m.fs);
@@ -1703,7 +1705,37 @@ private:
         }
     }
 
+    void build_coupling3d(const HostModel &m) {
+        const HostCoupling3D &h = m.sf3;
+        cp3_n_ = h.count;
+        if (!cp3_n_) return;
+        int nrm = 1;
+        for (int i = 0; i < h.count; i++) {
+            if (h.sp[i] < 0 || h.sp[i] >= m.sp.count || h.fp[i] < 0 || h.fp[i] >= m.fp.count ||
+                m.sp.nr[h.sp[i]] != m.fp.nr[h.fp[i]] || h.off[i] < 0 ||
+                h.off[i] + m.sp.nr[h.sp[i]] > (int64_t)(h.nu3.size() / 3))
+                throw Error(AXG_E_ARG, "SolidFluidCoupling3D::checkCompatibility || Incompatible sizes.");
+            nrm = std::max(nrm, m.sp.nr[h.sp[i]]);
+        }
+        cp3_nr_max_ = nrm;
+        cp3_sp_.upload(h.sp); cp3_fp_.upload(h.fp); cp3_off_.upload(h.off);
+        std::vector<T> a(h.nu3.begin(), h.nu3.end()), b(h.na3.begin(), h.na3.end());
+        cp3_nu_.upload(a); cp3_na_.upload(b);
+    }
+
     void launch_coupling() {
+        if (cp3_n_) {
+            Coupling3DArgs<T> a;
+            a.n = cp3_n_; a.sp = cp3_sp_.p; a.fp = cp3_fp_.p; a.coff = cp3_off_.p; a.nu3 = cp3_nu_.p;
+            a.na3 = cp3_na_.p; a.s_off = sp_.off.p; a.s_nr = sp_.nr.p; a.f_off = fp_.off.p;
+            a.tw = tw_.p; a.tw_off = tw_off_.p; a.s_displ = elem_displ(sp_); a.s_stiff = sp_.stiff.p;
+            a.f_stiff = fp_.stiff.p; a.nr_max = cp3_nr_max_; a.nwave = nwave_;
+            a.s_stride = (size_t)sp_.total * 3; a.f_stride = (size_t)fp_.total;
+            const int wpb = 4;
+            solid_fluid3d_kernel<T><<<(cp3_n_ * nwave_ + wpb - 1) / wpb, 32 * wpb,
+                                      (size_t)wpb * 4 * cp3_nr_max_ * sizeof(T), stream_>>>(a);
+            post_launch();
+        }
         if (!cp_n_) return;
         CouplingArgs<T> a;
         a.n = cp_n_; a.sp = cp_sp_.p; a.fp = cp_fp_.p;
@@ -1920,6 +1952,10 @@ private:
     DBuf<T> ms_stf_, fs_stf_;
     DBuf<int> e_nr_, e_pts_;
     int ps_n_ = 0;
+    int cp3_n_ = 0, cp3_nr_max_ = 1;
+    DBuf<int> cp3_sp_, cp3_fp_;
+    DBuf<int64_t> cp3_off_;
+    DBuf<T> cp3_nu_, cp3_na_;
     DBuf<int> ps_el_, ps_nu_, ps_wave_, fe_pts_;
     DBuf<int64_t> ps_po_;
     DBuf<C> ps_pat_;

@@ -317,6 +317,55 @@ __global__ void clayton3d_kernel(const Clayton3DArgs<T, D> a) {
     }
 }
 
+// SolidFluidCoupling3D (core/boundary/solid_fluid/SolidFluidCoupling3D.cpp:40-94): in the
+// slices of the pair's nr, fluid stiff += R2C(n_u . C2R(solid displ)), then solid stiff -=
+// R2C(C2R(fluid stiff) n_a / m_fluid), modes below nr/2 + 1. One warp per (pair, wavefield).
+template <class T>
+struct Coupling3DArgs {
+    int n;
+    const int *sp, *fp;
+    const int64_t *coff;           // per pair: offset of its nr slices
+    const T *nu3, *na3;            // [nr][3] unassembled normal, assembled normal / fluid mass
+    const int *s_off, *s_nr, *f_off;
+    const T *tw; const int *tw_off;
+    const cx_t<T> *s_displ;
+    cx_t<T> *s_stiff, *f_stiff;
+    int nr_max, nwave;
+    size_t s_stride, f_stride;
+};
+
+template <class T>
+__global__ void solid_fluid3d_kernel(const Coupling3DArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int w = threadIdx.x / 32, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * (blockDim.x / 32) + w;
+    if (item >= a.n * a.nwave) return;
+    const int i = item % a.n, wf = item / a.n;
+    const int s = a.sp[i], f = a.fp[i], nr = a.s_nr[s], nu = nr / 2 + 1;
+    T *ur = reinterpret_cast<T *>(sm) + (size_t)w * 4 * a.nr_max;        // [3][nr_max] solid slices
+    T *fr = ur + (size_t)3 * a.nr_max;                                   // [nr_max] fluid slices
+    const T *twc = a.tw + a.tw_off[nr], *tws = twc + nr;
+    const cx_t<T> *u = a.s_displ + (size_t)wf * a.s_stride + (size_t)a.s_off[s] * 3;
+    cx_t<T> *sst = a.s_stiff + (size_t)wf * a.s_stride + (size_t)a.s_off[s] * 3;
+    cx_t<T> *fst = a.f_stiff + (size_t)wf * a.f_stride + a.f_off[f];
+    const T *nu3 = a.nu3 + (size_t)a.coff[i] * 3, *na3 = a.na3 + (size_t)a.coff[i] * 3;
+    for (int c = 0; c < 3; c++) warp_c2r<T, cx_t<T>>(u + c, 3, nu, nr, twc, tws, ur + (size_t)c * a.nr_max, lane);
+    __syncwarp();
+    for (int k = lane; k < nr; k += 32)
+        fr[k] = nu3[3 * k] * ur[k] + nu3[3 * k + 1] * ur[a.nr_max + k] + nu3[3 * k + 2] * ur[2 * a.nr_max + k];
+    __syncwarp();
+    for (int al = lane; al < nu; al += 32) fst[al] = cadd(fst[al], r2c_mode<T>(fr, nr, al, twc, tws));
+    __syncwarp();
+    warp_c2r<T, cx_t<T>>(fst, 1, nu, nr, twc, tws, fr, lane);
+    __syncwarp();
+    for (int k = lane; k < nr; k += 32)
+        for (int c = 0; c < 3; c++) ur[(size_t)c * a.nr_max + k] = fr[k] * na3[3 * k + c];
+    __syncwarp();
+    for (int al = lane; al < nu; al += 32)
+        for (int c = 0; c < 3; c++)
+            sst[(size_t)al * 3 + c] = csub(sst[(size_t)al * 3 + c], r2c_mode<T>(ur + (size_t)c * a.nr_max, nr, al, twc, tws));
+}
+
 // Sponge::apply, 3-D branch (ABC/Sponge.hpp:74-98): in slices, accel -= 2 gamma veloc +
 // gamma^2 displ, then back to Fourier; after the mass term. One warp per point.
 template <class T, class D>

@@ -154,6 +154,8 @@ class Model:
     prt: Optional[dict] = None
     # the same for fluid elements, plus theta [n][25] for the RTZ frame (None: cartesian)
     prt_fluid: Optional[dict] = None
+    # SolidFluidCoupling3D: dict(solid, fluid, offset, normal_u [n][3], normal_a [n][3], mass_fluid [n])
+    sf3: Optional[dict] = None
     cl3_solid: Optional[dict] = None
     cl3_fluid: Optional[dict] = None
     sponge3d_solid: Optional[tuple] = None

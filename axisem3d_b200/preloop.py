@@ -1187,6 +1187,7 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     normal = np.zeros((ngll, 2))
     cl_s, cl_f, cl3_s, cl3_f = [], [], [], []
     ocean_pts = {}                                # point -> [summed top normal [n][3], sum rho depth]
+    normal3 = {}                                  # solid-fluid points whose normal varies with phi
     gamma_sum = np.zeros(ngll)
     gamma_cnt = np.zeros(ngll, np.int64)
     gamma3 = {}                                   # points whose gamma varies in phi
@@ -1201,15 +1202,18 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
                 _ocean_on_quad(q, quads, und, ocean_models, geo, gll, ocean_pts)
         if quads.sides["SOLID_FLUID"][q] != -1:
             pts, nsf = quads.normals(q, quads.sides["SOLID_FLUID"][q])
+            sign = .5 if quads.fluid[q] else -.5
             for p, n in zip(pts, nsf):
                 if has_und[q]:
                     n3 = und.normal3d(q, n, p)
                     if len(n3) > 1 and np.linalg.norm(n3 - n3[0]) > np.linalg.norm(n3) * DEPS:
-                        raise PreloopError("GLLPoint::release || A solid-fluid boundary with undulation that "
-                                           "varies in azimuth (SolidFluidCoupling3D) is not supported by "
-                                           "this build.")
+                        # varies with phi: SolidFluidCoupling3D at this point
+                        g = int(gll[q, p])
+                        cur = normal3.get(g)
+                        normal3[g] = sign * n3 if cur is None else cur + sign * n3
+                        continue
                     n = np.array([n3[0, 0], n3[0, 2]])
-                normal[gll[q, p]] += n / 2. if quads.fluid[q] else -n / 2.
+                normal[gll[q, p]] += sign * n
         if abc.clayton or abc.sponge:
             a_rho, a_vp, a_vs = quads.abc_rho_vp_vs(q)
         if abc.clayton:
@@ -1291,11 +1295,7 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
     m.sp_coords = coords[sp_used]
     m.fp_nr = pnr[fp_used].astype(np.int32)
     m.fp_mass, m.fp_mass_nr, m.fp_mass_off = _mass_layout(fmass, fmass3)
-    if fmass3 and len(np.intersect1d(sp_used, fp_used)):
-        iface_f = set(int(x) for x in fid[np.intersect1d(sp_used, fp_used)])
-        if any(k in iface_f and np.ptp(v + fmass[k]) > 0 for k, v in fmass3.items()):
-            raise PreloopError("GLLPoint::release || Solid-fluid coupling with 3-D fluid masses is not "
-                               "supported by this build.")
+
     m.fp_axial = axial_pt[fp_used].astype(np.uint8)
     m.fp_coords = coords[fp_used]
     fsurf = surface_pt & ("TOP" not in abc.keys)
@@ -1460,6 +1460,24 @@ def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_chan
                                    for k, q in enumerate(fluid_q)]) if nf else np.zeros(0))
     # solid-fluid coupling
     iface = np.intersect1d(sp_used, fp_used)
+    # SolidFluidCoupling3D where the normal or the fluid mass varies with phi (GLLPoint::release)
+    three = [g for g in iface if int(g) in normal3 or
+             (int(fid[g]) in fmass3 and np.ptp(fmass3[int(fid[g])]) > 0)]
+    if three:
+        ents = []
+        for g in three:
+            nrp = int(pnr[g])
+            n3 = np.tile([normal[g, 0], 0., normal[g, 1]], (nrp, 1))
+            if int(g) in normal3:
+                n3 = n3 + np.broadcast_to(normal3[int(g)], (nrp, 3))
+            mf = np.broadcast_to(fmass[fid[g]] + fmass3.get(int(fid[g]), np.zeros(1)), (nrp,)).copy()
+            ents.append((int(sid[g]), int(fid[g]), n3, mf))
+        off = np.concatenate([[0], np.cumsum([len(e[3]) for e in ents])[:-1]]).astype(np.int64)
+        nrm = np.concatenate([e[2] for e in ents])
+        m.sf3 = {"solid": np.array([e[0] for e in ents], np.int32), "fluid": np.array([e[1] for e in ents], np.int32),
+                 "offset": off, "normal_u": nrm, "normal_a": nrm.copy(),
+                 "mass_fluid": np.concatenate([e[3] for e in ents])}
+        iface = np.setdiff1d(iface, np.array(three))
     m.sf_solid = sid[iface].astype(np.int32)
     m.sf_fluid = fid[iface].astype(np.int32)
     m.sf_nsu = normal[iface, 0].copy()

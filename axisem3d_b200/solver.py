@@ -58,6 +58,15 @@ class Solver:
             self._check(self.lib.axg_set_force_sources(h, C.byref(s["fs"])))
         if s["ps"].count:
             self._check(self.lib.axg_set_pressure_sources(h, C.byref(s["ps"])))
+        if getattr(model, "sf3", None):
+            d3 = model.sf3
+            self._sf3 = [np.ascontiguousarray(d3[k], dt) for k, dt in (
+                ("solid", np.int32), ("fluid", np.int32), ("offset", np.int64), ("normal_u", np.float64),
+                ("normal_a", np.float64), ("mass_fluid", np.float64))]
+            a = self._sf3
+            self._check(self.lib.axg_set_solid_fluid3d(h, len(a[0]), a[0].ctypes.data_as(L.P_i32), a[1].ctypes.data_as(L.P_i32),
+                 a[2].ctypes.data_as(L.P_i64),  len(a[5]), a[3].ctypes.data_as(L.P_f64),
+                 a[4].ctypes.data_as(L.P_f64), a[5].ctypes.data_as(L.P_f64)))
         for kind, lst in enumerate((model.ms_stf, model.fs_stf, model.ps_stf)):
             for i, st in enumerate(lst):
                 if getattr(st, "table", None) is not None:

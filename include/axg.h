@@ -352,6 +352,15 @@ int  axg_set_prt_fluid(axg_solver *h, int32_t count, const int32_t *element, con
    in computeStiffToAccel the point's own mass acts along the surface and mass + mass_ocean
    across it, the surface normal at polar angle theta; each point at most once, points with
    1-D masses only (a Mass3D point takes axg_set_ocean_load3d) */
+/* SolidFluidCoupling3D (core/boundary/solid_fluid/SolidFluidCoupling3D.cpp:40-94; built in
+   GLLPoint.cpp:120-145 where the normal or the fluid mass varies with phi): per pair and
+   slice of the points' nr (equal on both points), fluid stiff += R2C(n_u . C2R(solid
+   displ)), then solid stiff -= R2C(C2R(fluid stiff) n_a / m_fluid); normal_u, normal_a
+   [n][3] (s, phi, z) and mass_fluid [n] from offset[i]. A pair given here is not also in
+   axg_set_solid_fluid. */
+int  axg_set_solid_fluid3d(axg_solver *h, int32_t count, const int32_t *solid_point, const int32_t *fluid_point,
+                           const int64_t *offset, int64_t nvalues, const double *normal_u,
+                           const double *normal_a, const double *mass_fluid);
 int  axg_set_ocean_load(axg_solver *h, int32_t count, const int32_t *point, const double *mass_ocean,
                         const double *theta);
 /* MassOceanLoad3D (point/mass/MassOceanLoad3D.cpp, built in GLLPoint.cpp:74-87) where the

@@ -463,6 +463,8 @@ struct OracleBase {
     virtual void set_moment_sources(const axg_moment_sources *) = 0;
     virtual void set_force_sources(const axg_force_sources *) = 0;
     virtual void set_pressure_sources(const axg_pressure_sources *) = 0;
+    virtual void set_solid_fluid3d(int n, const int *sp_, const int *fp_, const int64_t *off, const double *nu3,
+                                   const double *na3, const double *mf) = 0;
     virtual void set_stf_table(int kind, int index, int n, const double *t, const double *v, int padding,
                                double left, double right, int pad_first) = 0;
     virtual void set_stations(const axg_stations *, int) = 0;
@@ -508,6 +510,51 @@ struct Oracle : OracleBase {
     std::vector<MomentSrc<R>> msrc;
     std::vector<ForceSrc<R>> fsrc;
     std::vector<PressureSrc<R>> psrc;
+    // SolidFluidCoupling3D: pairs, per-slice unassembled normal and assembled normal / fluid mass
+    struct Cp3 { int s, f; std::vector<R> nu3, na3; };
+    std::vector<Cp3> cp3;
+    void set_solid_fluid3d(int n, const int *sp_, const int *fp_, const int64_t *off, const double *nu3,
+                           const double *na3, const double *mf) override {
+        cp3.resize(n);
+        for (int i = 0; i < n; i++) {
+            Cp3 &c = cp3[i];
+            c.s = sp_[i]; c.f = fp_[i];
+            const int nr = sp.nr[c.s];
+            prepare_twiddle(nr);
+            c.nu3.resize((size_t)nr * 3); c.na3.resize((size_t)nr * 3);
+            for (int k = 0; k < nr; k++)
+                for (int d = 0; d < 3; d++) {
+                    c.nu3[(size_t)k * 3 + d] = (R)nu3[(off[i] + k) * 3 + d];
+                    c.na3[(size_t)k * 3 + d] = (R)(na3[(off[i] + k) * 3 + d] / mf[off[i] + k]);
+                }
+        }
+    }
+    // SolidFluidCoupling3D::coupleSolidToFluid / coupleFluidToSolid (SolidFluidCoupling3D.cpp:40-94)
+    void couple3d() {
+        for (auto &c : cp3) {
+            const int nr = sp.nr[c.s], nu = nr / 2 + 1;
+            const Twiddle<R> &t = twiddle(nr);
+            std::vector<Cx<R>> cb(nu);
+            std::vector<R> ur((size_t)3 * nr), fr(nr);
+            for (int d = 0; d < 3; d++) {
+                for (int a = 0; a < nu; a++) cb[a] = sp.displ[((size_t)sp.off[c.s] + a) * 3 + d];
+                c2r(cb.data(), nu, &ur[(size_t)d * nr], nr, t);
+            }
+            for (int k = 0; k < nr; k++)
+                fr[k] = c.nu3[3 * k] * ur[k] + c.nu3[3 * k + 1] * ur[nr + k] + c.nu3[3 * k + 2] * ur[2 * nr + k];
+            r2c(fr.data(), nr, cb.data(), nu, t);
+            Cx<R> *fs = &fp.stiff[(size_t)fp.off[c.f]];
+            for (int a = 0; a < nu; a++) fs[a] += cb[a];
+            for (int a = 0; a < nu; a++) cb[a] = fs[a];
+            c2r(cb.data(), nu, fr.data(), nr, t);
+            Cx<R> *ss = &sp.stiff[(size_t)sp.off[c.s] * 3];
+            for (int d = 0; d < 3; d++) {
+                for (int k = 0; k < nr; k++) ur[(size_t)d * nr + k] = fr[k] * c.na3[3 * k + d];
+                r2c(&ur[(size_t)d * nr], nr, cb.data(), nu, t);
+                for (int a = 0; a < nu; a++) ss[a * 3 + d] -= cb[a];
+            }
+        }
+    }
     std::map<int, StfTable> stf_tab[3];   // moment, force, pressure sources with a table STF
     R src_stf(int kind, int i, const axg_stf &g, double t) const {
         auto it = stf_tab[kind].find(i);
@@ -1531,6 +1578,7 @@ struct Oracle : OracleBase {
                 sp.stiff[((size_t)sp.off[c.s] + a) * 3 + 2] -= c.nza_m * fp.stiff[(size_t)fp.off[c.f] + a];
             }
         }
+        couple3d();
     }
 
     // AxialBoundary::apply (AxialBoundary.cpp:21-51), FluidSurfaceBoundary::apply
@@ -1902,6 +1950,10 @@ int axo_set_solid_fluid(void *h, const axg_solid_fluid *c) { AXO_TRY(static_cast
 int axo_set_moment_sources(void *h, const axg_moment_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_moment_sources(s)) }
 int axo_set_force_sources(void *h, const axg_force_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_force_sources(s)) }
 int axo_set_pressure_sources(void *h, const axg_pressure_sources *s) { AXO_TRY(static_cast<OracleBase *>(h)->set_pressure_sources(s)) }
+int axo_set_solid_fluid3d(void *h, int n, const int *sp_, const int *fp_, const int64_t *off, const double *nu3,
+                          const double *na3, const double *mf) {
+    AXO_TRY(static_cast<OracleBase *>(h)->set_solid_fluid3d(n, sp_, fp_, off, nu3, na3, mf))
+}
 int axo_set_stf_table(void *h, int kind, int index, int n, const double *t, const double *v, int padding, double left,
                       double right, int pad_first) {
     AXO_TRY(static_cast<OracleBase *>(h)->set_stf_table(kind, index, n, t, v, padding, left, right, pad_first))

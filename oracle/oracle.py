@@ -49,6 +49,7 @@ def lib():
             "axo_set_moment_sources": (C.c_int, [V, C.POINTER(L.axg_moment_sources)]),
             "axo_set_force_sources": (C.c_int, [V, C.POINTER(L.axg_force_sources)]),
             "axo_set_pressure_sources": (C.c_int, [V, C.POINTER(L.axg_pressure_sources)]),
+            "axo_set_solid_fluid3d": (C.c_int, [V, C.c_int, L.P_i32, L.P_i32, L.P_i64, L.P_f64, L.P_f64, L.P_f64]),
             "axo_set_stf_table": (C.c_int, [V, C.c_int, C.c_int, C.c_int, L.P_f64, L.P_f64, C.c_int, C.c_double,
                                             C.c_double, C.c_int]),
             "axo_set_stations": (C.c_int, [V, C.POINTER(L.axg_stations), C.c_int]),
@@ -113,6 +114,15 @@ class Oracle:
         self._chk(self.O.axo_set_force_sources(self.h, C.byref(s["fs"])))
         if s["ps"].count:
             self._chk(self.O.axo_set_pressure_sources(self.h, C.byref(s["ps"])))
+        if getattr(model, "sf3", None):
+            d3 = model.sf3
+            self._sf3 = [np.ascontiguousarray(d3[k], dt) for k, dt in (
+                ("solid", np.int32), ("fluid", np.int32), ("offset", np.int64), ("normal_u", np.float64),
+                ("normal_a", np.float64), ("mass_fluid", np.float64))]
+            a = self._sf3
+            self._chk(self.O.axo_set_solid_fluid3d(self.h, len(a[0]), a[0].ctypes.data_as(L.P_i32), a[1].ctypes.data_as(L.P_i32),
+                 a[2].ctypes.data_as(L.P_i64),  a[3].ctypes.data_as(L.P_f64),
+                 a[4].ctypes.data_as(L.P_f64), a[5].ctypes.data_as(L.P_f64)))
         for kind, lst in enumerate((model.ms_stf, model.fs_stf, model.ps_stf)):
             for i, st in enumerate(lst):
                 if getattr(st, "table", None) is not None:

@@ -342,6 +342,15 @@ def _with_geometry(d, case):
                                                [0, 1], "dz", 400e3, 100e3, 800e3, angle_unit="degree"),
                              fx.ocean_yaml("sea", "sea.nc", "LATITUDE_LONGITUDE", ["lat", "lon"], [0, 1], "srd",
                                            angle_unit="degree")])
+    elif case == "shell_cmb":
+        # undulation that varies with phi on the solid-fluid boundary (3600 km radius):
+        # SolidFluidCoupling3D
+        lat, lon = np.linspace(-90, 90, 19), np.linspace(-180, 180, 37)
+        fx.write_grid_v3d(os.path.join(d, "cmb.nc"), {"lat": lat, "lon": lon},
+                          {"dz": 1500.0 * np.cos(np.radians(lat))[:, None] * np.cos(np.radians(lon))[None, :]},
+                          ["lat", "lon"])
+        fx.add_3d_models(d, [fx.geometric_yaml("cmb", "cmb.nc", "LATITUDE_LONGITUDE", "RADIUS", ["lat", "lon"],
+                                               [0, 1], "dz", 3600e3, 3500e3, 3800e3, angle_unit="degree")])
     else:
         fx.add_3d_models(d, [fx.ellipticity_yaml("ellipticity")])
         p = os.path.join(d, "inparam.model.yaml")
@@ -353,7 +362,7 @@ def _with_geometry(d, case):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("case", ["box", "shell", "shell_ellipticity"])
+@pytest.mark.parametrize("case", ["box", "shell", "shell_ellipticity", "shell_cmb"])
 def test_simulation_with_geometric_and_ocean_models_matches_oracle(built, tmp_path, case, precision):
     """Undulated geometry through the whole path: particle relabelling (1-D and 3-D, solid
     and fluid elements), the PRT Jacobian on the masses, 3-D ocean loads, slice-wise dt."""
@@ -362,8 +371,10 @@ def test_simulation_with_geometric_and_ocean_models_matches_oracle(built, tmp_pa
     res = simulation.run(d, None, precision=precision)
     m = res.sim.model
     assert m.prt is not None and len(m.prt["element"]) > 0
-    if case != "shell_ellipticity":
+    if case in ("box", "shell"):
         assert m.prt["is3d_prt"].any() and m.ocean_load3d is not None
+    if case == "shell_cmb":
+        assert m.sf3 is not None and len(m.sf3["solid"]) > 0
     ref = _oracle_traces(res.sim)
     for name, (t_ref, w_ref) in ref.items():
         t, w = res.traces[name]
