@@ -969,7 +969,8 @@ private:
                     soff[k] = state_total;
                     state_total += (int64_t)(cfg_.nsls + 1) * 6 * slots;
                 }
-                // algorithmic bytes and flops of this element (stiffness roofline)
+                // algorithmic bytes and flops of this element: every operand read once, the SLS state
+                // read and written once, point modes counted with the points (stiffness roofline)
                 double s = sizeof(T), sa = sizeof(AT);
                 bytes += 6 * 25 * s + 25 * 4 + 8;                        // geometry, point ids, nr
                 bytes += (double)nm * ns * 25 * s;                        // moduli
@@ -1539,9 +1540,9 @@ private:
     // STF table and seismogram buffer large enough for steps [0, nsteps)
     void ensure_capacity(int nsteps) {
         bool changed = false;
-        if ((ms_n_ || fs_n_ || ps_n_) && nsteps > stf_cap_) {
+        if ((ms_n_ || fs_n_ || ps_n_) && nsteps > stf_valid_) {
             int cap = std::max(nsteps, 2 * stf_cap_);
-            fill_stf(cap);
+            fill_stf(cap, nsteps);
             changed = true;
         }
         if (st_n_) {
@@ -1590,21 +1591,37 @@ private:
         }
         throw Error(AXG_E_ARG, "GaussianSTF::getValue || Unsupported derivative order.");
     }
-    void fill_stf(int cap) {
+    // Steps [0, need) must evaluate: a table source without padding throws there as
+    // StreamSTF::getValue does when the run asks for a time out of its range. The steps
+    // [need, cap) are evaluated ahead only as far as every source is defined; the table is
+    // valid up to the first step that is not (slots after it stay zero and are never read,
+    // ensure_capacity refills before a run needs them).
+    void fill_stf(int cap, int need) {
         // t accumulated as NewmarkTimeScheme::solve does (t += mDt)
-        std::vector<T> ms((size_t)cap * std::max(ms_n_, 1)), fs((size_t)cap * std::max(fs_n_, 1)),
-            ps((size_t)cap * std::max(ps_n_, 1));
+        std::vector<T> ms((size_t)cap * std::max(ms_n_, 1), (T)0), fs((size_t)cap * std::max(fs_n_, 1), (T)0),
+            ps((size_t)cap * std::max(ps_n_, 1), (T)0);
         double t = cfg_.t0;
+        int valid = cap;
         for (int k = 0; k < cap; k++) {
-            for (int i = 0; i < ms_n_; i++) ms[(size_t)k * ms_n_ + i] = src_stf(model_.ms, i, t);
-            for (int i = 0; i < fs_n_; i++) fs[(size_t)k * fs_n_ + i] = src_stf(model_.fs, i, t);
-            for (int i = 0; i < ps_n_; i++) ps[(size_t)k * ps_n_ + i] = src_stf(model_.ps, i, t);
+            try {
+                for (int i = 0; i < ms_n_; i++) ms[(size_t)k * ms_n_ + i] = src_stf(model_.ms, i, t);
+                for (int i = 0; i < fs_n_; i++) fs[(size_t)k * fs_n_ + i] = src_stf(model_.fs, i, t);
+                for (int i = 0; i < ps_n_; i++) ps[(size_t)k * ps_n_ + i] = src_stf(model_.ps, i, t);
+            } catch (const Error &) {
+                if (k < need) throw;
+                for (int i = 0; i < ms_n_; i++) ms[(size_t)k * ms_n_ + i] = (T)0;
+                for (int i = 0; i < fs_n_; i++) fs[(size_t)k * fs_n_ + i] = (T)0;
+                for (int i = 0; i < ps_n_; i++) ps[(size_t)k * ps_n_ + i] = (T)0;
+                valid = k;
+                break;
+            }
             t += cfg_.dt;
         }
         ms_stf_.upload(ms);
         fs_stf_.upload(fs);
         ps_stf_.upload(ps);
         stf_cap_ = cap;
+        stf_valid_ = valid;
     }
 
     // ------------------------------------------------------------ launches ---
@@ -1926,7 +1943,7 @@ private:
     int cp_n_ = 0;
     DBuf<int> cp_sp_, cp_fp_;
     DBuf<T> cp_nsu_, cp_nzu_, cp_nsa_, cp_nza_;
-    int ms_n_ = 0, fs_n_ = 0, stf_cap_ = 0;
+    int ms_n_ = 0, fs_n_ = 0, stf_cap_ = 0, stf_valid_ = 0;
     DBuf<int> ms_el_, ms_nu_, fs_el_, fs_nu_, ms_wave_, fs_wave_;
     int nwave_ = 1;
     int64_t state_wave_ = 0;

@@ -22,24 +22,88 @@ Workloads (sizes in SI units):
                     layer 3480-3600 km, 1-D layered background, 2 % Gaussian
                     random-field dlnVs setting per-element nr, Q = 300.
 """
+import contextlib
 import math
 
 import numpy as np
 
 from . import _lib as L
 from .model import Model, STF
-from .solver import att_alpha_beta_gamma, att_moduli, quad_dt
 
-# GLL / GLJ tables (nPol = 4)
-_TAB = None
+
+# ------------------------------------------------------- operand builders ---
+class EngineOperands:
+    """The engine's host operand builders (libaxg.so: axg_spectral_tables,
+    axg_quad_geometry_batch, axg_quad_dt, axg_att_alpha_beta_gamma, axg_att_moduli), the
+    restatements of the reference's preloop numbers that every workload here is built with."""
+
+    def tables(self):
+        from .solver import spectral_tables
+        return spectral_tables()
+
+    def geometry_batch(self, nodal, axial, mapping=L.AXG_MAP_LINEAR):
+        lib = L.lib()
+        ne = len(axial)
+        nodal = np.ascontiguousarray(nodal, dtype=np.float64).reshape(ne, 8)
+        ax = np.ascontiguousarray(axial, dtype=np.uint8)
+        g = np.zeros((ne, 6, 25))
+        sz = np.zeros((ne, 2, 25))
+        rc = lib.axg_quad_geometry_batch(ne, int(mapping), nodal.ctypes.data_as(L.P_f64),
+                                         ax.ctypes.data_as(L.P_u8), g.ctypes.data_as(L.P_f64),
+                                         sz.ctypes.data_as(L.P_f64))
+        if rc != L.AXG_OK:
+            raise RuntimeError("axg_quad_geometry_batch failed (%d)" % rc)
+        return g, sz
+
+    def quad_dt(self, sz, vmax):
+        from .solver import quad_dt
+        return quad_dt(sz, vmax)
+
+    def att_alpha_beta_gamma(self, w, y, dt):
+        from .solver import att_alpha_beta_gamma
+        return att_alpha_beta_gamma(w, y, dt)
+
+    def att_moduli(self, w, y, fmin, fmax, fref, qkappa, qmu, kp, mu):
+        from .solver import att_moduli
+        return att_moduli(w, y, fmin, fmax, fref, qkappa, qmu, kp, mu)
+
+
+# the builder in use: the engine's, unless a caller installs another with `operands`
+_OPS = [EngineOperands()]
+_TAB = {}
+
+
+@contextlib.contextmanager
+def operands(builder):
+    """Build workloads with another operand builder inside the block: an object with the
+    methods of EngineOperands (tables, geometry_batch, quad_dt, att_alpha_beta_gamma,
+    att_moduli). The models come out the same up to the builders' rounding; a model built
+    this way needs no engine library."""
+    _OPS.append(builder)
+    try:
+        yield builder
+    finally:
+        _OPS.pop()
 
 
 def tables():
-    global _TAB
-    if _TAB is None:
-        from .solver import spectral_tables
-        _TAB = spectral_tables()
-    return _TAB
+    """GLL / GLJ tables (nPol = 4) of the builder in use."""
+    b = _OPS[-1]
+    if id(b) not in _TAB:
+        _TAB[id(b)] = (b, b.tables())
+    return _TAB[id(b)][1]
+
+
+def quad_dt(sz, vmax):
+    return _OPS[-1].quad_dt(sz, vmax)
+
+
+def att_alpha_beta_gamma(w, y, dt):
+    return _OPS[-1].att_alpha_beta_gamma(w, y, dt)
+
+
+def att_moduli(w, y, fmin, fmax, fref, qkappa, qmu, kp, mu):
+    return _OPS[-1].att_moduli(w, y, fmin, fmax, fref, qkappa, qmu, kp, mu)
 
 
 def lagrange(nodes, x):
@@ -68,18 +132,7 @@ def round_dt(dt):
 # ------------------------------------------------------------------ geometry ---
 def geometry_batch(nodal, axial, mapping=L.AXG_MAP_LINEAR):
     """Quad::createGradient for all quads: (ne, 6, 25) operands and (ne, 2, 25) s, z."""
-    lib = L.lib()
-    ne = len(axial)
-    nodal = np.ascontiguousarray(nodal, dtype=np.float64).reshape(ne, 8)
-    ax = np.ascontiguousarray(axial, dtype=np.uint8)
-    g = np.zeros((ne, 6, 25))
-    sz = np.zeros((ne, 2, 25))
-    rc = lib.axg_quad_geometry_batch(ne, int(mapping), nodal.ctypes.data_as(L.P_f64),
-                                     ax.ctypes.data_as(L.P_u8), g.ctypes.data_as(L.P_f64),
-                                     sz.ctypes.data_as(L.P_f64))
-    if rc != L.AXG_OK:
-        raise RuntimeError("axg_quad_geometry_batch failed (%d)" % rc)
-    return g, sz
+    return _OPS[-1].geometry_batch(nodal, axial, mapping)
 
 
 def structured_points(nx, nz):

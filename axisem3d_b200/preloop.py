@@ -485,12 +485,13 @@ def _read_stf(gm, root, name, dt, path=None):
             t = list(np.asarray(nc[gm.get(root + ":nc_var_times")], np.float64).ravel())
             v = list(np.asarray(nc[gm.get(root + ":nc_var_data")], np.float64).ravel())
             where = "NetCDF_STF::NetCDF_STF"
-            if len(t) != len(v):
-                raise PreloopError(where + " || Times and values have different lengths. || NetCDF file: " + fname)
+        # NetCDF_STF.cpp:43-70 checks the count, then the order, then the lengths
         if len(t) < 2:
             raise PreloopError(where + " || Insufficient time points, at least 2. || File: " + fname)
         if np.any(np.diff(t) <= 0):
             raise PreloopError(where + " || Time points are not ascendingly sorted. || File: " + fname)
+        if len(t) != len(v):
+            raise PreloopError(where + " || Times and values have different lengths. || NetCDF file: " + fname)
         if pad == "FIRST_LAST":
             left, right = v[0], v[-1]
         return STF(table=(np.array(t), np.array(v)), padding=padding, left=left, right=right,

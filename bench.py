@@ -171,72 +171,83 @@ def profiled_traffic():
     return None
 
 
-def build_model(args, seed=1):
+def build_model(args, seed=1, builder=None):
+    """The workload, built with the engine's operand builder or with `builder` (the oracle's
+    own restatement, so that the CPU legs map no library of the engine)."""
+    import contextlib
     from axisem3d_b200 import meshgen
-    return meshgen.microbench_model(n_elem=args.elements, nr_max=args.nr_max, seed=seed)
+    with (meshgen.operands(builder) if builder is not None else contextlib.nullcontext()):
+        return meshgen.microbench_model(n_elem=args.elements, nr_max=args.nr_max, seed=seed)
+
+
+def oracle_workload(args, seed=1):
+    """The oracle module and the workload built through the oracle's operands."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O, build_model(args, seed, O.OracleOperands())
 
 
 def workload_config(args, m):
-    """The workload's description; m = None (the CPU reference arm, which times a bounded
-    sample of it) names the requested element count."""
-    n = m.n_solid_elements if m is not None else args.elements
-    c = {"workload": "stiffness microbenchmark, uneven nr: %d solid quads nPol=4, nr log-uniform "
-                     "[1,%d], TI 3-D slices, 3 SLS FULL, full Newmark step" % (n, args.nr_max),
-         "elements": int(n), "precision": args.precision,
-         "l2": "inputs larger than L2 (the step streams >10 GB)", "graph": "one CUDA graph per step"}
-    if m is not None:
-        c["updates_per_step"] = int(m.updates_per_step())
-    return c
+    """The workload's description; the same dictionary on both arms."""
+    return {"workload": "stiffness microbenchmark, uneven nr: %d solid quads nPol=4, nr log-uniform "
+                        "[1,%d], TI 3-D slices, 3 SLS FULL, full Newmark step" % (m.n_solid_elements, args.nr_max),
+            "elements": int(m.n_solid_elements), "updates_per_step": int(m.updates_per_step()),
+            "l2": "inputs larger than L2 (the step streams >10 GB)"}
 
 
-# --------------------------------------------------------------- CPU baseline ---
-_CPU_CASE = {}
+# --------------------------------------------------------------- CPU legs ---
+def cpu_timed_steps(o, steps):
+    t0 = time.perf_counter()
+    o.run(steps)
+    return time.perf_counter() - t0
 
 
 def cpu_baseline(args, seconds):
-    """Oracle (FP32, the reference's default precision) on all host cores, bounded sample
-    (1 % of the workload's elements, at least 200, at most 4000)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    """The oracle (FP32, the reference's default precision) on all host cores, on the full
+    workload built through the oracle's own operands: one untimed step, then whole steps
+    for about `seconds`."""
     from axisem3d_b200 import meshgen
-    n = max(200, min(4000, args.elements // 100))
+    O, m = oracle_workload(args, seed=1)
     cores = os.cpu_count() or 1
-    if "o" not in _CPU_CASE:
-        m = meshgen.microbench_model(n_elem=n, nr_max=args.nr_max, seed=7)
-        o = O.Oracle(m, "fp32", threads=cores)
-        o.set_field(meshgen.random_displacement(m, seed=3) * 1e-6, "displ")
-        _CPU_CASE.update(m=m, o=o)
-    m, o = _CPU_CASE["m"], _CPU_CASE["o"]
-    o.run(1)
-    steps, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < seconds:
-        o.run(1)
-        steps += 1
-    dt = time.perf_counter() - t0
-    upd = m.updates_per_step() * steps / dt
-    return {"value": upd, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "%d-element sample of the same distribution, %d full steps in %.1f s, FP32" %
-                      (m.n_solid_elements, steps, dt)}
+    o = O.Oracle(m, "fp32", threads=cores)
+    o.set_field(meshgen.random_displacement(m, seed=2) * 1e-6, "displ")
+    t1 = cpu_timed_steps(o, 1)
+    steps = max(1, min(20, int(seconds / max(t1, 1e-3))))
+    dt = cpu_timed_steps(o, steps)
+    U = m.updates_per_step()
+    return {"value": U * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d full steps of the whole %d-element workload in %.1f s (FP32 oracle, model built "
+                      "with the oracle's operands)" % (steps, m.n_solid_elements, dt)}
 
 
 # --------------------------------------------------------------------- arms ---
 def run_reference(args, world, rank):
+    """The reference's CPU path (the oracle port: the reference cannot be built here) on the
+    whole workload, FP32 like the reference's default build, all host threads: W untimed
+    steps, then K timed steps (a prefix of them, stated in `sample`, should K steps take
+    longer than about five minutes)."""
     if rank != 0:
         return
+    from axisem3d_b200 import meshgen
+    O, m = oracle_workload(args, seed=1)
+    cores = os.cpu_count() or 1
+    o = O.Oracle(m, "fp32", threads=cores)
+    o.set_field(meshgen.random_displacement(m, seed=2) * 1e-6, "displ")
+    tw = cpu_timed_steps(o, max(1, args.warmup))
+    per = tw / max(1, args.warmup)
     steps = max(1, args.steps)
-    # each step is a bounded sample: the whole run stays within a few minutes
-    per = max(0.5, min(args.cpu_seconds, 120.0 / (steps + args.warmup)))
-    for _ in range(args.warmup):
-        cpu_baseline(args, min(per, 2.0))
-    vals = [cpu_baseline(args, per) for _ in range(steps)]
-    v = float(np.median([x["value"] for x in vals]))
-    cb = dict(vals[0])
-    cb["value"] = v
+    timed = max(1, min(steps, int(300.0 / max(per, 1e-3))))
+    t = cpu_timed_steps(o, timed)
+    U = m.updates_per_step()
+    v = U * timed / t
+    sample = ("%d of %d full steps of the whole %d-element workload in %.1f s after %d warm-up steps "
+              "(FP32 oracle port on %d threads, model built with the oracle's operands)"
+              % (timed, steps, m.n_solid_elements, t, max(1, args.warmup), cores))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(workload_config(args, None), precision="fp32 (the reference's default build)"),
-            "cpu_baseline": cb,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": t / timed * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args, m),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -492,6 +503,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"mixed": "f32 (f64 Newmark d/v and SLS state)", "fp32": "f32", "fp64": "f64"}[args.precision],
             "data": "synthetic", "config": workload_config(args, m),
+            "precision": args.precision, "graph": "one CUDA graph per step",
             "gpu_launches": int(r["launches"]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

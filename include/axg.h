@@ -452,7 +452,9 @@ int  axg_launch_count(const axg_solver *h, int64_t *n);
 int  axg_set_timing(axg_solver *h, int32_t on);
 int  axg_stiffness_time_ms(axg_solver *h, double *ms, int64_t *launches);
 /* algorithmic HBM bytes and FP32/FP64 flops of one stiffness evaluation
-   (solid + fluid elements), from the mesh, by the formulas in DESIGN.md */
+   (solid + fluid elements), from the mesh: per element the geometry (6 x 25 reals), point ids,
+   moduli (nmod x nslice x 25), attenuation moduli (2 x nslice x npa) and the SLS state read
+   and written once; flops of the gradient, quadrature, stress and the two direct DFTs */
 int  axg_stiffness_cost(const axg_solver *h, double *bytes, double *flops);
 /* algorithmic bytes of one point update (stiff->accel + Newmark) */
 int  axg_point_cost(const axg_solver *h, double *bytes);
@@ -481,7 +483,9 @@ int  axg_set_team_size(axg_solver *h, int32_t nr_class, int32_t team);
    calls on a device share it, so calls whose GPU work overlaps (other streams, other handles)
    race: order them on one stream or synchronize between them. The work is queued on the
    handle's stream (axg_set_stream). The first call on a device looks the array up
-   (cudaGetSymbolAddress); make that first call before any stream capture. */
+   (cudaGetSymbolAddress); make that first call before any stream capture. The address is kept
+   for the life of the process: a device reset (cudaDeviceReset) after the first call on that
+   device is not supported. */
 #define AXG_NOALLOC_SCRATCH_BYTES (16u << 20)
 int  axg_compute_stiffness_noalloc(axg_solver *h, const void *solid_x, void *solid_f,
                                    const void *fluid_x, void *fluid_f);

@@ -18,10 +18,9 @@ import spectral  # noqa: E402
 
 
 def build():
-    src = os.path.join(HERE, "axg_oracle.cpp")
-    hdr = os.path.join(HERE, "..", "include", "axg.h")
-    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(os.path.getmtime(src),
-                                                                         os.path.getmtime(hdr)):
+    srcs = [os.path.join(HERE, "axg_oracle.cpp"), os.path.join(HERE, "axg_operands_oracle.cpp"),
+            os.path.join(HERE, "..", "include", "axg.h")]
+    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
@@ -77,6 +76,12 @@ def lib():
             "axo_get_seismograms": (C.c_int, [V, L.P_f64]),
             "axo_reset_attenuation": (C.c_int, [V]),
             "axo_current_step": (C.c_int, [V]),
+            "axo_quad_geometry_batch": (C.c_int, [C.c_int, C.c_int, L.P_f64, L.P_u8, L.P_f64, L.P_f64, L.P_f64]),
+            "axo_quad_dt": (C.c_int, [L.P_f64, C.c_double, L.P_f64]),
+            "axo_att_alpha_beta_gamma": (C.c_int, [C.c_int, L.P_f64, L.P_f64, C.c_double, L.P_f64, L.P_f64,
+                                                   L.P_f64]),
+            "axo_att_moduli": (C.c_int, [C.c_int, L.P_f64, L.P_f64, C.c_double, C.c_double, C.c_double, C.c_int,
+                                         L.P_f64, L.P_f64, L.P_f64, L.P_f64, L.P_f64, L.P_f64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(O, name)
@@ -88,6 +93,70 @@ def lib():
         O.axo_set_spectral(gll.ctypes.data_as(L.P_f64), glj.ctypes.data_as(L.P_f64))
         _lib = O
     return _lib
+
+
+class OracleOperands:
+    """The oracle's own restatement of the preloop numbers (axg_operands_oracle.cpp: the
+    mappings, Quad::computeIntegralFactor / createGradient, Quad::computeDt and AttBuilder),
+    with the GLL / GLJ tables of spectral.py. It has the methods of
+    ``axisem3d_b200.meshgen.EngineOperands``, so ``meshgen.operands(OracleOperands())`` builds
+    a workload without the engine's library: the CPU baselines use it, and the tests compare
+    the two builders."""
+
+    MAP_LINEAR, MAP_SPHERICAL = 0, 1
+
+    def tables(self):
+        return spectral.tables()
+
+    def geometry_batch(self, nodal, axial, mapping=0):
+        from axisem3d_b200 import _lib as L
+        ne = len(axial)
+        nodal = np.ascontiguousarray(nodal, dtype=np.float64).reshape(ne, 8)
+        ax = np.ascontiguousarray(axial, dtype=np.uint8)
+        t = spectral.tables()
+        tab = np.ascontiguousarray(np.concatenate([t["pGLL"], t["pGLJ"], t["wGLL"], t["wGLJ"]]))
+        g = np.zeros((ne, 6, 25))
+        sz = np.zeros((ne, 2, 25))
+        rc = lib().axo_quad_geometry_batch(ne, int(mapping), nodal.ctypes.data_as(L.P_f64),
+                                           ax.ctypes.data_as(L.P_u8), tab.ctypes.data_as(L.P_f64),
+                                           g.ctypes.data_as(L.P_f64), sz.ctypes.data_as(L.P_f64))
+        if rc != 0:
+            raise RuntimeError("oracle: MappingSpherical::MappingSpherical || Error identifying curved outer edge.")
+        return g, sz
+
+    def quad_dt(self, sz, vmax):
+        from axisem3d_b200 import _lib as L
+        s = np.ascontiguousarray(sz, dtype=np.float64).reshape(50)
+        dt = C.c_double()
+        lib().axo_quad_dt(s.ctypes.data_as(L.P_f64), float(vmax), C.byref(dt))
+        return dt.value
+
+    def att_alpha_beta_gamma(self, w, y, dt):
+        from axisem3d_b200 import _lib as L
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        a, b, g = np.zeros(len(w)), np.zeros(len(w)), np.zeros(len(w))
+        lib().axo_att_alpha_beta_gamma(len(w), w.ctypes.data_as(L.P_f64), y.ctypes.data_as(L.P_f64), float(dt),
+                                       a.ctypes.data_as(L.P_f64), b.ctypes.data_as(L.P_f64),
+                                       g.ctypes.data_as(L.P_f64))
+        return a, b, g
+
+    def att_moduli(self, w, y, fmin, fmax, fref, qkappa, qmu, kp, mu):
+        from axisem3d_b200 import _lib as L
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        qk = np.ascontiguousarray(np.broadcast_to(qkappa, np.shape(kp)), dtype=np.float64).ravel()
+        qm = np.ascontiguousarray(np.broadcast_to(qmu, np.shape(kp)), dtype=np.float64).ravel()
+        kp2 = np.array(kp, dtype=np.float64).ravel().copy()
+        mu2 = np.array(mu, dtype=np.float64).ravel().copy()
+        dk, dm = np.zeros_like(kp2), np.zeros_like(kp2)
+        P = L.P_f64
+        lib().axo_att_moduli(len(w), w.ctypes.data_as(P), y.ctypes.data_as(P), float(fmin), float(fmax),
+                             float(fref), len(kp2), qk.ctypes.data_as(P), qm.ctypes.data_as(P),
+                             kp2.ctypes.data_as(P), mu2.ctypes.data_as(P), dk.ctypes.data_as(P),
+                             dm.ctypes.data_as(P))
+        shp = np.shape(kp)
+        return kp2.reshape(shp), mu2.reshape(shp), dk.reshape(shp), dm.reshape(shp)
 
 
 class Oracle:

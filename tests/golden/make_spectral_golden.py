@@ -2,9 +2,9 @@
 
 Reads SOLVER/src/preloop/se_model/quad/spectrals.hpp of the reference checkout
 (as text, nothing is compiled or executed) and writes spectral_npol4.json next
-to this script. Run once in a container that holds the reference:
+to this script. Run once where a reference checkout is present, naming its root:
 
-    python tests/golden/make_spectral_golden.py /root/reference
+    python tests/golden/make_spectral_golden.py <reference checkout>
 """
 import json
 import os
@@ -23,7 +23,9 @@ def extract(path):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_spectral_golden.py <reference checkout root>")
+    ref = sys.argv[1]
     tables = extract(os.path.join(ref, "SOLVER/src/preloop/se_model/quad/spectrals.hpp"))
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "spectral_npol4.json")
     with open(dst, "w") as f:

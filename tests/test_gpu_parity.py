@@ -708,3 +708,42 @@ def test_fluid_prt_parity(built, precision, three_d):
         s.set_field(uf, "displ", solid=False)
         s.compute_stiffness()
         assert rel(s.get_field("stiff", solid=False), ref) <= TOL_STIFF[precision]
+
+
+@pytest.mark.parametrize("mode", ["hooks", "chunks"])
+def test_table_stf_without_padding_to_the_last_step(built, mode):
+    """A StreamSTF table with padding NONE whose last sample is the time of the last step the
+    run takes: the run needs no time beyond the table, so it completes, per hook or in chunks
+    of 7 steps (StreamSTF::getValue throws only for a time the run asks for), and matches the
+    oracle; one step more asks for a time past the table and raises."""
+    import math
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.model import STF
+    from axisem3d_b200.solver import EngineError, Solver
+    m = meshgen.cartesian_model(nx=5, nz=5, nr=5)
+    n = 40
+    t = m.t0 + np.arange(n) * m.dt
+    v = (1. - 2. * (math.pi * 2.0 * (t - t[n // 3])) ** 2) * np.exp(-(math.pi * 2.0 * (t - t[n // 3])) ** 2)
+    m.ms_stf = [STF(table=(t, v), padding=0)]
+    o = O.Oracle(m, "fp64")
+    o.run(n)
+    ref = o.get_field("displ")
+    with Solver(m, "fp64") as s:
+        if mode == "hooks":
+            for k in range(n):
+                s.apply_sources(k)
+                s.compute_stiffness()
+                s.apply_bc_before_assembly()
+                s.record_stations(k)
+                s.apply_bc_after_assembly()
+                s.stiff_to_accel()
+                s.newmark_update()
+        else:
+            for _ in range(n // 7):
+                s.run(7)
+            s.run(n % 7)
+        assert s.step == n
+        assert np.abs(ref).max() > 0 and rel(s.get_field("displ"), ref) <= 1e-11
+        with pytest.raises(EngineError):
+            s.run(1)

@@ -22,8 +22,11 @@ sys.path.insert(0, HERE)
 
 import exodus_fixture as fx  # noqa: E402
 
-REF = "/root/reference/examples"
-have_ref = pytest.mark.skipif(not os.path.isdir(REF), reason="reference examples not present")
+# the reference checkout's examples directory, named by AXISEM3D_REFERENCE (the checkout root);
+# the tests that read it are skipped where it is not set
+REF = os.path.join(os.environ.get("AXISEM3D_REFERENCE", ""), "examples")
+have_ref = pytest.mark.skipif(not os.environ.get("AXISEM3D_REFERENCE") or not os.path.isdir(REF),
+                              reason="AXISEM3D_REFERENCE (reference checkout with examples) not set")
 
 NX, NZ, W, H, R = 10, 8, 100e3, 80e3, 6371e3
 
