@@ -111,13 +111,14 @@ class Engine final : public EngineBase {
     };
     struct SolidBucket {
         int rheo, att, is3d, rtz, cls, team, tpc, qc, nr_max, n, grid = 1;
+        int mt = 1;   // Fourier modes per tile of the gather / gradient and the quadrature
         size_t team_bytes;
         DBuf<int> nr, pts;
         DBuf<uint8_t> axial;
         DBuf<T> geom, trig, mod, attmod;
         DBuf<int64_t> mod_off, att_off, state_off;
         double bytes = 0, flops = 0;
-        void (*kernel)(const SolidArgs<T, AT>, int, int, int, size_t) = nullptr;
+        void (*kernel)(const SolidArgs<T, AT>, int, int, int, int, size_t) = nullptr;
         // particle relabelling (undulated geometry): its own kernel and factors
         int prt = 0;
         DBuf<T> xpool;
@@ -833,7 +834,7 @@ private:
     }
 
     // ------------------------------------------------------- solid buckets ---
-    using SolidKernel = void (*)(const SolidArgs<T, AT>, int, int, int, size_t);
+    using SolidKernel = void (*)(const SolidArgs<T, AT>, int, int, int, int, size_t);
     // NS: the register-resident SLS recursions are built for 3 and 5 SLS (3-D slices and
     // 1-D Fourier slots); other counts take the generic path
     template <int RHEO, int ATT, bool IS3D, bool RTZ>
@@ -1040,27 +1041,39 @@ private:
         int team = team_req ? team_req
                             : (cfg_.plain ? 256 : (team_override_[b.cls] ? team_override_[b.cls] : default_team(b.cls)));
         // shared memory per team (the PRT kernel holds 9 gradient components instead of 6)
-        auto bytes_of = [&](int q) {
-            return b.prt ? prt_layout<T>(b.nr_max, q).total : team_layout<T>(b.nr_max, q).total;
+        const int nu_max = b.nr_max / 2 + 1;
+        auto bytes_of = [&](int q, int m) {
+            return b.prt ? prt_layout<T>(b.nr_max, q).total : team_layout<T>(b.nr_max, q, m).total;
         };
         const void *kfn = b.prt ? (const void *)b.pkernel : (const void *)b.kernel;
         // split the 25 points of the slice phase if needed
         const size_t budget = 200 * 1024;
-        int qc = 25;
-        size_t total = bytes_of(qc);
-        while (total > budget && qc > 1) { qc = (qc + 1) / 2; total = bytes_of(qc); }
+        int qc = 25, mt = nu_max;
+        size_t total = bytes_of(qc, mt);
+        while (total > budget && qc > 1) { qc = (qc + 1) / 2; total = bytes_of(qc, mt); }
+        if (total > budget && !b.prt) {
+            // large nr: the gather / gradient and the quadrature run over tiles of mt modes;
+            // the largest point chunk for which a tile of at least 8 modes fits (any tile
+            // with one-point chunks as the last resort)
+            for (qc = 25;; qc = (qc + 1) / 2) {
+                mt = nu_max;
+                while (mt > 1 && bytes_of(qc, mt) > budget) mt = (mt + 1) / 2;
+                total = bytes_of(qc, mt);
+                if ((total <= budget && mt >= std::min(8, nu_max)) || qc == 1) break;
+            }
+        }
         if (total > budget)
             throw Error(AXG_E_UNSUPPORTED, "SolidElement::expandWorkspace || nr too large for shared memory.");
 #if AXG_QC_FOR_TWO_CTAS
         // a one-element CTA too large for two per SM: smaller point chunks of the slice phase
         // often let a second CTA in
         // (kept only when it does: smaller chunks alone idle threads in the slice passes)
-        if (team >= 128 && b.is3d) {
+        if (team >= 128 && b.is3d && mt == nu_max) {
             const size_t two_per_sm = 110 * 1024;
             int qn = qc;
             size_t tn = total;
             while (qn > 5 && tn > two_per_sm) {
-                const size_t th = bytes_of((qn + 1) / 2);
+                const size_t th = bytes_of((qn + 1) / 2, mt);
                 if (th >= tn) break;
                 qn = (qn + 1) / 2;
                 tn = th;
@@ -1069,6 +1082,7 @@ private:
         }
 #endif
         b.qc = qc;
+        b.mt = mt;
         b.team_bytes = total;
         b.team = team;
         int tpc = std::max(1, 256 / team);
@@ -1698,7 +1712,7 @@ private:
             b.pkernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(pa, b.nr_max, b.qc, b.tpc,
                                                                                b.team_bytes);
         } else {
-            b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc, b.tpc,
+            b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc, b.mt, b.tpc,
                                                                               b.team_bytes);
         }
         post_launch();

@@ -20,7 +20,10 @@
 // Shared memory per team (T = float or double, C = complex T):
 //   geometry 10 x 25 T, trig 4 x 25 T, point tables 3 x 25 int, twiddles 2 x nr T,
 //   region A: 6 x nu x 25 C  (strain E, then stress S, then quadrature X/Y)
-//   region B: max(3 x nu x 25 C, nr x 6 x qc T)  (u, then stress slices, then A terms)
+//   region B: max(3 x mt x 25 C, nr x 6 x qc T)  (u, then stress slices, then A terms)
+// The gather + gradient and the two quadrature passes run over tiles of mt modes (each
+// Fourier mode is independent there), so region B holds one tile of u and of the A terms;
+// mt = nu unless the element's nr is too large for that (one tile, the common case).
 #pragma once
 
 #include "common.cuh"
@@ -126,11 +129,12 @@ struct TeamLayout {
 };
 
 template <class T>
-__host__ __device__ inline TeamLayout team_layout(int nr_max, int qc) {
+__host__ __device__ inline TeamLayout team_layout(int nr_max, int qc, int mt) {
     TeamLayout L;
     L.nr_max = nr_max;
     L.nu_max = nr_max / 2 + 1;
     L.qc = qc;
+    mt = mt < L.nu_max ? mt : L.nu_max;
     size_t o = 0;
     auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
     L.geom = o; o = al(o + 10 * 25 * sizeof(T));
@@ -138,7 +142,7 @@ __host__ __device__ inline TeamLayout team_layout(int nr_max, int qc) {
     L.ipt = o;  o = al(o + 3 * 25 * sizeof(int));
     L.tw = o;   o = al(o + 2 * (size_t)nr_max * sizeof(T));
     L.regA = o; o = al(o + 6 * (size_t)L.nu_max * 25 * 2 * sizeof(T));
-    size_t b1 = 3 * (size_t)L.nu_max * 25 * 2 * sizeof(T);
+    size_t b1 = 3 * (size_t)mt * 25 * 2 * sizeof(T);
     size_t b2 = (size_t)nr_max * 6 * qc * sizeof(T);
     L.regB = o; o = al(o + (b1 > b2 ? b1 : b2));
     L.total = o;
@@ -438,7 +442,7 @@ __device__ __forceinline__ int cg4_slot(int q) {
 // read at run time
 template <class T, class AT, int RHEO, int ATT, bool IS3D, bool RTZ, int NS>
 __global__ void __launch_bounds__(256, AXG_SOLID_MIN_BLOCKS)
-solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_max,
+solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_max, const int mt_max,
                        const int teams_per_cta, const size_t team_bytes) {
     using C = cx_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -457,7 +461,7 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
     __syncthreads();
     if (team >= teams_per_cta) return;
 
-    const TeamLayout L = team_layout<T>(nr_max, qc_max);
+    const TeamLayout L = team_layout<T>(nr_max, qc_max, mt_max);
     unsigned char *base = smem_raw + (size_t)team * team_bytes;
     T *sGeo = reinterpret_cast<T *>(base + L.geom);
     T *sTrig = reinterpret_cast<T *>(base + L.trig);
@@ -517,27 +521,29 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             prefetch_l2(statew + a.state_off[e], (size_t)(6 + 6 * NS) * nu * NPA_ * 2 * sizeof(AT), lane, TEAM);
         }
 #endif
-        // ---------------- gather displacement: U[a][c][q] in region B ----------------
-        for (int i = lane; i < nu * 25; i += TEAM) {
-            const int q = i / nu, al = i - q * nu;
+        const int64_t moff = a.mod_off[e];
+        const int nslice = IS3D ? nr : 1;
+        for (int t0 = 0; t0 < nu; t0 += mt_max) {
+        const int mt = min(mt_max, nu - t0);
+        // ---------------- gather displacement: U[a - t0][c][q] in region B ----------------
+        for (int i = lane; i < mt * 25; i += TEAM) {
+            const int q = i / mt, la = i - q * mt, al = t0 + la;
             C u0 = mk<T>(0, 0), u1 = u0, u2 = u0;
             if (al < sNu[q]) {
                 const C *src = displw + (size_t)(sOff[q] + al) * 3;
                 u0 = src[0]; u1 = src[1]; u2 = src[2];
             }
-            rBc[(al * 3 + 0) * 25 + q] = u0;
-            rBc[(al * 3 + 1) * 25 + q] = u1;
-            rBc[(al * 3 + 2) * 25 + q] = u2;
+            rBc[(la * 3 + 0) * 25 + q] = u0;
+            rBc[(la * 3 + 1) * 25 + q] = u1;
+            rBc[(la * 3 + 2) * 25 + q] = u2;
         }
         team_sync(team, TEAM);
 
         // ---------------- gradient (computeGrad6) ----------------
-        const int64_t moff = a.mod_off[e];
-        const int nslice = IS3D ? nr : 1;
-        for (int i = lane; i < nu * 25; i += TEAM) {
-            const int al = i / 25, q = i - al * 25;
+        for (int i = lane; i < mt * 25; i += TEAM) {
+            const int la = i / 25, q = i - la * 25, al = t0 + la;
             const int ii = q / 5, jj = q - ii * 5;
-            const C *U = rBc + al * 75;
+            const C *U = rBc + la * 75;
             C X[3], Y[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
@@ -627,6 +633,7 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             }
         }
         team_sync(team, TEAM);
+        }   // mode tiles of the gather + gradient
 
         // ---------------- 1-D attenuation: stress pass, SLS state in registers ----------------
         // strainToStress_FR on the strain left in region A, then the SLS recursion of each
@@ -960,9 +967,11 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             }
         }
 
+        for (int t0 = 0; t0 < nu; t0 += mt_max) {
+        const int mt = min(mt_max, nu - t0);
         // ---------------- quadrature (computeQuad6), pass 1: X, Y, A ----------------
-        for (int i = lane; i < nu * 25; i += TEAM) {
-            const int al = i / 25, q = i - al * 25;
+        for (int i = lane; i < mt * 25; i += TEAM) {
+            const int la = i / 25, q = i - la * 25, al = t0 + la;
             C s[6];
 #pragma unroll
             for (int d = 0; d < 6; d++) s[d] = rA[(al * 6 + d) * 25 + q];
@@ -975,18 +984,18 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             xy[4 * 25 + q] = cadd(cscale(s[4], ze), cscale(s[2], se));
             xy[5 * 25 + q] = cadd(cscale(s[4], zx), cscale(s[2], sx));
             const T alf = (T)al;
-            rBc[(al * 3 + 0) * 25 + q] = csub(cia(alf, s[5]), s[1]);
-            rBc[(al * 3 + 1) * 25 + q] = cadd(cia(alf, s[1]), s[5]);
-            rBc[(al * 3 + 2) * 25 + q] = cia(alf, s[3]);
+            rBc[(la * 3 + 0) * 25 + q] = csub(cia(alf, s[5]), s[1]);
+            rBc[(la * 3 + 1) * 25 + q] = cadd(cia(alf, s[1]), s[5]);
+            rBc[(la * 3 + 2) * 25 + q] = cia(alf, s[3]);
         }
         team_sync(team, TEAM);
 
         // ---------------- quadrature pass 2 + scatter-add ----------------
-        for (int i = lane; i < nu * 25; i += TEAM) {
-            const int al = i / 25, q = i - al * 25;
+        for (int i = lane; i < mt * 25; i += TEAM) {
+            const int la = i / 25, q = i - la * 25, al = t0 + la;
             const int ii = q / 5, jj = q - ii * 5;
             const C *xy = rA + al * 150;
-            const C *A = rBc + al * 75;
+            const C *A = rBc + la * 75;
             C f[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
@@ -1025,6 +1034,7 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             }
         }
         team_sync(team, TEAM);
+        }   // mode tiles of the quadrature
         }   // wavefields
     }
 }

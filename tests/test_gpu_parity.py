@@ -76,26 +76,42 @@ def test_stiffness_parity(built, case, precision):
     assert rel(f2, ref2) <= TOL_STIFF[precision], rel(f2, ref2)
 
 
+LARGE_NR = {
+    # (nr_min, nr_max) per precision: FP64 up to 128 (the spherical-shell workload's range),
+    # FP32 / mixed up to 256
+    "fp64": (96, 128), "fp32": (200, 256), "mixed": (200, 256),
+}
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
-def test_large_nr_chunked_slices(built, precision):
-    """nr up to 128 (the spherical-shell workload): the slice phase is split over
-    points when shared memory is short."""
+@pytest.mark.parametrize("kind", ["tiso_3d_full", "tiso_1d_full", "aniso_3d_axial"])
+def test_large_nr_mode_tiles(built, precision, kind):
+    """Large nr: an element's modes no longer fit shared memory whole, so the gather /
+    gradient and the quadrature run over tiles of modes and the slice phase over chunks of
+    points. Two evaluations in a row against the FP64 oracle (the second exercises the SLS
+    memory of every slice or mode)."""
     from axisem3d_b200 import meshgen
-    from axisem3d_b200.solver import Solver, EngineError
-    m = meshgen.microbench_model(n_elem=16, nr_min=90, nr_max=128, seed=31)
+    from axisem3d_b200.solver import Solver
+    lo, hi = LARGE_NR[precision]
+    if kind == "tiso_3d_full":
+        lo = hi          # every element at the largest nr: 128 in FP64, 256 in FP32 / mixed
+    kw = {"tiso_3d_full": dict(),
+          "tiso_1d_full": dict(is3d=False),
+          "aniso_3d_axial": dict(rheology="aniso", attenuation=None, axial_column=True)}[kind]
+    m = meshgen.microbench_model(n_elem=12, nr_min=lo, nr_max=hi, seed=31, **kw)
+    assert m.se_nr.max() >= hi - 4
     u = meshgen.random_displacement(m, seed=6)
-    ref = _oracle_stiff(m, u)
-    try:
-        s = Solver(m, precision)
-    except EngineError as e:
-        # FP64 with nr > ~100 does not fit one element's workspace in shared memory
-        assert precision == "fp64" and "shared memory" in str(e)
-        return
-    with s:
+    ref1 = _oracle_stiff(m, u, 1)
+    ref2 = _oracle_stiff(m, u, 2)
+    with Solver(m, precision) as s:
         s.set_field(u, "displ")
         s.compute_stiffness()
-        f = s.get_field("stiff")
-    assert rel(f, ref) <= TOL_STIFF[precision]
+        f1 = s.get_field("stiff")
+        s.set_field(np.zeros_like(u), "stiff")
+        s.compute_stiffness()
+        f2 = s.get_field("stiff")
+    assert rel(f1, ref1) <= TOL_STIFF[precision], rel(f1, ref1)
+    assert rel(f2, ref2) <= TOL_STIFF[precision], rel(f2, ref2)
 
 
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("fp32", 1e-5), ("mixed", 1e-5)])
@@ -743,7 +759,10 @@ def test_table_stf_without_padding_to_the_last_step(built, mode):
             for _ in range(n // 7):
                 s.run(7)
             s.run(n % 7)
-        assert s.step == n
+            assert s.step == n
         assert np.abs(ref).max() > 0 and rel(s.get_field("displ"), ref) <= 1e-11
         with pytest.raises(EngineError):
-            s.run(1)
+            if mode == "hooks":
+                s.apply_sources(n)
+            else:
+                s.run(1)
