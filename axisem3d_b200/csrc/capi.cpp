@@ -637,6 +637,18 @@ int axg_compute_stiffness_noalloc(axg_solver *h, const void *solid_x, void *soli
         h->eng->stiffness_noalloc(solid_x, solid_f, fluid_x, fluid_f, scratch, AXG_NOALLOC_SCRATCH_BYTES);
     });
 }
+int axg_gather_stiffness(axg_solver *h, int32_t solid, int64_t n, const int64_t *slots, void *buf) {
+    return guarded(h, [&] {
+        if (!h->finalized) throw axg::Error(AXG_E_STATE, "axg_gather_stiffness || axg_finalize not called.");
+        h->eng->gather_stiffness(solid, n, slots, buf);
+    });
+}
+int axg_scatter_add_stiffness(axg_solver *h, int32_t solid, int64_t n, const int64_t *slots, const void *buf) {
+    return guarded(h, [&] {
+        if (!h->finalized) throw axg::Error(AXG_E_STATE, "axg_scatter_add_stiffness || axg_finalize not called.");
+        h->eng->scatter_add_stiffness(solid, n, slots, buf);
+    });
+}
 int axg_apply_bc_before_assembly(axg_solver *h) {
     return guarded(h, [&] { h->eng->bc_before(); });
 }

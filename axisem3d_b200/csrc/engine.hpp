@@ -222,6 +222,9 @@ public:
     virtual void stiffness_noalloc(const void *sx, void *sf, const void *fx, void *ff, void *scratch,
                                    size_t cap) = 0;
     virtual int device() const = 0;
+    // boundary-stiffness exchange: n complex stiffness values at device slots <-> device buffer
+    virtual void gather_stiffness(int solid, int64_t n, const int64_t *slots, void *buf) = 0;
+    virtual void scatter_add_stiffness(int solid, int64_t n, const int64_t *slots, const void *buf) = 0;
     // Point::reportScanningNr per point (-1: not scanned)
     virtual void scanning_nr(int32_t *solid_nr, int32_t *fluid_nr) = 0;
 };

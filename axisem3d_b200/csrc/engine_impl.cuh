@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <tuple>
 
@@ -56,6 +57,10 @@ struct DBuf {
 
 // team size per nr class and the nr class boundaries
 inline int nr_class(int nr) { return nr <= 3 ? 0 : nr <= 9 ? 1 : nr <= 25 ? 2 : nr <= 64 ? 3 : 4; }
+// smallest nr of a 3-D element that takes the slice FFTs instead of the direct sums (0 = never)
+#ifndef AXG_FFT_MIN_NR
+#define AXG_FFT_MIN_NR 65
+#endif
 inline int default_team(int cls) { static const int t[5] = {32, 64, 128, 256, 256}; return t[cls]; }
 
 template <class T>
@@ -112,6 +117,7 @@ class Engine final : public EngineBase {
     struct SolidBucket {
         int rheo, att, is3d, rtz, cls, team, tpc, qc, nr_max, n, grid = 1;
         int mt = 1;   // Fourier modes per tile of the gather / gradient and the quadrature
+        int fft = 0;  // 3-D elements of nr >= AXG_FFT_MIN_NR take the slice FFTs
         size_t team_bytes;
         DBuf<int> nr, pts;
         DBuf<uint8_t> axial;
@@ -646,7 +652,35 @@ public:
     }
     int device() const override { return cfg_.device; }
 
+    void gather_stiffness(int solid, int64_t n, const int64_t *slots, void *buf) override {
+        need();
+        PointDev &P = solid ? sp_ : fp_;
+        check_slots("axg_gather_stiffness || ", P, n, slots, buf);
+        if (n == 0) return;
+        const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)prop_.multiProcessorCount * 8);
+        gather_slots_kernel<C><<<blocks, 256, 0, stream_>>>(P.stiff.p, slots, n, reinterpret_cast<C *>(buf));
+        post_launch();
+    }
+    void scatter_add_stiffness(int solid, int64_t n, const int64_t *slots, const void *buf) override {
+        need();
+        PointDev &P = solid ? sp_ : fp_;
+        check_slots("axg_scatter_add_stiffness || ", P, n, slots, buf);
+        if (n == 0) return;
+        const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)prop_.multiProcessorCount * 8);
+        scatter_add_slots_kernel<C><<<blocks, 256, 0, stream_>>>(P.stiff.p, slots, n, reinterpret_cast<const C *>(buf));
+        post_launch();
+    }
+
 private:
+    void check_slots(const char *who, const PointDev &P, int64_t n, const int64_t *slots, const void *buf) const {
+        if (n < 0) throw Error(AXG_E_ARG, std::string(who) + "negative count.");
+        if (n > 0 && (!slots || !buf)) throw Error(AXG_E_ARG, std::string(who) + "slot or buffer pointer missing.");
+        if (n > (int64_t)P.total * P.ndim)
+            throw Error(AXG_E_ARG, std::string(who) + "more slots than the field holds.");
+        if (nwave_ != 1) throw Error(AXG_E_UNSUPPORTED, std::string(who) + "one wavefield per handle.");
+        if ((reinterpret_cast<uintptr_t>(buf) % alignof(C)) != 0)
+            throw Error(AXG_E_ARG, std::string(who) + "buffer must be aligned to a complex value.");
+    }
     void check_adjoint_model() const {
         const HostSolidElements &h = model_.se;
         if (fp_.n > 0) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || fluid elements are not differentiated.");
@@ -705,8 +739,7 @@ private:
         int nu_max = adj_nr_max_ / 2 + 1;
         size_t smem = (size_t)nu_max * 300 * sizeof(C);
         if (smem > 200 * 1024) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || nr too large.");
-        AXG_CUDA(cudaFuncSetAttribute((const void *)adjoint_stiffness_kernel<T>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        raise_smem_limit((const void *)adjoint_stiffness_kernel<T>, smem);
         adj_built_ = true;
     }
 
@@ -838,37 +871,44 @@ private:
     // NS: the register-resident SLS recursions are built for 3 and 5 SLS (3-D slices and
     // 1-D Fourier slots); other counts take the generic path
     template <int RHEO, int ATT, bool IS3D, bool RTZ>
-    static SolidKernel pick4(int nsls) {
+    static SolidKernel pick4(int nsls, bool fft) {
 #ifndef AXG_GENERIC_SLS_ONLY
         if constexpr (ATT != ATT_NONE) {
+            if constexpr (IS3D) {
+                if (fft && nsls == 3) return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 3, true>;
+                if (fft && nsls == 5) return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 5, true>;
+            }
             if (nsls == 3) return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 3>;
             if (nsls == 5) return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 5>;
         }
 #endif
+        if constexpr (IS3D && ATT == ATT_NONE) {
+            if (fft) return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 0, true>;
+        }
         return solid_stiffness_kernel<T, AT, RHEO, ATT, IS3D, RTZ, 0>;
     }
     template <int RHEO, int ATT, bool IS3D>
-    static SolidKernel pick3(bool rtz, int nsls) {
-        if constexpr (RHEO == RHEO_ISO) return pick4<RHEO, ATT, IS3D, false>(nsls);
-        else return rtz ? pick4<RHEO, ATT, IS3D, true>(nsls) : pick4<RHEO, ATT, IS3D, false>(nsls);
+    static SolidKernel pick3(bool rtz, int nsls, bool fft) {
+        if constexpr (RHEO == RHEO_ISO) return pick4<RHEO, ATT, IS3D, false>(nsls, fft);
+        else return rtz ? pick4<RHEO, ATT, IS3D, true>(nsls, fft) : pick4<RHEO, ATT, IS3D, false>(nsls, fft);
     }
     template <int RHEO, int ATT>
-    static SolidKernel pick2(bool is3d, bool rtz, int nsls) {
-        return is3d ? pick3<RHEO, ATT, true>(rtz, nsls) : pick3<RHEO, ATT, false>(rtz, nsls);
+    static SolidKernel pick2(bool is3d, bool rtz, int nsls, bool fft) {
+        return is3d ? pick3<RHEO, ATT, true>(rtz, nsls, fft) : pick3<RHEO, ATT, false>(rtz, nsls, fft);
     }
     template <int RHEO>
-    static SolidKernel pick1(int att, bool is3d, bool rtz, int nsls) {
+    static SolidKernel pick1(int att, bool is3d, bool rtz, int nsls, bool fft) {
         switch (att) {
-            case ATT_NONE: return pick2<RHEO, ATT_NONE>(is3d, rtz, nsls);
-            case ATT_FULL: return pick2<RHEO, ATT_FULL>(is3d, rtz, nsls);
-            default: return pick2<RHEO, ATT_CG4>(is3d, rtz, nsls);
+            case ATT_NONE: return pick2<RHEO, ATT_NONE>(is3d, rtz, nsls, fft);
+            case ATT_FULL: return pick2<RHEO, ATT_FULL>(is3d, rtz, nsls, fft);
+            default: return pick2<RHEO, ATT_CG4>(is3d, rtz, nsls, fft);
         }
     }
-    static SolidKernel pick_solid(int rheo, int att, bool is3d, bool rtz, int nsls) {
+    static SolidKernel pick_solid(int rheo, int att, bool is3d, bool rtz, int nsls, bool fft) {
         switch (rheo) {
-            case RHEO_ISO: return pick1<RHEO_ISO>(att, is3d, rtz, nsls);
-            case RHEO_TISO: return pick1<RHEO_TISO>(att, is3d, rtz, nsls);
-            default: return pick1<RHEO_ANISO>(att, is3d, rtz, nsls);
+            case RHEO_ISO: return pick1<RHEO_ISO>(att, is3d, rtz, nsls, fft);
+            case RHEO_TISO: return pick1<RHEO_TISO>(att, is3d, rtz, nsls, fft);
+            default: return pick1<RHEO_ANISO>(att, is3d, rtz, nsls, fft);
         }
     }
 
@@ -1023,7 +1063,11 @@ private:
                 b->xpool.upload(xpool); b->xoff.upload(xoff); b->x3d.upload(x3d);
                 b->pkernel = pick_prt(b->rheo, b->att, b->is3d, b->rtz);
             } else {
-                b->kernel = pick_solid(b->rheo, b->att, b->is3d, b->rtz, cfg_.nsls);
+                // the slice FFTs: batched 3-D buckets of the register-resident slice path that
+                // hold an nr of at least AXG_FFT_MIN_NR (the plain method keeps the direct sums)
+                const bool reg_path = b->att == ATT_NONE || cfg_.nsls == 3 || cfg_.nsls == 5;
+                b->fft = (!cfg_.plain && b->is3d && reg_path && AXG_FFT_MIN_NR > 0 && b->nr_max >= AXG_FFT_MIN_NR) ? 1 : 0;
+                b->kernel = pick_solid(b->rheo, b->att, b->is3d, b->rtz, cfg_.nsls, b->fft != 0);
             }
             configure_bucket(*b);
             sb_.push_back(std::move(b));
@@ -1069,7 +1113,10 @@ private:
         // often let a second CTA in
         // (kept only when it does: smaller chunks alone idle threads in the slice passes)
         if (team >= 128 && b.is3d && mt == nu_max) {
-            const size_t two_per_sm = 110 * 1024;
+            // the shared memory of AXG_SOLID_MIN_BLOCKS CTAs per SM (228 KB per SM, 1 KB of it
+            // reserved per CTA)
+            const size_t two_per_sm = AXG_SOLID_MIN_BLOCKS >= 3 ? (size_t)(228 / AXG_SOLID_MIN_BLOCKS - 1) * 1024
+                                                                : (size_t)110 * 1024;
             int qn = qc;
             size_t tn = total;
             while (qn > 5 && tn > two_per_sm) {
@@ -1078,7 +1125,25 @@ private:
                 qn = (qn + 1) / 2;
                 tn = th;
             }
-            if (tn <= two_per_sm) { qc = qn; total = tn; }
+            if (tn <= two_per_sm) {
+                qc = qn;
+                total = tn;
+            } else if (!cfg_.plain && !b.prt) {
+                // large nr: point chunks alone cannot get there while region B holds a whole
+                // element's modes; mode tiles of at least 8 modes as well, the largest point
+                // chunk (of at least 2 points) first
+                for (int qm = qc; qm >= 2; qm = (qm + 1) / 2) {
+                    int mm = nu_max;
+                    while (mm > 8 && bytes_of(qm, mm) > two_per_sm) mm = (mm + 1) / 2;
+                    if (bytes_of(qm, mm) <= two_per_sm) {
+                        qc = qm;
+                        mt = mm;
+                        total = bytes_of(qm, mm);
+                        break;
+                    }
+                    if (qm == 2) break;
+                }
+            }
         }
 #endif
         b.qc = qc;
@@ -1140,10 +1205,14 @@ private:
         AXG_CUDA(cudaStreamSynchronize(stream_));
     }
 
-    // several buckets can share one kernel instantiation: its dynamic shared
-    // memory limit must cover the largest of them
+    // several buckets, and several handles on one device, can share one kernel instantiation,
+    // and its dynamic shared memory limit is an attribute of the function on that device, not of
+    // a handle: the limit only ever rises, to the largest any handle has asked for
     void raise_smem_limit(const void *kernel, size_t bytes) {
-        size_t &cur = smem_limit_[kernel];
+        static std::mutex mu;
+        static std::map<std::pair<int, const void *>, size_t> limits;
+        std::lock_guard<std::mutex> lock(mu);
+        size_t &cur = limits[{cfg_.device, kernel}];
         if (bytes <= cur) return;
         cur = bytes;
         AXG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -1712,7 +1781,9 @@ private:
             b.pkernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(pa, b.nr_max, b.qc, b.tpc,
                                                                                b.team_bytes);
         } else {
-            b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(a, b.nr_max, b.qc, b.mt, b.tpc,
+            SolidArgs<T, AT> af = a;
+            af.fft_min_nr = b.fft ? AXG_FFT_MIN_NR : 0;
+            b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(af, b.nr_max, b.qc, b.mt, b.tpc,
                                                                               b.team_bytes);
         }
         post_launch();
@@ -1936,7 +2007,6 @@ private:
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
     int team_override_[5];
-    std::map<const void *, size_t> smem_limit_;
     struct Tuned { int cls, team; float ms; };
     std::vector<Tuned> tuned_;
     // differentiation

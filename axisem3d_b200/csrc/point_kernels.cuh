@@ -1128,4 +1128,28 @@ __global__ void narrow_kernel(const cx_t<D> *src, cx_t<T> *dst, size_t n) {
 template <class T>
 __global__ void advance_step_kernel(int *step) { *step += 1; }
 
+
+// ------------------------------------------------- boundary-stiffness exchange ---
+// MessageRank::gatherFromPoints / scatterToPoints (MessageRank.cpp:40-63) with
+// SolidPoint::feedComm / extractComm (SolidPoint.hpp:55-67): the point stiffness of the points a
+// rank shares with a neighbour, as a list of complex slots of the field, copied into a
+// contiguous buffer and, after the exchange, the neighbour's buffer added back.
+template <class C>
+__global__ void gather_slots_kernel(const C *__restrict__ field, const int64_t *__restrict__ slots, int64_t n,
+                                    C *__restrict__ buf) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        buf[i] = field[slots[i]];
+}
+template <class C>
+__global__ void scatter_add_slots_kernel(C *__restrict__ field, const int64_t *__restrict__ slots, int64_t n,
+                                         const C *__restrict__ buf) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        C v = field[slots[i]];
+        const C b = buf[i];
+        v.x += b.x;
+        v.y += b.y;
+        field[slots[i]] = v;
+    }
+}
+
 }  // namespace axg

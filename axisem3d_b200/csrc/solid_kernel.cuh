@@ -62,6 +62,12 @@ constexpr int ATT_NONE = 0, ATT_FULL = 1, ATT_CG4 = 2;
 #ifndef AXG_AB_ELASTIC
 #define AXG_AB_ELASTIC 4
 #endif
+// 1 = the stress pass of 3-D elements streams the SLS state of a (slice, point) in two
+// groups of three stress components (the recursion acts on each component alone), so that
+// 12 state words are live at a time instead of 24; 0 = the whole state loaded at once
+#ifndef AXG_SLS_SPLIT
+#define AXG_SLS_SPLIT 0
+#endif
 // 1 = L2 prefetch of an element's slice operands (moduli, attenuation moduli, SLS state)
 // at the start of its slice phase
 #ifndef AXG_PREFETCH_SLICES
@@ -120,6 +126,7 @@ struct SolidArgs {
     int nwave;                 // wavefields sharing the mesh (independent sources)
     size_t fstride;            // complex values between wavefields in displ / stiff
     size_t sstride;            // AT values between wavefields in the state pool
+    int fft_min_nr;            // 3-D elements with nr >= this (and 13-smooth nr) take the FFT; 0 = never
 };
 
 // shared memory layout of one team
@@ -366,6 +373,56 @@ __device__ __forceinline__ void attenuate_regs(const AT *alpha, const AT *beta, 
     for (int d = 0; d < 6; d++) s[d] = (T)sv[d];
 }
 
+// SLS recursion on one real slice point with the state streamed from memory in two groups of
+// three stress components, (0, 1, 2) then (3, 4, 5): each group loads its 3 + 3 NS words at once,
+// updates them with the steps and order of attenuate_regs (per component the same operations,
+// so the same results) and stores them back. State word j of the slot is at j * nslot + slot.
+template <int NS, class T, class AT>
+__device__ __forceinline__ void attenuate_slice_split(const AT *alpha, const AT *beta, const AT *gamma, AT *st,
+                                                      size_t nslot, size_t slot, const T e[6], T s[6], T dl,
+                                                      T dm) {
+    const AT lam = (AT)dl, mu = (AT)dm, mu2 = mu + mu;
+#pragma unroll
+    for (int g = 0; g < 2; g++) {
+        const int d0 = 3 * g;
+        AT ds[3], mem[NS][3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) ds[c] = state_ld(st + (d0 + c) * nslot + slot);
+#pragma unroll
+        for (int l = 0; l < NS; l++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) mem[l][c] = state_ld(st + (6 + l * 6 + d0 + c) * nslot + slot);
+        AT dn[3];
+        if (g == 0) {
+            const AT e0 = (AT)e[0], e1 = (AT)e[1], e2 = (AT)e[2];
+            const AT sii = (e0 + e1 + e2) * lam;
+            dn[0] = sii + e0 * mu2;
+            dn[1] = sii + e1 * mu2;
+            dn[2] = sii + e2 * mu2;
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++) dn[c] = (AT)e[3 + c] * mu;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            AT sv = (AT)s[d0 + c];
+#pragma unroll
+            for (int l = 0; l < NS; l++) {
+                sv -= mem[l][c];
+                mem[l][c] = alpha[l] * mem[l][c] + beta[l] * ds[c];
+            }
+#pragma unroll
+            for (int l = 0; l < NS; l++) mem[l][c] += gamma[l] * dn[c];
+            s[d0 + c] = (T)sv;
+            state_st(st + (d0 + c) * nslot + slot, dn[c]);
+        }
+#pragma unroll
+        for (int l = 0; l < NS; l++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) state_st(st + (6 + l * 6 + d0 + c) * nslot + slot, mem[l][c]);
+    }
+}
+
 // SLS recursion on one complex Fourier-space slot of a 1-D element, state in registers. The
 // recursion is linear and acts on each stress component separately, on the real and the
 // imaginary parts alike, so the slot runs in four passes: (real, imaginary) x (components
@@ -436,11 +493,166 @@ __device__ __forceinline__ int cg4_slot(int q) {
     return q == 6 ? 0 : q == 8 ? 1 : q == 16 ? 2 : q == 18 ? 3 : -1;
 }
 
+// ------------------------------------------------------------- slice FFT ---
+// The phi transforms of a 3-D element (SolverFFTW::computeC2R / computeR2C, SolverFFTW.hpp:
+// 101-172: R2C scaled by 1/nr, the Nyquist mode halved, imaginary parts of modes 0 and nr/2
+// dropped; C2R with the Nyquist mode doubled) as complex FFTs of length nr over a batch of
+// S = 3 qc signals: the six strain / stress components of a point go in pairs, x_2p + i x_2p+1,
+// one complex signal per pair. The FFT is a mixed-radix Stockham transform in shared memory
+// (radices 4, 2, 3, 5, 7, 11, 13: every nr the reference's lucky-number rule admits), one pass
+// per radix between two buffers. Signal s = pair pp of
+// point qq of the chunk (s = pp qc + qq), sample n. The two buffers are views of shared memory
+// the element holds anyway: region B as [n][pp][qq] (row n of 3 qc values), and the columns of
+// the chunk's points in region A, whose strain the spectra were formed from and whose stress
+// the last pass's unpacking writes, as rows 3 n + pp of 25 values. Twiddles come from the
+// element's table of exp(2 pi i j / nr).
+
+// radices of n, powers of 4 first, then 2, 3, 5, 7, 11, 13, packed 3 bits per pass (codes
+// 1..7 for 4, 2, 3, 5, 7, 11, 13) into the returned plan; 0 if n has another prime factor
+// (those transforms take the direct sums)
+__device__ __forceinline__ unsigned fft_plan(int n) {
+    unsigned plan = 0;
+    int c = 0;
+    while (n % 4 == 0) { plan |= 1u << (3 * c++); n /= 4; }
+    while (n % 2 == 0) { plan |= 2u << (3 * c++); n /= 2; }
+    while (n % 3 == 0) { plan |= 3u << (3 * c++); n /= 3; }
+    while (n % 5 == 0) { plan |= 4u << (3 * c++); n /= 5; }
+    while (n % 7 == 0) { plan |= 5u << (3 * c++); n /= 7; }
+    while (n % 11 == 0) { plan |= 6u << (3 * c++); n /= 11; }
+    while (n % 13 == 0) { plan |= 7u << (3 * c++); n /= 13; }
+    return (n == 1 && c <= 10) ? plan : 0u;
+}
+
+// twiddle exp(sign 2 pi i m / N) from the interleaved (cos, sin) table
+template <class T>
+__device__ __forceinline__ cx_t<T> fft_tw(const cx_t<T> *tw2, int m, int sign) {
+    const cx_t<T> w = tw2[m];
+    return mk<T>(w.x, sign > 0 ? w.y : -w.y);
+}
+template <class T>
+__device__ __forceinline__ cx_t<T> cmul(cx_t<T> a, cx_t<T> b) {
+    return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// in-register DFT of R points with sign: V_t = sum_r v_r exp(sign 2 pi i r t / R)
+template <int R, class T>
+__device__ __forceinline__ void fft_radix(cx_t<T> v[R], int sign, const cx_t<T> *tw2, int N) {
+    using C = cx_t<T>;
+    if constexpr (R == 2) {
+        const C a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        const C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        const C s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
+        // j d13 with j = sign i
+        const C jd = sign > 0 ? mk<T>(-d13.y, d13.x) : mk<T>(d13.y, -d13.x);
+        v[0] = cadd(s02, s13);
+        v[2] = csub(s02, s13);
+        v[1] = cadd(d02, jd);
+        v[3] = csub(d02, jd);
+    } else {
+        C V[R];
+        const int step = N / R;
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+            C acc = v[0];
+#pragma unroll
+            for (int r = 1; r < R; r++) acc = cadd(acc, cmul<T>(v[r], fft_tw<T>(tw2, ((r * t) % R) * step, sign)));
+            V[t] = acc;
+        }
+#pragma unroll
+        for (int t = 0; t < R; t++) v[t] = V[t];
+    }
+}
+
+// a batch of signals in shared memory: sample n of signal (pp, qq) at p[n rs + pp ps + qq]
+template <class T>
+struct FftView {
+    cx_t<T> *p;
+    int rs, ps;
+    __device__ __forceinline__ cx_t<T> &at(int n, int pp, int qq) const { return p[n * rs + pp * ps + qq]; }
+};
+
+// one Stockham pass of radix R over 3 qc signals: Ns = product of the earlier radices
+template <int R, class T>
+__device__ __forceinline__ void fft_pass_r(const FftView<T> in, const FftView<T> out, int N, int qc, int Ns,
+                                           int sign, const cx_t<T> *tw2, int lane, int TEAM) {
+    using C = cx_t<T>;
+    const int S = 3 * qc;
+    const int NR = N / R, span = N / (Ns * R);
+    for (int i = lane; i < NR * S; i += TEAM) {
+        const int j = i / S, s = i - j * S;
+        const int pp = s / qc, qq = s - pp * qc;
+        const int k = j % Ns;
+        C v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = in.at(j + r * NR, pp, qq);
+        const int step = k * span;
+        int m = 0;
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+            m += step;
+            m = m >= N ? m - N : m;
+            if (step) v[r] = cmul<T>(v[r], fft_tw<T>(tw2, m, sign));
+        }
+        const int d = (j / Ns) * Ns * R + k;
+        if constexpr (R >= 11) {
+            // the larger primes: each output summed and stored in turn (fewer live registers)
+            const int stepR = N / R;
+#pragma unroll 1
+            for (int t = 0; t < R; t++) {
+                C acc = v[0];
+                int m2 = 0;
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    m2 += t;
+                    m2 = m2 >= R ? m2 - R : m2;
+                    acc = cadd(acc, cmul<T>(v[r], fft_tw<T>(tw2, m2 * stepR, sign)));
+                }
+                out.at(d + t * Ns, pp, qq) = acc;
+            }
+        } else {
+            fft_radix<R, T>(v, sign, tw2, N);
+#pragma unroll
+            for (int r = 0; r < R; r++) out.at(d + r * Ns, pp, qq) = v[r];
+        }
+    }
+}
+
+// the whole transform of the 3 qc signals of length N from view b0 by the packed plan, passes
+// alternating between b0 and b1; returns the view that holds the result (natural order); the
+// team synchronises after every pass
+template <class T>
+__device__ __forceinline__ FftView<T> fft_run(FftView<T> b0, FftView<T> b1, int N, int qc, unsigned plan,
+                                              int sign, const cx_t<T> *tw2, int team, int lane, int TEAM) {
+    FftView<T> in = b0, out = b1;
+    int Ns = 1;
+    for (; plan; plan >>= 3) {
+        int R;
+        switch (plan & 7u) {
+            case 1: fft_pass_r<4, T>(in, out, N, qc, Ns, sign, tw2, lane, TEAM); R = 4; break;
+            case 2: fft_pass_r<2, T>(in, out, N, qc, Ns, sign, tw2, lane, TEAM); R = 2; break;
+            case 3: fft_pass_r<3, T>(in, out, N, qc, Ns, sign, tw2, lane, TEAM); R = 3; break;
+            case 4: fft_pass_r<5, T>(in, out, N, qc, Ns, sign, tw2, lane, TEAM); R = 5; break;
+            case 5: fft_pass_r<7, T>(in, out, N, qc, Ns, sign, tw2, lane, TEAM); R = 7; break;
+            case 6: fft_pass_r<11, T>(in, out, N, qc, Ns, sign, tw2, lane, TEAM); R = 11; break;
+            default: fft_pass_r<13, T>(in, out, N, qc, Ns, sign, tw2, lane, TEAM); R = 13; break;
+        }
+        team_sync(team, TEAM);
+        Ns *= R;
+        const FftView<T> t = in; in = out; out = t;
+    }
+    return in;
+}
+
 // ----------------------------------------------------------------- kernel ---
 // NS: compile-time number of SLS for the register-resident recursions (the slice path of 3-D
 // elements, the Fourier-space path of 1-D elements); 0 = the generic path with the count
 // read at run time
-template <class T, class AT, int RHEO, int ATT, bool IS3D, bool RTZ, int NS>
+// FFT: the instantiation that holds the slice FFTs (3-D buckets with large nr); the others
+// keep only the direct sums, so the FFT code costs them no registers
+template <class T, class AT, int RHEO, int ATT, bool IS3D, bool RTZ, int NS, bool FFT = false>
 __global__ void __launch_bounds__(256, AXG_SOLID_MIN_BLOCKS)
 solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_max, const int mt_max,
                        const int teams_per_cta, const size_t team_bytes) {
@@ -697,9 +909,50 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 }
             }
 #endif
+            // the FFT path (register-resident slice path only): an nr the plan covers
+            unsigned plan = 0;
+            if constexpr (FFT && (NS > 0 || ATT == ATT_NONE)) {
+                if (a.fft_min_nr > 0 && nr >= a.fft_min_nr) plan = fft_plan(nr);
+            }
+            const bool use_fft = FFT && plan != 0;
             for (int q0 = 0; q0 < 25; q0 += qc_max) {
                 const int qcnt = min(qc_max, 25 - q0);
+                // slices of this chunk: [k][d][qq] reals in region B (direct sums) or, on the
+                // FFT path, x_2p + i x_2p+1 of sample k in whichever view the C2R left them
+                const FftView<T> vB{rBc, 3 * qcnt, qcnt}, vA{rA + q0, 75, 25};
+                FftView<T> vs = vB;
+                // component d of slice k at point qq: base(k, qq) + (d >> 1) sp + (d & 1) sq
+                auto sl_base = [&](int k, int qq) -> T * {
+                    return use_fft ? reinterpret_cast<T *>(&vs.at(k, 0, qq)) : rBr + (size_t)k * 6 * qcnt + qq;
+                };
                 if constexpr (NS > 0 || ATT == ATT_NONE) {
+                constexpr int NM = RHEO == RHEO_ISO ? 2 : RHEO == RHEO_TISO ? 5 : 21;
+                constexpr int NSR = NS > 0 ? NS : 1;
+                constexpr int NPA = ATT == ATT_CG4 ? 4 : 25;
+                const T *modp = a.mod + moff;
+                const size_t nsl = (size_t)nslice * 25;
+                if (FFT && use_fft) {
+                    // Hermitian spectra of the component pairs, Z = Y_2p + i Y_2p+1 over all nr
+                    // orders: Y_0 = Re c_0, Y_a = c_a, Y_nr-a = conj c_a, Y_nr/2 = 2 Re c_nr/2
+                    for (int i = lane; i < (nr / 2 + 1) * qcnt; i += TEAM) {
+                        const int al = i / qcnt, qq = i - al * qcnt, q = q0 + qq;
+#pragma unroll
+                        for (int pp = 0; pp < 3; pp++) {
+                            const C c1 = rA[(al * 6 + 2 * pp) * 25 + q], c2 = rA[(al * 6 + 2 * pp + 1) * 25 + q];
+                            if (al == 0) {
+                                vB.at(0, pp, qq) = mk<T>(c1.x, c2.x);
+                            } else if (2 * al == nr) {
+                                vB.at(al, pp, qq) = mk<T>((T)2 * c1.x, (T)2 * c2.x);
+                            } else {
+                                vB.at(al, pp, qq) = mk<T>(c1.x - c2.y, c1.y + c2.x);
+                                vB.at(nr - al, pp, qq) = mk<T>(c1.x + c2.y, c2.x - c1.y);
+                            }
+                        }
+                    }
+                    team_sync(team, TEAM);
+                    // from here on the chunk's columns of region A are free until the unpacking
+                    vs = fft_run<T>(vB, vA, nr, qcnt, plan, +1, tw2, team, lane, TEAM);
+                } else {
                 // Register-resident slice path. Two passes:
                 //  1. computeC2R, one thread per (slice pair, point): slices k and nr - k
                 //     share their twiddles (cos equal, sin opposite), so one pass over the
@@ -709,11 +962,6 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 //  2. one thread per (slice, point): the global operands of the point-slice
                 //     (moduli, attenuation moduli, SLS state) are loaded into registers,
                 //     stress and attenuation applied, the state stored back.
-                constexpr int NM = RHEO == RHEO_ISO ? 2 : RHEO == RHEO_TISO ? 5 : 21;
-                constexpr int NSR = NS > 0 ? NS : 1;
-                constexpr int NPA = ATT == ATT_CG4 ? 4 : 25;
-                const T *modp = a.mod + moff;
-                const size_t nsl = (size_t)nslice * 25;
 #if AXG_SLICE_PAIRS
                 // KPc slice pairs per thread: each mode value read from shared memory feeds
                 // 2 KPc products
@@ -763,8 +1011,11 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 }
                 team_sync(team, TEAM);
 #endif
+                }   // direct Fourier -> slice sums
+                const int sp = use_fft ? 2 * vs.ps : 2 * qcnt, sq = use_fft ? 1 : qcnt;
                 for (int i = lane; i < nr * qcnt; i += TEAM) {
                     const int k = i / qcnt, qq = i - k * qcnt, q = q0 + qq;
+                    T *slb = sl_base(k, qq);
                     T md[NM];
 #pragma unroll
                     for (int mm = 0; mm < NM; mm++) md[mm] = __ldg(modp + mm * nsl + (size_t)k * 25 + q);
@@ -783,18 +1034,20 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                             const T *am = a.attmod + a.att_off[e];
                             dl = __ldg(am + slot);
                             dmu = __ldg(am + nslot + slot);
+#if !AXG_SLS_SPLIT
 #pragma unroll
                             for (int d = 0; d < 6; d++) ds[d] = state_ld(st + d * nslot + slot);
 #pragma unroll
                             for (int l = 0; l < NSR; l++)
 #pragma unroll
                                 for (int d = 0; d < 6; d++) mem[l][d] = state_ld(st + (6 + l * 6 + d) * nslot + slot);
+#endif
                         }
                     }
                     T acc[6];
 #if AXG_SLICE_PAIRS
 #pragma unroll
-                    for (int d = 0; d < 6; d++) acc[d] = rBr[((size_t)k * 6 + d) * qcnt + qq];
+                    for (int d = 0; d < 6; d++) acc[d] = slb[(d >> 1) * sp + (d & 1) * sq];
 #else
                     // computeC2R at slice k: r = Re c0 + 2 sum Re(c_a e^{i a phi_k})
 #pragma unroll
@@ -827,6 +1080,12 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                             T e6[6], s6[6];
 #pragma unroll
                             for (int d = 0; d < 6; d++) { e6[d] = ev[d].x; s6[d] = sg[d].x; }
+#if AXG_SLS_SPLIT
+                            attenuate_slice_split<NSR, T, AT>(a.alpha, a.beta, a.gamma, st, nslot, slot, e6, s6, dl,
+                                                              dmu);
+#pragma unroll
+                            for (int d = 0; d < 6; d++) sg[d].x = s6[d];
+#else
                             attenuate_regs<NSR, T, AT>(a.alpha, a.beta, a.gamma, ds, mem, e6, s6, dl, dmu);
 #pragma unroll
                             for (int d = 0; d < 6; d++) sg[d].x = s6[d];
@@ -836,10 +1095,11 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                             for (int l = 0; l < NSR; l++)
 #pragma unroll
                                 for (int d = 0; d < 6; d++) state_st(st + (6 + l * 6 + d) * nslot + slot, mem[l][d]);
+#endif
                         }
                     }
 #pragma unroll
-                    for (int d = 0; d < 6; d++) rBr[((size_t)k * 6 + d) * qcnt + qq] = sg[d].x;
+                    for (int d = 0; d < 6; d++) slb[(d >> 1) * sp + (d & 1) * sq] = sg[d].x;
                 }
                 } else
                 // Fourier -> slices (computeC2R), stress, attenuation -> rBr[k][d][qq]
@@ -906,6 +1166,36 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                     }
                 }
                 team_sync(team, TEAM);
+                if (FFT && use_fft) {
+                    // forward FFT of the stress pairs, then each pair's two spectra:
+                    // S_2p = (Z_a + conj Z_nr-a) / 2, S_2p+1 = (Z_a - conj Z_nr-a) / 2i, scaled by 1/nr
+                    // an even number of passes in all: the spectra end in region B, and the
+                    // unpacking below writes the chunk's columns of region A without a race
+                    const FftView<T> Z = fft_run<T>(vs, vs.p == rBc ? vA : vB, nr, qcnt, plan, -1, tw2, team, lane, TEAM);
+                    const T h = (T)0.5 * inv_nr;
+                    for (int i = lane; i < nu * qcnt; i += TEAM) {
+                        const int al = i / qcnt, qq = i - al * qcnt, q = q0 + qq;
+                        const int bl = al == 0 ? 0 : nr - al;
+                        C sg[6];
+#pragma unroll
+                        for (int pp = 0; pp < 3; pp++) {
+                            const C za = Z.at(al, pp, qq), zb = Z.at(bl, pp, qq);
+                            T r1 = (za.x + zb.x) * h, m1 = (za.y - zb.y) * h;
+                            T r2 = (za.y + zb.y) * h, m2 = (zb.x - za.x) * h;
+                            if (al == 0) { m1 = 0; m2 = 0; }
+                            if ((nr & 1) == 0 && 2 * al == nr) { r1 *= (T)0.5; r2 *= (T)0.5; m1 = 0; m2 = 0; }
+                            sg[2 * pp] = mk<T>(r1, m1);
+                            sg[2 * pp + 1] = mk<T>(r2, m2);
+                        }
+                        if constexpr (RTZ) {
+                            rtz_to_spz6(sg, sTrig[q], sTrig[25 + q], sTrig[50 + q], sTrig[75 + q]);
+                        }
+#pragma unroll
+                        for (int d = 0; d < 6; d++) rA[(al * 6 + d) * 25 + q] = sg[d];
+                    }
+                    team_sync(team, TEAM);
+                    continue;
+                }
                 // slices -> Fourier (computeR2C) into region A for these points
                 for (int i = lane; i < nab * qcnt; i += TEAM) {
                     const int ab = i / qcnt, qq = i - ab * qcnt, q = q0 + qq;

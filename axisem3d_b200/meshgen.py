@@ -612,10 +612,11 @@ def with_mass3d(m, amp=0.05, seed=0, exclude=()):
 # ---------------------------------------------------------- microbenchmark ---
 def microbench_model(n_elem=200000, nr_max=64, seed=1, rheology="tiso", attenuation="full",
                      is3d=True, nsls=3, aspect=1.25, s_offset=1.0e6, h=2.0e3, axial_column=False,
-                     nr_min=1):
+                     nr_min=1, nr_choices=None):
     """Stiffness microbenchmark: non-axial structured quads with perturbed nodes,
     per-element nr log-uniform on [1, nr_max] (points take the minimum over their
-    elements, so each element's nr is the maximum over its points)."""
+    elements, so each element's nr is the maximum over its points). nr_choices: draw each
+    element's nr uniformly from this list instead."""
     rng = np.random.Generator(np.random.PCG64(seed))
     nz = max(1, int(round(math.sqrt(n_elem / aspect))))
     nx = max(1, int(math.ceil(n_elem / nz)))
@@ -642,6 +643,9 @@ def microbench_model(n_elem=200000, nr_max=64, seed=1, rheology="tiso", attenuat
     # nr: log-uniform per element; points take the minimum over their elements
     enr = np.clip(np.rint(np.exp(rng.uniform(math.log(nr_min), math.log(nr_max), ne))),
                   nr_min, nr_max).astype(np.int32)
+    if nr_choices is not None:
+        enr = rng.choice(np.asarray(nr_choices, np.int32), ne)
+        nr_max = int(np.max(nr_choices))
     pnr = np.full(npts, nr_max + 1, np.int32)
     np.minimum.at(pnr, pts.ravel(), np.repeat(enr, 25))
     enr = np.max(pnr[pts], axis=1).astype(np.int32)
@@ -845,23 +849,55 @@ class GaussianField:
         self.a = sigma * math.sqrt(2.0 / nfeatures)
 
     def __call__(self, x, y, z):
-        out = np.zeros(np.broadcast(x, y, z).shape)
+        # evaluated with torch's multi-threaded CPU kernels (the workloads sample the field at
+        # up to ~1e9 (slice, point) positions), in float64
+        import torch
+        x, y, z = (torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)) for v in (x, y, z))
+        shape = torch.broadcast_shapes(x.shape, y.shape, z.shape)
+        out = torch.zeros(shape, dtype=torch.float64)
         for k, p in zip(self.k, self.p):
-            out += np.cos(k[0] * x + k[1] * y + k[2] * z + p)
-        return self.a * out
+            t = x * float(k[0])
+            t = t + y * float(k[1])
+            t = t + z * float(k[2])
+            out += torch.cos(t + float(p))
+        return self.a * out.numpy()
+
+    def ring_nr(self, s, z, nr_min, nr_max, energy=0.999, nsamp=512, chunk=4096):
+        """The nr that resolves the field around the axis at each (s, z): the field sampled
+        on the ring of radius s at height z (nsamp azimuths), its azimuthal power spectrum,
+        and the smallest order M whose modes 1..M hold `energy` of the power above mode 0;
+        nr = 2 M + 1, clipped to [nr_min, nr_max]."""
+        s = np.asarray(s, np.float64).ravel()
+        z = np.asarray(z, np.float64).ravel()
+        phi = 2 * np.pi * np.arange(nsamp) / nsamp
+        c, sn = np.cos(phi), np.sin(phi)
+        out = np.empty(s.size, np.int32)
+        for i0 in range(0, s.size, chunk):
+            ss, zz = s[i0:i0 + chunk, None], z[i0:i0 + chunk, None]
+            f = self(ss * c[None, :], ss * sn[None, :], zz)
+            p = np.abs(np.fft.rfft(f, axis=1)[:, 1:]) ** 2
+            cum = np.cumsum(p, axis=1)
+            tot = np.maximum(cum[:, -1:], 1e-300)
+            M = 1 + np.argmax(cum >= energy * tot, axis=1)
+            out[i0:i0 + chunk] = np.clip(2 * M + 1, nr_min, nr_max)
+        return out
 
 
 def spherical_model(n_theta=96, n_solid_layers=24, n_fluid_layers=2, r_cmb=3480e3, r_fluid_top=3600e3,
                     r_surface=6371e3, nr_min=3, nr_max=128, dlnvs=0.02, corr_length=200e3, three_d=True,
                     q_mu=300.0, q_kappa=57823.0, attenuation="cg4", rheology="iso", period=20.0,
                     source_depth=100e3, nstations=20, courant=0.6, seed=12, nr_scale=1.0,
-                    aniso_pert=0.05, record_interval=1):
+                    aniso_pert=0.05, record_interval=1, nr_from="field", nr_energy=0.99):
     """Half-annulus r in [r_cmb, r_surface], theta in [0, pi] (axis at both ends), with
     a fluid layer r in [r_cmb, r_fluid_top] (FluidElement, scalar potential) coupled to
     the solid above, spherical mapping, a seeded 1-D layered background and (three_d)
-    a Gaussian random-field dlnVs sampled on each element's phi slices. Element nr
-    grows with the distance from the axis, nr = clip(round(nr_scale * pi s / L), nr_min,
-    nr_max) at the element centre, and points take the minimum over their elements.
+    a Gaussian random-field dlnVs sampled on each element's phi slices.
+    Element nr (nr_from = "field"): the azimuthal bandwidth of the dlnVs field at the
+    element centre -- the order that holds `nr_energy` of the field's power around the
+    ring through that centre (GaussianField.ring_nr) -- clipped to [nr_min, nr_max] and
+    rounded up to the reference's lucky numbers (7-smooth, or one factor 11 or 13);
+    nr_from = "distance" takes nr = clip(round(nr_scale * pi s / L)) instead. Points take
+    the minimum over their elements, and an element the maximum over its points.
     rheology 'aniso' carries 21 Cij: the isotropic background plus a seeded
     positive-definite perturbation of relative size aniso_pert."""
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -914,14 +950,22 @@ def spherical_model(n_theta=96, n_solid_layers=24, n_fluid_layers=2, r_cmb=3480e
     coords[pts.ravel(), 0] = szp[:, 0, :].ravel()
     coords[pts.ravel(), 1] = szp[:, 1, :].ravel()
     coords[:, 0] = np.where(np.abs(coords[:, 0]) < 1e-6, 0.0, coords[:, 0])
-    # element nr from the distance to the axis
+    field = GaussianField(dlnvs, corr_length, seed + 1)
     sc = np.mean(szp[:, 0, :], axis=1)
-    enr = np.clip(np.rint(nr_scale * np.pi * sc / corr_length), nr_min, nr_max).astype(np.int32)
+    if nr_from == "field":
+        # element nr from the azimuthal spectrum of the dlnVs field at the element centre,
+        # rounded up to the reference's lucky numbers (NrField::nextLuckyNumber) within nr_max
+        from .preloop import next_lucky
+        enr = field.ring_nr(sc, np.mean(szp[:, 1, :], axis=1), nr_min, nr_max, nr_energy)
+        lucky = np.array([0] + [next_lucky(n) for n in range(1, nr_max + 1)])
+        enr = np.where(lucky[enr] <= nr_max, lucky[enr], enr).astype(np.int32)
+    else:
+        # element nr from the distance to the axis
+        enr = np.clip(np.rint(nr_scale * np.pi * sc / corr_length), nr_min, nr_max).astype(np.int32)
     pnr = np.full(gmax, nr_max + 1, np.int64)
     np.minimum.at(pnr, pts.ravel(), np.repeat(enr, 25))
     enr = np.max(pnr[pts], axis=1).astype(np.int32)
     sel_s, sel_f = np.nonzero(~fluid_e)[0], np.nonzero(fluid_e)[0]
-    field = GaussianField(dlnvs, corr_length, seed + 1)
     sls = default_sls(3, fmin=1.0 / (4 * period), fmax=4.0 / period)
     m = Model(dt=1.0)
     # ---- solid elements: moduli per point (1-D) or per (slice, point) (3-D)
@@ -935,45 +979,50 @@ def spherical_model(n_theta=96, n_solid_layers=24, n_fluid_layers=2, r_cmb=3480e
     att_off[1:] = np.cumsum(2 * nss * npa)[:-1]
     att_mod = np.zeros(int(np.sum(2 * nss * npa))) if attenuation else None
     wcg4 = weights_cg4(geom[sel_s, 5, :]) if attenuation == "cg4" else None
-    rho_pt = np.zeros((len(sel_s), 25))
-    vmax = 0.0
-    for k, e in enumerate(sel_s):
-        s_ = szp[e, 0, :]
-        z_ = szp[e, 1, :]
-        r_ = np.hypot(s_, z_)
-        rho0 = _interp(bg["solid"], "rho", r_)
-        vp0 = _interp(bg["solid"], "vp", r_)
-        vs0 = _interp(bg["solid"], "vs", r_)
-        rho_pt[k] = rho0
-        ns = int(nss[k])
+    # background at every solid GLL point
+    s_all, z_all = szp[sel_s, 0, :], szp[sel_s, 1, :]
+    r_all = np.hypot(s_all, z_all)
+    rho_pt = _interp(bg["solid"], "rho", r_all)
+    vp_pt = _interp(bg["solid"], "vp", r_all)
+    vs_pt = _interp(bg["solid"], "vs", r_all)
+    vmax = float(np.max(vp_pt)) if len(sel_s) else 0.0
+    # elements with one slice count at a time, in chunks of about 2M (slice, point) values:
+    # moduli of shape (chunk, ns, 25)
+    groups = []
+    for ns in np.unique(nss):
+        kall = np.nonzero(nss == ns)[0]
+        step = max(1, (1 << 21) // (int(ns) * 25))
+        groups += [(int(ns), kall[i:i + step]) for i in range(0, len(kall), step)]
+    for ns, ks in groups:
         if three_d:
             phi = 2 * np.pi * np.arange(ns) / ns
-            x = s_[None, :] * np.cos(phi)[:, None]
-            y = s_[None, :] * np.sin(phi)[:, None]
-            vs = vs0[None, :] * (1.0 + field(x, y, z_[None, :]))
+            sg = s_all[ks][:, None, :]
+            vs = vs_pt[ks][:, None, :] * (1.0 + field(sg * np.cos(phi)[None, :, None],
+                                                      sg * np.sin(phi)[None, :, None], z_all[ks][:, None, :]))
         else:
-            vs = vs0[None, :] * np.ones((1, 25))
-        vp = np.broadcast_to(vp0[None, :], vs.shape)
-        rho = np.broadcast_to(rho0[None, :], vs.shape)
-        vmax = max(vmax, float(np.max(vp)))
+            vs = vs_pt[ks][:, None, :]
+        vp = np.broadcast_to(vp_pt[ks][:, None, :], vs.shape)
+        rho = np.broadcast_to(rho_pt[ks][:, None, :], vs.shape)
         lam, mu = isotropic_moduli(rho, vp, vs)
+        blk = np.arange(ns * 25)[None, :]
         if rheology == "aniso":
             C = aniso_moduli_from(lam, mu, rng, aniso_pert)
             for c in range(21):
-                moduli[mat_off[k] + c * ns * 25: mat_off[k] + (c + 1) * ns * 25] = C[c].ravel()
+                moduli[mat_off[ks][:, None] + c * ns * 25 + blk] = C[c].reshape(len(ks), ns * 25)
             continue
         if attenuation == "full":
             lam, mu, dl, dm = iso_with_attenuation(lam, mu, q_kappa, q_mu, sls)
-            att_mod[att_off[k]:att_off[k] + ns * 25] = dl.ravel()
-            att_mod[att_off[k] + ns * 25:att_off[k] + 2 * ns * 25] = dm.ravel()
+            att_mod[att_off[ks][:, None] + blk] = dl.reshape(len(ks), ns * 25)
+            att_mod[att_off[ks][:, None] + ns * 25 + blk] = dm.reshape(len(ks), ns * 25)
         elif attenuation == "cg4":
             kp = lam + (2. / 3.) * mu
-            kp2, mu2, dl4, dm4 = cg4_correct(kp[None], np.array(mu)[None], q_kappa, q_mu, wcg4[k:k + 1], sls)
-            lam, mu = (kp2 - (2. / 3.) * mu2)[0], mu2[0]
-            att_mod[att_off[k]:att_off[k] + ns * 4] = dl4.ravel()
-            att_mod[att_off[k] + ns * 4:att_off[k] + 2 * ns * 4] = dm4.ravel()
-        moduli[mat_off[k]:mat_off[k] + ns * 25] = np.asarray(lam).ravel()
-        moduli[mat_off[k] + ns * 25:mat_off[k] + 2 * ns * 25] = np.asarray(mu).ravel()
+            kp2, mu2, dl4, dm4 = cg4_correct(kp, np.array(mu), q_kappa, q_mu, wcg4[ks], sls)
+            lam, mu = kp2 - (2. / 3.) * mu2, mu2
+            b4 = np.arange(ns * 4)[None, :]
+            att_mod[att_off[ks][:, None] + b4] = dl4.reshape(len(ks), ns * 4)
+            att_mod[att_off[ks][:, None] + ns * 4 + b4] = dm4.reshape(len(ks), ns * 4)
+        moduli[mat_off[ks][:, None] + blk] = np.asarray(lam).reshape(len(ks), ns * 25)
+        moduli[mat_off[ks][:, None] + ns * 25 + blk] = np.asarray(mu).reshape(len(ks), ns * 25)
     # ---- fluid elements: K = 1 / rho (Material::createAcoustic), 1-D
     K = np.zeros((len(sel_f), 25))
     fmass_pt = np.zeros((len(sel_f), 25))
@@ -1157,28 +1206,40 @@ def _sph_map(nodal, xi, eta):
 
 def aniso_moduli_from(lam, mu, rng, pert):
     """21 Cij per (slice, point): the isotropic tensor of (lam, mu) plus a seeded
-    symmetric perturbation of relative size `pert`, checked positive definite."""
-    lam = np.asarray(lam)
-    mu = np.asarray(mu)
+    symmetric perturbation P = pert mu R / 3, whose 21 upper-triangle entries are drawn
+    independently, zero-mean and uniform, with variance 1 on the diagonal and 1/2 off it
+    (the variances of (G + G^T) / 2 for a standard normal G), checked positive definite.
+    Returns the 21 upper-triangle arrays (row-major), each of the shape of lam."""
+    lam = np.asarray(lam, np.float64)
+    mu = np.asarray(mu, np.float64)
     shp = lam.shape
-    n = lam.size
-    C = np.zeros((n, 6, 6))
     lf, mf = lam.ravel(), mu.ravel()
-    C[:, :3, :3] = lf[:, None, None]
-    for k in range(3):
-        C[:, k, k] = lf + 2 * mf
-        C[:, 3 + k, 3 + k] = mf
-    R = rng.normal(0.0, 1.0, (n, 6, 6))
-    R = 0.5 * (R + np.transpose(R, (0, 2, 1)))
-    P = pert * mf[:, None, None] * R / 3.0
-    C = C + P
-    # the isotropic part's smallest eigenvalue is mu (shear, Voigt), so |P|_F < mu
-    # proves C positive definite; only the rest need an eigenvalue check
-    unsure = np.sqrt(np.sum(P * P, axis=(1, 2))) >= mf * (1.0 - 1e-12)
-    if np.any(unsure) and np.min(np.linalg.eigvalsh(C[unsure])) <= 0:
-        raise ValueError("perturbed Cij not positive definite")
-    iu = np.triu_indices(6)
-    return [C[:, a, b].reshape(shp) for a, b in zip(*iu)]
+    iu = list(zip(*np.triu_indices(6)))
+    R = rng.random((21, lf.size))
+    R -= 0.5
+    R *= 2.0 * math.sqrt(3.0)            # U(-sqrt 3, sqrt 3): variance 1
+    off = np.array([a != b for a, b in iu])
+    R[off] *= math.sqrt(0.5)
+    scale = pert * mf / 3.0
+    # |P|_F below the isotropic tensor's smallest eigenvalue (mu, the shear Voigt term)
+    # proves C positive definite; only the rest take an eigenvalue check
+    fro2 = np.sum(np.where(off[:, None], 2.0, 1.0) * R * R, axis=0) * scale * scale
+    out = []
+    for k, (a, b) in enumerate(iu):
+        base = np.zeros_like(lf)
+        if a < 3 and b < 3:
+            base = lf + 2 * mf if a == b else lf.copy()
+        elif a == b:
+            base = mf.copy()
+        out.append(base + scale * R[k])
+    unsure = np.nonzero(fro2 >= mf * mf * (1.0 - 1e-12))[0]
+    if unsure.size:
+        C = np.zeros((unsure.size, 6, 6))
+        for k, (a, b) in enumerate(iu):
+            C[:, a, b] = C[:, b, a] = out[k][unsure]
+        if np.min(np.linalg.eigvalsh(C)) <= 0:
+            raise ValueError("perturbed Cij not positive definite")
+    return [x.reshape(shp) for x in out]
 
 
 def ensemble_model(base, nsrc=64, seed=21, periods=(10.0, 40.0), moment_scale=1e20):

@@ -163,6 +163,20 @@ class Solver:
         axg_compute_stiffness_noalloc in include/axg.h for its limit and sharing rules)."""
         self._check(self.lib.axg_compute_stiffness_noalloc(self.h, solid_x, solid_f, fluid_x, fluid_f))
 
+    def gather_stiffness(self, slots_ptr, n, buf_ptr, solid=True):
+        """buf[i] = stiff[slots[i]] for n DEVICE slots (int64) into a DEVICE buffer of complex
+        values in the stiffness precision (MessageRank::gatherFromPoints)."""
+        self._check(self.lib.axg_gather_stiffness(self.h, int(bool(solid)), int(n), slots_ptr, buf_ptr))
+
+    def scatter_add_stiffness(self, slots_ptr, n, buf_ptr, solid=True):
+        """stiff[slots[i]] += buf[i] (MessageRank::scatterToPoints / SolidPoint::extractComm)."""
+        self._check(self.lib.axg_scatter_add_stiffness(self.h, int(bool(solid)), int(n), slots_ptr, buf_ptr))
+
+    @property
+    def complex_dtype(self):
+        """numpy dtype of the stiffness field on the device."""
+        return np.complex128 if self.precision == "fp64" else np.complex64
+
     def apply_bc_before_assembly(self):
         self._check(self.lib.axg_apply_bc_before_assembly(self.h))
 

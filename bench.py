@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--ensemble", type=int, default=64, help="sources of the ensemble leg (0 = skip)")
     p.add_argument("--no-oned", action="store_true", help="skip the 1-D (in-Fourier) leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--shell-steps", type=int, default=200,
+                   help="steps of the spherical-shell leg in each precision (0 = skip; the full run is 5000)")
+    p.add_argument("--shell-theta", type=int, default=1200, help="quads along theta of the shell leg")
     return p.parse_args()
 
 
@@ -358,6 +361,64 @@ def run_ours(args, world, rank, local):
     if not args.no_oned:
         log("1-D leg")
         out["oned"] = oned_timing(args, local, stream, world)
+    if not args.no_fp64 and args.precision != "fp32":
+        log("fp32 run")
+        with Solver(m, "fp32", device=local) as s32:
+            s32.set_stream(stream.cuda_stream)
+            s32.set_field(u0, "displ")
+            s32.run(3)
+            t32 = dist_max(time_steps(s32, max(3, args.steps // 2), stream), world)
+            out["value_fp32"] = U * max(3, args.steps // 2) * world / t32
+    if args.shell_steps > 0:
+        log("shell leg")
+        out["shell"] = shell_timing(args, local, stream, world)
+    return out
+
+
+def shell_timing(args, local, stream, world):
+    """Spherical-shell workload: a half annulus r 3480-6371 km of --shell-theta x 250 quads
+    (10 fluid layers 3480-3600 km, FluidElement, then 240 solid layers), spherical mapping, a
+    seeded piecewise-linear 1-D background with a 2 % Gaussian random field dlnVs (200 km
+    correlation) sampled on every element's slices, per-element nr from the field's azimuthal
+    bandwidth in [3, 128], CG4 attenuation with Q_mu = 300, a moment tensor with a Ricker
+    wavelet of 20 s period, 20 surface stations. From rest, --shell-steps steps in the bench
+    precision and in FP64: updates/s of each (the first 3 steps, which capture the step graph,
+    untimed), the solid stiffness kernels against the HBM roofline, and the seismograms of the
+    bench precision against FP64 (relative L2)."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = meshgen.spherical_model(n_theta=args.shell_theta, n_solid_layers=240, n_fluid_layers=10)
+    U = m.updates_per_step()
+    n = max(4, args.shell_steps)
+    peak, kind = measured_peaks()
+    out = {"workload": "spherical shell %d solid + %d fluid quads, nr %d..%d (mean %.1f) from the dlnVs field, "
+                       "iso 3-D slices, CG4 Q=300, Ricker 20 s, %d steps from rest"
+                       % (m.n_solid_elements, len(m.fe_nr), int(m.se_nr.min()), int(m.se_nr.max()),
+                          float(np.mean(m.se_nr)), n),
+           "updates_per_step": int(U), "dt": m.dt}
+    seis = {}
+    for prec in (args.precision, "fp64"):
+        with Solver(m, prec, device=local) as s:
+            s.set_stream(stream.cuda_stream)
+            s.run(3)
+            t = dist_max(time_steps(s, n - 3, stream), world)
+            seis[prec] = s.seismograms()
+            out["value_" + prec] = U * (n - 3) * world / t
+            out["ms_per_step_" + prec] = t / (n - 3) * 1e3
+            if prec == args.precision:
+                s.set_timing(True)
+                s.run(3, graph=False)
+                kms, kn = s.stiffness_time()
+                s.set_timing(False)
+                b, _ = s.stiffness_cost()
+                kms /= max(kn, 1)
+                out["stiffness_ms"] = kms
+                out["stiffness_GBps"] = b / (kms / 1e3) / 1e9
+                out["stiffness_frac_of_" + kind + "_hbm"] = out["stiffness_GBps"] / peak
+        log("shell %s done" % prec)
+    ref = seis["fp64"]
+    out["trace_rel_l2_vs_fp64"] = float(np.linalg.norm(seis[args.precision] - ref) / np.linalg.norm(ref))
+    out[args.precision + "_over_fp64"] = out["value_" + args.precision] / out["value_fp64"]
     return out
 
 
@@ -529,6 +590,12 @@ def main():
             line["ensemble"] = r["ensemble"]
         if "oned" in r:
             line["oned"] = r["oned"]
+        if "value_fp32" in r:
+            line["value_fp32"] = r["value_fp32"]
+            if "value_fp64_plain" in r:
+                line["fp32_only_over_fp64_plain"] = r["value_fp32"] / r["value_fp64_plain"]
+        if "shell" in r:
+            line["shell"] = r["shell"]
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -465,6 +465,23 @@ int  axg_set_stream(axg_solver *h, void *stream);
    4: larger); 32, 64, 128 or 256; before axg_finalize (the autotuner's knob) */
 int  axg_set_team_size(axg_solver *h, int32_t nr_class, int32_t team);
 
+/* ---- boundary-stiffness exchange of a partitioned mesh ----
+   The reference sums the stiffness of the points that MPI ranks share once per step, between
+   the boundary conditions before assembly and those after it: Messaging::commGatherSendRecv /
+   commWaitScatter (SOLVER/src/core/domain/Messaging.hpp:26-47), MessageRank::gatherFromPoints /
+   scatterToPoints (MessageRank.cpp:40-63), SolidPoint::feedComm / extractComm
+   (SolidPoint.hpp:55-67), called from NewmarkTimeScheme::solve (NewmarkTimeScheme.cpp:57-83).
+   Here a handle holds one rank's sub-mesh; the host moves the buffers between ranks (NCCL or
+   another transport). slots: DEVICE array of n indices, in complex values, into the handle's
+   solid (solid = 1) or fluid (solid = 0) stiffness field (the layout of axg_field_size:
+   [sum nu][3] or [sum nu]); buf: DEVICE buffer of n complex values in the stiffness precision
+   (complex float for AXG_FP32 / AXG_MIXED, complex double for AXG_FP64). Both run on the
+   handle's stream (axg_set_stream) and need one wavefield per handle. */
+/* buf[i] = stiff[slots[i]] */
+int  axg_gather_stiffness(axg_solver *h, int32_t solid, int64_t n, const int64_t *slots, void *buf);
+/* stiff[slots[i]] += buf[i]; the slots of one call must be distinct */
+int  axg_scatter_add_stiffness(axg_solver *h, int32_t solid, int64_t n, const int64_t *slots, const void *buf);
+
 /* ---- stiffness of a caller's field with no device allocation ----
    No counterpart in the reference. Adds -K x to f for every element of a finalized handle,
    as axg_compute_stiffness does for the handle's own displacement on a freshly created

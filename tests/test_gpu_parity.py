@@ -766,3 +766,35 @@ def test_table_stf_without_padding_to_the_last_step(built, mode):
                 s.apply_sources(n)
             else:
                 s.run(1)
+
+
+# lucky numbers above the FFT threshold (nr > 64): every radix of the slice FFTs (4, 2, 3, 5,
+# 7, 11, 13) and plans of two to four passes
+FFT_NR = [66, 70, 75, 77, 78, 81, 88, 91, 98, 99, 104, 105, 110, 117, 120, 125, 126, 128]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
+@pytest.mark.parametrize("kind", ["tiso_3d_full", "iso_3d_cg4", "aniso_3d_axial"])
+def test_slice_fft_parity(built, precision, kind):
+    """3-D elements of large nr take the slice FFTs (mixed-radix Stockham passes in shared
+    memory, component pairs as complex signals) instead of the direct sums: two evaluations
+    against the FP64 oracle's direct DFT."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    kw = {"tiso_3d_full": dict(nr_choices=FFT_NR),
+          "iso_3d_cg4": dict(nr_choices=[117], rheology="iso", attenuation="cg4"),
+          "aniso_3d_axial": dict(nr_choices=FFT_NR, rheology="aniso", attenuation=None, axial_column=True)}[kind]
+    m = meshgen.microbench_model(n_elem=60, seed=32, **kw)
+    assert m.se_nr.min() > 64
+    u = meshgen.random_displacement(m, seed=7)
+    ref1 = _oracle_stiff(m, u, 1)
+    ref2 = _oracle_stiff(m, u, 2)
+    with Solver(m, precision) as s:
+        s.set_field(u, "displ")
+        s.compute_stiffness()
+        f1 = s.get_field("stiff")
+        s.set_field(np.zeros_like(u), "stiff")
+        s.compute_stiffness()
+        f2 = s.get_field("stiff")
+    assert rel(f1, ref1) <= TOL_STIFF[precision], rel(f1, ref1)
+    assert rel(f2, ref2) <= TOL_STIFF[precision], rel(f2, ref2)
