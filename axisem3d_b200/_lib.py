@@ -139,6 +139,8 @@ SIGNATURES = {
     "axg_apply_sources": (C.c_int, [H, C.c_int32]),
     "axg_compute_stiffness": (C.c_int, [H]),
     "axg_compute_stiffness_noalloc": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "axg_set_adjoint_slices": (C.c_int, [H, C.c_int32]),
+    "axg_get_adjoint_slices": (C.c_int, [H, P_f64, P_f64]),
     "axg_gather_stiffness": (C.c_int, [H, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p]),
     "axg_scatter_add_stiffness": (C.c_int, [H, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p]),
     "axg_apply_bc_before_assembly": (C.c_int, [H]),

@@ -48,7 +48,39 @@ struct AdjointArgs {
     const T *ifact;             // [n][25] integral factor
     T *grad;                    // [n][2][25]: dJ/dlambda, dJ/dmu per element point
     const T *gmat;
+    // per-slice sensitivities (NULL = off): dJ/dlambda, dJ/dmu at the slices
+    // phi_k = 2 pi k / nr of every element point, [2][nr][25] per element from grad3_off
+    T *grad3;
+    const int64_t *grad3_off;
+    const T *tw;                // twiddle pool: for each nr, nr cos then nr sin
+    const int *tw_off;
 };
+
+// The per-slice sensitivities. A 3-D element's stress at slice k is C(phi_k) e(phi_k) with the
+// strain slices e(phi_k) = C2R(e) and the stress modes R2C(sigma) (SolverFFTW conventions), so
+// the derivative of -<g, K u> by a modulus at (slice k, point q) is
+//     -ifact_q / nr  sum_d  dsigma_d/dtheta(e_u(phi_k))  y_d(phi_k),
+//     y(phi_k) = Re E_0 + sum_{0 < a < nu} w_a Re(E_a e^{i a phi_k}),  w_a = 1/2 at a = nr/2,
+// E = e(g), the real adjoint of R2C at slice k: the conjugate-transpose sum with the R2C rules
+// (imaginary part of mode 0 dropped, the Nyquist mode halved). At phi-constant moduli with odd
+// nr a 3-D element equals the 1-D one, and these values are the gradient of the 3-D
+// parameterisation of the same step; their sum over the slices is the 1-D gradient.
+template <class T>
+__device__ __forceinline__ void slice_sums(const cx_t<T> *E, int nu, int nr, int k, const T *cs, const T *sn,
+                                           T &c2r, T &adj) {
+    // c2r = C2R(E)(phi_k) = Re E_0 + 2 sum_a Re(E_a e^{i a phi_k}); adj = y(phi_k)
+    T sum = 0, half = 0;
+    int j = 0;
+    for (int al = 1; al < nu; al++) {
+        j += k;
+        j = j >= nr ? j - nr : j;
+        const T v = E[al * 150].x * cs[j] - E[al * 150].y * sn[j];
+        if (2 * al == nr) half += v;
+        else sum += v;
+    }
+    c2r = E[0].x + (T)2 * (sum + half);
+    adj = E[0].x + sum + (T)0.5 * half;
+}
 
 // strains of one element field at (mode al, point q) from U[a][c][25] in shared memory
 template <class T>
@@ -120,6 +152,8 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
     C *Ug = reinterpret_cast<C *>(smem_raw);            // [nu][3][25] g, then A terms
     C *Uu = Ug + (size_t)nu_max * 75;                    // [nu][3][25] u
     C *S = Uu + (size_t)nu_max * 75;                     // [nu][6][25] stress of g, then X/Y
+    C *Eg = S + (size_t)nu_max * 150;                    // per-slice sensitivities only:
+    C *Eu = Eg + (size_t)nu_max * 150;                   // [nu][6][25] strains of g and of u
     for (int i = threadIdx.x; i < 25; i += blockDim.x) {
         sGll[i] = a.gmat[i];
         sGlj[i] = a.gmat[25 + i];
@@ -160,6 +194,13 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
             stress_iso(eg, sg, lam, mu);
 #pragma unroll
             for (int d = 0; d < 6; d++) S[(al * 6 + d) * 25 + q] = sg[d];
+            if (a.grad3) {
+#pragma unroll
+                for (int d = 0; d < 6; d++) {
+                    Eg[(al * 6 + d) * 25 + q] = eg[d];
+                    Eu[(al * 6 + d) * 25 + q] = eu[d];
+                }
+            }
             // sensitivities Re(conj(e(g)) . de/dm e(u)), times ifact below
             const C tg = cadd(cadd(eg[0], eg[1]), eg[2]), tu = cadd(cadd(eu[0], eu[1]), eu[2]);
             const T pl = tg.x * tu.x + tg.y * tu.y;
@@ -170,6 +211,29 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
             atomicAdd(&sGm[q], pm);
         }
         __syncthreads();
+        if (a.grad3) {
+            const T *cs = a.tw + a.tw_off[nr], *sn = cs + nr;
+            T *g3 = a.grad3 + a.grad3_off[e];
+            for (int i = threadIdx.x; i < nr * 25; i += blockDim.x) {
+                const int k = i / 25, q = i - k * 25;
+                T u6[6], y6[6];
+#pragma unroll
+                for (int d = 0; d < 6; d++) {
+                    T c_u, a_u, c_g, a_g;
+                    slice_sums<T>(Eu + d * 25 + q, nu, nr, k, cs, sn, c_u, a_u);
+                    slice_sums<T>(Eg + d * 25 + q, nu, nr, k, cs, sn, c_g, a_g);
+                    u6[d] = c_u;
+                    y6[d] = a_g;
+                }
+                const T f = a.ifact[(size_t)e * 25 + q] / (T)nr;
+                const T gl = (u6[0] + u6[1] + u6[2]) * (y6[0] + y6[1] + y6[2]);
+                T gm = 0;
+#pragma unroll
+                for (int d = 0; d < 6; d++) gm += (d < 3 ? (T)2 : (T)1) * u6[d] * y6[d];
+                g3[(size_t)k * 25 + q] -= f * gl;
+                g3[(size_t)(nr + k) * 25 + q] -= f * gm;
+            }
+        }
         // quadrature of the stress of g (computeQuad6): pass 1, X/Y in place, A terms in Ug
         const T *dsdxii_if = sGeo + 125, *dsdeta_if = sGeo + 150, *dzdxii_if = sGeo + 175,
                 *dzdeta_if = sGeo + 200, *invs_if = sGeo + 225;
@@ -276,6 +340,50 @@ __global__ void adjoint_point_kernel(const AdjPointArgs<T> a) {
     for (int c = 0; c < 3; c++) gv[c] = ab[c];
     for (int c = 0; c < 3; c++) a.g[(size_t)m * 3 + c] = gv[c];
     atomicAdd(&a.grad_mass[p], dm);
+}
+
+// per-slice mass sensitivities of step n, before adjoint_point_kernel updates the cotangents.
+// The axial and Nyquist projection acts on the stiffness before the mass term, so with a 3-D
+// mass a(phi_k) = f(phi_k) / M(phi_k) (Mass3D) the derivative by M at slice k of a point is
+// -(1/nr) sum_c a_c(phi_k) y_c(phi_k) / M, y = the adjoint R2C sum of abar_n (see slice_sums);
+// a grid-stride walk over the (point, slice) pairs, [nr_p] per point from off3
+template <class T>
+__global__ void adjoint_mass_slices_kernel(int npoints, const int *off, const int *nrp, const int64_t *off3,
+                                           const T *inv_mass1, const cx_t<T> *ubar, const cx_t<T> *vbar,
+                                           const cx_t<T> *abar_out, const cx_t<T> *a_n, T h, const T *tw,
+                                           const int *tw_off, T *gmass3) {
+    const int64_t total = off3[npoints];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        // the point of pair i by its slice offsets (binary search)
+        int lo = 0, hi = npoints;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) / 2;
+            if (off3[mid] <= i) lo = mid;
+            else hi = mid;
+        }
+        const int p = lo, nr = nrp[p], nu = nr / 2 + 1, k = (int)(i - off3[p]);
+        const T *cs = tw + tw_off[nr], *sn = cs + nr;
+        T acc = 0;
+        for (int c = 0; c < 3; c++) {
+            T sa = 0, ha = 0, sy = 0, hy = 0, a0 = 0, y0 = 0;
+            int j = 0;
+            for (int al = 0; al < nu; al++) {
+                const size_t q = (size_t)(off[p] + al) * 3 + c;
+                const cx_t<T> ub = ubar[q], vb = vbar[q], ao = abar_out[q], an = a_n[q];
+                const cx_t<T> abn = mk<T>(ao.x + h / 2 * vb.x + h * h * ub.x, ao.y + h / 2 * vb.y + h * h * ub.y);
+                if (al == 0) { a0 = an.x; y0 = abn.x; continue; }
+                j += k;
+                j = j >= nr ? j - nr : j;
+                const T va = an.x * cs[j] - an.y * sn[j], vy = abn.x * cs[j] - abn.y * sn[j];
+                if (2 * al == nr) { ha += va; hy += vy; }
+                else { sa += va; sy += vy; }
+            }
+            const T ak = a0 + (T)2 * (sa + ha), yk = y0 + sy + (T)0.5 * hy;
+            acc += ak * yk;
+        }
+        gmass3[i] -= acc * inv_mass1[p] / (T)nr;
+    }
 }
 
 // ubar_n = ubar_{n+1} + (-K g), -K g being in `kg` (which is then cleared)

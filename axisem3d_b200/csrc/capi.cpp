@@ -701,6 +701,12 @@ int axg_adjoint_run(axg_solver *h, const double *seis_adjoint, double *grad_modu
                     double *grad_displ0, double *grad_veloc0) {
     return guarded(h, [&] { h->eng->adjoint_run(seis_adjoint, grad_moduli, grad_mass, grad_displ0, grad_veloc0); });
 }
+int axg_set_adjoint_slices(axg_solver *h, int32_t on) {
+    return guarded(h, [&] { h->eng->set_adjoint_slices(on != 0); });
+}
+int axg_get_adjoint_slices(axg_solver *h, double *grad_moduli_slices, double *grad_mass_slices) {
+    return guarded(h, [&] { h->eng->get_adjoint_slices(grad_moduli_slices, grad_mass_slices); });
+}
 int axg_field_raw_bytes(const axg_solver *h, int32_t solid, int32_t which, int64_t *bytes) {
     if (!h || !bytes || which < 0 || which > 3) return AXG_E_ARG;
     if (!h->finalized) return AXG_E_STATE;

@@ -217,6 +217,9 @@ public:
     virtual void forward_checkpointed(int nsteps, int interval) = 0;
     virtual void adjoint_run(const double *seis_adj, double *grad_mod, double *grad_mass,
                              double *grad_u0, double *grad_v0) = 0;
+    // per-slice sensitivities of the next adjoint runs (3-D parameterisation)
+    virtual void set_adjoint_slices(bool on) = 0;
+    virtual void get_adjoint_slices(double *grad_mod_slices, double *grad_mass_slices) = 0;
     // -K x added to f (device pointers, one wavefield), SLS memory in `scratch` (cap bytes,
     // cleared here); queues work on the handle's stream and allocates nothing
     virtual void stiffness_noalloc(const void *sx, void *sf, const void *fx, void *ff, void *scratch,

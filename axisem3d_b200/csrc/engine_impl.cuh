@@ -516,6 +516,11 @@ public:
         seg_u.alloc(nf * ck_interval_); seg_a.alloc(nf * ck_interval_);
         adj_grad_.zero(stream_);
         adj_gmass_.zero(stream_);
+        if (adj_slices_) {
+            build_adjoint_slices();
+            adj_grad3_.zero(stream_);
+            adj_gmass3_.zero(stream_);
+        }
         DBuf<double> r;
         if (st_n_) r.alloc((size_t)st_n_ * 3);
         const int threads = 256;
@@ -541,6 +546,14 @@ public:
                 pa.flags = sp_.flags.p; pa.inv_mass1 = sp_.inv1.p; pa.ubar = ub.p; pa.vbar = vb.p;
                 pa.abar_out = ab.p; pa.a_n = seg_a.p + nf * i; pa.g = g.p; pa.grad_mass = adj_gmass_.p;
                 pa.h = (T)cfg_.dt;
+                if (adj_slices_) {
+                    const int sblocks = (int)std::min<int64_t>((adj_mass3_pairs_ + threads - 1) / threads,
+                                                               (int64_t)prop_.multiProcessorCount * 8);
+                    adjoint_mass_slices_kernel<T><<<std::max(sblocks, 1), threads, 0, stream_>>>(
+                        sp_.n, sp_.off.p, sp_.nr.p, adj_gmass3_off_.p, sp_.inv1.p, ub.p, vb.p, ab.p,
+                        seg_a.p + nf * i, pa.h, adj_tw_.p, adj_tw_off_.p, adj_gmass3_.p);
+                    post_launch();
+                }
                 adjoint_point_kernel<T><<<mblocks, threads, 0, stream_>>>(pa);
                 post_launch();
                 AdjointArgs<T> aa;
@@ -548,8 +561,12 @@ public:
                 aa.geom = adj_geom_.p; aa.mod = adj_mod_.p; aa.mod_off = adj_mod_off_.p;
                 aa.pt_off = sp_.off.p; aa.pt_nu = sp_.nu.p; aa.u = seg_u.p + nf * i; aa.g = g.p;
                 aa.out = kg.p; aa.ifact = adj_ifact_.p; aa.grad = adj_grad_.p; aa.gmat = gmat_.p;
+                aa.grad3 = adj_slices_ ? adj_grad3_.p : nullptr;
+                aa.grad3_off = adj_grad3_off_.p;
+                aa.tw = adj_tw_.p;
+                aa.tw_off = adj_tw_off_.p;
                 const int nu_max = adj_nr_max_ / 2 + 1;
-                const size_t smem = (size_t)nu_max * (75 + 75 + 150) * sizeof(C);
+                const size_t smem = (size_t)nu_max * (75 + 75 + 150 + (adj_slices_ ? 300 : 0)) * sizeof(C);
                 const int grid = std::min(model_.se.count, prop_.multiProcessorCount * 8);
                 adjoint_stiffness_kernel<T><<<grid, 128, smem, stream_>>>(aa, nu_max);
                 post_launch();
@@ -710,6 +727,57 @@ private:
         AXG_CUDA(cudaMemcpyAsync(sp_.accel.p, ck_accel_.p + nf * c, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
         sp_.stiff.zero(stream_);
     }
+    // per-slice sensitivity buffers: [2][nr_e][25] per element, [nr_p] per point, and the
+    // twiddles of every nr they use
+    void build_adjoint_slices() {
+        if (adj_slices_built_) return;
+        const HostSolidElements &h = model_.se;
+        std::vector<int64_t> goff(h.count), moff(sp_.n + 1);
+        int64_t o = 0;
+        std::vector<int> nrs;
+        for (int e = 0; e < h.count; e++) { goff[e] = o; o += (int64_t)2 * h.nr[e] * 25; nrs.push_back(h.nr[e]); }
+        adj_grad3_.alloc(std::max<int64_t>(o, 1));
+        adj_grad3_n_ = o;
+        o = 0;
+        for (int p = 0; p < sp_.n; p++) { moff[p] = o; o += sp_.h_nr[p]; nrs.push_back(sp_.h_nr[p]); }
+        moff[sp_.n] = o;
+        adj_mass3_pairs_ = o;
+        adj_gmass3_.alloc(std::max<int64_t>(o, 1));
+        adj_grad3_off_.upload(goff);
+        adj_gmass3_off_.upload(moff);
+        int nrm = 1;
+        for (int n : nrs) nrm = std::max(nrm, n);
+        std::vector<int> toff;
+        std::vector<T> tw = twiddle_pool<T>(nrs, nrm, toff);
+        adj_tw_.upload(tw);
+        adj_tw_off_.upload(toff);
+        const int nu_max = adj_nr_max_ / 2 + 1;
+        const size_t smem = (size_t)nu_max * 600 * sizeof(C);
+        if (smem > 200 * 1024) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || nr too large for per-slice sensitivities.");
+        raise_smem_limit((const void *)adjoint_stiffness_kernel<T>, smem);
+        adj_slices_built_ = true;
+    }
+
+public:
+    void set_adjoint_slices(bool on) override { need(); adj_slices_ = on; }
+    void get_adjoint_slices(double *g3, double *m3) override {
+        need();
+        if (!adj_slices_built_)
+            throw Error(AXG_E_STATE, "axg_get_adjoint_slices || no adjoint run with per-slice sensitivities.");
+        AXG_CUDA(cudaStreamSynchronize(stream_));
+        if (g3) {
+            std::vector<T> hb((size_t)adj_grad3_n_);
+            if (!hb.empty()) AXG_CUDA(cudaMemcpy(hb.data(), adj_grad3_.p, hb.size() * sizeof(T), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < hb.size(); i++) g3[i] = (double)hb[i];
+        }
+        if (m3) {
+            std::vector<T> hb((size_t)adj_mass3_pairs_);
+            if (!hb.empty()) AXG_CUDA(cudaMemcpy(hb.data(), adj_gmass3_.p, hb.size() * sizeof(T), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < hb.size(); i++) m3[i] = (double)hb[i];
+        }
+    }
+
+private:
     void build_adjoint_arrays() {
         if (adj_built_) return;
         const HostSolidElements &h = model_.se;
@@ -936,12 +1004,42 @@ private:
 
     int nmod_of(int rheo) const { return rheo == RHEO_ISO ? 2 : rheo == RHEO_TISO ? 5 : 21; }
 
+    // Colour of every element for deterministic assembly (axg_config.deterministic): greedy, in
+    // element order, the smallest colour none of the element's points has seen yet; all zero
+    // otherwise. Within one colour no two elements share a point, so each launch adds at most
+    // one contribution to any point stiffness, and the launches run one after another: the sums
+    // come out in the same order on every run.
+    std::vector<int> element_colours(const std::vector<int> &pts, int count, int npoints) const {
+        std::vector<int> colour(count, 0);
+        if (!cfg_.deterministic) return colour;
+        std::vector<uint64_t> seen(std::max(npoints, 1), 0);
+        for (int e = 0; e < count; e++) {
+            uint64_t used = 0;
+            for (int q = 0; q < 25; q++) {
+                const int p = pts[(size_t)e * 25 + q];
+                if (p >= 0 && p < npoints) used |= seen[p];
+            }
+            if (~used == 0) throw Error(AXG_E_UNSUPPORTED, "Engine::finalize || more than 64 element colours.");
+            int c = 0;
+            while (used & (uint64_t(1) << c)) c++;
+            colour[e] = c;
+            for (int q = 0; q < 25; q++) {
+                const int p = pts[(size_t)e * 25 + q];
+                if (p >= 0 && p < npoints) seen[p] |= uint64_t(1) << c;
+            }
+        }
+        return colour;
+    }
+
     void build_solid_buckets(const HostSolidElements &h) {
         // group elements by (rheology, attenuation, 1-D/3-D, RTZ, nr class, PRT)
         const HostPrt &hp = model_.prt;
         std::vector<int> prt_of(h.count, -1);
         for (int i = 0; i < hp.count; i++) prt_of[hp.elem[i]] = i;
-        std::map<std::tuple<int, int, int, int, int, int>, std::vector<int>> groups;
+        // deterministic assembly: elements coloured so that no two of one colour share a point,
+        // one bucket per colour, the buckets launched in turn
+        const std::vector<int> colour = element_colours(h.pts, h.count, sp_.n);
+        std::map<std::tuple<int, int, int, int, int, int, int>, std::vector<int>> groups;
         for (int e = 0; e < h.count; e++) {
             int att = h.att.size() ? h.att[e] : ATT_NONE;
             int is3d = h.is3d.size() ? h.is3d[e] : 0;
@@ -951,13 +1049,13 @@ private:
             if (h.rheo[e] == RHEO_ISO && !prt) rtz = 0;
             if (att != ATT_NONE && cfg_.nsls <= 0)
                 throw Error(AXG_E_ARG, "Attenuation::checkCompatibility || nsls must be > 0.");
-            groups[{h.rheo[e], att, is3d, rtz, cfg_.plain ? 0 : nr_class(h.nr[e]), prt}].push_back(e);
+            groups[{h.rheo[e], att, is3d, rtz, cfg_.plain ? 0 : nr_class(h.nr[e]), prt, colour[e]}].push_back(e);
         }
         int64_t state_total = 0;
         std::vector<std::vector<int64_t>> state_offs;
         for (auto &kv : groups) {
             auto b = std::make_unique<SolidBucket>();
-            std::tie(b->rheo, b->att, b->is3d, b->rtz, b->cls, b->prt) = kv.first;
+            std::tie(b->rheo, b->att, b->is3d, b->rtz, b->cls, b->prt, std::ignore) = kv.first;
             std::vector<T> xpool;
             std::vector<int64_t> xoff;
             std::vector<uint8_t> x3d;
@@ -1225,14 +1323,15 @@ private:
         const HostPrt &hp = model_.prt_f;
         std::vector<int> prt_of(h.count, -1);
         for (int i = 0; i < hp.count; i++) prt_of[hp.elem[i]] = i;
-        std::map<std::tuple<int, int, int>, std::vector<int>> groups;
+        const std::vector<int> colour = element_colours(h.pts, h.count, fp_.n);
+        std::map<std::tuple<int, int, int, int>, std::vector<int>> groups;
         for (int e = 0; e < h.count; e++) {
             const int mode = prt_of[e] < 0 ? 0 : (hp.theta.empty() ? 1 : 2);
-            groups[{h.is3d.size() ? h.is3d[e] : 0, cfg_.plain ? 0 : nr_class(h.nr[e]), mode}].push_back(e);
+            groups[{h.is3d.size() ? h.is3d[e] : 0, cfg_.plain ? 0 : nr_class(h.nr[e]), mode, colour[e]}].push_back(e);
         }
         for (auto &kv : groups) {
             auto b = std::make_unique<FluidBucket>();
-            std::tie(b->is3d, b->cls, b->prt) = kv.first;
+            std::tie(b->is3d, b->cls, b->prt, std::ignore) = kv.first;
             std::vector<T> xpool, trig;
             std::vector<int64_t> xoff;
             std::vector<uint8_t> x3d;
@@ -2015,6 +2114,11 @@ private:
     int ck_n_ = 0, ck_interval_ = 0, ck_step0_ = 0;
     bool adj_built_ = false;
     int adj_nr_max_ = 1;
+    bool adj_slices_ = false, adj_slices_built_ = false;
+    int64_t adj_grad3_n_ = 0, adj_mass3_pairs_ = 0;
+    DBuf<T> adj_grad3_, adj_gmass3_, adj_tw_;
+    DBuf<int64_t> adj_grad3_off_, adj_gmass3_off_;
+    DBuf<int> adj_tw_off_;
     DBuf<T> adj_geom_, adj_ifact_, adj_mod_, adj_grad_, adj_gmass_;
     DBuf<int64_t> adj_mod_off_;
 

@@ -186,7 +186,8 @@ class Model:
         return u
 
     # ---------------------------------------------------------- C structs ---
-    def config(self, precision, device=0, stability_interval=0, compensated=1, plain=0, autotune=0):
+    def config(self, precision, device=0, stability_interval=0, compensated=1, plain=0, autotune=0,
+               deterministic=0):
         cfg = L.axg_config()
         cfg.precision = L.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         cfg.device = device
@@ -198,7 +199,7 @@ class Model:
             cfg.att_beta[i] = float(self.att_beta[i])
             cfg.att_gamma[i] = float(self.att_gamma[i])
         cfg.stability_interval = stability_interval
-        cfg.deterministic = 0
+        cfg.deterministic = int(bool(deterministic))
         cfg.compensated = compensated
         cfg.plain = int(bool(plain))
         cfg.autotune = int(bool(autotune))

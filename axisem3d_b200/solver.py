@@ -31,12 +31,13 @@ class EngineError(RuntimeError):
 
 class Solver:
     def __init__(self, model, precision="fp32", device=0, stability_interval=0, compensated=True,
-                 team_sizes=None, plain=False, autotune=False):
+                 team_sizes=None, plain=False, autotune=False, deterministic=False):
         self.lib = L.lib()
         self.model = model
         self.precision = precision
         cfg = model.config(precision, device=device, stability_interval=stability_interval,
-                           compensated=int(bool(compensated)), plain=plain, autotune=autotune)
+                           compensated=int(bool(compensated)), plain=plain, autotune=autotune,
+                           deterministic=deterministic)
         h = C.c_void_p()
         rc = self.lib.axg_create(C.byref(cfg), C.byref(h))
         if rc != L.AXG_OK:
@@ -298,12 +299,16 @@ class Solver:
         """nsteps forward steps keeping a device checkpoint every `interval` steps."""
         self._check(self.lib.axg_forward_checkpointed(self.h, int(nsteps), int(interval)))
 
-    def adjoint(self, seis_adjoint):
+    def adjoint(self, seis_adjoint, slices=False):
         """Discrete adjoint of the last checkpointed run for dJ/d(seismograms).
 
         Returns dJ/d(lambda, mu) per element point (ne, 2, 25), dJ/d(point mass),
-        and dJ/d(initial displacement / velocity) in the field layout."""
+        and dJ/d(initial displacement / velocity) in the field layout. With slices=True also
+        the per-slice sensitivities of the 3-D parameterisation: "moduli_slices", a list of
+        (2, nr_e, 25) arrays (lambda, mu at phi_k = 2 pi k / nr_e), and "mass_slices", a list of
+        (nr_p,) arrays per solid point."""
         ne = self.model.n_solid_elements
+        self._check(self.lib.axg_set_adjoint_slices(self.h, int(bool(slices))))
         r = np.ascontiguousarray(seis_adjoint, dtype=np.float64)
         gm = np.zeros((ne, 2, 25))
         gmass = np.zeros(len(self.model.sp_nr))
@@ -314,7 +319,19 @@ class Solver:
                                              gmass.ctypes.data_as(L.P_f64),
                                              gu.view(np.float64).ctypes.data_as(L.P_f64),
                                              gv.view(np.float64).ctypes.data_as(L.P_f64)))
-        return {"moduli": gm, "mass": gmass, "displ0": gu, "veloc0": gv}
+        out = {"moduli": gm, "mass": gmass, "displ0": gu, "veloc0": gv}
+        if slices:
+            enr = np.asarray(self.model.se_nr, np.int64)
+            pnr = np.asarray(self.model.sp_nr, np.int64)
+            g3 = np.zeros(int(np.sum(2 * enr * 25)))
+            m3 = np.zeros(int(np.sum(pnr)))
+            self._check(self.lib.axg_get_adjoint_slices(self.h, g3.ctypes.data_as(L.P_f64),
+                                                        m3.ctypes.data_as(L.P_f64)))
+            eo = np.concatenate([[0], np.cumsum(2 * enr * 25)])
+            po = np.concatenate([[0], np.cumsum(pnr)])
+            out["moduli_slices"] = [g3[eo[e]:eo[e + 1]].reshape(2, enr[e], 25) for e in range(ne)]
+            out["mass_slices"] = [m3[po[p]:po[p + 1]] for p in range(len(pnr))]
+        return out
 
     # ------------------------------------------------------------ diagnostics ---
     def launch_count(self):

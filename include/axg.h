@@ -105,7 +105,12 @@ typedef struct axg_config {
     double  att_beta[AXG_MAX_SLS];
     double  att_gamma[AXG_MAX_SLS];
     int32_t stability_interval; /* steps between non-finite checks (0 = never)            */
-    int32_t deterministic;      /* reserved: 0 = atomic scatter-add                        */
+    int32_t deterministic;      /* 1 = bitwise-reproducible assembly: elements coloured so
+                                   that no two of a colour share a point, one launch per
+                                   colour and bucket (sources in elements that share
+                                   points still add in either order); 0 = one launch per
+                                   bucket (atomic scatter-add, summation order may vary from
+                                   run to run) */
     int32_t compensated;        /* MIXED only: 1 = compensated (Kahan) d/v summation      */
     int32_t plain;              /* 1 = the plain method: one element bucket per material
                                    kind with a fixed 256-thread team (no nr bucketing, no
@@ -407,6 +412,17 @@ int  axg_forward_checkpointed(axg_solver *h, int32_t nsteps, int32_t checkpoint_
    displacement / velocity). The fields end in the state after the forward run. */
 int  axg_adjoint_run(axg_solver *h, const double *seis_adjoint, double *grad_moduli,
                      double *grad_mass, double *grad_displ0, double *grad_veloc0);
+/* per-slice sensitivities (no counterpart in the reference): with on = 1 the next
+   axg_adjoint_run also accumulates the gradient of the misfit with respect to the moduli and
+   masses of the 3-D parameterisation, the values at the slices phi_k = 2 pi k / nr that a 3-D
+   element or a Mass3D point holds (PhysicalProperty.hpp:99-120): dJ/dlambda and dJ/dmu at
+   every (slice, point) of every element, dJ/dM at every slice of every solid point. The
+   linearisation point is the handle's phi-constant model; with odd nr a 3-D element there
+   equals the 1-D one, and the sum over slices is the 1-D gradient. */
+int  axg_set_adjoint_slices(axg_solver *h, int32_t on);
+/* after such a run: grad_moduli_slices per element [2][nr_e][25] (lambda, mu), elements in
+   order; grad_mass_slices per solid point [nr_p]; either may be NULL */
+int  axg_get_adjoint_slices(axg_solver *h, double *grad_moduli_slices, double *grad_mass_slices);
 
 /* ---- fields ---- */
 /* solid = 1 for solid points, 0 for fluid; host buffer of sum(nu_p)*ndim complex doubles */

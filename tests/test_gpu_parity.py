@@ -798,3 +798,26 @@ def test_slice_fft_parity(built, precision, kind):
         f2 = s.get_field("stiff")
     assert rel(f1, ref1) <= TOL_STIFF[precision], rel(f1, ref1)
     assert rel(f2, ref2) <= TOL_STIFF[precision], rel(f2, ref2)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_deterministic_assembly_is_bitwise_reproducible(built, precision):
+    """axg_config.deterministic: coloured element launches make the assembled stiffness and
+    the fields bitwise identical from run to run (the reference's serial scatter is
+    deterministic, SolidPoint.hpp:101-109), and equal to the atomic path within the FP32
+    tolerance. 3-D TI with FULL SLS, a fluid-free microbenchmark with many shared points, and
+    the spherical shell with its fluid layer."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    for m, nsteps in ((meshgen.microbench_model(n_elem=800, nr_max=40, seed=44), 4),
+                      (meshgen.spherical_model(n_theta=24, n_solid_layers=6, n_fluid_layers=2, nr_max=24), 20)):
+        u = meshgen.random_displacement(m, seed=3) * 1e-6
+        runs = []
+        for det in (True, True, False):
+            with Solver(m, precision, deterministic=det) as s:
+                s.set_field(u, "displ")
+                s.run(nsteps)
+                runs.append((s.get_field("displ"), s.get_field("stiff")))
+        (d1, k1), (d2, k2), (d3, k3) = runs
+        assert np.array_equal(d1, d2) and np.array_equal(k1, k2)
+        assert rel(d1, d3) <= 1e-5 and rel(k1, k3) <= 1e-5
