@@ -61,6 +61,7 @@ inline int nr_class(int nr) { return nr <= 3 ? 0 : nr <= 9 ? 1 : nr <= 25 ? 2 : 
 #ifndef AXG_FFT_MIN_NR
 #define AXG_FFT_MIN_NR 65
 #endif
+
 inline int default_team(int cls) { static const int t[5] = {32, 64, 128, 256, 256}; return t[cls]; }
 
 template <class T>
@@ -118,6 +119,7 @@ class Engine final : public EngineBase {
         int rheo, att, is3d, rtz, cls, team, tpc, qc, nr_max, n, grid = 1;
         int mt = 1;   // Fourier modes per tile of the gather / gradient and the quadrature
         int fft = 0;  // 3-D elements of nr >= AXG_FFT_MIN_NR take the slice FFTs
+        int ahead = 0;   // L2 prefetch distance in elements (AXG_PREFETCH_AHEAD waves), 0 = off
         size_t team_bytes;
         DBuf<int> nr, pts;
         DBuf<uint8_t> axial;
@@ -1258,6 +1260,14 @@ private:
         // tail of uneven nr better than a fixed walk). AXG_PERSISTENT_GRID restores the
         // persistent walk with next-element L2 prefetch.
         b.grid = (b.n + tpc - 1) / tpc;
+        b.ahead = 0;
+#if AXG_PREFETCH_AHEAD > 0
+        if (!cfg_.plain && !b.prt) {
+            int per_sm = 0;
+            AXG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, team * tpc, tpc * total));
+            b.ahead = AXG_PREFETCH_AHEAD * std::max(per_sm, 1) * prop_.multiProcessorCount * tpc;
+        }
+#endif
 #ifdef AXG_PERSISTENT_GRID
         int per_sm = 0;
         AXG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, team * tpc, tpc * total));
@@ -1882,6 +1892,7 @@ private:
         } else {
             SolidArgs<T, AT> af = a;
             af.fft_min_nr = b.fft ? AXG_FFT_MIN_NR : 0;
+            af.prefetch_ahead = b.ahead;
             b.kernel<<<b.grid, b.team * b.tpc, b.tpc * b.team_bytes, stream_>>>(af, b.nr_max, b.qc, b.mt, b.tpc,
                                                                               b.team_bytes);
         }

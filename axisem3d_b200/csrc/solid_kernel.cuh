@@ -68,6 +68,16 @@ constexpr int ATT_NONE = 0, ATT_FULL = 1, ATT_CG4 = 2;
 #ifndef AXG_SLS_SPLIT
 #define AXG_SLS_SPLIT 0
 #endif
+// > 0: each team prefetches into L2 the operands of the element AXG_PREFETCH_AHEAD waves of
+// resident CTAs ahead (the distance in SolidArgs::prefetch_ahead)
+#ifndef AXG_PREFETCH_AHEAD
+#define AXG_PREFETCH_AHEAD 0
+#endif
+// 1 = the stress pass's first (slice, point) of each thread has its SLS state loaded before the
+// Fourier -> slice pass (its latency hidden under that pass)
+#ifndef AXG_STATE_EARLY
+#define AXG_STATE_EARLY 0
+#endif
 // 1 = L2 prefetch of an element's slice operands (moduli, attenuation moduli, SLS state)
 // at the start of its slice phase
 #ifndef AXG_PREFETCH_SLICES
@@ -127,6 +137,8 @@ struct SolidArgs {
     size_t fstride;            // complex values between wavefields in displ / stiff
     size_t sstride;            // AT values between wavefields in the state pool
     int fft_min_nr;            // 3-D elements with nr >= this (and 13-smooth nr) take the FFT; 0 = never
+    int prefetch_ahead;        // > 0: each team prefetches into L2 the operands of the element this
+                               // many places ahead (about one wave of resident CTAs); 0 = off
 };
 
 // shared memory layout of one team
@@ -702,6 +714,9 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
         // the next element of this team streams into L2 while this one computes
         if (AXG_PREFETCH_NEXT && e + stride < a.n_elem)
             prefetch_element<T, AT, RHEO, ATT, IS3D>(a, e + stride, lane, TEAM);
+        // the element about one wave of resident CTAs ahead streams into L2 while this one computes
+        if (AXG_PREFETCH_AHEAD > 0 && a.prefetch_ahead > 0 && e + a.prefetch_ahead < a.n_elem)
+            prefetch_element<T, AT, RHEO, ATT, IS3D>(a, e + a.prefetch_ahead, lane, TEAM);
 
         // ---------------- element header -> shared memory ----------------
         for (int i = lane; i < 250; i += TEAM) sGeo[i] = a.geom[(size_t)e * 250 + i];
@@ -931,6 +946,29 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 constexpr int NPA = ATT == ATT_CG4 ? 4 : 25;
                 const T *modp = a.mod + moff;
                 const size_t nsl = (size_t)nslice * 25;
+#if AXG_STATE_EARLY
+                // the SLS state of this thread's first (slice, point) of the stress pass is
+                // loaded now, so that its latency runs under the Fourier -> slice pass
+                AT ds0[6], mem0[NSR][6];
+                bool pre = false;
+                if constexpr (ATT != ATT_NONE && NS > 0) {
+                    if (lane < nr * qcnt) {
+                        const int k = lane / qcnt, q = q0 + lane - k * qcnt;
+                        const int k4 = ATT == ATT_CG4 ? cg4_slot(q) : q;
+                        if (k4 >= 0) {
+                            const size_t nslot = (size_t)nr * NPA, slot = (size_t)k * NPA + k4;
+                            const AT *st = statew + a.state_off[e];
+#pragma unroll
+                            for (int d = 0; d < 6; d++) ds0[d] = state_ld(st + d * nslot + slot);
+#pragma unroll
+                            for (int l = 0; l < NSR; l++)
+#pragma unroll
+                                for (int d = 0; d < 6; d++) mem0[l][d] = state_ld(st + (6 + l * 6 + d) * nslot + slot);
+                            pre = true;
+                        }
+                    }
+                }
+#endif
                 if (FFT && use_fft) {
                     // Hermitian spectra of the component pairs, Z = Y_2p + i Y_2p+1 over all nr
                     // orders: Y_0 = Re c_0, Y_a = c_a, Y_nr-a = conj c_a, Y_nr/2 = 2 Re c_nr/2
@@ -1035,12 +1073,24 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                             dl = __ldg(am + slot);
                             dmu = __ldg(am + nslot + slot);
 #if !AXG_SLS_SPLIT
+#if AXG_STATE_EARLY
+                            if (pre && i == lane) {
+#pragma unroll
+                                for (int d = 0; d < 6; d++) ds[d] = ds0[d];
+#pragma unroll
+                                for (int l = 0; l < NSR; l++)
+#pragma unroll
+                                    for (int d = 0; d < 6; d++) mem[l][d] = mem0[l][d];
+                            } else
+#endif
+                            {
 #pragma unroll
                             for (int d = 0; d < 6; d++) ds[d] = state_ld(st + d * nslot + slot);
 #pragma unroll
                             for (int l = 0; l < NSR; l++)
 #pragma unroll
                                 for (int d = 0; d < 6; d++) mem[l][d] = state_ld(st + (6 + l * 6 + d) * nslot + slot);
+                            }
 #endif
                         }
                     }

@@ -60,7 +60,7 @@ def parse():
     p.add_argument("--ensemble", type=int, default=64, help="sources of the ensemble leg (0 = skip)")
     p.add_argument("--no-oned", action="store_true", help="skip the 1-D (in-Fourier) leg")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--shell-steps", type=int, default=200,
+    p.add_argument("--shell-steps", type=int, default=100,
                    help="steps of the spherical-shell leg in each precision (0 = skip; the full run is 5000)")
     p.add_argument("--shell-theta", type=int, default=1200, help="quads along theta of the shell leg")
     return p.parse_args()
@@ -417,7 +417,13 @@ def shell_timing(args, local, stream, world):
                 out["stiffness_frac_of_" + kind + "_hbm"] = out["stiffness_GBps"] / peak
         log("shell %s done" % prec)
     ref = seis["fp64"]
-    out["trace_rel_l2_vs_fp64"] = float(np.linalg.norm(seis[args.precision] - ref) / np.linalg.norm(ref))
+    if n >= 2000:
+        out["trace_rel_l2_vs_fp64"] = float(np.linalg.norm(seis[args.precision] - ref) / np.linalg.norm(ref))
+    else:
+        # before ~2000 steps the waves have not reached the stations: both precisions record
+        # values at the underflow level, and their difference says nothing
+        out["trace_rel_l2_vs_fp64"] = None
+        out["trace_note"] = "seismograms are compared on the full run (--shell-steps 5000)"
     out[args.precision + "_over_fp64"] = out["value_" + args.precision] / out["value_fp64"]
     return out
 
