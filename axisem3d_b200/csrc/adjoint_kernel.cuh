@@ -142,7 +142,9 @@ __device__ __forceinline__ void strain_at(const cx_t<T> *U, int al, int q, bool 
 
 // one CTA (team of blockDim.x threads) per element: -K g scattered to `out`, and the
 // lambda / mu sensitivities of this step accumulated into grad
-template <class T>
+// SLICES: the instantiation that also accumulates the per-slice sensitivities (a.grad3); the
+// other holds none of that code, so it costs the plain adjoint no registers
+template <class T, bool SLICES>
 __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArgs<T> a, const int nu_max) {
     using C = cx_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
             stress_iso(eg, sg, lam, mu);
 #pragma unroll
             for (int d = 0; d < 6; d++) S[(al * 6 + d) * 25 + q] = sg[d];
-            if (a.grad3) {
+            if constexpr (SLICES) {
 #pragma unroll
                 for (int d = 0; d < 6; d++) {
                     Eg[(al * 6 + d) * 25 + q] = eg[d];
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
             atomicAdd(&sGm[q], pm);
         }
         __syncthreads();
-        if (a.grad3) {
+        if constexpr (SLICES) {
             const T *cs = a.tw + a.tw_off[nr], *sn = cs + nr;
             T *g3 = a.grad3 + a.grad3_off[e];
             for (int i = threadIdx.x; i < nr * 25; i += blockDim.x) {

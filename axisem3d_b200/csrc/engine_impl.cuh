@@ -523,8 +523,14 @@ public:
             adj_grad3_.zero(stream_);
             adj_gmass3_.zero(stream_);
         }
+        // every seismogram cotangent of the run on the device at once (no host round trip per step)
         DBuf<double> r;
-        if (st_n_) r.alloc((size_t)st_n_ * 3);
+        if (st_n_) {
+            const size_t nrec = (size_t)(end_step + st_interval_ - 1) / st_interval_;
+            r.alloc(nrec * st_n_ * 3);
+            AXG_CUDA(cudaMemcpyAsync(r.p, seis_adj, nrec * st_n_ * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                     stream_));
+        }
         const int threads = 256;
         const int mblocks = (sp_.total + threads - 1) / threads;
         const int vblocks = (int)((nf + threads - 1) / threads);
@@ -570,19 +576,17 @@ public:
                 const int nu_max = adj_nr_max_ / 2 + 1;
                 const size_t smem = (size_t)nu_max * (75 + 75 + 150 + (adj_slices_ ? 300 : 0)) * sizeof(C);
                 const int grid = std::min(model_.se.count, prop_.multiProcessorCount * 8);
-                adjoint_stiffness_kernel<T><<<grid, 128, smem, stream_>>>(aa, nu_max);
+                if (adj_slices_) adjoint_stiffness_kernel<T, true><<<grid, 128, smem, stream_>>>(aa, nu_max);
+                else adjoint_stiffness_kernel<T, false><<<grid, 128, smem, stream_>>>(aa, nu_max);
                 post_launch();
                 adjoint_combine_kernel<T><<<vblocks, threads, 0, stream_>>>((int)nf, ub.p, kg.p);
                 post_launch();
                 if (st_n_ && n % st_interval_ == 0) {
                     const int rec = n / st_interval_;
-                    AXG_CUDA(cudaMemcpyAsync(r.p, seis_adj + (size_t)rec * st_n_ * 3,
-                                             (size_t)st_n_ * 3 * sizeof(double), cudaMemcpyHostToDevice,
-                                             stream_));
                     adjoint_station_kernel<T><<<(st_n_ * 3 + 127) / 128, 128, 0, stream_>>>(
-                        st_n_, st_el_.p, st_w_.p, st_phi_.p, e_nr_.p, e_pts_.p, sp_.off.p, sp_.nu.p, r.p, ub.p);
+                        st_n_, st_el_.p, st_w_.p, st_phi_.p, e_nr_.p, e_pts_.p, sp_.off.p, sp_.nu.p,
+                        r.p + (size_t)rec * st_n_ * 3, ub.p);
                     post_launch();
-                    AXG_CUDA(cudaStreamSynchronize(stream_));   // r is reused next step
                 }
             }
         }
@@ -756,7 +760,7 @@ private:
         const int nu_max = adj_nr_max_ / 2 + 1;
         const size_t smem = (size_t)nu_max * 600 * sizeof(C);
         if (smem > 200 * 1024) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || nr too large for per-slice sensitivities.");
-        raise_smem_limit((const void *)adjoint_stiffness_kernel<T>, smem);
+        raise_smem_limit((const void *)adjoint_stiffness_kernel<T, true>, smem);
         adj_slices_built_ = true;
     }
 
@@ -809,7 +813,8 @@ private:
         int nu_max = adj_nr_max_ / 2 + 1;
         size_t smem = (size_t)nu_max * 300 * sizeof(C);
         if (smem > 200 * 1024) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || nr too large.");
-        raise_smem_limit((const void *)adjoint_stiffness_kernel<T>, smem);
+        raise_smem_limit((const void *)adjoint_stiffness_kernel<T, false>, smem);
+        raise_smem_limit((const void *)adjoint_stiffness_kernel<T, true>, smem);
         adj_built_ = true;
     }
 

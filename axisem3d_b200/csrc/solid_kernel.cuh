@@ -73,6 +73,13 @@ constexpr int ATT_NONE = 0, ATT_FULL = 1, ATT_CG4 = 2;
 #ifndef AXG_PREFETCH_AHEAD
 #define AXG_PREFETCH_AHEAD 0
 #endif
+// 1 = attenuating 3-D elements on the direct sums run the Fourier -> slice sums and the stress
+// pass as one pass: a thread per (slice pair, point) loads the operands of slice k, forms slices
+// k and nr - k, and applies stress and SLS recursion to both (one barrier less, no strain slices
+// through shared memory, the first slice's loads under the sums)
+#ifndef AXG_FUSED_SLICE
+#define AXG_FUSED_SLICE 0
+#endif
 // 1 = the stress pass's first (slice, point) of each thread has its SLS state loaded before the
 // Fourier -> slice pass (its latency hidden under that pass)
 #ifndef AXG_STATE_EARLY
@@ -969,6 +976,7 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                     }
                 }
 #endif
+                bool fused_done = false;
                 if (FFT && use_fft) {
                     // Hermitian spectra of the component pairs, Z = Y_2p + i Y_2p+1 over all nr
                     // orders: Y_0 = Re c_0, Y_a = c_a, Y_nr-a = conj c_a, Y_nr/2 = 2 Re c_nr/2
@@ -991,6 +999,96 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                     // from here on the chunk's columns of region A are free until the unpacking
                     vs = fft_run<T>(vB, vA, nr, qcnt, plan, +1, tw2, team, lane, TEAM);
                 } else {
+#if AXG_FUSED_SLICE
+                if constexpr (ATT != ATT_NONE && NS > 0) {
+                    fused_done = true;
+                    const int npair = nr / 2 + 1;
+                    const size_t nslot = (size_t)nr * NPA;
+                    AT *st = statew + a.state_off[e];
+                    const T *am = a.attmod + a.att_off[e];
+                    // the operands of (slice k, point q): moduli, attenuation moduli, SLS state
+                    auto load_ops = [&](int k, int q, int k4, T (&md)[NM], T &dl, T &dmu, AT (&ds)[6],
+                                        AT (&mem)[NSR][6]) {
+#pragma unroll
+                        for (int mm = 0; mm < NM; mm++) md[mm] = __ldg(modp + mm * nsl + (size_t)k * 25 + q);
+                        if (k4 >= 0) {
+                            const size_t slot = (size_t)k * NPA + k4;
+                            dl = __ldg(am + slot);
+                            dmu = __ldg(am + nslot + slot);
+#pragma unroll
+                            for (int d = 0; d < 6; d++) ds[d] = state_ld(st + d * nslot + slot);
+#pragma unroll
+                            for (int l = 0; l < NSR; l++)
+#pragma unroll
+                                for (int d = 0; d < 6; d++) mem[l][d] = state_ld(st + (6 + l * 6 + d) * nslot + slot);
+                        }
+                    };
+                    // stress and SLS recursion of one slice; the stress to region B
+                    auto stress_slice = [&](int k, int qq, int k4, const T (&x)[6], const T (&md)[NM], T dl, T dmu,
+                                            AT (&ds)[6], AT (&mem)[NSR][6]) {
+                        re1<T> ev[6], sg[6];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) ev[d].x = x[d];
+                        if constexpr (RHEO == RHEO_ISO) stress_iso(ev, sg, md[0], md[1]);
+                        else if constexpr (RHEO == RHEO_TISO) stress_tiso(ev, sg, md[0], md[1], md[2], md[3], md[4]);
+                        else stress_aniso(ev, sg, md);
+                        if (k4 >= 0) {
+                            const size_t slot = (size_t)k * NPA + k4;
+                            T e6[6], s6[6];
+#pragma unroll
+                            for (int d = 0; d < 6; d++) { e6[d] = ev[d].x; s6[d] = sg[d].x; }
+                            attenuate_regs<NSR, T, AT>(a.alpha, a.beta, a.gamma, ds, mem, e6, s6, dl, dmu);
+#pragma unroll
+                            for (int d = 0; d < 6; d++) sg[d].x = s6[d];
+#pragma unroll
+                            for (int d = 0; d < 6; d++) state_st(st + d * nslot + slot, ds[d]);
+#pragma unroll
+                            for (int l = 0; l < NSR; l++)
+#pragma unroll
+                                for (int d = 0; d < 6; d++) state_st(st + (6 + l * 6 + d) * nslot + slot, mem[l][d]);
+                        }
+#pragma unroll
+                        for (int d = 0; d < 6; d++) rBr[((size_t)k * 6 + d) * qcnt + qq] = sg[d].x;
+                    };
+                    for (int i = lane; i < npair * qcnt; i += TEAM) {
+                        const int k = i / qcnt, qq = i - k * qcnt, q = q0 + qq;
+                        const int k4 = ATT == ATT_CG4 ? cg4_slot(q) : q;
+                        T md[NM], dl = 0, dmu = 0;
+                        AT ds[6], mem[NSR][6];
+                        load_ops(k, q, k4, md, dl, dmu, ds, mem);
+                        // slices k and nr - k from one pass over the modes
+                        T Ac[6], Bc[6];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) { Ac[d] = 0; Bc[d] = 0; }
+                        int j = 0;
+                        for (int al = 1; al < nu; al++) {
+                            j += k;
+                            j = j >= nr ? j - nr : j;
+                            const T2 w2 = tw2[j];
+#pragma unroll
+                            for (int d = 0; d < 6; d++) {
+                                const C ev = rA[(al * 6 + d) * 25 + q];
+                                Ac[d] += ev.x * w2.x;
+                                Bc[d] += ev.y * w2.y;
+                            }
+                        }
+                        T x1[6], x2[6];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) {
+                            const T c0 = rA[d * 25 + q].x;
+                            x1[d] = c0 + (T)2 * (Ac[d] - Bc[d]);
+                            x2[d] = c0 + (T)2 * (Ac[d] + Bc[d]);
+                        }
+                        stress_slice(k, qq, k4, x1, md, dl, dmu, ds, mem);
+                        if (k != 0 && 2 * k != nr) {
+                            load_ops(nr - k, q, k4, md, dl, dmu, ds, mem);
+                            stress_slice(nr - k, qq, k4, x2, md, dl, dmu, ds, mem);
+                        }
+                    }
+                    team_sync(team, TEAM);
+                } else
+#endif
+                {
                 // Register-resident slice path. Two passes:
                 //  1. computeC2R, one thread per (slice pair, point): slices k and nr - k
                 //     share their twiddles (cos equal, sin opposite), so one pass over the
@@ -1049,9 +1147,10 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 }
                 team_sync(team, TEAM);
 #endif
+                }
                 }   // direct Fourier -> slice sums
                 const int sp = use_fft ? 2 * vs.ps : 2 * qcnt, sq = use_fft ? 1 : qcnt;
-                for (int i = lane; i < nr * qcnt; i += TEAM) {
+                for (int i = lane; i < (fused_done ? 0 : nr * qcnt); i += TEAM) {
                     const int k = i / qcnt, qq = i - k * qcnt, q = q0 + qq;
                     T *slb = sl_base(k, qq);
                     T md[NM];
