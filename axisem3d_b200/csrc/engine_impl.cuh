@@ -56,13 +56,17 @@ struct DBuf {
 };
 
 // team size per nr class and the nr class boundaries
+constexpr int kNrClasses = 5;
 inline int nr_class(int nr) { return nr <= 3 ? 0 : nr <= 9 ? 1 : nr <= 25 ? 2 : nr <= 64 ? 3 : 4; }
 // smallest nr of a 3-D element that takes the slice FFTs instead of the direct sums (0 = never)
 #ifndef AXG_FFT_MIN_NR
 #define AXG_FFT_MIN_NR 65
 #endif
 
-inline int default_team(int cls) { static const int t[5] = {32, 64, 128, 256, 256}; return t[cls]; }
+inline int default_team(int cls) {
+    static const int t[kNrClasses] = {32, 64, 128, 256, 256};
+    return t[cls];
+}
 
 template <class T>
 std::vector<T> twiddle_pool(const std::vector<int> &nrs, int nr_max, std::vector<int> &off) {
@@ -155,7 +159,7 @@ public:
         AXG_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
         stream_ = own_stream_;
         AXG_CUDA(cudaGetDeviceProperties(&prop_, cfg_.device));
-        for (int i = 0; i < 5; i++) team_override_[i] = 0;
+        for (int i = 0; i < kNrClasses; i++) team_override_[i] = 0;
     }
     ~Engine() override {
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
@@ -473,7 +477,7 @@ public:
         if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
     }
     void set_team_override(int cls, int team) override {
-        if (cls < 0 || cls > 4) throw Error(AXG_E_ARG, "Engine::set_team_override || bad class");
+        if (cls < 0 || cls >= kNrClasses) throw Error(AXG_E_ARG, "Engine::set_team_override || bad class");
         team_override_[cls] = team;
     }
     int bucket_count() const override { return (int)(sb_.size() + fb_.size()); }
@@ -2121,7 +2125,7 @@ private:
     int64_t time_n_ = 0;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
-    int team_override_[5];
+    int team_override_[kNrClasses];
     struct Tuned { int cls, team; float ms; };
     std::vector<Tuned> tuned_;
     // differentiation

@@ -90,9 +90,23 @@ constexpr int ATT_NONE = 0, ATT_FULL = 1, ATT_CG4 = 2;
 #ifndef AXG_PREFETCH_SLICES
 #define AXG_PREFETCH_SLICES 1
 #endif
+// 1 = when a chunk holds all 25 points (and, for the slice -> Fourier pass, outside RTZ
+// elements), the two direct-sum passes give each thread 6 consecutive columns of the
+// (component, point) block instead of the 6 components of one point, read and written as
+// 16- / 8-byte vectors, and order the threads 5 column groups by pair (or mode) groups, so
+// that a warp touches few distinct words of region A, region B and the twiddle table per step
+#ifndef AXG_COLUMN_TILES
+#define AXG_COLUMN_TILES 1
+#endif
+// unrolling of the mode loop (Fourier -> slice) and of the slice loop (slice -> Fourier) of
+// the column-tiled passes
+#ifndef AXG_DFT_UNROLL
+#define AXG_DFT_UNROLL 1
+#endif
 constexpr int KP = AXG_KP;   // slice pairs per thread in the paired Fourier -> slice pass
 constexpr int KB = AXG_KB;   // slices per thread in the Fourier -> slice transform
 constexpr int AB = AXG_AB;   // modes per thread in the slice -> Fourier transform
+constexpr int DFT_UNROLL = AXG_DFT_UNROLL;
 
 // The SLS state is read once and written once per step: with AXG_STREAM_STATE its loads and
 // stores carry the streaming cache hint (evict first), so that it does not push the moduli and
@@ -173,6 +187,52 @@ __host__ __device__ inline TeamLayout team_layout(int nr_max, int qc, int mt) {
     L.regB = o; o = al(o + (b1 > b2 ? b1 : b2));
     L.total = o;
     return L;
+}
+
+// six consecutive complex / real values of a team's shared buffers as 16- or 8-byte vectors;
+// complex groups start on 16 bytes, real groups on 2 T (the callers' column groups start at
+// even offsets of 16-byte aligned regions)
+template <class T>
+__device__ __forceinline__ void ld6c(const cx_t<T> *p, cx_t<T> (&v)[6]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 *q = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const float4 t = q[i];
+            v[2 * i] = mk<T>(t.x, t.y);
+            v[2 * i + 1] = mk<T>(t.z, t.w);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 6; i++) v[i] = p[i];
+    }
+}
+template <class T>
+__device__ __forceinline__ void st6c(cx_t<T> *p, const cx_t<T> (&v)[6]) {
+    if constexpr (sizeof(T) == 4) {
+        float4 *q = reinterpret_cast<float4 *>(p);
+#pragma unroll
+        for (int i = 0; i < 3; i++) q[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 6; i++) p[i] = v[i];
+    }
+}
+template <class T>
+__device__ __forceinline__ void ld6r(const T *p, T (&v)[6]) {
+    const cx_t<T> *q = reinterpret_cast<const cx_t<T> *>(p);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const cx_t<T> t = q[i];
+        v[2 * i] = t.x;
+        v[2 * i + 1] = t.y;
+    }
+}
+template <class T>
+__device__ __forceinline__ void st6r(T *p, const T (&v)[6]) {
+    cx_t<T> *q = reinterpret_cast<cx_t<T> *>(p);
+#pragma unroll
+    for (int i = 0; i < 3; i++) q[i] = mk<T>(v[2 * i], v[2 * i + 1]);
 }
 
 // ------------------------------------------------------------ rheology ---
@@ -1103,6 +1163,57 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 // 2 KPc products
                 const int npair = nr / 2 + 1;
                 const int npb = (npair + KPc - 1) / KPc;
+#if AXG_COLUMN_TILES
+                if (qcnt == 25) {
+                    // column n = d * 25 + q of the block: mode a at rA[a * 150 + n], slice k
+                    // at rBr[k * 150 + n]; a thread takes KPc pairs x 6 columns
+                    for (int i = lane; i < 25 * npb; i += TEAM) {
+                        const int pb = (i / 5) % npb, n0 = 6 * ((i / (5 * npb)) * 5 + i % 5);
+                        const int k0 = pb * KPc;
+                        T A[KPc][6], B[KPc][6];
+                        int j[KPc], kst[KPc];
+#pragma unroll
+                        for (int kk = 0; kk < KPc; kk++) {
+                            j[kk] = 0;
+                            kst[kk] = k0 + kk < npair ? k0 + kk : 0;
+#pragma unroll
+                            for (int c = 0; c < 6; c++) { A[kk][c] = 0; B[kk][c] = 0; }
+                        }
+#pragma unroll DFT_UNROLL
+                        for (int al = 1; al < nu; al++) {
+                            C ev[6];
+                            ld6c<T>(rA + al * 150 + n0, ev);
+#pragma unroll
+                            for (int kk = 0; kk < KPc; kk++) {
+                                j[kk] += kst[kk];
+                                j[kk] = j[kk] >= nr ? j[kk] - nr : j[kk];
+                                const T2 w2 = tw2[j[kk]];
+#pragma unroll
+                                for (int c = 0; c < 6; c++) {
+                                    A[kk][c] += ev[c].x * w2.x;
+                                    B[kk][c] += ev[c].y * w2.y;
+                                }
+                            }
+                        }
+                        C c0[6];
+                        ld6c<T>(rA + n0, c0);
+#pragma unroll
+                        for (int kk = 0; kk < KPc; kk++) {
+                            const int k = k0 + kk;
+                            if (k >= npair) break;
+                            T x[6];
+#pragma unroll
+                            for (int c = 0; c < 6; c++) x[c] = c0[c].x + (T)2 * (A[kk][c] - B[kk][c]);
+                            st6r<T>(rBr + (size_t)k * 150 + n0, x);
+                            if (k != 0 && 2 * k != nr) {
+#pragma unroll
+                                for (int c = 0; c < 6; c++) x[c] = c0[c].x + (T)2 * (A[kk][c] + B[kk][c]);
+                                st6r<T>(rBr + (size_t)(nr - k) * 150 + n0, x);
+                            }
+                        }
+                    }
+                } else
+#endif
                 for (int i = lane; i < npb * qcnt; i += TEAM) {
                     const int pb = i / qcnt, qq = i - pb * qcnt, q = q0 + qq;
                     const int k0 = pb * KPc;
@@ -1346,6 +1457,65 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                     continue;
                 }
                 // slices -> Fourier (computeR2C) into region A for these points
+#if AXG_COLUMN_TILES
+                if (!RTZ && qcnt == 25) {
+                    // ABc modes x 6 columns per thread (the column layout of the Fourier ->
+                    // slice pass); the 1/nr scaling applied once to the sums
+                    for (int i = lane; i < 25 * nab; i += TEAM) {
+                        const int ab = (i / 5) % nab, n0 = 6 * ((i / (5 * nab)) * 5 + i % 5);
+                        const int a0 = ab * ABc;
+                        T re[ABc][6], im[ABc][6];
+                        int j[ABc], astep[ABc];
+#pragma unroll
+                        for (int aa = 0; aa < ABc; aa++) {
+                            j[aa] = 0;
+                            astep[aa] = (a0 + aa) % nr;
+#pragma unroll
+                            for (int c = 0; c < 6; c++) { re[aa][c] = 0; im[aa][c] = 0; }
+                        }
+#pragma unroll DFT_UNROLL
+                        for (int k = 0; k <= nr / 2; k++) {
+                            T xs[6], xd[6];
+                            ld6r<T>(rBr + (size_t)k * 150 + n0, xs);
+                            if (k != 0 && 2 * k != nr) {
+                                T x2[6];
+                                ld6r<T>(rBr + (size_t)(nr - k) * 150 + n0, x2);
+#pragma unroll
+                                for (int c = 0; c < 6; c++) {
+                                    xd[c] = xs[c] - x2[c];
+                                    xs[c] += x2[c];
+                                }
+                            } else {
+#pragma unroll
+                                for (int c = 0; c < 6; c++) xd[c] = xs[c];
+                            }
+#pragma unroll
+                            for (int aa = 0; aa < ABc; aa++) {
+                                const T2 w2 = tw2[j[aa]];
+#pragma unroll
+                                for (int c = 0; c < 6; c++) {
+                                    re[aa][c] += xs[c] * w2.x;
+                                    im[aa][c] -= xd[c] * w2.y;
+                                }
+                                j[aa] += astep[aa];
+                                j[aa] = j[aa] >= nr ? j[aa] - nr : j[aa];
+                            }
+                        }
+#pragma unroll
+                        for (int aa = 0; aa < ABc; aa++) {
+                            const int al = a0 + aa;
+                            if (al >= nu) break;
+                            const bool nyq = (nr & 1) == 0 && al == nr / 2;
+                            const T sr = nyq ? (T)0.5 * inv_nr : inv_nr;
+                            const bool noim = al == 0 || nyq;
+                            C sg[6];
+#pragma unroll
+                            for (int c = 0; c < 6; c++) sg[c] = mk<T>(re[aa][c] * sr, noim ? (T)0 : im[aa][c] * inv_nr);
+                            st6c<T>(rA + al * 150 + n0, sg);
+                        }
+                    }
+                } else
+#endif
                 for (int i = lane; i < nab * qcnt; i += TEAM) {
                     const int ab = i / qcnt, qq = i - ab * qcnt, q = q0 + qq;
                     const int a0 = ab * ABc;
