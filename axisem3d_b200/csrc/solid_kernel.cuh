@@ -98,6 +98,16 @@ constexpr int ATT_NONE = 0, ATT_FULL = 1, ATT_CG4 = 2;
 #ifndef AXG_COLUMN_TILES
 #define AXG_COLUMN_TILES 1
 #endif
+// 1 = in FP32 arithmetic (the FP32 and mixed modes) the two direct-sum passes of a chunk of all
+// 25 points run on the tensor cores as small matrix products, (columns x modes) x (modes x
+// slice pairs) and (columns x slice pairs) x (slice pairs x modes), each operand split into a
+// TF32 head and tail and three products accumulated in FP32 (head x head + head x tail +
+// tail x head: the FP32 accuracy of the direct sums); the slice -> Fourier pass only outside
+// RTZ elements. Warp-level mma.sync tiles: parity holds, but measured slower than the column-
+// tiled FP32 sums on B200, so off
+#ifndef AXG_TC_DFT
+#define AXG_TC_DFT 0
+#endif
 // unrolling of the mode loop (Fourier -> slice) and of the slice loop (slice -> Fourier) of
 // the column-tiled passes
 #ifndef AXG_DFT_UNROLL
@@ -165,7 +175,7 @@ struct SolidArgs {
 // shared memory layout of one team
 struct TeamLayout {
     int nr_max, nu_max, qc;
-    size_t geom, trig, ipt, tw, regA, regB, total;
+    size_t geom, trig, ipt, tw, tws, regA, regB, total;
 };
 
 template <class T>
@@ -181,6 +191,8 @@ __host__ __device__ inline TeamLayout team_layout(int nr_max, int qc, int mt) {
     L.trig = o; o = al(o + 4 * 25 * sizeof(T));
     L.ipt = o;  o = al(o + 3 * 25 * sizeof(int));
     L.tw = o;   o = al(o + 2 * (size_t)nr_max * sizeof(T));
+    // the twiddles split for the tensor-core sums: (cos head, cos tail, sin head, sin tail)
+    L.tws = o;  o = al(o + (AXG_TC_DFT && sizeof(T) == 4 ? 4 * (size_t)nr_max * sizeof(T) : 0));
     L.regA = o; o = al(o + 6 * (size_t)L.nu_max * 25 * 2 * sizeof(T));
     size_t b1 = 3 * (size_t)mt * 25 * 2 * sizeof(T);
     size_t b2 = (size_t)nr_max * 6 * qc * sizeof(T);
@@ -233,6 +245,171 @@ __device__ __forceinline__ void st6r(T *p, const T (&v)[6]) {
     cx_t<T> *q = reinterpret_cast<cx_t<T> *>(p);
 #pragma unroll
     for (int i = 0; i < 3; i++) q[i] = mk<T>(v[2 * i], v[2 * i + 1]);
+}
+
+// ------------------------------------------------- tensor-core direct sums ---
+// TF32 head of x (round to nearest, ties away: exact in TF32, whatever the tensor core does with
+// the low 13 bits of an operand) and the tail x - head (exact in FP32; its own rounding to TF32
+// costs at most 2^-22 |x|)
+__device__ __forceinline__ uint32_t tf32_head(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void tf32_split(float x, uint32_t &h, uint32_t &t) {
+    h = tf32_head(x);
+    t = tf32_head(x - __uint_as_float(h));
+}
+// d += a b for one m16n8k8 tile: a (16 x 8, row-major fragment: a0 (g, c), a1 (g + 8, c),
+// a2 (g, c + 4), a3 (g + 8, c + 4)), b (8 x 8: b0 (c, g), b1 (c + 4, g)), d (16 x 8: d0 (g, 2c),
+// d1 (g, 2c + 1), d2 (g + 8, 2c), d3 (g + 8, 2c + 1)); g = lane / 4, c = lane % 4
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// (ah + at) (bh + bt) without the tail x tail product, into three accumulators (head x head,
+// and the two cross terms) so that the three products do not wait on one another
+__device__ __forceinline__ void mma_tf32x3(float (&d)[3][4], const uint32_t (&ah)[4], const uint32_t (&at)[4],
+                                           uint32_t bh0, uint32_t bh1, uint32_t bt0, uint32_t bt1) {
+    mma_tf32(d[0], ah, bh0, bh1);
+    mma_tf32(d[1], at, bh0, bh1);
+    mma_tf32(d[2], ah, bt0, bt1);
+}
+// x mod n for 0 <= x < 2^22 with rn = 1 / n (a float quotient off by at most one, corrected)
+__device__ __forceinline__ int mod_n(int x, int n, float rn) {
+    int r = x - (int)((float)x * rn) * n;
+    r += r < 0 ? n : 0;
+    return r >= n ? r - n : r;
+}
+
+// Fourier -> slices of a chunk holding all 25 points, on the tensor cores. Rows n = d * 25 + q of
+// the (component, point) block (10 tiles of 16), columns k = slice pairs 0 .. nr/2 (tiles of 8),
+// modes a = 1 .. nu - 1 in steps of 8: A[n][k] = sum_a Re c_a[n] cos(a k 2pi/nr) and
+// B[n][k] = sum_a Im c_a[n] sin(a k 2pi/nr), then x_k = c0 + 2 (A - B), x_{nr-k} = c0 + 2 (A + B)
+// (the paired direct sums, each product in three TF32 parts)
+template <class T>
+__device__ __forceinline__ void tc_fourier_to_slices(const cx_t<T> *rA, T *rBr, const float4 *tws, int nr,
+                                                     int lane, int TEAM) {
+    if constexpr (sizeof(T) == 4) {
+        const int nu = nr / 2 + 1;
+        const int wi = lane >> 5, nw = TEAM >> 5, g = (lane & 31) >> 2, c = lane & 3;
+        const int NT = (nu + 7) >> 3, KS = (nu - 1 + 7) >> 3;
+        const float rnr = 1.f / (float)nr;
+        for (int t = wi; t < 10 * NT; t += nw) {
+            const int mt = t % 10, nt = t / 10;
+            const int n0 = mt * 16 + g, n1 = n0 + 8, kp = nt * 8 + g;
+            float dA[3][4] = {}, dB[3][4] = {};
+            // twiddle indices (a k) mod nr of this thread's two B rows, modes 1 + c and 5 + c
+            int j0 = mod_n((1 + c) * kp, nr, rnr), j1 = mod_n((5 + c) * kp, nr, rnr);
+            const int s8 = mod_n(8 * kp, nr, rnr);
+            for (int ks = 0; ks < KS; ks++) {
+                const int a0 = 1 + 8 * ks + c, a1 = a0 + 4;
+                const float2 z = make_float2(0.f, 0.f);
+                float2 v[4];
+                v[0] = (a0 < nu && n0 < 150) ? rA[a0 * 150 + n0] : z;
+                v[1] = (a0 < nu && n1 < 150) ? rA[a0 * 150 + n1] : z;
+                v[2] = (a1 < nu && n0 < 150) ? rA[a1 * 150 + n0] : z;
+                v[3] = (a1 < nu && n1 < 150) ? rA[a1 * 150 + n1] : z;
+                uint32_t rh[4], rt[4], ih[4], it[4];
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    tf32_split(v[r].x, rh[r], rt[r]);
+                    tf32_split(v[r].y, ih[r], it[r]);
+                }
+                const float4 w0 = tws[j0], w1 = tws[j1];
+                mma_tf32x3(dA, rh, rt, __float_as_uint(w0.x), __float_as_uint(w1.x), __float_as_uint(w0.y),
+                           __float_as_uint(w1.y));
+                mma_tf32x3(dB, ih, it, __float_as_uint(w0.z), __float_as_uint(w1.z), __float_as_uint(w0.w),
+                           __float_as_uint(w1.w));
+                j0 += s8;
+                j0 = j0 >= nr ? j0 - nr : j0;
+                j1 += s8;
+                j1 = j1 >= nr ? j1 - nr : j1;
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int n = r < 2 ? n0 : n1, k = nt * 8 + 2 * c + (r & 1);
+                if (n < 150 && k < nu) {
+                    const float c0 = rA[n].x;
+                    const float A = dA[0][r] + (dA[1][r] + dA[2][r]), B = dB[0][r] + (dB[1][r] + dB[2][r]);
+                    rBr[k * 150 + n] = c0 + 2.f * (A - B);
+                    if (k != 0 && 2 * k != nr) rBr[(nr - k) * 150 + n] = c0 + 2.f * (A + B);
+                }
+            }
+        }
+    }
+}
+
+// slices -> Fourier of a chunk holding all 25 points, on the tensor cores: rows n of the block,
+// columns a = 0 .. nu - 1 (tiles of 8), slice pairs k = 0 .. nr/2 in steps of 8:
+// Re S_a[n] = sum_k xs_k[n] cos(a k 2pi/nr) / nr, Im S_a[n] = -sum_k xd_k[n] sin(a k 2pi/nr) / nr
+// with xs_k = x_k + x_{nr-k}, xd_k = x_k - x_{nr-k} (x_k alone at k = 0 and nr/2), the Nyquist
+// mode halved and the imaginary parts of modes 0 and nr/2 dropped
+template <class T>
+__device__ __forceinline__ void tc_slices_to_fourier(cx_t<T> *rA, const T *rBr, const float4 *tws, int nr,
+                                                     T inv_nr, int lane, int TEAM) {
+    if constexpr (sizeof(T) == 4) {
+        const int nu = nr / 2 + 1;
+        const int wi = lane >> 5, nw = TEAM >> 5, g = (lane & 31) >> 2, c = lane & 3;
+        const int NT = (nu + 7) >> 3, KS = (nu + 7) >> 3;
+        const float rnr = 1.f / (float)nr;
+        auto sd = [&](int k, int n, float &xs, float &xd) {
+            xs = 0.f;
+            xd = 0.f;
+            if (k < nu && n < 150) {
+                const float x1 = rBr[k * 150 + n];
+                xs = x1;
+                if (k != 0 && 2 * k != nr) {
+                    const float x2 = rBr[(nr - k) * 150 + n];
+                    xs = x1 + x2;
+                    xd = x1 - x2;
+                }
+            }
+        };
+        for (int t = wi; t < 10 * NT; t += nw) {
+            const int mt = t % 10, nt = t / 10;
+            const int n0 = mt * 16 + g, n1 = n0 + 8, am = nt * 8 + g;
+            float dC[3][4] = {}, dS[3][4] = {};
+            // twiddle indices (k a) mod nr of this thread's two B rows, slices c and c + 4
+            int j0 = mod_n(c * am, nr, rnr), j1 = mod_n((c + 4) * am, nr, rnr);
+            const int s8 = mod_n(8 * am, nr, rnr);
+            for (int ks = 0; ks < KS; ks++) {
+                const int k0 = 8 * ks + c, k1 = k0 + 4;
+                float xs[4], xd[4];
+                sd(k0, n0, xs[0], xd[0]);
+                sd(k0, n1, xs[1], xd[1]);
+                sd(k1, n0, xs[2], xd[2]);
+                sd(k1, n1, xs[3], xd[3]);
+                uint32_t sh[4], st[4], dh[4], dt[4];
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    tf32_split(xs[r], sh[r], st[r]);
+                    tf32_split(xd[r], dh[r], dt[r]);
+                }
+                const float4 w0 = tws[j0], w1 = tws[j1];
+                mma_tf32x3(dC, sh, st, __float_as_uint(w0.x), __float_as_uint(w1.x), __float_as_uint(w0.y),
+                           __float_as_uint(w1.y));
+                mma_tf32x3(dS, dh, dt, __float_as_uint(w0.z), __float_as_uint(w1.z), __float_as_uint(w0.w),
+                           __float_as_uint(w1.w));
+                j0 += s8;
+                j0 = j0 >= nr ? j0 - nr : j0;
+                j1 += s8;
+                j1 = j1 >= nr ? j1 - nr : j1;
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int n = r < 2 ? n0 : n1, al = nt * 8 + 2 * c + (r & 1);
+                if (n < 150 && al < nu) {
+                    const bool nyq = (nr & 1) == 0 && al == nr / 2;
+                    const float re = (dC[0][r] + (dC[1][r] + dC[2][r])) * (nyq ? 0.5f * inv_nr : inv_nr);
+                    const float im = (al == 0 || nyq) ? 0.f : -(dS[0][r] + (dS[1][r] + dS[2][r])) * inv_nr;
+                    rA[al * 150 + n] = make_float2(re, im);
+                }
+            }
+        }
+    }
 }
 
 // ------------------------------------------------------------ rheology ---
@@ -760,6 +937,7 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
     int *sOff = sPt + 25;
     int *sNu = sPt + 50;
     T *sTw = reinterpret_cast<T *>(base + L.tw);
+    float4 *sTws = reinterpret_cast<float4 *>(base + L.tws);
     C *rA = reinterpret_cast<C *>(base + L.regA);
     C *rBc = reinterpret_cast<C *>(base + L.regB);
     T *rBr = reinterpret_cast<T *>(base + L.regB);
@@ -799,6 +977,15 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
             const T *tw = a.tw + a.tw_off[nr];
             // interleaved (cos, sin) pairs: one 2-word shared load per twiddle
             for (int i = lane; i < 2 * nr; i += TEAM) sTw[i] = (i & 1) ? tw[nr + (i >> 1)] : tw[i >> 1];
+            if constexpr (AXG_TC_DFT && sizeof(T) == 4) {
+                for (int i = lane; i < nr; i += TEAM) {
+                    uint32_t ch, ct, sh, st;
+                    tf32_split((float)tw[i], ch, ct);
+                    tf32_split((float)tw[nr + i], sh, st);
+                    sTws[i] = make_float4(__uint_as_float(ch), __uint_as_float(ct), __uint_as_float(sh),
+                                          __uint_as_float(st));
+                }
+            }
         }
         team_sync(team, TEAM);
 
@@ -1163,6 +1350,11 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                 // 2 KPc products
                 const int npair = nr / 2 + 1;
                 const int npb = (npair + KPc - 1) / KPc;
+#if AXG_TC_DFT
+                if (sizeof(T) == 4 && qcnt == 25) {
+                    tc_fourier_to_slices<T>(rA, rBr, sTws, nr, lane, TEAM);
+                } else
+#endif
 #if AXG_COLUMN_TILES
                 if (qcnt == 25) {
                     // column n = d * 25 + q of the block: mode a at rA[a * 150 + n], slice k
@@ -1457,6 +1649,11 @@ solid_stiffness_kernel(const SolidArgs<T, AT> a, const int nr_max, const int qc_
                     continue;
                 }
                 // slices -> Fourier (computeR2C) into region A for these points
+#if AXG_TC_DFT
+                if (!RTZ && sizeof(T) == 4 && qcnt == 25) {
+                    tc_slices_to_fourier<T>(rA, rBr, sTws, nr, inv_nr, lane, TEAM);
+                } else
+#endif
 #if AXG_COLUMN_TILES
                 if (!RTZ && qcnt == 25) {
                     // ABc modes x 6 columns per thread (the column layout of the Fourier ->
