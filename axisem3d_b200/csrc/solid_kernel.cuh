@@ -830,6 +830,16 @@ struct FftView {
     __device__ __forceinline__ cx_t<T> &at(int n, int pp, int qq) const { return p[n * rs + pp * ps + qq]; }
 };
 
+// quotient of 0 <= x < 2^22 by d > 0, rd = 1 / d (the float quotient is off by at most one and
+// corrected): the index splits of the FFT passes without integer division
+__device__ __forceinline__ int div_n(int x, int d, float rd) {
+    int q = (int)((float)x * rd);
+    const int r = x - q * d;
+    q -= r < 0 ? 1 : 0;
+    q += r >= d ? 1 : 0;
+    return q;
+}
+
 // one Stockham pass of radix R over 3 qc signals: Ns = product of the earlier radices
 template <int R, class T>
 __device__ __forceinline__ void fft_pass_r(const FftView<T> in, const FftView<T> out, int N, int qc, int Ns,
@@ -837,10 +847,11 @@ __device__ __forceinline__ void fft_pass_r(const FftView<T> in, const FftView<T>
     using C = cx_t<T>;
     const int S = 3 * qc;
     const int NR = N / R, span = N / (Ns * R);
+    const float rS = 1.f / (float)S, rNs = 1.f / (float)Ns;
     for (int i = lane; i < NR * S; i += TEAM) {
-        const int j = i / S, s = i - j * S;
-        const int pp = s / qc, qq = s - pp * qc;
-        const int k = j % Ns;
+        const int j = div_n(i, S, rS), s = i - j * S;
+        const int pp = (s >= qc) + (s >= 2 * qc), qq = s - pp * qc;
+        const int jn = div_n(j, Ns, rNs), k = j - jn * Ns;
         C v[R];
 #pragma unroll
         for (int r = 0; r < R; r++) v[r] = in.at(j + r * NR, pp, qq);
@@ -852,7 +863,7 @@ __device__ __forceinline__ void fft_pass_r(const FftView<T> in, const FftView<T>
             m = m >= N ? m - N : m;
             if (step) v[r] = cmul<T>(v[r], fft_tw<T>(tw2, m, sign));
         }
-        const int d = (j / Ns) * Ns * R + k;
+        const int d = jn * Ns * R + k;
         if constexpr (R >= 11) {
             // the larger primes: each output summed and stored in turn (fewer live registers)
             const int stepR = N / R;

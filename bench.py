@@ -21,7 +21,12 @@ the Newmark update. Updates per step = sum_e 25 nu_e (nu = nr/2 + 1).
   roofline  the solid stiffness kernels: algorithmic bytes per evaluation /
          measured duration, against the measured HBM copy bandwidth
   cpu_baseline  the C++ CPU restatement (oracle, FP32 like the reference's
-         default build) on all host cores, on a bounded sample of the workload
+         default build) on all host cores: full steps of the whole workload,
+         built with the oracle's own operands, as many as fit the time bound
+
+--impl reference times the same restatement on the same workload and config
+(W warm-up and K timed full steps, a stated prefix of them if K steps would
+run over five minutes).
 
 Run with N GPUs (torchrun): every rank advances its own replica of the
 workload (weak scaling, no exchange); value = all ranks' updates / max time.
