@@ -2056,7 +2056,7 @@ private:
             a.mask = mask;
             a.nwave = nwave_;
             a.sponge = solid ? sg_s_.p : sg_f_.p;
-            int threads = 256, blocks = (int)(((int64_t)P.total * nwave_ + threads - 1) / threads);
+            int threads = POINT_BLOCK, blocks = (int)(((int64_t)P.total * nwave_ * P.ndim + threads - 1) / threads);
             Abc3D &g3 = solid ? sg3_s_ : sg3_f_;
             const bool press = !solid && ps_n_ && (mask & 2);
             if ((g3.n || press) && (mask & 2)) {

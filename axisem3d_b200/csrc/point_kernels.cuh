@@ -627,82 +627,107 @@ struct PointArgs {
     const T *sponge;             // [npoints] Kosloff gamma (0 = none) or null
 };
 
+// One thread per complex value of the point fields ([nwave][nmodes][ndim]), so that every field
+// is read and written in consecutive 8- / 16-byte words. The only condition that mixes the
+// components of a mode (the axial order-1 rule) reads the other component before the block's
+// barrier and every thread writes after it; blocks of POINT_BLOCK threads hold whole modes.
+constexpr int POINT_BLOCK = 288;   // 96 modes of 3 components, 9 warps
 template <class T, class D, bool COMP>
-__global__ void point_update_kernel(const PointArgs<T, D> a) {
-    const int64_t mw = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (mw >= (int64_t)a.nmodes * a.nwave) return;
-    const int mm = (int)(mw % a.nmodes);
-    const size_t m = (size_t)mw;              // index into the batched fields
+__global__ void __launch_bounds__(POINT_BLOCK) point_update_kernel(const PointArgs<T, D> a) {
+    const int nd = a.ndim;
+    const int64_t q64 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = q64 < (int64_t)a.nmodes * a.nwave * nd;
+    const size_t q = valid ? (size_t)q64 : 0;
+    const size_t m = nd == 3 ? q / 3 : q;              // mode of the batched fields
+    const int d = (int)(q - m * nd);
+    const int mm = a.nwave == 1 ? (int)m : (int)(m % (size_t)a.nmodes);
     const int p = a.mode_pt[mm];
     const int off = a.off[p], nr = a.nr[p], nu = nr / 2 + 1, al = mm - off;
     const uint8_t fl = a.flags[p];
-    const int nd = a.ndim;
-    cx_t<T> f[3];
-    for (int d = 0; d < nd; d++) f[d] = a.stiff[(size_t)m * nd + d];
+    cx_t<T> f = valid ? a.stiff[q] : mk<T>(0, 0);
+    // the axial rule of order 1 (solid): both horizontal components of the mode
+    const bool mix = valid && (a.mask & 1) && a.solid && (fl & PT_AXIAL) && al == 1 && d < 2 &&
+                     !(fl & (PT_MASS3D | PT_OCEAN));
+    cx_t<T> g0 = f, g1 = f;
+    if (mix) {
+        g0 = a.stiff[m * 3];
+        g1 = a.stiff[m * 3 + 1];
+    }
+    __syncthreads();
+    if (!valid) return;
     if (!(fl & (PT_MASS3D | PT_OCEAN))) {
-        if (a.mask & 1) point_bc<T>(f, nd, al, nu, nr, fl, a.solid);
-        if (a.mask & 2) {
-            const T im = a.inv_mass1[p];
-            for (int d = 0; d < nd; d++) f[d] = cscale(f[d], im);
+        if (a.mask & 1) {
+            // point_bc for one component (AxialBoundary::apply, the fluid surface, the Nyquist
+            // imaginary parts)
+            const T half = (T)0.5;
+            if (fl & PT_AXIAL) {
+                if (a.solid) {
+                    if (al == 0) {
+                        if (d < 2) f = mk<T>(0, 0);
+                    } else if (al == 1) {
+                        const cx_t<T> t = mk<T>((g0.x + g1.y) * half, (g0.y - g1.x) * half);
+                        f = d == 0 ? t : d == 1 ? mk<T>(-t.y, t.x) : mk<T>(0, 0);
+                    } else {
+                        f = mk<T>(0, 0);
+                    }
+                } else if (al >= 1) {
+                    f = mk<T>(0, 0);
+                }
+            }
+            if (!a.solid && (fl & PT_SURFACE)) f = mk<T>(0, 0);
+            if ((nr & 1) == 0 && al == nu - 1) f.y = 0;
         }
+        if (a.mask & 2) f = cscale(f, a.inv_mass1[p]);
     }
     if ((a.mask & 2) && a.sponge) {
         // Sponge::apply (ABC/Sponge.hpp:74-98), 1-D gamma, on the acceleration
         const T g = a.sponge[p];
         if (g != (T)0) {
             const T two = 2;
-            for (int d = 0; d < nd; d++) {
-                const size_t q = m * nd + d;
-                const cx_t<T> v = mk<T>((T)a.veloc[q].x, (T)a.veloc[q].y);
-                const cx_t<T> u = mk<T>((T)a.displ[q].x, (T)a.displ[q].y);
-                f[d] = csub(f[d], cadd(cscale(v, two * g), cscale(u, g * g)));
-            }
+            const cx_t<T> v = mk<T>((T)a.veloc[q].x, (T)a.veloc[q].y);
+            const cx_t<T> u = mk<T>((T)a.displ[q].x, (T)a.displ[q].y);
+            f = csub(f, cadd(cscale(v, two * g), cscale(u, g * g)));
         }
     }
     if (!(a.mask & 4)) {
         // stages without the update: the result stays in the stiffness field, as
         // computeStiffToAccel works in place on mStiff
-        for (int d = 0; d < nd; d++) a.stiff[(size_t)m * nd + d] = f[d];
+        a.stiff[q] = f;
         return;
     }
-    bool bad = false;
-    for (int d = 0; d < nd; d++) {
-        const size_t q = (size_t)m * nd + d;
-        const cx_t<T> acc = a.accel[q];
-        cx_t<D> v = a.veloc[q], u = a.displ[q];
-        if constexpr (sizeof(D) == sizeof(T)) {
-            // NewmarkTimeScheme::update in the working precision
-            v.x += a.half_dt * (acc.x + f[d].x);
-            v.y += a.half_dt * (acc.y + f[d].y);
-            u.x += a.dt * v.x + a.half_dt_dt * f[d].x;
-            u.y += a.dt * v.y + a.half_dt_dt * f[d].y;
+    const cx_t<T> acc = a.accel[q];
+    cx_t<D> v = a.veloc[q], u = a.displ[q];
+    if constexpr (sizeof(D) == sizeof(T)) {
+        // NewmarkTimeScheme::update in the working precision
+        v.x += a.half_dt * (acc.x + f.x);
+        v.y += a.half_dt * (acc.y + f.y);
+        u.x += a.dt * v.x + a.half_dt_dt * f.x;
+        u.y += a.dt * v.y + a.half_dt_dt * f.y;
+    } else {
+        const D dvx = a.half_dt * ((D)acc.x + (D)f.x);
+        const D dvy = a.half_dt * ((D)acc.y + (D)f.y);
+        if constexpr (COMP) {
+            cx_t<float> cv = a.cv[q], cd = a.cd[q];
+            D y = dvx - (D)cv.x, t = v.x + y; cv.x = (float)((t - v.x) - y); v.x = t;
+            y = dvy - (D)cv.y; t = v.y + y; cv.y = (float)((t - v.y) - y); v.y = t;
+            const D dux = a.dt * v.x + a.half_dt_dt * (D)f.x;
+            const D duy = a.dt * v.y + a.half_dt_dt * (D)f.y;
+            y = dux - (D)cd.x; t = u.x + y; cd.x = (float)((t - u.x) - y); u.x = t;
+            y = duy - (D)cd.y; t = u.y + y; cd.y = (float)((t - u.y) - y); u.y = t;
+            a.cv[q] = cv;
+            a.cd[q] = cd;
         } else {
-            const D dvx = a.half_dt * ((D)acc.x + (D)f[d].x);
-            const D dvy = a.half_dt * ((D)acc.y + (D)f[d].y);
-            if constexpr (COMP) {
-                cx_t<float> cv = a.cv[q], cd = a.cd[q];
-                D y = dvx - (D)cv.x, t = v.x + y; cv.x = (float)((t - v.x) - y); v.x = t;
-                y = dvy - (D)cv.y; t = v.y + y; cv.y = (float)((t - v.y) - y); v.y = t;
-                const D dux = a.dt * v.x + a.half_dt_dt * (D)f[d].x;
-                const D duy = a.dt * v.y + a.half_dt_dt * (D)f[d].y;
-                y = dux - (D)cd.x; t = u.x + y; cd.x = (float)((t - u.x) - y); u.x = t;
-                y = duy - (D)cd.y; t = u.y + y; cd.y = (float)((t - u.y) - y); u.y = t;
-                a.cv[q] = cv;
-                a.cd[q] = cd;
-            } else {
-                v.x += dvx; v.y += dvy;
-                u.x += a.dt * v.x + a.half_dt_dt * (D)f[d].x;
-                u.y += a.dt * v.y + a.half_dt_dt * (D)f[d].y;
-            }
-            a.displ_elem[q] = mk<T>((T)u.x, (T)u.y);
+            v.x += dvx; v.y += dvy;
+            u.x += a.dt * v.x + a.half_dt_dt * (D)f.x;
+            u.y += a.dt * v.y + a.half_dt_dt * (D)f.y;
         }
-        bad |= !(isfinite(u.x) && isfinite(u.y));
-        a.veloc[q] = v;
-        a.displ[q] = u;
-        a.accel[q] = f[d];
-        a.stiff[q] = mk<T>(0, 0);
+        a.displ_elem[q] = mk<T>((T)u.x, (T)u.y);
     }
-    if (bad) atomicOr(a.nonfinite, 1);
+    a.veloc[q] = v;
+    a.displ[q] = u;
+    a.accel[q] = f;
+    a.stiff[q] = mk<T>(0, 0);
+    if (!(isfinite(u.x) && isfinite(u.y))) atomicOr(a.nonfinite, 1);
 }
 
 // ------------------------------------------------------------------ sources ---
