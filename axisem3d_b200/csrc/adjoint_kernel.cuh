@@ -316,32 +316,56 @@ struct AdjPointArgs {
     T h;
 };
 
+// One thread per complex value (mode m, component c), blocks of ADJ_POINT_BLOCK threads holding
+// whole modes, so that the seven cotangent and field streams move in consecutive words. The
+// block shares the scaled cotangents for the axial order-1 rule (which mixes components 0 and 1)
+// and the mass terms, which it sums per point before one atomic add per (point, block).
+constexpr int ADJ_POINT_BLOCK = 288;   // 96 modes of 3 components
 template <class T>
-__global__ void adjoint_point_kernel(const AdjPointArgs<T> a) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= a.nmodes) return;
+__global__ void __launch_bounds__(ADJ_POINT_BLOCK) adjoint_point_kernel(const AdjPointArgs<T> a) {
+    __shared__ cx_t<T> sab[ADJ_POINT_BLOCK];
+    __shared__ T sdm[ADJ_POINT_BLOCK];
+    const int t = threadIdx.x;
+    const int64_t q64 = (int64_t)blockIdx.x * ADJ_POINT_BLOCK + t;
+    const bool valid = q64 < (int64_t)a.nmodes * 3;
+    const size_t q = valid ? (size_t)q64 : 0;
+    const int m = (int)(q / 3), c = (int)(q - (size_t)m * 3);
     const int p = a.mode_pt[m];
     const int off = a.off[p], nr = a.nr[p], nu = nr / 2 + 1, al = m - off;
     const T im = a.inv_mass1[p];
     const T h = a.h;
-    cx_t<T> ab[3], gv[3];
+    cx_t<T> ab = mk<T>(0, 0);
     T dm = 0;
-    for (int c = 0; c < 3; c++) {
-        const size_t q = (size_t)m * 3 + c;
+    if (valid) {
         const cx_t<T> ub = a.ubar[q], vb = a.vbar[q], ao = a.abar_out[q];
         const cx_t<T> abn = mk<T>(ao.x + h / 2 * vb.x + h * h * ub.x, ao.y + h / 2 * vb.y + h * h * ub.y);
         const cx_t<T> an = a.a_n[q];
-        dm -= (abn.x * an.x + abn.y * an.y) * im;
-        ab[c] = cscale(abn, im);
+        dm = -(abn.x * an.x + abn.y * an.y) * im;
+        ab = cscale(abn, im);
         const cx_t<T> vn = mk<T>(vb.x + h * ub.x, vb.y + h * ub.y);
         a.vbar[q] = vn;
         a.abar_out[q] = mk<T>(h / 2 * vn.x, h / 2 * vn.y);
     }
-    // P is symmetric (axial projection and Nyquist rule), so P^T = P
-    point_bc<T>(ab, 3, al, nu, nr, a.flags[p], true);
-    for (int c = 0; c < 3; c++) gv[c] = ab[c];
-    for (int c = 0; c < 3; c++) a.g[(size_t)m * 3 + c] = gv[c];
-    atomicAdd(&a.grad_mass[p], dm);
+    sab[t] = ab;
+    sdm[t] = dm;
+    __syncthreads();
+    if (!valid) return;
+    // P is symmetric (axial projection and Nyquist rule), so P^T = P: point_bc on the mode,
+    // this thread's component
+    const int t0 = t - c;   // component 0 of this mode in the block
+    cx_t<T> f[3] = {sab[t0], sab[t0 + 1], sab[t0 + 2]};
+    point_bc<T>(f, 3, al, nu, nr, a.flags[p], true);
+    a.g[q] = f[c];
+    // the mass terms of this point's modes in the block, summed by the thread of the first
+    if (c == 0 && (al == 0 || t0 == 0)) {
+        T sum = 0;
+        for (int u = t0; u < ADJ_POINT_BLOCK && (int64_t)blockIdx.x * ADJ_POINT_BLOCK + u < (int64_t)a.nmodes * 3;
+             u += 3) {
+            if (u != t0 && a.mode_pt[(int)(((int64_t)blockIdx.x * ADJ_POINT_BLOCK + u) / 3)] != p) break;
+            sum += sdm[u] + sdm[u + 1] + sdm[u + 2];
+        }
+        atomicAdd(&a.grad_mass[p], sum);
+    }
 }
 
 // per-slice mass sensitivities of step n, before adjoint_point_kernel updates the cotangents.

@@ -536,18 +536,24 @@ public:
                                      stream_));
         }
         const int threads = 256;
-        const int mblocks = (sp_.total + threads - 1) / threads;
         const int vblocks = (int)((nf + threads - 1) / threads);
         for (int c = nck - 1; c >= 0; c--) {
             const int len = std::min(ck_interval_, ck_n_ - c * ck_interval_);
             copy_fields_in(c);
             step_ = ck_step0_ + c * ck_interval_;
             set_step(step_);
-            // recompute the segment, keeping u_n and a_n
+            // recompute the segment, keeping u_n and a_n (the forward step's graph, which reads
+            // the step from the device counter set above)
+            if (!cfg_.plain && !graph_exec_) capture();
             for (int i = 0; i < len; i++) {
                 AXG_CUDA(cudaMemcpyAsync(seg_u.p + nf * i, sp_.displ.p, nf * sizeof(C),
                                          cudaMemcpyDeviceToDevice, stream_));
-                launch_step();
+                if (cfg_.plain) {
+                    launch_step();
+                } else {
+                    AXG_CUDA(cudaGraphLaunch(graph_exec_, stream_));
+                    launches_ += kernels_per_step_;
+                }
                 AXG_CUDA(cudaMemcpyAsync(seg_a.p + nf * i, sp_.accel.p, nf * sizeof(C),
                                          cudaMemcpyDeviceToDevice, stream_));
             }
@@ -566,7 +572,8 @@ public:
                         seg_a.p + nf * i, pa.h, adj_tw_.p, adj_tw_off_.p, adj_gmass3_.p);
                     post_launch();
                 }
-                adjoint_point_kernel<T><<<mblocks, threads, 0, stream_>>>(pa);
+                adjoint_point_kernel<T><<<(unsigned)((nf + ADJ_POINT_BLOCK - 1) / ADJ_POINT_BLOCK), ADJ_POINT_BLOCK, 0,
+                                          stream_>>>(pa);
                 post_launch();
                 AdjointArgs<T> aa;
                 aa.n_elem = model_.se.count; aa.nr = e_nr_.p; aa.pts = e_pts_.p; aa.axial = e_axial_.p;
