@@ -324,7 +324,7 @@ class StructuredGridV3D:
             rpi = rp + ":[%d]:%s" % (i, key)
             if key.startswith("C"):
                 raise Model3DError("StructuredGridV3D::StructuredGridV3D || Cij properties are not "
-                                   "supported by this build. || Model name = " + name)
+                                   "supported by this engine. || Model name = " + name)
             if key not in self.PROPERTIES:
                 raise Model3DError("Material::addProperty3D || Unacceptable property key: %s || Model "
                                    "name = %s" % (key, name))

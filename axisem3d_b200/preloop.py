@@ -1054,7 +1054,7 @@ def _gll_numbering(conn: np.ndarray) -> np.ndarray:
 def build(input_dir: str, max_steps: Optional[int] = None, skip_unsupported_channels: bool = False
           ) -> Simulation:
     """Run the preloop on one input directory. skip_unsupported_channels: drop station channels
-    this build does not record (strain, curl, ...) instead of raising; a group left without
+    this engine does not record (strain, curl, ...) instead of raising; a group left without
     channels is dropped, and info["skipped_channels"] names them."""
     inp = Inparam(input_dir)
     mesh = ExodusMesh(inp.path(inp.model.get("model1D:exodus_mesh")))
@@ -1984,7 +1984,7 @@ def _pattern(mtype, data, Q, on_axis, w, phi, nu_1, axial_quad):
 # ----------------------------------------------------------------- stations ---
 # channel::solid::gChannelMap (core/output/channel.hpp:37-73): standard name, the names a user
 # may give, field; kept in the map's order. Stress channels (S*) need the stress of the
-# element at the station and are not recorded by this build.
+# element at the station and are not recorded by this engine.
 SOLID_CHANNELS = (
     ("U1", ("U1", "U"), "U"), ("U2", ("U2", "U"), "U"), ("U3", ("U3", "U"), "U"),
     ("U_NORM", ("U_NORM", "|U|"), "U"),
@@ -2015,7 +2015,7 @@ def standard_channels(user, skipped=None):
         if not found:
             if skipped is None or uch not in UNSUPPORTED_CHANNELS:
                 raise PreloopError("channel::solid::ChannelOptions::ChannelOptions || %s: %s" %
-                                   ("Stress channels are not supported by this build"
+                                   ("Stress channels are not supported by this engine"
                                     if uch in UNSUPPORTED_CHANNELS else "Unknown channel for solid", uch))
             skipped.append(uch)
     return [std for std, _, _ in SOLID_CHANNELS if std in out]
@@ -2053,7 +2053,7 @@ def _release_stations(inp, m, ctx, geo, dt, tmin_simu, tmax_simu, nsteps, enr, s
                                                           "xyz": "xyz"})
         if gm.get_options(rw + ":medium", {"SOLID": False, "FLUID": True}):
             raise PreloopError("StationOutput::release || Fluid station groups are not supported by "
-                               "this build. || Station group name: " + name)
+                               "this engine. || Station group name: " + name)
         chans = standard_channels(gm.get_vector(rw + ":channels"), skipped)
         if not chans:
             continue
@@ -2218,7 +2218,7 @@ def _release_elements(inp, quads, coords, gll, ctx, geo, dt, tmin_simu, tmax_sim
         fluid = gm.get_options(rw + ":medium", {"SOLID": False, "FLUID": True})
         if fluid:
             raise PreloopError("ElementOutput::release || Fluid element groups are not supported by "
-                               "this build. || Element group name: " + name)
+                               "this engine. || Element group name: " + name)
         chans = standard_channels(gm.get_vector(rw + ":channels"))
         rt = root + ":temporal"
         sp = gm.get(rt + ":sampling_period")
