@@ -54,7 +54,42 @@ struct AdjointArgs {
     const int64_t *grad3_off;
     const T *tw;                // twiddle pool: for each nr, nr cos then nr sin
     const int *tw_off;
+    // wider rheologies (the GENERIC instantiation): per element the rheology code (RHEO_ISO,
+    // RHEO_TISO, RHEO_ANISO), the RTZ flag with sin t, cos t, sin 2t, cos 2t per point
+    // ([n][4][25]), and the offsets of the element's moduli [nmod][25] in mod (mod_off) and of
+    // its sensitivities [nmod][25] in grad (grad_off)
+    const int *rheo;
+    const uint8_t *rtz;
+    const T *trig;
+    const int64_t *grad_off;
 };
+
+// Sensitivities of one (mode, point) of a TI or 21-Cij element: the derivative of
+// Re(conj(e(g)) . C e(u)) by each modulus, with P(i, j) = Re(conj(eg_i) eu_j) over the
+// engineering (Voigt) strains that stress_tiso / stress_aniso take. TI (A, C, F, L, N):
+//   A: (g0 + g1)(u0 + u1)   C: g2 u2   F: (g0 + g1) u2 + g2 (u0 + u1)
+//   L: g3 u3 + g4 u4        N: -2 (g0 u1 + g1 u0) + g5 u5
+// 21 Cij, upper triangle row by row: P(i, i) on the diagonal, P(i, j) + P(j, i) off it.
+template <class T>
+__device__ __forceinline__ T pcx(const cx_t<T> &g, const cx_t<T> &u) { return g.x * u.x + g.y * u.y; }
+template <class T>
+__device__ __forceinline__ void add_sens_tiso(const cx_t<T> eg[6], const cx_t<T> eu[6], T *sG, int q) {
+    const cx_t<T> g01 = cadd(eg[0], eg[1]), u01 = cadd(eu[0], eu[1]);
+    atomicAdd(&sG[q], pcx<T>(g01, u01));
+    atomicAdd(&sG[25 + q], pcx<T>(eg[2], eu[2]));
+    atomicAdd(&sG[50 + q], pcx<T>(g01, eu[2]) + pcx<T>(eg[2], u01));
+    atomicAdd(&sG[75 + q], pcx<T>(eg[3], eu[3]) + pcx<T>(eg[4], eu[4]));
+    atomicAdd(&sG[100 + q], (T)-2 * (pcx<T>(eg[0], eu[1]) + pcx<T>(eg[1], eu[0])) + pcx<T>(eg[5], eu[5]));
+}
+template <class T>
+__device__ __forceinline__ void add_sens_aniso(const cx_t<T> eg[6], const cx_t<T> eu[6], T *sG, int q) {
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int j = i; j < 6; j++, k++)
+            atomicAdd(&sG[k * 25 + q], i == j ? pcx<T>(eg[i], eu[i]) : pcx<T>(eg[i], eu[j]) + pcx<T>(eg[j], eu[i]));
+}
 
 // The per-slice sensitivities. A 3-D element's stress at slice k is C(phi_k) e(phi_k) with the
 // strain slices e(phi_k) = C2R(e) and the stress modes R2C(sigma) (SolverFFTW conventions), so
@@ -144,13 +179,18 @@ __device__ __forceinline__ void strain_at(const cx_t<T> *U, int al, int q, bool 
 // lambda / mu sensitivities of this step accumulated into grad
 // SLICES: the instantiation that also accumulates the per-slice sensitivities (a.grad3); the
 // other holds none of that code, so it costs the plain adjoint no registers
-template <class T, bool SLICES>
+// GENERIC: the instantiation for models holding TI or 21-Cij elements (moduli and
+// sensitivities per element at mod_off / grad_off, RTZ frames); the isotropic one keeps its
+// lambda / mu layout. GENERIC is not combined with SLICES.
+template <class T, bool SLICES, bool GENERIC = false>
 __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArgs<T> a, const int nu_max) {
+    static_assert(!(SLICES && GENERIC), "per-slice sensitivities are isotropic only");
     using C = cx_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ T sGll[25], sGlj[25], sGeo[250];
     __shared__ int sOff[25], sNu[25];
     __shared__ T sGl[25], sGm[25];
+    __shared__ T sGx[GENERIC ? 21 * 25 : 1];   // GENERIC: per (modulus, point) sums
     C *Ug = reinterpret_cast<C *>(smem_raw);            // [nu][3][25] g, then A terms
     C *Uu = Ug + (size_t)nu_max * 75;                    // [nu][3][25] u
     C *S = Uu + (size_t)nu_max * 75;                     // [nu][6][25] stress of g, then X/Y
@@ -172,6 +212,8 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
             sGl[i] = 0;
             sGm[i] = 0;
         }
+        if constexpr (GENERIC)
+            for (int i = threadIdx.x; i < 21 * 25; i += blockDim.x) sGx[i] = 0;
         __syncthreads();
         const T *Gxi = axial ? sGlj : sGll;
         for (int i = threadIdx.x; i < nu * 25; i += blockDim.x) {
@@ -192,25 +234,61 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
             C eg[6], eu[6], sg[6];
             strain_at<T>(Ug + al * 75, al, q, axial, Gxi, sGll, sGeo, eg);
             strain_at<T>(Uu + al * 75, al, q, axial, Gxi, sGll, sGeo, eu);
-            const T lam = mod[q], mu = mod[25 + q];
-            stress_iso(eg, sg, lam, mu);
-#pragma unroll
-            for (int d = 0; d < 6; d++) S[(al * 6 + d) * 25 + q] = sg[d];
-            if constexpr (SLICES) {
-#pragma unroll
-                for (int d = 0; d < 6; d++) {
-                    Eg[(al * 6 + d) * 25 + q] = eg[d];
-                    Eu[(al * 6 + d) * 25 + q] = eu[d];
+            if constexpr (GENERIC) {
+                // the forward rheology (elastic_at), in the RTZ frame where the element asks:
+                // sigma = R^T C R e with R = spz_to_rtz6 and R^T = rtz_to_spz6, so each mode's
+                // block stays Hermitian and the sensitivities are those of the RTZ strains
+                const int rh = a.rheo[e];
+                const bool rtz = a.rtz[e] != 0;
+                T s1 = 0, c1 = 1, s2 = 0, c2 = 1;
+                if (rtz) {
+                    const T *tr = a.trig + (size_t)e * 100;
+                    s1 = tr[q]; c1 = tr[25 + q]; s2 = tr[50 + q]; c2 = tr[75 + q];
+                    spz_to_rtz6(eg, s1, c1, s2, c2);
+                    spz_to_rtz6(eu, s1, c1, s2, c2);
                 }
-            }
-            // sensitivities Re(conj(e(g)) . de/dm e(u)), times ifact below
-            const C tg = cadd(cadd(eg[0], eg[1]), eg[2]), tu = cadd(cadd(eu[0], eu[1]), eu[2]);
-            const T pl = tg.x * tu.x + tg.y * tu.y;
-            T pm = 0;
+                if (rh == RHEO_ISO) {
+                    stress_iso(eg, sg, mod[q], mod[25 + q]);
+                    const C tg = cadd(cadd(eg[0], eg[1]), eg[2]), tu = cadd(cadd(eu[0], eu[1]), eu[2]);
+                    T pm = 0;
 #pragma unroll
-            for (int d = 0; d < 6; d++) pm += (d < 3 ? (T)2 : (T)1) * (eg[d].x * eu[d].x + eg[d].y * eu[d].y);
-            atomicAdd(&sGl[q], pl);
-            atomicAdd(&sGm[q], pm);
+                    for (int d = 0; d < 6; d++) pm += (d < 3 ? (T)2 : (T)1) * pcx<T>(eg[d], eu[d]);
+                    atomicAdd(&sGx[q], pcx<T>(tg, tu));
+                    atomicAdd(&sGx[25 + q], pm);
+                } else if (rh == RHEO_TISO) {
+                    stress_tiso(eg, sg, mod[q], mod[25 + q], mod[50 + q], mod[75 + q], mod[100 + q]);
+                    add_sens_tiso<T>(eg, eu, sGx, q);
+                } else {
+                    T cm[21];
+#pragma unroll
+                    for (int k = 0; k < 21; k++) cm[k] = mod[k * 25 + q];
+                    stress_aniso(eg, sg, cm);
+                    add_sens_aniso<T>(eg, eu, sGx, q);
+                }
+                if (rtz) rtz_to_spz6(sg, s1, c1, s2, c2);
+#pragma unroll
+                for (int d = 0; d < 6; d++) S[(al * 6 + d) * 25 + q] = sg[d];
+            } else {
+                const T lam = mod[q], mu = mod[25 + q];
+                stress_iso(eg, sg, lam, mu);
+#pragma unroll
+                for (int d = 0; d < 6; d++) S[(al * 6 + d) * 25 + q] = sg[d];
+                if constexpr (SLICES) {
+#pragma unroll
+                    for (int d = 0; d < 6; d++) {
+                        Eg[(al * 6 + d) * 25 + q] = eg[d];
+                        Eu[(al * 6 + d) * 25 + q] = eu[d];
+                    }
+                }
+                // sensitivities Re(conj(e(g)) . de/dm e(u)), times ifact below
+                const C tg = cadd(cadd(eg[0], eg[1]), eg[2]), tu = cadd(cadd(eu[0], eu[1]), eu[2]);
+                const T pl = tg.x * tu.x + tg.y * tu.y;
+                T pm = 0;
+#pragma unroll
+                for (int d = 0; d < 6; d++) pm += (d < 3 ? (T)2 : (T)1) * (eg[d].x * eu[d].x + eg[d].y * eu[d].y);
+                atomicAdd(&sGl[q], pl);
+                atomicAdd(&sGm[q], pm);
+            }
         }
         __syncthreads();
         if constexpr (SLICES) {
@@ -293,11 +371,21 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
         }
         __syncthreads();
         // grad (each element belongs to one CTA per launch, so no race): -ifact * products
-        for (int q = threadIdx.x; q < 25; q += blockDim.x) {
-            const T f = a.ifact[(size_t)e * 25 + q];
-            T *gr = a.grad + (size_t)e * 50;
-            gr[q] -= f * sGl[q];
-            gr[25 + q] -= f * sGm[q];
+        if constexpr (GENERIC) {
+            const int rh = a.rheo[e];
+            const int nm = rh == RHEO_ISO ? 2 : rh == RHEO_TISO ? 5 : 21;
+            T *gr = a.grad + a.grad_off[e];
+            for (int i = threadIdx.x; i < nm * 25; i += blockDim.x) {
+                const int q = i % 25;
+                gr[i] -= a.ifact[(size_t)e * 25 + q] * sGx[i];
+            }
+        } else {
+            for (int q = threadIdx.x; q < 25; q += blockDim.x) {
+                const T f = a.ifact[(size_t)e * 25 + q];
+                T *gr = a.grad + (size_t)e * 50;
+                gr[q] -= f * sGl[q];
+                gr[25 + q] -= f * sGm[q];
+            }
         }
     }
 }

@@ -507,6 +507,8 @@ public:
         if (ck_n_ <= 0) throw Error(AXG_E_STATE, "axg_adjoint_run || no checkpointed forward run.");
         if (st_n_ > 0 && !seis_adj) throw Error(AXG_E_ARG, "axg_adjoint_run || seismogram cotangents missing.");
         build_adjoint_arrays();
+        if (adj_slices_ && !adj_iso_only_)
+            throw Error(AXG_E_UNSUPPORTED, "axg_adjoint_run || per-slice sensitivities need isotropic elements.");
         const size_t nf = (size_t)sp_.total * 3;
         const int nck = (ck_n_ + ck_interval_ - 1) / ck_interval_;
         const int end_step = ck_step0_ + ck_n_;
@@ -584,10 +586,12 @@ public:
                 aa.grad3_off = adj_grad3_off_.p;
                 aa.tw = adj_tw_.p;
                 aa.tw_off = adj_tw_off_.p;
+                aa.rheo = adj_rheo_.p; aa.rtz = adj_rtz_.p; aa.trig = adj_trig_.p; aa.grad_off = adj_grad_off_.p;
                 const int nu_max = adj_nr_max_ / 2 + 1;
                 const size_t smem = (size_t)nu_max * (75 + 75 + 150 + (adj_slices_ ? 300 : 0)) * sizeof(C);
                 const int grid = std::min(model_.se.count, prop_.multiProcessorCount * 8);
                 if (adj_slices_) adjoint_stiffness_kernel<T, true><<<grid, 128, smem, stream_>>>(aa, nu_max);
+                else if (adj_generic_) adjoint_stiffness_kernel<T, false, true><<<grid, 128, smem, stream_>>>(aa, nu_max);
                 else adjoint_stiffness_kernel<T, false><<<grid, 128, smem, stream_>>>(aa, nu_max);
                 post_launch();
                 adjoint_combine_kernel<T><<<vblocks, threads, 0, stream_>>>((int)nf, ub.p, kg.p);
@@ -610,7 +614,7 @@ public:
         if (grad_u0) d2h_cx(ub.p, grad_u0);
         if (grad_v0) d2h_cx(vb.p, grad_v0);
         if (grad_mod) {
-            std::vector<T> hg((size_t)model_.se.count * 50);
+            std::vector<T> hg((size_t)adj_grad_n_);
             AXG_CUDA(cudaMemcpy(hg.data(), adj_grad_.p, hg.size() * sizeof(T), cudaMemcpyDeviceToHost));
             for (size_t i = 0; i < hg.size(); i++) grad_mod[i] = (double)hg[i];
         }
@@ -721,11 +725,12 @@ private:
         if (nwave_ != 1) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || one wavefield per handle.");
         if (model_.prt.count) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || PRT elements are not differentiated.");
         for (int e = 0; e < h.count; e++) {
-            bool ok = h.rheo[e] == AXG_ISO && !(h.is3d.size() && h.is3d[e]) &&
-                      !(h.att.size() && h.att[e] != AXG_ATT_NONE);
+            bool ok = !(h.is3d.size() && h.is3d[e]) && !(h.att.size() && h.att[e] != AXG_ATT_NONE);
             if (!ok)
                 throw Error(AXG_E_UNSUPPORTED,
-                            "axg_adjoint || needs isotropic, phi-constant, non-attenuating solid elements.");
+                            "axg_adjoint || needs phi-constant, non-attenuating solid elements.");
+            if (h.rheo[e] != RHEO_ISO && h.rtz.size() && h.rtz[e] && h.theta.size() < (size_t)(e + 1) * 25)
+                throw Error(AXG_E_ARG, "axg_adjoint || RTZ element without theta.");
         }
         for (int p = 0; p < sp_.n; p++)
             if (model_.sp.mass_nr.size() && model_.sp.mass_nr[p] > 1)
@@ -798,9 +803,13 @@ private:
     void build_adjoint_arrays() {
         if (adj_built_) return;
         const HostSolidElements &h = model_.se;
-        std::vector<T> geom((size_t)h.count * 250), ifact((size_t)h.count * 25), mod((size_t)h.count * 50);
-        std::vector<int64_t> moff(h.count);
+        std::vector<T> geom((size_t)h.count * 250), ifact((size_t)h.count * 25), mod, trig;
+        std::vector<int64_t> moff(h.count), goff(h.count);
+        std::vector<int> rheo(h.count);
+        std::vector<uint8_t> rtz(h.count, 0);
         adj_nr_max_ = 1;
+        adj_generic_ = false;
+        adj_iso_only_ = true;
         for (int e = 0; e < h.count; e++) {
             adj_nr_max_ = std::max(adj_nr_max_, h.nr[e]);
             for (int c = 0; c < 5; c++)
@@ -810,11 +819,36 @@ private:
                         (T)(h.geom[(size_t)e * 150 + c * 25 + q] * h.geom[(size_t)e * 150 + 125 + q]);
                 }
             for (int q = 0; q < 25; q++) ifact[(size_t)e * 25 + q] = (T)h.geom[(size_t)e * 150 + 125 + q];
-            for (int i = 0; i < 50; i++) mod[(size_t)e * 50 + i] = (T)h.moduli[h.mat_off[e] + i];
-            moff[e] = (int64_t)e * 50;
+            // phi-constant moduli [nmod][1][25]; isotropic-only models keep [n][2][25]
+            const int nm = nmod_of(h.rheo[e]);
+            moff[e] = goff[e] = (int64_t)mod.size();
+            for (int i = 0; i < nm * 25; i++) mod.push_back((T)h.moduli[h.mat_off[e] + i]);
+            rheo[e] = h.rheo[e];
+            if (h.rheo[e] != RHEO_ISO) {
+                adj_generic_ = true;
+                adj_iso_only_ = false;
+                // RTZ frames matter to TI / 21-Cij elements only (the isotropic stress is frame-free)
+                if (h.rtz.size() && h.rtz[e]) {
+                    rtz[e] = 1;
+                    trig.resize((size_t)h.count * 100, (T)0);
+                    for (int q = 0; q < 25; q++) {
+                        const double t = h.theta[(size_t)e * 25 + q];
+                        trig[(size_t)e * 100 + q] = (T)std::sin(t);
+                        trig[(size_t)e * 100 + 25 + q] = (T)std::cos(t);
+                        trig[(size_t)e * 100 + 50 + q] = (T)std::sin(2. * t);
+                        trig[(size_t)e * 100 + 75 + q] = (T)std::cos(2. * t);
+                    }
+                }
+            }
         }
+        if (trig.empty()) trig.push_back((T)0);
         adj_geom_.upload(geom); adj_ifact_.upload(ifact); adj_mod_.upload(mod); adj_mod_off_.upload(moff);
-        adj_grad_.alloc((size_t)h.count * 50);
+        adj_grad_n_ = (int64_t)mod.size();
+        adj_grad_off_.upload(goff);
+        adj_rheo_.upload(rheo);
+        adj_rtz_.upload(rtz);
+        adj_trig_.upload(trig);
+        adj_grad_.alloc(std::max<int64_t>(adj_grad_n_, 1));
         adj_gmass_.alloc(sp_.n);
         if (!e_nr_.p) {
             e_nr_.upload(h.nr); e_pts_.upload(h.pts);
@@ -826,6 +860,7 @@ private:
         if (smem > 200 * 1024) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || nr too large.");
         raise_smem_limit((const void *)adjoint_stiffness_kernel<T, false>, smem);
         raise_smem_limit((const void *)adjoint_stiffness_kernel<T, true>, smem);
+        raise_smem_limit((const void *)adjoint_stiffness_kernel<T, false, true>, smem);
         adj_built_ = true;
     }
 
@@ -2147,7 +2182,12 @@ private:
     DBuf<int64_t> adj_grad3_off_, adj_gmass3_off_;
     DBuf<int> adj_tw_off_;
     DBuf<T> adj_geom_, adj_ifact_, adj_mod_, adj_grad_, adj_gmass_;
-    DBuf<int64_t> adj_mod_off_;
+    DBuf<int64_t> adj_mod_off_, adj_grad_off_;
+    DBuf<int> adj_rheo_;
+    DBuf<uint8_t> adj_rtz_;
+    DBuf<T> adj_trig_;
+    int64_t adj_grad_n_ = 0;
+    bool adj_generic_ = false, adj_iso_only_ = true;
 
     DBuf<T> gmat_, tw_;
     DBuf<int> tw_off_;

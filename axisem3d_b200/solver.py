@@ -302,23 +302,33 @@ class Solver:
     def adjoint(self, seis_adjoint, slices=False):
         """Discrete adjoint of the last checkpointed run for dJ/d(seismograms).
 
-        Returns dJ/d(lambda, mu) per element point (ne, 2, 25), dJ/d(point mass),
-        and dJ/d(initial displacement / velocity) in the field layout. With slices=True also
+        Returns dJ/d(moduli) per element point, dJ/d(point mass), and dJ/d(initial
+        displacement / velocity) in the field layout. The moduli gradient follows each
+        element's moduli (lambda, mu; A, C, F, L, N; the 21 Cij): an (ne, nmod, 25) array when
+        every element has the same rheology, (ne, 2, 25) for an isotropic model, else a list of
+        (nmod_e, 25) arrays. With slices=True also
         the per-slice sensitivities of the 3-D parameterisation: "moduli_slices", a list of
         (2, nr_e, 25) arrays (lambda, mu at phi_k = 2 pi k / nr_e), and "mass_slices", a list of
         (nr_p,) arrays per solid point."""
         ne = self.model.n_solid_elements
         self._check(self.lib.axg_set_adjoint_slices(self.h, int(bool(slices))))
         r = np.ascontiguousarray(seis_adjoint, dtype=np.float64)
-        gm = np.zeros((ne, 2, 25))
+        nmod = np.array([{L.AXG_ISO: 2, L.AXG_TISO: 5, L.AXG_ANISO: 21}[int(r)]
+                         for r in np.asarray(self.model.se_rheo).ravel()], np.int64)
+        gflat = np.zeros(int(np.sum(nmod)) * 25)
         gmass = np.zeros(len(self.model.sp_nr))
         nf = self.field_size(True)
         gu = np.zeros(nf, dtype=np.complex128)
         gv = np.zeros(nf, dtype=np.complex128)
-        self._check(self.lib.axg_adjoint_run(self.h, r.ctypes.data_as(L.P_f64), gm.ctypes.data_as(L.P_f64),
+        self._check(self.lib.axg_adjoint_run(self.h, r.ctypes.data_as(L.P_f64), gflat.ctypes.data_as(L.P_f64),
                                              gmass.ctypes.data_as(L.P_f64),
                                              gu.view(np.float64).ctypes.data_as(L.P_f64),
                                              gv.view(np.float64).ctypes.data_as(L.P_f64)))
+        if ne == 0 or np.all(nmod == nmod[0]):
+            gm = gflat.reshape(ne, int(nmod[0]) if ne else 2, 25)
+        else:
+            go = np.concatenate([[0], np.cumsum(nmod * 25)])
+            gm = [gflat[go[e]:go[e + 1]].reshape(nmod[e], 25) for e in range(ne)]
         out = {"moduli": gm, "mass": gmass, "displ0": gu, "veloc0": gv}
         if slices:
             enr = np.asarray(self.model.se_nr, np.int64)

@@ -1,0 +1,155 @@
+"""GPU tests of the discrete adjoint on transversely isotropic and 21-Cij elements (FP64,
+phi-constant moduli, SPZ and RTZ frames): the dot-product test of the linear map
+(initial state -> seismograms) and the moduli gradient of an L2 waveform misfit against
+central finite differences along random directions."""
+import copy
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NMOD = {0: 2, 1: 5, 2: 21}
+
+
+def _wide_model(kind, rtz, sources, nx=8, nz=8, nr=9, seed=5):
+    """The 8 x 8, nr = 9 box with its elements made TI ("tiso"), 21-Cij ("aniso") or a mix of
+    isotropic, TI and 21-Cij elements ("mixed"): the isotropic background's moduli with seeded
+    3 % perturbations (TI: each of A, C, F, L, N; 21 Cij: a positive-definite symmetric one).
+    With rtz the TI and 21-Cij elements take their moduli in the RTZ frame at smooth
+    per-point polar angles."""
+    from axisem3d_b200 import _lib as L
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=nx, nz=nz, nr=nr, nstations=12, nr_aware_dt=True)
+    m.dt = meshgen.round_dt(m.dt * 0.9)       # headroom for the stiffer perturbed moduli
+    if not sources:
+        m.ms_elem = np.zeros(0, np.int32)
+        m.ms_nu = np.zeros(0, np.int32)
+        m.ms_pat_off = np.zeros(0, np.int64)
+        m.ms_pattern = np.zeros(0, np.complex128)
+        m.ms_stf = []
+    rng = np.random.default_rng(seed)
+    ne = m.n_solid_elements
+    iso = m.se_moduli.reshape(ne, 2, 25)
+    codes = {"tiso": [L.AXG_TISO] * ne, "aniso": [L.AXG_ANISO] * ne,
+             "mixed": [(L.AXG_ISO, L.AXG_TISO, L.AXG_ANISO)[e % 3] for e in range(ne)]}[kind]
+    pool, off = [], []
+    o = 0
+    for e in range(ne):
+        lam, mu = iso[e, 0], iso[e, 1]
+        if codes[e] == L.AXG_ISO:
+            mods = np.stack([lam, mu])
+        elif codes[e] == L.AXG_TISO:
+            base = np.stack([lam + 2 * mu, lam + 2 * mu, lam, mu, mu])
+            mods = base * (1.0 + 0.03 * rng.uniform(-1.0, 1.0, base.shape))
+        else:
+            mods = np.stack(meshgen.aniso_moduli_from(lam, mu, rng, 0.03))
+        off.append(o)
+        o += mods.size
+        pool.append(mods.ravel())
+    m.se_rheo = np.array(codes, np.int32)
+    m.se_mat_off = np.array(off, np.int64)
+    m.se_moduli = np.concatenate(pool)
+    if rtz:
+        m.se_rtz = np.ones(ne, np.uint8)
+        sz = m.sp_coords[m.se_pts]                      # (ne, 25, 2)
+        m.se_theta = 0.4 + 0.6 * sz[..., 0] / 100e3 - 0.3 * sz[..., 1] / 100e3
+    return m
+
+
+def _flat(g):
+    return np.concatenate([np.ravel(x) for x in g]) if isinstance(g, list) else np.ravel(g)
+
+
+@pytest.mark.parametrize("kind,rtz", [("tiso", False), ("aniso", True), ("mixed", True)])
+def test_wide_adjoint_dot_product(built, kind, rtz):
+    """<R Phi(u0, v0), r> == <u0, ubar0(r)> + <v0, vbar0(r)> in FP64 over several checkpoint
+    segments, for TI, 21-Cij (RTZ frame) and mixed-rheology models."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = _wide_model(kind, rtz, sources=False)
+    rng = np.random.default_rng(0)
+    u0 = meshgen.random_displacement(m, seed=1)
+    v0 = meshgen.random_displacement(m, seed=2) * 50.0
+    with Solver(m, "fp64") as s:
+        s.set_field(u0, "displ")
+        s.set_field(v0, "veloc")
+        s.forward_checkpointed(230, 64)
+        seis = s.seismograms()
+        r = rng.normal(size=seis.shape)
+        g = s.adjoint(r)
+    assert np.all(np.isfinite(seis)) and float(np.max(np.abs(seis))) > 0
+    lhs = float(np.sum(seis * r))
+    rhs = float(np.sum(np.real(np.conj(u0) * g["displ0"])) + np.sum(np.real(np.conj(v0) * g["veloc0"])))
+    assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), 1e-300), (lhs, rhs)
+    # the gradient comes back in each element's own moduli layout
+    gm = g["moduli"]
+    nm = [NMOD[int(c)] for c in m.se_rheo]
+    if kind == "mixed":
+        assert isinstance(gm, list) and [x.shape for x in gm] == [(k, 25) for k in nm]
+    else:
+        assert gm.shape == (m.n_solid_elements, nm[0], 25)
+
+
+@pytest.mark.parametrize("kind,rtz", [("tiso", True), ("aniso", False), ("mixed", True)])
+def test_wide_adjoint_moduli_gradient(built, kind, rtz):
+    """Misfit J = 1/2 |d(C) - d_obs|^2 at the receivers (d_obs: the unperturbed model's
+    synthetics): the adjoint gradient by every modulus of every element point against central
+    differences at eps and eps/2, Richardson-extrapolated, along six random directions."""
+    from axisem3d_b200.solver import Solver
+    base = _wide_model(kind, rtz, sources=True)
+    nsteps, interval = 300, 50
+
+    def run(model):
+        with Solver(model, "fp64") as s:
+            s.forward_checkpointed(nsteps, interval)
+            return s.seismograms()
+
+    obs = run(base)
+    rng = np.random.default_rng(11)
+    x0 = base.se_moduli * (1.0 + 0.02 * rng.uniform(-1.0, 1.0, base.se_moduli.shape))
+
+    def model_at(x):
+        m = copy.deepcopy(base)
+        m.se_moduli = x
+        return m
+
+    with Solver(model_at(x0), "fp64") as s:
+        s.forward_checkpointed(nsteps, interval)
+        d = s.seismograms()
+        g = s.adjoint(d - obs)
+    grad = _flat(g["moduli"])
+    assert grad.shape == x0.shape
+    J0 = 0.5 * float(np.sum((d - obs) ** 2))
+    assert J0 > 0
+
+    def misfit_at(eps, dirv):
+        return 0.5 * float(np.sum((run(model_at(x0 + eps * dirv)) - obs) ** 2))
+
+    scale = float(np.mean(np.abs(x0)))
+    eps = 1e-4
+    for k in range(6):
+        dirv = rng.normal(size=x0.shape) * scale
+        f1 = (misfit_at(eps, dirv) - misfit_at(-eps, dirv)) / (2 * eps)
+        f2 = (misfit_at(eps / 2, dirv) - misfit_at(-eps / 2, dirv)) / eps
+        fd = (4 * f2 - f1) / 3
+        an = float(np.dot(grad, dirv))
+        assert abs(fd - an) <= 1e-6 * max(abs(an), 1e-300), (k, f1, f2, fd, an)
+
+
+def test_wide_adjoint_rejects_slices_and_attenuation(built):
+    """Per-slice sensitivities stay isotropic; attenuating elements stay undifferentiated."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import EngineError, Solver
+    m = _wide_model("tiso", False, sources=False)
+    with Solver(m, "fp64") as s:
+        s.set_field(meshgen.random_displacement(m, seed=1), "displ")
+        s.forward_checkpointed(20, 10)
+        r = np.zeros_like(s.seismograms())
+        with pytest.raises(EngineError, match="per-slice sensitivities need isotropic"):
+            s.adjoint(r, slices=True)
+    att = meshgen.cartesian_model(nx=4, nz=4, nr=5, nstations=4,
+                                  attenuation=dict(meshgen.default_sls(3), qkappa=57823.0, qmu=120.0))
+    with Solver(att, "fp64") as s:
+        with pytest.raises(EngineError, match="non-attenuating"):
+            s.forward_checkpointed(10, 5)
