@@ -62,6 +62,17 @@ struct AdjointArgs {
     const uint8_t *rtz;
     const T *trig;
     const int64_t *grad_off;
+    // attenuating elements (GENERIC): att code per element (ATT_NONE / ATT_FULL / ATT_CG4), its
+    // dlambda, dmu [2][npa] at attmod_off, and its adjoint SLS state at astate_off (complex
+    // units): [nsls + 1][6][nu][npa], the cotangents of the memory variables and, last, of the
+    // dstress; npa = 25 (FULL) or 4 (CG4)
+    const int *att;
+    const T *attmod;
+    const int64_t *attmod_off;
+    cx_t<T> *astate;
+    const int64_t *astate_off;
+    int nsls;
+    T alpha[8], beta[8], gamma[8];
 };
 
 // Sensitivities of one (mode, point) of a TI or 21-Cij element: the derivative of
@@ -190,7 +201,7 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
     __shared__ T sGll[25], sGlj[25], sGeo[250];
     __shared__ int sOff[25], sNu[25];
     __shared__ T sGl[25], sGm[25];
-    __shared__ T sGx[GENERIC ? 21 * 25 : 1];   // GENERIC: per (modulus, point) sums
+    __shared__ T sGx[GENERIC ? 23 * 25 : 1];   // GENERIC: per (modulus, point) sums
     C *Ug = reinterpret_cast<C *>(smem_raw);            // [nu][3][25] g, then A terms
     C *Uu = Ug + (size_t)nu_max * 75;                    // [nu][3][25] u
     C *S = Uu + (size_t)nu_max * 75;                     // [nu][6][25] stress of g, then X/Y
@@ -213,7 +224,7 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
             sGm[i] = 0;
         }
         if constexpr (GENERIC)
-            for (int i = threadIdx.x; i < 21 * 25; i += blockDim.x) sGx[i] = 0;
+            for (int i = threadIdx.x; i < 23 * 25; i += blockDim.x) sGx[i] = 0;
         __syncthreads();
         const T *Gxi = axial ? sGlj : sGll;
         for (int i = threadIdx.x; i < nu * 25; i += blockDim.x) {
@@ -264,6 +275,51 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
                     for (int k = 0; k < 21; k++) cm[k] = mod[k * 25 + q];
                     stress_aniso(eg, sg, cm);
                     add_sens_aniso<T>(eg, eu, sGx, q);
+                }
+                const int at = a.att[e];
+                const int k4 = at == ATT_CG4 ? cg4_slot(q) : q;
+                if (at != ATT_NONE && k4 >= 0) {
+                    // the reverse SLS recursion. Forward (AttenuationFull::apply, in the frame of
+                    // the elastic stress): sigma_n = C e_n - sum_l m_l^n,
+                    // m_l^{n+1} = alpha_l m_l^n + beta_l d^n + gamma_l D e_n, d^{n+1} = D e_n, with
+                    // D = iso(dlambda, dmu). With the cotangents divided by the integral factor
+                    // (mb_l of m_l, db of d, held per slot from step n+1): z = sum_l gamma_l mb_l
+                    // + db enters the stress of g as sigma = C e(g) - D z, then db <- sum_l
+                    // beta_l mb_l and mb_l <- alpha_l mb_l + e(g); dJ/d(dlambda, dmu) gains
+                    // +ifact Re(conj(z) . dD e(u_n)).
+                    const int npa = at == ATT_CG4 ? 4 : 25;
+                    const size_t ns = (size_t)nu * npa, sl = (size_t)al * npa + k4;
+                    C *st = a.astate + a.astate_off[e];
+                    const T *am = a.attmod + a.attmod_off[e];
+                    C z[6], dn[6], dz[6];
+#pragma unroll
+                    for (int d = 0; d < 6; d++) {
+                        z[d] = st[((size_t)a.nsls * 6 + d) * ns + sl];
+                        dn[d] = mk<T>(0, 0);
+                    }
+                    for (int l = 0; l < a.nsls; l++) {
+                        const T al_ = a.alpha[l], be = a.beta[l], ga = a.gamma[l];
+#pragma unroll
+                        for (int d = 0; d < 6; d++) {
+                            C &mv = st[((size_t)l * 6 + d) * ns + sl];
+                            const C m = mv;
+                            z[d] = cadd(z[d], cscale(m, ga));
+                            dn[d] = cadd(dn[d], cscale(m, be));
+                            mv = cadd(cscale(m, al_), eg[d]);
+                        }
+                    }
+#pragma unroll
+                    for (int d = 0; d < 6; d++) st[((size_t)a.nsls * 6 + d) * ns + sl] = dn[d];
+                    stress_iso(z, dz, am[k4], am[npa + k4]);
+#pragma unroll
+                    for (int d = 0; d < 6; d++) sg[d] = csub(sg[d], dz[d]);
+                    const int nm = rh == RHEO_ISO ? 2 : rh == RHEO_TISO ? 5 : 21;
+                    const C tz = cadd(cadd(z[0], z[1]), z[2]), tu = cadd(cadd(eu[0], eu[1]), eu[2]);
+                    T pm = 0;
+#pragma unroll
+                    for (int d = 0; d < 6; d++) pm += (d < 3 ? (T)2 : (T)1) * pcx<T>(z[d], eu[d]);
+                    atomicAdd(&sGx[nm * 25 + q], -pcx<T>(tz, tu));
+                    atomicAdd(&sGx[(nm + 1) * 25 + q], -pm);
                 }
                 if (rtz) rtz_to_spz6(sg, s1, c1, s2, c2);
 #pragma unroll
@@ -373,7 +429,7 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
         // grad (each element belongs to one CTA per launch, so no race): -ifact * products
         if constexpr (GENERIC) {
             const int rh = a.rheo[e];
-            const int nm = rh == RHEO_ISO ? 2 : rh == RHEO_TISO ? 5 : 21;
+            const int nm = (rh == RHEO_ISO ? 2 : rh == RHEO_TISO ? 5 : 21) + (a.att[e] != ATT_NONE ? 2 : 0);
             T *gr = a.grad + a.grad_off[e];
             for (int i = threadIdx.x; i < nm * 25; i += blockDim.x) {
                 const int q = i % 25;

@@ -493,6 +493,7 @@ public:
         const size_t nf = (size_t)sp_.total * 3;
         const int nck = (nsteps + interval - 1) / interval;
         ck_displ_.alloc(nf * nck); ck_veloc_.alloc(nf * nck); ck_accel_.alloc(nf * nck);
+        if (state_wave_ > 0) ck_state_.alloc((size_t)state_wave_ * nck);
         ck_n_ = nsteps; ck_interval_ = interval; ck_step0_ = step_;
         for (int c = 0; c < nck; c++) {
             copy_fields_out(c);
@@ -508,7 +509,7 @@ public:
         if (st_n_ > 0 && !seis_adj) throw Error(AXG_E_ARG, "axg_adjoint_run || seismogram cotangents missing.");
         build_adjoint_arrays();
         if (adj_slices_ && !adj_iso_only_)
-            throw Error(AXG_E_UNSUPPORTED, "axg_adjoint_run || per-slice sensitivities need isotropic elements.");
+            throw Error(AXG_E_UNSUPPORTED, "axg_adjoint_run || per-slice sensitivities need isotropic, non-attenuating elements.");
         const size_t nf = (size_t)sp_.total * 3;
         const int nck = (ck_n_ + ck_interval_ - 1) / ck_interval_;
         const int end_step = ck_step0_ + ck_n_;
@@ -518,6 +519,13 @@ public:
         AXG_CUDA(cudaMemcpyAsync(fin_d.p, sp_.displ.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
         AXG_CUDA(cudaMemcpyAsync(fin_v.p, sp_.veloc.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
         AXG_CUDA(cudaMemcpyAsync(fin_a.p, sp_.accel.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        DBuf<AT> fin_s;
+        if (state_wave_ > 0) {
+            fin_s.alloc((size_t)state_wave_);
+            AXG_CUDA(cudaMemcpyAsync(fin_s.p, state_.p, (size_t)state_wave_ * sizeof(AT), cudaMemcpyDeviceToDevice,
+                                     stream_));
+        }
+        if (adj_astate_n_ > 0) adj_astate_.zero(stream_);
         DBuf<C> ub, vb, ab, g, kg, seg_u, seg_a;
         ub.alloc(nf); vb.alloc(nf); ab.alloc(nf); g.alloc(nf); kg.alloc(nf);
         ub.zero(stream_); vb.zero(stream_); ab.zero(stream_); kg.zero(stream_);
@@ -587,6 +595,13 @@ public:
                 aa.tw = adj_tw_.p;
                 aa.tw_off = adj_tw_off_.p;
                 aa.rheo = adj_rheo_.p; aa.rtz = adj_rtz_.p; aa.trig = adj_trig_.p; aa.grad_off = adj_grad_off_.p;
+                aa.att = adj_att_.p; aa.attmod = adj_attmod_.p; aa.attmod_off = adj_attmod_off_.p;
+                aa.astate = adj_astate_.p; aa.astate_off = adj_astate_off_.p; aa.nsls = cfg_.nsls;
+                for (int l = 0; l < 8; l++) {
+                    aa.alpha[l] = l < cfg_.nsls ? (T)cfg_.att_alpha[l] : (T)0;
+                    aa.beta[l] = l < cfg_.nsls ? (T)cfg_.att_beta[l] : (T)0;
+                    aa.gamma[l] = l < cfg_.nsls ? (T)cfg_.att_gamma[l] : (T)0;
+                }
                 const int nu_max = adj_nr_max_ / 2 + 1;
                 const size_t smem = (size_t)nu_max * (75 + 75 + 150 + (adj_slices_ ? 300 : 0)) * sizeof(C);
                 const int grid = std::min(model_.se.count, prop_.multiProcessorCount * 8);
@@ -627,6 +642,9 @@ public:
         AXG_CUDA(cudaMemcpyAsync(sp_.displ.p, fin_d.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
         AXG_CUDA(cudaMemcpyAsync(sp_.veloc.p, fin_v.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
         AXG_CUDA(cudaMemcpyAsync(sp_.accel.p, fin_a.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        if (state_wave_ > 0)
+            AXG_CUDA(cudaMemcpyAsync(state_.p, fin_s.p, (size_t)state_wave_ * sizeof(AT), cudaMemcpyDeviceToDevice,
+                                     stream_));
         sp_.stiff.zero(stream_);
         step_ = end_step;
         set_step(step_);
@@ -725,10 +743,8 @@ private:
         if (nwave_ != 1) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || one wavefield per handle.");
         if (model_.prt.count) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || PRT elements are not differentiated.");
         for (int e = 0; e < h.count; e++) {
-            bool ok = !(h.is3d.size() && h.is3d[e]) && !(h.att.size() && h.att[e] != AXG_ATT_NONE);
-            if (!ok)
-                throw Error(AXG_E_UNSUPPORTED,
-                            "axg_adjoint || needs phi-constant, non-attenuating solid elements.");
+            if (h.is3d.size() && h.is3d[e])
+                throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || needs phi-constant solid elements.");
             if (h.rheo[e] != RHEO_ISO && h.rtz.size() && h.rtz[e] && h.theta.size() < (size_t)(e + 1) * 25)
                 throw Error(AXG_E_ARG, "axg_adjoint || RTZ element without theta.");
         }
@@ -741,12 +757,18 @@ private:
         AXG_CUDA(cudaMemcpyAsync(ck_displ_.p + nf * c, sp_.displ.p, nf * sizeof(CD), cudaMemcpyDeviceToDevice, stream_));
         AXG_CUDA(cudaMemcpyAsync(ck_veloc_.p + nf * c, sp_.veloc.p, nf * sizeof(CD), cudaMemcpyDeviceToDevice, stream_));
         AXG_CUDA(cudaMemcpyAsync(ck_accel_.p + nf * c, sp_.accel.p, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        if (state_wave_ > 0)   // the SLS memory variables of the step
+            AXG_CUDA(cudaMemcpyAsync(ck_state_.p + (size_t)state_wave_ * c, state_.p, (size_t)state_wave_ * sizeof(AT),
+                                     cudaMemcpyDeviceToDevice, stream_));
     }
     void copy_fields_in(int c) {
         const size_t nf = (size_t)sp_.total * 3;
         AXG_CUDA(cudaMemcpyAsync(sp_.displ.p, ck_displ_.p + nf * c, nf * sizeof(CD), cudaMemcpyDeviceToDevice, stream_));
         AXG_CUDA(cudaMemcpyAsync(sp_.veloc.p, ck_veloc_.p + nf * c, nf * sizeof(CD), cudaMemcpyDeviceToDevice, stream_));
         AXG_CUDA(cudaMemcpyAsync(sp_.accel.p, ck_accel_.p + nf * c, nf * sizeof(C), cudaMemcpyDeviceToDevice, stream_));
+        if (state_wave_ > 0)
+            AXG_CUDA(cudaMemcpyAsync(state_.p, ck_state_.p + (size_t)state_wave_ * c, (size_t)state_wave_ * sizeof(AT),
+                                     cudaMemcpyDeviceToDevice, stream_));
         sp_.stiff.zero(stream_);
     }
     // per-slice sensitivity buffers: [2][nr_e][25] per element, [nr_p] per point, and the
@@ -804,9 +826,13 @@ private:
         if (adj_built_) return;
         const HostSolidElements &h = model_.se;
         std::vector<T> geom((size_t)h.count * 250), ifact((size_t)h.count * 25), mod, trig;
+        int64_t gsize = 0;
         std::vector<int64_t> moff(h.count), goff(h.count);
-        std::vector<int> rheo(h.count);
+        std::vector<int> rheo(h.count), att(h.count, ATT_NONE);
         std::vector<uint8_t> rtz(h.count, 0);
+        std::vector<T> attmod;
+        std::vector<int64_t> aoff(h.count, -1), soff(h.count, -1);
+        int64_t astate_n = 0;
         adj_nr_max_ = 1;
         adj_generic_ = false;
         adj_iso_only_ = true;
@@ -821,9 +847,25 @@ private:
             for (int q = 0; q < 25; q++) ifact[(size_t)e * 25 + q] = (T)h.geom[(size_t)e * 150 + 125 + q];
             // phi-constant moduli [nmod][1][25]; isotropic-only models keep [n][2][25]
             const int nm = nmod_of(h.rheo[e]);
-            moff[e] = goff[e] = (int64_t)mod.size();
+            moff[e] = (int64_t)mod.size();
+            goff[e] = gsize;
             for (int i = 0; i < nm * 25; i++) mod.push_back((T)h.moduli[h.mat_off[e] + i]);
+            gsize += nm * 25;
             rheo[e] = h.rheo[e];
+            if (h.att.size() && h.att[e] != AXG_ATT_NONE) {
+                // dlambda, dmu [2][npa] and the adjoint SLS state [nsls + 1][6][nu][npa]; the
+                // gradient gains two rows (dlambda, dmu at the element points; with CG4 at its
+                // four points)
+                const int npa = h.att[e] == AXG_ATT_CG4 ? 4 : 25;
+                att[e] = h.att[e] == AXG_ATT_CG4 ? ATT_CG4 : ATT_FULL;
+                aoff[e] = (int64_t)attmod.size();
+                for (int i = 0; i < 2 * npa; i++) attmod.push_back((T)h.att_moduli[h.att_off[e] + i]);
+                soff[e] = astate_n;
+                astate_n += (int64_t)(cfg_.nsls + 1) * 6 * (h.nr[e] / 2 + 1) * npa;
+                gsize += 50;
+                adj_generic_ = true;
+                adj_iso_only_ = false;
+            }
             if (h.rheo[e] != RHEO_ISO) {
                 adj_generic_ = true;
                 adj_iso_only_ = false;
@@ -843,8 +885,15 @@ private:
         }
         if (trig.empty()) trig.push_back((T)0);
         adj_geom_.upload(geom); adj_ifact_.upload(ifact); adj_mod_.upload(mod); adj_mod_off_.upload(moff);
-        adj_grad_n_ = (int64_t)mod.size();
+        adj_grad_n_ = gsize;
         adj_grad_off_.upload(goff);
+        if (attmod.empty()) attmod.push_back((T)0);
+        adj_att_.upload(att);
+        adj_attmod_.upload(attmod);
+        adj_attmod_off_.upload(aoff);
+        adj_astate_off_.upload(soff);
+        adj_astate_n_ = astate_n;
+        adj_astate_.alloc(std::max<int64_t>(astate_n, 1));
         adj_rheo_.upload(rheo);
         adj_rtz_.upload(rtz);
         adj_trig_.upload(trig);
@@ -2186,7 +2235,12 @@ private:
     DBuf<int> adj_rheo_;
     DBuf<uint8_t> adj_rtz_;
     DBuf<T> adj_trig_;
-    int64_t adj_grad_n_ = 0;
+    int64_t adj_grad_n_ = 0, adj_astate_n_ = 0;
+    DBuf<int> adj_att_;
+    DBuf<T> adj_attmod_;
+    DBuf<int64_t> adj_attmod_off_, adj_astate_off_;
+    DBuf<C> adj_astate_;
+    DBuf<AT> ck_state_;
     bool adj_generic_ = false, adj_iso_only_ = true;
 
     DBuf<T> gmat_, tw_;

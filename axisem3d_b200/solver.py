@@ -304,7 +304,8 @@ class Solver:
 
         Returns dJ/d(moduli) per element point, dJ/d(point mass), and dJ/d(initial
         displacement / velocity) in the field layout. The moduli gradient follows each
-        element's moduli (lambda, mu; A, C, F, L, N; the 21 Cij): an (ne, nmod, 25) array when
+        element's moduli (lambda, mu; A, C, F, L, N; the 21 Cij), then, for an attenuating
+        element, its dlambda, dmu (with CG4 at the four CG4 points): an (ne, nmod, 25) array when
         every element has the same rheology, (ne, 2, 25) for an isotropic model, else a list of
         (nmod_e, 25) arrays. With slices=True also
         the per-slice sensitivities of the 3-D parameterisation: "moduli_slices", a list of
@@ -315,6 +316,8 @@ class Solver:
         r = np.ascontiguousarray(seis_adjoint, dtype=np.float64)
         nmod = np.array([{L.AXG_ISO: 2, L.AXG_TISO: 5, L.AXG_ANISO: 21}[int(r)]
                          for r in np.asarray(self.model.se_rheo).ravel()], np.int64)
+        if self.model.se_att is not None:       # attenuating elements: + dlambda, dmu
+            nmod = nmod + 2 * (np.asarray(self.model.se_att).ravel() != L.AXG_ATT_NONE)
         gflat = np.zeros(int(np.sum(nmod)) * 25)
         gmass = np.zeros(len(self.model.sp_nr))
         nf = self.field_size(True)

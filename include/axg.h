@@ -399,8 +399,8 @@ int  axg_run(axg_solver *h, int32_t nsteps, int32_t use_graph);
 int  axg_current_step(const axg_solver *h, int32_t *tstep);
 
 /* ---- differentiation (FP64 handles; phi-constant isotropic, TI or 21-Cij solid
-        elements, RTZ frames included, no attenuation, no fluid; no counterpart in the
-        reference, which has no adjoint) ---- */
+        elements, RTZ frames included, elastic or with FULL / CG4 attenuation, no fluid; no
+        counterpart in the reference, which has no adjoint) ---- */
 /* nsteps forward steps from the current state, storing the state every
    checkpoint_interval steps on the device for axg_adjoint_run */
 int  axg_forward_checkpointed(axg_solver *h, int32_t nsteps, int32_t checkpoint_interval);
@@ -408,7 +408,9 @@ int  axg_forward_checkpointed(axg_solver *h, int32_t nsteps, int32_t checkpoint_
    segment recomputed from its checkpoint. seis_adjoint = dJ/d(seismograms),
    [nrecords][nstations][3]. Outputs (host, each may be NULL):
    grad_moduli per element [nmod_e][25] in the order of its moduli (lambda, mu; A, C, F, L,
-   N; the 21 Cij), elements in order, so [n_solid_elements][2][25] for an isotropic model;
+   N; the 21 Cij), then, for an attenuating element, two rows dJ/d(dlambda, dmu) (CG4: at its
+   four points q = 6, 8, 16, 18, zero elsewhere), elements in order, so
+   [n_solid_elements][2][25] for an elastic isotropic model;
    grad_mass [n_solid_points]
    dJ/d(point mass), grad_displ0 / grad_veloc0 (sum(nu)*3 complex) dJ/d(initial
    displacement / velocity). The fields end in the state after the forward run. */
@@ -420,8 +422,8 @@ int  axg_adjoint_run(axg_solver *h, const double *seis_adjoint, double *grad_mod
    element or a Mass3D point holds (PhysicalProperty.hpp:99-120): dJ/dlambda and dJ/dmu at
    every (slice, point) of every element, dJ/dM at every slice of every solid point. The
    linearisation point is the handle's phi-constant model; with odd nr a 3-D element there
-   equals the 1-D one, and the sum over slices is the 1-D gradient. Isotropic models only
-   (axg_adjoint_run returns AXG_E_UNSUPPORTED otherwise). */
+   equals the 1-D one, and the sum over slices is the 1-D gradient. Elastic isotropic models
+   only (axg_adjoint_run returns AXG_E_UNSUPPORTED otherwise). */
 int  axg_set_adjoint_slices(axg_solver *h, int32_t on);
 /* after such a run: grad_moduli_slices per element [2][nr_e][25] (lambda, mu), elements in
    order; grad_mass_slices per solid point [nr_p]; either may be NULL */

@@ -12,16 +12,28 @@ pytestmark = pytest.mark.gpu
 NMOD = {0: 2, 1: 5, 2: 21}
 
 
-def _wide_model(kind, rtz, sources, nx=8, nz=8, nr=9, seed=5):
+def _wide_model(kind, rtz, sources, nx=8, nz=8, nr=9, seed=5, att=None):
     """The 8 x 8, nr = 9 box with its elements made TI ("tiso"), 21-Cij ("aniso") or a mix of
-    isotropic, TI and 21-Cij elements ("mixed"): the isotropic background's moduli with seeded
-    3 % perturbations (TI: each of A, C, F, L, N; 21 Cij: a positive-definite symmetric one).
-    With rtz the TI and 21-Cij elements take their moduli in the RTZ frame at smooth
-    per-point polar angles."""
+    isotropic, TI and 21-Cij elements ("mixed"), or left isotropic ("iso"): the isotropic
+    background's moduli with seeded 3 % perturbations (TI: each of A, C, F, L, N; 21 Cij: a
+    positive-definite symmetric one). With rtz the TI and 21-Cij elements take their moduli in
+    the RTZ frame at smooth per-point polar angles. att = "full" or "cg4": 3 SLS with
+    Q_mu = 120 (the unrelaxed moduli of the background), CG4 taking dlambda, dmu at its four
+    points."""
     from axisem3d_b200 import _lib as L
     from axisem3d_b200 import meshgen
-    m = meshgen.cartesian_model(nx=nx, nz=nz, nr=nr, nstations=12, nr_aware_dt=True)
+    sls = dict(meshgen.default_sls(3), qkappa=57823.0, qmu=120.0) if att else None
+    m = meshgen.cartesian_model(nx=nx, nz=nz, nr=nr, nstations=12, nr_aware_dt=True, attenuation=sls)
     m.dt = meshgen.round_dt(m.dt * 0.9)       # headroom for the stiffer perturbed moduli
+    if att:
+        a, b, g = meshgen.att_alpha_beta_gamma(sls["w"], sls["y"], m.dt)
+        m.att_alpha, m.att_beta, m.att_gamma = a, b, g
+        if att == "cg4":
+            ne_ = m.n_solid_elements
+            am = m.se_att_moduli.reshape(ne_, 2, 25)[:, :, meshgen.CG4_POINTS]
+            m.se_att = np.full(ne_, L.AXG_ATT_CG4, np.int32)
+            m.se_att_off = np.arange(ne_, dtype=np.int64) * 8
+            m.se_att_moduli = np.ascontiguousarray(am).ravel()
     if not sources:
         m.ms_elem = np.zeros(0, np.int32)
         m.ms_nu = np.zeros(0, np.int32)
@@ -31,7 +43,7 @@ def _wide_model(kind, rtz, sources, nx=8, nz=8, nr=9, seed=5):
     rng = np.random.default_rng(seed)
     ne = m.n_solid_elements
     iso = m.se_moduli.reshape(ne, 2, 25)
-    codes = {"tiso": [L.AXG_TISO] * ne, "aniso": [L.AXG_ANISO] * ne,
+    codes = {"iso": [L.AXG_ISO] * ne, "tiso": [L.AXG_TISO] * ne, "aniso": [L.AXG_ANISO] * ne,
              "mixed": [(L.AXG_ISO, L.AXG_TISO, L.AXG_ANISO)[e % 3] for e in range(ne)]}[kind]
     pool, off = [], []
     o = 0
@@ -137,8 +149,118 @@ def test_wide_adjoint_moduli_gradient(built, kind, rtz):
         assert abs(fd - an) <= 1e-6 * max(abs(an), 1e-300), (k, f1, f2, fd, an)
 
 
-def test_wide_adjoint_rejects_slices_and_attenuation(built):
-    """Per-slice sensitivities stay isotropic; attenuating elements stay undifferentiated."""
+def _att_grad(model, gm):
+    """The adjoint's dlambda, dmu rows (the last two of each attenuating element) in the layout
+    of model.se_att_moduli: [2][25] per element (FULL), [2][4] at the CG4 points (CG4)."""
+    from axisem3d_b200 import _lib as L
+    from axisem3d_b200 import meshgen
+    rows = gm if isinstance(gm, list) else list(gm)
+    out = []
+    for e, r in enumerate(rows):
+        d = r[-2:]
+        out.append((d[:, meshgen.CG4_POINTS] if model.se_att[e] == L.AXG_ATT_CG4 else d).ravel())
+    return np.concatenate(out)
+
+
+@pytest.mark.parametrize("kind,rtz,att", [("iso", False, "full"), ("tiso", True, "full"),
+                                          ("aniso", True, "cg4"), ("mixed", True, "full")])
+def test_attenuation_adjoint_dot_product(built, kind, rtz, att):
+    """The dot-product test through the SLS recursion (FULL and CG4; checkpoints hold the
+    memory variables, each segment is recomputed from them): <R Phi(u0, v0), r> ==
+    <u0, ubar0(r)> + <v0, vbar0(r)> in FP64 over several checkpoint segments."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = _wide_model(kind, rtz, sources=False, att=att)
+    rng = np.random.default_rng(0)
+    u0 = meshgen.random_displacement(m, seed=1)
+    v0 = meshgen.random_displacement(m, seed=2) * 50.0
+    with Solver(m, "fp64") as s:
+        s.set_field(u0, "displ")
+        s.set_field(v0, "veloc")
+        s.forward_checkpointed(230, 64)
+        seis = s.seismograms()
+        r = rng.normal(size=seis.shape)
+        g = s.adjoint(r)
+        # the adjoint leaves the handle in the state after the forward run, SLS memory included
+        d_end = s.get_field("displ")
+        s.run(5)
+        d_more = s.get_field("displ")
+    with Solver(m, "fp64") as s2:
+        s2.set_field(u0, "displ")
+        s2.set_field(v0, "veloc")
+        s2.run(230)
+        ref_end = s2.get_field("displ")
+        s2.run(5)
+        ref_more = s2.get_field("displ")
+    # equal up to the order of the atomic scatter-adds
+    assert np.linalg.norm(d_end - ref_end) <= 1e-11 * np.linalg.norm(ref_end)
+    assert np.linalg.norm(d_more - ref_more) <= 1e-11 * np.linalg.norm(ref_more)
+    lhs = float(np.sum(seis * r))
+    rhs = float(np.sum(np.real(np.conj(u0) * g["displ0"])) + np.sum(np.real(np.conj(v0) * g["veloc0"])))
+    assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), 1e-300), (lhs, rhs)
+
+
+@pytest.mark.parametrize("kind,rtz,att", [("iso", False, "full"), ("tiso", True, "cg4")])
+def test_attenuation_adjoint_moduli_gradient(built, kind, rtz, att):
+    """The gradient by the unrelaxed moduli and by dlambda, dmu of every attenuating element
+    point against Richardson-extrapolated central differences of the L2 waveform misfit along
+    six random directions."""
+    from axisem3d_b200.solver import Solver
+    base = _wide_model(kind, rtz, sources=True, att=att)
+    nsteps, interval = 300, 50
+    nm = base.se_moduli.size
+
+    def model_at(x):
+        m = copy.deepcopy(base)
+        m.se_moduli = x[:nm].copy()
+        m.se_att_moduli = x[nm:].copy()
+        return m
+
+    def run(model):
+        with Solver(model, "fp64") as s:
+            s.forward_checkpointed(nsteps, interval)
+            return s.seismograms()
+
+    obs = run(base)
+    rng = np.random.default_rng(13)
+    xb = np.concatenate([base.se_moduli, base.se_att_moduli])
+    x0 = xb * (1.0 + 0.02 * rng.uniform(-1.0, 1.0, xb.shape))
+    with Solver(model_at(x0), "fp64") as s:
+        s.forward_checkpointed(nsteps, interval)
+        d = s.seismograms()
+        g = s.adjoint(d - obs)
+    gm = g["moduli"]
+    rows = gm if isinstance(gm, list) else list(gm)
+    grad = np.concatenate([np.concatenate([r[:-2].ravel() for r in rows]), _att_grad(base, gm)])
+    assert grad.shape == x0.shape
+    assert float(np.max(np.abs(_att_grad(base, gm)))) > 0
+
+    def misfit_at(eps, dirv):
+        return 0.5 * float(np.sum((run(model_at(x0 + eps * dirv)) - obs) ** 2))
+
+    # directions scaled per block: the attenuation moduli are a few % of the elastic ones
+    sc = np.concatenate([np.full(nm, np.mean(np.abs(x0[:nm]))), np.full(x0.size - nm, np.mean(np.abs(x0[nm:])))])
+    eps = 1e-4
+    for k in range(6):
+        dirv = rng.normal(size=x0.shape) * sc
+        f1 = (misfit_at(eps, dirv) - misfit_at(-eps, dirv)) / (2 * eps)
+        f2 = (misfit_at(eps / 2, dirv) - misfit_at(-eps / 2, dirv)) / eps
+        fd = (4 * f2 - f1) / 3
+        an = float(np.dot(grad, dirv))
+        assert abs(fd - an) <= 1e-6 * max(abs(an), 1e-300), (k, f1, f2, fd, an)
+    # the attenuation moduli alone
+    dirv = np.zeros_like(x0)
+    dirv[nm:] = rng.normal(size=x0.size - nm) * sc[nm:]
+    f1 = (misfit_at(eps, dirv) - misfit_at(-eps, dirv)) / (2 * eps)
+    f2 = (misfit_at(eps / 2, dirv) - misfit_at(-eps / 2, dirv)) / eps
+    fd = (4 * f2 - f1) / 3
+    an = float(np.dot(grad, dirv))
+    assert abs(fd - an) <= 1e-6 * max(abs(an), 1e-300), (f1, f2, fd, an)
+
+
+def test_wide_adjoint_rejects_slices_and_3d_moduli(built):
+    """Per-slice sensitivities stay isotropic and elastic; 3-D (per-slice) moduli stay
+    undifferentiated."""
     from axisem3d_b200 import meshgen
     from axisem3d_b200.solver import EngineError, Solver
     m = _wide_model("tiso", False, sources=False)
@@ -148,8 +270,11 @@ def test_wide_adjoint_rejects_slices_and_attenuation(built):
         r = np.zeros_like(s.seismograms())
         with pytest.raises(EngineError, match="per-slice sensitivities need isotropic"):
             s.adjoint(r, slices=True)
-    att = meshgen.cartesian_model(nx=4, nz=4, nr=5, nstations=4,
-                                  attenuation=dict(meshgen.default_sls(3), qkappa=57823.0, qmu=120.0))
-    with Solver(att, "fp64") as s:
-        with pytest.raises(EngineError, match="non-attenuating"):
+    m3 = meshgen.cartesian_model(nx=4, nz=4, nr=5, nstations=4)
+    ne = m3.n_solid_elements
+    m3.se_is3d = np.ones(ne, np.uint8)
+    m3.se_moduli = np.repeat(m3.se_moduli.reshape(ne, 2, 1, 25), 5, axis=2).ravel()
+    m3.se_mat_off = np.arange(ne, dtype=np.int64) * 250
+    with Solver(m3, "fp64") as s:
+        with pytest.raises(EngineError, match="phi-constant"):
             s.forward_checkpointed(10, 5)
