@@ -312,6 +312,14 @@ class PartitionedRun:
         self.torch = torch
         self._dev = {}
         if self.device_path:
+            # The engine's hooks, its gather / scatter-add and the NCCL send / receive are
+            # ordered on one stream of this run's own: ProcessGroupNCCL makes its stream wait on
+            # the current torch stream when an operation is queued, and req.wait() makes the
+            # current stream wait on it, so the exchange runs with that stream current and the
+            # handle launches on it (the engine's own stream does not synchronise with others).
+            self.stream = torch.cuda.Stream(device=device)
+            if hasattr(self.solver, "set_stream"):
+                self.solver.set_stream(self.stream.cuda_stream)
             cdt = torch.complex128 if self.solver.precision == "fp64" else torch.complex64
             for other, (ss, fs) in self.plan.items():
                 ent = []
@@ -327,19 +335,20 @@ class PartitionedRun:
         dist, torch = self.dist, self.torch
         ops, recv = [], []
         if self.device_path:
-            for other in sorted(self.plan):
-                for solid, sl, sbuf, rbuf in self._dev[other]:
-                    if len(sl) == 0:
-                        continue
-                    self.solver.gather_stiffness(sl.data_ptr(), len(sl), sbuf.data_ptr(), solid)
-                    ops.append(dist.P2POp(dist.isend, torch.view_as_real(sbuf), other))
-                    ops.append(dist.P2POp(dist.irecv, torch.view_as_real(rbuf), other))
-                    recv.append((solid, sl, rbuf))
-            if ops:
-                for req in dist.batch_isend_irecv(ops):
-                    req.wait()
-            for solid, sl, rbuf in recv:
-                self.solver.scatter_add_stiffness(sl.data_ptr(), len(sl), rbuf.data_ptr(), solid)
+            with torch.cuda.stream(self.stream):
+                for other in sorted(self.plan):
+                    for solid, sl, sbuf, rbuf in self._dev[other]:
+                        if len(sl) == 0:
+                            continue
+                        self.solver.gather_stiffness(sl.data_ptr(), len(sl), sbuf.data_ptr(), solid)
+                        ops.append(dist.P2POp(dist.isend, torch.view_as_real(sbuf), other))
+                        ops.append(dist.P2POp(dist.irecv, torch.view_as_real(rbuf), other))
+                        recv.append((solid, sl, rbuf))
+                if ops:
+                    for req in dist.batch_isend_irecv(ops):
+                        req.wait()
+                for solid, sl, rbuf in recv:
+                    self.solver.scatter_add_stiffness(sl.data_ptr(), len(sl), rbuf.data_ptr(), solid)
             return
         fields = {}
         for solid in (True, False):

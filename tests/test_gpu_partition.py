@@ -125,3 +125,102 @@ def test_two_subdomains_equal_one_domain(built, name, precision):
     assert rel(got, ref) <= TOL[precision], rel(got, ref)
     if ref_f is not None:
         assert rel(got_f, ref_f) <= TOL[precision], rel(got_f, ref_f)
+
+
+class _ThreadTransport:
+    """The part of torch.distributed that PartitionedRun.exchange calls (P2POp, isend, irecv,
+    batch_isend_irecv), for ranks that live as threads of one process on one GPU: a send
+    waits for the sender's current stream and hands a copy of the buffer to the receiver
+    through the host, a receive copies it into the buffer on the receiver's current stream.
+    No kernel waits on another rank; the host orders everything."""
+
+    def __init__(self, rank, box, cv, timeout=120.0):
+        self.rank, self.box, self.cv, self.timeout = rank, box, cv, timeout
+        self.isend, self.irecv = "isend", "irecv"
+
+    @staticmethod
+    def P2POp(op, tensor, peer):
+        from types import SimpleNamespace
+        return SimpleNamespace(op=op, tensor=tensor, peer=peer)
+
+    def batch_isend_irecv(self, ops):
+        import torch
+        torch.cuda.current_stream().synchronize()
+        with self.cv:
+            for op in ops:
+                if op.op == self.isend:
+                    self.box.setdefault((self.rank, op.peer), []).append(op.tensor.cpu().clone())
+            self.cv.notify_all()
+        for op in ops:
+            if op.op != self.irecv:
+                continue
+            key = (op.peer, self.rank)
+            with self.cv:
+                if not self.cv.wait_for(lambda: self.box.get(key), timeout=self.timeout):
+                    raise TimeoutError("no message from rank %d" % op.peer)
+                data = self.box[key].pop(0)
+            op.tensor.copy_(data.to(op.tensor.device))
+
+        class _Done:
+            def wait(self):
+                return True
+        return [_Done()]
+
+
+@pytest.mark.parametrize("name", ["box_abc", "shell_fluid"])
+def test_partitioned_run_device_path(built, name):
+    """PartitionedRun's device path (the engine's gather / scatter-add on the run's own stream,
+    buffers handed over by the transport between the boundary conditions before and after
+    assembly) with two ranks as two threads of this process, against one handle holding the
+    whole mesh: FP64 <= 1e-12. NCCL itself is not exercised (one GPU); the transport stands in
+    for its point-to-point calls."""
+    import threading
+    import torch
+    from axisem3d_b200 import partition as P
+    from axisem3d_b200.solver import Solver
+    m, nsteps, _ = _model(name)
+    runs = [P.PartitionedRun(m, lambda sub: Solver(sub, "fp64"), rank=r, nparts=2, device="cuda")
+            for r in range(2)]
+    box, cv = {}, threading.Condition()
+    for r, run in enumerate(runs):
+        assert run.device_path
+        run.dist = _ThreadTransport(r, box, cv)
+    errors, parts = [None, None], [None, None]
+
+    def rank_main(r):
+        try:
+            runs[r].run(nsteps)
+            runs[r].stream.synchronize()
+            sub, s = runs[r].sub, runs[r].solver
+            parts[r] = (sub.meta["global"], s.get_field("displ"),
+                        s.get_field("displ", solid=False) if len(sub.fp_nr) else None)
+        except BaseException as exc:  # reported by the main thread
+            errors[r] = exc
+
+    try:
+        threads = [threading.Thread(target=rank_main, args=(r,)) for r in range(2)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join(timeout=600)
+        assert not any(t.is_alive() for t in threads), "rank thread did not finish"
+        for e in errors:
+            if e is not None:
+                raise e
+    finally:
+        for run in runs:
+            run.solver.close()
+    with Solver(m, "fp64") as s:
+        s.run(nsteps)
+        ref = s.get_field("displ")
+        ref_f = s.get_field("displ", solid=False) if len(m.fp_nr) else None
+    got = np.zeros_like(ref)
+    got_f = np.zeros_like(ref_f) if ref_f is not None else None
+    for g, d, df in parts:
+        got[_global_slots(m.sp_nr, g["solid_points"], 3)] = d
+        if df is not None:
+            got_f[_global_slots(m.fp_nr, g["fluid_points"], 1)] = df
+    assert np.abs(ref).max() > 0
+    assert rel(got, ref) <= TOL["fp64"], rel(got, ref)
+    if ref_f is not None:
+        assert rel(got_f, ref_f) <= TOL["fp64"], rel(got_f, ref_f)
