@@ -142,6 +142,8 @@ SIGNATURES = {
     "axg_set_adjoint_slices": (C.c_int, [H, C.c_int32]),
     "axg_get_adjoint_slices": (C.c_int, [H, P_f64, P_f64]),
     "axg_gather_stiffness": (C.c_int, [H, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p]),
+    "axg_set_element_parts": (C.c_int, [H, C.c_void_p, C.c_void_p]),
+    "axg_compute_stiffness_part": (C.c_int, [H, C.c_int32]),
     "axg_scatter_add_stiffness": (C.c_int, [H, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p]),
     "axg_apply_bc_before_assembly": (C.c_int, [H]),
     "axg_apply_bc_after_assembly": (C.c_int, [H]),

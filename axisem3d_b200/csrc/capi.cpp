@@ -627,6 +627,26 @@ int axg_apply_sources(axg_solver *h, int32_t tstep) {
 int axg_compute_stiffness(axg_solver *h) {
     return guarded(h, [&] { h->eng->compute_stiffness(); });
 }
+int axg_compute_stiffness_part(axg_solver *h, int32_t part) {
+    return guarded(h, [&] {
+        if (!h->finalized) throw axg::Error(AXG_E_STATE, "axg_compute_stiffness_part || axg_finalize not called.");
+        h->eng->compute_stiffness_part(part);
+    });
+}
+int axg_set_element_parts(axg_solver *h, const uint8_t *solid_part, const uint8_t *fluid_part) {
+    return guarded(h, [&] {
+        need_open(h);
+        auto take = [](std::vector<uint8_t> &dst, const uint8_t *src, int count) {
+            dst.clear();
+            if (!src) return;
+            for (int e = 0; e < count; e++)
+                if (src[e] > 1) throw axg::Error(AXG_E_ARG, "axg_set_element_parts || a part is 0 or 1.");
+            dst.assign(src, src + count);
+        };
+        take(h->model.se.part, solid_part, h->model.se.count);
+        take(h->model.fe.part, fluid_part, h->model.fe.count);
+    });
+}
 // no device allocation: the SLS memory of the evaluation lives in the library's fixed
 // device array (noalloc.cu), looked up on this handle's device at the first call there
 int axg_compute_stiffness_noalloc(axg_solver *h, const void *solid_x, void *solid_f, const void *fluid_x,

@@ -36,6 +36,7 @@ struct HostSolidElements {
     std::vector<double> geom, theta;
     std::vector<int64_t> mat_off, att_off;
     std::vector<double> moduli, att_moduli;
+    std::vector<uint8_t> part;   // axg_set_element_parts: 0 / 1 per element, empty = all 0
 };
 
 struct HostFluidElements {
@@ -45,6 +46,7 @@ struct HostFluidElements {
     std::vector<double> geom;
     std::vector<int64_t> mat_off;
     std::vector<double> moduli;
+    std::vector<uint8_t> part;
 };
 
 struct HostCoupling {
@@ -188,6 +190,7 @@ public:
     virtual void finalize(const HostModel &m) = 0;
     virtual void apply_sources(int tstep) = 0;
     virtual void compute_stiffness() = 0;
+    virtual void compute_stiffness_part(int part) = 0;   // the buckets of one element part
     virtual void bc_before() = 0;
     virtual void point_stage(int mask) = 0;   // 1 = BC after assembly, 2 = 1/M, 4 = Newmark
     virtual void record(int tstep) = 0;

@@ -121,6 +121,7 @@ class Engine final : public EngineBase {
     };
     struct SolidBucket {
         int rheo, att, is3d, rtz, cls, team, tpc, qc, nr_max, n, grid = 1;
+        int part = 0;   // element part (axg_set_element_parts)
         int mt = 1;   // Fourier modes per tile of the gather / gradient and the quadrature
         int fft = 0;  // 3-D elements of nr >= AXG_FFT_MIN_NR take the slice FFTs
         int ahead = 0;   // L2 prefetch distance in elements (AXG_PREFETCH_AHEAD waves), 0 = off
@@ -140,6 +141,7 @@ class Engine final : public EngineBase {
     };
     struct FluidBucket {
         int is3d, cls, team, tpc, nr_max, n, prt = 0;
+        int part = 0;
         DBuf<T> xpool, trig;
         DBuf<int64_t> xoff;
         DBuf<uint8_t> x3d;
@@ -233,6 +235,11 @@ public:
         launch_sources();
     }
     void compute_stiffness() override { need(); launch_stiffness(); }
+    void compute_stiffness_part(int part) override {
+        need();
+        if (part < 0 || part > 1) throw Error(AXG_E_ARG, "axg_compute_stiffness_part || part must be 0 or 1.");
+        launch_stiffness(part);
+    }
     void bc_before() override { need(); launch_clayton(); launch_coupling(); }
     void point_stage(int mask) override { need(); launch_points(mask); }
     void record(int tstep) override {
@@ -1141,7 +1148,7 @@ private:
         // deterministic assembly: elements coloured so that no two of one colour share a point,
         // one bucket per colour, the buckets launched in turn
         const std::vector<int> colour = element_colours(h.pts, h.count, sp_.n);
-        std::map<std::tuple<int, int, int, int, int, int, int>, std::vector<int>> groups;
+        std::map<std::tuple<int, int, int, int, int, int, int, int>, std::vector<int>> groups;
         for (int e = 0; e < h.count; e++) {
             int att = h.att.size() ? h.att[e] : ATT_NONE;
             int is3d = h.is3d.size() ? h.is3d[e] : 0;
@@ -1151,13 +1158,14 @@ private:
             if (h.rheo[e] == RHEO_ISO && !prt) rtz = 0;
             if (att != ATT_NONE && cfg_.nsls <= 0)
                 throw Error(AXG_E_ARG, "Attenuation::checkCompatibility || nsls must be > 0.");
-            groups[{h.rheo[e], att, is3d, rtz, cfg_.plain ? 0 : nr_class(h.nr[e]), prt, colour[e]}].push_back(e);
+            const int part = h.part.size() == (size_t)h.count ? h.part[e] : 0;
+            groups[{h.rheo[e], att, is3d, rtz, cfg_.plain ? 0 : nr_class(h.nr[e]), prt, colour[e], part}].push_back(e);
         }
         int64_t state_total = 0;
         std::vector<std::vector<int64_t>> state_offs;
         for (auto &kv : groups) {
             auto b = std::make_unique<SolidBucket>();
-            std::tie(b->rheo, b->att, b->is3d, b->rtz, b->cls, b->prt, std::ignore) = kv.first;
+            std::tie(b->rheo, b->att, b->is3d, b->rtz, b->cls, b->prt, std::ignore, b->part) = kv.first;
             std::vector<T> xpool;
             std::vector<int64_t> xoff;
             std::vector<uint8_t> x3d;
@@ -1434,14 +1442,16 @@ private:
         std::vector<int> prt_of(h.count, -1);
         for (int i = 0; i < hp.count; i++) prt_of[hp.elem[i]] = i;
         const std::vector<int> colour = element_colours(h.pts, h.count, fp_.n);
-        std::map<std::tuple<int, int, int, int>, std::vector<int>> groups;
+        std::map<std::tuple<int, int, int, int, int>, std::vector<int>> groups;
         for (int e = 0; e < h.count; e++) {
             const int mode = prt_of[e] < 0 ? 0 : (hp.theta.empty() ? 1 : 2);
-            groups[{h.is3d.size() ? h.is3d[e] : 0, cfg_.plain ? 0 : nr_class(h.nr[e]), mode, colour[e]}].push_back(e);
+            const int part = h.part.size() == (size_t)h.count ? h.part[e] : 0;
+            groups[{h.is3d.size() ? h.is3d[e] : 0, cfg_.plain ? 0 : nr_class(h.nr[e]), mode, colour[e], part}]
+                .push_back(e);
         }
         for (auto &kv : groups) {
             auto b = std::make_unique<FluidBucket>();
-            std::tie(b->is3d, b->cls, b->prt, std::ignore) = kv.first;
+            std::tie(b->is3d, b->cls, b->prt, std::ignore, b->part) = kv.first;
             std::vector<T> xpool, trig;
             std::vector<int64_t> xoff;
             std::vector<uint8_t> x3d;
@@ -1953,11 +1963,13 @@ private:
         post_launch();
     }
 
-    void launch_stiffness() {
+    // every bucket (part < 0) or the buckets of one element part
+    void launch_stiffness(int part = -1) {
         if (timing_) AXG_CUDA(cudaEventRecord(ev0_, stream_));
-        for (auto &bp : sb_) launch_solid_bucket(*bp);
+        for (auto &bp : sb_)
+            if (part < 0 || bp->part == part) launch_solid_bucket(*bp);
         if (timing_) AXG_CUDA(cudaEventRecord(ev1_, stream_));
-        launch_fluid();
+        launch_fluid(part);
     }
 
     void launch_solid_bucket(SolidBucket &b) {
@@ -1999,9 +2011,10 @@ private:
         post_launch();
     }
 
-    void launch_fluid() {
+    void launch_fluid(int part = -1) {
         for (auto &bp : fb_) {
             FluidBucket &b = *bp;
+            if (part >= 0 && b.part != part) continue;
             FluidArgs<T> a;
             a.n_elem = b.n; a.nr = b.nr.p; a.pts = b.pts.p; a.axial = b.axial.p; a.geom = b.geom.p;
             a.K = b.K.p; a.K_off = b.K_off.p; a.pt_off = fp_.off.p; a.pt_nu = fp_.nu.p;

@@ -88,6 +88,8 @@ class Model:
     se_att: Optional[np.ndarray] = None
     se_att_off: Optional[np.ndarray] = None
     se_att_moduli: Optional[np.ndarray] = None
+    se_part: Optional[np.ndarray] = None          # (ne,) 0 / 1 element parts (overlapped exchange)
+    fe_part: Optional[np.ndarray] = None
     se_rtz: Optional[np.ndarray] = None
     se_theta: Optional[np.ndarray] = None         # (ne, 25)
     # fluid elements

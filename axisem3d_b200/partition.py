@@ -114,9 +114,15 @@ def _slice_pool(pool, off, sizes, sel):
     return (np.concatenate(parts) if parts else np.zeros(0, np.asarray(pool).dtype)), np.array(offs, np.int64)
 
 
-def split(model, se_part, fe_part, rank):
+def split(model, se_part, fe_part, rank, overlap=False):
     """The sub-model of one rank, with the maps to the global numbering in `sub.meta['global']`
-    (solid / fluid points, solid / fluid elements, stations)."""
+    (solid / fluid points, solid / fluid elements, stations).
+
+    overlap: the sub-model of a rank that hides the exchange behind element work. Its elements
+    carry parts (`se_part` / `fe_part`: 0 for the elements that touch a point another rank
+    holds, 1 for the rest), and the Clayton conditions of a shared point sit on every copy,
+    since they are then added after the exchange (each copy adds the whole term to the
+    assembled sum) instead of once before it."""
     for key in _UNSUPPORTED:
         if getattr(model, key, None):
             raise NotImplementedError("partition.split || %s is not partitioned" % key)
@@ -231,7 +237,7 @@ def split(model, se_part, fe_part, rank):
         cl = getattr(model, key)
         if cl:
             pt = np.asarray(cl["point"])
-            keep = np.array([lmap[p] >= 0 and holders[p][0] == rank for p in pt], bool)
+            keep = np.array([lmap[p] >= 0 and (overlap or holders[p][0] == rank) for p in pt], bool)
             d = {k: np.asarray(v)[keep] for k, v in cl.items()}
             d["point"] = lmap[pt[keep]].astype(np.int32)
             setattr(sub, key, d if len(d["point"]) else None)
@@ -242,6 +248,14 @@ def split(model, se_part, fe_part, rank):
             keep = lmap[pt] >= 0
             setattr(sub, key, (lmap[pt[keep]].astype(np.int32), g[keep]) if np.any(keep) else None)
 
+    if overlap:
+        shared_s = np.array([len(h) > 1 for h in sranks], bool)
+        sub.se_part = np.where(shared_s[np.asarray(model.se_pts)[se]].any(axis=1), 0, 1).astype(np.uint8) \
+            if len(se) else np.zeros(0, np.uint8)
+        if model.n_fluid_elements:
+            shared_f = np.array([len(h) > 1 for h in franks], bool)
+            sub.fe_part = np.where(shared_f[np.asarray(model.fe_pts)[fe]].any(axis=1), 0, 1).astype(np.uint8) \
+                if len(fe) else np.zeros(0, np.uint8)
     sub.meta = dict(model.meta, rank=int(rank),
                     **{"global": {"solid_points": sp_glob, "fluid_points": fp_glob, "solid_elements": se,
                                   "fluid_elements": fe, "stations": st_keep}})
@@ -296,18 +310,21 @@ class PartitionedRun:
     newmark_update, and get_field / set_field; with gather_stiffness / scatter_add_stiffness
     (the engine) the buffers stay on the device."""
 
-    def __init__(self, model, make_solver, rank=None, nparts=None, device=None):
+    def __init__(self, model, make_solver, rank=None, nparts=None, device=None, overlap=False):
         import torch
         import torch.distributed as dist
         self.dist = dist
         self.rank = dist.get_rank() if rank is None else rank
         self.nparts = dist.get_world_size() if nparts is None else nparts
         self.se_part, self.fe_part = partition(model, self.nparts)
-        self.sub = split(model, self.se_part, self.fe_part, self.rank)
+        self.overlap = bool(overlap)
+        self.sub = split(model, self.se_part, self.fe_part, self.rank, overlap=self.overlap)
         self._nr_global = (np.asarray(model.sp_nr), np.asarray(model.fp_nr))
         self.plan = exchange_plan(model, self.se_part, self.fe_part, self.nparts)[self.rank]
         self.solver = make_solver(self.sub)
         self.device_path = hasattr(self.solver, "gather_stiffness") and device is not None
+        if self.overlap and not (self.device_path and hasattr(self.solver, "compute_stiffness_part")):
+            raise ValueError("PartitionedRun || overlap needs the engine's device path")
         self.device = device
         self.torch = torch
         self._dev = {}
@@ -336,19 +353,7 @@ class PartitionedRun:
         ops, recv = [], []
         if self.device_path:
             with torch.cuda.stream(self.stream):
-                for other in sorted(self.plan):
-                    for solid, sl, sbuf, rbuf in self._dev[other]:
-                        if len(sl) == 0:
-                            continue
-                        self.solver.gather_stiffness(sl.data_ptr(), len(sl), sbuf.data_ptr(), solid)
-                        ops.append(dist.P2POp(dist.isend, torch.view_as_real(sbuf), other))
-                        ops.append(dist.P2POp(dist.irecv, torch.view_as_real(rbuf), other))
-                        recv.append((solid, sl, rbuf))
-                if ops:
-                    for req in dist.batch_isend_irecv(ops):
-                        req.wait()
-                for solid, sl, rbuf in recv:
-                    self.solver.scatter_add_stiffness(sl.data_ptr(), len(sl), rbuf.data_ptr(), solid)
+                self._exchange_finish(*self._exchange_start())
             return
         fields = {}
         for solid in (True, False):
@@ -372,9 +377,48 @@ class PartitionedRun:
         for solid, f in fields.items():
             self.solver.set_field(f, "stiff", solid=solid)
 
+    def _exchange_start(self):
+        """Gather the shared points' stiffness and queue the transfers (device path, with the
+        run's stream current); returns what _exchange_finish waits on and adds."""
+        dist, torch = self.dist, self.torch
+        ops, recv = [], []
+        for other in sorted(self.plan):
+            for solid, sl, sbuf, rbuf in self._dev[other]:
+                if len(sl) == 0:
+                    continue
+                self.solver.gather_stiffness(sl.data_ptr(), len(sl), sbuf.data_ptr(), solid)
+                ops.append(dist.P2POp(dist.isend, torch.view_as_real(sbuf), other))
+                ops.append(dist.P2POp(dist.irecv, torch.view_as_real(rbuf), other))
+                recv.append((solid, sl, rbuf))
+        reqs = dist.batch_isend_irecv(ops) if ops else []
+        return reqs, recv
+
+    def _exchange_finish(self, reqs, recv):
+        for req in reqs:
+            req.wait()
+        for solid, sl, rbuf in recv:
+            self.solver.scatter_add_stiffness(sl.data_ptr(), len(sl), rbuf.data_ptr(), solid)
+
     def step(self, tstep):
-        """One Newmark step in the order of NewmarkTimeScheme::solve."""
+        """One Newmark step in the order of NewmarkTimeScheme::solve. With overlap, the
+        elements that touch a shared point go first, the transfers run while the others
+        compute, and the boundary conditions before assembly follow the exchange (the
+        solid-fluid pairs live on one rank; the Clayton terms of shared points are on every
+        copy)."""
         s = self.solver
+        if self.overlap:
+            with self.torch.cuda.stream(self.stream):
+                s.apply_sources(tstep)
+                s.compute_stiffness_part(0)
+                pending = self._exchange_start()
+                s.compute_stiffness_part(1)
+                self._exchange_finish(*pending)
+                s.apply_bc_before_assembly()
+            s.record_stations(tstep)
+            s.apply_bc_after_assembly()
+            s.stiff_to_accel()
+            s.newmark_update()
+            return
         s.apply_sources(tstep)
         s.compute_stiffness()
         s.apply_bc_before_assembly()

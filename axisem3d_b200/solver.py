@@ -117,6 +117,12 @@ class Solver:
                                                     mo.ctypes.data_as(L.P_f64), th.ctypes.data_as(L.P_f64)))
         for cls, team in (team_sizes or {}).items():
             self._check(self.lib.axg_set_team_size(h, int(cls), int(team)))
+        sp_, fp_ = getattr(model, "se_part", None), getattr(model, "fe_part", None)
+        if sp_ is not None or fp_ is not None:
+            a = np.ascontiguousarray(sp_, np.uint8) if sp_ is not None else None
+            b = np.ascontiguousarray(fp_, np.uint8) if fp_ is not None else None
+            self._check(self.lib.axg_set_element_parts(h, a.ctypes.data if a is not None else None,
+                                                       b.ctypes.data if b is not None else None))
         self._check(self.lib.axg_finalize(h))
 
     # ------------------------------------------------------------------ util ---
@@ -177,6 +183,10 @@ class Solver:
     def complex_dtype(self):
         """numpy dtype of the stiffness field on the device."""
         return np.complex128 if self.precision == "fp64" else np.complex64
+
+    def compute_stiffness_part(self, part):
+        """Domain::computeStiffness for the elements of one part (model.se_part / fe_part)."""
+        self._check(self.lib.axg_compute_stiffness_part(self.h, int(part)))
 
     def apply_bc_before_assembly(self):
         self._check(self.lib.axg_apply_bc_before_assembly(self.h))

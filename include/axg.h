@@ -502,6 +502,16 @@ int  axg_set_team_size(axg_solver *h, int32_t nr_class, int32_t team);
 int  axg_gather_stiffness(axg_solver *h, int32_t solid, int64_t n, const int64_t *slots, void *buf);
 /* stiff[slots[i]] += buf[i]; the slots of one call must be distinct */
 int  axg_scatter_add_stiffness(axg_solver *h, int32_t solid, int64_t n, const int64_t *slots, const void *buf);
+/* Element parts, so that a rank can hide the exchange behind element work: the elements that
+   touch a shared point (part 0) first, the gather and the transfer, then the others (part 1)
+   while the transfer runs. The reference overlaps its exchange with output and scanning only
+   (NewmarkTimeScheme.cpp:57-83); this split has no counterpart there. part: 0 or 1 per solid /
+   fluid element (NULL = all 0), after the element setters and before axg_finalize; no bucket
+   mixes parts. */
+int  axg_set_element_parts(axg_solver *h, const uint8_t *solid_part, const uint8_t *fluid_part);
+/* Domain::computeStiffness (Domain.cpp:298-308) for the elements of one part (0 or 1): the two
+   parts together add what axg_compute_stiffness adds */
+int  axg_compute_stiffness_part(axg_solver *h, int32_t part);
 
 /* ---- stiffness of a caller's field with no device allocation ----
    No counterpart in the reference. Adds -K x to f for every element of a finalized handle,

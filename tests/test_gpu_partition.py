@@ -167,20 +167,27 @@ class _ThreadTransport:
         return [_Done()]
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("name", ["box_abc", "shell_fluid"])
-def test_partitioned_run_device_path(built, name):
+def test_partitioned_run_device_path(built, name, overlap):
     """PartitionedRun's device path (the engine's gather / scatter-add on the run's own stream,
     buffers handed over by the transport between the boundary conditions before and after
     assembly) with two ranks as two threads of this process, against one handle holding the
-    whole mesh: FP64 <= 1e-12. NCCL itself is not exercised (one GPU); the transport stands in
-    for its point-to-point calls."""
+    whole mesh: FP64 <= 1e-12. With overlap, the elements at shared points first, the transfer
+    queued before the other elements (axg_compute_stiffness_part), the Clayton terms of shared
+    points on every copy after the exchange. NCCL itself is not exercised (one GPU); the
+    transport stands in for its point-to-point calls."""
     import threading
     import torch
     from axisem3d_b200 import partition as P
     from axisem3d_b200.solver import Solver
     m, nsteps, _ = _model(name)
-    runs = [P.PartitionedRun(m, lambda sub: Solver(sub, "fp64"), rank=r, nparts=2, device="cuda")
-            for r in range(2)]
+    runs = [P.PartitionedRun(m, lambda sub: Solver(sub, "fp64"), rank=r, nparts=2, device="cuda",
+                             overlap=overlap) for r in range(2)]
+    if overlap:
+        for run in runs:
+            part = np.asarray(run.sub.se_part)
+            assert 0 < int(part.sum()) < len(part)
     box, cv = {}, threading.Condition()
     for r, run in enumerate(runs):
         assert run.device_path

@@ -158,3 +158,28 @@ def test_partitioned_run_equals_single_domain(built, name, world, nsteps):
             if len(st):
                 got[:, st, :] = seis
         assert np.linalg.norm(got - ref_seis) / np.linalg.norm(ref_seis) <= 1e-12
+
+
+def test_overlap_split_parts_and_clayton_copies():
+    """split(overlap=True): part 0 = the elements touching a point another rank holds, part 1
+    = the rest; the Clayton conditions of shared points on every copy (added after the
+    exchange), the others unchanged."""
+    from axisem3d_b200 import partition as P
+    m = _model("box_abc")
+    se, fe = P.partition(m, 2)
+    holders = P._point_ranks(m.se_pts, se, len(m.sp_nr))
+    plain = [P.split(m, se, fe, r) for r in range(2)]
+    over = [P.split(m, se, fe, r, overlap=True) for r in range(2)]
+    ncl_plain = ncl_over = 0
+    for r in range(2):
+        g = over[r].meta["global"]
+        pts = np.asarray(m.se_pts)[g["solid_elements"]]
+        shared = np.array([[len(holders[p]) > 1 for p in row] for row in pts])
+        assert np.array_equal(np.asarray(over[r].se_part), np.where(shared.any(axis=1), 0, 1))
+        ncl_plain += len(plain[r].cl_solid["point"]) if plain[r].cl_solid else 0
+        ncl_over += len(over[r].cl_solid["point"]) if over[r].cl_solid else 0
+        assert plain[r].se_part is None
+    pt = np.asarray(m.cl_solid["point"])
+    nshared = sum(len(holders[p]) - 1 for p in pt)
+    assert nshared > 0
+    assert ncl_plain == len(pt) and ncl_over == len(pt) + nshared
