@@ -556,15 +556,6 @@ __global__ void adjoint_mass_slices_kernel(int npoints, const int *off, const in
     }
 }
 
-// ubar_n = ubar_{n+1} + (-K g), -K g being in `kg` (which is then cleared)
-template <class T>
-__global__ void adjoint_combine_kernel(int nvals, cx_t<T> *ubar, cx_t<T> *kg) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nvals) return;
-    const cx_t<T> k = kg[q];
-    ubar[q] = mk<T>(ubar[q].x + k.x, ubar[q].y + k.y);
-    kg[q] = mk<T>(0, 0);
-}
 
 // R^T r_n: the seismogram cotangent of step n injected into ubar
 template <class T>

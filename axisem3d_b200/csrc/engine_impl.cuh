@@ -533,9 +533,9 @@ public:
                                      stream_));
         }
         if (adj_astate_n_ > 0) adj_astate_.zero(stream_);
-        DBuf<C> ub, vb, ab, g, kg, seg_u, seg_a;
-        ub.alloc(nf); vb.alloc(nf); ab.alloc(nf); g.alloc(nf); kg.alloc(nf);
-        ub.zero(stream_); vb.zero(stream_); ab.zero(stream_); kg.zero(stream_);
+        DBuf<C> ub, vb, ab, g, seg_u, seg_a;
+        ub.alloc(nf); vb.alloc(nf); ab.alloc(nf); g.alloc(nf);
+        ub.zero(stream_); vb.zero(stream_); ab.zero(stream_);
         seg_u.alloc(nf * ck_interval_); seg_a.alloc(nf * ck_interval_);
         adj_grad_.zero(stream_);
         adj_gmass_.zero(stream_);
@@ -553,7 +553,6 @@ public:
                                      stream_));
         }
         const int threads = 256;
-        const int vblocks = (int)((nf + threads - 1) / threads);
         for (int c = nck - 1; c >= 0; c--) {
             const int len = std::min(ck_interval_, ck_n_ - c * ck_interval_);
             copy_fields_in(c);
@@ -596,7 +595,9 @@ public:
                 aa.n_elem = model_.se.count; aa.nr = e_nr_.p; aa.pts = e_pts_.p; aa.axial = e_axial_.p;
                 aa.geom = adj_geom_.p; aa.mod = adj_mod_.p; aa.mod_off = adj_mod_off_.p;
                 aa.pt_off = sp_.off.p; aa.pt_nu = sp_.nu.p; aa.u = seg_u.p + nf * i; aa.g = g.p;
-                aa.out = kg.p; aa.ifact = adj_ifact_.p; aa.grad = adj_grad_.p; aa.gmat = gmat_.p;
+                // -K g goes straight into ubar: the point kernel above has read ubar of step n+1,
+                // and ubar_n = ubar + (-K g) + R^T r_n is a sum
+                aa.out = ub.p; aa.ifact = adj_ifact_.p; aa.grad = adj_grad_.p; aa.gmat = gmat_.p;
                 aa.grad3 = adj_slices_ ? adj_grad3_.p : nullptr;
                 aa.grad3_off = adj_grad3_off_.p;
                 aa.tw = adj_tw_.p;
@@ -615,8 +616,6 @@ public:
                 if (adj_slices_) adjoint_stiffness_kernel<T, true><<<grid, 128, smem, stream_>>>(aa, nu_max);
                 else if (adj_generic_) adjoint_stiffness_kernel<T, false, true><<<grid, 128, smem, stream_>>>(aa, nu_max);
                 else adjoint_stiffness_kernel<T, false><<<grid, 128, smem, stream_>>>(aa, nu_max);
-                post_launch();
-                adjoint_combine_kernel<T><<<vblocks, threads, 0, stream_>>>((int)nf, ub.p, kg.p);
                 post_launch();
                 if (st_n_ && n % st_interval_ == 0) {
                     const int rec = n / st_interval_;
