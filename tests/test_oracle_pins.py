@@ -423,3 +423,68 @@ def test_identity_fluid_prt_equals_no_prt(built, three_d):
         o.compute_stiffness()
         out.append(o.get_field("stiff", solid=False))
     assert np.linalg.norm(out[1] - out[0]) <= 1e-14 * np.linalg.norm(out[0])
+
+
+@pytest.mark.parametrize("nm", ["GLL", "GLJ"])
+def test_reference_tables_are_exact_on_polynomials(nm):
+    """The reference's own 12-decimal tables (spectrals.hpp:73-102, as text in the golden file):
+    G(j, i) = l_j'(x_i) differentiates every polynomial of degree <= 4 at the nodes, and the
+    weights integrate degree <= 7 exactly, against dx (GLL) or (1 + x) dx (GLJ, the axial
+    direction), to the tables' rounding."""
+    t = _golden()
+    x, w = np.asarray(t["p" + nm]), np.asarray(t["w" + nm])
+    G = np.asarray(t["g" + nm]).reshape(5, 5)
+    for k in range(5):
+        dp = k * x ** (k - 1) if k else np.zeros_like(x)
+        assert np.abs((x ** k) @ G - dp).max() < 1e-10, k
+    for k in range(8):
+        exact = (1 - (-1) ** (k + 1)) / (k + 1)
+        if nm == "GLJ":
+            exact += (1 - (-1) ** (k + 2)) / (k + 2)
+        assert abs(w @ x ** k - exact) < 1e-11, k
+
+
+@pytest.mark.parametrize("rheology", ["iso", "tiso"])
+def test_oracle_patch_test_uniform_strain(built, rheology):
+    """Patch test of gradient, stress and quadrature together: the Cartesian-linear field
+    u_x = a x, u_y = a y, u_z = b z (in the mesh's frame u_s = a s, u_z = b z, Fourier mode 0)
+    has uniform strain, so in a homogeneous isotropic or z-axis TI medium the stress is
+    constant and divergence-free and the assembled force vanishes at every point off the
+    outer boundary of the box, the axis points included; the boundary points carry the
+    traction."""
+    import oracle as O
+    from axisem3d_b200 import _lib as L
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=6, nz=5, nr=5)
+    ne = m.n_solid_elements
+    if rheology == "tiso":
+        lam, mu = m.se_moduli.reshape(ne, 2, 25)[0, :, 0]
+        A, Cc, F, Lm, N = (lam + 2 * mu) * 1.08, (lam + 2 * mu) * 0.95, lam * 1.1, mu * 0.9, mu * 1.05
+        m.se_rheo = np.full(ne, L.AXG_TISO, np.int32)
+        m.se_moduli = np.tile(np.repeat(np.array([A, Cc, F, Lm, N]), 25), ne)
+        m.se_mat_off = np.arange(ne, dtype=np.int64) * 125
+    o = O.Oracle(m, "fp64")
+    nu = np.asarray(m.sp_nr) // 2 + 1
+    first = np.concatenate([[0], np.cumsum(nu)[:-1]])
+    s, z = m.sp_coords[:, 0], m.sp_coords[:, 1]
+    u = np.zeros((int(nu.sum()), 3), complex)
+    u[first, 0] = 1e-3 * s
+    u[first, 2] = -2e-3 * z
+    f = _stiff(o, u.ravel()).reshape(-1, 3)[first]
+    width, height = s.max(), -z.min()
+    tol = 1e-9 * max(width, height)
+    boundary = (np.abs(s - width) < tol) | (np.abs(z) < tol) | (np.abs(z + height) < tol)
+    # on the axis mode 0 keeps its z component only (AxialBoundary::apply, AxialBoundary.cpp:
+    # 21-51, after assembly): the s and phi forces there are projected out
+    f[s < tol, :2] = 0
+    fb = np.linalg.norm(f[boundary])
+    assert fb > 0 and np.any(~boundary & (s < tol))        # axis points among the interior
+    assert np.linalg.norm(f[~boundary]) <= 1e-10 * fb, np.linalg.norm(f[~boundary]) / fb
+    # the other modes stay zero
+    assert np.linalg.norm(np.delete(_stiff(o, u.ravel()).reshape(-1, 3), first, axis=0)) == 0
+    # the same field with its z component tilted off the linear (u_z = b z + c z^2) is not a
+    # patch: the check has teeth
+    u[first, 2] += 1e-8 * z ** 2
+    f2 = _stiff(o, u.ravel()).reshape(-1, 3)[first]
+    f2[s < tol, :2] = 0
+    assert np.linalg.norm(f2[~boundary]) > 1e-6 * fb
