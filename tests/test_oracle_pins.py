@@ -444,14 +444,32 @@ def test_reference_tables_are_exact_on_polynomials(nm):
         assert abs(w @ x ** k - exact) < 1e-11, k
 
 
+def _axial_projection(f, mode):
+    """AxialBoundary::apply (AxialBoundary.cpp:21-51) on one mode of axis points' forces:
+    mode 0 keeps z; mode 1 keeps t = (f_s - i f_phi) / 2 as f_s = t, f_phi = i t; higher
+    modes vanish."""
+    f = f.copy()
+    if mode == 0:
+        f[:, :2] = 0
+    elif mode == 1:
+        t = 0.5 * (f[:, 0] - 1j * f[:, 1])
+        f[:, 0], f[:, 1], f[:, 2] = t, 1j * t, 0
+    else:
+        f[:] = 0
+    return f
+
+
+@pytest.mark.parametrize("mode", [0, 1])
 @pytest.mark.parametrize("rheology", ["iso", "tiso"])
-def test_oracle_patch_test_uniform_strain(built, rheology):
-    """Patch test of gradient, stress and quadrature together: the Cartesian-linear field
-    u_x = a x, u_y = a y, u_z = b z (in the mesh's frame u_s = a s, u_z = b z, Fourier mode 0)
-    has uniform strain, so in a homogeneous isotropic or z-axis TI medium the stress is
-    constant and divergence-free and the assembled force vanishes at every point off the
-    outer boundary of the box, the axis points included; the boundary points carry the
-    traction."""
+def test_oracle_patch_test_uniform_strain(built, rheology, mode):
+    """Patch test of gradient, stress and quadrature together: a Cartesian-linear field has
+    uniform strain, so in a homogeneous isotropic or z-axis TI medium the stress is constant
+    and divergence-free and the assembled force vanishes at every point off the outer boundary
+    of the box, the axis points included (after their axial projection); the boundary points
+    carry the traction. Mode 0: u_x = a x, u_y = a y, u_z = b z, i.e. u_s = a s, u_z = b z.
+    Mode 1 (the azimuthal derivative terms and the axis rows of the gradient): the shear
+    u_x = a z, u_z = b x, i.e. u_s = a z cos phi, u_phi = -a z sin phi, u_z = b s cos phi, whose
+    mode-1 coefficients (u = 2 Re(c e^{i phi})) are a z / 2, i a z / 2 and b s / 2."""
     import oracle as O
     from axisem3d_b200 import _lib as L
     from axisem3d_b200 import meshgen
@@ -468,23 +486,31 @@ def test_oracle_patch_test_uniform_strain(built, rheology):
     first = np.concatenate([[0], np.cumsum(nu)[:-1]])
     s, z = m.sp_coords[:, 0], m.sp_coords[:, 1]
     u = np.zeros((int(nu.sum()), 3), complex)
-    u[first, 0] = 1e-3 * s
-    u[first, 2] = -2e-3 * z
-    f = _stiff(o, u.ravel()).reshape(-1, 3)[first]
+    rows = first + mode
+    if mode == 0:
+        u[rows, 0] = 1e-3 * s
+        u[rows, 2] = -2e-3 * z
+    else:
+        u[rows, 0] = 0.5e-3 * z
+        u[rows, 1] = 0.5e-3j * z
+        u[rows, 2] = 0.7e-3 * s
     width, height = s.max(), -z.min()
     tol = 1e-9 * max(width, height)
+    axis = s < tol
     boundary = (np.abs(s - width) < tol) | (np.abs(z) < tol) | (np.abs(z + height) < tol)
-    # on the axis mode 0 keeps its z component only (AxialBoundary::apply, AxialBoundary.cpp:
-    # 21-51, after assembly): the s and phi forces there are projected out
-    f[s < tol, :2] = 0
+
+    def force(u):
+        f = _stiff(o, u.ravel()).reshape(-1, 3)
+        g = f[rows].copy()
+        g[axis] = _axial_projection(g[axis], mode)
+        return f, g
+
+    f_all, f = force(u)
     fb = np.linalg.norm(f[boundary])
-    assert fb > 0 and np.any(~boundary & (s < tol))        # axis points among the interior
+    assert fb > 0 and np.any(~boundary & axis)        # axis points among the interior
     assert np.linalg.norm(f[~boundary]) <= 1e-10 * fb, np.linalg.norm(f[~boundary]) / fb
-    # the other modes stay zero
-    assert np.linalg.norm(np.delete(_stiff(o, u.ravel()).reshape(-1, 3), first, axis=0)) == 0
-    # the same field with its z component tilted off the linear (u_z = b z + c z^2) is not a
-    # patch: the check has teeth
-    u[first, 2] += 1e-8 * z ** 2
-    f2 = _stiff(o, u.ravel()).reshape(-1, 3)[first]
-    f2[s < tol, :2] = 0
-    assert np.linalg.norm(f2[~boundary]) > 1e-6 * fb
+    # the other modes stay zero (phi-constant medium: the modes decouple)
+    assert np.linalg.norm(np.delete(f_all, rows, axis=0)) == 0
+    # the same field with a quadratic term in z is not a patch: the check has teeth
+    u[rows, 2] += 1e-8 * z ** 2
+    assert np.linalg.norm(force(u)[1][~boundary]) > 1e-6 * fb
