@@ -1084,6 +1084,7 @@ def spherical_model(n_theta=96, n_solid_layers=24, n_fluid_layers=2, r_cmb=3480e
     m.fp_nr = pnr[fp_used].astype(np.int32)
     m.fp_mass = fmass
     m.fp_axial = (coords[fp_used, 0] == 0.0).astype(np.uint8)
+    m.fp_coords = coords[fp_used]
     m.fp_surface = np.zeros(nfp, np.uint8)
     m.se_nr = enr[sel_s]
     m.se_pts = sid[pts[sel_s]].astype(np.int32)
