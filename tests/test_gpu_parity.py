@@ -821,3 +821,37 @@ def test_deterministic_assembly_is_bitwise_reproducible(built, precision):
         (d1, k1), (d2, k2), (d3, k3) = runs
         assert np.array_equal(d1, d2) and np.array_equal(k1, k2)
         assert rel(d1, d3) <= 1e-5 and rel(k1, k3) <= 1e-5
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 1e-5), ("mixed", 1e-5)])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_engine_patch_test(built, mode, precision, tol):
+    """The patch test on the CUDA path itself, not only through the oracle: a Cartesian-linear
+    (uniform-strain) field in a homogeneous medium leaves no force off the box's outer boundary,
+    axis points included after their axial projection. Mode 0: u_s = a s, u_z = b z; mode 1:
+    the shear u_x = a z, u_z = b x (coefficients a z / 2, i a z / 2, b s / 2)."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    from test_oracle_pins import _axial_projection
+    m = meshgen.cartesian_model(nx=6, nz=5, nr=5)
+    nu = np.asarray(m.sp_nr) // 2 + 1
+    first = np.concatenate([[0], np.cumsum(nu)[:-1]])
+    rows = first + mode
+    s, z = m.sp_coords[:, 0], m.sp_coords[:, 1]
+    u = np.zeros((int(nu.sum()), 3), complex)
+    if mode == 0:
+        u[rows, 0], u[rows, 2] = 1e-3 * s, -2e-3 * z
+    else:
+        u[rows, 0], u[rows, 1], u[rows, 2] = 0.5e-3 * z, 0.5e-3j * z, 0.7e-3 * s
+    with Solver(m, precision) as h:
+        h.set_field(u.ravel(), "displ")
+        h.compute_stiffness()
+        f = h.get_field("stiff").reshape(-1, 3)[rows]
+    width, height = s.max(), -z.min()
+    eps = 1e-9 * max(width, height)
+    axis = s < eps
+    boundary = (np.abs(s - width) < eps) | (np.abs(z) < eps) | (np.abs(z + height) < eps)
+    f[axis] = _axial_projection(f[axis], mode)
+    fb = np.linalg.norm(f[boundary])
+    assert fb > 0 and np.any(~boundary & axis)
+    assert np.linalg.norm(f[~boundary]) <= tol * fb, np.linalg.norm(f[~boundary]) / fb
