@@ -402,7 +402,11 @@ int  axg_current_step(const axg_solver *h, int32_t *tstep);
         elements, RTZ frames included, elastic or with FULL / CG4 attenuation, no fluid; no
         counterpart in the reference, which has no adjoint) ---- */
 /* nsteps forward steps from the current state, storing the state every
-   checkpoint_interval steps on the device for axg_adjoint_run */
+   checkpoint_interval steps on the device for axg_adjoint_run. A checkpoint holds the point
+   displacement, velocity and acceleration and, with attenuation, the SLS memory variables
+   ((nsls + 1) x 6 x npa x nu complex values per attenuating element, npa = 25 FULL / 4 CG4),
+   so attenuating models may want a longer interval; axg_adjoint_run also takes two segment
+   buffers of checkpoint_interval fields each. */
 int  axg_forward_checkpointed(axg_solver *h, int32_t nsteps, int32_t checkpoint_interval);
 /* time-reversed discrete adjoint of the last axg_forward_checkpointed run, each
    segment recomputed from its checkpoint. seis_adjoint = dJ/d(seismograms),
