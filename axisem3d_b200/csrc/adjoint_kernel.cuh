@@ -370,7 +370,10 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
                 g3[(size_t)(nr + k) * 25 + q] -= f * gm;
             }
         }
-        // quadrature of the stress of g (computeQuad6): pass 1, X/Y in place, A terms in Ug
+        // quadrature of the stress of g (computeQuad6): pass 1, X/Y in place, A terms in Ug.
+        // out == NULL: sensitivities only (models with 3-D elements take -K^T g from the
+        // forward kernels)
+        if (a.out) {
         const T *dsdxii_if = sGeo + 125, *dsdeta_if = sGeo + 150, *dzdxii_if = sGeo + 175,
                 *dzdeta_if = sGeo + 200, *invs_if = sGeo + 225;
         for (int i = threadIdx.x; i < nu * 25; i += blockDim.x) {
@@ -425,6 +428,7 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
                 if (al < sNu[q]) atomic_add_cx(a.out + (size_t)(sOff[q] + al) * 3 + c, mk<T>(-fc.x, -fc.y));
             }
         }
+        }
         __syncthreads();
         // grad (each element belongs to one CTA per launch, so no race): -ifact * products
         if constexpr (GENERIC) {
@@ -443,6 +447,27 @@ __global__ void __launch_bounds__(256) adjoint_stiffness_kernel(const AdjointArg
                 gr[25 + q] -= f * sGm[q];
             }
         }
+    }
+}
+
+// Models with 3-D (per-slice) moduli. The element's slice transforms make its stiffness
+// self-adjoint in the azimuthally weighted product <a, W b> (w = 1 for mode 0, 2 for the other
+// modes, 4 for the Nyquist mode of an even nr, where C2R doubles and R2C halves it), not in the
+// plain one, so K^T = W K W^-1: stage 0 forms gw = W^-1 g for the forward kernels, which add
+// -K gw to kt; stage 1 adds W kt to ubar and clears kt.
+template <class T>
+__global__ void adjoint_weight_kernel(int nvals, const int *mode_pt, const int *off, const int *nr,
+                                      const cx_t<T> *g, cx_t<T> *gw, cx_t<T> *ubar, cx_t<T> *kt, int stage) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nvals) return;
+    const int m = q / 3, p = mode_pt[m], al = m - off[p], n = nr[p];
+    const T w = al == 0 ? (T)1 : ((n & 1) == 0 && 2 * al == n) ? (T)4 : (T)2;
+    if (stage == 0) {
+        gw[q] = mk<T>(g[q].x / w, g[q].y / w);
+    } else {
+        const cx_t<T> k = kt[q];
+        ubar[q] = mk<T>(ubar[q].x + w * k.x, ubar[q].y + w * k.y);
+        kt[q] = mk<T>(0, 0);
     }
 }
 

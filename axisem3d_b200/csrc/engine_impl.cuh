@@ -533,9 +533,13 @@ public:
                                      stream_));
         }
         if (adj_astate_n_ > 0) adj_astate_.zero(stream_);
-        DBuf<C> ub, vb, ab, g, seg_u, seg_a;
+        DBuf<C> ub, vb, ab, g, seg_u, seg_a, gw, kt;
         ub.alloc(nf); vb.alloc(nf); ab.alloc(nf); g.alloc(nf);
         ub.zero(stream_); vb.zero(stream_); ab.zero(stream_);
+        if (adj_3d_) {   // W^-1 g and the forward kernels' -K W^-1 g
+            gw.alloc(nf); kt.alloc(nf);
+            kt.zero(stream_);
+        }
         seg_u.alloc(nf * ck_interval_); seg_a.alloc(nf * ck_interval_);
         adj_grad_.zero(stream_);
         adj_gmass_.zero(stream_);
@@ -596,8 +600,39 @@ public:
                 aa.geom = adj_geom_.p; aa.mod = adj_mod_.p; aa.mod_off = adj_mod_off_.p;
                 aa.pt_off = sp_.off.p; aa.pt_nu = sp_.nu.p; aa.u = seg_u.p + nf * i; aa.g = g.p;
                 // -K g goes straight into ubar: the point kernel above has read ubar of step n+1,
-                // and ubar_n = ubar + (-K g) + R^T r_n is a sum
-                aa.out = ub.p; aa.ifact = adj_ifact_.p; aa.grad = adj_grad_.p; aa.gmat = gmat_.p;
+                // and ubar_n = ubar + (-K g) + R^T r_n is a sum. With 3-D elements -K^T g =
+                // -W K W^-1 g comes from the forward kernels and the adjoint kernel adds only
+                // the sensitivities.
+                if (adj_3d_) {
+                    const int wblocks = (int)((nf + 255) / 256);
+                    adjoint_weight_kernel<T><<<wblocks, 256, 0, stream_>>>((int)nf, sp_.mode_pt.p, sp_.off.p,
+                                                                          sp_.nr.p, g.p, gw.p, ub.p, kt.p, 0);
+                    post_launch();
+                    for (auto &bp : sb_) {
+                        SolidBucket &b = *bp;
+                        SolidArgs<T, AT> sa;
+                        sa.n_elem = b.n; sa.nr = b.nr.p; sa.pts = b.pts.p; sa.axial = b.axial.p;
+                        sa.geom = b.geom.p; sa.trig = b.trig.p; sa.mod = b.mod.p; sa.mod_off = b.mod_off.p;
+                        sa.attmod = b.attmod.p; sa.att_off = b.att_off.p; sa.state = state_.p;
+                        sa.state_off = b.state_off.p; sa.pt_off = sp_.off.p; sa.pt_nu = sp_.nu.p;
+                        sa.displ = gw.p;
+                        sa.stiff = kt.p; sa.tw = tw_.p; sa.tw_off = tw_off_.p;
+                        sa.nsls = cfg_.nsls;
+                        for (int l = 0; l < 8; l++) {
+                            sa.alpha[l] = (AT)cfg_.att_alpha[l]; sa.beta[l] = (AT)cfg_.att_beta[l];
+                            sa.gamma[l] = (AT)cfg_.att_gamma[l];
+                        }
+                        sa.gmat = gmat_.p;
+                        sa.nwave = 1;
+                        sa.fstride = nf;
+                        sa.sstride = (size_t)state_wave_;
+                        launch_solid_args(b, sa);
+                    }
+                    adjoint_weight_kernel<T><<<wblocks, 256, 0, stream_>>>((int)nf, sp_.mode_pt.p, sp_.off.p,
+                                                                          sp_.nr.p, g.p, gw.p, ub.p, kt.p, 1);
+                    post_launch();
+                }
+                aa.out = adj_3d_ ? nullptr : ub.p; aa.ifact = adj_ifact_.p; aa.grad = adj_grad_.p; aa.gmat = gmat_.p;
                 aa.grad3 = adj_slices_ ? adj_grad3_.p : nullptr;
                 aa.grad3_off = adj_grad3_off_.p;
                 aa.tw = adj_tw_.p;
@@ -748,12 +783,33 @@ private:
         if (fp_.n > 0) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || fluid elements are not differentiated.");
         if (nwave_ != 1) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || one wavefield per handle.");
         if (model_.prt.count) throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || PRT elements are not differentiated.");
+        bool any3d = false, wide = false;
         for (int e = 0; e < h.count; e++) {
-            if (h.is3d.size() && h.is3d[e])
-                throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || needs phi-constant solid elements.");
+            const bool e3d = h.is3d.size() && h.is3d[e];
+            const bool att = h.att.size() && h.att[e] != AXG_ATT_NONE;
+            any3d |= e3d;
+            wide |= att || h.rheo[e] != RHEO_ISO;
+            if (e3d) {
+                // 3-D (per-slice) moduli: isotropic and elastic, and no Nyquist mode that the
+                // element and a point of it treat differently (where elements of different
+                // even nr share a point the reference's operator is not self-adjoint in any
+                // one weighted product)
+                if (h.rheo[e] != RHEO_ISO || att)
+                    throw Error(AXG_E_UNSUPPORTED,
+                                "axg_adjoint || 3-D elements must be isotropic and non-attenuating.");
+                for (int q = 0; q < 25; q++) {
+                    const int np_ = sp_.h_nr[h.pts[(size_t)e * 25 + q]];
+                    if (((h.nr[e] % 2) == 0 || (np_ % 2) == 0) && np_ != h.nr[e])
+                        throw Error(AXG_E_UNSUPPORTED,
+                                    "axg_adjoint || a 3-D element of even nr needs the same nr at its points.");
+                }
+            }
             if (h.rheo[e] != RHEO_ISO && h.rtz.size() && h.rtz[e] && h.theta.size() < (size_t)(e + 1) * 25)
                 throw Error(AXG_E_ARG, "axg_adjoint || RTZ element without theta.");
         }
+        if (any3d && wide)
+            throw Error(AXG_E_UNSUPPORTED,
+                        "axg_adjoint || 3-D elements do not mix with TI, 21-Cij or attenuating ones.");
         for (int p = 0; p < sp_.n; p++)
             if (model_.sp.mass_nr.size() && model_.sp.mass_nr[p] > 1)
                 throw Error(AXG_E_UNSUPPORTED, "axg_adjoint || 3-D masses are not differentiated.");
@@ -842,6 +898,7 @@ private:
         adj_nr_max_ = 1;
         adj_generic_ = false;
         adj_iso_only_ = true;
+        adj_3d_ = false;
         for (int e = 0; e < h.count; e++) {
             adj_nr_max_ = std::max(adj_nr_max_, h.nr[e]);
             for (int c = 0; c < 5; c++)
@@ -855,7 +912,16 @@ private:
             const int nm = nmod_of(h.rheo[e]);
             moff[e] = (int64_t)mod.size();
             goff[e] = gsize;
-            for (int i = 0; i < nm * 25; i++) mod.push_back((T)h.moduli[h.mat_off[e] + i]);
+            if (h.is3d.size() && h.is3d[e]) {
+                // 3-D element (isotropic): -K^T g comes from the forward kernels; the pool keeps
+                // slice 0 of lambda, mu, which only feeds the skipped quadrature
+                adj_3d_ = true;
+                for (int c = 0; c < 2; c++)
+                    for (int q = 0; q < 25; q++)
+                        mod.push_back((T)h.moduli[h.mat_off[e] + (size_t)c * h.nr[e] * 25 + q]);
+            } else {
+                for (int i = 0; i < nm * 25; i++) mod.push_back((T)h.moduli[h.mat_off[e] + i]);
+            }
             gsize += nm * 25;
             rheo[e] = h.rheo[e];
             if (h.att.size() && h.att[e] != AXG_ATT_NONE) {
@@ -2253,7 +2319,7 @@ private:
     DBuf<int64_t> adj_attmod_off_, adj_astate_off_;
     DBuf<C> adj_astate_;
     DBuf<AT> ck_state_;
-    bool adj_generic_ = false, adj_iso_only_ = true;
+    bool adj_generic_ = false, adj_iso_only_ = true, adj_3d_ = false;
 
     DBuf<T> gmat_, tw_;
     DBuf<int> tw_off_;

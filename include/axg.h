@@ -399,8 +399,10 @@ int  axg_run(axg_solver *h, int32_t nsteps, int32_t use_graph);
 int  axg_current_step(const axg_solver *h, int32_t *tstep);
 
 /* ---- differentiation (FP64 handles; phi-constant isotropic, TI or 21-Cij solid
-        elements, RTZ frames included, elastic or with FULL / CG4 attenuation, no fluid; no
-        counterpart in the reference, which has no adjoint) ---- */
+        elements, RTZ frames included, elastic or with FULL / CG4 attenuation, or isotropic
+        elastic 3-D elements with per-slice moduli (where an element or a point of it has an
+        even nr, both have the same nr); 1-D masses, no fluid; no counterpart in the
+        reference, which has no adjoint) ---- */
 /* nsteps forward steps from the current state, storing the state every
    checkpoint_interval steps on the device for axg_adjoint_run. A checkpoint holds the point
    displacement, velocity and acceleration and, with attenuation, the SLS memory variables
@@ -425,8 +427,8 @@ int  axg_adjoint_run(axg_solver *h, const double *seis_adjoint, double *grad_mod
    masses of the 3-D parameterisation, the values at the slices phi_k = 2 pi k / nr that a 3-D
    element or a Mass3D point holds (PhysicalProperty.hpp:99-120): dJ/dlambda and dJ/dmu at
    every (slice, point) of every element, dJ/dM at every slice of every solid point. The
-   linearisation point is the handle's phi-constant model; with odd nr a 3-D element there
-   equals the 1-D one, and the sum over slices is the 1-D gradient. Elastic isotropic models
+   linearisation point is the handle's model, 1-D or with 3-D isotropic moduli (its masses
+   1-D); the sum over slices is the gradient by a phi-constant change (grad_moduli). Elastic isotropic models
    only (axg_adjoint_run returns AXG_E_UNSUPPORTED otherwise). */
 int  axg_set_adjoint_slices(axg_solver *h, int32_t on);
 /* after such a run: grad_moduli_slices per element [2][nr_e][25] (lambda, mu), elements in

@@ -259,8 +259,8 @@ def test_attenuation_adjoint_moduli_gradient(built, kind, rtz, att):
 
 
 def test_wide_adjoint_rejects_slices_and_3d_moduli(built):
-    """Per-slice sensitivities stay isotropic and elastic; 3-D (per-slice) moduli stay
-    undifferentiated."""
+    """Per-slice sensitivities stay isotropic and elastic; 3-D (per-slice) TI moduli stay
+    undifferentiated (3-D elements must be isotropic and elastic)."""
     from axisem3d_b200 import meshgen
     from axisem3d_b200.solver import EngineError, Solver
     m = _wide_model("tiso", False, sources=False)
@@ -270,11 +270,108 @@ def test_wide_adjoint_rejects_slices_and_3d_moduli(built):
         r = np.zeros_like(s.seismograms())
         with pytest.raises(EngineError, match="per-slice sensitivities need isotropic"):
             s.adjoint(r, slices=True)
+    from axisem3d_b200 import _lib as L
     m3 = meshgen.cartesian_model(nx=4, nz=4, nr=5, nstations=4)
     ne = m3.n_solid_elements
+    lam, mu = m3.se_moduli.reshape(ne, 2, 25)[0, :, 0]
     m3.se_is3d = np.ones(ne, np.uint8)
-    m3.se_moduli = np.repeat(m3.se_moduli.reshape(ne, 2, 1, 25), 5, axis=2).ravel()
-    m3.se_mat_off = np.arange(ne, dtype=np.int64) * 250
+    m3.se_rheo = np.full(ne, L.AXG_TISO, np.int32)
+    m3.se_moduli = np.tile(np.repeat(np.array([lam + 2 * mu, lam + 2 * mu, lam, mu, mu]), 5 * 25), ne)
+    m3.se_mat_off = np.arange(ne, dtype=np.int64) * 5 * 5 * 25
     with Solver(m3, "fp64") as s:
-        with pytest.raises(EngineError, match="phi-constant"):
+        with pytest.raises(EngineError, match="3-D elements must be isotropic"):
             s.forward_checkpointed(10, 5)
+
+
+def _model3d_elastic(nr, sources, seed=7, pert=0.05):
+    """The 8 x 8 box with 3-D isotropic elements: lambda, mu per (slice, point) with seeded
+    5 % perturbations around the background (a 3-D model), 1-D masses."""
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=8, nz=8, nr=nr, nstations=12, nr_aware_dt=True)
+    m.dt = meshgen.round_dt(m.dt * 0.9)
+    if not sources:
+        m.ms_elem = np.zeros(0, np.int32)
+        m.ms_nu = np.zeros(0, np.int32)
+        m.ms_pat_off = np.zeros(0, np.int64)
+        m.ms_pattern = np.zeros(0, np.complex128)
+        m.ms_stf = []
+    ne = m.n_solid_elements
+    rng = np.random.default_rng(seed)
+    iso = m.se_moduli.reshape(ne, 2, 1, 25)
+    m3 = np.repeat(iso, nr, axis=2) * (1.0 + pert * rng.uniform(-1.0, 1.0, (ne, 2, nr, 25)))
+    m.se_is3d = np.ones(ne, np.uint8)
+    m.se_moduli = m3.ravel()
+    m.se_mat_off = np.arange(ne, dtype=np.int64) * 2 * nr * 25
+    return m
+
+
+@pytest.mark.parametrize("nr", [9, 8])
+def test_3d_moduli_adjoint_dot_product(built, nr):
+    """The dot-product test on a 3-D model (per-slice moduli couple the Fourier modes; the
+    transpose is W K W^-1 with the azimuthal weights, the Nyquist mode of the even nr
+    included): <R Phi(u0, v0), r> == <u0, ubar0(r)> + <v0, vbar0(r)> in FP64."""
+    from axisem3d_b200 import meshgen
+    from axisem3d_b200.solver import Solver
+    m = _model3d_elastic(nr, sources=False)
+    rng = np.random.default_rng(0)
+    u0 = meshgen.random_displacement(m, seed=1)
+    v0 = meshgen.random_displacement(m, seed=2) * 50.0
+    with Solver(m, "fp64") as s:
+        s.set_field(u0, "displ")
+        s.set_field(v0, "veloc")
+        s.forward_checkpointed(230, 64)
+        seis = s.seismograms()
+        r = rng.normal(size=seis.shape)
+        g = s.adjoint(r)
+    assert np.all(np.isfinite(seis)) and float(np.max(np.abs(seis))) > 0
+    lhs = float(np.sum(seis * r))
+    rhs = float(np.sum(np.real(np.conj(u0) * g["displ0"])) + np.sum(np.real(np.conj(v0) * g["veloc0"])))
+    assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), 1e-300), (lhs, rhs)
+
+
+def test_3d_moduli_adjoint_per_slice_gradient(built):
+    """On a 3-D background (per-slice lambda, mu): the per-slice sensitivities against
+    Richardson-extrapolated central differences of the L2 waveform misfit along six random
+    per-slice directions, and their sums over the slices against the gradient by a
+    phi-constant change."""
+    from axisem3d_b200.solver import Solver
+    nr = 9
+    base = _model3d_elastic(nr, sources=True, seed=7)
+    ne = base.n_solid_elements
+    nsteps, interval = 300, 50
+
+    def run(model):
+        with Solver(model, "fp64") as s:
+            s.forward_checkpointed(nsteps, interval)
+            return s.seismograms()
+
+    obs = run(base)
+    rng = np.random.default_rng(17)
+    x0 = base.se_moduli * (1.0 + 0.02 * rng.uniform(-1.0, 1.0, base.se_moduli.shape))
+
+    def model_at(x):
+        m = copy.deepcopy(base)
+        m.se_moduli = x
+        return m
+
+    with Solver(model_at(x0), "fp64") as s:
+        s.forward_checkpointed(nsteps, interval)
+        d = s.seismograms()
+        g = s.adjoint(d - obs, slices=True)
+    g3 = np.stack(g["moduli_slices"])                    # (ne, 2, nr, 25)
+    assert g3.shape == (ne, 2, nr, 25)
+    assert np.allclose(g3.sum(axis=2), g["moduli"], rtol=1e-9, atol=1e-12 * np.abs(g["moduli"]).max())
+    grad = g3.ravel()
+
+    def misfit_at(eps, dirv):
+        return 0.5 * float(np.sum((run(model_at(x0 + eps * dirv)) - obs) ** 2))
+
+    scale = float(np.mean(np.abs(x0)))
+    eps = 1e-4
+    for k in range(6):
+        dirv = rng.normal(size=x0.shape) * scale
+        f1 = (misfit_at(eps, dirv) - misfit_at(-eps, dirv)) / (2 * eps)
+        f2 = (misfit_at(eps / 2, dirv) - misfit_at(-eps / 2, dirv)) / eps
+        fd = (4 * f2 - f1) / 3
+        an = float(np.dot(grad, dirv))
+        assert abs(fd - an) <= 1e-6 * max(abs(an), 1e-300), (k, f1, f2, fd, an)
