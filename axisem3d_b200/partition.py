@@ -323,8 +323,8 @@ class PartitionedRun:
         self.plan = exchange_plan(model, self.se_part, self.fe_part, self.nparts)[self.rank]
         self.solver = make_solver(self.sub)
         self.device_path = hasattr(self.solver, "gather_stiffness") and device is not None
-        if self.overlap and not (self.device_path and hasattr(self.solver, "compute_stiffness_part")):
-            raise ValueError("PartitionedRun || overlap needs the engine's device path")
+        if self.overlap and not hasattr(self.solver, "compute_stiffness_part"):
+            raise ValueError("PartitionedRun || overlap needs a solver with compute_stiffness_part")
         self.device = device
         self.torch = torch
         self._dev = {}
@@ -393,6 +393,37 @@ class PartitionedRun:
         reqs = dist.batch_isend_irecv(ops) if ops else []
         return reqs, recv
 
+    def _host_exchange_start(self):
+        """Host path: send the shared points' stiffness as it stands, post the receives."""
+        dist, torch = self.dist, self.torch
+        ops, recv = [], []
+        for solid in (True, False):
+            if not ((solid and len(self.sub.sp_nr)) or (not solid and len(self.sub.fp_nr))):
+                continue
+            f = self.solver.get_field("stiff", solid=solid)
+            for other in sorted(self.plan):
+                slots = self.plan[other][0 if solid else 1]
+                if not len(slots):
+                    continue
+                send = torch.view_as_real(torch.from_numpy(np.ascontiguousarray(f[slots])))
+                rbuf = torch.zeros_like(send)
+                ops.append(dist.P2POp(dist.isend, send, other))
+                ops.append(dist.P2POp(dist.irecv, rbuf, other))
+                recv.append((solid, slots, rbuf))
+        reqs = dist.batch_isend_irecv(ops) if ops else []
+        return reqs, recv
+
+    def _host_exchange_finish(self, reqs, recv):
+        for req in reqs:
+            req.wait()
+        fields = {}
+        for solid, slots, rbuf in recv:
+            if solid not in fields:
+                fields[solid] = self.solver.get_field("stiff", solid=solid)
+            fields[solid][slots] += self.torch.view_as_complex(rbuf).numpy()
+        for solid, f in fields.items():
+            self.solver.set_field(f, "stiff", solid=solid)
+
     def _exchange_finish(self, reqs, recv):
         for req in reqs:
             req.wait()
@@ -406,6 +437,20 @@ class PartitionedRun:
         solid-fluid pairs live on one rank; the Clayton terms of shared points are on every
         copy)."""
         s = self.solver
+        if self.overlap and not self.device_path:
+            # host transport: the shared points' values after part 0 travel while part 1
+            # (which touches none of them) computes
+            s.apply_sources(tstep)
+            s.compute_stiffness_part(0)
+            pending = self._host_exchange_start()
+            s.compute_stiffness_part(1)
+            self._host_exchange_finish(*pending)
+            s.apply_bc_before_assembly()
+            s.record_stations(tstep)
+            s.apply_bc_after_assembly()
+            s.stiff_to_accel()
+            s.newmark_update()
+            return
         if self.overlap:
             with self.torch.cuda.stream(self.stream):
                 s.apply_sources(tstep)

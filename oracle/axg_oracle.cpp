@@ -482,6 +482,14 @@ struct OracleBase {
     virtual void set_sponge3d(int solid, int n, const int32_t *pt, const int64_t *off, const double *g) = 0;
     virtual void apply_sources(int tstep) = 0;
     virtual void compute_stiffness(int nthreads) = 0;
+    // the elements of one part only (part 0 / 1 per element from set_element_parts): the
+    // order of a rank that hides its exchange behind the elements off the shared points
+    virtual void compute_stiffness_part(int nthreads, int part) = 0;
+    void set_element_parts(const uint8_t *s, int ns, const uint8_t *f, int nf) {
+        se_part.assign(s ? s : nullptr, s ? s + ns : nullptr);
+        fe_part.assign(f ? f : nullptr, f ? f + nf : nullptr);
+    }
+    std::vector<uint8_t> se_part, fe_part;
     virtual void bc_before() = 0;
     virtual void bc_after() = 0;
     virtual void stiff_to_accel() = 0;
@@ -1476,9 +1484,21 @@ struct Oracle : OracleBase {
         }
     }
 
-    void compute_stiffness(int nthreads) override {
+    void compute_stiffness(int nthreads) override { stiffness_of(nthreads, -1); }
+    void compute_stiffness_part(int nthreads, int part) override {
+        if (part < 0 || part > 1) throw std::runtime_error("axo_compute_stiffness_part || part must be 0 or 1.");
+        stiffness_of(nthreads, part);
+    }
+    // part < 0: every element
+    void stiffness_of(int nthreads, int part) {
         // elements are computed in parallel, assembled serially in element order
         // (Domain::computeStiffness, Domain.cpp:298-308)
+        auto in_s = [&](int i) {
+            return part < 0 || (int)(se_part.size() == se.size() ? se_part[i] : 0) == part;
+        };
+        auto in_f = [&](int i) {
+            return part < 0 || (int)(fe_part.size() == fe.size() ? fe_part[i] : 0) == part;
+        };
         int ne = (int)se.size();
         if (nthreads < 1) nthreads = 1;
         int chunk = 256;
@@ -1487,7 +1507,8 @@ struct Oracle : OracleBase {
             std::vector<std::vector<Cx<R>>> out(hi - base);
             auto work = [&](int t) {
                 std::vector<CM<R>> S, E;
-                for (int i = base + t; i < hi; i += nthreads) solid_element(se[i], out[i - base], S, E);
+                for (int i = base + t; i < hi; i += nthreads)
+                    if (in_s(i)) solid_element(se[i], out[i - base], S, E);
             };
             if (nthreads == 1) work(0);
             else {
@@ -1496,6 +1517,7 @@ struct Oracle : OracleBase {
                 for (auto &x : th) x.join();
             }
             for (int i = base; i < hi; i++) {
+                if (!in_s(i)) continue;
                 // addStiffToPoints -> SolidPoint::gatherStiffFromElement (SolidPoint.hpp:101-109)
                 const SolidElem<R> &el = se[i];
                 const std::vector<Cx<R>> &f = out[i - base];
@@ -1508,7 +1530,9 @@ struct Oracle : OracleBase {
             }
         }
         std::vector<Cx<R>> f;
-        for (auto &el : fe) {
+        for (size_t i = 0; i < fe.size(); i++) {
+            if (!in_f((int)i)) continue;
+            const FluidElem<R> &el = fe[i];
             fluid_element(el, f);
             for (int q = 0; q < N; q++) {
                 int p = el.pts[q];
@@ -1971,6 +1995,12 @@ int axo_set_clayton3d(void *h, int solid, const axg_clayton3d *c) { AXO_TRY(stat
 int axo_set_sponge3d(void *h, int solid, int n, const int32_t *pt, const int64_t *off, const double *g) { AXO_TRY(static_cast<OracleBase *>(h)->set_sponge3d(solid, n, pt, off, g)) }
 int axo_apply_sources(void *h, int tstep) { AXO_TRY(static_cast<OracleBase *>(h)->apply_sources(tstep)) }
 int axo_compute_stiffness(void *h, int nthreads) { AXO_TRY(static_cast<OracleBase *>(h)->compute_stiffness(nthreads)) }
+int axo_compute_stiffness_part(void *h, int nthreads, int part) {
+    AXO_TRY(static_cast<OracleBase *>(h)->compute_stiffness_part(nthreads, part))
+}
+int axo_set_element_parts(void *h, const uint8_t *s, int ns, const uint8_t *f, int nf) {
+    AXO_TRY(static_cast<OracleBase *>(h)->set_element_parts(s, ns, f, nf))
+}
 int axo_bc_before(void *h) { AXO_TRY(static_cast<OracleBase *>(h)->bc_before()) }
 int axo_bc_after(void *h) { AXO_TRY(static_cast<OracleBase *>(h)->bc_after()) }
 int axo_stiff_to_accel(void *h) { AXO_TRY(static_cast<OracleBase *>(h)->stiff_to_accel()) }

@@ -64,6 +64,8 @@ def lib():
             "axo_scanning_nr": (C.c_int, [V, L.P_i32, L.P_i32]),
             "axo_set_sponge3d": (C.c_int, [V, C.c_int, C.c_int, L.P_i32, L.P_i64, L.P_f64]),
             "axo_compute_stiffness": (C.c_int, [V, C.c_int]),
+            "axo_compute_stiffness_part": (C.c_int, [V, C.c_int, C.c_int]),
+            "axo_set_element_parts": (C.c_int, [V, C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
             "axo_bc_before": (C.c_int, [V]),
             "axo_bc_after": (C.c_int, [V]),
             "axo_stiff_to_accel": (C.c_int, [V]),
@@ -235,6 +237,14 @@ class Oracle:
         if pt is not None and len(pt):
             self._chk(self.O.axo_set_ocean_load(self.h, len(pt), pt.ctypes.data_as(L.P_i32),
                                                 mo.ctypes.data_as(L.P_f64), th.ctypes.data_as(L.P_f64)))
+        sp_, fp_ = getattr(model, "se_part", None), getattr(model, "fe_part", None)
+        if sp_ is not None or fp_ is not None:
+            self._parts = [np.ascontiguousarray(x, np.uint8) if x is not None else None for x in (sp_, fp_)]
+            a, b = self._parts
+            self._chk(self.O.axo_set_element_parts(self.h, a.ctypes.data if a is not None else None,
+                                                   0 if a is None else len(a),
+                                                   b.ctypes.data if b is not None else None,
+                                                   0 if b is None else len(b)))
 
     def _chk(self, rc):
         if rc != 0:
@@ -256,6 +266,9 @@ class Oracle:
 
     def compute_stiffness(self):
         self._chk(self.O.axo_compute_stiffness(self.h, int(self.threads)))
+
+    def compute_stiffness_part(self, part):
+        self._chk(self.O.axo_compute_stiffness_part(self.h, int(self.threads), int(part)))
 
     def apply_bc_before_assembly(self):
         self._chk(self.O.axo_bc_before(self.h))
