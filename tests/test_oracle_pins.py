@@ -511,6 +511,20 @@ def test_oracle_patch_test_uniform_strain(built, rheology, mode):
     assert np.linalg.norm(f[~boundary]) <= 1e-10 * fb, np.linalg.norm(f[~boundary]) / fb
     # the other modes stay zero (phi-constant medium: the modes decouple)
     assert np.linalg.norm(np.delete(f_all, rows, axis=0)) == 0
+    # the energy scale: <u, K u> with the azimuthal weight (1 for mode 0, 2 for mode 1) is the
+    # strain energy density sigma : e of the uniform strain times the box's integral of s ds dz
+    # (the integral factor carries s; the engine's Fourier-space operator is the energy per 2 pi)
+    if rheology == "iso":
+        lam, mu = m.se_moduli.reshape(ne, 2, 25)[0, :, 0]
+        A = Cc = lam + 2 * mu
+        F, Lm, N = lam, mu, mu
+    if mode == 0:
+        ea, eb = 1e-3, -2e-3             # e_ss = e_phiphi = ea, e_zz = eb
+        density = 4 * A * ea * ea - 4 * N * ea * ea + 4 * F * ea * eb + Cc * eb * eb
+    else:
+        density = Lm * (1e-3 + 1.4e-3) ** 2    # gamma_xz = a + b
+    uKu = -(1.0 if mode == 0 else 2.0) * float(np.sum(np.real(np.conj(u.ravel()) * f_all.ravel())))
+    assert abs(uKu - density * width ** 2 / 2 * height) <= 1e-10 * abs(uKu), uKu / (density * width ** 2 / 2 * height)
     # the same field with a quadratic term in z is not a patch: the check has teeth
     u[rows, 2] += 1e-8 * z ** 2
     assert np.linalg.norm(force(u)[1][~boundary]) > 1e-6 * fb
