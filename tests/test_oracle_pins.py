@@ -469,7 +469,9 @@ def test_oracle_patch_test_uniform_strain(built, rheology, mode):
     carry the traction. Mode 0: u_x = a x, u_y = a y, u_z = b z, i.e. u_s = a s, u_z = b z.
     Mode 1 (the azimuthal derivative terms and the axis rows of the gradient): the shear
     u_x = a z, u_z = b x, i.e. u_s = a z cos phi, u_phi = -a z sin phi, u_z = b s cos phi, whose
-    mode-1 coefficients (u = 2 Re(c e^{i phi})) are a z / 2, i a z / 2 and b s / 2."""
+    mode-1 coefficients (u = 2 Re(c e^{i phi})) are a z / 2, i a z / 2 and b s / 2. The
+    absolute scale too: <u, K u> (azimuthal weight 1 / 2) equals sigma : e times the integral
+    of s ds dz over the box (1e-10)."""
     import oracle as O
     from axisem3d_b200 import _lib as L
     from axisem3d_b200 import meshgen
