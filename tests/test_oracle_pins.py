@@ -667,3 +667,49 @@ def test_oracle_newmark_conserves_discrete_energy(built):
     assert E[0] > 0
     assert np.abs(E - E[0]).max() <= 1e-13 * E[0], np.abs(E - E[0]).max() / E[0]
     assert np.abs(E_plain - E_plain[0]).max() > 1e-3 * E_plain[0]
+
+
+@pytest.mark.parametrize("alpha", [2, 3, 4])
+@pytest.mark.parametrize("rheology", ["iso", "tiso"])
+def test_oracle_antiplane_patch_higher_modes(built, rheology, alpha):
+    """The patch test in the higher Fourier modes: the anti-plane field u_z = Re((x + i y)^a)
+    / W^a = (s / W)^a cos(a phi) is harmonic, so in a homogeneous isotropic or z-axis TI medium
+    (sigma_xz, sigma_yz = L grad u_z) it is in equilibrium and leaves no force off the box's
+    outer boundary, the axis included (all modes a >= 2 vanish there). (s / W)^a with a <= 4 is
+    in the element basis and the weak form's integrands stay within the GLL / GLJ rules'
+    degree 7, so the check is exact to round-off: it pins the a^2 / s terms of the gradient and
+    the quadrature and their axis rows. Scale: <u, K u> (weight 2) = L a H / 2."""
+    import oracle as O
+    from axisem3d_b200 import _lib as L
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=6, nz=5, nr=9)
+    ne = m.n_solid_elements
+    lam, mu = m.se_moduli.reshape(ne, 2, 25)[0, :, 0]
+    shear = mu
+    if rheology == "tiso":
+        A, Cc, F, Lm, N = (lam + 2 * mu) * 1.08, (lam + 2 * mu) * 0.95, lam * 1.1, mu * 0.9, mu * 1.05
+        m.se_rheo = np.full(ne, L.AXG_TISO, np.int32)
+        m.se_moduli = np.tile(np.repeat(np.array([A, Cc, F, Lm, N]), 25), ne)
+        m.se_mat_off = np.arange(ne, dtype=np.int64) * 125
+        shear = Lm
+    o = O.Oracle(m, "fp64")
+    nu = np.asarray(m.sp_nr) // 2 + 1
+    first = np.concatenate([[0], np.cumsum(nu)[:-1]])
+    rows = first + alpha
+    s, z = m.sp_coords[:, 0], m.sp_coords[:, 1]
+    width, height = s.max(), -z.min()
+    u = np.zeros((int(nu.sum()), 3), complex)
+    u[rows, 2] = 0.5 * (s / width) ** alpha         # u_z = 2 Re(c e^{i a phi})
+    f_all = _stiff(o, u.ravel()).reshape(-1, 3)
+    f = f_all[rows].copy()
+    eps = 1e-9 * max(width, height)
+    axis = s < eps
+    boundary = (np.abs(s - width) < eps) | (np.abs(z) < eps) | (np.abs(z + height) < eps)
+    f[axis] = _axial_projection(f[axis], alpha)
+    fb = np.linalg.norm(f[boundary])
+    assert fb > 0 and np.any(~boundary & axis)
+    assert np.linalg.norm(f[~boundary]) <= 1e-10 * fb, np.linalg.norm(f[~boundary]) / fb
+    assert np.linalg.norm(np.delete(f_all, rows, axis=0)) == 0
+    uKu = -2.0 * float(np.sum(np.real(np.conj(u.ravel()) * f_all.ravel())))
+    want = shear * alpha * height / 2
+    assert abs(uKu - want) <= 1e-10 * want, uKu / want
