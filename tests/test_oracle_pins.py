@@ -713,3 +713,79 @@ def test_oracle_antiplane_patch_higher_modes(built, rheology, alpha):
     uKu = -2.0 * float(np.sum(np.real(np.conj(u.ravel()) * f_all.ravel())))
     want = shear * alpha * height / 2
     assert abs(uKu - want) <= 1e-10 * want, uKu / want
+
+
+def _fluid_box(nr=9):
+    """The plain forward box with every element made a fluid element (scalar potential) of
+    homogeneous 1/rho, no solid elements, sources or stations."""
+    import copy
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=6, nz=5, nr=nr, nstations=1)
+    f = copy.copy(m)
+    ne = m.n_solid_elements
+    f.fe_nr, f.fe_pts, f.fe_axial, f.fe_geom = m.se_nr, m.se_pts, m.se_axial, m.se_geom
+    f.fe_is3d = np.zeros(ne, np.uint8)
+    f.fe_mat_off = np.arange(ne, dtype=np.int64) * 25
+    f.fe_moduli = np.full(ne * 25, 1.0 / 2700.0)
+    f.fp_nr, f.fp_mass, f.fp_axial = m.sp_nr, m.sp_mass, m.sp_axial
+    f.fp_surface = np.zeros(len(m.sp_nr), np.uint8)
+    f.fp_coords = m.sp_coords
+    f.se_nr = np.zeros(0, np.int32)
+    f.se_pts = np.zeros((0, 25), np.int32)
+    f.se_axial = np.zeros(0, np.uint8)
+    f.se_geom = np.zeros((0, 6, 25))
+    f.se_rheo = np.zeros(0, np.int32)
+    f.se_is3d = np.zeros(0, np.uint8)
+    f.se_mat_off = np.zeros(0, np.int64)
+    f.se_moduli = np.zeros(0)
+    f.meta_rho = None
+    f.sp_nr = np.zeros(0, np.int32)
+    f.sp_mass = np.zeros(0)
+    f.sp_axial = np.zeros(0, np.uint8)
+    f.sp_coords = np.zeros((0, 2))
+    f.ms_elem = np.zeros(0, np.int32)
+    f.ms_nu = np.zeros(0, np.int32)
+    f.ms_pat_off = np.zeros(0, np.int64)
+    f.ms_pattern = np.zeros(0, np.complex128)
+    f.ms_stf = []
+    f.st_elem = np.zeros(0, np.int32)
+    f.st_w = np.zeros((0, 25))
+    f.st_phi = np.zeros(0)
+    return f
+
+
+@pytest.mark.parametrize("alpha", [0, 1, 2, 3, 4])
+def test_oracle_fluid_patch_test(built, alpha):
+    """The fluid element's patch test: in a homogeneous fluid the weak form of div(grad chi / rho)
+    leaves no force off the box's outer boundary for a harmonic potential, exactly for one in
+    the element basis: chi = z / H (mode 0) and chi = (s / W)^a cos(a phi) = Re((x + i y)^a) / W^a
+    (modes 1-4), axis points included (mode >= 1 of a fluid axis point is projected out).
+    Scale: <chi, K chi> (azimuthal weight 1 / 2) = (1 / rho) times the integral of |grad chi|^2
+    s ds dz over the box per 2 pi: W^2 / (2 H) for mode 0, a H / 2 for mode a."""
+    import oracle as O
+    m = _fluid_box()
+    o = O.Oracle(m, "fp64")
+    nu = np.asarray(m.fp_nr) // 2 + 1
+    first = np.concatenate([[0], np.cumsum(nu)[:-1]])
+    rows = first + alpha
+    s, z = m.fp_coords[:, 0], m.fp_coords[:, 1]
+    width, height = s.max(), -z.min()
+    chi = np.zeros(int(nu.sum()), complex)
+    chi[rows] = z / height if alpha == 0 else 0.5 * (s / width) ** alpha
+    o.set_field(chi, "displ", solid=False)
+    o.set_field(np.zeros_like(chi), "stiff", solid=False)
+    o.compute_stiffness()
+    f_all = o.get_field("stiff", solid=False)
+    f = f_all[rows].copy()
+    eps = 1e-9 * max(width, height)
+    axis = s < eps
+    boundary = (np.abs(s - width) < eps) | (np.abs(z) < eps) | (np.abs(z + height) < eps)
+    if alpha >= 1:
+        f[axis] = 0                          # AxialBoundary: fluid modes >= 1 vanish on the axis
+    fb = np.linalg.norm(f[boundary])
+    assert fb > 0 and np.any(~boundary & axis)
+    assert np.linalg.norm(f[~boundary]) <= 1e-10 * fb, np.linalg.norm(f[~boundary]) / fb
+    assert np.linalg.norm(np.delete(f_all, rows)) == 0
+    kk = -(1.0 if alpha == 0 else 2.0) * float(np.sum(np.real(np.conj(chi) * f_all)))
+    want = (width ** 2 / (2 * height) if alpha == 0 else alpha * height / 2) / 2700.0
+    assert abs(kk - want) <= 1e-10 * want, kk / want
