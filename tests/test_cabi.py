@@ -46,6 +46,31 @@ def _dump(m, path):
             f.write(a.tobytes())
 
 
+def test_header_is_plain_c_and_links_from_c(built, tmp_path):
+    """include/axg.h is an ISO C99 header (plain pointers, fixed-width integers, no C++): a C
+    translation unit that takes the address of every declared entry point compiles with
+    -std=c99 -pedantic -Werror and links against libaxg.so with the C driver, so C and Fortran
+    (ISO_C_BINDING) callers can bind it as well as the reference's C++. Runs without a GPU (no
+    entry point is called)."""
+    import re
+    from axisem3d_b200.build import build
+    lib = build()
+    hdr = open(os.path.join(ROOT, "include", "axg.h")).read()
+    names = sorted(set(re.findall(r"\b(axg_[a-z0-9_]+)\s*\(", hdr)))
+    src = os.path.join(str(tmp_path), "c_abi.c")
+    with open(src, "w") as f:
+        f.write('#include "axg.h"\n#include <stdio.h>\ntypedef void (*fn_t)(void);\nint main(void) {\n'
+                "    fn_t fns[] = {\n")
+        f.write("".join("        (fn_t)%s,\n" % n for n in names))
+        f.write('    };\n    printf("%d\\n", (int)(sizeof fns / sizeof fns[0]));\n    return 0;\n}\n')
+    exe = os.path.join(str(tmp_path), "c_abi")
+    libdir = os.path.dirname(lib)
+    subprocess.run(["gcc", "-std=c99", "-pedantic", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    src, "-L", libdir, "-laxg", "-Wl,-rpath," + libdir, "-o", exe], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    assert int(out) == len(names) > 30
+
+
 def test_cabi_program_compiles_and_links(built, tmp_path):
     exe = _build(tmp_path)
     assert os.access(exe, os.X_OK)
