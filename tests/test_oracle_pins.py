@@ -789,3 +789,53 @@ def test_oracle_fluid_patch_test(built, alpha):
     kk = -(1.0 if alpha == 0 else 2.0) * float(np.sum(np.real(np.conj(chi) * f_all)))
     want = (width ** 2 / (2 * height) if alpha == 0 else alpha * height / 2) / 2700.0
     assert abs(kk - want) <= 1e-10 * want, kk / want
+
+
+def test_oracle_station_records_the_analytic_field(built):
+    """Station recording (Station::interpolate, computeFourierAtPhiExp, eigen_tools.hpp:78-106):
+    with a displacement whose Fourier coefficients are polynomials of degree <= 4 in s and in
+    z (inside the element basis, GLJ rows on the axis), a station at any (xi, eta, phi) of any
+    element records the field's value there, u(s, z, phi) = Re c_0 + 2 sum_a Re(c_a e^{i a phi}),
+    to round-off: on and off the axis, at interior and edge positions."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=6, nz=5, nr=5, nstations=1)
+    nu = np.asarray(m.sp_nr) // 2 + 1
+    first = np.concatenate([[0], np.cumsum(nu)[:-1]])
+    s, z = m.sp_coords[:, 0], m.sp_coords[:, 1]
+    width, height = s.max(), -z.min()
+
+    def coeffs(s, z):
+        x, y = s / width, z / height
+        return [np.asarray(1.0 + 0.5 * x - 2.0 * y ** 2 + x ** 3 * y, complex),
+                (x - 0.3 * x ** 2 * y) + 1j * (0.7 * x * y ** 2 - x ** 4),
+                (x ** 2 + 0.2 * y ** 4) * (0.5 - 1.5j)]
+
+    u = np.zeros((int(nu.sum()), 3), complex)
+    for al, c in enumerate(coeffs(s, z)):
+        for comp, scale in enumerate((1.0, -0.4, 2.5)):
+            u[first + al, comp] = scale * (c if al else c.real)
+    rng = np.random.default_rng(5)
+    ne, nz_ = m.n_solid_elements, 5
+    picks = [(0, -1.0, 0.3), (0, 0.2, -0.7), (7, 0.5, 0.5), (12, -0.9, 1.0), (29, 1.0, -1.0), (3, 0.0, 0.0)]
+    st_e, st_w, st_phi, where = [], [], [], []
+    for e, xi, eta in picks:
+        axial = bool(m.se_axial[e])
+        st_e.append(e)
+        st_w.append(meshgen.inplane_weights(xi, eta, axial))
+        st_phi.append(rng.uniform(0, 2 * np.pi))
+        i, j = divmod(e, nz_)
+        h_s, h_z = width / 6, height / 5
+        where.append(((i + (xi + 1) / 2) * h_s, -height + (j + (eta + 1) / 2) * h_z))
+    m.st_elem = np.array(st_e, np.int32)
+    m.st_w = np.array(st_w)
+    m.st_phi = np.array(st_phi)
+    o = O.Oracle(m, "fp64")
+    o.set_field(u.ravel(), "displ")
+    o.record_stations(0)
+    got = o.seismograms()[0]
+    for k, ((ss, zz), phi) in enumerate(zip(where, st_phi)):
+        c = coeffs(np.array(ss), np.array(zz))
+        for comp, scale in enumerate((1.0, -0.4, 2.5)):
+            want = scale * (c[0].real + sum(2 * np.real(c[al] * np.exp(1j * al * phi)) for al in (1, 2)))
+            assert abs(got[k, comp] - want) <= 1e-12 * (1 + abs(want)), (k, comp, got[k, comp], want)
