@@ -839,3 +839,48 @@ def test_oracle_station_records_the_analytic_field(built):
         for comp, scale in enumerate((1.0, -0.4, 2.5)):
             want = scale * (c[0].real + sum(2 * np.real(c[al] * np.exp(1j * al * phi)) for al in (1, 2)))
             assert abs(got[k, comp] - want) <= 1e-12 * (1 + abs(want)), (k, comp, got[k, comp], want)
+
+
+def test_oracle_moment_source_does_the_moment_tensors_work(built):
+    """The moment-tensor source (Mechanism::release for a source on the axis, Mechanism.cpp:
+    131-222, injected through SolidElement::addMomentSource, SolidElement.cpp:273-356): its
+    nodal force does on any uniform-strain virtual displacement du the work M : e(du) at the
+    source, up to one common factor (the STF value, 2 pi, sign). With the azimuthal weights
+    (1 for mode 0, 2 for the others), the ratios of <du, F> over seven Cartesian-linear fields
+    in modes 0, 1 and 2 equal those of M_zz, M_xx + M_yy, M_xz (twice: du_x = z and du_z = x),
+    M_yz, M_xx - M_yy and 2 M_xy, with (x, y, z) = (theta, phi, r) of the source frame at the
+    axis: a pin of the pattern's mode structure and of the quadrature without integration."""
+    import oracle as O
+    from axisem3d_b200 import meshgen
+    m = meshgen.cartesian_model(nx=6, nz=5, nr=5, nstations=1)
+    mrr, mtt, mpp, mrt, mrp, mtp = m.meta["moment"]
+    Mxx, Myy, Mzz, Mxz, Myz, Mxy = mtt, mpp, mrr, mrt, mrp, mtp
+    o = O.Oracle(m, "fp64")
+    step = int(round(2.5 / m.dt))                     # near the Ricker's peak
+    o.apply_sources(step)
+    F = o.get_field("stiff").reshape(-1, 3)
+    assert np.abs(F).max() > 0
+    nu = np.asarray(m.sp_nr) // 2 + 1
+    first = np.concatenate([[0], np.cumsum(nu)[:-1]])
+    s, z = m.sp_coords[:, 0], m.sp_coords[:, 1]
+
+    def work(mode, cs, cp, cz):
+        du = np.zeros_like(F)
+        du[first + mode, 0], du[first + mode, 1], du[first + mode, 2] = cs, cp, cz
+        return (1.0 if mode == 0 else 2.0) * float(np.sum(np.real(np.conj(du) * F)))
+
+    zero = np.zeros_like(s)
+    fields = [
+        (work(0, zero, zero, z), Mzz),                        # du_z = z
+        (work(0, s, zero, zero), Mxx + Myy),                  # du = (x, y, 0)
+        (work(1, z / 2, 1j * z / 2, zero), Mxz),              # du_x = z
+        (work(1, zero, zero, s / 2), Mxz),                    # du_z = x
+        (work(1, -1j * z / 2, z / 2, zero), Myz),             # du_y = z
+        (work(2, s / 2, 1j * s / 2, zero), Mxx - Myy),        # du = (x, -y, 0)
+        (work(2, -1j * s / 2, s / 2, zero), 2 * Mxy),         # du = (y, x, 0)
+    ]
+    k = fields[0][0] / fields[0][1]
+    assert k != 0 and all(abs(w) > 0 for _, w in fields)
+    scale = max(abs(w) for _, w in fields)
+    for i, (got, want) in enumerate(fields):
+        assert abs(got - k * want) <= 1e-10 * abs(k) * scale, (i, got / k, want)
